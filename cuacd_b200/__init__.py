@@ -1,0 +1,353 @@
+"""cuacd_b200 — B200 (sm_100a) engine for cuacd's lookahead candidate path.
+
+`Context` mirrors `cuacd.Context` (cuacd/__init__.py:55-454 in the
+reference): same constructor, method names, argument meaning, return types
+and error behaviour (RuntimeError "cuacd error <code>: <message>").  Every
+method runs hand-written CUDA kernels from libcuacd_b200.so through its C
+ABI (include/cuacd_b200.h); there is no CPU fallback — importing this
+package fails if the library is missing.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "libcuacd_b200.so")
+
+if not os.path.exists(_LIB_PATH):
+    raise ImportError(
+        f"cuacd_b200 native library is missing ({_LIB_PATH}); build it with "
+        f"`python -c 'import cuacd_b200.build as b; b.build()'` (needs nvcc)")
+
+_lib = ctypes.CDLL(_LIB_PATH)
+
+_P = ctypes.c_void_p
+_I = ctypes.c_int
+_F = ctypes.c_float
+
+
+class CandResult(ctypes.Structure):
+    """Mirror of cuacd_cand_result (include/cuacd_b200.h)."""
+    _fields_ = [
+        ("ok", _I), ("nv", _I * 2), ("nt", _I * 2), ("n_cap", _I),
+        ("hull_nv", _I * 2), ("hull_nt", _I * 2),
+        ("mesh_vol", _F * 2), ("hull_vol", _F * 2), ("hausdorff", _F * 2),
+        ("cost_rv", _F * 2), ("cost_full", _F * 2),
+        ("score_rv", _F), ("score_full", _F), ("err", _I),
+    ]
+
+
+class PartResult(ctypes.Structure):
+    _fields_ = [
+        ("verts", ctypes.POINTER(ctypes.c_float)), ("tris", ctypes.POINTER(ctypes.c_int)),
+        ("nv", _I), ("nt", _I),
+        ("hull_verts", ctypes.POINTER(ctypes.c_float)), ("hull_tris", ctypes.POINTER(ctypes.c_int)),
+        ("hull_nv", _I), ("hull_nt", _I),
+        ("mesh_vol", _F), ("hull_vol", _F), ("hausdorff", _F),
+    ]
+
+
+class GpuResult(ctypes.Structure):
+    _fields_ = [("parts", ctypes.POINTER(PartResult)), ("nparts", _I)]
+
+
+def _sig(name, res, args):
+    fn = getattr(_lib, name)
+    fn.restype = res
+    fn.argtypes = args
+    return fn
+
+
+_sig("gpu_init", _I, [ctypes.POINTER(_P), _I, ctypes.c_size_t])
+_sig("gpu_destroy", None, [_P])
+_sig("gpu_last_error", ctypes.c_char_p, [_P])
+_sig("gpu_heap_compact", _I, [_P])
+_sig("gpu_pool_usage", ctypes.c_size_t, [_P])
+_sig("gpu_heap_stats", _I, [_P, ctypes.POINTER(ctypes.c_ulonglong * 6)])
+_sig("gpu_hull_dandc", _I, [_P, _P, _I, _P, _I, _I, _I, _I, _P, _P, _P, _P, _P])
+_sig("gpu_kdop_hull", _I, [_P, _P, _I, _P, _I, _I, _I, _P, _P, _P, _P, _P, _P])
+_sig("gpu_batch_mesh_volume", _I, [_P, _P, _I, _P, _I, _P, _P, _I, _P])
+_sig("gpu_test_mesh_volume", _I, [_P, _P, _I, _P, _I, _P])
+_sig("cuacd_launch_count", ctypes.c_ulonglong, [_P])
+
+_OPTIONAL = {}
+
+
+def _opt(name, res, args):
+    """Entry points bound lazily (a missing symbol raises at call time)."""
+    try:
+        _OPTIONAL[name] = _sig(name, res, args)
+    except AttributeError:
+        _OPTIONAL[name] = None
+
+
+_opt("gpu_test_hausdorff", _I, [_P, _P, _I, _P, _I, _P, _I, _P, _I, _P])
+_opt("cuacd_hausdorff", _I, [_P, _P, _I, _P, _I, _P, _I, _P, _I, _F, _I, _I, _P])
+_opt("gpu_test_plane_cut", _I, [_P, _P, _I, _P, _I, _F, _F, _F, _F,
+                                _P, _I, _P, _I, _P, _I, _P, _I, _P, _P, _P, _P])
+_opt("gpu_test_warp_sort", _I, [_P, _P, _I, _P, _I])
+_opt("cuacd_eval_candidates", _I, [_P, _P, _I, _P, _I, _P, _I, _I, _F, _I, _I, _P])
+_opt("cuacd_eval_candidates_device", _I, [_P, _P, _I, _P, _I, _P, _I, _I, _F, _I, _I, _P, _P])
+_opt("cuacd_hull_batch_device", _I, [_P, _P, _P, _I, _I, _I, _I, _P, _P, _P, _P, _P, _P, _P])
+_opt("lookahead_decompose", _I, [_P, _P, _I, _P, _I, _P, _I, _P, _I,
+                                 _I, _I, _I, _F, _I, _I, _I, _I, _I, _I, _I,
+                                 _I, _F, _F, _I, _I, ctypes.POINTER(GpuResult)])
+_opt("gpu_result_free", None, [ctypes.POINTER(GpuResult)])
+
+
+def _fn(name):
+    f = _OPTIONAL.get(name) or getattr(_lib, name, None)
+    if f is None:
+        raise RuntimeError(f"cuacd error -1: {name} is not available in this build")
+    return f
+
+
+def native_library_path():
+    return _LIB_PATH
+
+
+def _as_f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def _as_i32(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def _ptr(a):
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+class Context:
+    """GPU context (mirror of cuacd.Context, cuacd/__init__.py:55-118).
+
+    Parameters
+    ----------
+    device : int
+        CUDA device ordinal; -1 keeps the current device.
+    pool_bytes : int
+        Device pool size in bytes; 0 lets the pool grow on demand.
+    """
+
+    def __init__(self, device=-1, pool_bytes=0):
+        h = ctypes.c_void_p()
+        rc = _lib.gpu_init(ctypes.byref(h), int(device), int(pool_bytes))
+        if rc != 0:
+            raise RuntimeError(f"cuacd error {rc}: gpu_init failed")
+        self._h = h
+        self._alive = True
+
+    # -- lifecycle ---------------------------------------------------------
+    def close(self):
+        if getattr(self, "_alive", False):
+            _lib.gpu_destroy(self._h)
+            self._alive = False
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *args):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    def _check(self, rc):
+        if rc != 0:
+            msg = _lib.gpu_last_error(self._h)
+            raise RuntimeError(f"cuacd error {rc}: {msg.decode() if msg else ''}")
+
+    def heap_compact(self):
+        """No-op kept for API compatibility (the pool is an arena)."""
+        self._check(_lib.gpu_heap_compact(self._h))
+
+    def pool_usage(self):
+        """High-water mark of device pool bytes."""
+        return int(_lib.gpu_pool_usage(self._h))
+
+    def heap_stats(self):
+        """(output_live, output_allocs, output_releases, scratch_live,
+        scratch_allocs, scratch_releases)."""
+        out = (ctypes.c_ulonglong * 6)()
+        self._check(_lib.gpu_heap_stats(self._h, ctypes.byref(out)))
+        return tuple(int(x) for x in out)
+
+    def launch_count(self):
+        return int(_lib.cuacd_launch_count(self._h))
+
+    # -- out of scope in this engine ---------------------------------------
+    def check_mesh(self, verts, tris):
+        raise NotImplementedError("check_mesh (mesh audit) is outside the candidate-evaluation path")
+
+    def preprocess(self, verts, tris, resolution=64):
+        raise NotImplementedError("preprocess (remeshing) is outside the candidate-evaluation path")
+
+    # -- hulls --------------------------------------------------------------
+    @staticmethod
+    def _pack(pts_list):
+        arrs = [_as_f32(p).reshape(-1, 3) for p in pts_list]
+        packed = np.ascontiguousarray(np.concatenate(arrs, axis=0)) if arrs else np.zeros((0, 3), np.float32)
+        off = np.zeros(len(arrs) + 1, dtype=np.int32)
+        for i, a in enumerate(arrs):
+            off[i + 1] = off[i] + len(a)
+        return arrs, packed, off
+
+    def _hull(self, pts_list, max_hv=None, max_ht=None):
+        arrs, packed, off = self._pack(pts_list)
+        n = len(arrs)
+        ns = [len(a) for a in arrs]
+        max_pts = max(ns)
+        max_hv = max_pts if max_hv is None else max_hv
+        max_ht = max(max(2 * k - 4 for k in ns), 4) if max_ht is None else max_ht
+        ov = np.empty(n * max(max_hv, 1) * 3, np.float32)
+        ot = np.empty(n * max(max_ht, 1) * 3, np.int32)
+        onv = np.empty(n, np.int32)
+        ont = np.empty(n, np.int32)
+        vol = np.empty(n, np.float32)
+        err = np.empty(n, np.int32)
+        self._check(_lib.gpu_kdop_hull(self._h, _ptr(packed), int(off[-1]), _ptr(off), n,
+                                       max_hv, max_ht, _ptr(ov), _ptr(ot), _ptr(onv), _ptr(ont),
+                                       _ptr(vol), _ptr(err)))
+        return ov, ot, onv, ont, vol, err, max_hv, max_ht
+
+    def batch_hull_volume(self, pts_list, algo=2):
+        """Convex hull volume per cloud -> (float32[n] volumes, int32[n] errors).
+        `algo` is accepted for compatibility and ignored."""
+        if len(pts_list) == 0:
+            return np.empty(0, np.float32), np.empty(0, np.int32)
+        _, _, onv, ont, vol, err, _, _ = self._hull(pts_list)
+        vol = np.where((onv > 0) & (ont > 0), vol, 0.0).astype(np.float32)
+        return vol, err
+
+    def _hull_meshes(self, pts_list, max_hv=None, max_ht=None):
+        if len(pts_list) == 0:
+            return []
+        ov, ot, onv, ont, vol, err, mhv, mht = self._hull(pts_list, max_hv, max_ht)
+        out = []
+        for i in range(len(pts_list)):
+            nv, nt = int(onv[i]), int(ont[i])
+            v = ov[i * mhv * 3: i * mhv * 3 + nv * 3].reshape(nv, 3).copy()
+            t = ot[i * mht * 3: i * mht * 3 + nt * 3].reshape(nt, 3).copy()
+            out.append((v, t, float(vol[i]) if nt > 0 else 0.0))
+        return out
+
+    def batch_hull_dandc_mesh(self, pts_list):
+        """Exact hull mesh per cloud -> [(verts f32[nv,3], tris i32[nt,3], volume)].
+        Bounds: nv <= n_pts, nt <= 2*n_pts - 4."""
+        return self._hull_meshes(pts_list)
+
+    def batch_kdop_hull_mesh(self, pts_list):
+        """Hull mesh per cloud with the reference's fixed output caps
+        (4096 vertices / 8192 triangles, cuacd/__init__.py:289-290)."""
+        return self._hull_meshes(pts_list, 4096, 8192)
+
+    # -- volumes -------------------------------------------------------------
+    def batch_mesh_volume(self, verts_list, tris_list):
+        """Volume of each watertight mesh -> float32[n]."""
+        n = len(verts_list)
+        if n == 0:
+            return np.empty(0, np.float32)
+        va = [_as_f32(v).reshape(-1, 3) for v in verts_list]
+        ta = [_as_i32(t).reshape(-1, 3) for t in tris_list]
+        allv = np.ascontiguousarray(np.concatenate(va, axis=0))
+        allt = np.ascontiguousarray(np.concatenate(ta, axis=0))
+        vo = np.zeros(n + 1, np.int32)
+        to = np.zeros(n + 1, np.int32)
+        for i in range(n):
+            vo[i + 1] = vo[i] + len(va[i])
+            to[i + 1] = to[i] + len(ta[i])
+        out = np.empty(n, np.float32)
+        self._check(_lib.gpu_batch_mesh_volume(self._h, _ptr(allv), int(vo[-1]), _ptr(allt), int(to[-1]),
+                                               _ptr(to), _ptr(vo), n, _ptr(out)))
+        return out
+
+    # -- Hausdorff / plane cut ---------------------------------------------
+    def hausdorff(self, a_verts, a_tris, b_verts, b_tris, resolution=2000.0, min_samples=1000, total=0):
+        """Bidirectional sampled Hausdorff distance between two meshes."""
+        av, at = _as_f32(a_verts).reshape(-1, 3), _as_i32(a_tris).reshape(-1, 3)
+        bv, bt = _as_f32(b_verts).reshape(-1, 3), _as_i32(b_tris).reshape(-1, 3)
+        out = np.zeros(1, np.float32)
+        self._check(_fn("cuacd_hausdorff")(self._h, _ptr(av), len(av), _ptr(at), len(at),
+                                           _ptr(bv), len(bv), _ptr(bt), len(bt),
+                                           float(resolution), int(min_samples), int(total), _ptr(out)))
+        return float(out[0])
+
+    def plane_cut(self, verts, tris, plane):
+        """Cut a closed mesh by plane (a,b,c,d) -> (pos_v, pos_t, neg_v, neg_t)."""
+        v, t = _as_f32(verts).reshape(-1, 3), _as_i32(tris).reshape(-1, 3)
+        cv, ct = 2 * len(v) + 16, 3 * len(t) + 16
+        pv = np.empty((cv, 3), np.float32); pt = np.empty((ct, 3), np.int32)
+        nv_ = np.empty((cv, 3), np.float32); nt_ = np.empty((ct, 3), np.int32)
+        c = [ctypes.c_int(0) for _ in range(4)]
+        self._check(_fn("gpu_test_plane_cut")(self._h, _ptr(v), len(v), _ptr(t), len(t),
+                                              *[float(x) for x in plane],
+                                              _ptr(pv), cv, _ptr(pt), ct, _ptr(nv_), cv, _ptr(nt_), ct,
+                                              *[ctypes.byref(x) for x in c]))
+        a, b, d, e = [x.value for x in c]
+        return pv[:a].copy(), pt[:b].copy(), nv_[:d].copy(), nt_[:e].copy()
+
+    # -- candidate evaluator -------------------------------------------------
+    def eval_candidates(self, verts, tris, planes, hausdorff=True, resolution=2000.0,
+                        min_samples=1000, total=0):
+        """Evaluate candidate planes on one closed mesh (cut, volumes, hulls,
+        Hausdorff, part costs).  Returns a list of dicts, one per plane."""
+        v, t = _as_f32(verts).reshape(-1, 3), _as_i32(tris).reshape(-1, 3)
+        p = _as_f32(planes).reshape(-1, 4)
+        out = (CandResult * len(p))()
+        self._check(_fn("cuacd_eval_candidates")(self._h, _ptr(v), len(v), _ptr(t), len(t), _ptr(p), len(p),
+                                                 1 if hausdorff else 0, float(resolution), int(min_samples),
+                                                 int(total), ctypes.cast(out, ctypes.c_void_p)))
+        return [cand_to_dict(r) for r in out]
+
+    # -- lookahead -----------------------------------------------------------
+    def lookahead_decompose(self, verts, tris, *, max_iters=100, width=60, width2=5, threshold=0.05,
+                            depth=2, quick_depth=0, max_n_cutting=16, verbose=0, debug=0,
+                            decompose_components=False, no_decompose_components_per_iter=False,
+                            n_concave_edges=32, concave_eps=0.005, concave_threshold=3.49,
+                            concave_iters=10, merge_hulls=False):
+        """Convex decomposition by lookahead tree search ->
+        [(verts, tris, hull_verts, hull_tris)] (cuacd/__init__.py:367-454)."""
+        verts = _as_f32(verts).reshape(-1, 3)
+        tris = _as_i32(tris).reshape(-1, 3)
+        if width2 is None:
+            width2 = width
+        total_width = width + 4 * n_concave_edges
+        if total_width >= 512:
+            raise ValueError(f"width + 4*n_concave_edges must be < 512 (got {total_width})")
+        hull = self.batch_hull_dandc_mesh([verts])[0]
+        hv, ht = _as_f32(hull[0]), _as_i32(hull[1])
+        res = GpuResult()
+        fn = _fn("lookahead_decompose")
+        self._check(fn(self._h, _ptr(verts), len(verts), _ptr(tris), len(tris), _ptr(hv), len(hv), _ptr(ht), len(ht),
+                       int(max_iters), int(width), int(width2), float(threshold), int(depth), int(quick_depth),
+                       int(max_n_cutting), int(verbose), int(debug), int(bool(decompose_components)),
+                       int(not no_decompose_components_per_iter), int(n_concave_edges), float(concave_eps),
+                       float(concave_threshold), int(concave_iters), int(bool(merge_hulls)), ctypes.byref(res)))
+        out = []
+        try:
+            for i in range(res.nparts):
+                p = res.parts[i]
+                v = np.ctypeslib.as_array(p.verts, (p.nv * 3,)).reshape(p.nv, 3).copy() if p.nv else np.zeros((0, 3), np.float32)
+                t = np.ctypeslib.as_array(p.tris, (p.nt * 3,)).reshape(p.nt, 3).copy() if p.nt else np.zeros((0, 3), np.int32)
+                hv_ = np.ctypeslib.as_array(p.hull_verts, (p.hull_nv * 3,)).reshape(p.hull_nv, 3).copy() if p.hull_nv else np.zeros((0, 3), np.float32)
+                ht_ = np.ctypeslib.as_array(p.hull_tris, (p.hull_nt * 3,)).reshape(p.hull_nt, 3).copy() if p.hull_nt else np.zeros((0, 3), np.int32)
+                out.append((v, t, hv_, ht_))
+        finally:
+            _fn("gpu_result_free")(ctypes.byref(res))
+        return out
+
+
+def cand_to_dict(r):
+    return {
+        "ok": r.ok, "nv": tuple(r.nv), "nt": tuple(r.nt), "n_cap": r.n_cap,
+        "hull_nv": tuple(r.hull_nv), "hull_nt": tuple(r.hull_nt),
+        "mesh_vol": tuple(r.mesh_vol), "hull_vol": tuple(r.hull_vol),
+        "hausdorff": tuple(r.hausdorff), "cost_rv": tuple(r.cost_rv),
+        "cost_full": tuple(r.cost_full), "score_rv": r.score_rv,
+        "score_full": r.score_full, "err": r.err,
+    }

@@ -1,0 +1,293 @@
+// capi.cu — extern "C" entry points of libcuacd_b200.so (see
+// include/cuacd_b200.h for the contract of each function).
+#include <cstdlib>
+#include <vector>
+#include <algorithm>
+#include "context.cuh"
+#include "volume.cuh"
+#include "hull.cuh"
+
+// ---------------------------------------------------------------------------
+// kernels
+// ---------------------------------------------------------------------------
+__global__ void k_arena_reset(Arena* a, char* base, unsigned long long cap)
+{
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        a->base = base; a->capacity = cap; a->offset = 0;
+        a->n_resets += 1;
+    }
+}
+
+__global__ void __launch_bounds__(HULL_NT)
+k_hull_batch(const float* __restrict__ pts, const int* __restrict__ offsets, int n_hulls,
+             char* scratch, size_t stride, int max_hv, int max_ht,
+             float* out_v, int* out_t, int* out_nv, int* out_nt, float* out_vol, int* out_err)
+{
+    __shared__ HullShared sh;
+    __shared__ int s_err;
+    int h = blockIdx.x;
+    if (h >= n_hulls) return;
+    if (threadIdx.x == 0) s_err = 0;
+    __syncthreads();
+    int a = offsets[h], n = offsets[h + 1] - offsets[h];
+    HullOut o;
+    o.verts = out_v + (size_t)h * max_hv * 3;
+    o.tris = out_t + (size_t)h * max_ht * 3;
+    o.vidx = nullptr;
+    o.max_hv = max_hv; o.max_ht = max_ht;
+    hull_cta(pts + 3 * (size_t)a, n, scratch + (size_t)h * stride, o,
+             &out_nv[h], &out_nt[h], out_vol ? &out_vol[h] : nullptr, &s_err, sh);
+    __syncthreads();
+    if (threadIdx.x == 0 && out_err) out_err[h] = s_err;
+}
+
+// ---------------------------------------------------------------------------
+// context
+// ---------------------------------------------------------------------------
+extern "C" void gpu_set_fatbin(const void* data, size_t len) { (void)data; (void)len; }
+
+extern "C" int gpu_init(gpu_ctx_t* out, int device_ordinal, size_t pool_bytes)
+{
+    if (!out) return -1;
+    *out = nullptr;
+    gpu_ctx* ctx = (gpu_ctx*)calloc(1, sizeof(gpu_ctx));
+    if (!ctx) return -1;
+    int dev = device_ordinal;
+    cudaError_t e;
+    if (dev < 0) {
+        e = cudaGetDevice(&dev);
+        if (e != cudaSuccess) { free(ctx); return (int)e; }
+    } else {
+        e = cudaSetDevice(dev);
+        if (e != cudaSuccess) { free(ctx); return (int)e; }
+    }
+    ctx->device = dev;
+    e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) { free(ctx); return (int)e; }
+    e = cudaMalloc(&ctx->d_arena, sizeof(Arena));
+    if (e != cudaSuccess) { cudaStreamDestroy(ctx->stream); free(ctx); return (int)e; }
+    cudaMemset(ctx->d_arena, 0, sizeof(Arena));
+    ctx->fixed = pool_bytes > 0;
+    size_t want = pool_bytes > 0 ? pool_bytes : ((size_t)256 << 20);
+    e = cudaMalloc(&ctx->pool, want);
+    if (e != cudaSuccess) {
+        cudaFree(ctx->d_arena); cudaStreamDestroy(ctx->stream); free(ctx); return (int)e;
+    }
+    ctx->cap = want;
+    *out = ctx;
+    return 0;
+}
+
+extern "C" void gpu_destroy(gpu_ctx_t ctx)
+{
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    if (ctx->pool) cudaFree(ctx->pool);
+    if (ctx->d_arena) cudaFree(ctx->d_arena);
+    cudaStreamDestroy(ctx->stream);
+    free(ctx);
+}
+
+extern "C" const char* gpu_last_error(gpu_ctx_t ctx) { return ctx ? ctx->last_error : "no context"; }
+extern "C" int gpu_heap_compact(gpu_ctx_t ctx) { (void)ctx; return 0; }
+extern "C" size_t gpu_pool_usage(gpu_ctx_t ctx)
+{
+    if (!ctx) return 0;
+    Arena a;
+    if (cudaMemcpy(&a, ctx->d_arena, sizeof(Arena), cudaMemcpyDeviceToHost) != cudaSuccess) return ctx->high_water;
+    size_t dev_hw = (size_t)a.high_water;
+    return ctx->high_water + dev_hw;
+}
+extern "C" int gpu_heap_stats(gpu_ctx_t ctx, unsigned long long out[6])
+{
+    if (!ctx || !out) return -1;
+    Arena a;
+    CK(cudaMemcpy(&a, ctx->d_arena, sizeof(Arena), cudaMemcpyDeviceToHost));
+    out[0] = a.offset;            // output bytes live in the device arena
+    out[1] = a.n_allocs;          // device allocations served
+    out[2] = a.n_resets;          // arena releases (resets)
+    out[3] = ctx->stats[3];       // scratch bytes carved by the last call
+    out[4] = ctx->stats[4];       // scratch carves
+    out[5] = ctx->stats[5];       // scratch releases
+    return 0;
+}
+extern "C" unsigned long long cuacd_launch_count(gpu_ctx_t ctx) { return ctx ? ctx->launches : 0; }
+
+static int sync_and_check(gpu_ctx* ctx, const char* what)
+{
+    cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) return ctx_fail(ctx, (int)e, "%s: %s", what, cudaGetErrorString(e));
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return ctx_fail(ctx, (int)e, "%s: %s", what, cudaGetErrorString(e));
+    return 0;
+}
+
+// ---------------------------------------------------------------------------
+// hulls
+// ---------------------------------------------------------------------------
+static int launch_hull_batch(gpu_ctx* ctx, const float* d_pts, const int* d_off, int n_hulls,
+                             int max_pts, int max_hv, int max_ht, float* d_v, int* d_t,
+                             int* d_nv, int* d_nt, float* d_vol, int* d_err, cudaStream_t s)
+{
+    size_t stride = al256(hull_scratch_bytes(max_pts));
+    char* scratch = pool_take<char>(ctx, stride * (size_t)n_hulls);
+    if (!scratch) return ctx_fail(ctx, KERR_HEAP_OOM, "hull scratch does not fit the pool");
+    k_hull_batch<<<n_hulls, HULL_NT, 0, s>>>(d_pts, d_off, n_hulls, scratch, stride, max_hv, max_ht,
+                                             d_v, d_t, d_nv, d_nt, d_vol, d_err);
+    ctx->launches++;
+    CK(cudaGetLastError());
+    return 0;
+}
+
+static int hull_common(gpu_ctx_t ctx, const float* pts, int total_pts, const int* offsets, int n_hulls,
+                       int max_pts, int max_hv, int max_ht, float* out_verts, int* out_tris,
+                       int* out_nv, int* out_nt, float* out_vol, int* out_err)
+{
+    if (!ctx) return -1;
+    if (n_hulls <= 0) return 0;
+    if (total_pts < 0 || max_pts < 0 || max_hv < 0 || max_ht < 0)
+        return ctx_fail(ctx, KERR_MESH_INVALID, "negative size");
+    for (int i = 0; i < n_hulls; i++) {
+        int n = offsets[i + 1] - offsets[i];
+        if (n < 0 || n > max_pts || offsets[i + 1] > total_pts)
+            return ctx_fail(ctx, KERR_MESH_INVALID, "hull %d: bad offsets", i);
+    }
+    if (max_pts >= (1 << 22)) return ctx_fail(ctx, KERR_MESH_INVALID, "more than 2^22 points in one cloud");
+    CK(cudaSetDevice(ctx->device));
+    size_t need = al256(sizeof(float) * 3 * (size_t)total_pts) + al256(sizeof(int) * (size_t)(n_hulls + 1))
+                + al256(sizeof(float) * 3 * (size_t)n_hulls * max_hv) + al256(sizeof(int) * 3 * (size_t)n_hulls * max_ht)
+                + 4 * al256(sizeof(int) * (size_t)n_hulls)
+                + al256(hull_scratch_bytes(max_pts)) * (size_t)n_hulls + 4096;
+    int rc = pool_begin(ctx, need);
+    if (rc) return rc;
+    float* d_pts = pool_take<float>(ctx, 3 * (size_t)total_pts);
+    int* d_off = pool_take<int>(ctx, n_hulls + 1);
+    float* d_v = pool_take<float>(ctx, 3 * (size_t)n_hulls * max_hv);
+    int* d_t = pool_take<int>(ctx, 3 * (size_t)n_hulls * max_ht);
+    int* d_nv = pool_take<int>(ctx, n_hulls);
+    int* d_nt = pool_take<int>(ctx, n_hulls);
+    float* d_vol = pool_take<float>(ctx, n_hulls);
+    int* d_err = pool_take<int>(ctx, n_hulls);
+    cudaStream_t s = ctx->stream;
+    if (total_pts > 0) CK(cudaMemcpyAsync(d_pts, pts, sizeof(float) * 3 * (size_t)total_pts, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(d_off, offsets, sizeof(int) * (size_t)(n_hulls + 1), cudaMemcpyHostToDevice, s));
+    rc = launch_hull_batch(ctx, d_pts, d_off, n_hulls, max_pts, max_hv, max_ht, d_v, d_t, d_nv, d_nt, d_vol, d_err, s);
+    if (rc) return rc;
+    if (out_verts) CK(cudaMemcpyAsync(out_verts, d_v, sizeof(float) * 3 * (size_t)n_hulls * max_hv, cudaMemcpyDeviceToHost, s));
+    if (out_tris) CK(cudaMemcpyAsync(out_tris, d_t, sizeof(int) * 3 * (size_t)n_hulls * max_ht, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(out_nv, d_nv, sizeof(int) * n_hulls, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(out_nt, d_nt, sizeof(int) * n_hulls, cudaMemcpyDeviceToHost, s));
+    if (out_vol) CK(cudaMemcpyAsync(out_vol, d_vol, sizeof(float) * n_hulls, cudaMemcpyDeviceToHost, s));
+    if (out_err) CK(cudaMemcpyAsync(out_err, d_err, sizeof(int) * n_hulls, cudaMemcpyDeviceToHost, s));
+    return sync_and_check(ctx, "hull");
+}
+
+extern "C" int gpu_hull_dandc(gpu_ctx_t ctx, const float* pts, int total_pts, const int* offsets, int n_hulls,
+                              int max_pts_per_hull, int max_hull_verts, int max_hull_tris,
+                              float* out_verts, int* out_tris, int* out_nv, int* out_nt, int* out_errors)
+{
+    return hull_common(ctx, pts, total_pts, offsets, n_hulls, max_pts_per_hull, max_hull_verts, max_hull_tris,
+                       out_verts, out_tris, out_nv, out_nt, nullptr, out_errors);
+}
+
+extern "C" int gpu_kdop_hull(gpu_ctx_t ctx, const float* pts, int total_pts, const int* offsets, int n_hulls,
+                             int max_hull_verts, int max_hull_tris, float* out_verts, int* out_tris,
+                             int* out_nv, int* out_nt, float* out_volumes, int* out_errors)
+{
+    if (!ctx) return -1;
+    int max_pts = 0;
+    for (int i = 0; i < n_hulls; i++) max_pts = std::max(max_pts, offsets[i + 1] - offsets[i]);
+    return hull_common(ctx, pts, total_pts, offsets, n_hulls, max_pts, max_hull_verts, max_hull_tris,
+                       out_verts, out_tris, out_nv, out_nt, out_volumes, out_errors);
+}
+
+extern "C" int cuacd_hull_batch_device(gpu_ctx_t ctx, const float* d_pts, const int* d_offsets, int n_hulls,
+                                       int max_pts, int max_hv, int max_ht, float* d_v, int* d_t,
+                                       int* d_nv, int* d_nt, float* d_vol, int* d_err, void* stream)
+{
+    if (!ctx) return -1;
+    if (n_hulls <= 0) return 0;
+    if (max_pts >= (1 << 22)) return ctx_fail(ctx, KERR_MESH_INVALID, "more than 2^22 points in one cloud");
+    CK(cudaSetDevice(ctx->device));
+    int rc = pool_begin(ctx, al256(hull_scratch_bytes(max_pts)) * (size_t)n_hulls + 4096);
+    if (rc) return rc;
+    return launch_hull_batch(ctx, d_pts, d_offsets, n_hulls, max_pts, max_hv, max_ht, d_v, d_t, d_nv, d_nt,
+                             d_vol, d_err, stream ? (cudaStream_t)stream : ctx->stream);
+}
+
+// ---------------------------------------------------------------------------
+// volumes
+// ---------------------------------------------------------------------------
+extern "C" int gpu_batch_mesh_volume(gpu_ctx_t ctx, const float* verts, int total_verts, const int* tris,
+                                     int total_tris, const int* tri_offsets, const int* vert_offsets,
+                                     int n_meshes, float* out_volumes)
+{
+    if (!ctx) return -1;
+    if (n_meshes <= 0) return 0;
+    for (int m = 0; m < n_meshes; m++) {
+        if (tri_offsets[m + 1] < tri_offsets[m] || tri_offsets[m + 1] > total_tris)
+            return ctx_fail(ctx, KERR_MESH_INVALID, "mesh %d: bad tri offsets", m);
+        if (vert_offsets && (vert_offsets[m + 1] < vert_offsets[m] || vert_offsets[m + 1] > total_verts))
+            return ctx_fail(ctx, KERR_MESH_INVALID, "mesh %d: bad vert offsets", m);
+    }
+    // tiles never straddle meshes; empty meshes get no tile (volume 0)
+    std::vector<int> tile_mesh, tile_first, mesh_tile0(n_meshes + 1);
+    for (int m = 0; m < n_meshes; m++) {
+        mesh_tile0[m] = (int)tile_mesh.size();
+        bool has_verts = vert_offsets ? vert_offsets[m + 1] > vert_offsets[m] : total_verts > 0;
+        if (!has_verts) continue;
+        for (int t = tri_offsets[m]; t < tri_offsets[m + 1]; t += VOL_TILE) {
+            tile_mesh.push_back(m); tile_first.push_back(t);
+        }
+    }
+    mesh_tile0[n_meshes] = (int)tile_mesh.size();
+    int n_tiles = (int)tile_mesh.size();
+    CK(cudaSetDevice(ctx->device));
+    size_t need = al256(sizeof(float) * 3 * (size_t)total_verts) + al256(sizeof(int) * 3 * (size_t)total_tris)
+                + 2 * al256(sizeof(int) * (size_t)(n_meshes + 1)) + 2 * al256(sizeof(int) * (size_t)n_tiles)
+                + al256(sizeof(int) * (size_t)(n_meshes + 1)) + al256(sizeof(double) * (size_t)n_tiles)
+                + al256(sizeof(float) * (size_t)n_meshes) + 4096;
+    int rc = pool_begin(ctx, need);
+    if (rc) return rc;
+    float* d_v = pool_take<float>(ctx, 3 * (size_t)total_verts);
+    int* d_t = pool_take<int>(ctx, 3 * (size_t)total_tris);
+    int* d_to = pool_take<int>(ctx, n_meshes + 1);
+    int* d_vo = vert_offsets ? pool_take<int>(ctx, n_meshes + 1) : nullptr;
+    int* d_tm = pool_take<int>(ctx, n_tiles);
+    int* d_tf = pool_take<int>(ctx, n_tiles);
+    int* d_mt0 = pool_take<int>(ctx, n_meshes + 1);
+    double* d_part = pool_take<double>(ctx, n_tiles);
+    float* d_out = pool_take<float>(ctx, n_meshes);
+    cudaStream_t s = ctx->stream;
+    if (total_verts > 0) CK(cudaMemcpyAsync(d_v, verts, sizeof(float) * 3 * (size_t)total_verts, cudaMemcpyHostToDevice, s));
+    if (total_tris > 0) CK(cudaMemcpyAsync(d_t, tris, sizeof(int) * 3 * (size_t)total_tris, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(d_to, tri_offsets, sizeof(int) * (size_t)(n_meshes + 1), cudaMemcpyHostToDevice, s));
+    if (d_vo) CK(cudaMemcpyAsync(d_vo, vert_offsets, sizeof(int) * (size_t)(n_meshes + 1), cudaMemcpyHostToDevice, s));
+    if (n_tiles) {
+        CK(cudaMemcpyAsync(d_tm, tile_mesh.data(), sizeof(int) * n_tiles, cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(d_tf, tile_first.data(), sizeof(int) * n_tiles, cudaMemcpyHostToDevice, s));
+    }
+    CK(cudaMemcpyAsync(d_mt0, mesh_tile0.data(), sizeof(int) * (n_meshes + 1), cudaMemcpyHostToDevice, s));
+    if (n_tiles) {
+        k_volume_tiles<<<n_tiles, VOL_NT, 0, s>>>(d_v, d_t, d_to, d_vo, d_tm, d_tf, n_tiles, d_part);
+        ctx->launches++;
+    }
+    k_volume_reduce<<<(n_meshes + 127) / 128, 128, 0, s>>>(d_mt0, d_part, n_meshes, d_out);
+    ctx->launches++;
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(out_volumes, d_out, sizeof(float) * n_meshes, cudaMemcpyDeviceToHost, s));
+    return sync_and_check(ctx, "batch_mesh_volume");
+}
+
+extern "C" int gpu_test_mesh_volume(gpu_ctx_t ctx, const float* verts, int n_verts, const int* tris,
+                                    int n_tris, float* out_volume)
+{
+    int to[2] = {0, n_tris};
+    int vo[2] = {0, n_verts};
+    return gpu_batch_mesh_volume(ctx, verts, n_verts, tris, n_tris, to, vo, 1, out_volume);
+}
+
+// ---------------------------------------------------------------------------
+// entry points implemented in the remaining translation units
+// ---------------------------------------------------------------------------

@@ -1,0 +1,210 @@
+/*
+ * cuacd_b200.h — C ABI of libcuacd_b200.so, the B200 (sm_100a) engine for
+ * cuacd's lookahead candidate-evaluation path.
+ *
+ * The gpu_* / lookahead_decompose entry points keep the names, argument order,
+ * meaning and return conventions of the reference's host layer, so the
+ * reference's CPython module (csrc/module.c) can link against this library in
+ * place of csrc/heap.c, csrc/test.c and csrc/lookahead.c:
+ *   - every pointer is a HOST pointer; the call copies in, computes, copies
+ *     out and synchronises before returning;
+ *   - return 0 on success, otherwise a CUDA error code or a device error word
+ *     (KERR_* bit flags, layout of the reference's cuda/error_codes.cuh:14-53);
+ *     the message is available from gpu_last_error();
+ *   - per-item error words go to out_errors.
+ * The cuacd_* entry points are additions for callers that keep data on the
+ * device (device pointers + a CUDA stream) and for the candidate evaluator.
+ */
+#ifndef CUACD_B200_H
+#define CUACD_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct gpu_ctx* gpu_ctx_t;
+
+/* ---- context and pool (reference csrc/heap.h:19-50) ---------------------- */
+
+/* Replaces gpu_set_fatbin (csrc/heap.h:19).  The kernels are linked into this
+ * library, so the blob is ignored; kept so existing callers still link. */
+void gpu_set_fatbin(const void* data, size_t len);
+
+/* Replaces gpu_init (csrc/heap.h:26).  device_ordinal < 0 keeps the calling
+ * thread's current device.  pool_bytes = 0 lets the device pool grow on
+ * demand; > 0 fixes its capacity. */
+int  gpu_init(gpu_ctx_t* ctx, int device_ordinal, size_t pool_bytes);
+/* Replaces gpu_destroy (csrc/heap.h:27). */
+void gpu_destroy(gpu_ctx_t ctx);
+/* Replaces gpu_last_error (csrc/heap.h:29). */
+const char* gpu_last_error(gpu_ctx_t ctx);
+/* Replaces gpu_heap_compact (csrc/heap.h:34); a no-op, as in the reference
+ * (csrc/heap.c:274-277): the pool is an arena reset between calls. */
+int  gpu_heap_compact(gpu_ctx_t ctx);
+/* Replaces gpu_pool_usage (csrc/heap.h:40): high-water mark of pool bytes. */
+size_t gpu_pool_usage(gpu_ctx_t ctx);
+/* Replaces gpu_heap_stats (csrc/heap.h:45).  out = {output bytes live,
+ * output allocations, output releases, scratch bytes live, scratch
+ * allocations, scratch releases}. */
+int gpu_heap_stats(gpu_ctx_t ctx, unsigned long long out[6]);
+
+/* ---- batch kernels (reference csrc/test.h) ------------------------------- */
+
+/* Replaces gpu_hull_dandc (csrc/test.h:30-43): exact convex hull of each
+ * cloud.  Corners are the input floats in ascending input order; triangles
+ * index into them (per-hull relative), canonical order. */
+int gpu_hull_dandc(gpu_ctx_t ctx, const float* pts, int total_pts,
+                   const int* offsets, int n_hulls, int max_pts_per_hull,
+                   int max_hull_verts, int max_hull_tris,
+                   float* out_verts, int* out_tris, int* out_nv, int* out_nt,
+                   int* out_errors);
+
+/* Replaces gpu_test_mesh_volume (csrc/test.h:48-54). */
+int gpu_test_mesh_volume(gpu_ctx_t ctx, const float* verts, int n_verts,
+                         const int* tris, int n_tris, float* out_volume);
+
+/* Replaces gpu_batch_mesh_volume (csrc/test.h:64-73). vert_offsets may be
+ * NULL (all meshes index one shared vertex array). */
+int gpu_batch_mesh_volume(gpu_ctx_t ctx, const float* verts, int total_verts,
+                          const int* tris, int total_tris,
+                          const int* tri_offsets, const int* vert_offsets,
+                          int n_meshes, float* out_volumes);
+
+/* Replaces gpu_kdop_hull (csrc/test.h:78-91): the same exact hull (the
+ * reference's extreme-point prefilter is subsumed by the BVH search) plus
+ * its volume. */
+int gpu_kdop_hull(gpu_ctx_t ctx, const float* pts, int total_pts,
+                  const int* offsets, int n_hulls,
+                  int max_hull_verts, int max_hull_tris,
+                  float* out_verts, int* out_tris, int* out_nv, int* out_nt,
+                  float* out_volumes, int* out_errors);
+
+/* Replaces gpu_test_hausdorff (csrc/test.h:96-102): bidirectional sampled
+ * Hausdorff distance (2000 samples per unit area, at least 1000). */
+int gpu_test_hausdorff(gpu_ctx_t ctx,
+                       const float* hull_verts, int hull_nv,
+                       const int* hull_tris, int hull_nt,
+                       const float* mesh_verts, int mesh_nv,
+                       const int* mesh_tris, int mesh_nt,
+                       float* out_hausdorff);
+
+/* Replaces gpu_test_plane_cut (csrc/test.h:112-122): cut a closed mesh by
+ * pa*x+pb*y+pc_n*z+pd = 0 and cap both halves. */
+int gpu_test_plane_cut(gpu_ctx_t ctx,
+                       const float* vertices, int n_verts,
+                       const int* triangles, int n_tris,
+                       float pa, float pb, float pc_n, float pd,
+                       float* out_pos_verts, int out_pos_verts_cap,
+                       int* out_pos_tris, int out_pos_tris_cap,
+                       float* out_neg_verts, int out_neg_verts_cap,
+                       int* out_neg_tris, int out_neg_tris_cap,
+                       int* out_n_pv, int* out_n_pt,
+                       int* out_n_nv, int* out_n_nt);
+
+/* Replaces gpu_test_warp_sort (csrc/test.h:19-20): sort each sub-array of
+ * (x,y,z,index) int records by (y,x,z,index) in place. */
+int gpu_test_warp_sort(gpu_ctx_t ctx, int* points, int total_pts,
+                       const int* offsets, int n_arrays);
+
+/* ---- candidate evaluator (additions) ------------------------------------- */
+
+/* Per-candidate result of cut + volumes + hulls (+ Hausdorff). */
+typedef struct {
+    int   ok;              /* both halves non-empty */
+    int   nv[2], nt[2];    /* fragment sizes (pos, neg), caps included */
+    int   n_cap;           /* cap triangles */
+    int   hull_nv[2], hull_nt[2];
+    float mesh_vol[2], hull_vol[2], hausdorff[2];
+    float cost_rv[2], cost_full[2];
+    float score_rv, score_full;   /* worst part cost of the candidate */
+    int   err;             /* KERR_* bits raised for this candidate */
+} cuacd_cand_result;
+
+#define CUACD_EVAL_HAUSDORFF 1
+
+/* Evaluate n_planes candidate planes (4 floats each) on one closed mesh:
+ * cut with caps, volume of both halves, exact hull of both halves,
+ * optionally the sampled Hausdorff distance fragment<->hull, and the part
+ * costs of cuda/la_common.cuh:21-34.  Host pointers.  hd_resolution <= 0
+ * selects the reference defaults (2000 per unit area, min 1000 samples);
+ * hd_total > 0 fixes the per-surface sample budget instead. */
+int cuacd_eval_candidates(gpu_ctx_t ctx, const float* verts, int nv,
+                          const int* tris, int nt, const float* planes,
+                          int n_planes, int flags, float hd_resolution,
+                          int hd_min_samples, int hd_total,
+                          cuacd_cand_result* out);
+
+/* Same with device pointers on `stream` (cudaStream_t as void*); results
+ * stay on the device in d_out.  Does not synchronise. */
+int cuacd_eval_candidates_device(gpu_ctx_t ctx, const float* d_verts, int nv,
+                                 const int* d_tris, int nt,
+                                 const float* d_planes, int n_planes, int flags,
+                                 float hd_resolution, int hd_min_samples,
+                                 int hd_total, cuacd_cand_result* d_out,
+                                 void* stream);
+
+/* Hausdorff with an explicit sample budget (config of a fixed total), host
+ * pointers. */
+int cuacd_hausdorff(gpu_ctx_t ctx,
+                    const float* a_verts, int a_nv, const int* a_tris, int a_nt,
+                    const float* b_verts, int b_nv, const int* b_tris, int b_nt,
+                    float resolution, int min_samples, int total,
+                    float* out_hausdorff);
+
+/* Device-pointer batch hull for callers with resident data (used by the
+ * benchmark's device-resident leg).  Does not synchronise. */
+int cuacd_hull_batch_device(gpu_ctx_t ctx, const float* d_pts,
+                            const int* d_offsets, int n_hulls, int max_pts,
+                            int max_hull_verts, int max_hull_tris,
+                            float* d_out_verts, int* d_out_tris,
+                            int* d_out_nv, int* d_out_nt, float* d_out_vol,
+                            int* d_out_errors, void* stream);
+
+/* Number of kernel launches issued by this context so far (a counter the
+ * benchmark reads around its timed region). */
+unsigned long long cuacd_launch_count(gpu_ctx_t ctx);
+
+/* ---- lookahead search (reference csrc/lookahead.h, csrc/heap.h) ---------- */
+
+struct gpu_part_result {
+    float* verts;       /* malloc'd, nv*3 floats */
+    int*   tris;        /* malloc'd, nt*3 ints */
+    int    nv;
+    int    nt;
+    float* hull_verts;  /* malloc'd, hull_nv*3 floats */
+    int*   hull_tris;   /* malloc'd, hull_nt*3 ints */
+    int    hull_nv;
+    int    hull_nt;
+    float  mesh_vol;
+    float  hull_vol;
+    float  hausdorff;
+};
+
+struct gpu_result {
+    struct gpu_part_result* parts;
+    int nparts;
+};
+
+/* Replaces gpu_result_free (csrc/heap.h:85). */
+void gpu_result_free(struct gpu_result* result);
+
+/* Replaces lookahead_decompose (csrc/lookahead.h:28-43). */
+int lookahead_decompose(gpu_ctx_t ctx,
+                        const float* verts, int nv, const int* tris, int nt,
+                        const float* hull_verts, int hull_nv,
+                        const int* hull_tris, int hull_nt,
+                        int max_iters, int width, int width2, float threshold,
+                        int depth, int quick_depth, int max_n_cutting,
+                        int verbose, int debug, int decompose_components,
+                        int decompose_components_per_iter,
+                        int n_concave_edges, float concave_eps,
+                        float concave_threshold, int concave_iters,
+                        int merge_hulls, struct gpu_result* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

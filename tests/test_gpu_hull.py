@@ -1,0 +1,80 @@
+"""GPU hull parity against the oracle (bit-exact corner sets and triangles,
+volume within 1e-5 relative)."""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, is_watertight
+from cuacd_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+VOL_RTOL = 1e-5
+
+
+def _gpu_hulls(ctx, clouds):
+    return ctx.batch_hull_dandc_mesh(clouds)
+
+
+def _check_exact(oracle, clouds, gpu):
+    for c, (hv, ht, vol) in zip(clouds, gpu):
+        vidx, tris, ovol = oracle.hull(c)
+        np.testing.assert_array_equal(hv, c[vidx])
+        np.testing.assert_array_equal(ht, tris)
+        if ovol > 0:
+            assert abs(vol - ovol) / ovol < VOL_RTOL
+
+
+def test_config1_clouds_exact(ctx, oracle):
+    clouds = W.hull_clouds(256, 1000, 0)
+    _check_exact(oracle, clouds, _gpu_hulls(ctx, clouds))
+
+
+def test_golden_clouds_exact(ctx, oracle):
+    g = np.load(os.path.join(GOLDEN, "hull_qhull.npz"))
+    clouds = [g[f"pts_{i}"] for i in range(int(g["n"]))]
+    gpu = _gpu_hulls(ctx, clouds)
+    _check_exact(oracle, clouds, gpu)
+    for i, (hv, ht, vol) in enumerate(gpu):
+        idx = np.array([np.flatnonzero((clouds[i] == p).all(1))[0] for p in hv])
+        assert np.array_equal(np.sort(idx), g[f"qhull_vertices_{i}"])
+
+
+def test_known_answers(ctx):
+    cube = np.array([[x, y, z] for x in (0, 1) for y in (0, 1) for z in (0, 1)], np.float32)
+    tet = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [0, 0, 1]], np.float32)
+    (cv, ct, cvol), (tv, tt, tvol) = ctx.batch_hull_dandc_mesh([cube, tet])
+    assert (len(cv), len(ct)) == (8, 12) and abs(cvol - 1) < 1e-6 and is_watertight(ct)
+    assert (len(tv), len(tt)) == (4, 4) and abs(tvol - 1 / 6) < 1e-6
+    vols, errs = ctx.batch_hull_volume([cube, tet])
+    assert np.all(errs == 0) and abs(vols[0] - 1) < 1e-6
+
+
+def test_degenerate_and_uneven(ctx, oracle):
+    rng = np.random.default_rng(7)
+    cube = np.array([[x, y, z] for x in (0, 1) for y in (0, 1) for z in (0, 1)], np.float32)
+    clouds = [
+        np.zeros((3, 3), np.float32),                                     # n < 4
+        np.concatenate([cube, rng.uniform(0.1, 0.9, (200, 3))]).astype(np.float32),
+        np.concatenate([cube, cube, cube]).astype(np.float32),           # duplicates
+        rng.uniform(-1, 1, (5, 3)).astype(np.float32),
+        rng.standard_normal((3000, 3)).astype(np.float32),
+        np.c_[rng.uniform(0, 1, (100, 2)), np.zeros(100)].astype(np.float32),  # flat
+    ]
+    gpu = _gpu_hulls(ctx, clouds)
+    assert len(gpu[0][0]) == 0
+    _check_exact(oracle, clouds[1:5], gpu[1:5])
+    assert abs(gpu[5][2]) < 1e-6
+
+
+def test_large_fragment_like(ctx, oracle):
+    v, _ = W.candidate_mesh()
+    (hv, ht, vol), = _gpu_hulls(ctx, [v])
+    _check_exact(oracle, [v], [(hv, ht, vol)])
+    assert is_watertight(ht)
+
+
+def test_kdop_caps(ctx):
+    v, _ = W.candidate_mesh(64, 20)
+    (hv, ht, vol), = ctx.batch_kdop_hull_mesh([v])
+    assert 0 < len(hv) <= 4096 and len(ht) == 2 * len(hv) - 4
