@@ -26,13 +26,17 @@ def sources():
     return sorted(f for f in os.listdir(CSRC) if f.endswith(".cu"))
 
 
+# Per-file flags: the cut's FP32/FP64 expressions must not be contracted.
+PER_FILE = {"cut.cu": ["-fmad=false"]}
+
+
 def _compile(src, extra):
     obj = os.path.join(BUILD, src[:-3] + ".o")
     deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC)] + [
         os.path.join(HERE, "..", "include", "cuacd_b200.h")]
     if os.path.exists(obj) and os.path.getmtime(obj) >= max(os.path.getmtime(d) for d in deps):
         return obj, ""
-    cmd = [NVCC, *ARCH, *FLAGS, *extra, "-c", os.path.join(CSRC, src), "-o", obj]
+    cmd = [NVCC, *ARCH, *FLAGS, *PER_FILE.get(src, []), *extra, "-c", os.path.join(CSRC, src), "-o", obj]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"nvcc failed for {src}:\n{r.stdout}\n{r.stderr}")

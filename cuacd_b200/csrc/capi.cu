@@ -6,6 +6,7 @@
 #include "context.cuh"
 #include "volume.cuh"
 #include "hull.cuh"
+#include "launch.h"
 
 // ---------------------------------------------------------------------------
 // kernels
@@ -39,6 +40,11 @@ k_hull_batch(const float* __restrict__ pts, const int* __restrict__ offsets, int
              &out_nv[h], &out_nt[h], out_vol ? &out_vol[h] : nullptr, &s_err, sh);
     __syncthreads();
     if (threadIdx.x == 0 && out_err) out_err[h] = s_err;
+}
+
+void launch_arena_reset(Arena* a, char* base, unsigned long long cap, cudaStream_t s)
+{
+    k_arena_reset<<<1, 32, 0, s>>>(a, base, cap);
 }
 
 // ---------------------------------------------------------------------------
@@ -113,15 +119,6 @@ extern "C" int gpu_heap_stats(gpu_ctx_t ctx, unsigned long long out[6])
     return 0;
 }
 extern "C" unsigned long long cuacd_launch_count(gpu_ctx_t ctx) { return ctx ? ctx->launches : 0; }
-
-static int sync_and_check(gpu_ctx* ctx, const char* what)
-{
-    cudaError_t e = cudaStreamSynchronize(ctx->stream);
-    if (e != cudaSuccess) return ctx_fail(ctx, (int)e, "%s: %s", what, cudaGetErrorString(e));
-    e = cudaGetLastError();
-    if (e != cudaSuccess) return ctx_fail(ctx, (int)e, "%s: %s", what, cudaGetErrorString(e));
-    return 0;
-}
 
 // ---------------------------------------------------------------------------
 // hulls

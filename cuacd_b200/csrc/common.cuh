@@ -50,7 +50,7 @@ struct Arena {
 
 // Allocate `bytes` (rounded to 256) from the arena; nullptr + KERR_HEAP_OOM when
 // exhausted.  Call from one thread.
-__device__ __forceinline__ void* arena_alloc(Arena* a, unsigned long long bytes, int* err)
+static __device__ __forceinline__ void* arena_alloc(Arena* a, unsigned long long bytes, int* err)
 {
     bytes = (bytes + 255ull) & ~255ull;
     unsigned long long off = atomicAdd(&a->offset, bytes);
@@ -66,22 +66,22 @@ __device__ __forceinline__ void* arena_alloc(Arena* a, unsigned long long bytes,
 // ---------------------------------------------------------------------------
 // warp / block helpers
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ float warp_min(float v) {
+static __device__ __forceinline__ float warp_min(float v) {
     #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v = fminf(v, __shfl_xor_sync(FULL_MASK, v, o));
     return v;
 }
-__device__ __forceinline__ float warp_max(float v) {
+static __device__ __forceinline__ float warp_max(float v) {
     #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(FULL_MASK, v, o));
     return v;
 }
-__device__ __forceinline__ double warp_sum_d(double v) {
+static __device__ __forceinline__ double warp_sum_d(double v) {
     #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL_MASK, v, o);
     return v;
 }
-__device__ __forceinline__ int warp_sum_i(int v) {
+static __device__ __forceinline__ int warp_sum_i(int v) {
     #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL_MASK, v, o);
     return v;
@@ -89,7 +89,7 @@ __device__ __forceinline__ int warp_sum_i(int v) {
 
 // Block-wide exclusive scan of one int per thread; returns the exclusive
 // prefix, writes the block total to *total.  `sh` needs blockDim/32 + 1 ints.
-__device__ __forceinline__ int block_exclusive_scan(int v, int* sh, int* total)
+static __device__ __forceinline__ int block_exclusive_scan(int v, int* sh, int* total)
 {
     int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
     int x = v;
@@ -117,7 +117,7 @@ __device__ __forceinline__ int block_exclusive_scan(int v, int* sh, int* total)
     return excl;
 }
 
-__device__ __forceinline__ double block_sum_d(double v, double* sh)
+static __device__ __forceinline__ double block_sum_d(double v, double* sh)
 {
     int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
     v = warp_sum_d(v);
@@ -136,7 +136,7 @@ __device__ __forceinline__ double block_sum_d(double v, double* sh)
 }
 
 // float atomic max for non-negative values (bit patterns order like ints)
-__device__ __forceinline__ void atomic_max_nonneg(float* addr, float v) {
+static __device__ __forceinline__ void atomic_max_nonneg(float* addr, float v) {
     atomicMax(reinterpret_cast<int*>(addr), __float_as_int(v));
 }
 
@@ -144,7 +144,7 @@ __device__ __forceinline__ void atomic_max_nonneg(float* addr, float v) {
 // mesh volume (divergence theorem), FP64 accumulation
 // cuda/mesh_volume.cuh:20-57: signed-tet sum anchored at vertex 0.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ double tet6_d(const float* __restrict__ v, int a, int b, int c,
+static __device__ __forceinline__ double tet6_d(const float* __restrict__ v, int a, int b, int c,
                                          double ox, double oy, double oz)
 {
     double ax = (double)v[3*a] - ox, ay = (double)v[3*a+1] - oy, az = (double)v[3*a+2] - oz;
@@ -155,7 +155,7 @@ __device__ __forceinline__ double tet6_d(const float* __restrict__ v, int a, int
 }
 
 // Block-cooperative signed volume of one mesh (all threads call).
-__device__ __forceinline__ double block_mesh_signed_volume(const float* __restrict__ v, int nv,
+static __device__ __forceinline__ double block_mesh_signed_volume(const float* __restrict__ v, int nv,
                                                            const int* __restrict__ t, int nt,
                                                            double* sh)
 {
@@ -170,7 +170,7 @@ __device__ __forceinline__ double block_mesh_signed_volume(const float* __restri
 // ---------------------------------------------------------------------------
 // part costs: cuda/la_common.cuh:21-34
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ float part_cost_rv(double hull_vol, double mesh_vol) {
+static __device__ __forceinline__ float part_cost_rv(double hull_vol, double mesh_vol) {
     const double pi = 3.14159265358979;
     double g = hull_vol - mesh_vol; if (g < 0.0) g = 0.0;
     return (float)(0.3 * cbrt((3.0 / (4.0 * pi)) * g));

@@ -88,3 +88,12 @@ static int arena_reset(gpu_ctx* ctx)
     ctx->stats[5]++;
     return 0;
 }
+
+static int sync_and_check(gpu_ctx* ctx, const char* what)
+{
+    cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) return ctx_fail(ctx, (int)e, "%s: %s", what, cudaGetErrorString(e));
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return ctx_fail(ctx, (int)e, "%s: %s", what, cudaGetErrorString(e));
+    return 0;
+}

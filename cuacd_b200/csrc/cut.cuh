@@ -1,0 +1,786 @@
+// cut.cuh — mesh/plane cut with cap triangulation, one CTA per cut (sm_100a).
+//
+// Replaces plane_cut_block (cuda/plane_cut.cuh:167-1562; 64 threads, ~15
+// locked heap allocations, thread-0 serial phases).  Here:
+//   classify (:270-275)         one pass over the vertices, all threads
+//   crossing edges (:277-303)   per-triangle ballot compaction, CTA bitonic
+//                               sort + dedup of 64-bit edge keys
+//   new vertices (:536-569)     exclusive scan over the unique edges; an edge
+//                               with one on-plane end reuses that vertex
+//   split (:582-652)            per-triangle piece counts, exclusive scan,
+//                               pieces written in input-triangle order
+//   boundary (:661-811)         unmatched edges of the positive side among
+//                               edges whose ends both lie on the cut, found
+//                               by sorting (min,max,dir) keys
+//   caps (:893-1294)            loops (smallest unused edge first), FP64
+//                               orientation, even/odd nesting, hole bridging
+//                               and ear clipping with a warp-parallel
+//                               point-in-triangle scan
+//   failure (:1341-1368)        the mesh is returned unsplit on the + side
+//   output (:1394-1550)         per-side vertex compaction in index order,
+//                               cap winding rule
+// Every scratch buffer is bump-allocated from the arena once its size is
+// known; nothing waits on a lock.  This translation unit is compiled with
+// -fmad=false: the FP32 and FP64 expressions round exactly as written (the
+// checker evaluates the same sequence), and every fused multiply-add that is
+// wanted is spelled fmaf().
+#pragma once
+#include "common.cuh"
+#include "cta_util.cuh"
+
+#define CUT_NT  256
+#define CUT_EPS 1e-6f
+
+struct CutResult {
+    float* pv; int* pt; int npv, npt;      // positive side (caps included)
+    float* nv; int* nt; int nnv, nnt;      // negative side
+    int n_pos_tris, n_neg_tris;            // before caps
+    int n_cap, n_loops, n_boundary, cap_failed, n_cross;
+    int err;
+    int _pad[2];
+};
+
+struct CutFixedOut {          // caller-sized outputs; null -> allocate in the arena
+    float* pv; int pv_cap; int* pt; int pt_cap;
+    float* nv; int nv_cap; int* nt; int nt_cap;
+};
+
+static __device__ __forceinline__ float cut_plane_eval(float pa, float pb, float pc, float pd, const float* v)
+{
+    return fmaf(pa, v[0], fmaf(pb, v[1], fmaf(pc, v[2], pd)));
+}
+
+struct CutShared {
+    int scan[34];
+    int cnt[8];
+    int ok;
+    void* ptr[16];
+    int ival[16];
+};
+
+// ---- FP64 cap helpers (same operation order as the checker) --------------
+struct Cap2D { const float* V; int pu, pv; };
+static __device__ __forceinline__ double cU(const Cap2D& c, int v) { return (double)c.V[3 * v + c.pu]; }
+static __device__ __forceinline__ double cW(const Cap2D& c, int v) { return (double)c.V[3 * v + c.pv]; }
+
+static __device__ double cut_signed_area(const Cap2D& c, const int* poly, int n)
+{
+    double a = 0.0;
+    for (int i = 0; i < n; i++) {
+        int j = (i + 1) % n;
+        a += cU(c, poly[i]) * cW(c, poly[j]) - cU(c, poly[j]) * cW(c, poly[i]);
+    }
+    return a * 0.5;
+}
+static __device__ void cut_reverse(int* a, int n) {
+    for (int i = 0; i < n / 2; i++) { int t = a[i]; a[i] = a[n - 1 - i]; a[n - 1 - i] = t; }
+}
+static __device__ __forceinline__ double cut_cross2(double ax, double ay, double bx, double by, double cx, double cy) {
+    return (bx - ax) * (cy - ay) - (by - ay) * (cx - ax);
+}
+static __device__ __forceinline__ int cut_pt_in_tri(double px, double py, double ax, double ay, double bx, double by,
+                                             double cx, double cy)
+{
+    double d1 = cut_cross2(ax, ay, bx, by, px, py);
+    double d2 = cut_cross2(bx, by, cx, cy, px, py);
+    double d3 = cut_cross2(cx, cy, ax, ay, px, py);
+    int neg = (d1 < -1e-10) || (d2 < -1e-10) || (d3 < -1e-10);
+    int pos = (d1 > 1e-10) || (d2 > 1e-10) || (d3 > 1e-10);
+    return !(neg && pos);
+}
+
+// Ear clipping of one polygon by warp 0 (lane 0 drives; lanes scan).
+// Returns triangles appended to cap (lane 0's count).
+static __device__ int cut_ear_clip(const Cap2D& c, const int* poly, int n, int* prv, int* nxt, int* cap, int lane)
+{
+    int nc = 0;
+    for (int i = lane; i < n; i += 32) { prv[i] = (i + n - 1) % n; nxt[i] = (i + 1) % n; }
+    __syncwarp();
+    int remaining = n, cur = 0, iter = 0;
+    while (remaining > 3 && iter < remaining) {
+        iter++;
+        int p = prv[cur], q = nxt[cur];
+        int vp = poly[p], vc = poly[cur], vn = poly[q];
+        double up = cU(c, vp), wp = cW(c, vp), uc = cU(c, vc), wc = cW(c, vc), un = cU(c, vn), wn = cW(c, vn);
+        double cr = (uc - up) * (wn - wp) - (wc - wp) * (un - up);
+        if (cr < -1e-9) { cur = q; continue; }
+        bool clip;
+        if (cr <= 1e-9) clip = true;
+        else {
+            int inside = 0;
+            for (int idx = lane; idx < n; idx += 32) {
+                if (idx == p || idx == cur || idx == q) continue;
+                if (nxt[prv[idx]] != idx) continue;
+                int vi = poly[idx];
+                double cu = cU(c, vi), cw = cW(c, vi);
+                if (fabs(cu - up) + fabs(cw - wp) > 1e-6 &&
+                    fabs(cu - uc) + fabs(cw - wc) > 1e-6 &&
+                    fabs(cu - un) + fabs(cw - wn) > 1e-6 &&
+                    cut_pt_in_tri(cu, cw, up, wp, uc, wc, un, wn)) inside = 1;
+            }
+            clip = __ballot_sync(FULL_MASK, inside) == 0;
+        }
+        if (clip) {
+            if (lane == 0) {
+                cap[3 * nc] = vp; cap[3 * nc + 1] = vc; cap[3 * nc + 2] = vn;
+                nxt[p] = q; prv[q] = p;
+            }
+            nc++;
+            __syncwarp();
+            remaining--; cur = q; iter = 0;
+        } else cur = q;
+    }
+    if (remaining == 3) {
+        int p = prv[cur], q = nxt[cur];
+        if (lane == 0) { cap[3 * nc] = poly[p]; cap[3 * nc + 1] = poly[cur]; cap[3 * nc + 2] = poly[q]; }
+        nc++;
+    }
+    __syncwarp();
+    return nc;
+}
+
+// Caps from the directed boundary edges be[] (sorted by (a,b), packed a<<32|b).
+// Warp 0 only.  Returns n_cap >= 0 or -1 on failure.
+static __device__ int cut_build_caps(const float* V, int n_all, const unsigned long long* be, int nb,
+                              float pa, float pb, float pc, int* used, int* lv, int* ls, int* lsz,
+                              int* poly, int* tmp, int poly_cap, int* cap_out, int* n_loops_out, int lane)
+{
+    Cap2D C; C.V = V;
+    {
+        float ax = fabsf(pa), ay = fabsf(pb), az = fabsf(pc);
+        if (ax >= ay && ax >= az) { C.pu = 1; C.pv = 2; }
+        else if (ay >= az)        { C.pu = 0; C.pv = 2; }
+        else                      { C.pu = 0; C.pv = 1; }
+    }
+    int n_loops = 0, fail = 0;
+    if (lane == 0) {
+        int lvi = 0;
+        for (int i = 0; i < nb; i++) used[i] = 0;
+        for (int st = 0; st < nb && !fail; st++) {
+            if (used[st]) continue;
+            int first = (int)(be[st] >> 32), cur = (int)(be[st] & 0xffffffffu);
+            if (first < 0 || first >= n_all || cur < 0 || cur >= n_all) { fail = 1; break; }
+            used[st] = 1;
+            int start = lvi;
+            lv[lvi++] = first;
+            int guard = nb + 2;
+            while (cur != first && guard-- > 0) {
+                if (lvi >= nb) { fail = 1; break; }
+                lv[lvi++] = cur;
+                int lo = lower_bound_u64(be, nb, (unsigned long long)(unsigned)cur << 32);
+                int found = -1;
+                for (int k = lo; k < nb && (int)(be[k] >> 32) == cur; k++) if (!used[k]) { found = k; break; }
+                if (found < 0) { fail = 1; break; }
+                used[found] = 1;
+                cur = (int)(be[found] & 0xffffffffu);
+            }
+            if (fail || cur != first) { fail = 1; break; }
+            ls[n_loops] = start; lsz[n_loops] = lvi - start; n_loops++;
+        }
+        if (n_loops > 128) fail = 1;
+    }
+    n_loops = __shfl_sync(FULL_MASK, n_loops, 0);
+    fail = __shfl_sync(FULL_MASK, fail, 0);
+    *n_loops_out = n_loops;
+    if (fail) return -1;
+    __shared__ int parent[128], is_hole[128], hidx[128];
+    __shared__ double hmax[128];
+    int n_cap = 0;
+    if (lane == 0) {
+        for (int i = 0; i < n_loops; i++)
+            if (cut_signed_area(C, lv + ls[i], lsz[i]) < 0) cut_reverse(lv + ls[i], lsz[i]);
+        for (int i = 0; i < n_loops; i++) { parent[i] = -1; is_hole[i] = 0; }
+        for (int i = 0; i < n_loops; i++) {
+            if (lsz[i] < 3) continue;
+            int vi = lv[ls[i]];
+            double pu_ = cU(C, vi), pv_ = cW(C, vi);
+            double best_area = 1e300;
+            for (int j = 0; j < n_loops; j++) {
+                if (j == i || lsz[j] < 3) continue;
+                const int* lp = lv + ls[j];
+                int m = lsz[j], crossings = 0;
+                for (int k = 0; k < m; k++) {
+                    int kn = (k + 1) % m;
+                    double ay = cW(C, lp[k]), by = cW(C, lp[kn]);
+                    if ((ay <= pv_) == (by <= pv_)) continue;
+                    double ax = cU(C, lp[k]), bx = cU(C, lp[kn]);
+                    double t = (pv_ - ay) / (by - ay);
+                    if (ax + t * (bx - ax) > pu_) crossings++;
+                }
+                if (crossings & 1) {
+                    double a = fabs(cut_signed_area(C, lp, m));
+                    if (a < best_area) { best_area = a; parent[i] = j; }
+                }
+            }
+        }
+        for (int i = 0; i < n_loops && !fail; i++) {
+            int steps = 0;
+            for (int p = parent[i]; p >= 0; p = parent[p]) if (++steps > n_loops) { fail = 1; break; }
+        }
+        if (!fail) {
+            for (int i = 0; i < n_loops; i++) {
+                int depth = 0;
+                for (int p = parent[i]; p >= 0; p = parent[p]) depth++;
+                is_hole[i] = depth & 1;
+                if (!is_hole[i] && depth >= 2) parent[i] = -1;
+            }
+            for (int i = 0; i < n_loops; i++) if (is_hole[i]) cut_reverse(lv + ls[i], lsz[i]);
+        }
+    }
+    fail = __shfl_sync(FULL_MASK, fail, 0);
+    __syncwarp();
+    if (fail) return -1;
+    int expected = 0;
+    for (int oi = 0; oi < n_loops; oi++) {
+        if (is_hole[oi] || lsz[oi] < 3) continue;
+        int pn = 0;
+        if (lane == 0) {
+            pn = lsz[oi];
+            for (int i = 0; i < pn; i++) poly[i] = lv[ls[oi] + i];
+            int nin = 0;
+            for (int i = 0; i < n_loops && nin < 128; i++) {
+                if (parent[i] != oi || lsz[i] < 3) continue;
+                double mu = -1e300;
+                for (int j = 0; j < lsz[i]; j++) { double u = cU(C, lv[ls[i] + j]); if (u > mu) mu = u; }
+                hidx[nin] = i; hmax[nin] = mu; nin++;
+            }
+            for (int i = 0; i < nin - 1; i++) {
+                int best = i;
+                for (int j = i + 1; j < nin; j++) if (hmax[j] > hmax[best]) best = j;
+                if (best != i) {
+                    int ti = hidx[i]; hidx[i] = hidx[best]; hidx[best] = ti;
+                    double tf = hmax[i]; hmax[i] = hmax[best]; hmax[best] = tf;
+                }
+            }
+            for (int ii = 0; ii < nin && !fail; ii++) {
+                int hi = hidx[ii], hs = lsz[hi];
+                const int* hole = lv + ls[hi];
+                int m_idx = 0; double max_u = -1e300;
+                for (int j = 0; j < hs; j++) { double u = cU(C, hole[j]); if (u > max_u) { max_u = u; m_idx = j; } }
+                double mu_ = cU(C, hole[m_idx]), mv_ = cW(C, hole[m_idx]);
+                double best_t = 1e300; int best_edge = -1;
+                for (int j = 0; j < pn; j++) {
+                    int jn = (j + 1) % pn;
+                    double au = cU(C, poly[j]), av = cW(C, poly[j]);
+                    double bu = cU(C, poly[jn]), bv = cW(C, poly[jn]);
+                    double dv = bv - av; if (fabs(dv) < 1e-12) continue;
+                    double s_ = (mv_ - av) / dv;
+                    if (s_ < -1e-12 || s_ > 1.0 + 1e-12) continue;
+                    double tv = au + s_ * (bu - au) - mu_;
+                    if (tv > 1e-12 && tv < best_t) { best_t = tv; best_edge = j; }
+                }
+                if (best_edge < 0) { fail = 1; break; }
+                int jn = (best_edge + 1) % pn;
+                int p_pos = (cU(C, poly[best_edge]) >= cU(C, poly[jn])) ? best_edge : jn;
+                if (pn + hs + 2 > poly_cap) { fail = 1; break; }
+                int k = 0;
+                for (int j = 0; j <= p_pos; j++) tmp[k++] = poly[j];
+                for (int j = 0; j < hs; j++) tmp[k++] = hole[(m_idx + j) % hs];
+                tmp[k++] = hole[m_idx]; tmp[k++] = poly[p_pos];
+                for (int j = p_pos + 1; j < pn; j++) tmp[k++] = poly[j];
+                for (int j = 0; j < k; j++) poly[j] = tmp[j];
+                pn = k;
+            }
+        }
+        fail = __shfl_sync(FULL_MASK, fail, 0);
+        pn = __shfl_sync(FULL_MASK, pn, 0);
+        __syncwarp();
+        if (fail) return -1;
+        expected += pn - 2;
+        if (pn >= 3) n_cap += cut_ear_clip(C, poly, pn, tmp, tmp + poly_cap, cap_out + 3 * n_cap, lane);
+    }
+    if (n_cap < expected) return -1;
+    return n_cap;
+}
+
+// ---------------------------------------------------------------------------
+// the CTA cut.  All CUT_NT threads call.  Scratch and (if fixed.pv == null)
+// outputs come from the arena.  Writes *res.
+// ---------------------------------------------------------------------------
+static __device__ void cut_cta(const float* __restrict__ verts, int nv, const int* __restrict__ tris, int nt,
+                        float pa, float pb, float pc, float pd, Arena* arena, CutFixedOut fixed,
+                        CutResult* res, CutShared& sh)
+{
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    __shared__ int s_err;
+    if (tid == 0) s_err = 0;
+    __syncthreads();
+#define CUT_ALLOC(slot, T, count) do { if (tid == 0) { \
+        sh.ptr[slot] = s_err ? nullptr : arena_alloc(arena, sizeof(T) * (unsigned long long)((count) > 0 ? (count) : 1), &s_err); \
+        if (!sh.ptr[slot]) s_err |= KERR_PC_SCRATCH_OOM; } } while (0)
+    // ---- classify
+    CUT_ALLOC(0, signed char, nv);
+    __syncthreads();
+    if (s_err) goto fail_out;
+    {
+        signed char* sg = (signed char*)sh.ptr[0];
+        for (int v = tid; v < nv; v += CUT_NT) {
+            float d = cut_plane_eval(pa, pb, pc, pd, verts + 3 * v);
+            sg[v] = (d > CUT_EPS) ? 1 : ((d < -CUT_EPS) ? -1 : 0);
+        }
+        if (tid < 8) sh.cnt[tid] = 0;
+        __syncthreads();
+        // count crossing occurrences, and sides present
+        int occ = 0, anyp = 0, anyn = 0;
+        for (int t = tid; t < nt; t += CUT_NT) {
+            int s0 = sg[tris[3 * t]], s1 = sg[tris[3 * t + 1]], s2 = sg[tris[3 * t + 2]];
+            int e0 = s0 >= 0, e1 = s1 >= 0, e2 = s2 >= 0;
+            occ += (e0 != e1) + (e1 != e2) + (e2 != e0);
+        }
+        for (int v = tid; v < nv; v += CUT_NT) { anyp |= sg[v] > 0; anyn |= sg[v] < 0; }
+        occ = warp_sum_i(occ);
+        if (lane == 0) atomicAdd(&sh.cnt[0], occ);
+        if (anyp) sh.cnt[1] = 1;
+        if (anyn) sh.cnt[2] = 1;
+        __syncthreads();
+    }
+    {
+    const signed char* sg = (const signed char*)sh.ptr[0];
+    const int n_occ = sh.cnt[0];
+    const int any_pos = sh.cnt[1], any_neg = sh.cnt[2];
+    if (n_occ == 0) {
+        // ---------------- no crossing edge: whole mesh or side split
+        if (!any_pos || !any_neg) {
+            int to_neg = any_neg && !any_pos;
+            // copy whole mesh to one side
+            if (tid == 0) {
+                float* ov = to_neg ? fixed.nv : fixed.pv; int* ot = to_neg ? fixed.nt : fixed.pt;
+                int vc = to_neg ? fixed.nv_cap : fixed.pv_cap, tc = to_neg ? fixed.nt_cap : fixed.pt_cap;
+                if (!fixed.pv) {
+                    ov = (float*)arena_alloc(arena, sizeof(float) * 3ull * (nv > 0 ? nv : 1), &s_err);
+                    ot = (int*)arena_alloc(arena, sizeof(int) * 3ull * (nt > 0 ? nt : 1), &s_err);
+                    vc = nv; tc = nt;
+                }
+                if (!ov || !ot || nv > vc || nt > tc) s_err |= KERR_PC_POOL_OOM;
+                sh.ptr[1] = ov; sh.ptr[2] = ot; sh.ival[0] = to_neg;
+            }
+            __syncthreads();
+            if (s_err) goto fail_out;
+            float* ov = (float*)sh.ptr[1]; int* ot = (int*)sh.ptr[2];
+            for (int i = tid; i < 3 * nv; i += CUT_NT) ov[i] = verts[i];
+            for (int i = tid; i < 3 * nt; i += CUT_NT) ot[i] = tris[i];
+            if (tid == 0) {
+                memset(res, 0, sizeof(CutResult));
+                if (sh.ival[0]) { res->nv = ov; res->nt = ot; res->nnv = nv; res->nnt = nt; res->n_neg_tris = nt; }
+                else            { res->pv = ov; res->pt = ot; res->npv = nv; res->npt = nt; res->n_pos_tris = nt; }
+            }
+            return;
+        }
+        // disjoint components on both sides: triangle goes to the negative side
+        // if any vertex is negative; vertices renumbered by first use
+        CUT_ALLOC(3, int, nv);                 // first use
+        __syncthreads();
+        if (s_err) goto fail_out;
+        int* first = (int*)sh.ptr[3];
+        for (int side = 0; side < 2; side++) {
+            for (int v = tid; v < nv; v += CUT_NT) first[v] = 0x7fffffff;
+            __syncthreads();
+            int cnt_t = 0;
+            for (int t = tid; t < nt; t += CUT_NT) {
+                int i0 = tris[3 * t], i1 = tris[3 * t + 1], i2 = tris[3 * t + 2];
+                int isneg = sg[i0] < 0 || sg[i1] < 0 || sg[i2] < 0;
+                if (isneg != side) continue;
+                cnt_t++;
+                atomicMin(&first[i0], 3 * t); atomicMin(&first[i1], 3 * t + 1); atomicMin(&first[i2], 3 * t + 2);
+            }
+            cnt_t = warp_sum_i(cnt_t);
+            if (tid == 0) sh.cnt[3] = 0;
+            __syncthreads();
+            if (lane == 0) atomicAdd(&sh.cnt[3], cnt_t);
+            __syncthreads();
+            // rank of each first use among positions 0..3nt-1: flag array over positions
+            CUT_ALLOC(4 + side, int, 3 * nt);
+            __syncthreads();
+            if (s_err) goto fail_out;
+            int* rank = (int*)sh.ptr[4 + side];
+            for (int p = tid; p < 3 * nt; p += CUT_NT) rank[p] = 0;
+            __syncthreads();
+            for (int v = tid; v < nv; v += CUT_NT) if (first[v] != 0x7fffffff) rank[first[v]] = 1;
+            __syncthreads();
+            int nvs = cta_scan_inplace(rank, 3 * nt, sh.scan);
+            int nts = sh.cnt[3];
+            if (tid == 0) {
+                float* ov = side ? fixed.nv : fixed.pv; int* ot = side ? fixed.nt : fixed.pt;
+                int vc = side ? fixed.nv_cap : fixed.pv_cap, tc = side ? fixed.nt_cap : fixed.pt_cap;
+                if (!fixed.pv) {
+                    ov = (float*)arena_alloc(arena, sizeof(float) * 3ull * (nvs > 0 ? nvs : 1), &s_err);
+                    ot = (int*)arena_alloc(arena, sizeof(int) * 3ull * (nts > 0 ? nts : 1), &s_err);
+                    vc = nvs; tc = nts;
+                }
+                if (!ov || !ot || nvs > vc || nts > tc) s_err |= KERR_PC_POOL_OOM;
+                sh.ptr[6 + 2 * side] = ov; sh.ptr[7 + 2 * side] = ot;
+                sh.ival[2 + 2 * side] = nvs; sh.ival[3 + 2 * side] = nts;
+                sh.cnt[4] = 0;
+            }
+            __syncthreads();
+            if (s_err) goto fail_out;
+            float* ov = (float*)sh.ptr[6 + 2 * side]; int* ot = (int*)sh.ptr[7 + 2 * side];
+            for (int v = tid; v < nv; v += CUT_NT) {
+                if (first[v] == 0x7fffffff) continue;
+                int j = rank[first[v]];
+                ov[3 * j] = verts[3 * v]; ov[3 * j + 1] = verts[3 * v + 1]; ov[3 * j + 2] = verts[3 * v + 2];
+            }
+            // triangles of this side in input order: scan over per-triangle flags
+            CUT_ALLOC(10 + side, int, nt);
+            __syncthreads();
+            if (s_err) goto fail_out;
+            int* tpos = (int*)sh.ptr[10 + side];
+            for (int t = tid; t < nt; t += CUT_NT) {
+                int isneg = sg[tris[3 * t]] < 0 || sg[tris[3 * t + 1]] < 0 || sg[tris[3 * t + 2]] < 0;
+                tpos[t] = isneg == side;
+            }
+            __syncthreads();
+            cta_scan_inplace(tpos, nt, sh.scan);
+            for (int t = tid; t < nt; t += CUT_NT) {
+                int i0 = tris[3 * t], i1 = tris[3 * t + 1], i2 = tris[3 * t + 2];
+                int isneg = sg[i0] < 0 || sg[i1] < 0 || sg[i2] < 0;
+                if (isneg != side) continue;
+                int k = tpos[t];
+                ot[3 * k] = rank[first[i0]]; ot[3 * k + 1] = rank[first[i1]]; ot[3 * k + 2] = rank[first[i2]];
+            }
+            __syncthreads();
+        }
+        if (tid == 0) {
+            memset(res, 0, sizeof(CutResult));
+            res->pv = (float*)sh.ptr[6]; res->pt = (int*)sh.ptr[7]; res->npv = sh.ival[2]; res->npt = sh.ival[3];
+            res->nv = (float*)sh.ptr[8]; res->nt = (int*)sh.ptr[9]; res->nnv = sh.ival[4]; res->nnt = sh.ival[5];
+            res->n_pos_tris = res->npt; res->n_neg_tris = res->nnt;
+        }
+        return;
+    }
+    // ---------------- crossing edges: collect, sort, dedup
+    const int occN = next_pow2_i(n_occ);
+    CUT_ALLOC(3, unsigned long long, occN);
+    __syncthreads();
+    if (s_err) goto fail_out;
+    unsigned long long* ce = (unsigned long long*)sh.ptr[3];
+    if (tid == 0) sh.cnt[3] = 0;
+    __syncthreads();
+    for (int base = 0; base < nt; base += CUT_NT) {
+        int t = base + tid;
+        unsigned long long k[3]; int m = 0;
+        if (t < nt) {
+            for (int e = 0; e < 3; e++) {
+                int va = tris[3 * t + e], vb = tris[3 * t + (e + 1) % 3];
+                int ea = sg[va] >= 0, eb = sg[vb] >= 0;
+                if (ea != eb) {
+                    int lo = min(va, vb), hi = max(va, vb);
+                    k[m++] = ((unsigned long long)(unsigned)lo << 32) | (unsigned)hi;
+                }
+            }
+        }
+        int off = 0, tot = 0;
+        off = block_exclusive_scan(m, sh.scan, &tot);
+        int b0 = sh.cnt[3];
+        for (int j = 0; j < m; j++) ce[b0 + off + j] = k[j];
+        __syncthreads();
+        if (tid == 0) sh.cnt[3] += tot;
+        __syncthreads();
+    }
+    cta_sort_u64(ce, n_occ);
+    // unique keys (sorted order) and the intersection vertex of each
+    CUT_ALLOC(4, int, n_occ);                  // 1 where a new key starts
+    CUT_ALLOC(5, int, n_occ);                  // scanned copy: unique rank
+    __syncthreads();
+    if (s_err) goto fail_out;
+    int* uflag = (int*)sh.ptr[4];
+    int* urank = (int*)sh.ptr[5];
+    for (int i = tid; i < n_occ; i += CUT_NT) {
+        int f = (i == 0 || ce[i] != ce[i - 1]) ? 1 : 0;
+        uflag[i] = f; urank[i] = f;
+    }
+    __syncthreads();
+    const int n_u = cta_scan_inplace(urank, n_occ, sh.scan);
+    CUT_ALLOC(6, unsigned long long, n_u);     // unique edge keys
+    CUT_ALLOC(7, int, n_u);                    // intersection vertex per edge
+    CUT_ALLOC(2, int, n_u);                    // new-vertex rank
+    __syncthreads();
+    if (s_err) goto fail_out;
+    unsigned long long* ue = (unsigned long long*)sh.ptr[6];
+    int* isect = (int*)sh.ptr[7];
+    int* upos = (int*)sh.ptr[2];
+    for (int i = tid; i < n_occ; i += CUT_NT) if (uflag[i]) ue[urank[i]] = ce[i];
+    __syncthreads();
+    for (int i = tid; i < n_u; i += CUT_NT) {
+        int va = (int)(ue[i] >> 32), vb = (int)(ue[i] & 0xffffffffu);
+        float d0 = cut_plane_eval(pa, pb, pc, pd, verts + 3 * va);
+        float d1 = cut_plane_eval(pa, pb, pc, pd, verts + 3 * vb);
+        int reuse;
+        if (fabsf(d0) <= CUT_EPS && fabsf(d1) > CUT_EPS) reuse = va;
+        else if (fabsf(d1) <= CUT_EPS && fabsf(d0) > CUT_EPS) reuse = vb;
+        else reuse = -1;
+        isect[i] = reuse;
+        upos[i] = reuse < 0 ? 1 : 0;
+    }
+    __syncthreads();
+    const int n_new = cta_scan_inplace(upos, n_u, sh.scan);
+    const int n_all = nv + n_new;
+    CUT_ALLOC(8, float, 3 * n_all);            // all vertices
+    __syncthreads();
+    if (s_err) goto fail_out;
+    float* all = (float*)sh.ptr[8];
+    for (int i = tid; i < 3 * nv; i += CUT_NT) all[i] = verts[i];
+    for (int i = tid; i < n_u; i += CUT_NT) {
+        if (isect[i] >= 0) continue;
+        int va = (int)(ue[i] >> 32), vb = (int)(ue[i] & 0xffffffffu);
+        float d0 = cut_plane_eval(pa, pb, pc, pd, verts + 3 * va);
+        float d1 = cut_plane_eval(pa, pb, pc, pd, verts + 3 * vb);
+        float t = d0 / (d0 - d1);
+        int ni = nv + upos[i];
+        for (int k = 0; k < 3; k++)
+            all[3 * ni + k] = fmaf(t, verts[3 * vb + k] - verts[3 * va + k], verts[3 * va + k]);
+        isect[i] = ni;
+    }
+    __syncthreads();
+    // ---------------- split: per-triangle piece counts then write in order
+    CUT_ALLOC(9, int, nt);     // pos offsets
+    CUT_ALLOC(10, int, nt);    // neg offsets
+    __syncthreads();
+    if (s_err) goto fail_out;
+    int* poff = (int*)sh.ptr[9];
+    int* noff = (int*)sh.ptr[10];
+    auto isect_of = [&](int a, int b) -> int {
+        int lo = min(a, b), hi = max(a, b);
+        unsigned long long key = ((unsigned long long)(unsigned)lo << 32) | (unsigned)hi;
+        int f = lower_bound_u64(ue, n_u, key);
+        return (f < n_u && ue[f] == key) ? isect[f] : -1;
+    };
+    // piece emitter: mode 0 = count, 1 = write
+    auto split = [&](int t, int mode, int* pt_, int* nt_, int po, int no) {
+        int i0 = tris[3 * t], i1 = tris[3 * t + 1], i2 = tris[3 * t + 2];
+        int s0 = sg[i0], s1 = sg[i1], s2 = sg[i2];
+        int np_ = 0, nn_ = 0;
+        auto P = [&](int x, int y, int z) { if (mode) { pt_[3 * (po + np_)] = x; pt_[3 * (po + np_) + 1] = y; pt_[3 * (po + np_) + 2] = z; } np_++; };
+        auto N = [&](int x, int y, int z) { if (mode) { nt_[3 * (no + nn_)] = x; nt_[3 * (no + nn_) + 1] = y; nt_[3 * (no + nn_) + 2] = z; } nn_++; };
+        int hp = s0 > 0 || s1 > 0 || s2 > 0, hn = s0 < 0 || s1 < 0 || s2 < 0;
+        if (!hp || !hn) {
+            if (hn) N(i0, i1, i2);
+            else if (hp) P(i0, i1, i2);
+            else {
+                float e1x = all[3 * i1] - all[3 * i0], e1y = all[3 * i1 + 1] - all[3 * i0 + 1], e1z = all[3 * i1 + 2] - all[3 * i0 + 2];
+                float e2x = all[3 * i2] - all[3 * i0], e2y = all[3 * i2 + 1] - all[3 * i0 + 1], e2z = all[3 * i2 + 2] - all[3 * i0 + 2];
+                double dot = (double)pa * ((double)e1y * e2z - (double)e1z * e2y)
+                           + (double)pb * ((double)e1z * e2x - (double)e1x * e2z)
+                           + (double)pc * ((double)e1x * e2y - (double)e1y * e2x);
+                if (dot > 0) P(i0, i1, i2); else N(i0, i1, i2);
+            }
+            return make_int2(np_, nn_);
+        }
+        int vi[3] = {i0, i1, i2}, si[3] = {s0, s1, s2};
+        int on = -1;
+        for (int k = 0; k < 3; k++) if (si[k] == 0) { on = k; break; }
+        if (on >= 0) {
+            int ov = vi[on], a_i = vi[(on + 1) % 3], b_i = vi[(on + 2) % 3], sa = si[(on + 1) % 3], sb = si[(on + 2) % 3];
+            if (sa == sb) { if (sa > 0) P(i0, i1, i2); else N(i0, i1, i2); }
+            else {
+                int nvi = isect_of(a_i, b_i);
+                if (nvi >= 0) {
+                    if (sa > 0) { P(ov, a_i, nvi); N(ov, nvi, b_i); }
+                    else        { N(ov, a_i, nvi); P(ov, nvi, b_i); }
+                }
+            }
+        } else {
+            int lone = -1;
+            for (int k = 0; k < 3; k++) if (si[k] != si[(k + 1) % 3] && si[k] != si[(k + 2) % 3]) { lone = k; break; }
+            if (lone >= 0) {
+                int lv = vi[lone], ov1 = vi[(lone + 1) % 3], ov2 = vi[(lone + 2) % 3], lsg = si[lone];
+                int nv1 = isect_of(lv, ov1), nv2 = isect_of(lv, ov2);
+                if (nv1 >= 0 && nv2 >= 0) {
+                    if (lsg > 0) { P(lv, nv1, nv2); N(ov1, nv2, nv1); N(ov1, ov2, nv2); }
+                    else         { N(lv, nv1, nv2); P(ov1, nv2, nv1); P(ov1, ov2, nv2); }
+                }
+            }
+        }
+        return make_int2(np_, nn_);
+    };
+    for (int t = tid; t < nt; t += CUT_NT) {
+        int2 c = split(t, 0, nullptr, nullptr, 0, 0);
+        poff[t] = c.x; noff[t] = c.y;
+    }
+    __syncthreads();
+    const int n_pos = cta_scan_inplace(poff, nt, sh.scan);
+    const int n_neg = cta_scan_inplace(noff, nt, sh.scan);
+    CUT_ALLOC(11, int, 3 * n_pos);
+    CUT_ALLOC(12, int, 3 * n_neg);
+    __syncthreads();
+    if (s_err) goto fail_out;
+    int* ptri = (int*)sh.ptr[11];
+    int* ntri = (int*)sh.ptr[12];
+    for (int t = tid; t < nt; t += CUT_NT) split(t, 1, ptri, ntri, poff[t], noff[t]);
+    __syncthreads();
+    // ---------------- boundary of the positive side among edges on the cut
+    // key = min<<33 | max<<1 | (a > b)
+    if (tid == 0) sh.cnt[5] = 0;
+    __syncthreads();
+    int nbc_local = 0;
+    for (int t = tid; t < n_pos; t += CUT_NT)
+        for (int e = 0; e < 3; e++) {
+            int a = ptri[3 * t + e], b = ptri[3 * t + (e + 1) % 3];
+            bool ona = a >= nv || sg[a] == 0, onb = b >= nv || sg[b] == 0;
+            nbc_local += (ona && onb);
+        }
+    nbc_local = warp_sum_i(nbc_local);
+    if (lane == 0) atomicAdd(&sh.cnt[5], nbc_local);
+    __syncthreads();
+    const int nbc = sh.cnt[5];
+    CUT_ALLOC(13, unsigned long long, next_pow2_i(nbc));
+    __syncthreads();
+    if (s_err) goto fail_out;
+    unsigned long long* bk = (unsigned long long*)sh.ptr[13];
+    if (tid == 0) sh.cnt[6] = 0;
+    __syncthreads();
+    for (int t = tid; t < n_pos; t += CUT_NT)
+        for (int e = 0; e < 3; e++) {
+            int a = ptri[3 * t + e], b = ptri[3 * t + (e + 1) % 3];
+            bool ona = a >= nv || sg[a] == 0, onb = b >= nv || sg[b] == 0;
+            if (ona && onb) {
+                int lo = min(a, b), hi = max(a, b);
+                int s = atomicAdd(&sh.cnt[6], 1);
+                bk[s] = ((unsigned long long)(unsigned)lo << 33) | ((unsigned long long)(unsigned)hi << 1) | (a > b ? 1ull : 0ull);
+            }
+        }
+    __syncthreads();
+    cta_sort_u64(bk, nbc);
+    // unmatched directed edges -> be (a<<32|b), sorted
+    CUT_ALLOC(14, unsigned long long, next_pow2_i(nbc > 0 ? nbc : 1));
+    __syncthreads();
+    if (s_err) goto fail_out;
+    unsigned long long* be = (unsigned long long*)sh.ptr[14];
+    if (tid == 0) sh.cnt[7] = 0;
+    __syncthreads();
+    for (int i = tid; i < nbc; i += CUT_NT) {
+        unsigned long long k = bk[i] >> 1;
+        bool dup = (i > 0 && (bk[i - 1] >> 1) == k) || (i + 1 < nbc && (bk[i + 1] >> 1) == k);
+        if (!dup) {
+            int lo = (int)(k >> 32), hi = (int)(k & 0xffffffffu);
+            int a = (bk[i] & 1ull) ? hi : lo, b = (bk[i] & 1ull) ? lo : hi;
+            int s = atomicAdd(&sh.cnt[7], 1);
+            be[s] = ((unsigned long long)(unsigned)a << 32) | (unsigned)b;
+        }
+    }
+    __syncthreads();
+    const int nb = sh.cnt[7];
+    cta_sort_u64(be, nb);
+    // ---------------- caps (warp 0)
+    const int poly_cap = nb * 4 + 64;
+    CUT_ALLOC(15, int, 4 * nb + 3 * poly_cap + 3 * poly_cap);
+    __syncthreads();
+    if (s_err) goto fail_out;
+    {
+        int* blk = (int*)sh.ptr[15];
+        int* used = blk; int* lv = used + nb; int* ls = lv + nb; int* lsz = ls + nb;
+        int* poly = lsz + nb; int* tmp = poly + poly_cap; int* capt = tmp + 2 * poly_cap;
+        if (warp == 0) {
+            int nl = 0;
+            int nc = (nb > 0) ? cut_build_caps(all, n_all, be, nb, pa, pb, pc, used, lv, ls, lsz, poly, tmp,
+                                               poly_cap, capt, &nl, lane) : 0;
+            if (lane == 0) { sh.ival[8] = nc; sh.ival[9] = nl; }
+        }
+        __syncthreads();
+    }
+    {
+        const int n_cap = sh.ival[8];
+        int* capt = (int*)sh.ptr[15] + 4 * nb + 3 * poly_cap;
+        if (n_cap < 0) {
+            // cap failure: whole mesh on the positive side
+            if (tid == 0) {
+                float* ov = fixed.pv; int* ot = fixed.pt;
+                int vc = fixed.pv_cap, tc = fixed.pt_cap;
+                if (!fixed.pv) {
+                    ov = (float*)arena_alloc(arena, sizeof(float) * 3ull * nv, &s_err);
+                    ot = (int*)arena_alloc(arena, sizeof(int) * 3ull * nt, &s_err);
+                    vc = nv; tc = nt;
+                }
+                if (!ov || !ot || nv > vc || nt > tc) s_err |= KERR_PC_POOL_OOM;
+                sh.ptr[1] = ov; sh.ptr[2] = ot;
+            }
+            __syncthreads();
+            if (s_err) goto fail_out;
+            float* ov = (float*)sh.ptr[1]; int* ot = (int*)sh.ptr[2];
+            for (int i = tid; i < 3 * nv; i += CUT_NT) ov[i] = verts[i];
+            for (int i = tid; i < 3 * nt; i += CUT_NT) ot[i] = tris[i];
+            if (tid == 0) {
+                memset(res, 0, sizeof(CutResult));
+                res->pv = ov; res->pt = ot; res->npv = nv; res->npt = nt;
+                res->n_pos_tris = n_pos; res->n_neg_tris = n_neg; res->cap_failed = 1;
+                res->n_loops = sh.ival[9]; res->n_boundary = nb; res->n_cross = n_u;
+            }
+            return;
+        }
+        // ---------------- output compaction per side
+        int flip;
+        {
+            float ax = fabsf(pa), ay = fabsf(pb), az = fabsf(pc);
+            float n2d[3] = {0.f, 0.f, 0.f};
+            if (ax >= ay && ax >= az) n2d[0] = 1.0f;
+            else if (ay >= az)        n2d[1] = -1.0f;
+            else                      n2d[2] = 1.0f;
+            flip = (n2d[0] * (-pa) + n2d[1] * (-pb) + n2d[2] * (-pc) < 0) ? 1 : 0;
+        }
+        CUT_ALLOC(1, int, n_all);
+        __syncthreads();
+        if (s_err) goto fail_out;
+        int* remap = (int*)sh.ptr[1];
+        for (int side = 0; side < 2; side++) {
+            const int* st = side == 0 ? ptri : ntri;
+            const int ns = side == 0 ? n_pos : n_neg;
+            for (int v = tid; v < n_all; v += CUT_NT) remap[v] = 0;
+            __syncthreads();
+            for (int i = tid; i < 3 * ns; i += CUT_NT) remap[st[i]] = 1;
+            for (int i = tid; i < 3 * n_cap; i += CUT_NT) remap[capt[i]] = 1;
+            __syncthreads();
+            // remember used flags in the sign bit region: scan destroys them,
+            // so mark unused as -1 after the scan by re-deriving from triangles
+            CUT_ALLOC(2, int, n_all);
+            __syncthreads();
+            if (s_err) goto fail_out;
+            int* usedf = (int*)sh.ptr[2];
+            for (int v = tid; v < n_all; v += CUT_NT) usedf[v] = remap[v];
+            __syncthreads();
+            const int cnv = cta_scan_inplace(remap, n_all, sh.scan);
+            const int cnt_ = ns + n_cap;
+            if (tid == 0) {
+                float* ov = side ? fixed.nv : fixed.pv; int* ot = side ? fixed.nt : fixed.pt;
+                int vc = side ? fixed.nv_cap : fixed.pv_cap, tc = side ? fixed.nt_cap : fixed.pt_cap;
+                if (!fixed.pv) {
+                    ov = (float*)arena_alloc(arena, sizeof(float) * 3ull * (cnv > 0 ? cnv : 1), &s_err);
+                    ot = (int*)arena_alloc(arena, sizeof(int) * 3ull * (cnt_ > 0 ? cnt_ : 1), &s_err);
+                    vc = cnv; tc = cnt_;
+                }
+                if (!ov || !ot || cnv > vc || cnt_ > tc) s_err |= KERR_PC_POOL_OOM;
+                sh.ptr[6 + 2 * side] = ov; sh.ptr[7 + 2 * side] = ot;
+                sh.ival[2 + 2 * side] = cnv; sh.ival[3 + 2 * side] = cnt_;
+            }
+            __syncthreads();
+            if (s_err) goto fail_out;
+            float* ov = (float*)sh.ptr[6 + 2 * side]; int* ot = (int*)sh.ptr[7 + 2 * side];
+            for (int v = tid; v < n_all; v += CUT_NT)
+                if (usedf[v]) { int j = remap[v]; ov[3 * j] = all[3 * v]; ov[3 * j + 1] = all[3 * v + 1]; ov[3 * j + 2] = all[3 * v + 2]; }
+            for (int i = tid; i < 3 * ns; i += CUT_NT) ot[i] = remap[st[i]];
+            for (int t = tid; t < n_cap; t += CUT_NT) {
+                int v0 = capt[3 * t], v1 = capt[3 * t + 1], v2 = capt[3 * t + 2];
+                int o = 3 * (ns + t);
+                ot[o] = remap[v0];
+                if (side == 0) { ot[o + 1] = flip ? remap[v2] : remap[v1]; ot[o + 2] = flip ? remap[v1] : remap[v2]; }
+                else           { ot[o + 1] = flip ? remap[v1] : remap[v2]; ot[o + 2] = flip ? remap[v2] : remap[v1]; }
+            }
+            __syncthreads();
+        }
+        if (tid == 0) {
+            memset(res, 0, sizeof(CutResult));
+            res->pv = (float*)sh.ptr[6]; res->pt = (int*)sh.ptr[7]; res->npv = sh.ival[2]; res->npt = sh.ival[3];
+            res->nv = (float*)sh.ptr[8]; res->nt = (int*)sh.ptr[9]; res->nnv = sh.ival[4]; res->nnt = sh.ival[5];
+            res->n_pos_tris = n_pos; res->n_neg_tris = n_neg; res->n_cap = n_cap;
+            res->n_loops = sh.ival[9]; res->n_boundary = nb; res->n_cross = n_u;
+        }
+        return;
+    }
+    }
+fail_out:
+    __syncthreads();
+    if (tid == 0) {
+        memset(res, 0, sizeof(CutResult));
+        res->err = s_err ? s_err : KERR_PC_SCRATCH_OOM;
+    }
+#undef CUT_ALLOC
+}

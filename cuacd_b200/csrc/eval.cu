@@ -1,0 +1,243 @@
+// eval.cu — candidate evaluator: for each plane, cut the mesh with caps,
+// compute both fragments' volumes and exact hulls, optionally the sampled
+// Hausdorff distance fragment<->hull, and the part costs of
+// cuda/la_common.cuh:21-34.  This is the per-candidate scorer of the
+// reference's la_expand (cuda/la_expand.cu:65-340) + la_hull
+// (:357-424) + la_hausdorff_parts (cuda/la_refine.cu:19-45), as one
+// device-resident pipeline of four launches with no host round trip:
+//   k_cut_planes  (cut.cu)   one CTA per plane, fragments into the arena
+//   k_frag_hull              one CTA per fragment: volume + exact hull
+//   Hausdorff prep/plan/query (hausdorff.cu), pairs (hull, fragment)
+//   k_eval_finish            costs and the per-candidate record
+#include "context.cuh"
+#include "hull.cuh"
+#include "cut.cuh"
+#include "hausdorff.cuh"
+#include "launch.h"
+
+struct FragInfo {
+    float* hv; int* ht; int hnv, hnt;
+    double mesh_vol;
+    float hull_vol; int err;
+};
+
+__global__ void __launch_bounds__(HULL_NT)
+k_frag_hull(const CutResult* __restrict__ cuts, int n_cand, Arena* arena, FragInfo* frags)
+{
+    __shared__ HullShared sh;
+    __shared__ char* s_scr;
+    __shared__ float* s_ov;
+    __shared__ int* s_ot;
+    __shared__ int s_err, s_nv, s_nt;
+    __shared__ float s_vol;
+    const int f = blockIdx.x, cand = f >> 1, side = f & 1;
+    if (cand >= n_cand) return;
+    const CutResult& C = cuts[cand];
+    const float* v = side ? C.nv : C.pv;
+    const int* t = side ? C.nt : C.pt;
+    const int nv = side ? C.nnv : C.npv, nt = side ? C.nnt : C.npt;
+    const bool empty = C.err != 0 || nv <= 0 || nt <= 0 || C.npv <= 0 || C.nnv <= 0;
+    if (threadIdx.x == 0) {
+        s_err = 0; s_scr = nullptr; s_ov = nullptr; s_ot = nullptr;
+        if (!empty) {
+            s_scr = (char*)arena_alloc(arena, hull_scratch_bytes(nv), &s_err);
+            s_ov = (float*)arena_alloc(arena, 12ull * nv, &s_err);
+            s_ot = (int*)arena_alloc(arena, 12ull * (2 * nv + 4), &s_err);
+        }
+    }
+    __syncthreads();
+    FragInfo F;
+    memset(&F, 0, sizeof(F));
+    if (empty || s_err || !s_scr || !s_ov || !s_ot) {
+        if (threadIdx.x == 0) { F.err = s_err; frags[f] = F; }
+        return;
+    }
+    double mv = block_mesh_signed_volume(v, nv, t, nt, sh.dsh);
+    HullOut o; o.verts = s_ov; o.tris = s_ot; o.vidx = nullptr; o.max_hv = nv; o.max_ht = 2 * nv + 4;
+    hull_cta(v, nv, s_scr, o, &s_nv, &s_nt, &s_vol, &s_err, sh);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        F.hv = s_ov; F.ht = s_ot; F.hnv = s_nv; F.hnt = s_nt;
+        F.mesh_vol = fabs(mv); F.hull_vol = s_vol; F.err = s_err;
+        frags[f] = F;
+    }
+}
+
+// surfaces for the Hausdorff pairs: pair f = (hull of fragment f, fragment f)
+__global__ void k_make_surfs(const CutResult* __restrict__ cuts, const FragInfo* __restrict__ frags, int n_frag,
+                             HDSurf* surfs)
+{
+    int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= n_frag) return;
+    const CutResult& C = cuts[f >> 1];
+    const FragInfo& F = frags[f];
+    bool ok = F.err == 0 && F.hnt > 0 && C.npv > 0 && C.nnv > 0;
+    HDSurf A = {F.hv, F.ht, ok ? F.hnv : 0, ok ? F.hnt : 0};
+    HDSurf B;
+    if (f & 1) { B.v = C.nv; B.t = C.nt; B.nv = ok ? C.nnv : 0; B.nt = ok ? C.nnt : 0; }
+    else       { B.v = C.pv; B.t = C.pt; B.nv = ok ? C.npv : 0; B.nt = ok ? C.npt : 0; }
+    surfs[2 * f] = A;
+    surfs[2 * f + 1] = B;
+}
+
+__global__ void k_eval_finish(const CutResult* __restrict__ cuts, const FragInfo* __restrict__ frags,
+                              const float* __restrict__ hd, int n_cand, int with_hd, const int* arena_err,
+                              cuacd_cand_result* out)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_cand) return;
+    const CutResult& C = cuts[i];
+    cuacd_cand_result r;
+    memset(&r, 0, sizeof(r));
+    r.err = C.err | frags[2 * i].err | frags[2 * i + 1].err | (arena_err ? *arena_err : 0);
+    r.ok = (r.err == 0 && C.npv > 0 && C.nnv > 0) ? 1 : 0;
+    r.nv[0] = C.npv; r.nv[1] = C.nnv; r.nt[0] = C.npt; r.nt[1] = C.nnt;
+    r.n_cap = C.n_cap;
+    if (r.ok) {
+        float worst_rv = 0.f, worst_full = 0.f;
+        for (int s = 0; s < 2; s++) {
+            const FragInfo& F = frags[2 * i + s];
+            r.hull_nv[s] = F.hnv; r.hull_nt[s] = F.hnt;
+            r.mesh_vol[s] = (float)F.mesh_vol; r.hull_vol[s] = F.hull_vol;
+            float h = with_hd ? hd[2 * i + s] : 0.f;
+            r.hausdorff[s] = h;
+            r.cost_rv[s] = part_cost_rv((double)F.hull_vol, F.mesh_vol);
+            r.cost_full[s] = fmaxf(r.cost_rv[s], h);
+            worst_rv = fmaxf(worst_rv, r.cost_rv[s]);
+            worst_full = fmaxf(worst_full, r.cost_full[s]);
+        }
+        r.score_rv = worst_rv; r.score_full = worst_full;
+    }
+    out[i] = r;
+}
+
+// ---------------------------------------------------------------------------
+// workspace and launch sequence (shared by the host and device entry points)
+// ---------------------------------------------------------------------------
+struct EvalWork {
+    float4* planes; CutResult* cuts; FragInfo* frags; HDSurf* surfs; HDPrep* preps;
+    char* dirs; int* i4; float* pmax; float* hd;
+};
+
+static size_t eval_fixed_bytes(int n)
+{
+    return al256(sizeof(float4) * n) + al256(sizeof(CutResult) * n) + al256(sizeof(FragInfo) * 2 * n)
+         + al256(sizeof(HDSurf) * 4 * n) + al256(sizeof(HDPrep) * 4 * n) + al256(hd_dir_bytes() * 4 * n)
+         + al256(sizeof(int) * 4) + 2 * al256(sizeof(float) * 2 * n);
+}
+
+static size_t eval_arena_bytes(int nv, int nt, int n)
+{
+    // per candidate: cut scratch + fragments; per fragment: hull scratch and
+    // output, two Hausdorff preps (hull and fragment)
+    int fv = nv + nv / 2 + 64, ft = nt + nt / 2 + 64;
+    size_t per = cut_scratch_bytes(nv, nt)
+               + 2 * (al256(hull_scratch_bytes(fv)) + al256(12 * (size_t)fv) + al256(12 * (size_t)(2 * fv + 4)))
+               + 2 * (al256(hd_prep_bytes(2 * fv)) + al256(hd_prep_bytes(ft)))
+               + 64 * 1024;
+    return per * (size_t)n;
+}
+
+static int eval_take(gpu_ctx* ctx, int n, EvalWork& W)
+{
+    W.planes = pool_take<float4>(ctx, n);
+    W.cuts = pool_take<CutResult>(ctx, n);
+    W.frags = pool_take<FragInfo>(ctx, 2 * n);
+    W.surfs = pool_take<HDSurf>(ctx, 4 * n);
+    W.preps = pool_take<HDPrep>(ctx, 4 * n);
+    W.dirs = pool_take<char>(ctx, hd_dir_bytes() * 4 * n);
+    W.i4 = pool_take<int>(ctx, 4);
+    W.pmax = pool_take<float>(ctx, 2 * n);
+    W.hd = pool_take<float>(ctx, 2 * n);
+    return W.hd ? 0 : -1;
+}
+
+static int sm_count_dev(int dev)
+{
+    int n = 148;
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    return n > 0 ? n : 148;
+}
+
+// All launches of one evaluation on stream s (planes already in W.planes).
+static void eval_launch(gpu_ctx* ctx, const float* d_v, int nv, const int* d_t, int nt, int n, int flags,
+                        float res, int mins, int total, EvalWork& W, cuacd_cand_result* d_out, cudaStream_t s)
+{
+    cudaMemsetAsync(W.i4, 0, 4 * sizeof(int), s);
+    launch_arena_reset(ctx->d_arena, ctx->pool + ctx->carve, ctx->cap - ctx->carve, s);
+    launch_cut_planes(d_v, nv, d_t, nt, W.planes, n, ctx->d_arena, W.cuts, s);
+    k_frag_hull<<<2 * n, HULL_NT, 0, s>>>(W.cuts, n, ctx->d_arena, W.frags);
+    ctx->launches += 3;
+    const bool hd = flags & CUACD_EVAL_HAUSDORFF;
+    if (hd) {
+        k_make_surfs<<<(2 * n + 127) / 128, 128, 0, s>>>(W.cuts, W.frags, 2 * n, W.surfs);
+        launch_hausdorff_pairs(W.surfs, 2 * n, ctx->d_arena, res, mins, total, W.preps, W.dirs, W.i4, W.pmax,
+                               W.i4 + 2, sm_count_dev(ctx->device), s);
+        launch_hd_sqrt(W.pmax, 2 * n, W.hd, 1, s);
+        ctx->launches += 5;
+    }
+    k_eval_finish<<<(n + 127) / 128, 128, 0, s>>>(W.cuts, W.frags, W.hd, n, hd ? 1 : 0, W.i4 + 2, d_out);
+    ctx->launches += 1;
+}
+
+extern "C" int cuacd_eval_candidates_device(gpu_ctx_t ctx, const float* d_verts, int nv, const int* d_tris, int nt,
+                                            const float* d_planes, int n_planes, int flags, float hd_resolution,
+                                            int hd_min_samples, int hd_total, cuacd_cand_result* d_out, void* stream)
+{
+    if (!ctx) return -1;
+    if (n_planes <= 0) return 0;
+    if (nv <= 0 || nt <= 0) return ctx_fail(ctx, KERR_MESH_INVALID, "empty mesh");
+    if (hd_resolution <= 0.f) { hd_resolution = 2000.f; }
+    if (hd_min_samples < 0) hd_min_samples = 1000;
+    CK(cudaSetDevice(ctx->device));
+    cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+    int rc = pool_begin(ctx, eval_fixed_bytes(n_planes) + eval_arena_bytes(nv, nt, n_planes));
+    if (rc) return rc;
+    EvalWork W;
+    if (eval_take(ctx, n_planes, W)) return ctx_fail(ctx, KERR_HEAP_OOM, "pool too small");
+    CK(cudaMemcpyAsync(W.planes, d_planes, sizeof(float4) * n_planes, cudaMemcpyDeviceToDevice, s));
+    eval_launch(ctx, d_verts, nv, d_tris, nt, n_planes, flags, hd_resolution, hd_min_samples, hd_total, W, d_out, s);
+    CK(cudaGetLastError());
+    return 0;
+}
+
+extern "C" int cuacd_eval_candidates(gpu_ctx_t ctx, const float* verts, int nv, const int* tris, int nt,
+                                     const float* planes, int n_planes, int flags, float hd_resolution,
+                                     int hd_min_samples, int hd_total, cuacd_cand_result* out)
+{
+    if (!ctx) return -1;
+    if (n_planes <= 0) return 0;
+    if (nv <= 0 || nt <= 0) return ctx_fail(ctx, KERR_MESH_INVALID, "empty mesh");
+    for (int i = 0; i < 3 * nt; i++)
+        if (tris[i] < 0 || tris[i] >= nv) return ctx_fail(ctx, KERR_MESH_INVALID, "triangle index out of range");
+    if (hd_resolution <= 0.f) hd_resolution = 2000.f;
+    if (hd_min_samples < 0) hd_min_samples = 1000;
+    CK(cudaSetDevice(ctx->device));
+    size_t extra = 0;
+    for (int attempt = 0; attempt < 4; attempt++) {
+        size_t need = al256(12 * (size_t)nv) + al256(12 * (size_t)nt) + al256(sizeof(cuacd_cand_result) * n_planes)
+                    + eval_fixed_bytes(n_planes) + eval_arena_bytes(nv, nt, n_planes) + extra;
+        int rc = pool_begin(ctx, need);
+        if (rc) return rc;
+        float* dv = pool_take<float>(ctx, 3 * (size_t)nv);
+        int* dt = pool_take<int>(ctx, 3 * (size_t)nt);
+        cuacd_cand_result* dout = pool_take<cuacd_cand_result>(ctx, n_planes);
+        EvalWork W;
+        if (eval_take(ctx, n_planes, W)) return ctx_fail(ctx, KERR_HEAP_OOM, "pool too small");
+        cudaStream_t s = ctx->stream;
+        CK(cudaMemcpyAsync(dv, verts, 12 * (size_t)nv, cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(dt, tris, 12 * (size_t)nt, cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(W.planes, planes, sizeof(float4) * n_planes, cudaMemcpyHostToDevice, s));
+        eval_launch(ctx, dv, nv, dt, nt, n_planes, flags, hd_resolution, hd_min_samples, hd_total, W, dout, s);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(out, dout, sizeof(cuacd_cand_result) * n_planes, cudaMemcpyDeviceToHost, s));
+        rc = sync_and_check(ctx, "eval_candidates");
+        if (rc) return rc;
+        bool oom = false;
+        for (int i = 0; i < n_planes; i++) if (out[i].err & (KERR_HEAP_OOM | KERR_PC_SCRATCH_OOM | KERR_HD_SCRATCH_OOM)) oom = true;
+        if (!oom) return 0;
+        if (ctx->fixed) return ctx_fail(ctx, KERR_HEAP_OOM, "device pool too small for this evaluation");
+        extra = (ctx->cap) * 2;       // grow and retry
+    }
+    return ctx_fail(ctx, KERR_HEAP_OOM, "device pool exhausted");
+}

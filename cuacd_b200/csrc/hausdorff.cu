@@ -1,0 +1,187 @@
+// hausdorff.cu — Hausdorff kernels and the gpu_test_hausdorff /
+// cuacd_hausdorff entry points.
+#include "context.cuh"
+#include "hausdorff.cuh"
+#include "launch.h"
+
+// One CTA per surface: budget, offsets, BVH.  Scratch from the arena.
+__global__ void __launch_bounds__(HD_NT)
+k_hd_prep(const HDSurf* __restrict__ surfs, int n_surf, Arena* arena, float resolution, int min_samples,
+          int total_override, HDPrep* preps, int* err)
+{
+    __shared__ HDShared sh;
+    __shared__ char* s_scr;
+    int i = blockIdx.x;
+    if (i >= n_surf) return;
+    HDSurf S = surfs[i];
+    if (threadIdx.x == 0) {
+        s_scr = nullptr;
+        if (S.nt > 0 && S.nv > 0) {
+            s_scr = (char*)arena_alloc(arena, hd_prep_bytes(S.nt), err);
+            if (!s_scr) atomicOr(err, KERR_HD_SCRATCH_OOM);
+        }
+    }
+    __syncthreads();
+    if (!s_scr) {
+        if (threadIdx.x == 0) { HDPrep P; memset(&P, 0, sizeof(P)); preps[i] = P; }
+        return;
+    }
+    hd_prep_cta(S, s_scr, resolution, min_samples, total_override, &preps[i], sh);
+}
+
+struct HDDir { int src, dst, pair, n_samples, chunk0; };
+
+// Plan the query directions: pair p has surfaces 2p (A) and 2p+1 (B);
+// direction 2p samples A against B, 2p+1 samples B against A.
+__global__ void k_hd_plan(const HDSurf* surfs, const HDPrep* preps, int n_pairs, HDDir* dirs, int* total_chunks,
+                          int* counter, float* pair_max)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    int c = 0;
+    for (int p = 0; p < n_pairs; p++) {
+        bool valid = surfs[2 * p].nt > 0 && surfs[2 * p].nv > 0 && surfs[2 * p + 1].nt > 0 && surfs[2 * p + 1].nv > 0;
+        bool has = valid && preps[2 * p].n_samples > 0 && preps[2 * p + 1].n_samples > 0;
+        for (int d = 0; d < 2; d++) {
+            HDDir D;
+            D.src = 2 * p + d; D.dst = 2 * p + 1 - d; D.pair = p;
+            D.n_samples = has ? preps[D.src].n_samples : 0;
+            D.chunk0 = c;
+            c += (D.n_samples + HD_CHUNK - 1) / HD_CHUNK;
+            dirs[2 * p + d] = D;
+        }
+        pair_max[p] = 0.f;
+    }
+    *total_chunks = c;
+    *counter = 0;
+}
+
+__global__ void __launch_bounds__(HD_NT)
+k_hd_query(const HDSurf* __restrict__ surfs, const HDPrep* __restrict__ preps, const HDDir* __restrict__ dirs,
+           int n_dirs, const int* total_chunks, int* counter, float* pair_max)
+{
+    __shared__ int s_chunk;
+    const int total = *total_chunks;
+    for (;;) {
+        if (threadIdx.x == 0) s_chunk = atomicAdd(counter, 1);
+        __syncthreads();
+        const int c = s_chunk;
+        __syncthreads();
+        if (c >= total) break;
+        int lo = 0, hi = n_dirs;                 // last dir with chunk0 <= c
+        while (hi - lo > 1) { int m = (lo + hi) >> 1; if (dirs[m].chunk0 <= c) lo = m; else hi = m; }
+        while (lo + 1 < n_dirs && dirs[lo + 1].chunk0 <= c && dirs[lo].n_samples == 0) lo++;
+        const HDDir D = dirs[lo];
+        const HDSurf S = surfs[D.src];
+        const HDPrep& PS = preps[D.src];
+        const HDPrep PD = preps[D.dst];
+        const int s0 = (c - D.chunk0) * HD_CHUNK;
+        const int s1 = min(s0 + HD_CHUNK, D.n_samples);
+        volatile float* vmax = pair_max + D.pair;
+        for (int s = s0 + threadIdx.x; s < s1; s += HD_NT) {
+            // triangle owning sample s: last t with offsets[t] <= s
+            int a = 0, b = S.nt;
+            while (b - a > 1) { int m = (a + b) >> 1; if (PS.offsets[m] <= s) a = m; else b = m; }
+            int t = a;
+            int k = s - PS.offsets[t];
+            float3 q = hd_sample(S.v, S.t[3 * t], S.t[3 * t + 1], S.t[3 * t + 2], t, k);
+            float stop = *vmax;
+            float d2 = hd_nearest(PD, q, stop);
+            if (d2 > stop) atomic_max_nonneg(pair_max + D.pair, d2);
+        }
+    }
+}
+
+__global__ void k_hd_sqrt(const float* pair_max, int n, float* out, int stride_floats)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[(size_t)i * stride_floats] = sqrtf(pair_max[i]);
+}
+
+size_t hd_pairs_scratch_bytes(int n_pairs, int max_nt_a, int max_nt_b)
+{
+    return (size_t)n_pairs * (al256(hd_prep_bytes(max_nt_a)) + al256(hd_prep_bytes(max_nt_b)) + 2048)
+         + al256(sizeof(HDDir) * 2 * (size_t)n_pairs) + al256(sizeof(HDPrep) * 2 * (size_t)n_pairs) + 4096;
+}
+
+// Launch the three Hausdorff stages for n_pairs pairs whose surfaces are in
+// d_surfs[2p] (A) / d_surfs[2p+1] (B).  Work buffers: d_preps[2n], d_dirs[2n],
+// d_i2[2] (total chunks, counter), d_pmax[n].
+void launch_hausdorff_pairs(const HDSurf* d_surfs, int n_pairs, Arena* arena, float resolution, int min_samples,
+                            int total, HDPrep* d_preps, void* d_dirs, int* d_i2, float* d_pmax, int* d_err,
+                            int n_sm, cudaStream_t s)
+{
+    if (n_pairs <= 0) return;
+    k_hd_prep<<<2 * n_pairs, HD_NT, 0, s>>>(d_surfs, 2 * n_pairs, arena, resolution, min_samples, total, d_preps, d_err);
+    k_hd_plan<<<1, 32, 0, s>>>(d_surfs, d_preps, n_pairs, (HDDir*)d_dirs, d_i2, d_i2 + 1, d_pmax);
+    k_hd_query<<<n_sm * 8, HD_NT, 0, s>>>(d_surfs, d_preps, (const HDDir*)d_dirs, 2 * n_pairs, d_i2, d_i2 + 1, d_pmax);
+}
+
+size_t hd_dir_bytes() { return sizeof(HDDir); }
+
+void launch_hd_sqrt(const float* pmax, int n, float* out, int stride_floats, cudaStream_t s)
+{
+    if (n > 0) k_hd_sqrt<<<(n + 127) / 128, 128, 0, s>>>(pmax, n, out, stride_floats);
+}
+
+static int sm_count(gpu_ctx* ctx)
+{
+    int n = 148;
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, ctx->device);
+    return n > 0 ? n : 148;
+}
+
+extern "C" int cuacd_hausdorff(gpu_ctx_t ctx, const float* a_verts, int a_nv, const int* a_tris, int a_nt,
+                               const float* b_verts, int b_nv, const int* b_tris, int b_nt,
+                               float resolution, int min_samples, int total, float* out_hausdorff)
+{
+    if (!ctx) return -1;
+    if (a_nv < 0 || a_nt < 0 || b_nv < 0 || b_nt < 0) return ctx_fail(ctx, KERR_MESH_INVALID, "negative size");
+    for (int i = 0; i < 3 * a_nt; i++) if (a_tris[i] < 0 || a_tris[i] >= a_nv) return ctx_fail(ctx, KERR_MESH_INVALID, "mesh a: index out of range");
+    for (int i = 0; i < 3 * b_nt; i++) if (b_tris[i] < 0 || b_tris[i] >= b_nv) return ctx_fail(ctx, KERR_MESH_INVALID, "mesh b: index out of range");
+    if (resolution <= 0.f) resolution = 2000.f;
+    if (min_samples < 0) min_samples = 1000;
+    CK(cudaSetDevice(ctx->device));
+    size_t need = al256(12 * (size_t)a_nv) + al256(12 * (size_t)a_nt) + al256(12 * (size_t)b_nv) + al256(12 * (size_t)b_nt)
+                + al256(sizeof(HDSurf) * 2) + al256(sizeof(int) * 4) + al256(sizeof(float) * 2)
+                + hd_pairs_scratch_bytes(1, a_nt, b_nt) + (1 << 20);
+    int rc = pool_begin(ctx, need);
+    if (rc) return rc;
+    float* dav = pool_take<float>(ctx, 3 * (size_t)a_nv); int* dat = pool_take<int>(ctx, 3 * (size_t)a_nt);
+    float* dbv = pool_take<float>(ctx, 3 * (size_t)b_nv); int* dbt = pool_take<int>(ctx, 3 * (size_t)b_nt);
+    HDSurf* dsurf = pool_take<HDSurf>(ctx, 2);
+    HDPrep* dprep = pool_take<HDPrep>(ctx, 2);
+    char* ddirs = pool_take<char>(ctx, 2 * sizeof(HDDir));
+    int* di = pool_take<int>(ctx, 4);
+    float* dmax = pool_take<float>(ctx, 2);
+    cudaStream_t s = ctx->stream;
+    if (a_nv) CK(cudaMemcpyAsync(dav, a_verts, 12 * (size_t)a_nv, cudaMemcpyHostToDevice, s));
+    if (a_nt) CK(cudaMemcpyAsync(dat, a_tris, 12 * (size_t)a_nt, cudaMemcpyHostToDevice, s));
+    if (b_nv) CK(cudaMemcpyAsync(dbv, b_verts, 12 * (size_t)b_nv, cudaMemcpyHostToDevice, s));
+    if (b_nt) CK(cudaMemcpyAsync(dbt, b_tris, 12 * (size_t)b_nt, cudaMemcpyHostToDevice, s));
+    HDSurf hs[2] = {{dav, dat, a_nv, a_nt}, {dbv, dbt, b_nv, b_nt}};
+    CK(cudaMemcpyAsync(dsurf, hs, sizeof(hs), cudaMemcpyHostToDevice, s));
+    CK(cudaMemsetAsync(di, 0, 4 * sizeof(int), s));
+    launch_arena_reset(ctx->d_arena, ctx->pool + ctx->carve, ctx->cap - ctx->carve, s);
+    launch_hausdorff_pairs(dsurf, 1, ctx->d_arena, resolution, min_samples, total, dprep, ddirs, di, dmax, di + 2,
+                           sm_count(ctx), s);
+    launch_hd_sqrt(dmax, 1, dmax + 1, 1, s);
+    ctx->launches += 5;
+    CK(cudaGetLastError());
+    int herr = 0;
+    float h = 0.f;
+    CK(cudaMemcpyAsync(&herr, di + 2, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(&h, dmax + 1, sizeof(float), cudaMemcpyDeviceToHost, s));
+    rc = sync_and_check(ctx, "hausdorff");
+    if (rc) return rc;
+    if (herr) return ctx_fail(ctx, herr, "hausdorff failed (error word 0x%x)", herr);
+    *out_hausdorff = h;
+    return 0;
+}
+
+extern "C" int gpu_test_hausdorff(gpu_ctx_t ctx, const float* hull_verts, int hull_nv, const int* hull_tris,
+                                  int hull_nt, const float* mesh_verts, int mesh_nv, const int* mesh_tris,
+                                  int mesh_nt, float* out_hausdorff)
+{
+    return cuacd_hausdorff(ctx, hull_verts, hull_nv, hull_tris, hull_nt, mesh_verts, mesh_nv, mesh_tris, mesh_nt,
+                           2000.f, 1000, 0, out_hausdorff);
+}

@@ -95,11 +95,11 @@ struct HullCtx {
     int m, P, nleaf;
 };
 
-__device__ __forceinline__ int pidx(float4 p) { return __float_as_int(p.w); }
+static __device__ __forceinline__ int pidx(float4 p) { return __float_as_int(p.w); }
 
 // Sign of N.(q - a) for integer-valued N (|N| < 2^30) and grid points,
 // FP32 with error bound, exact FP64 fallback.
-__device__ __forceinline__ int plane_sign(double nx, double ny, double nz,
+static __device__ __forceinline__ int plane_sign(double nx, double ny, double nz,
                                           float fx, float fy, float fz,
                                           float4 a, float4 q)
 {
@@ -113,21 +113,21 @@ __device__ __forceinline__ int plane_sign(double nx, double ny, double nz,
 }
 
 // Is q on the line through a with integer direction d?  (exact int32)
-__device__ __forceinline__ bool on_line(int dx, int dy, int dz, float4 a, float4 q)
+static __device__ __forceinline__ bool on_line(int dx, int dy, int dz, float4 a, float4 q)
 {
     int ex = (int)(q.x - a.x), ey = (int)(q.y - a.y), ez = (int)(q.z - a.z);
     return (dy * ez - dz * ey) == 0 && (dz * ex - dx * ez) == 0 && (dx * ey - dy * ex) == 0;
 }
 
 // min over the box of N.(x - a)
-__device__ __forceinline__ double box_min(double nx, double ny, double nz, float4 lo, float4 hi, float4 a)
+static __device__ __forceinline__ double box_min(double nx, double ny, double nz, float4 lo, float4 hi, float4 a)
 {
     double r = nx * (double)(nx >= 0 ? lo.x - a.x : hi.x - a.x)
              + ny * (double)(ny >= 0 ? lo.y - a.y : hi.y - a.y)
              + nz * (double)(nz >= 0 ? lo.z - a.z : hi.z - a.z);
     return r;
 }
-__device__ __forceinline__ double box_max(double nx, double ny, double nz, float4 lo, float4 hi, float4 a)
+static __device__ __forceinline__ double box_max(double nx, double ny, double nz, float4 lo, float4 hi, float4 a)
 {
     double r = nx * (double)(nx >= 0 ? hi.x - a.x : lo.x - a.x)
              + ny * (double)(ny >= 0 ? hi.y - a.y : lo.y - a.y)
@@ -138,7 +138,7 @@ __device__ __forceinline__ double box_max(double nx, double ny, double nz, float
 // Wrap: rotate the supporting plane about the line (a, d) into the cloud and
 // return the first point hit (sorted-point id), or -1 when every point lies
 // on the line.  q replaces c when (d x (c - a)).(q - a) < 0.
-__device__ int hull_wrap(const HullCtx& H, int a_id, int dx, int dy, int dz, int start_leaf)
+static __device__ int hull_wrap(const HullCtx& H, int a_id, int dx, int dy, int dz, int start_leaf)
 {
     float4 a = H.pts[a_id];
     int c = -1;
@@ -190,7 +190,7 @@ __device__ int hull_wrap(const HullCtx& H, int a_id, int dx, int dy, int dz, int
 // Collect up to `cap` points on the plane through a with outward normal N
 // (all points satisfy N.(q-a) <= 0).  Returns the count (may exceed cap:
 // the caller then treats the face as large).
-__device__ int hull_coplanar(const HullCtx& H, int a_id, double nx, double ny, double nz, int* out, int cap)
+static __device__ int hull_coplanar(const HullCtx& H, int a_id, double nx, double ny, double nz, int* out, int cap)
 {
     float4 a = H.pts[a_id];
     float fx = (float)nx, fy = (float)ny, fz = (float)nz;
@@ -223,7 +223,7 @@ __device__ int hull_coplanar(const HullCtx& H, int a_id, double nx, double ny, d
 // 2D projection dropping the dominant component of N; sign makes CCW
 // (w.r.t. N) positive.
 struct Proj { int ku, kv; int sgn; };
-__device__ __forceinline__ Proj make_proj(double nx, double ny, double nz)
+static __device__ __forceinline__ Proj make_proj(double nx, double ny, double nz)
 {
     double ax = fabs(nx), ay = fabs(ny), az = fabs(nz);
     int k = (ax >= ay && ax >= az) ? 0 : (ay >= az ? 1 : 2);
@@ -231,24 +231,24 @@ __device__ __forceinline__ Proj make_proj(double nx, double ny, double nz)
     Proj p; p.ku = (k + 1) % 3; p.kv = (k + 2) % 3; p.sgn = nk > 0 ? 1 : -1;
     return p;
 }
-__device__ __forceinline__ float comp(float4 p, int k) { return k == 0 ? p.x : (k == 1 ? p.y : p.z); }
+static __device__ __forceinline__ float comp(float4 p, int k) { return k == 0 ? p.x : (k == 1 ? p.y : p.z); }
 
 // 2D orientation of (p, r, t) in projected grid units (exact in int64)
-__device__ __forceinline__ long long o2d(const Proj& P, float4 p, float4 r, float4 t)
+static __device__ __forceinline__ long long o2d(const Proj& P, float4 p, float4 r, float4 t)
 {
     long long ux = (long long)(comp(r, P.ku) - comp(p, P.ku)), uy = (long long)(comp(r, P.kv) - comp(p, P.kv));
     long long wx = (long long)(comp(t, P.ku) - comp(p, P.ku)), wy = (long long)(comp(t, P.kv) - comp(p, P.kv));
     return (ux * wy - uy * wx) * P.sgn;
 }
-__device__ __forceinline__ long long d2d(const Proj& P, float4 p, float4 r)
+static __device__ __forceinline__ long long d2d(const Proj& P, float4 p, float4 r)
 {
     long long ux = (long long)(comp(r, P.ku) - comp(p, P.ku)), uy = (long long)(comp(r, P.kv) - comp(p, P.kv));
     return ux * ux + uy * uy;
 }
-__device__ __forceinline__ bool same_pos(float4 a, float4 b) { return a.x == b.x && a.y == b.y && a.z == b.z; }
+static __device__ __forceinline__ bool same_pos(float4 a, float4 b) { return a.x == b.x && a.y == b.y && a.z == b.z; }
 
 // Is candidate t better than r as the next CCW corner after cur?
-__device__ __forceinline__ bool next_better(const Proj& P, float4 cur, float4 r, float4 t)
+static __device__ __forceinline__ bool next_better(const Proj& P, float4 cur, float4 r, float4 t)
 {
     long long o = o2d(P, cur, r, t);
     if (o < 0) return true;
@@ -259,7 +259,7 @@ __device__ __forceinline__ bool next_better(const Proj& P, float4 cur, float4 r,
 
 // Serial polygon walk over a small coplanar set; writes corners (sorted-point
 // ids) starting with prev, cur.  Returns the corner count or -1.
-__device__ int hull_small_polygon(const HullCtx& H, const int* S, int ns, double nx, double ny, double nz,
+static __device__ int hull_small_polygon(const HullCtx& H, const int* S, int ns, double nx, double ny, double nz,
                                   int prev, int cur, int* out)
 {
     Proj P = make_proj(nx, ny, nz);
@@ -285,14 +285,14 @@ __device__ int hull_small_polygon(const HullCtx& H, const int* S, int ns, double
 // ---------------------------------------------------------------------------
 // hash sets of 64-bit keys (open addressing, empty = ~0)
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ unsigned long long ekey(int u, int v) {
+static __device__ __forceinline__ unsigned long long ekey(int u, int v) {
     return ((unsigned long long)(unsigned)u << 32) | (unsigned)v;
 }
-__device__ __forceinline__ unsigned hslot(unsigned long long k, int cap) {
+static __device__ __forceinline__ unsigned hslot(unsigned long long k, int cap) {
     return (unsigned)((k * 0x9E3779B97F4A7C15ull) >> 32) & (unsigned)(cap - 1);
 }
 // returns 1 inserted, 0 present, -1 full
-__device__ __forceinline__ int hset_insert(unsigned long long* tab, int cap, unsigned long long k) {
+static __device__ __forceinline__ int hset_insert(unsigned long long* tab, int cap, unsigned long long k) {
     unsigned s = hslot(k, cap);
     for (int i = 0; i < cap; i++) {
         unsigned long long prev = atomicCAS(&tab[s], ~0ull, k);
@@ -302,7 +302,7 @@ __device__ __forceinline__ int hset_insert(unsigned long long* tab, int cap, uns
     }
     return -1;
 }
-__device__ __forceinline__ bool hset_has(const unsigned long long* tab, int cap, unsigned long long k) {
+static __device__ __forceinline__ bool hset_has(const unsigned long long* tab, int cap, unsigned long long k) {
     unsigned s = hslot(k, cap);
     for (int i = 0; i < cap; i++) {
         unsigned long long x = tab[s];
@@ -334,7 +334,7 @@ struct HullShared {
 // (AoS xyz) of this cloud; `scratch` holds hull_scratch_bytes(n).
 // Writes the hull into `out` and returns (via *o_nv, *o_nt, *o_vol from
 // thread 0) the counts and FP64 volume; error bits go to *err_word.
-__device__ void hull_cta(const float* __restrict__ pts, int n, char* scratch,
+static __device__ void hull_cta(const float* __restrict__ pts, int n, char* scratch,
                          HullOut out, int* o_nv, int* o_nt, float* o_vol, int* err_word,
                          HullShared& sh)
 {

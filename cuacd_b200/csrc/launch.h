@@ -1,0 +1,24 @@
+// launch.h — host-side launch wrappers shared between translation units.
+#pragma once
+#include <cuda_runtime.h>
+#include "common.cuh"
+
+struct CutResult;
+
+// capi.cu
+void launch_arena_reset(Arena* a, char* base, unsigned long long cap, cudaStream_t s);
+
+// cut.cu
+size_t cut_scratch_bytes(int nv, int nt);
+void launch_cut_planes(const float* v, int nv, const int* t, int nt, const float4* planes, int n_planes,
+                       Arena* arena, CutResult* res, cudaStream_t s);
+
+// hausdorff.cu
+struct HDSurf;
+struct HDPrep;
+size_t hd_pairs_scratch_bytes(int n_pairs, int max_nt_a, int max_nt_b);
+size_t hd_dir_bytes();
+void launch_hausdorff_pairs(const HDSurf* d_surfs, int n_pairs, Arena* arena, float resolution, int min_samples,
+                            int total, HDPrep* d_preps, void* d_dirs, int* d_i2, float* d_pmax, int* d_err,
+                            int n_sm, cudaStream_t s);
+void launch_hd_sqrt(const float* pmax, int n, float* out, int stride_floats, cudaStream_t s);
