@@ -94,6 +94,9 @@ _opt("lookahead_decompose", _I, [_P, _P, _I, _P, _I, _P, _I, _P, _I,
                                  _I, _I, _I, _F, _I, _I, _I, _I, _I, _I, _I,
                                  _I, _F, _F, _I, _I, ctypes.POINTER(GpuResult)])
 _opt("gpu_result_free", None, [ctypes.POINTER(GpuResult)])
+_opt("cuacd_candidate_planes", _I, [_P, _P, _I, _P, _I, _I, _F, _F, _I, _F, _P, _P, _P])
+_opt("cuacd_profile_stages", _I, [_P, _I])
+_opt("cuacd_stage_times", _I, [_P, _P])
 
 
 def _fn(name):
@@ -290,6 +293,22 @@ class Context:
                                               *[ctypes.byref(x) for x in c]))
         a, b, d, e = [x.value for x in c]
         return pv[:a].copy(), pt[:b].copy(), nv_[:d].copy(), nt_[:e].copy()
+
+    # -- candidate planes ----------------------------------------------------
+    def candidate_planes(self, verts, tris, n_concave_edges=32, concave_eps=0.005, concave_threshold=3.49,
+                         width=0, min_edge_dist=0.0125):
+        """Concave-edge planes (la_concave.cu rule) followed by `width` axis
+        cuts -> (float32[n,4] concave planes, float32[width,4] axis planes,
+        bool[width] axis valid)."""
+        v, t = _as_f32(verts).reshape(-1, 3), _as_i32(tris).reshape(-1, 3)
+        out = np.zeros((4 * n_concave_edges + width + 1, 4), np.float32)
+        nc = ctypes.c_int(0)
+        valid = np.zeros(max(width, 1), np.int32)
+        self._check(_fn("cuacd_candidate_planes")(self._h, _ptr(v), len(v), _ptr(t), len(t), int(n_concave_edges),
+                                                  float(concave_eps), float(concave_threshold), int(width),
+                                                  float(min_edge_dist), _ptr(out), ctypes.byref(nc), _ptr(valid)))
+        k = nc.value
+        return out[:k].copy(), out[k:k + width].copy(), valid[:width].astype(bool)
 
     # -- candidate evaluator -------------------------------------------------
     def eval_candidates(self, verts, tris, planes, hausdorff=True, resolution=2000.0,

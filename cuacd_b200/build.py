@@ -26,8 +26,9 @@ def sources():
     return sorted(f for f in os.listdir(CSRC) if f.endswith(".cu"))
 
 
-# Per-file flags: the cut's FP32/FP64 expressions must not be contracted.
-PER_FILE = {"cut.cu": ["-fmad=false"]}
+# Per-file flags: the cut's and the plane generator's FP32/FP64 expressions
+# must not be contracted.
+PER_FILE = {"cut.cu": ["-fmad=false"], "concave.cu": ["-fmad=false"]}
 
 
 def _compile(src, extra):

@@ -22,7 +22,8 @@ __global__ void k_arena_reset(Arena* a, char* base, unsigned long long cap)
 __global__ void __launch_bounds__(HULL_NT)
 k_hull_batch(const float* __restrict__ pts, const int* __restrict__ offsets, int n_hulls,
              char* scratch, size_t stride, int max_hv, int max_ht,
-             float* out_v, int* out_t, int* out_nv, int* out_nt, float* out_vol, int* out_err)
+             float* out_v, int* out_t, int* out_nv, int* out_nt, float* out_vol, int* out_err,
+             unsigned long long* stats)
 {
     __shared__ HullShared sh;
     __shared__ int s_err;
@@ -40,6 +41,7 @@ k_hull_batch(const float* __restrict__ pts, const int* __restrict__ offsets, int
              &out_nv[h], &out_nt[h], out_vol ? &out_vol[h] : nullptr, &s_err, sh);
     __syncthreads();
     if (threadIdx.x == 0 && out_err) out_err[h] = s_err;
+    if (stats && threadIdx.x < 8) stats[8 * h + threadIdx.x] = sh.stats[threadIdx.x];
 }
 
 void launch_arena_reset(Arena* a, char* base, unsigned long long cap, cudaStream_t s)
@@ -125,13 +127,14 @@ extern "C" unsigned long long cuacd_launch_count(gpu_ctx_t ctx) { return ctx ? c
 // ---------------------------------------------------------------------------
 static int launch_hull_batch(gpu_ctx* ctx, const float* d_pts, const int* d_off, int n_hulls,
                              int max_pts, int max_hv, int max_ht, float* d_v, int* d_t,
-                             int* d_nv, int* d_nt, float* d_vol, int* d_err, cudaStream_t s)
+                             int* d_nv, int* d_nt, float* d_vol, int* d_err, cudaStream_t s,
+                             unsigned long long* d_stats = nullptr)
 {
     size_t stride = al256(hull_scratch_bytes(max_pts));
     char* scratch = pool_take<char>(ctx, stride * (size_t)n_hulls);
     if (!scratch) return ctx_fail(ctx, KERR_HEAP_OOM, "hull scratch does not fit the pool");
     k_hull_batch<<<n_hulls, HULL_NT, 0, s>>>(d_pts, d_off, n_hulls, scratch, stride, max_hv, max_ht,
-                                             d_v, d_t, d_nv, d_nt, d_vol, d_err);
+                                             d_v, d_t, d_nv, d_nt, d_vol, d_err, d_stats);
     ctx->launches++;
     CK(cudaGetLastError());
     return 0;
@@ -139,7 +142,8 @@ static int launch_hull_batch(gpu_ctx* ctx, const float* d_pts, const int* d_off,
 
 static int hull_common(gpu_ctx_t ctx, const float* pts, int total_pts, const int* offsets, int n_hulls,
                        int max_pts, int max_hv, int max_ht, float* out_verts, int* out_tris,
-                       int* out_nv, int* out_nt, float* out_vol, int* out_err)
+                       int* out_nv, int* out_nt, float* out_vol, int* out_err,
+                       unsigned long long* out_stats = nullptr)
 {
     if (!ctx) return -1;
     if (n_hulls <= 0) return 0;
@@ -155,9 +159,10 @@ static int hull_common(gpu_ctx_t ctx, const float* pts, int total_pts, const int
     size_t need = al256(sizeof(float) * 3 * (size_t)total_pts) + al256(sizeof(int) * (size_t)(n_hulls + 1))
                 + al256(sizeof(float) * 3 * (size_t)n_hulls * max_hv) + al256(sizeof(int) * 3 * (size_t)n_hulls * max_ht)
                 + 4 * al256(sizeof(int) * (size_t)n_hulls)
-                + al256(hull_scratch_bytes(max_pts)) * (size_t)n_hulls + 4096;
+                + al256(hull_scratch_bytes(max_pts)) * (size_t)n_hulls + al256(64 * (size_t)n_hulls) + 4096;
     int rc = pool_begin(ctx, need);
     if (rc) return rc;
+    unsigned long long* d_stats = out_stats ? pool_take<unsigned long long>(ctx, 8 * (size_t)n_hulls) : nullptr;
     float* d_pts = pool_take<float>(ctx, 3 * (size_t)total_pts);
     int* d_off = pool_take<int>(ctx, n_hulls + 1);
     float* d_v = pool_take<float>(ctx, 3 * (size_t)n_hulls * max_hv);
@@ -169,8 +174,10 @@ static int hull_common(gpu_ctx_t ctx, const float* pts, int total_pts, const int
     cudaStream_t s = ctx->stream;
     if (total_pts > 0) CK(cudaMemcpyAsync(d_pts, pts, sizeof(float) * 3 * (size_t)total_pts, cudaMemcpyHostToDevice, s));
     CK(cudaMemcpyAsync(d_off, offsets, sizeof(int) * (size_t)(n_hulls + 1), cudaMemcpyHostToDevice, s));
-    rc = launch_hull_batch(ctx, d_pts, d_off, n_hulls, max_pts, max_hv, max_ht, d_v, d_t, d_nv, d_nt, d_vol, d_err, s);
+    rc = launch_hull_batch(ctx, d_pts, d_off, n_hulls, max_pts, max_hv, max_ht, d_v, d_t, d_nv, d_nt, d_vol, d_err, s,
+                           d_stats);
     if (rc) return rc;
+    if (out_stats) CK(cudaMemcpyAsync(out_stats, d_stats, 64 * (size_t)n_hulls, cudaMemcpyDeviceToHost, s));
     if (out_verts) CK(cudaMemcpyAsync(out_verts, d_v, sizeof(float) * 3 * (size_t)n_hulls * max_hv, cudaMemcpyDeviceToHost, s));
     if (out_tris) CK(cudaMemcpyAsync(out_tris, d_t, sizeof(int) * 3 * (size_t)n_hulls * max_ht, cudaMemcpyDeviceToHost, s));
     CK(cudaMemcpyAsync(out_nv, d_nv, sizeof(int) * n_hulls, cudaMemcpyDeviceToHost, s));
@@ -288,3 +295,13 @@ extern "C" int gpu_test_mesh_volume(gpu_ctx_t ctx, const float* verts, int n_ver
 // ---------------------------------------------------------------------------
 // entry points implemented in the remaining translation units
 // ---------------------------------------------------------------------------
+
+extern "C" int cuacd_hull_stats(gpu_ctx_t ctx, const float* pts, int total_pts, const int* offsets, int n_hulls,
+                                int* out_nv, int* out_nt, float* out_vol, unsigned long long* out_stats)
+{
+    if (!ctx) return -1;
+    int max_pts = 0;
+    for (int i = 0; i < n_hulls; i++) max_pts = std::max(max_pts, offsets[i + 1] - offsets[i]);
+    return hull_common(ctx, pts, total_pts, offsets, n_hulls, max_pts, max_pts, 2 * max_pts + 4,
+                       nullptr, nullptr, out_nv, out_nt, out_vol, nullptr, out_stats);
+}

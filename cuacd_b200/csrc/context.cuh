@@ -25,6 +25,9 @@ struct gpu_ctx {
     Arena*         d_arena;
     unsigned long long stats[6];
     unsigned long long launches;
+    int            profile;            // record stage events in the evaluator
+    cudaEvent_t    ev[8];              // stage boundaries of the last evaluation
+    int            n_ev;
     char           last_error[256];
 };
 

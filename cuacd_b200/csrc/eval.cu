@@ -163,21 +163,46 @@ static int sm_count_dev(int dev)
 static void eval_launch(gpu_ctx* ctx, const float* d_v, int nv, const int* d_t, int nt, int n, int flags,
                         float res, int mins, int total, EvalWork& W, cuacd_cand_result* d_out, cudaStream_t s)
 {
+    auto mark = [&](int i) { if (ctx->profile) { cudaEventRecord(ctx->ev[i], s); ctx->n_ev = i + 1; } };
     cudaMemsetAsync(W.i4, 0, 4 * sizeof(int), s);
     launch_arena_reset(ctx->d_arena, ctx->pool + ctx->carve, ctx->cap - ctx->carve, s);
+    mark(0);
     launch_cut_planes(d_v, nv, d_t, nt, W.planes, n, ctx->d_arena, W.cuts, s);
+    mark(1);
     k_frag_hull<<<2 * n, HULL_NT, 0, s>>>(W.cuts, n, ctx->d_arena, W.frags);
+    mark(2);
     ctx->launches += 3;
     const bool hd = flags & CUACD_EVAL_HAUSDORFF;
     if (hd) {
         k_make_surfs<<<(2 * n + 127) / 128, 128, 0, s>>>(W.cuts, W.frags, 2 * n, W.surfs);
-        launch_hausdorff_pairs(W.surfs, 2 * n, ctx->d_arena, res, mins, total, W.preps, W.dirs, W.i4, W.pmax,
-                               W.i4 + 2, sm_count_dev(ctx->device), s);
+        launch_hausdorff_stages(W.surfs, 2 * n, ctx->d_arena, res, mins, total, W.preps, W.dirs, W.i4, W.pmax,
+                                W.i4 + 2, sm_count_dev(ctx->device), s, [&](int k) { mark(3 + k); });
         launch_hd_sqrt(W.pmax, 2 * n, W.hd, 1, s);
         ctx->launches += 5;
-    }
+    } else { mark(3); mark(4); mark(5); }
     k_eval_finish<<<(n + 127) / 128, 128, 0, s>>>(W.cuts, W.frags, W.hd, n, hd ? 1 : 0, W.i4 + 2, d_out);
+    mark(6);
     ctx->launches += 1;
+}
+
+extern "C" int cuacd_profile_stages(gpu_ctx_t ctx, int enable)
+{
+    if (!ctx) return -1;
+    CK(cudaSetDevice(ctx->device));
+    if (enable && !ctx->ev[0])
+        for (int i = 0; i < 8; i++) CK(cudaEventCreate(&ctx->ev[i]));
+    ctx->profile = enable ? 1 : 0;
+    ctx->n_ev = 0;
+    return 0;
+}
+
+extern "C" int cuacd_stage_times(gpu_ctx_t ctx, float* ms_out)
+{
+    if (!ctx || !ms_out) return -1;
+    if (ctx->n_ev < CUACD_N_STAGES + 1) return ctx_fail(ctx, -1, "no profiled evaluation recorded");
+    CK(cudaEventSynchronize(ctx->ev[CUACD_N_STAGES]));
+    for (int i = 0; i < CUACD_N_STAGES; i++) CK(cudaEventElapsedTime(&ms_out[i], ctx->ev[i], ctx->ev[i + 1]));
+    return 0;
 }
 
 extern "C" int cuacd_eval_candidates_device(gpu_ctx_t ctx, const float* d_verts, int nv, const int* d_tris, int nt,

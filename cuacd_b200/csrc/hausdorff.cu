@@ -106,14 +106,24 @@ size_t hd_pairs_scratch_bytes(int n_pairs, int max_nt_a, int max_nt_b)
 // Launch the three Hausdorff stages for n_pairs pairs whose surfaces are in
 // d_surfs[2p] (A) / d_surfs[2p+1] (B).  Work buffers: d_preps[2n], d_dirs[2n],
 // d_i2[2] (total chunks, counter), d_pmax[n].
+void launch_hausdorff_stages(const HDSurf* d_surfs, int n_pairs, Arena* arena, float resolution, int min_samples,
+                             int total, HDPrep* d_preps, void* d_dirs, int* d_i2, float* d_pmax, int* d_err,
+                             int n_sm, cudaStream_t s, const std::function<void(int)>& after)
+{
+    if (n_pairs > 0) k_hd_prep<<<2 * n_pairs, HD_NT, 0, s>>>(d_surfs, 2 * n_pairs, arena, resolution, min_samples, total, d_preps, d_err);
+    after(0);
+    if (n_pairs > 0) k_hd_plan<<<1, 32, 0, s>>>(d_surfs, d_preps, n_pairs, (HDDir*)d_dirs, d_i2, d_i2 + 1, d_pmax);
+    after(1);
+    if (n_pairs > 0) k_hd_query<<<n_sm * 8, HD_NT, 0, s>>>(d_surfs, d_preps, (const HDDir*)d_dirs, 2 * n_pairs, d_i2, d_i2 + 1, d_pmax);
+    after(2);
+}
+
 void launch_hausdorff_pairs(const HDSurf* d_surfs, int n_pairs, Arena* arena, float resolution, int min_samples,
                             int total, HDPrep* d_preps, void* d_dirs, int* d_i2, float* d_pmax, int* d_err,
                             int n_sm, cudaStream_t s)
 {
-    if (n_pairs <= 0) return;
-    k_hd_prep<<<2 * n_pairs, HD_NT, 0, s>>>(d_surfs, 2 * n_pairs, arena, resolution, min_samples, total, d_preps, d_err);
-    k_hd_plan<<<1, 32, 0, s>>>(d_surfs, d_preps, n_pairs, (HDDir*)d_dirs, d_i2, d_i2 + 1, d_pmax);
-    k_hd_query<<<n_sm * 8, HD_NT, 0, s>>>(d_surfs, d_preps, (const HDDir*)d_dirs, 2 * n_pairs, d_i2, d_i2 + 1, d_pmax);
+    launch_hausdorff_stages(d_surfs, n_pairs, arena, resolution, min_samples, total, d_preps, d_dirs, d_i2, d_pmax,
+                            d_err, n_sm, s, [](int) {});
 }
 
 size_t hd_dir_bytes() { return sizeof(HDDir); }

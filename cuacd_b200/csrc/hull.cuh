@@ -25,7 +25,7 @@
 #pragma once
 #include "common.cuh"
 
-#define HULL_NT       256
+#define HULL_NT       512
 #define HULL_LEAF     16
 #define HULL_SMALL_S  24
 #define HULL_MORTON_BITS 4            // bits per axis for the bucket sort
@@ -82,6 +82,8 @@ __host__ __device__ inline size_t hull_scratch_bytes(int n)
     b += hull_align(sizeof(int) * (size_t)(n > 0 ? n : 1));           // S / per-point flags
     b += hull_align(sizeof(int) * (size_t)(n > 0 ? n : 1));           // positions
     b += hull_align(sizeof(int) * (size_t)(n > 0 ? n : 1) * 2);       // owner count/fill
+    b += hull_align(sizeof(float4) * 4 * (size_t)c.P);                // leaf OBBs
+    b += hull_align(sizeof(int) * (HULL_NT / 32) * (2 * (size_t)(n + 2) + 3 * (size_t)c.P)); // per-warp buffers
     return b;
 }
 
@@ -92,8 +94,26 @@ struct HullCtx {
     const float4* __restrict__ pts;     // (qx,qy,qz, input index as int bits)
     const float4* __restrict__ nlo;     // node boxes, heap order [1, 2P)
     const float4* __restrict__ nhi;
+    const float4* __restrict__ obb;     // per leaf: centre (w = 1 if valid), axes e1..e3 with half extents in w
     int m, P, nleaf;
 };
+
+// Bounds of N.(x - a) over a leaf's points from its oriented box:
+// N.(c - a) -+ (sum_i h_i |N.e_i| + margin).  The margin covers the float
+// rounding of the stored centre and axes (|N|_1 * 1e-5 * (sum h + 1)).
+static __device__ __forceinline__ bool leaf_obb(const HullCtx& H, int leaf, double nx, double ny, double nz,
+                                                float4 a, double* lo, double* hi)
+{
+    float4 c = H.obb[4 * leaf];
+    if (c.w == 0.f) return false;
+    float4 e1 = H.obb[4 * leaf + 1], e2 = H.obb[4 * leaf + 2], e3 = H.obb[4 * leaf + 3];
+    double mid = nx * (double)(c.x - a.x) + ny * (double)(c.y - a.y) + nz * (double)(c.z - a.z);
+    double r = fabs(nx * e1.x + ny * e1.y + nz * e1.z) * e1.w + fabs(nx * e2.x + ny * e2.y + nz * e2.z) * e2.w
+             + fabs(nx * e3.x + ny * e3.y + nz * e3.z) * e3.w;
+    r += (fabs(nx) + fabs(ny) + fabs(nz)) * 1e-5 * ((double)e1.w + e2.w + e3.w + 1.0);
+    *lo = mid - r; *hi = mid + r;
+    return true;
+}
 
 static __device__ __forceinline__ int pidx(float4 p) { return __float_as_int(p.w); }
 
@@ -101,13 +121,14 @@ static __device__ __forceinline__ int pidx(float4 p) { return __float_as_int(p.w
 // FP32 with error bound, exact FP64 fallback.
 static __device__ __forceinline__ int plane_sign(double nx, double ny, double nz,
                                           float fx, float fy, float fz,
-                                          float4 a, float4 q)
+                                          float4 a, float4 q, unsigned& n64)
 {
     float ex = q.x - a.x, ey = q.y - a.y, ez = q.z - a.z;     // exact
     float s = fmaf(fz, ez, fmaf(fy, ey, fx * ex));
     float bound = fmaf(fabsf(fz), fabsf(ez), fmaf(fabsf(fy), fabsf(ey), fabsf(fx) * fabsf(ex))) * 4.8e-7f;
     if (s > bound) return 1;
     if (s < -bound) return -1;
+    n64++;
     double d = nx * (double)ex + ny * (double)ey + nz * (double)ez;   // exact
     return (d > 0.0) - (d < 0.0);
 }
@@ -138,7 +159,8 @@ static __device__ __forceinline__ double box_max(double nx, double ny, double nz
 // Wrap: rotate the supporting plane about the line (a, d) into the cloud and
 // return the first point hit (sorted-point id), or -1 when every point lies
 // on the line.  q replaces c when (d x (c - a)).(q - a) < 0.
-static __device__ int hull_wrap(const HullCtx& H, int a_id, int dx, int dy, int dz, int start_leaf)
+static __device__ int hull_wrap(const HullCtx& H, int a_id, int dx, int dy, int dz, int start_leaf,
+                                unsigned& n_pts, unsigned& n64)
 {
     float4 a = H.pts[a_id];
     int c = -1;
@@ -146,9 +168,10 @@ static __device__ int hull_wrap(const HullCtx& H, int a_id, int dx, int dy, int 
     float fx = 0, fy = 0, fz = 0;
     auto consider = [&](int qi) {
         float4 q = H.pts[qi];
+        n_pts++;
         if (on_line(dx, dy, dz, a, q)) return;
         bool take = (c < 0);
-        if (!take) take = plane_sign(mx, my, mz, fx, fy, fz, a, q) < 0;
+        if (!take) take = plane_sign(mx, my, mz, fx, fy, fz, a, q, n64) < 0;
         if (take) {
             c = qi;
             double ex = q.x - a.x, ey = q.y - a.y, ez = q.z - a.z;
@@ -190,7 +213,8 @@ static __device__ int hull_wrap(const HullCtx& H, int a_id, int dx, int dy, int 
 // Collect up to `cap` points on the plane through a with outward normal N
 // (all points satisfy N.(q-a) <= 0).  Returns the count (may exceed cap:
 // the caller then treats the face as large).
-static __device__ int hull_coplanar(const HullCtx& H, int a_id, double nx, double ny, double nz, int* out, int cap)
+static __device__ int hull_coplanar(const HullCtx& H, int a_id, double nx, double ny, double nz, int* out, int cap,
+                                    unsigned& n_pts, unsigned& n64)
 {
     float4 a = H.pts[a_id];
     float fx = (float)nx, fy = (float)ny, fz = (float)nz;
@@ -207,7 +231,8 @@ static __device__ int hull_coplanar(const HullCtx& H, int a_id, double nx, doubl
             int leaf = node - H.P;
             int l0 = leaf * HULL_LEAF, l1 = min(l0 + HULL_LEAF, H.m);
             for (int i = l0; i < l1; i++) {
-                if (plane_sign(nx, ny, nz, fx, fy, fz, a, H.pts[i]) == 0) {
+                n_pts++;
+                if (plane_sign(nx, ny, nz, fx, fy, fz, a, H.pts[i], n64) == 0) {
                     if (cnt < cap) out[cnt] = i;
                     cnt++;
                 }
@@ -217,6 +242,148 @@ static __device__ int hull_coplanar(const HullCtx& H, int a_id, double nx, doubl
             stack[sp++] = 2 * node;
         }
     }
+    return cnt;
+}
+
+// Per-warp scratch of the cooperative wrap.  The node queue and the leaf
+// list live in global scratch sized to the whole tree, so they never overflow.
+struct HullWarp {
+    int* q;                    // BVH node queue (2P), reused as the coplanar leaf list
+    int* leaf;                 // leaves reached by the sweep (P)
+    int S[HULL_SMALL_S + 8];   // coplanar points of the new face
+};
+
+// Is q strictly beyond the plane through a spanned by d and (c - a)?
+static __device__ __forceinline__ bool wrap_better(float4 a, int dx, int dy, int dz, float4 c, float4 q, unsigned& n64)
+{
+    double ex = c.x - a.x, ey = c.y - a.y, ez = c.z - a.z;
+    double mx = dy * ez - dz * ey, my = dz * ex - dx * ez, mz = dx * ey - dy * ex;
+    return plane_sign(mx, my, mz, (float)mx, (float)my, (float)mz, a, q, n64) < 0;
+}
+
+// Warp-wide best candidate (comparator reduction), broadcast from lane 0.
+static __device__ __forceinline__ void warp_best(int& ci, float4& cq, float4 a, int dx, int dy, int dz, unsigned& n64)
+{
+    #pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        int c2 = __shfl_xor_sync(FULL_MASK, ci, o);
+        float4 q2;
+        q2.x = __shfl_xor_sync(FULL_MASK, cq.x, o); q2.y = __shfl_xor_sync(FULL_MASK, cq.y, o);
+        q2.z = __shfl_xor_sync(FULL_MASK, cq.z, o); q2.w = __shfl_xor_sync(FULL_MASK, cq.w, o);
+        if (c2 >= 0 && (ci < 0 || wrap_better(a, dx, dy, dz, cq, q2, n64))) { ci = c2; cq = q2; }
+    }
+    ci = __shfl_sync(FULL_MASK, ci, 0);
+    cq.x = __shfl_sync(FULL_MASK, cq.x, 0); cq.y = __shfl_sync(FULL_MASK, cq.y, 0);
+    cq.z = __shfl_sync(FULL_MASK, cq.z, 0); cq.w = __shfl_sync(FULL_MASK, cq.w, 0);
+}
+
+// Warp-cooperative wrap about edge (u, v): seed the candidate from the
+// leaves holding u and v, sweep the BVH breadth first keeping every box that
+// reaches on or beyond the seed plane (strict pruning, so the kept leaves
+// also hold every point of the final face), then scan the kept leaves'
+// points on 32 lanes and reduce with the exact comparator.
+// Returns c (sorted id), -1 if all points are on the line, -2 if the warp
+// queues overflowed (the caller then uses the serial search).
+static __device__ int warp_wrap(const HullCtx& H, int u, int v, HullWarp& W, int lane, int* nleaf_out,
+                                unsigned& n_pts, unsigned& n64)
+{
+    const unsigned lt = (1u << lane) - 1u;
+    float4 a = H.pts[u], pv = H.pts[v];
+    const int dx = (int)(pv.x - a.x), dy = (int)(pv.y - a.y), dz = (int)(pv.z - a.z);
+    int ci = -1; float4 cq = a;
+    double mx = 0, my = 0, mz = 0; float fx = 0, fy = 0, fz = 0;
+    auto setm = [&]() {
+        double ex = cq.x - a.x, ey = cq.y - a.y, ez = cq.z - a.z;
+        mx = dy * ez - dz * ey; my = dz * ex - dx * ez; mz = dx * ey - dy * ex;
+        fx = (float)mx; fy = (float)my; fz = (float)mz;
+    };
+    auto take = [&](int qi) {
+        float4 q = H.pts[qi];
+        n_pts++;
+        if (on_line(dx, dy, dz, a, q)) return;
+        bool t = ci < 0;
+        if (!t) t = plane_sign(mx, my, mz, fx, fy, fz, a, q, n64) < 0;
+        if (t) { ci = qi; cq = q; setm(); }
+    };
+    {
+        const int lu = u / HULL_LEAF, lv = v / HULL_LEAF;
+        const int leaf = lane < 16 ? lu : lv;
+        const int i = leaf * HULL_LEAF + (lane & 15);
+        if ((lane < 16 || lv != lu) && i < H.m) take(i);
+    }
+    warp_best(ci, cq, a, dx, dy, dz, n64);
+    if (ci >= 0) setm();
+    int qh = 0, qt = 1, nl = 0;
+    if (lane == 0) W.q[0] = 1;
+    __syncwarp();
+    while (qh < qt) {
+        const int batch = min(32, qt - qh);
+        int node = lane < batch ? W.q[qh + lane] : 0;
+        bool kl = false, ki = false;
+        if (lane < batch) {
+            float4 lo = H.nlo[node], hi = H.nhi[node];
+            bool pruned = lo.x > hi.x || (ci >= 0 && box_min(mx, my, mz, lo, hi, a) > 0.0);
+            if (!pruned && ci >= 0 && node >= H.P) {
+                double olo, ohi;
+                if (leaf_obb(H, node - H.P, mx, my, mz, a, &olo, &ohi) && olo > 0.0) pruned = true;
+            }
+            if (!pruned) { if (node >= H.P) kl = true; else ki = true; }
+        }
+        const unsigned bl = __ballot_sync(FULL_MASK, kl), bi = __ballot_sync(FULL_MASK, ki);
+        const int nbl = __popc(bl), nbi = __popc(bi);
+        if (nl + nbl > H.P || qt + 2 * nbi > 2 * H.P) return -2;
+        if (kl) W.leaf[nl + __popc(bl & lt)] = node - H.P;
+        if (ki) { int p = qt + 2 * __popc(bi & lt); W.q[p] = 2 * node; W.q[p + 1] = 2 * node + 1; }
+        __syncwarp();
+        qh += batch; qt += 2 * nbi; nl += nbl;
+    }
+    const int total = nl * HULL_LEAF;
+    for (int i = lane; i < total; i += 32) {
+        int p = W.leaf[i / HULL_LEAF] * HULL_LEAF + (i % HULL_LEAF);
+        if (p < H.m) take(p);
+    }
+    warp_best(ci, cq, a, dx, dy, dz, n64);
+    *nleaf_out = nl;
+    return ci;
+}
+
+// Points of the kept leaves lying on the plane through a with outward normal
+// N (all points satisfy N.(q-a) <= 0).  Leaves whose box stays below the
+// plane are skipped first.  Returns the count; the first `cap` ids go to W.S.
+static __device__ int warp_coplanar(const HullCtx& H, float4 a, double nx, double ny, double nz, HullWarp& W,
+                                    int nl, int lane, int cap, unsigned& n_pts, unsigned& n64)
+{
+    const unsigned lt = (1u << lane) - 1u;
+    const float fx = (float)nx, fy = (float)ny, fz = (float)nz;
+    int nk = 0;
+    for (int base = 0; base < nl; base += 32) {
+        int j = base + lane;
+        bool keep = false;
+        if (j < nl) {
+            int node = W.leaf[j] + H.P;
+            keep = box_max(nx, ny, nz, H.nlo[node], H.nhi[node], a) >= 0.0;
+            double olo, ohi;
+            if (keep && leaf_obb(H, W.leaf[j], nx, ny, nz, a, &olo, &ohi) && ohi < 0.0) keep = false;
+        }
+        unsigned b = __ballot_sync(FULL_MASK, keep);
+        if (keep) W.q[nk + __popc(b & lt)] = W.leaf[j];
+        nk += __popc(b);
+    }
+    __syncwarp();
+    int cnt = 0;
+    const int total = nk * HULL_LEAF;
+    for (int base = 0; base < total; base += 32) {
+        int i = base + lane, p = -1;
+        bool on = false;
+        if (i < total) {
+            p = W.q[i / HULL_LEAF] * HULL_LEAF + (i % HULL_LEAF);
+            if (p < H.m) { n_pts++; on = plane_sign(nx, ny, nz, fx, fy, fz, a, H.pts[p], n64) == 0; }
+        }
+        unsigned b = __ballot_sync(FULL_MASK, on);
+        if (on) { int pos = cnt + __popc(b & lt); if (pos < cap) W.S[pos] = p; }
+        cnt += __popc(b);
+    }
+    __syncwarp();
     return cnt;
 }
 
@@ -282,6 +449,62 @@ static __device__ int hull_small_polygon(const HullCtx& H, const int* S, int ns,
     return -1;
 }
 
+// Large coplanar face (more than HULL_SMALL_S points) built by one warp:
+// collect the face's points from the kept leaves into Sg, then walk the
+// polygon CCW from (v, u) with a warp-wide comparator reduction per corner.
+// Corners go to Pg; returns their count or -1.
+static __device__ int warp_big_polygon(const HullCtx& H, int u, int v, double nx, double ny, double nz,
+                                       const int* leaves, int nl, int* Sg, int* Pg, int lane,
+                                       unsigned& n_pts, unsigned& n64)
+{
+    const unsigned lt = (1u << lane) - 1u;
+    const float4 a = H.pts[u];
+    const float fx = (float)nx, fy = (float)ny, fz = (float)nz;
+    int ns = nl < 0 ? -nl : 0;     // nl < 0: Sg already holds -nl points
+    for (int base = 0; nl > 0 && base < nl * HULL_LEAF; base += 32) {
+        int i = base + lane, p = -1;
+        bool on = false;
+        if (i < nl * HULL_LEAF) {
+            p = leaves[i / HULL_LEAF] * HULL_LEAF + (i % HULL_LEAF);
+            if (p < H.m) { n_pts++; on = plane_sign(nx, ny, nz, fx, fy, fz, a, H.pts[p], n64) == 0; }
+        }
+        unsigned b = __ballot_sync(FULL_MASK, on);
+        if (on) Sg[ns + __popc(b & lt)] = p;
+        ns += __popc(b);
+    }
+    __syncwarp();
+    const Proj PR = make_proj(nx, ny, nz);
+    const float4 pv4 = H.pts[v];
+    if (lane == 0) Pg[0] = v;
+    int k = 1, cur = u;
+    for (int guard = 0; guard <= ns; guard++) {
+        if (lane == 0) Pg[k] = cur;
+        k++;
+        const float4 pc = H.pts[cur];
+        int r = -1; float4 pr = pc;
+        for (int i = lane; i < ns; i += 32) {
+            float4 pt = H.pts[Sg[i]];
+            if (same_pos(pt, pc)) continue;
+            if (r < 0 || next_better(PR, pc, pr, pt)) { r = Sg[i]; pr = pt; }
+        }
+        #pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            int r2 = __shfl_xor_sync(FULL_MASK, r, o);
+            float4 p2;
+            p2.x = __shfl_xor_sync(FULL_MASK, pr.x, o); p2.y = __shfl_xor_sync(FULL_MASK, pr.y, o);
+            p2.z = __shfl_xor_sync(FULL_MASK, pr.z, o); p2.w = __shfl_xor_sync(FULL_MASK, pr.w, o);
+            if (r2 >= 0 && (r < 0 || next_better(PR, pc, pr, p2))) { r = r2; pr = p2; }
+        }
+        r = __shfl_sync(FULL_MASK, r, 0);
+        pr.x = __shfl_sync(FULL_MASK, pr.x, 0); pr.y = __shfl_sync(FULL_MASK, pr.y, 0);
+        pr.z = __shfl_sync(FULL_MASK, pr.z, 0); pr.w = __shfl_sync(FULL_MASK, pr.w, 0);
+        if (r < 0) return -1;
+        if (same_pos(pr, pv4)) { __syncwarp(); return k; }
+        cur = r;
+    }
+    return -1;
+}
+
 // ---------------------------------------------------------------------------
 // hash sets of 64-bit keys (open addressing, empty = ~0)
 // ---------------------------------------------------------------------------
@@ -305,7 +528,7 @@ static __device__ __forceinline__ int hset_insert(unsigned long long* tab, int c
 static __device__ __forceinline__ bool hset_has(const unsigned long long* tab, int cap, unsigned long long k) {
     unsigned s = hslot(k, cap);
     for (int i = 0; i < cap; i++) {
-        unsigned long long x = tab[s];
+        unsigned long long x = __ldcg(&tab[s]);
         if (x == k) return true;
         if (x == ~0ull) return false;
         s = (s + 1) & (unsigned)(cap - 1);
@@ -326,8 +549,11 @@ struct HullShared {
     int red_id[HULL_NT / 32];
     int scan[33];
     double dsh[33];
-    int small_S[HULL_NT][HULL_SMALL_S];
+    HullWarp ws[HULL_NT / 32];
     int cells[HULL_CELLS];
+    unsigned long long stats[8];   // rounds, wraps, small faces, large faces,
+                                   // large-face walk steps, wrap points,
+                                   // coplanar points, FP64 fallbacks
 };
 
 // Build one hull.  All HULL_NT threads call.  `pts` are the input floats
@@ -358,8 +584,10 @@ static __device__ void hull_cta(const float* __restrict__ pts, int n, char* scra
     int4* bigq = (int4*)p;              p += hull_align(sizeof(int4) * (size_t)C.bq_cap);
     int* Sbuf = (int*)p;                p += hull_align(sizeof(int) * (size_t)n);
     int* posn = (int*)p;                p += hull_align(sizeof(int) * (size_t)n);
-    int* ocnt = (int*)p;                                 // [n] owner tri counts, [n] fill
+    int* ocnt = (int*)p;                p += hull_align(sizeof(int) * (size_t)n * 2);  // owner counts, fill
     int* ofill = ocnt + n;
+    float4* obb = (float4*)p;           p += hull_align(sizeof(float4) * 4 * (size_t)C.P);
+    int* wbuf = (int*)p;                                 // per warp: S (n+2) then polygon (n+2)
 
     // ---- 1. bounding box and quantisation parameters
     {
@@ -448,6 +676,65 @@ static __device__ void hull_cta(const float* __restrict__ pts, int n, char* scra
             }
         }
         nlo[C.P + l] = lo; nhi[C.P + l] = hi;
+        // oriented box: e1 towards the farthest point from the first, e2 the
+        // farthest direction off that line, e3 = e1 x e2
+        float4 ob[4] = {make_float4(0.f, 0.f, 0.f, 0.f), make_float4(0.f, 0.f, 0.f, 0.f),
+                        make_float4(0.f, 0.f, 0.f, 0.f), make_float4(0.f, 0.f, 0.f, 0.f)};
+        if (l < C.m_leaves) {
+            int a = l * HULL_LEAF, b = min(a + HULL_LEAF, n);
+            float4 x0 = P4[a];
+            double best = 0; double e1[3] = {0, 0, 0};
+            for (int i = a + 1; i < b; i++) {
+                float4 q = P4[i];
+                double dx = q.x - x0.x, dy = q.y - x0.y, dz = q.z - x0.z, d2 = dx * dx + dy * dy + dz * dz;
+                if (d2 > best) { best = d2; e1[0] = dx; e1[1] = dy; e1[2] = dz; }
+            }
+            if (best > 0) {
+                double inv = 1.0 / sqrt(best);
+                e1[0] *= inv; e1[1] *= inv; e1[2] *= inv;
+                double best2 = 0; double e2[3] = {0, 0, 0};
+                for (int i = a + 1; i < b; i++) {
+                    float4 q = P4[i];
+                    double dx = q.x - x0.x, dy = q.y - x0.y, dz = q.z - x0.z;
+                    double t = dx * e1[0] + dy * e1[1] + dz * e1[2];
+                    double ox = dx - t * e1[0], oy = dy - t * e1[1], oz = dz - t * e1[2], d2 = ox * ox + oy * oy + oz * oz;
+                    if (d2 > best2) { best2 = d2; e2[0] = ox; e2[1] = oy; e2[2] = oz; }
+                }
+                if (best2 > 1e-12) {
+                    double inv2 = 1.0 / sqrt(best2);
+                    e2[0] *= inv2; e2[1] *= inv2; e2[2] *= inv2;
+                    double e3[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2], e1[0] * e2[1] - e1[1] * e2[0]};
+                    float fe[3][3];
+                    for (int k = 0; k < 3; k++) { fe[0][k] = (float)e1[k]; fe[1][k] = (float)e2[k]; fe[2][k] = (float)e3[k]; }
+                    double tmin[3] = {1e300, 1e300, 1e300}, tmax[3] = {-1e300, -1e300, -1e300};
+                    for (int i = a; i < b; i++) {
+                        float4 q = P4[i];
+                        for (int k = 0; k < 3; k++) {
+                            double t = (double)fe[k][0] * (q.x - x0.x) + (double)fe[k][1] * (q.y - x0.y) + (double)fe[k][2] * (q.z - x0.z);
+                            tmin[k] = fmin(tmin[k], t); tmax[k] = fmax(tmax[k], t);
+                        }
+                    }
+                    double cx = x0.x, cy = x0.y, cz = x0.z;
+                    for (int k = 0; k < 3; k++) {
+                        double mid = 0.5 * (tmin[k] + tmax[k]);
+                        cx += mid * fe[k][0]; cy += mid * fe[k][1]; cz += mid * fe[k][2];
+                    }
+                    float4 cf = make_float4((float)cx, (float)cy, (float)cz, 1.f);
+                    // half extents measured from the stored (rounded) centre and axes
+                    double h[3] = {0, 0, 0};
+                    for (int i = a; i < b; i++) {
+                        float4 q = P4[i];
+                        for (int k = 0; k < 3; k++) {
+                            double t = (double)fe[k][0] * (q.x - cf.x) + (double)fe[k][1] * (q.y - cf.y) + (double)fe[k][2] * (q.z - cf.z);
+                            h[k] = fmax(h[k], fabs(t));
+                        }
+                    }
+                    ob[0] = cf;
+                    for (int k = 0; k < 3; k++) ob[k + 1] = make_float4(fe[k][0], fe[k][1], fe[k][2], (float)(h[k] * (1.0 + 1e-6) + 1e-6));
+                }
+            }
+        }
+        for (int k = 0; k < 4; k++) obb[4 * l + k] = ob[k];
     }
     __syncthreads();
     for (int width = C.P >> 1; width >= 1; width >>= 1) {
@@ -463,8 +750,9 @@ static __device__ void hull_cta(const float* __restrict__ pts, int n, char* scra
     for (int i = tid; i < C.eh; i += HULL_NT) eset[i] = ~0ull;
     for (int i = tid; i < C.fh; i += HULL_NT) fset[i] = ~0ull;
     if (tid == 0) { sh.n_faces = 0; sh.n_corners = 0; sh.n_front = 0; sh.n_next = 0; sh.n_big = 0; sh.lexmin = ~0ull; }
+    if (tid < 8) sh.stats[tid] = 0;
     __syncthreads();
-    HullCtx H; H.pts = P4; H.nlo = nlo; H.nhi = nhi; H.m = n; H.P = C.P; H.nleaf = C.m_leaves;
+    HullCtx H; H.pts = P4; H.nlo = nlo; H.nhi = nhi; H.obb = obb; H.m = n; H.P = C.P; H.nleaf = C.m_leaves;
 
     // lexmin (x,y,z,input index) -> first face seed
     {
@@ -505,7 +793,8 @@ static __device__ void hull_cta(const float* __restrict__ pts, int n, char* scra
         float fx = (float)nx, fy = (float)ny, fz = (float)nz;
         for (int base = 0; base < n; base += HULL_NT) {
             int i = base + tid;
-            bool on = i < n && plane_sign(nx, ny, nz, fx, fy, fz, a, P4[i]) == 0;
+            unsigned dummy = 0;
+            bool on = i < n && plane_sign(nx, ny, nz, fx, fy, fz, a, P4[i], dummy) == 0;
             unsigned bal = __ballot_sync(FULL_MASK, on);
             int wbase = 0;
             if ((tid & 31) == 0 && bal) wbase = atomicAdd(&sh.n_S, __popc(bal));
@@ -552,9 +841,11 @@ static __device__ void hull_cta(const float* __restrict__ pts, int n, char* scra
             if (u >= 0) { if (s_cstart < C.ccap) corners[s_cstart] = v; s_k = 1; }
         }
         __syncthreads();
+        if (tid == 0) sh.stats[3]++;
         for (int guard = 0; guard <= ns + 1; guard++) {
             int cur = s_cur;
             if (tid == 0) {
+                sh.stats[4]++;
                 int slot = s_cstart + s_k;
                 if (slot < C.ccap) corners[slot] = cur; else s_face_ok = 0;
                 s_k++;
@@ -611,8 +902,9 @@ static __device__ void hull_cta(const float* __restrict__ pts, int n, char* scra
     };
 
     // ---- 5. first face (cooperative, thread 0 finds the plane)
+    unsigned st_pts = 0, st_cop = 0, st_64 = 0, st_wraps = 0, st_small = 0;
     if (tid == 0) {
-        int c = hull_wrap(H, p0, 0, 0, 1, p0 / HULL_LEAF);
+        int c = hull_wrap(H, p0, 0, 0, 1, p0 / HULL_LEAF, st_pts, st_64);
         double nx = 0, ny = 0, nz = 0;
         int ok = c >= 0;
         if (ok) {
@@ -621,13 +913,13 @@ static __device__ void hull_cta(const float* __restrict__ pts, int n, char* scra
             nx = ey; ny = -ex; nz = 0;                      // (c - p0) x (0,0,1)
             // collinear contact set? then wrap again about (p0, c)
             int tmp[HULL_SMALL_S];
-            int cnt = hull_coplanar(H, p0, nx, ny, nz, tmp, HULL_SMALL_S);
+            int cnt = hull_coplanar(H, p0, nx, ny, nz, tmp, HULL_SMALL_S, st_cop, st_64);
             bool noncol = cnt > HULL_SMALL_S;
             int ix = (int)ex, iy = (int)ey, iz = (int)ez;
             for (int i = 0; i < cnt && i < HULL_SMALL_S && !noncol; i++)
                 if (!on_line(ix, iy, iz, a, P4[tmp[i]])) noncol = true;
             if (!noncol) {
-                int c2 = hull_wrap(H, p0, ix, iy, iz, p0 / HULL_LEAF);
+                int c2 = hull_wrap(H, p0, ix, iy, iz, p0 / HULL_LEAF, st_pts, st_64);
                 if (c2 < 0) ok = 0;
                 else {
                     float4 q2 = P4[c2];
@@ -647,109 +939,150 @@ static __device__ void hull_cta(const float* __restrict__ pts, int n, char* scra
     }
     coop_face(-1, -1, s_N[0], s_N[1], s_N[2], p0);
 
-    // ---- 6. rounds of parallel wrapping
-    int2* cur_front = front0;
-    int2* nxt_front = front1;
-    __shared__ int s_round_f0;
-    if (tid == 0) s_round_f0 = 0;
+    // ---- 6. wrapping: each warp pops a frontier edge (u,v) from a CTA queue,
+    // finds the face across it, and pushes the new face's edges whose twins
+    // are not registered yet.  No CTA-wide rounds; every wait is bounded.
+    unsigned long long* Q = (unsigned long long*)front0;   // 2*fr_cap slots
+    const int qcap = 2 * C.fr_cap;
+    __shared__ int q_head, q_tail, q_pending;
+    for (int i = tid; i < qcap; i += HULL_NT) Q[i] = ~0ull;
     __syncthreads();
-    for (int round = 0; round < 4 * C.fcap + 8; round++) {
-        // register edges of faces created since s_round_f0, build the frontier
-        int f0 = s_round_f0, f1 = sh.n_faces;
-        if (f1 > C.fcap) f1 = C.fcap;
-        for (int f = f0 + tid; f < f1; f += HULL_NT) {
+    if (tid == 0) {
+        q_head = 0; q_tail = 0; q_pending = 0;
+        const int nf0 = min(sh.n_faces, C.fcap);
+        for (int f = 0; f < nf0; f++) {
+            int2 F = faces[f];
+            for (int i = 0; i < F.y; i++)
+                if (hset_insert(eset, C.eh, ekey(corners[F.x + i], corners[F.x + (i + 1) % F.y])) < 0)
+                    sh.err |= KERR_BT_POOL_EXHAUST;
+        }
+        for (int f = 0; f < nf0; f++) {
             int2 F = faces[f];
             for (int i = 0; i < F.y; i++) {
                 int u = corners[F.x + i], v = corners[F.x + (i + 1) % F.y];
-                if (hset_insert(eset, C.eh, ekey(u, v)) < 0) atomicOr(&sh.err, KERR_BT_POOL_EXHAUST);
+                if (!hset_has(eset, C.eh, ekey(v, u)) && q_tail < qcap) { Q[q_tail++] = ekey(u, v); q_pending++; }
             }
         }
-        __syncthreads();
-        if (tid == 0) sh.n_front = 0;
-        __syncthreads();
-        for (int f = f0 + tid; f < f1; f += HULL_NT) {
-            int2 F = faces[f];
-            for (int i = 0; i < F.y; i++) {
-                int u = corners[F.x + i], v = corners[F.x + (i + 1) % F.y];
-                if (!hset_has(eset, C.eh, ekey(v, u))) {
-                    int s = atomicAdd(&sh.n_front, 1);
-                    if (s < C.fr_cap) cur_front[s] = make_int2(u, v);
-                    else atomicOr(&sh.err, KERR_BT_POOL_EXHAUST);
-                }
-            }
-        }
-        __syncthreads();
-        if (tid == 0) { s_round_f0 = f1; sh.n_big = 0; }
-        __syncthreads();
-        int nf = min(sh.n_front, C.fr_cap);
-        if (nf == 0 || sh.err) break;
-        // wrap each frontier edge
-        for (int e = tid; e < nf; e += HULL_NT) {
-            int2 E = cur_front[e];
-            int u = E.x, v = E.y;
-            if (hset_has(eset, C.eh, ekey(v, u))) continue;
-            float4 pu = P4[u], pv = P4[v];
-            int dx = (int)(pv.x - pu.x), dy = (int)(pv.y - pu.y), dz = (int)(pv.z - pu.z);
-            int c = hull_wrap(H, u, dx, dy, dz, u / HULL_LEAF);
-            if (c < 0) { atomicOr(&sh.err, KERR_BT_EXTRACT_FAIL); continue; }
-            float4 pc = P4[c];
-            double ex = pc.x - pu.x, ey = pc.y - pu.y, ez = pc.z - pu.z;
-            // outward normal (c - u) x d
-            double nx = ey * dz - ez * dy, ny = ez * dx - ex * dz, nz = ex * dy - ey * dx;
-            int* S = sh.small_S[tid];
-            int ns = hull_coplanar(H, u, nx, ny, nz, S, HULL_SMALL_S);
-            if (ns > HULL_SMALL_S) {
-                int b = atomicAdd(&sh.n_big, 1);
-                if (b < C.bq_cap) bigq[b] = make_int4(u, v, c, 0);
-                else atomicOr(&sh.err, KERR_BT_POOL_EXHAUST);
-                continue;
-            }
-            int poly[HULL_SMALL_S + 2];
-            int k = (ns == 3) ? 3 : -1;
-            if (ns == 3) { poly[0] = v; poly[1] = u; poly[2] = c; }
-            else k = hull_small_polygon(H, S, ns, nx, ny, nz, v, u, poly);
-            if (k < 3) { atomicOr(&sh.err, KERR_BT_EXTRACT_FAIL); continue; }
-            int mi = 0;
-            for (int i = 1; i < k; i++) if (pidx(P4[poly[i]]) < pidx(P4[poly[mi]])) mi = i;
-            int ins = hset_insert(fset, C.fh, ekey(poly[mi], poly[(mi + 1) % k]));
-            if (ins == 1) {
-                int cs = atomicAdd(&sh.n_corners, k);
-                int f = atomicAdd(&sh.n_faces, 1);
-                if (cs + k <= C.ccap && f < C.fcap) {
-                    for (int i = 0; i < k; i++) corners[cs + i] = poly[i];
-                    faces[f] = make_int2(cs, k);
-                } else atomicOr(&sh.err, KERR_BT_POOL_EXHAUST);
-            } else if (ins < 0) atomicOr(&sh.err, KERR_BT_POOL_EXHAUST);
-        }
-        __syncthreads();
-        // large faces, one at a time, whole CTA
-        int nb = min(sh.n_big, C.bq_cap);
-        for (int b = 0; b < nb; b++) {
-            int4 B = bigq[b];
-            int u = B.x, v = B.y, c = B.z;
-            if (hset_has(eset, C.eh, ekey(v, u))) continue;
-            float4 pu = P4[u], pv = P4[v], pc = P4[c];
-            double dx = pv.x - pu.x, dy = pv.y - pu.y, dz = pv.z - pu.z;
-            double ex = pc.x - pu.x, ey = pc.y - pu.y, ez = pc.z - pu.z;
-            double nx = ey * dz - ez * dy, ny = ez * dx - ex * dz, nz = ex * dy - ey * dx;
-            // skip if a face owning edge (v,u) was already added this round
-            __shared__ int s_dup;
-            if (tid == 0) s_dup = 0;
-            __syncthreads();
-            int fstart = s_round_f0, fend = min(sh.n_faces, C.fcap);
-            for (int f = fstart + tid; f < fend; f += HULL_NT) {
-                int2 F = faces[f];
-                for (int i = 0; i < F.y; i++)
-                    if (corners[F.x + i] == v && corners[F.x + (i + 1) % F.y] == u) s_dup = 1;
-            }
-            __syncthreads();
-            if (s_dup) continue;
-            coop_face(u, v, nx, ny, nz, u);
-        }
-        __syncthreads();
-        int2* t = cur_front; cur_front = nxt_front; nxt_front = t;
     }
     __syncthreads();
+    {
+        const int lane = tid & 31, warp = tid >> 5;
+        HullWarp& W = sh.ws[warp];
+        int* Sg = wbuf + (size_t)warp * (2 * (size_t)(n + 2) + 3 * (size_t)C.P);
+        int* Pg = Sg + (n + 2);
+        if (lane == 0) { W.q = Pg + (n + 2); W.leaf = W.q + 2 * C.P; }
+        __syncwarp();
+        for (;;) {
+            int idx = -1;
+            if (lane == 0) {
+                int spin = 0;
+                for (; spin < (1 << 24); spin++) {
+                    int h = *(volatile int*)&q_head, t = *(volatile int*)&q_tail;
+                    if (h < t) {
+                        if (atomicCAS(&q_head, h, h + 1) == h) { idx = h; break; }
+                        continue;
+                    }
+                    if (*(volatile int*)&q_pending == 0 || *(volatile int*)&sh.err) { idx = -2; break; }
+                    __nanosleep(32);
+                }
+                if (idx == -1) { atomicOr(&sh.err, KERR_TIMEOUT); idx = -2; }
+            }
+            idx = __shfl_sync(FULL_MASK, idx, 0);
+            if (idx == -2) break;
+            unsigned long long key = ~0ull;
+            bool skip = false;
+            if (lane == 0) {
+                for (int spin = 0; spin < (1 << 22); spin++) {
+                    key = atomicAdd(&Q[idx], 0ull);
+                    if (key != ~0ull) break;
+                    __nanosleep(32);
+                }
+                if (key == ~0ull) atomicOr(&sh.err, KERR_TIMEOUT);
+                else skip = hset_has(eset, C.eh, ekey((int)(key & 0xffffffffu), (int)(key >> 32)));
+            }
+            key = __shfl_sync(FULL_MASK, key, 0);
+            skip = __shfl_sync(FULL_MASK, skip, 0);
+            if (key != ~0ull && !skip) {
+                const int u = (int)(key >> 32), v = (int)(key & 0xffffffffu);
+                int nl = 0;
+                int c = warp_wrap(H, u, v, W, lane, &nl, st_pts, st_64);
+                const float4 pu = P4[u], pv = P4[v];
+                const int dx = (int)(pv.x - pu.x), dy = (int)(pv.y - pu.y), dz = (int)(pv.z - pu.z);
+                int ns = 0;
+                double nx = 0, ny = 0, nz = 0;
+                bool serial = (c == -2);
+                if (serial) {
+                    // the warp queues overflowed: serial search on lane 0
+                    int cc = -1;
+                    if (lane == 0) cc = hull_wrap(H, u, dx, dy, dz, u / HULL_LEAF, st_pts, st_64);
+                    c = __shfl_sync(FULL_MASK, cc, 0);
+                }
+                if (c >= 0) {
+                    float4 pc = P4[c];
+                    double ex = pc.x - pu.x, ey = pc.y - pu.y, ez = pc.z - pu.z;
+                    nx = ey * dz - ez * dy; ny = ez * dx - ex * dz; nz = ex * dy - ey * dx;
+                    if (serial) {
+                        int nn = 0;
+                        if (lane == 0) {
+                            nn = hull_coplanar(H, u, nx, ny, nz, Sg, n, st_cop, st_64);
+                            for (int i = 0; i < nn && i < HULL_SMALL_S; i++) W.S[i] = Sg[i];
+                        }
+                        ns = __shfl_sync(FULL_MASK, nn, 0);
+                        __syncwarp();
+                    } else {
+                        ns = warp_coplanar(H, pu, nx, ny, nz, W, nl, lane, HULL_SMALL_S, st_cop, st_64);
+                    }
+                }
+                int k = -1;
+                const int* poly = Pg;
+                if (c >= 0 && ns > HULL_SMALL_S) {
+                    k = warp_big_polygon(H, u, v, nx, ny, nz, W.leaf, serial ? -ns : nl, Sg, Pg, lane, st_cop, st_64);
+                    if (lane == 0) sh.stats[3]++;
+                } else if (c >= 0) {
+                    if (lane == 0) {
+                        if (ns == 3) { Pg[0] = v; Pg[1] = u; Pg[2] = c; k = 3; }
+                        else k = hull_small_polygon(H, W.S, ns, nx, ny, nz, v, u, Pg);
+                    }
+                    k = __shfl_sync(FULL_MASK, k, 0);
+                }
+                __syncwarp();
+                if (lane == 0) {
+                    st_wraps++;
+                    if (c < 0 || k < 3) atomicOr(&sh.err, KERR_BT_EXTRACT_FAIL);
+                    else {
+                        int mi = 0;
+                        for (int i = 1; i < k; i++) if (pidx(P4[poly[i]]) < pidx(P4[poly[mi]])) mi = i;
+                        int ins = hset_insert(fset, C.fh, ekey(poly[mi], poly[(mi + 1) % k]));
+                        if (ins == 1) {
+                            st_small++;
+                            int cs = atomicAdd(&sh.n_corners, k);
+                            int f = atomicAdd(&sh.n_faces, 1);
+                            if (cs + k <= C.ccap && f < C.fcap) {
+                                for (int i = 0; i < k; i++) corners[cs + i] = poly[i];
+                                faces[f] = make_int2(cs, k);
+                                for (int i = 0; i < k; i++)
+                                    if (hset_insert(eset, C.eh, ekey(poly[i], poly[(i + 1) % k])) < 0)
+                                        atomicOr(&sh.err, KERR_BT_POOL_EXHAUST);
+                                for (int i = 0; i < k; i++) {
+                                    int x = poly[i], y = poly[(i + 1) % k];
+                                    if (!hset_has(eset, C.eh, ekey(y, x))) {
+                                        atomicAdd(&q_pending, 1);
+                                        int slot = atomicAdd(&q_tail, 1);
+                                        if (slot < qcap) atomicExch(&Q[slot], ekey(x, y));
+                                        else { atomicOr(&sh.err, KERR_BT_POOL_EXHAUST); atomicSub(&q_pending, 1); }
+                                    }
+                                }
+                            } else atomicOr(&sh.err, KERR_BT_POOL_EXHAUST);
+                        } else if (ins < 0) atomicOr(&sh.err, KERR_BT_POOL_EXHAUST);
+                    }
+                }
+            }
+            __syncwarp();
+            if (lane == 0) atomicSub(&q_pending, 1);
+        }
+    }
+    __syncthreads();
+    if (tid == 0) sh.stats[0] = (unsigned long long)q_tail;
 
     // ---- 7. canonical output
     const int nfaces = min(sh.n_faces, C.fcap);

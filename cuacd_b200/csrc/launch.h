@@ -1,6 +1,7 @@
 // launch.h — host-side launch wrappers shared between translation units.
 #pragma once
 #include <cuda_runtime.h>
+#include <functional>
 #include "common.cuh"
 
 struct CutResult;
@@ -21,4 +22,7 @@ size_t hd_dir_bytes();
 void launch_hausdorff_pairs(const HDSurf* d_surfs, int n_pairs, Arena* arena, float resolution, int min_samples,
                             int total, HDPrep* d_preps, void* d_dirs, int* d_i2, float* d_pmax, int* d_err,
                             int n_sm, cudaStream_t s);
+void launch_hausdorff_stages(const HDSurf* d_surfs, int n_pairs, Arena* arena, float resolution, int min_samples,
+                             int total, HDPrep* d_preps, void* d_dirs, int* d_i2, float* d_pmax, int* d_err,
+                             int n_sm, cudaStream_t s, const std::function<void(int)>& after);
 void launch_hd_sqrt(const float* pmax, int n, float* out, int stride_floats, cudaStream_t s);

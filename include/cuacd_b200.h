@@ -146,6 +146,19 @@ int cuacd_eval_candidates_device(gpu_ctx_t ctx, const float* d_verts, int nv,
                                  int hd_total, cuacd_cand_result* d_out,
                                  void* stream);
 
+/* Candidate planes of one mesh (host pointers): the concave-edge planes of
+ * la_find_concave_edges (cuda/la_concave.cu:48-363; up to 4 per sampled
+ * edge, written first, count in *out_n_concave) followed by the `width`
+ * axis-aligned cuts of la_axis_cut_candidate/la_expand
+ * (cuda/la_axis_cut.cuh:10-19, cuda/la_expand.cu:182-199), 4 floats each.
+ * out_planes holds 4*n_concave_edges + width planes; out_axis_valid[i] = 0
+ * marks an axis too narrow to cut (its plane is all zeros). */
+int cuacd_candidate_planes(gpu_ctx_t ctx, const float* verts, int nv,
+                           const int* tris, int nt, int n_concave_edges,
+                           float concave_eps, float concave_threshold,
+                           int width, float min_edge_dist, float* out_planes,
+                           int* out_n_concave, int* out_axis_valid);
+
 /* Hausdorff with an explicit sample budget (config of a fixed total), host
  * pointers. */
 int cuacd_hausdorff(gpu_ctx_t ctx,
@@ -163,9 +176,26 @@ int cuacd_hull_batch_device(gpu_ctx_t ctx, const float* d_pts,
                             int* d_out_nv, int* d_out_nt, float* d_out_vol,
                             int* d_out_errors, void* stream);
 
+/* Diagnostic: exact hulls of a batch of clouds (host pointers) with the
+ * hull kernel's work counters, 8 per cloud: wrap rounds, wraps, small faces,
+ * large faces, large-face walk steps, points tested by wraps, points tested
+ * for coplanarity, FP64 predicate fallbacks. */
+int cuacd_hull_stats(gpu_ctx_t ctx, const float* pts, int total_pts,
+                     const int* offsets, int n_hulls, int* out_nv, int* out_nt,
+                     float* out_vol, unsigned long long* out_stats);
+
 /* Number of kernel launches issued by this context so far (a counter the
  * benchmark reads around its timed region). */
 unsigned long long cuacd_launch_count(gpu_ctx_t ctx);
+
+/* Per-stage timing of the candidate evaluator: when enabled, CUDA events are
+ * recorded on the evaluator's stream between its launches.  After a call,
+ * cuacd_stage_times fills ms[i] (i < CUACD_N_STAGES, in launch order: cut,
+ * fragment hull+volume, Hausdorff prep, Hausdorff plan, Hausdorff query,
+ * finish) for the last evaluation; it synchronises on the last event. */
+#define CUACD_N_STAGES 6
+int cuacd_profile_stages(gpu_ctx_t ctx, int enable);
+int cuacd_stage_times(gpu_ctx_t ctx, float* ms_out);
 
 /* ---- lookahead search (reference csrc/lookahead.h, csrc/heap.h) ---------- */
 

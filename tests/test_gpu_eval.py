@@ -36,7 +36,7 @@ def test_config3_candidates(ctx, oracle):
     assert len(planes) == 30
     g = ctx.eval_candidates(v, t, planes)
     o = oracle.eval_candidates(v, t, planes, threads=8)
-    assert all(r["err"] == 0 for r in g)
+    assert all(r["err"] == 0 for r in g), [hex(r["err"]) for r in g]
     for a, b in zip(g, o):
         _compare(a, b)
 
@@ -60,3 +60,17 @@ def test_rv_only(ctx, oracle):
     for a, b in zip(g, o):
         _compare(a, b)
         assert a["hausdorff"] == (0.0, 0.0)
+
+
+def test_candidate_planes_bit_exact(ctx, oracle):
+    for v, t in [W.candidate_mesh(), W.candidate_mesh(64, 24)] + W.batch_meshes(4, 500, 5000, seed=5):
+        for K, width in ((16, 3), (32, 30), (4, 5)):
+            conc, axis, valid = ctx.candidate_planes(v, t, K, 0.005, 3.49, width, 0.0125)
+            ref = oracle.concave_planes(v, t, K, 0.005, 3.49)
+            np.testing.assert_array_equal(conc, ref)
+            for i in range(width):
+                a = oracle.axis_plane(v, width, i, 0.0125)
+                if a is None:
+                    assert not valid[i]
+                else:
+                    np.testing.assert_array_equal(axis[i], a)
