@@ -1,5 +1,6 @@
 // hausdorff.cu — Hausdorff kernels and the gpu_test_hausdorff /
 // cuacd_hausdorff entry points.
+#include <mutex>
 #include "context.cuh"
 #include "hausdorff.cuh"
 #include "launch.h"
@@ -194,4 +195,87 @@ extern "C" int gpu_test_hausdorff(gpu_ctx_t ctx, const float* hull_verts, int hu
 {
     return cuacd_hausdorff(ctx, hull_verts, hull_nv, hull_tris, hull_nt, mesh_verts, mesh_nv, mesh_tris, mesh_nt,
                            2000.f, 1000, 0, out_hausdorff);
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free Hausdorff distance.
+//
+// For callers that cannot allocate device memory themselves — code that runs
+// inside a host framework which owns every device allocation, or a plugin
+// loaded where cudaMalloc is forbidden or may block — this entry point uses a
+// fixed block of static device memory instead of the context pool.  The block
+// is a file-scope __device__ array, so every GPU that loads the library holds
+// CUACD_HD_NOALLOC_BYTES of it until the process exits.  All calls share it:
+// its contents persist between calls, the per-call state that must start at
+// zero is cleared by the first kernel of each call, and two calls whose work
+// overlaps on the GPU (different streams, no ordering between them) race on
+// it.  The first call on a device resolves the array's device address; make
+// that first call before any stream capture.
+// ---------------------------------------------------------------------------
+#define CUACD_HD_NOALLOC_BYTES (32ull << 20)
+static __device__ __align__(256) char g_hd_noalloc_scratch[CUACD_HD_NOALLOC_BYTES];
+
+// Layout of the static block: [Arena | 2 HDSurf | 2 HDPrep | 2 HDDir |
+// 4 ints | 2 floats | arena space for the two surfaces' preps].
+static const size_t NOALLOC_HDR = 4096;
+
+__global__ void k_hd_noalloc_setup(char* base, const float* av, int anv, const int* at, int ant,
+                                   const float* bv, int bnv, const int* bt, int bnt)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    Arena* A = (Arena*)base;
+    A->base = base + NOALLOC_HDR;
+    A->capacity = CUACD_HD_NOALLOC_BYTES - NOALLOC_HDR;
+    A->offset = 0;
+    HDSurf* S = (HDSurf*)(base + 256);
+    S[0].v = av; S[0].t = at; S[0].nv = anv; S[0].nt = ant;
+    S[1].v = bv; S[1].t = bt; S[1].nv = bnv; S[1].nt = bnt;
+    int* I = (int*)(base + 1024);
+    I[0] = 0; I[1] = 0; I[2] = 0; I[3] = 0;            // chunks, counter, error word
+    float* M = (float*)(base + 1088);
+    M[0] = 0.f; M[1] = 0.f;
+}
+
+static char* g_noalloc_base[64];
+static std::mutex g_noalloc_mu;
+
+extern "C" int cuacd_hausdorff_noalloc(const float* d_av, int anv, const int* d_at, int ant,
+                                       const float* d_bv, int bnv, const int* d_bt, int bnt,
+                                       float resolution, int min_samples, int total,
+                                       float* d_out, void* stream)
+{
+    if (anv < 0 || ant < 0 || bnv < 0 || bnt < 0 || !d_out) return CUACD_NOALLOC_BAD_ARGS;
+    size_t need = NOALLOC_HDR + hd_prep_bytes(ant) + hd_prep_bytes(bnt) + 8 * 256;
+    if (need > CUACD_HD_NOALLOC_BYTES) return CUACD_NOALLOC_TOO_LARGE;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return (int)e;
+    if (dev < 0 || dev >= 64) return CUACD_NOALLOC_BAD_ARGS;
+    char* base;
+    {
+        std::lock_guard<std::mutex> lock(g_noalloc_mu);
+        if (!g_noalloc_base[dev]) {
+            void* p = nullptr;
+            e = cudaGetSymbolAddress(&p, g_hd_noalloc_scratch);
+            if (e != cudaSuccess) return (int)e;
+            g_noalloc_base[dev] = (char*)p;
+        }
+        base = g_noalloc_base[dev];
+    }
+    if (resolution <= 0.f) resolution = 2000.f;
+    if (min_samples < 0) min_samples = 1000;
+    int n_sm = 148;
+    cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+    cudaStream_t s = (cudaStream_t)stream;
+    k_hd_noalloc_setup<<<1, 32, 0, s>>>(base, d_av, anv, d_at, ant, d_bv, bnv, d_bt, bnt);
+    HDSurf* surfs = (HDSurf*)(base + 256);
+    HDPrep* preps = (HDPrep*)(base + 384);
+    void* dirs = (void*)(base + 768);
+    int* i4 = (int*)(base + 1024);
+    float* pmax = (float*)(base + 1088);
+    launch_hausdorff_pairs(surfs, 1, (Arena*)base, resolution, min_samples, total, preps, dirs, i4, pmax, i4 + 2,
+                           n_sm > 0 ? n_sm : 148, s);
+    launch_hd_sqrt(pmax, 1, d_out, 1, s);
+    e = cudaGetLastError();
+    return e == cudaSuccess ? 0 : (int)e;
 }

@@ -167,6 +167,30 @@ int cuacd_hausdorff(gpu_ctx_t ctx,
                     float resolution, int min_samples, int total,
                     float* out_hausdorff);
 
+/* Allocation-free Hausdorff distance (no counterpart in the reference).
+ * For callers that cannot allocate device memory — plugins inside a host
+ * framework that owns all device allocations, or code where cudaMalloc is
+ * not allowed — and so cannot create a gpu_ctx_t either: no context, no
+ * cudaMalloc/cudaFree, no allocating library call.  Inputs and the output
+ * (one float) are device pointers the caller owns; work is enqueued on
+ * `stream` (cudaStream_t as void*, NULL = legacy default stream) and the call
+ * does not synchronise.  Scratch is a static 32 MiB device array held by
+ * every GPU that loads this library until exit; all calls share it, so calls
+ * whose work overlaps on the GPU race.  The first call on a device looks up
+ * the array's device address; make it before any stream capture.  Returns 0,
+ * CUACD_NOALLOC_TOO_LARGE when the two surfaces' prep data would not fit
+ * (two surfaces of up to 161,000 triangles each fit; the exact test is the
+ * sum of both surfaces' per-triangle prep sizes), CUACD_NOALLOC_BAD_ARGS, or
+ * a CUDA error code. */
+#define CUACD_NOALLOC_TOO_LARGE (-2)
+#define CUACD_NOALLOC_BAD_ARGS  (-3)
+int cuacd_hausdorff_noalloc(const float* d_a_verts, int a_nv,
+                            const int* d_a_tris, int a_nt,
+                            const float* d_b_verts, int b_nv,
+                            const int* d_b_tris, int b_nt,
+                            float resolution, int min_samples, int total,
+                            float* d_out, void* stream);
+
 /* Device-pointer batch hull for callers with resident data (used by the
  * benchmark's device-resident leg).  Does not synchronise. */
 int cuacd_hull_batch_device(gpu_ctx_t ctx, const float* d_pts,
