@@ -87,6 +87,7 @@ _opt("cuacd_hausdorff", _I, [_P, _P, _I, _P, _I, _P, _I, _P, _I, _F, _I, _I, _P]
 _opt("gpu_test_plane_cut", _I, [_P, _P, _I, _P, _I, _F, _F, _F, _F,
                                 _P, _I, _P, _I, _P, _I, _P, _I, _P, _P, _P, _P])
 _opt("gpu_test_warp_sort", _I, [_P, _P, _I, _P, _I])
+_opt("gpu_test_postprocess_dc", _I, [_P, _P, _I, _P, _I, _I, _I, _I, _P, _P, _P, _P, _P])
 _opt("cuacd_eval_candidates", _I, [_P, _P, _I, _P, _I, _P, _I, _I, _F, _I, _I, _P])
 _opt("cuacd_eval_candidates_device", _I, [_P, _P, _I, _P, _I, _P, _I, _I, _F, _I, _I, _P, _P])
 _opt("cuacd_hull_batch_device", _I, [_P, _P, _P, _I, _I, _I, _I, _P, _P, _P, _P, _P, _P, _P])
@@ -293,6 +294,26 @@ class Context:
                                               *[ctypes.byref(x) for x in c]))
         a, b, d, e = [x.value for x in c]
         return pv[:a].copy(), pt[:b].copy(), nv_[:d].copy(), nt_[:e].copy()
+
+    def decompose_components(self, verts, tris, max_comp=4096):
+        """Split a mesh into its vertex-connected components -> list of
+        (verts, tris).  Same entry point as the reference's
+        ``_gpu.test_postprocess_dc`` (tests/test_decompose_components.py:82-112):
+        components in order of their smallest vertex, inner shells dropped
+        when outer shells exist, a connected mesh returned as one component."""
+        v, t = _as_f32(verts).reshape(-1, 3), _as_i32(tris).reshape(-1, 3)
+        nv, nt = len(v), len(t)
+        max_comp = max(1, min(int(max_comp), max(nv, 1)))
+        vcap, tcap = nv + 16, nt + 16
+        ov = np.zeros((max_comp * vcap, 3), np.float32)
+        ot = np.zeros((max_comp * tcap, 3), np.int32)
+        cnv = np.zeros(max_comp, np.int32)
+        cnt = np.zeros(max_comp, np.int32)
+        n = ctypes.c_int(0)
+        self._check(_fn("gpu_test_postprocess_dc")(self._h, _ptr(v), nv, _ptr(t), nt, max_comp, vcap, tcap,
+                                                   _ptr(ov), _ptr(ot), _ptr(cnv), _ptr(cnt), ctypes.byref(n)))
+        return [(ov[c * vcap:c * vcap + cnv[c]].copy(), ot[c * tcap:c * tcap + cnt[c]].copy())
+                for c in range(n.value)]
 
     # -- candidate planes ----------------------------------------------------
     def candidate_planes(self, verts, tris, n_concave_edges=32, concave_eps=0.005, concave_threshold=3.49,

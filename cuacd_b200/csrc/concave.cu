@@ -258,3 +258,38 @@ extern "C" int cuacd_candidate_planes(gpu_ctx_t ctx, const float* verts, int nv,
     *out_n_concave = cnt;
     return 0;
 }
+
+// Concave-edge planes of a device-resident mesh, scratch carved from
+// [scr, scr+cap); the planes (at most 4*K) land in out_host.  Synchronises
+// the stream.  Used by the lookahead search for each cutting part.
+int concave_planes_device(gpu_ctx* ctx, const float* d_v, int nv, const int* d_t, int nt, int K, float eps,
+                          float thr, char* scr, size_t cap, float4* out_host, int* out_count, cudaStream_t s)
+{
+    *out_count = 0;
+    if (K <= 0 || nt < 2) return 0;
+    if (nv >= (1 << 21) || nt >= (1 << 22)) return ctx_fail(ctx, KERR_MESH_INVALID, "mesh too large for edge keys");
+    const int nd = 3 * nt;
+    int N = 1; while (N < nd) N <<= 1;
+    size_t need = al256(8 * (size_t)N) + al256(4 * (size_t)nd) + al256(4 * (size_t)(4 * (K + 1)))
+                + al256(16 * (size_t)(4 * K + 1)) + al256(16);
+    if (need > cap) return ctx_fail(ctx, KERR_HEAP_OOM, "concave planes need %zu scratch bytes, have %zu", need, cap);
+    char* p = scr;
+    unsigned long long* dk = (unsigned long long*)p; p += al256(8 * (size_t)N);
+    int* df = (int*)p; p += al256(4 * (size_t)nd);
+    int* dr = (int*)p; p += al256(4 * (size_t)(4 * (K + 1)));
+    float4* dp = (float4*)p; p += al256(16 * (size_t)(4 * K + 1));
+    int* dc = (int*)p;
+    CK(cudaMemsetAsync(dc, 0, 16, s));
+    ConcaveParams P = concave_params(K, eps, thr);
+    k_concave_planes<<<1, CC_NT, 0, s>>>(d_v, nv, d_t, nt, P, dk, df, dr, dp, dc);
+    ctx->launches += 1;
+    CK(cudaGetLastError());
+    int cnt = 0;
+    CK(cudaMemcpyAsync(&cnt, dc, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (cnt > 4 * K) return ctx_fail(ctx, KERR_MESH_INVALID, "concave plane count %d above %d", cnt, 4 * K);
+    if (cnt > 0) CK(cudaMemcpyAsync(out_host, dp, 16 * (size_t)cnt, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    *out_count = cnt;
+    return 0;
+}

@@ -37,8 +37,12 @@ struct CutResult {
     int n_pos_tris, n_neg_tris;            // before caps
     int n_cap, n_loops, n_boundary, cap_failed, n_cross;
     int err;
-    int _pad[2];
+    int flags;                             // CUT_FLAG_* (set by callers that skip the cut)
+    int _pad;
 };
+
+#define CUT_FLAG_SMALL   1    // the part is too small on every axis to be cut
+#define CUT_FLAG_NOPLANE 2    // no valid plane: nothing was cut
 
 struct CutFixedOut {          // caller-sized outputs; null -> allocate in the arena
     float* pv; int pv_cap; int* pt; int pt_cap;
@@ -294,14 +298,16 @@ static __device__ int cut_build_caps(const float* V, int n_all, const unsigned l
 }
 
 // ---------------------------------------------------------------------------
-// the CTA cut.  All CUT_NT threads call.  Scratch and (if fixed.pv == null)
-// outputs come from the arena.  Writes *res.
+// the CTA cut.  All CUT_NT threads call.  Scratch comes from `arena`; if
+// fixed.pv == null the fragments come from `out_arena` (default: `arena`).
+// Writes *res.
 // ---------------------------------------------------------------------------
 static __device__ void cut_cta(const float* __restrict__ verts, int nv, const int* __restrict__ tris, int nt,
                         float pa, float pb, float pc, float pd, Arena* arena, CutFixedOut fixed,
-                        CutResult* res, CutShared& sh)
+                        CutResult* res, CutShared& sh, Arena* out_arena = nullptr)
 {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    Arena* const oarena = out_arena ? out_arena : arena;
     __shared__ int s_err;
     if (tid == 0) s_err = 0;
     __syncthreads();
@@ -347,8 +353,8 @@ static __device__ void cut_cta(const float* __restrict__ verts, int nv, const in
                 float* ov = to_neg ? fixed.nv : fixed.pv; int* ot = to_neg ? fixed.nt : fixed.pt;
                 int vc = to_neg ? fixed.nv_cap : fixed.pv_cap, tc = to_neg ? fixed.nt_cap : fixed.pt_cap;
                 if (!fixed.pv) {
-                    ov = (float*)arena_alloc(arena, sizeof(float) * 3ull * (nv > 0 ? nv : 1), &s_err);
-                    ot = (int*)arena_alloc(arena, sizeof(int) * 3ull * (nt > 0 ? nt : 1), &s_err);
+                    ov = (float*)arena_alloc(oarena, sizeof(float) * 3ull * (nv > 0 ? nv : 1), &s_err);
+                    ot = (int*)arena_alloc(oarena, sizeof(int) * 3ull * (nt > 0 ? nt : 1), &s_err);
                     vc = nv; tc = nt;
                 }
                 if (!ov || !ot || nv > vc || nt > tc) s_err |= KERR_PC_POOL_OOM;
@@ -403,8 +409,8 @@ static __device__ void cut_cta(const float* __restrict__ verts, int nv, const in
                 float* ov = side ? fixed.nv : fixed.pv; int* ot = side ? fixed.nt : fixed.pt;
                 int vc = side ? fixed.nv_cap : fixed.pv_cap, tc = side ? fixed.nt_cap : fixed.pt_cap;
                 if (!fixed.pv) {
-                    ov = (float*)arena_alloc(arena, sizeof(float) * 3ull * (nvs > 0 ? nvs : 1), &s_err);
-                    ot = (int*)arena_alloc(arena, sizeof(int) * 3ull * (nts > 0 ? nts : 1), &s_err);
+                    ov = (float*)arena_alloc(oarena, sizeof(float) * 3ull * (nvs > 0 ? nvs : 1), &s_err);
+                    ot = (int*)arena_alloc(oarena, sizeof(int) * 3ull * (nts > 0 ? nts : 1), &s_err);
                     vc = nvs; tc = nts;
                 }
                 if (!ov || !ot || nvs > vc || nts > tc) s_err |= KERR_PC_POOL_OOM;
@@ -687,8 +693,8 @@ static __device__ void cut_cta(const float* __restrict__ verts, int nv, const in
                 float* ov = fixed.pv; int* ot = fixed.pt;
                 int vc = fixed.pv_cap, tc = fixed.pt_cap;
                 if (!fixed.pv) {
-                    ov = (float*)arena_alloc(arena, sizeof(float) * 3ull * nv, &s_err);
-                    ot = (int*)arena_alloc(arena, sizeof(int) * 3ull * nt, &s_err);
+                    ov = (float*)arena_alloc(oarena, sizeof(float) * 3ull * nv, &s_err);
+                    ot = (int*)arena_alloc(oarena, sizeof(int) * 3ull * nt, &s_err);
                     vc = nv; tc = nt;
                 }
                 if (!ov || !ot || nv > vc || nt > tc) s_err |= KERR_PC_POOL_OOM;
@@ -743,8 +749,8 @@ static __device__ void cut_cta(const float* __restrict__ verts, int nv, const in
                 float* ov = side ? fixed.nv : fixed.pv; int* ot = side ? fixed.nt : fixed.pt;
                 int vc = side ? fixed.nv_cap : fixed.pv_cap, tc = side ? fixed.nt_cap : fixed.pt_cap;
                 if (!fixed.pv) {
-                    ov = (float*)arena_alloc(arena, sizeof(float) * 3ull * (cnv > 0 ? cnv : 1), &s_err);
-                    ot = (int*)arena_alloc(arena, sizeof(int) * 3ull * (cnt_ > 0 ? cnt_ : 1), &s_err);
+                    ov = (float*)arena_alloc(oarena, sizeof(float) * 3ull * (cnv > 0 ? cnv : 1), &s_err);
+                    ot = (int*)arena_alloc(oarena, sizeof(int) * 3ull * (cnt_ > 0 ? cnt_ : 1), &s_err);
                     vc = cnv; tc = cnt_;
                 }
                 if (!ov || !ot || cnv > vc || cnt_ > tc) s_err |= KERR_PC_POOL_OOM;

@@ -26,3 +26,12 @@ void launch_hausdorff_stages(const HDSurf* d_surfs, int n_pairs, Arena* arena, f
                              int total, HDPrep* d_preps, void* d_dirs, int* d_i2, float* d_pmax, int* d_err,
                              int n_sm, cudaStream_t s, const std::function<void(int)>& after);
 void launch_hd_sqrt(const float* pmax, int n, float* out, int stride_floats, cudaStream_t s);
+
+// components.cu
+struct CompResult;
+void launch_components(const HDSurf* d_meshes, int n, Arena* scratch, Arena* out, CompResult* res, cudaStream_t s);
+
+// concave.cu
+struct gpu_ctx;
+int concave_planes_device(gpu_ctx* ctx, const float* d_v, int nv, const int* d_t, int nt, int K, float eps,
+                          float thr, char* scr, size_t cap, float4* out_host, int* out_count, cudaStream_t s);

@@ -1,0 +1,745 @@
+// lookahead.cu — lookahead_decompose: the tree search that calls the
+// candidate evaluator (reference csrc/lookahead.c:144-1124 and the la_*
+// kernels of cuda/la_expand.cu, la_refine.cu, la_lifecycle.cu, la_concave.cu).
+//
+// One iteration:
+//   0. with decompose_components_per_iter, every part not yet known to be
+//      connected is split into its connected components, each with a fresh
+//      exact hull (la_decompose_components + la_hull_decomp,
+//      csrc/lookahead.c:329-347 and :909-925; components.cuh);
+//   1. Hausdorff of every part whose rv cost is below tau and not yet known
+//      (la_hausdorff_parts, la_refine.cu:19-45);
+//   2. parts sorted by full cost max(rv, H); the up-to-max_n_cutting
+//      costliest parts with cost >= tau are cut this iteration
+//      (la_sort_and_count_cutting, la_lifecycle.cu:90-144);
+//   3. concave-edge planes of each cutting part (la_concave.cu);
+//   4. `depth` expansion levels: level 0 cuts each cutting part with `width`
+//      axis cuts + its edge planes, level d > 0 cuts the worst part of every
+//      surviving item with `width2` axis cuts (la_expand.cu:65-340); every new
+//      fragment gets its volume and exact hull (la_hull, :357-424); the item
+//      records its worst rv cost per level (la_sort_and_record,
+//      la_refine.cu:359-409); a part too small on every axis ends its branch
+//      as a leaf padded with zero costs (la_expand.cu:155-174);
+//   5. per cutting part the initial cut with the lowest mean level cost over
+//      its descendant leaves wins, with the greedy level-0 fallback
+//      (la_evaluate, la_refine.cu:418-527);
+//   6. the part is replaced by the two halves of its winning level-0 item
+//      (la_apply_cuts, la_lifecycle.cu:151-261), whose hulls are already known.
+// Cuts and hulls run as device jobs in waves: fragments go to an output arena
+// kept for the iteration, scratch to a second arena reset between waves.
+// The branch-and-bound pruning of the last level (la_hull's rough-hull bound)
+// only skips provably dominated items and is not needed for the result; the
+// quick levels (quick_depth) and the merge-hulls post-pass are not part of
+// this engine and are ignored.
+#include <vector>
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include "context.cuh"
+#include "cut.cuh"
+#include "hull.cuh"
+#include "hausdorff.cuh"
+#include "components.cuh"
+#include "launch.h"
+
+struct CutJob {
+    const float* v; const int* t; int nv, nt;
+    float4 plane;
+    int axis, slice, cpa, _pad;     // axis >= 0: axis-aligned cut computed on the part's bbox
+};
+
+struct FragRes {                    // per fragment: hull + volumes
+    float* hv; int* ht; int hnv, hnt;
+    double mesh_vol;
+    float hull_vol; int err;
+};
+
+__global__ void __launch_bounds__(CUT_NT)
+k_cut_jobs(const CutJob* __restrict__ jobs, int j0, int j1, Arena* scratch, Arena* out, float min_edge_dist,
+           CutResult* res)
+{
+    __shared__ CutShared sh;
+    __shared__ float s_lo[3], s_hi[3];
+    __shared__ float4 s_plane;
+    __shared__ int s_flags;
+    __shared__ float red[6][CUT_NT / 32];
+    const int j = j0 + blockIdx.x;
+    if (j >= j1) return;
+    const CutJob J = jobs[j];
+    if (threadIdx.x == 0) { s_flags = 0; s_plane = J.plane; }
+    if (J.axis >= 0) {
+        float l[3] = {1e30f, 1e30f, 1e30f}, h[3] = {-1e30f, -1e30f, -1e30f};
+        for (int i = threadIdx.x; i < J.nv; i += CUT_NT)
+            for (int k = 0; k < 3; k++) { float x = J.v[3 * i + k]; l[k] = fminf(l[k], x); h[k] = fmaxf(h[k], x); }
+        for (int k = 0; k < 3; k++) { l[k] = warp_min(l[k]); h[k] = warp_max(h[k]); }
+        if ((threadIdx.x & 31) == 0) for (int k = 0; k < 3; k++) { red[k][threadIdx.x >> 5] = l[k]; red[3 + k][threadIdx.x >> 5] = h[k]; }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            for (int k = 0; k < 3; k++) {
+                float a = 1e30f, b = -1e30f;
+                for (int w = 0; w < CUT_NT / 32; w++) { a = fminf(a, red[k][w]); b = fmaxf(b, red[3 + k][w]); }
+                s_lo[k] = a; s_hi[k] = b;
+            }
+            const float eps = 1e-6f;
+            bool all_small = (s_hi[0] - s_lo[0] <= 2.f * min_edge_dist + eps) &&
+                             (s_hi[1] - s_lo[1] <= 2.f * min_edge_dist + eps) &&
+                             (s_hi[2] - s_lo[2] <= 2.f * min_edge_dist + eps);
+            if (all_small) s_flags = CUT_FLAG_SMALL | CUT_FLAG_NOPLANE;
+            else {
+                float lv = s_lo[J.axis] + min_edge_dist, hv = s_hi[J.axis] - min_edge_dist;
+                if (lv >= hv) s_flags = CUT_FLAG_NOPLANE;
+                else {
+                    float frac = ((float)J.slice + 1.0f) / ((float)J.cpa + 1.0f);
+                    float cut = fmaf(frac, hv - lv, lv);
+                    s_plane = make_float4(J.axis == 0 ? 1.f : 0.f, J.axis == 1 ? 1.f : 0.f, J.axis == 2 ? 1.f : 0.f, -cut);
+                }
+            }
+        }
+    } else if (threadIdx.x == 0 && J.plane.x == 0.f && J.plane.y == 0.f && J.plane.z == 0.f) {
+        s_flags = CUT_FLAG_NOPLANE;
+    }
+    __syncthreads();
+    if (s_flags & CUT_FLAG_NOPLANE) {
+        if (threadIdx.x == 0) { CutResult r; memset(&r, 0, sizeof(r)); r.flags = s_flags; res[j] = r; }
+        return;
+    }
+    CutFixedOut none;
+    memset(&none, 0, sizeof(none));
+    float4 p = s_plane;
+    cut_cta(J.v, J.nv, J.t, J.nt, p.x, p.y, p.z, p.w, scratch, none, &res[j], sh, out);
+}
+
+// Hull + mesh volume of one fragment into *dst (whole CTA).  Hull scratch
+// from `scratch`, hull vertices/triangles from `out`.
+static __device__ void frag_hull_cta(const float* v, int nv, const int* t, int nt, bool empty,
+                                     Arena* scratch, Arena* out, FragRes* dst, HullShared& sh)
+{
+    __shared__ char* s_scr;
+    __shared__ float* s_ov;
+    __shared__ int* s_ot;
+    __shared__ int s_err, s_nv, s_nt;
+    __shared__ float s_vol;
+    if (threadIdx.x == 0) {
+        s_err = 0; s_scr = nullptr; s_ov = nullptr; s_ot = nullptr;
+        if (!empty) {
+            s_scr = (char*)arena_alloc(scratch, hull_scratch_bytes(nv), &s_err);
+            s_ov = (float*)arena_alloc(out, 12ull * nv, &s_err);
+            s_ot = (int*)arena_alloc(out, 12ull * (2 * nv + 4), &s_err);
+        }
+    }
+    __syncthreads();
+    FragRes F;
+    memset(&F, 0, sizeof(F));
+    if (empty || s_err || !s_scr || !s_ov || !s_ot) {
+        if (threadIdx.x == 0) { F.err = s_err; *dst = F; }
+        return;
+    }
+    double mv = block_mesh_signed_volume(v, nv, t, nt, sh.dsh);
+    HullOut o; o.verts = s_ov; o.tris = s_ot; o.vidx = nullptr; o.max_hv = nv; o.max_ht = 2 * nv + 4;
+    hull_cta(v, nv, s_scr, o, &s_nv, &s_nt, &s_vol, &s_err, sh);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        F.hv = s_ov; F.ht = s_ot; F.hnv = s_nv; F.hnt = s_nt;
+        F.mesh_vol = fabs(mv); F.hull_vol = s_vol; F.err = s_err;
+        *dst = F;
+    }
+}
+
+// Hull + volume of fragment f (2 per job), fragments f0..f1 of this wave.
+__global__ void __launch_bounds__(HULL_NT)
+k_hull_jobs(const CutResult* __restrict__ cuts, int f0, int f1, Arena* scratch, Arena* out, FragRes* frags)
+{
+    __shared__ HullShared sh;
+    const int f = f0 + blockIdx.x;
+    if (f >= f1) return;
+    const CutResult& C = cuts[f >> 1];
+    const int side = f & 1;
+    const float* v = side ? C.nv : C.pv;
+    const int* t = side ? C.nt : C.pt;
+    const int nv = side ? C.nnv : C.npv, nt = side ? C.nnt : C.npt;
+    const bool empty = C.err != 0 || nv <= 0 || nt <= 0 || C.npv <= 0 || C.nnv <= 0;
+    frag_hull_cta(v, nv, t, nt, empty, scratch, out, &frags[f], sh);
+}
+
+// Hull + volume of meshes f0..f1 (connected components of split parts).
+__global__ void __launch_bounds__(HULL_NT)
+k_hull_surfs(const HDSurf* __restrict__ meshes, int f0, int f1, Arena* scratch, Arena* out, FragRes* frags)
+{
+    __shared__ HullShared sh;
+    const int f = f0 + blockIdx.x;
+    if (f >= f1) return;
+    const HDSurf m = meshes[f];
+    frag_hull_cta(m.v, m.nv, m.t, m.nt, m.nv <= 0 || m.nt <= 0, scratch, out, &frags[f], sh);
+}
+
+__global__ void k_mesh_volumes(const HDSurf* meshes, int n, double* out)
+{
+    __shared__ double sh[33];
+    int i = blockIdx.x;
+    if (i >= n) return;
+    double v = block_mesh_signed_volume(meshes[i].v, meshes[i].nv, meshes[i].t, meshes[i].nt, sh);
+    if (threadIdx.x == 0) out[i] = fabs(v);
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+namespace {
+
+struct HPart {                 // a part of the decomposition (persistent storage)
+    float* v; int* t; int nv, nt;
+    float* hv; int* ht; int hnv, hnt;
+    double mesh_vol, hull_vol;
+    double hd;                 // < 0: not computed
+    char* block;               // owning allocation (nullptr: caller's input)
+    int cc_id = 0;             // source connected component (0: not assigned)
+    bool checked = false;      // already known to be one connected component
+};
+
+struct LPart {                 // a part inside a search item (arena or persistent)
+    const float* v; const int* t; int nv, nt;
+    double mesh_vol, hull_vol;
+    const float* hv; const int* ht; int hnv, hnt;
+};
+
+struct Item {
+    int src;                   // index into the cutting list
+    int cut0;                  // initial cut index
+    std::vector<LPart> parts;
+    std::vector<float> costs;  // level costs
+    bool leaf_small = false;
+};
+
+float cost_rv(double hull_vol, double mesh_vol)
+{
+    const double pi = 3.14159265358979;
+    double g = hull_vol - mesh_vol; if (g < 0) g = 0;
+    return (float)(0.3 * std::cbrt((3.0 / (4.0 * pi)) * g));
+}
+float cost_rv(const LPart& p) { return cost_rv(p.hull_vol, p.mesh_vol); }
+
+struct Axis { int axis, slice, cpa; };
+Axis axis_candidate(int width, int idx)
+{
+    int count = width / 3, rem = width % 3;
+    int xc = count + (rem > 0), yc = count + (rem > 1);
+    if (idx < xc) return {0, idx, xc};
+    if (idx < xc + yc) return {1, idx - xc, yc};
+    return {2, idx - xc - yc, count};
+}
+
+struct Lookahead {
+    gpu_ctx* ctx;
+    cudaStream_t s;
+    char* out_base; size_t out_cap;       // output arena memory
+    char* scr_base; size_t scr_cap;       // scratch arena memory
+    Arena* d_out; Arena* d_scr;           // device arena structs
+    float min_edge = 0.0125f;
+    // buffers for the components pass
+    HDSurf* d_surfs = nullptr; int surf_cap = 0;
+    CompResult* d_cres = nullptr;
+    FragRes* d_frags = nullptr; int frag_cap = 0;
+
+    void reset_out() { launch_arena_reset(d_out, out_base, out_cap, s); }
+    void reset_scr() { launch_arena_reset(d_scr, scr_base, scr_cap, s); }
+
+    // Run cut jobs then hull jobs; returns 0 or an error (OOM -> KERR_HEAP_OOM).
+    int run_level(const std::vector<CutJob>& jobs, std::vector<CutResult>& cuts, std::vector<FragRes>& frags,
+                  CutJob* d_jobs, CutResult* d_cuts, FragRes* d_fr)
+    {
+        const int n = (int)jobs.size();
+        cuts.assign(n, CutResult());
+        frags.assign(2 * n, FragRes());
+        if (n == 0) return 0;
+        CK(cudaMemcpyAsync(d_jobs, jobs.data(), sizeof(CutJob) * n, cudaMemcpyHostToDevice, s));
+        // cut waves by a scratch estimate
+        int j = 0;
+        while (j < n) {
+            size_t acc = 0; int j1 = j;
+            while (j1 < n) {
+                size_t e = 48 * ((size_t)jobs[j1].nv + 2 * (size_t)jobs[j1].nt) + (256 << 10);
+                if (j1 > j && acc + e > scr_cap) break;
+                acc += e; j1++;
+            }
+            reset_scr();
+            k_cut_jobs<<<j1 - j, CUT_NT, 0, s>>>(d_jobs, j, j1, d_scr, d_out, min_edge, d_cuts);
+            ctx->launches += 2;
+            j = j1;
+        }
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(cuts.data(), d_cuts, sizeof(CutResult) * n, cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        for (auto& c : cuts) if (c.err & (KERR_HEAP_OOM | KERR_PC_SCRATCH_OOM | KERR_PC_POOL_OOM)) return KERR_HEAP_OOM;
+        // hull waves by exact fragment sizes
+        int f = 0;
+        while (f < 2 * n) {
+            size_t acc = 0; int f1 = f;
+            while (f1 < 2 * n) {
+                const CutResult& c = cuts[f1 >> 1];
+                int fv = (f1 & 1) ? c.nnv : c.npv;
+                size_t e = hull_scratch_bytes(fv > 0 ? fv : 1) + 4096;
+                if (f1 > f && acc + e > scr_cap) break;
+                acc += e; f1++;
+            }
+            reset_scr();
+            k_hull_jobs<<<f1 - f, HULL_NT, 0, s>>>(d_cuts, f, f1, d_scr, d_out, d_fr);
+            ctx->launches += 2;
+            f = f1;
+        }
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(frags.data(), d_fr, sizeof(FragRes) * 2 * n, cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        for (auto& r : frags) if (r.err & (KERR_HEAP_OOM | KERR_BT_POOL_EXHAUST)) return KERR_HEAP_OOM;
+        return 0;
+    }
+
+    // A persistent part holding copies of a mesh and its hull.
+    int make_part(HPart& p, const float* v, const int* t, int nv, int nt,
+                  const float* hv, const int* ht, int hnv, int hnt)
+    {
+        size_t b0 = al256(12 * (size_t)nv), b1 = al256(12 * (size_t)nt), b2 = al256(12 * (size_t)hnv);
+        size_t b3 = al256(12 * (size_t)hnt);
+        char* blk = nullptr;
+        CK(cudaMallocAsync((void**)&blk, b0 + b1 + b2 + b3 + 256, s));
+        p.block = blk;
+        p.v = (float*)blk; p.t = (int*)(blk + b0); p.hv = (float*)(blk + b0 + b1); p.ht = (int*)(blk + b0 + b1 + b2);
+        p.nv = nv; p.nt = nt; p.hnv = hnv; p.hnt = hnt;
+        CK(cudaMemcpyAsync(p.v, v, 12 * (size_t)nv, cudaMemcpyDeviceToDevice, s));
+        CK(cudaMemcpyAsync(p.t, t, 12 * (size_t)nt, cudaMemcpyDeviceToDevice, s));
+        if (hnv) CK(cudaMemcpyAsync(p.hv, hv, 12 * (size_t)hnv, cudaMemcpyDeviceToDevice, s));
+        if (hnt) CK(cudaMemcpyAsync(p.ht, ht, 12 * (size_t)hnt, cudaMemcpyDeviceToDevice, s));
+        return 0;
+    }
+    void free_part(HPart& p) { if (p.block) cudaFreeAsync(p.block, s); p.block = nullptr; }
+
+    int split_components(std::vector<HPart>& parts, const std::vector<int>& idx, int& cc_counter);
+};
+
+// Replace every part of `idx` that has several connected components by its
+// components, each with a fresh exact hull and volumes (la_decompose_components
+// + la_hull_decomp, csrc/lookahead.c:329-347 and :909-925).  The first
+// component takes the part's slot, the others are appended
+// (la_lifecycle.cu:384-406); cc ids follow la_lifecycle.cu:363-378.
+int Lookahead::split_components(std::vector<HPart>& parts, const std::vector<int>& idx, int& cc_counter)
+{
+    size_t gi = 0;
+    while (gi < idx.size()) {
+        size_t g1 = gi, oacc = 0, sacc = 0;
+        while (g1 < idx.size() && g1 - gi < (size_t)surf_cap) {
+            const HPart& p = parts[idx[g1]];
+            const size_t nc = (size_t)std::min(p.nv, CC_MAX_COMP);
+            size_t oe = cc_output_bytes(p.nv, p.nt) + 36 * (size_t)p.nv + 600 * nc + 4096;
+            size_t se = cc_scratch_bytes(p.nv) + 4096;
+            if (g1 > gi && (oacc + oe > out_cap || sacc + se > scr_cap)) break;
+            oacc += oe; sacc += se; g1++;
+        }
+        const int m = (int)(g1 - gi);
+        std::vector<HDSurf> sf(m);
+        for (int k = 0; k < m; k++) { const HPart& p = parts[idx[gi + k]]; sf[k] = {p.v, p.t, p.nv, p.nt}; }
+        CK(cudaMemcpyAsync(d_surfs, sf.data(), sizeof(HDSurf) * m, cudaMemcpyHostToDevice, s));
+        reset_out();
+        reset_scr();
+        launch_components(d_surfs, m, d_scr, d_out, d_cres, s);
+        ctx->launches += 3;
+        CK(cudaGetLastError());
+        std::vector<CompResult> cr(m);
+        CK(cudaMemcpyAsync(cr.data(), d_cres, sizeof(CompResult) * m, cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        std::vector<CompMesh> comps;
+        for (int k = 0; k < m; k++) {
+            if (cr[k].err) return ctx_fail(ctx, cr[k].err, "connected components failed (0x%x)", cr[k].err);
+            parts[idx[gi + k]].checked = true;
+            if (cr[k].n <= 0) continue;
+            size_t o = comps.size();
+            comps.resize(o + cr[k].n);
+            CK(cudaMemcpyAsync(comps.data() + o, cr[k].comps, sizeof(CompMesh) * cr[k].n, cudaMemcpyDeviceToHost, s));
+        }
+        CK(cudaStreamSynchronize(s));
+        // exact hull of every component, in chunks and scratch waves
+        std::vector<FragRes> fr(comps.size());
+        const size_t chunk = (size_t)std::min(surf_cap, frag_cap);
+        for (size_t c0 = 0; c0 < comps.size(); c0 += chunk) {
+            const int cn = (int)std::min(chunk, comps.size() - c0);
+            std::vector<HDSurf> hs(cn);
+            for (int k = 0; k < cn; k++) hs[k] = {comps[c0 + k].v, comps[c0 + k].t, comps[c0 + k].nv, comps[c0 + k].nt};
+            CK(cudaMemcpyAsync(d_surfs, hs.data(), sizeof(HDSurf) * cn, cudaMemcpyHostToDevice, s));
+            int f = 0;
+            while (f < cn) {
+                size_t acc = 0; int f1 = f;
+                while (f1 < cn) {
+                    size_t e = hull_scratch_bytes(hs[f1].nv > 0 ? hs[f1].nv : 1) + 4096;
+                    if (f1 > f && acc + e > scr_cap) break;
+                    acc += e; f1++;
+                }
+                reset_scr();
+                k_hull_surfs<<<f1 - f, HULL_NT, 0, s>>>(d_surfs, f, f1, d_scr, d_out, d_frags);
+                ctx->launches += 2;
+                f = f1;
+            }
+            CK(cudaGetLastError());
+            CK(cudaMemcpyAsync(fr.data() + c0, d_frags, sizeof(FragRes) * cn, cudaMemcpyDeviceToHost, s));
+            CK(cudaStreamSynchronize(s));
+        }
+        for (auto& r : fr)
+            if (r.err) return ctx_fail(ctx, r.err, "component hull failed (0x%x)", r.err);
+        size_t c = 0;
+        for (int k = 0; k < m; k++) {
+            if (cr[k].n <= 0) continue;
+            const int slot = idx[gi + k];
+            const int parent_cc = parts[slot].cc_id;
+            const int base_cc = cc_counter;
+            if (parent_cc == 0) cc_counter += cr[k].n;
+            std::vector<HPart> made(cr[k].n);
+            for (int j = 0; j < cr[k].n; j++, c++) {
+                HPart& p = made[j];
+                int rc = make_part(p, comps[c].v, comps[c].t, comps[c].nv, comps[c].nt,
+                                   fr[c].hv, fr[c].ht, fr[c].hnv, fr[c].hnt);
+                if (rc) return rc;
+                p.hull_vol = fr[c].hull_vol;
+                p.mesh_vol = std::min(comps[c].vol, (double)fr[c].hull_vol);   // la_hull_decomp clamp
+                p.hd = -1;
+                p.checked = true;
+                p.cc_id = parent_cc ? parent_cc : base_cc + j + 1;
+            }
+            free_part(parts[slot]);
+            parts[slot] = made[0];
+            for (int j = 1; j < cr[k].n; j++) parts.push_back(made[j]);
+        }
+        CK(cudaStreamSynchronize(s));      // copies out of the output arena are done
+        gi = g1;
+    }
+    return 0;
+}
+
+} // namespace
+
+extern "C" void gpu_result_free(struct gpu_result* r)
+{
+    if (!r) return;
+    for (int i = 0; i < r->nparts; i++) {
+        free(r->parts[i].verts); free(r->parts[i].tris);
+        free(r->parts[i].hull_verts); free(r->parts[i].hull_tris);
+    }
+    free(r->parts);
+    r->parts = nullptr; r->nparts = 0;
+}
+
+extern "C" int lookahead_decompose(gpu_ctx_t ctx, const float* verts, int nv, const int* tris, int nt,
+                                   const float* hull_verts, int hull_nv, const int* hull_tris, int hull_nt,
+                                   int max_iters, int width, int width2, float threshold,
+                                   int depth, int quick_depth, int max_n_cutting,
+                                   int verbose, int debug, int decompose_components,
+                                   int decompose_components_per_iter,
+                                   int n_concave_edges, float concave_eps, float concave_threshold,
+                                   int concave_iters, int merge_hulls, struct gpu_result* out)
+{
+    (void)quick_depth; (void)debug; (void)merge_hulls;
+    if (!ctx || !out) return -1;
+    out->parts = nullptr; out->nparts = 0;
+    if (nv <= 0 || nt <= 0) return ctx_fail(ctx, KERR_MESH_INVALID, "empty mesh");
+    if (width < 1 || width2 < 1 || depth < 1 || depth > 4 || max_n_cutting < 1 || n_concave_edges < 0 || n_concave_edges > 256)
+        return ctx_fail(ctx, KERR_MESH_INVALID, "bad search parameters");
+    for (int i = 0; i < 3 * nt; i++) if (tris[i] < 0 || tris[i] >= nv) return ctx_fail(ctx, KERR_MESH_INVALID, "index out of range");
+    for (int i = 0; i < 3 * hull_nt; i++) if (hull_tris[i] < 0 || hull_tris[i] >= hull_nv) return ctx_fail(ctx, KERR_MESH_INVALID, "hull index out of range");
+    CK(cudaSetDevice(ctx->device));
+    cudaStream_t s = ctx->stream;
+    const int K = n_concave_edges;
+    const int tw_max = width + 4 * K;
+    // ---- pool: fixed buffers + output arena + scratch arena
+    size_t mesh_bytes = 12 * ((size_t)nv + nt);
+    size_t max_jobs = (size_t)max_n_cutting * tw_max;
+    for (int d = 1; d < depth; d++) max_jobs *= width2;
+    size_t fixed = al256(sizeof(CutJob) * max_jobs) + al256(sizeof(CutResult) * max_jobs) + al256(sizeof(FragRes) * 2 * max_jobs)
+                 + al256(2 * sizeof(Arena)) + al256(mesh_bytes) + al256(12 * ((size_t)hull_nv + hull_nt))
+                 + al256(sizeof(HDSurf) * 2 * 4096) + al256(sizeof(HDPrep) * 2 * 4096) + al256(hd_dir_bytes() * 2 * 4096)
+                 + al256(64) + al256(sizeof(float) * 2 * 4096) + al256(sizeof(double) * 4096)
+                 + al256(sizeof(CompResult) * 2 * 4096);
+    size_t out_cap = std::max<size_t>((size_t)1 << 30, 8 * mesh_bytes * std::min<size_t>(max_jobs, 512));
+    size_t scr_cap = std::max<size_t>((size_t)2 << 30, hull_scratch_bytes(nv) * 64);
+    int rc = pool_begin(ctx, fixed + out_cap + scr_cap + (1 << 20));
+    if (rc) return rc;
+    CutJob* d_jobs = pool_take<CutJob>(ctx, max_jobs);
+    CutResult* d_cuts = pool_take<CutResult>(ctx, max_jobs);
+    FragRes* d_frags = pool_take<FragRes>(ctx, 2 * max_jobs);
+    Arena* d_arenas = pool_take<Arena>(ctx, 2);
+    float* d_v0 = pool_take<float>(ctx, 3 * (size_t)nv);
+    int* d_t0 = pool_take<int>(ctx, 3 * (size_t)nt);
+    float* d_hv0 = pool_take<float>(ctx, 3 * (size_t)hull_nv);
+    int* d_ht0 = pool_take<int>(ctx, 3 * (size_t)hull_nt);
+    HDSurf* d_surfs = pool_take<HDSurf>(ctx, 2 * 4096);
+    HDPrep* d_preps = pool_take<HDPrep>(ctx, 2 * 4096);
+    char* d_dirs = pool_take<char>(ctx, hd_dir_bytes() * 2 * 4096);
+    int* d_i4 = pool_take<int>(ctx, 16);
+    float* d_pmax = pool_take<float>(ctx, 2 * 4096);
+    double* d_vols = pool_take<double>(ctx, 4096);
+    CompResult* d_cres = pool_take<CompResult>(ctx, 2 * 4096);
+    char* out_base = pool_take<char>(ctx, out_cap);
+    char* scr_base = pool_take<char>(ctx, scr_cap);
+    if (!scr_base) return ctx_fail(ctx, KERR_HEAP_OOM, "pool carve failed");
+    Lookahead L;
+    L.ctx = ctx; L.s = s; L.out_base = out_base; L.out_cap = out_cap; L.scr_base = scr_base; L.scr_cap = scr_cap;
+    L.d_out = d_arenas; L.d_scr = d_arenas + 1;
+    L.min_edge = std::min(threshold * 0.25f, 0.015f);
+    L.d_surfs = d_surfs; L.surf_cap = 2 * 4096; L.d_cres = d_cres;
+    L.d_frags = d_frags; L.frag_cap = (int)std::min<size_t>(2 * max_jobs, 1 << 30);
+    CK(cudaMemcpyAsync(d_v0, verts, 12 * (size_t)nv, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(d_t0, tris, 12 * (size_t)nt, cudaMemcpyHostToDevice, s));
+    if (hull_nv) CK(cudaMemcpyAsync(d_hv0, hull_verts, 12 * (size_t)hull_nv, cudaMemcpyHostToDevice, s));
+    if (hull_nt) CK(cudaMemcpyAsync(d_ht0, hull_tris, 12 * (size_t)hull_nt, cudaMemcpyHostToDevice, s));
+    // ---- initial part: the mesh and the caller's hull (la_initialize, la_lifecycle.cu:18-81)
+    std::vector<HPart> parts;
+    {
+        HDSurf m[2] = {{d_v0, d_t0, nv, nt}, {d_hv0, d_ht0, hull_nv, hull_nt}};
+        CK(cudaMemcpyAsync(d_surfs, m, sizeof(m), cudaMemcpyHostToDevice, s));
+        k_mesh_volumes<<<2, 256, 0, s>>>(d_surfs, 2, d_vols);
+        ctx->launches++;
+        double vols[2];
+        CK(cudaMemcpyAsync(vols, d_vols, sizeof(vols), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        HPart p;
+        p.v = d_v0; p.t = d_t0; p.nv = nv; p.nt = nt;
+        p.hv = d_hv0; p.ht = d_ht0; p.hnv = hull_nv; p.hnt = hull_nt;
+        p.mesh_vol = vols[0]; p.hull_vol = vols[1]; p.hd = -1; p.block = nullptr;
+        parts.push_back(p);
+    }
+    int result = 0;
+    int cc_counter = 0;
+    auto unchecked = [&]() {
+        std::vector<int> u;
+        for (int i = 0; i < (int)parts.size(); i++) if (!parts[i].checked) u.push_back(i);
+        return u;
+    };
+    std::vector<CutJob> jobs;
+    std::vector<CutResult> cuts;
+    std::vector<FragRes> frs;
+    for (int iter = 0; iter < max_iters && result == 0; iter++) {
+        // ---- 0. split parts made of several connected components
+        //      (dc_pre_eval / dc_post_cuts, csrc/lookahead.c:329-347, :909-925)
+        if (decompose_components_per_iter) {
+            result = L.split_components(parts, unchecked(), cc_counter);
+            if (result) break;
+        }
+        // ---- 1. Hausdorff of parts below tau
+        {
+            std::vector<int> need;
+            for (int i = 0; i < (int)parts.size(); i++)
+                if (parts[i].hd < 0 && parts[i].hnt > 0 && cost_rv(parts[i].hull_vol, parts[i].mesh_vol) < threshold)
+                    need.push_back(i);
+            for (size_t b = 0; b < need.size(); b += 4096) {
+                int m = (int)std::min<size_t>(4096, need.size() - b);
+                std::vector<HDSurf> sf(2 * m);
+                for (int k = 0; k < m; k++) {
+                    const HPart& p = parts[need[b + k]];
+                    sf[2 * k] = {p.hv, p.ht, p.hnv, p.hnt};
+                    sf[2 * k + 1] = {p.v, p.t, p.nv, p.nt};
+                }
+                CK(cudaMemcpyAsync(d_surfs, sf.data(), sizeof(HDSurf) * 2 * m, cudaMemcpyHostToDevice, s));
+                CK(cudaMemsetAsync(d_i4, 0, 16 * sizeof(int), s));
+                L.reset_scr();
+                launch_hausdorff_pairs(d_surfs, m, L.d_scr, 2000.f, 1000, 0, d_preps, d_dirs, d_i4, d_pmax, d_i4 + 2,
+                                       148, s);
+                launch_hd_sqrt(d_pmax, m, d_pmax + 4096, 1, s);
+                ctx->launches += 5;
+                std::vector<float> h(m);
+                int herr = 0;
+                CK(cudaMemcpyAsync(h.data(), d_pmax + 4096, sizeof(float) * m, cudaMemcpyDeviceToHost, s));
+                CK(cudaMemcpyAsync(&herr, d_i4 + 2, sizeof(int), cudaMemcpyDeviceToHost, s));
+                CK(cudaStreamSynchronize(s));
+                if (herr) { result = ctx_fail(ctx, herr, "hausdorff failed at iter %d (0x%x)", iter, herr); break; }
+                for (int k = 0; k < m; k++) parts[need[b + k]].hd = h[k];
+            }
+            if (result) break;
+        }
+        // ---- 2. cutting parts (costliest first, la_sort_and_count_cutting)
+        std::vector<int> order(parts.size());
+        for (size_t i = 0; i < parts.size(); i++) order[i] = (int)i;
+        auto full = [&](int i) {
+            const HPart& p = parts[i];
+            float rv = cost_rv(p.hull_vol, p.mesh_vol);
+            return std::max(rv, p.hd > 0 ? (float)p.hd : 0.f);
+        };
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return full(a) < full(b); });
+        std::vector<int> cutting;
+        int first_above = (int)order.size();
+        for (int i = 0; i < (int)order.size(); i++) if (full(order[i]) >= threshold) { first_above = i; break; }
+        int start = std::max(first_above, (int)order.size() - max_n_cutting);
+        for (int i = start; i < (int)order.size(); i++) if (full(order[i]) >= threshold) cutting.push_back(order[i]);
+        if (verbose) fprintf(stderr, "[la] iter %d: parts=%zu cutting=%zu\n", iter, parts.size(), cutting.size());
+        if (cutting.empty()) break;
+        const int nc = (int)cutting.size();
+        // ---- 3. concave-edge planes per cutting part
+        std::vector<std::vector<float4>> eplanes(nc);
+        if (K > 0 && iter < concave_iters) {
+            for (int c = 0; c < nc; c++) {
+                const HPart& p = parts[cutting[c]];
+                if (p.nt < 2) continue;
+                float4 pl[1024]; int cnt = 0;
+                rc = concave_planes_device(ctx, p.v, p.nv, p.t, p.nt, K, concave_eps, concave_threshold,
+                                           L.scr_base, L.scr_cap, pl, &cnt, s);
+                if (rc) { result = rc; break; }
+                eplanes[c].assign(pl, pl + cnt);
+            }
+            if (result) break;
+        }
+        int n_edge = 0;
+        for (auto& e : eplanes) n_edge = std::max(n_edge, (int)e.size());
+        const int tw0 = width + n_edge;
+        // ---- 4. expansion levels
+        std::vector<Item> cur, leaves, extra;
+        for (int c = 0; c < nc; c++) {
+            Item it; it.src = c; it.cut0 = -1;
+            const HPart& p = parts[cutting[c]];
+            it.parts.push_back({p.v, p.t, p.nv, p.nt, p.mesh_vol, p.hull_vol, p.hv, p.ht, p.hnv, p.hnt});
+            cur.push_back(it);
+        }
+        std::vector<Item> level0;              // level-0 items by (src, cut) for apply
+        std::vector<std::vector<int>> l0index(nc, std::vector<int>(tw0, -1));
+        L.reset_out();
+        for (int d = 0; d < depth && !cur.empty() && result == 0; d++) {
+            const int wd = d == 0 ? width : width2;
+            jobs.clear();
+            std::vector<std::pair<int, int>> job_of;   // (item, cut idx)
+            for (int ii = 0; ii < (int)cur.size(); ii++) {
+                const Item& it = cur[ii];
+                const LPart& w = it.parts.back();      // worst part (parts sorted by rv)
+                int tw = d == 0 ? tw0 : wd;
+                for (int ci = 0; ci < tw; ci++) {
+                    CutJob J;
+                    J.v = w.v; J.t = w.t; J.nv = w.nv; J.nt = w.nt; J._pad = 0;
+                    if (ci < wd) {
+                        Axis a = axis_candidate(wd, ci);
+                        J.axis = a.axis; J.slice = a.slice; J.cpa = a.cpa; J.plane = make_float4(0, 0, 0, 0);
+                    } else {
+                        const auto& ep = eplanes[it.src];
+                        int k = ci - wd;
+                        J.axis = -1; J.slice = 0; J.cpa = 0;
+                        J.plane = k < (int)ep.size() ? ep[k] : make_float4(0, 0, 0, 0);
+                    }
+                    jobs.push_back(J);
+                    job_of.push_back({ii, ci});
+                }
+            }
+            int lr = L.run_level(jobs, cuts, frs, d_jobs, d_cuts, d_frags);
+            if (lr) { result = ctx_fail(ctx, lr, "lookahead level %d failed at iter %d (0x%x)", d, iter, lr); break; }
+            std::vector<Item> next;
+            std::vector<bool> small_done(cur.size(), false);
+            for (size_t j = 0; j < jobs.size(); j++) {
+                const int ii = job_of[j].first, ci = job_of[j].second;
+                const Item& it = cur[ii];
+                const CutResult& c = cuts[j];
+                if (c.flags & CUT_FLAG_SMALL) {
+                    if (!small_done[ii]) {
+                        small_done[ii] = true;
+                        Item x = it;
+                        if (d == 0) x.cut0 = ci;
+                        while ((int)x.costs.size() < depth) x.costs.push_back(0.f);
+                        x.leaf_small = true;
+                        extra.push_back(x);
+                    }
+                    continue;
+                }
+                if (c.flags & CUT_FLAG_NOPLANE) continue;
+                if (c.err || c.npv == 0 || c.nnv == 0) continue;
+                const FragRes& a = frs[2 * j];
+                const FragRes& b = frs[2 * j + 1];
+                if (a.err || b.err) { result = ctx_fail(ctx, a.err | b.err, "fragment hull failed (0x%x)", a.err | b.err); break; }
+                Item x;
+                x.src = it.src; x.cut0 = d == 0 ? ci : it.cut0;
+                x.parts.assign(it.parts.begin(), it.parts.end() - 1);
+                x.parts.push_back({c.pv, c.pt, c.npv, c.npt, a.mesh_vol, (double)a.hull_vol, a.hv, a.ht, a.hnv, a.hnt});
+                x.parts.push_back({c.nv, c.nt, c.nnv, c.nnt, b.mesh_vol, (double)b.hull_vol, b.hv, b.ht, b.hnv, b.hnt});
+                std::stable_sort(x.parts.begin(), x.parts.end(), [](const LPart& p, const LPart& q) { return cost_rv(p) < cost_rv(q); });
+                x.costs = it.costs;
+                x.costs.push_back(cost_rv(x.parts.back()));
+                if (d == 0) { l0index[x.src][ci] = (int)level0.size(); level0.push_back(x); }
+                next.push_back(std::move(x));
+            }
+            if (result) break;
+            cur.swap(next);
+        }
+        if (result) break;
+        for (auto& it : cur) leaves.push_back(it);
+        for (auto& it : extra) leaves.push_back(it);
+        // ---- 5. evaluate (la_evaluate)
+        std::vector<int> best_cut(nc, -1);
+        for (int c = 0; c < nc; c++) {
+            std::vector<float> cb(tw0, 1e30f);
+            for (const Item& it : leaves) {
+                if (it.src != c || it.costs.empty() || it.cut0 < 0 || it.cut0 >= tw0) continue;
+                float pc = 0.f;
+                for (float x : it.costs) pc += x;
+                pc /= (float)it.costs.size();
+                cb[it.cut0] = std::min(cb[it.cut0], pc);
+            }
+            bool any = false;
+            for (float x : cb) if (x < 1e30f) any = true;
+            if (!any)
+                for (int ci = 0; ci < tw0; ci++) {
+                    int li = l0index[c][ci];
+                    if (li >= 0 && !level0[li].costs.empty()) cb[ci] = level0[li].costs[0];
+                }
+            float best = 1e30f; int bi = -1;
+            for (int ci = 0; ci < tw0; ci++) if (cb[ci] < best) { best = cb[ci]; bi = ci; }
+            best_cut[c] = bi;
+        }
+        // ---- 6. apply: the part becomes the two halves of its best level-0 item
+        bool applied = false;
+        std::vector<HPart> added;
+        for (int c = 0; c < nc; c++) {
+            int bi = best_cut[c];
+            if (bi < 0) continue;
+            int li = l0index[c][bi];
+            if (li < 0) continue;                    // winner was a small-part leaf: nothing to cut
+            const Item& x = level0[li];
+            HPart nw[2];
+            for (int k = 0; k < 2; k++) {
+                const LPart& q = x.parts[k];
+                HPart& p = nw[k];
+                rc = L.make_part(p, q.v, q.t, q.nv, q.nt, q.hv, q.ht, q.hnv, q.hnt);
+                if (rc) { result = rc; break; }
+                p.hull_vol = q.hull_vol;
+                p.mesh_vol = std::min(q.mesh_vol, q.hull_vol);   // la_hull_decomp clamp (la_lifecycle.cu:294-297)
+                p.hd = -1;
+                p.cc_id = parts[cutting[c]].cc_id;             // cut pieces inherit (la_expand.cu:253-258)
+            }
+            if (result) break;
+            L.free_part(parts[cutting[c]]);
+            parts[cutting[c]] = nw[0];
+            added.push_back(nw[1]);
+            applied = true;
+        }
+        for (auto& p : added) parts.push_back(p);
+        if (result) break;
+        CK(cudaStreamSynchronize(s));
+        if (!applied) break;
+    }
+    // ---- post-pass components (csrc/lookahead.c:969-985); with the per-iteration
+    //      pass on, only the pieces of the last iteration's cuts are left
+    if (result == 0 && (decompose_components || decompose_components_per_iter))
+        result = L.split_components(parts, unchecked(), cc_counter);
+    // ---- results (host copies)
+    if (result == 0) {
+        out->parts = (gpu_part_result*)calloc(parts.size() > 0 ? parts.size() : 1, sizeof(gpu_part_result));
+        out->nparts = (int)parts.size();
+        for (size_t i = 0; i < parts.size() && result == 0; i++) {
+            const HPart& p = parts[i];
+            gpu_part_result& r = out->parts[i];
+            r.nv = p.nv; r.nt = p.nt; r.hull_nv = p.hnv; r.hull_nt = p.hnt;
+            r.verts = (float*)malloc(12 * (size_t)(p.nv > 0 ? p.nv : 1));
+            r.tris = (int*)malloc(12 * (size_t)(p.nt > 0 ? p.nt : 1));
+            r.hull_verts = (float*)malloc(12 * (size_t)(p.hnv > 0 ? p.hnv : 1));
+            r.hull_tris = (int*)malloc(12 * (size_t)(p.hnt > 0 ? p.hnt : 1));
+            r.mesh_vol = (float)p.mesh_vol; r.hull_vol = (float)p.hull_vol; r.hausdorff = (float)std::max(p.hd, 0.0);
+            cudaError_t e1 = cudaMemcpy(r.verts, p.v, 12 * (size_t)p.nv, cudaMemcpyDeviceToHost);
+            cudaError_t e2 = cudaMemcpy(r.tris, p.t, 12 * (size_t)p.nt, cudaMemcpyDeviceToHost);
+            cudaError_t e3 = p.hnv ? cudaMemcpy(r.hull_verts, p.hv, 12 * (size_t)p.hnv, cudaMemcpyDeviceToHost) : cudaSuccess;
+            cudaError_t e4 = p.hnt ? cudaMemcpy(r.hull_tris, p.ht, 12 * (size_t)p.hnt, cudaMemcpyDeviceToHost) : cudaSuccess;
+            if (e1 || e2 || e3 || e4) result = ctx_fail(ctx, -1, "result copy failed");
+        }
+    }
+    for (auto& p : parts) L.free_part(p);
+    cudaStreamSynchronize(s);
+    if (result) { gpu_result_free(out); return result; }
+    return 0;
+}

@@ -104,6 +104,23 @@ int gpu_test_plane_cut(gpu_ctx_t ctx,
                        int* out_n_pv, int* out_n_pt,
                        int* out_n_nv, int* out_n_nt);
 
+/* Replaces gpu_test_postprocess_dc (csrc/postprocess.h:20-27): split a mesh
+ * into its vertex-connected components.  Component c's vertices go to
+ * out_verts[c*max_verts_per*3 ...] and its triangles (component-local
+ * indices) to out_tris[c*max_tris_per*3 ...]; components are numbered by
+ * their smallest input vertex, vertices and triangles keep input order.
+ * Components with negative signed volume (inner shells) are dropped when
+ * outer shells exist.  A mesh that is one component comes back unchanged
+ * as component 0; an empty mesh gives 0 components.  Buffers too small for
+ * the result: non-zero return, message from gpu_last_error. */
+int gpu_test_postprocess_dc(gpu_ctx_t ctx,
+                            const float* verts, int n_verts,
+                            const int* tris, int n_tris,
+                            int max_components, int max_verts_per, int max_tris_per,
+                            float* out_verts, int* out_tris,
+                            int* out_nv, int* out_nt,
+                            int* out_n_components);
+
 /* Replaces gpu_test_warp_sort (csrc/test.h:19-20): sort each sub-array of
  * (x,y,z,index) int records by (y,x,z,index) in place. */
 int gpu_test_warp_sort(gpu_ctx_t ctx, int* points, int total_pts,

@@ -16,6 +16,7 @@
  *   - concave-edge planes    cuda/la_concave.cu:48-363
  *   - axis candidates        cuda/la_axis_cut.cuh:10-19, cuda/la_expand.cu:182-199
  *   - part costs             cuda/la_common.cuh:21-34
+ *   - connected components   cuda/postprocess.cuh:139-527
  *
  * Output orders are canonical (see each function) so the CUDA path can be
  * compared bit-for-bit on integer results.  Parity pins for this oracle live
@@ -119,6 +120,16 @@ int orc_eval_candidates(const float* verts, int nv, const int* tris, int nt,
                         float hd_resolution, int hd_min_samples,
                         int hd_total_override, int n_threads,
                         orc_cand_result* out);
+
+/* ---------------- connected components ---------------- */
+/* Split into vertex-connected components (postprocess.cuh:139-527).
+ * Components are written back to back: out_v (component vertices, input
+ * order), out_t (component-local indices, input order), comp_nv/comp_nt/
+ * comp_vol per component (|signed volume|, FP64).  Returns the number of
+ * components written; 0 when the mesh is one component (or empty, or has
+ * more than 4096 components); -1 when a capacity is exceeded. */
+int orc_components(const float* v, int nv, const int* t, int nt, int max_comp, int max_out_v, int max_out_t,
+                   float* out_v, int* out_t, int* comp_nv, int* comp_nt, double* comp_vol);
 
 /* Part costs (la_common.cuh:21-34). */
 double orc_cost_rv(double hull_vol, double mesh_vol);

@@ -61,6 +61,7 @@ def lib():
         _lib.orc_concave_planes.argtypes = [P, I, P, I, I, F, F, P]
         _lib.orc_axis_plane.argtypes = [P, I, I, I, F, P]
         _lib.orc_eval_candidates.argtypes = [P, I, P, I, P, I, I, F, I, I, I, P]
+        _lib.orc_components.argtypes = [P, I, P, I, I, I, I, P, P, P, P, P]
         _lib.orc_cost_rv.restype = ctypes.c_double
         _lib.orc_cost_rv.argtypes = [ctypes.c_double, ctypes.c_double]
     return _lib
@@ -173,3 +174,25 @@ def eval_candidates(verts, tris, planes, hausdorff=True, resolution=2000.0,
             "cost_full": tuple(r.cost_full), "score_rv": r.score_rv,
             "score_full": r.score_full})
     return res
+
+
+def components(verts, tris, max_comp=4096):
+    """Connected components: list of (verts, tris, |volume|) in canonical
+    order, or [] when the mesh is one component."""
+    v, t = _f32(verts), _i32(tris)
+    ov = np.empty((max(len(v), 1), 3), np.float32)
+    ot = np.empty((max(len(t), 1), 3), np.int32)
+    cnv = np.zeros(max_comp, np.int32)
+    cnt = np.zeros(max_comp, np.int32)
+    cvol = np.zeros(max_comp, np.float64)
+    n = lib().orc_components(v.ctypes.data, len(v), t.ctypes.data, len(t), max_comp, len(ov), len(ot),
+                             ov.ctypes.data, ot.ctypes.data, cnv.ctypes.data, cnt.ctypes.data,
+                             cvol.ctypes.data)
+    if n < 0:
+        raise RuntimeError("oracle components capacity overflow")
+    out, vo, to = [], 0, 0
+    for c in range(n):
+        out.append((ov[vo:vo + cnv[c]].copy(), ot[to:to + cnt[c]].copy(), float(cvol[c])))
+        vo += cnv[c]
+        to += cnt[c]
+    return out
