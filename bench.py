@@ -48,6 +48,20 @@ def peaks():
         return 6650.0, "fallback"
 
 
+def ncu_traffic(kernel):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary
+    (profiles/roofline_traffic.txt), or None."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "roofline_traffic.txt")) as f:
+            for line in f:
+                parts = line.split()
+                if len(parts) >= 2 and parts[0] == kernel:
+                    return int(parts[1])
+    except OSError:
+        pass
+    return None
+
+
 def workload():
     from cuacd_b200 import workloads as W
     v, t = W.candidate_mesh()
@@ -313,7 +327,7 @@ def main():
     peak, peak_kind = peaks()
     achieved = alg[names[dom]] / (stage_ms[dom] / 1000.0) / 1e9
     roof = {"bound": "hbm", "kernel": names[dom], "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
+            "frac": achieved / peak, "peak_source": peak_kind, "traffic": ncu_traffic(names[dom]),
             "algorithmic_bytes": int(alg[names[dom]]),
             "stage_ms": {k: round(x, 4) for k, x in zip(names, stage_ms)}}
 

@@ -551,9 +551,8 @@ struct HullShared {
     double dsh[33];
     HullWarp ws[HULL_NT / 32];
     int cells[HULL_CELLS];
-    unsigned long long stats[8];   // rounds, wraps, small faces, large faces,
-                                   // large-face walk steps, wrap points,
-                                   // coplanar points, FP64 fallbacks
+    unsigned long long stats[8];   // queued edges, wraps, faces, large faces,
+                                   // setup / wrap / output cycles, corners
 };
 
 // Build one hull.  All HULL_NT threads call.  `pts` are the input floats
@@ -565,6 +564,7 @@ static __device__ void hull_cta(const float* __restrict__ pts, int n, char* scra
                          HullShared& sh)
 {
     const int tid = threadIdx.x;
+    const long long t_begin = clock64();
     if (tid == 0) { sh.err = 0; }
     if (n < 4) {
         if (tid == 0) { *o_nv = 0; *o_nt = 0; if (o_vol) *o_vol = 0.f; }
@@ -845,7 +845,6 @@ static __device__ void hull_cta(const float* __restrict__ pts, int n, char* scra
         for (int guard = 0; guard <= ns + 1; guard++) {
             int cur = s_cur;
             if (tid == 0) {
-                sh.stats[4]++;
                 int slot = s_cstart + s_k;
                 if (slot < C.ccap) corners[slot] = cur; else s_face_ok = 0;
                 s_k++;
@@ -942,6 +941,7 @@ static __device__ void hull_cta(const float* __restrict__ pts, int n, char* scra
     // ---- 6. wrapping: each warp pops a frontier edge (u,v) from a CTA queue,
     // finds the face across it, and pushes the new face's edges whose twins
     // are not registered yet.  No CTA-wide rounds; every wait is bounded.
+    const long long t_wrap = clock64();
     unsigned long long* Q = (unsigned long long*)front0;   // 2*fr_cap slots
     const int qcap = 2 * C.fr_cap;
     __shared__ int q_head, q_tail, q_pending;
@@ -1037,7 +1037,7 @@ static __device__ void hull_cta(const float* __restrict__ pts, int n, char* scra
                 const int* poly = Pg;
                 if (c >= 0 && ns > HULL_SMALL_S) {
                     k = warp_big_polygon(H, u, v, nx, ny, nz, W.leaf, serial ? -ns : nl, Sg, Pg, lane, st_cop, st_64);
-                    if (lane == 0) sh.stats[3]++;
+                    if (lane == 0) atomicAdd(&sh.stats[3], 1ull);
                 } else if (c >= 0) {
                     if (lane == 0) {
                         if (ns == 3) { Pg[0] = v; Pg[1] = u; Pg[2] = c; k = 3; }
@@ -1081,8 +1081,15 @@ static __device__ void hull_cta(const float* __restrict__ pts, int n, char* scra
             if (lane == 0) atomicSub(&q_pending, 1);
         }
     }
+    if ((tid & 31) == 0) atomicAdd(&sh.stats[1], (unsigned long long)st_wraps);
     __syncthreads();
-    if (tid == 0) sh.stats[0] = (unsigned long long)q_tail;
+    const long long t_out = clock64();
+    if (tid == 0) {
+        sh.stats[0] = (unsigned long long)q_tail;
+        sh.stats[2] = (unsigned long long)sh.n_faces;
+        sh.stats[4] = (unsigned long long)(t_wrap - t_begin);
+        sh.stats[5] = (unsigned long long)(t_out - t_wrap);
+    }
 
     // ---- 7. canonical output
     const int nfaces = min(sh.n_faces, C.fcap);
@@ -1168,7 +1175,11 @@ static __device__ void hull_cta(const float* __restrict__ pts, int n, char* scra
         }
         __syncthreads();
         double vol = block_mesh_signed_volume(out.verts, nv_out, out.tris, nt_out, sh.dsh);
-        if (tid == 0) { *o_nv = nv_out; *o_nt = nt_out; if (o_vol) *o_vol = (float)fabs(vol); }
+        if (tid == 0) {
+            *o_nv = nv_out; *o_nt = nt_out; if (o_vol) *o_vol = (float)fabs(vol);
+            sh.stats[6] = (unsigned long long)(clock64() - t_out);
+            sh.stats[7] = (unsigned long long)nv_out;
+        }
     } else {
         if (tid == 0) {
             *o_nv = 0; *o_nt = 0; if (o_vol) *o_vol = 0.f;
