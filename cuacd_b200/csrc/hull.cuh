@@ -30,6 +30,9 @@
 #define HULL_SMALL_S  24
 #define HULL_MORTON_BITS 4            // bits per axis for the bucket sort
 #define HULL_CELLS    (1 << (3 * HULL_MORTON_BITS))
+#define HULL_WSM      (HULL_CELLS / (HULL_NT / 32))   // shared ints per warp while wrapping
+#define HULL_WQ       160                          // of which: node stack
+#define HULL_WL       (HULL_WSM - HULL_WQ)         //           kept-leaf list
 
 struct HullOut {
     float* verts;     // hull corner coordinates (input floats), cap max_hv
@@ -248,9 +251,15 @@ static __device__ int hull_coplanar(const HullCtx& H, int a_id, double nx, doubl
 // Per-warp scratch of the cooperative wrap.  The node queue and the leaf
 // list live in global scratch sized to the whole tree, so they never overflow.
 struct HullWarp {
-    int* q;                    // BVH node queue (2P), reused as the coplanar leaf list
-    int* leaf;                 // leaves reached by the sweep (P)
     int S[HULL_SMALL_S + 8];   // coplanar points of the new face
+};
+
+// A warp's work lists (same value on every lane): the BVH node stack, reused
+// as the coplanar leaf list, and the leaves reached by the sweep, with their
+// capacities (shared memory first, the global 2P / P lists when too small).
+struct WarpLists {
+    int* q; int* leaf;
+    int qcap, lcap;
 };
 
 // Is q strictly beyond the plane through a spanned by d and (c - a)?
@@ -278,13 +287,14 @@ static __device__ __forceinline__ void warp_best(int& ci, float4& cq, float4 a, 
 }
 
 // Warp-cooperative wrap about edge (u, v): seed the candidate from the
-// leaves holding u and v, sweep the BVH breadth first keeping every box that
-// reaches on or beyond the seed plane (strict pruning, so the kept leaves
-// also hold every point of the final face), then scan the kept leaves'
-// points on 32 lanes and reduce with the exact comparator.
+// leaves holding u and v, then sweep the BVH depth first keeping every box
+// that reaches on or beyond the current plane (strict pruning, so the kept
+// leaves also hold every point of the final face), scanning kept leaves'
+// points on 32 lanes as they are reached and reducing with the exact
+// comparator.
 // Returns c (sorted id), -1 if all points are on the line, -2 if the warp
 // queues overflowed (the caller then uses the serial search).
-static __device__ int warp_wrap(const HullCtx& H, int u, int v, HullWarp& W, int lane, int* nleaf_out,
+static __device__ int warp_wrap(const HullCtx& H, int u, int v, const WarpLists W, int lane, int* nleaf_out,
                                 unsigned& n_pts, unsigned& n64)
 {
     const unsigned lt = (1u << lane) - 1u;
@@ -313,12 +323,20 @@ static __device__ int warp_wrap(const HullCtx& H, int u, int v, HullWarp& W, int
     }
     warp_best(ci, cq, a, dx, dy, dz, n64);
     if (ci >= 0) setm();
-    int qh = 0, qt = 1, nl = 0;
+    // Depth-first sweep, 32 nodes per step from the top of a warp stack.
+    // Each step's newly kept leaves are scanned at once, so the plane
+    // tightens while the sweep is still near the seed and later boxes are
+    // pruned against it.  Every leaf not pruned when reached is recorded:
+    // a point on the final plane is never strictly below an earlier (less
+    // rotated) plane, so the list holds the final face's points.
+    int sp = 1, nl = 0, scanned = 0;
     if (lane == 0) W.q[0] = 1;
     __syncwarp();
-    while (qh < qt) {
-        const int batch = min(32, qt - qh);
-        int node = lane < batch ? W.q[qh + lane] : 0;
+    while (sp > 0) {
+        const int batch = min(32, sp);
+        const int base = sp - batch;
+        const int node = lane < batch ? W.q[base + lane] : 0;
+        __syncwarp();                                   // all pops read before pushes overwrite
         bool kl = false, ki = false;
         if (lane < batch) {
             float4 lo = H.nlo[node], hi = H.nhi[node];
@@ -331,18 +349,22 @@ static __device__ int warp_wrap(const HullCtx& H, int u, int v, HullWarp& W, int
         }
         const unsigned bl = __ballot_sync(FULL_MASK, kl), bi = __ballot_sync(FULL_MASK, ki);
         const int nbl = __popc(bl), nbi = __popc(bi);
-        if (nl + nbl > H.P || qt + 2 * nbi > 2 * H.P) return -2;
+        if (nl + nbl > W.lcap || base + 2 * nbi > W.qcap) return -2;
         if (kl) W.leaf[nl + __popc(bl & lt)] = node - H.P;
-        if (ki) { int p = qt + 2 * __popc(bi & lt); W.q[p] = 2 * node; W.q[p + 1] = 2 * node + 1; }
+        if (ki) { int p = base + 2 * __popc(bi & lt); W.q[p] = 2 * node; W.q[p + 1] = 2 * node + 1; }
         __syncwarp();
-        qh += batch; qt += 2 * nbi; nl += nbl;
+        sp = base + 2 * nbi; nl += nbl;
+        if (nl > scanned) {                             // scan the new leaves, tighten the plane
+            const int total = (nl - scanned) * HULL_LEAF;
+            for (int i = lane; i < total; i += 32) {
+                int p = W.leaf[scanned + i / HULL_LEAF] * HULL_LEAF + (i % HULL_LEAF);
+                if (p < H.m) take(p);
+            }
+            warp_best(ci, cq, a, dx, dy, dz, n64);
+            if (ci >= 0) setm();
+            scanned = nl;
+        }
     }
-    const int total = nl * HULL_LEAF;
-    for (int i = lane; i < total; i += 32) {
-        int p = W.leaf[i / HULL_LEAF] * HULL_LEAF + (i % HULL_LEAF);
-        if (p < H.m) take(p);
-    }
-    warp_best(ci, cq, a, dx, dy, dz, n64);
     *nleaf_out = nl;
     return ci;
 }
@@ -351,7 +373,7 @@ static __device__ int warp_wrap(const HullCtx& H, int u, int v, HullWarp& W, int
 // N (all points satisfy N.(q-a) <= 0).  Leaves whose box stays below the
 // plane are skipped first.  Returns the count; the first `cap` ids go to W.S.
 static __device__ int warp_coplanar(const HullCtx& H, float4 a, double nx, double ny, double nz, HullWarp& W,
-                                    int nl, int lane, int cap, unsigned& n_pts, unsigned& n64)
+                                    const WarpLists L, int nl, int lane, int cap, unsigned& n_pts, unsigned& n64)
 {
     const unsigned lt = (1u << lane) - 1u;
     const float fx = (float)nx, fy = (float)ny, fz = (float)nz;
@@ -360,13 +382,13 @@ static __device__ int warp_coplanar(const HullCtx& H, float4 a, double nx, doubl
         int j = base + lane;
         bool keep = false;
         if (j < nl) {
-            int node = W.leaf[j] + H.P;
+            int node = L.leaf[j] + H.P;
             keep = box_max(nx, ny, nz, H.nlo[node], H.nhi[node], a) >= 0.0;
             double olo, ohi;
-            if (keep && leaf_obb(H, W.leaf[j], nx, ny, nz, a, &olo, &ohi) && ohi < 0.0) keep = false;
+            if (keep && leaf_obb(H, L.leaf[j], nx, ny, nz, a, &olo, &ohi) && ohi < 0.0) keep = false;
         }
         unsigned b = __ballot_sync(FULL_MASK, keep);
-        if (keep) W.q[nk + __popc(b & lt)] = W.leaf[j];
+        if (keep) L.q[nk + __popc(b & lt)] = L.leaf[j];
         nk += __popc(b);
     }
     __syncwarp();
@@ -376,7 +398,7 @@ static __device__ int warp_coplanar(const HullCtx& H, float4 a, double nx, doubl
         int i = base + lane, p = -1;
         bool on = false;
         if (i < total) {
-            p = W.q[i / HULL_LEAF] * HULL_LEAF + (i % HULL_LEAF);
+            p = L.q[i / HULL_LEAF] * HULL_LEAF + (i % HULL_LEAF);
             if (p < H.m) { n_pts++; on = plane_sign(nx, ny, nz, fx, fy, fz, a, H.pts[p], n64) == 0; }
         }
         unsigned b = __ballot_sync(FULL_MASK, on);
@@ -550,9 +572,11 @@ struct HullShared {
     int scan[33];
     double dsh[33];
     HullWarp ws[HULL_NT / 32];
-    int cells[HULL_CELLS];
-    unsigned long long stats[8];   // queued edges, wraps, faces, large faces,
-                                   // setup / wrap / output cycles, corners
+    int cells[HULL_CELLS];           // bucket sort
+    int wsm[HULL_NT / 32][HULL_WSM]; // per-warp node stack + leaf list
+    unsigned long long stats[8];   // leaves kept by wraps, wraps, faces, points
+                                   // tested by wraps, setup / wrap / output
+                                   // cycles, large faces
 };
 
 // Build one hull.  All HULL_NT threads call.  `pts` are the input floats
@@ -901,7 +925,7 @@ static __device__ void hull_cta(const float* __restrict__ pts, int n, char* scra
     };
 
     // ---- 5. first face (cooperative, thread 0 finds the plane)
-    unsigned st_pts = 0, st_cop = 0, st_64 = 0, st_wraps = 0, st_small = 0;
+    unsigned st_pts = 0, st_cop = 0, st_64 = 0, st_wraps = 0, st_small = 0, st_leaves = 0;
     if (tid == 0) {
         int c = hull_wrap(H, p0, 0, 0, 1, p0 / HULL_LEAF, st_pts, st_64);
         double nx = 0, ny = 0, nz = 0;
@@ -970,7 +994,10 @@ static __device__ void hull_cta(const float* __restrict__ pts, int n, char* scra
         HullWarp& W = sh.ws[warp];
         int* Sg = wbuf + (size_t)warp * (2 * (size_t)(n + 2) + 3 * (size_t)C.P);
         int* Pg = Sg + (n + 2);
-        if (lane == 0) { W.q = Pg + (n + 2); W.leaf = W.q + 2 * C.P; }
+        int* const gq = Pg + (n + 2);                    // global lists: 2P + P ints
+        WarpLists Ls, Lg;
+        Ls.q = sh.wsm[warp]; Ls.leaf = sh.wsm[warp] + HULL_WQ; Ls.qcap = HULL_WQ; Ls.lcap = HULL_WL;
+        Lg.q = gq; Lg.leaf = gq + 2 * C.P; Lg.qcap = 2 * C.P; Lg.lcap = C.P;
         __syncwarp();
         for (;;) {
             int idx = -1;
@@ -1005,7 +1032,13 @@ static __device__ void hull_cta(const float* __restrict__ pts, int n, char* scra
             if (key != ~0ull && !skip) {
                 const int u = (int)(key >> 32), v = (int)(key & 0xffffffffu);
                 int nl = 0;
-                int c = warp_wrap(H, u, v, W, lane, &nl, st_pts, st_64);
+                WarpLists L = Ls;
+                int c = warp_wrap(H, u, v, L, lane, &nl, st_pts, st_64);
+                if (c == -2) {                               // shared lists too small: global ones
+                    L = Lg;
+                    c = warp_wrap(H, u, v, L, lane, &nl, st_pts, st_64);
+                }
+                st_leaves += nl;
                 const float4 pu = P4[u], pv = P4[v];
                 const int dx = (int)(pv.x - pu.x), dy = (int)(pv.y - pu.y), dz = (int)(pv.z - pu.z);
                 int ns = 0;
@@ -1030,14 +1063,14 @@ static __device__ void hull_cta(const float* __restrict__ pts, int n, char* scra
                         ns = __shfl_sync(FULL_MASK, nn, 0);
                         __syncwarp();
                     } else {
-                        ns = warp_coplanar(H, pu, nx, ny, nz, W, nl, lane, HULL_SMALL_S, st_cop, st_64);
+                        ns = warp_coplanar(H, pu, nx, ny, nz, W, L, nl, lane, HULL_SMALL_S, st_cop, st_64);
                     }
                 }
                 int k = -1;
                 const int* poly = Pg;
                 if (c >= 0 && ns > HULL_SMALL_S) {
-                    k = warp_big_polygon(H, u, v, nx, ny, nz, W.leaf, serial ? -ns : nl, Sg, Pg, lane, st_cop, st_64);
-                    if (lane == 0) atomicAdd(&sh.stats[3], 1ull);
+                    k = warp_big_polygon(H, u, v, nx, ny, nz, L.leaf, serial ? -ns : nl, Sg, Pg, lane, st_cop, st_64);
+                    if (lane == 0) atomicAdd(&sh.stats[7], 1ull);
                 } else if (c >= 0) {
                     if (lane == 0) {
                         if (ns == 3) { Pg[0] = v; Pg[1] = u; Pg[2] = c; k = 3; }
@@ -1046,6 +1079,10 @@ static __device__ void hull_cta(const float* __restrict__ pts, int n, char* scra
                     k = __shfl_sync(FULL_MASK, k, 0);
                 }
                 __syncwarp();
+                // register the face: lane 0 claims it (face key = its smallest
+                // corner and the next one), then the lanes insert its edges and
+                // queue those whose twin is not known yet
+                int fs = -1;
                 if (lane == 0) {
                     st_wraps++;
                     if (c < 0 || k < 3) atomicOr(&sh.err, KERR_BT_EXTRACT_FAIL);
@@ -1057,23 +1094,26 @@ static __device__ void hull_cta(const float* __restrict__ pts, int n, char* scra
                             st_small++;
                             int cs = atomicAdd(&sh.n_corners, k);
                             int f = atomicAdd(&sh.n_faces, 1);
-                            if (cs + k <= C.ccap && f < C.fcap) {
-                                for (int i = 0; i < k; i++) corners[cs + i] = poly[i];
-                                faces[f] = make_int2(cs, k);
-                                for (int i = 0; i < k; i++)
-                                    if (hset_insert(eset, C.eh, ekey(poly[i], poly[(i + 1) % k])) < 0)
-                                        atomicOr(&sh.err, KERR_BT_POOL_EXHAUST);
-                                for (int i = 0; i < k; i++) {
-                                    int x = poly[i], y = poly[(i + 1) % k];
-                                    if (!hset_has(eset, C.eh, ekey(y, x))) {
-                                        atomicAdd(&q_pending, 1);
-                                        int slot = atomicAdd(&q_tail, 1);
-                                        if (slot < qcap) atomicExch(&Q[slot], ekey(x, y));
-                                        else { atomicOr(&sh.err, KERR_BT_POOL_EXHAUST); atomicSub(&q_pending, 1); }
-                                    }
-                                }
-                            } else atomicOr(&sh.err, KERR_BT_POOL_EXHAUST);
+                            if (cs + k <= C.ccap && f < C.fcap) { faces[f] = make_int2(cs, k); fs = cs; }
+                            else atomicOr(&sh.err, KERR_BT_POOL_EXHAUST);
                         } else if (ins < 0) atomicOr(&sh.err, KERR_BT_POOL_EXHAUST);
+                    }
+                }
+                fs = __shfl_sync(FULL_MASK, fs, 0);
+                if (fs >= 0) {
+                    for (int i = lane; i < k; i += 32) {
+                        corners[fs + i] = poly[i];
+                        if (hset_insert(eset, C.eh, ekey(poly[i], poly[(i + 1) % k])) < 0)
+                            atomicOr(&sh.err, KERR_BT_POOL_EXHAUST);
+                    }
+                    for (int i = lane; i < k; i += 32) {
+                        int x = poly[i], y = poly[(i + 1) % k];
+                        if (!hset_has(eset, C.eh, ekey(y, x))) {
+                            atomicAdd(&q_pending, 1);
+                            int slot = atomicAdd(&q_tail, 1);
+                            if (slot < qcap) atomicExch(&Q[slot], ekey(x, y));
+                            else { atomicOr(&sh.err, KERR_BT_POOL_EXHAUST); atomicSub(&q_pending, 1); }
+                        }
                     }
                 }
             }
@@ -1081,11 +1121,14 @@ static __device__ void hull_cta(const float* __restrict__ pts, int n, char* scra
             if (lane == 0) atomicSub(&q_pending, 1);
         }
     }
-    if ((tid & 31) == 0) atomicAdd(&sh.stats[1], (unsigned long long)st_wraps);
+    if ((tid & 31) == 0) {
+        atomicAdd(&sh.stats[0], (unsigned long long)st_leaves);
+        atomicAdd(&sh.stats[1], (unsigned long long)st_wraps);
+    }
+    atomicAdd(&sh.stats[3], (unsigned long long)st_pts);
     __syncthreads();
     const long long t_out = clock64();
     if (tid == 0) {
-        sh.stats[0] = (unsigned long long)q_tail;
         sh.stats[2] = (unsigned long long)sh.n_faces;
         sh.stats[4] = (unsigned long long)(t_wrap - t_begin);
         sh.stats[5] = (unsigned long long)(t_out - t_wrap);
@@ -1178,7 +1221,6 @@ static __device__ void hull_cta(const float* __restrict__ pts, int n, char* scra
         if (tid == 0) {
             *o_nv = nv_out; *o_nt = nt_out; if (o_vol) *o_vol = (float)fabs(vol);
             sh.stats[6] = (unsigned long long)(clock64() - t_out);
-            sh.stats[7] = (unsigned long long)nv_out;
         }
     } else {
         if (tid == 0) {
