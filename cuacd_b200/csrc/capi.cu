@@ -19,31 +19,6 @@ __global__ void k_arena_reset(Arena* a, char* base, unsigned long long cap)
     }
 }
 
-__global__ void __launch_bounds__(HULL_NT)
-k_hull_batch(const float* __restrict__ pts, const int* __restrict__ offsets, int n_hulls,
-             char* scratch, size_t stride, int max_hv, int max_ht,
-             float* out_v, int* out_t, int* out_nv, int* out_nt, float* out_vol, int* out_err,
-             unsigned long long* stats)
-{
-    __shared__ HullShared sh;
-    __shared__ int s_err;
-    int h = blockIdx.x;
-    if (h >= n_hulls) return;
-    if (threadIdx.x == 0) s_err = 0;
-    __syncthreads();
-    int a = offsets[h], n = offsets[h + 1] - offsets[h];
-    HullOut o;
-    o.verts = out_v + (size_t)h * max_hv * 3;
-    o.tris = out_t + (size_t)h * max_ht * 3;
-    o.vidx = nullptr;
-    o.max_hv = max_hv; o.max_ht = max_ht;
-    hull_cta(pts + 3 * (size_t)a, n, scratch + (size_t)h * stride, o,
-             &out_nv[h], &out_nt[h], out_vol ? &out_vol[h] : nullptr, &s_err, sh);
-    __syncthreads();
-    if (threadIdx.x == 0 && out_err) out_err[h] = s_err;
-    if (stats && threadIdx.x < 8) stats[8 * h + threadIdx.x] = sh.stats[threadIdx.x];
-}
-
 void launch_arena_reset(Arena* a, char* base, unsigned long long cap, cudaStream_t s)
 {
     k_arena_reset<<<1, 32, 0, s>>>(a, base, cap);
@@ -70,6 +45,9 @@ extern "C" int gpu_init(gpu_ctx_t* out, int device_ordinal, size_t pool_bytes)
         if (e != cudaSuccess) { free(ctx); return (int)e; }
     }
     ctx->device = dev;
+    ctx->n_sm = 0;
+    cudaDeviceGetAttribute(&ctx->n_sm, cudaDevAttrMultiProcessorCount, dev);
+    if (ctx->n_sm <= 0) ctx->n_sm = 148;
     e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) { free(ctx); return (int)e; }
     e = cudaMalloc(&ctx->d_arena, sizeof(Arena));
@@ -125,17 +103,34 @@ extern "C" unsigned long long cuacd_launch_count(gpu_ctx_t ctx) { return ctx ? c
 // ---------------------------------------------------------------------------
 // hulls
 // ---------------------------------------------------------------------------
+// Device bytes of one hull batch: jobs, states, results, control words,
+// per-warp wrap lists and per-cloud scratch.
+static size_t hull_batch_need(int n_hulls, int max_pts, int nwc)
+{
+    return al256(sizeof(HullJob) * (size_t)n_hulls) + al256(sizeof(HullState) * (size_t)n_hulls)
+         + al256(sizeof(HullRes) * (size_t)n_hulls) + al256(64) + al256(hull_wrap_buf_bytes(nwc))
+         + al256(hull_scratch_bytes(max_pts)) * (size_t)n_hulls + 4096;
+}
+
 static int launch_hull_batch(gpu_ctx* ctx, const float* d_pts, const int* d_off, int n_hulls,
                              int max_pts, int max_hv, int max_ht, float* d_v, int* d_t,
                              int* d_nv, int* d_nt, float* d_vol, int* d_err, cudaStream_t s,
                              unsigned long long* d_stats = nullptr)
 {
-    size_t stride = al256(hull_scratch_bytes(max_pts));
-    char* scratch = pool_take<char>(ctx, stride * (size_t)n_hulls);
+    const int nwc = hull_wrap_ctas((long long)n_hulls * max_pts, ctx->n_sm);
+    HullJob* jobs = pool_take<HullJob>(ctx, n_hulls);
+    HullState* states = pool_take<HullState>(ctx, n_hulls);
+    HullRes* res = pool_take<HullRes>(ctx, n_hulls);
+    int* ctl = pool_take<int>(ctx, 16);
+    int* wbuf = (int*)pool_take<char>(ctx, hull_wrap_buf_bytes(nwc));
+    const size_t scr_bytes = al256(hull_scratch_bytes(max_pts)) * (size_t)n_hulls;
+    char* scratch = pool_take<char>(ctx, scr_bytes);
     if (!scratch) return ctx_fail(ctx, KERR_HEAP_OOM, "hull scratch does not fit the pool");
-    k_hull_batch<<<n_hulls, HULL_NT, 0, s>>>(d_pts, d_off, n_hulls, scratch, stride, max_hv, max_ht,
-                                             d_v, d_t, d_nv, d_nt, d_vol, d_err, d_stats);
-    ctx->launches++;
+    launch_arena_reset(ctx->d_arena, scratch, scr_bytes, s);
+    launch_jobs_from_offsets(d_pts, d_off, n_hulls, d_v, d_t, max_hv, max_ht, jobs, s);
+    launch_hull_jobs(jobs, n_hulls, states, res, ctx->d_arena, ctx->d_arena, ctl, wbuf, nwc, d_stats, s);
+    launch_unpack_results(res, n_hulls, d_nv, d_nt, d_vol, d_err, s);
+    ctx->launches += 6;
     CK(cudaGetLastError());
     return 0;
 }
@@ -159,7 +154,8 @@ static int hull_common(gpu_ctx_t ctx, const float* pts, int total_pts, const int
     size_t need = al256(sizeof(float) * 3 * (size_t)total_pts) + al256(sizeof(int) * (size_t)(n_hulls + 1))
                 + al256(sizeof(float) * 3 * (size_t)n_hulls * max_hv) + al256(sizeof(int) * 3 * (size_t)n_hulls * max_ht)
                 + 4 * al256(sizeof(int) * (size_t)n_hulls)
-                + al256(hull_scratch_bytes(max_pts)) * (size_t)n_hulls + al256(64 * (size_t)n_hulls) + 4096;
+                + hull_batch_need(n_hulls, max_pts, hull_wrap_ctas((long long)n_hulls * max_pts, ctx->n_sm))
+                + al256(64 * (size_t)n_hulls);
     int rc = pool_begin(ctx, need);
     if (rc) return rc;
     unsigned long long* d_stats = out_stats ? pool_take<unsigned long long>(ctx, 8 * (size_t)n_hulls) : nullptr;
@@ -214,7 +210,7 @@ extern "C" int cuacd_hull_batch_device(gpu_ctx_t ctx, const float* d_pts, const 
     if (n_hulls <= 0) return 0;
     if (max_pts >= (1 << 22)) return ctx_fail(ctx, KERR_MESH_INVALID, "more than 2^22 points in one cloud");
     CK(cudaSetDevice(ctx->device));
-    int rc = pool_begin(ctx, al256(hull_scratch_bytes(max_pts)) * (size_t)n_hulls + 4096);
+    int rc = pool_begin(ctx, hull_batch_need(n_hulls, max_pts, hull_wrap_ctas((long long)n_hulls * max_pts, ctx->n_sm)));
     if (rc) return rc;
     return launch_hull_batch(ctx, d_pts, d_offsets, n_hulls, max_pts, max_hv, max_ht, d_v, d_t, d_nv, d_nt,
                              d_vol, d_err, stream ? (cudaStream_t)stream : ctx->stream);

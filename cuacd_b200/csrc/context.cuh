@@ -16,6 +16,7 @@
 
 struct gpu_ctx {
     int            device;
+    int            n_sm;               // streaming multiprocessors of the device
     cudaStream_t   stream;
     char*          pool;
     size_t         cap;

@@ -4,9 +4,9 @@
 // cuda/la_common.cuh:21-34.  This is the per-candidate scorer of the
 // reference's la_expand (cuda/la_expand.cu:65-340) + la_hull
 // (:357-424) + la_hausdorff_parts (cuda/la_refine.cu:19-45), as one
-// device-resident pipeline of four launches with no host round trip:
+// device-resident pipeline with no host round trip:
 //   k_cut_planes  (cut.cu)   one CTA per plane, fragments into the arena
-//   k_frag_hull              one CTA per fragment: volume + exact hull
+//   hull pipeline (hull.cu)  volume + exact hull of every fragment
 //   Hausdorff prep/plan/query (hausdorff.cu), pairs (hull, fragment)
 //   k_eval_finish            costs and the per-candidate record
 #include "context.cuh"
@@ -15,52 +15,24 @@
 #include "hausdorff.cuh"
 #include "launch.h"
 
-struct FragInfo {
-    float* hv; int* ht; int hnv, hnt;
-    double mesh_vol;
-    float hull_vol; int err;
-};
+typedef HullRes FragInfo;     // per fragment: hull, mesh and hull volume, error
 
-__global__ void __launch_bounds__(HULL_NT)
-k_frag_hull(const CutResult* __restrict__ cuts, int n_cand, Arena* arena, FragInfo* frags)
+// Hull jobs for both fragments of every candidate (empty when the cut failed
+// or left one side empty).  The fragment's triangles give its mesh volume.
+__global__ void k_frag_jobs(const CutResult* __restrict__ cuts, int n_cand, HullJob* jobs)
 {
-    __shared__ HullShared sh;
-    __shared__ char* s_scr;
-    __shared__ float* s_ov;
-    __shared__ int* s_ot;
-    __shared__ int s_err, s_nv, s_nt;
-    __shared__ float s_vol;
-    const int f = blockIdx.x, cand = f >> 1, side = f & 1;
-    if (cand >= n_cand) return;
-    const CutResult& C = cuts[cand];
-    const float* v = side ? C.nv : C.pv;
-    const int* t = side ? C.nt : C.pt;
-    const int nv = side ? C.nnv : C.npv, nt = side ? C.nnt : C.npt;
-    const bool empty = C.err != 0 || nv <= 0 || nt <= 0 || C.npv <= 0 || C.nnv <= 0;
-    if (threadIdx.x == 0) {
-        s_err = 0; s_scr = nullptr; s_ov = nullptr; s_ot = nullptr;
-        if (!empty) {
-            s_scr = (char*)arena_alloc(arena, hull_scratch_bytes(nv), &s_err);
-            s_ov = (float*)arena_alloc(arena, 12ull * nv, &s_err);
-            s_ot = (int*)arena_alloc(arena, 12ull * (2 * nv + 4), &s_err);
-        }
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= 2 * n_cand) return;
+    const CutResult& C = cuts[f >> 1];
+    const int side = f & 1;
+    const bool empty = C.err != 0 || C.npv <= 0 || C.nnv <= 0;
+    HullJob J;
+    memset(&J, 0, sizeof(J));
+    if (!empty) {
+        J.pts = side ? C.nv : C.pv; J.n = side ? C.nnv : C.npv;
+        J.tris = side ? C.nt : C.pt; J.nt = side ? C.nnt : C.npt;
     }
-    __syncthreads();
-    FragInfo F;
-    memset(&F, 0, sizeof(F));
-    if (empty || s_err || !s_scr || !s_ov || !s_ot) {
-        if (threadIdx.x == 0) { F.err = s_err; frags[f] = F; }
-        return;
-    }
-    double mv = block_mesh_signed_volume(v, nv, t, nt, sh.dsh);
-    HullOut o; o.verts = s_ov; o.tris = s_ot; o.vidx = nullptr; o.max_hv = nv; o.max_ht = 2 * nv + 4;
-    hull_cta(v, nv, s_scr, o, &s_nv, &s_nt, &s_vol, &s_err, sh);
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        F.hv = s_ov; F.ht = s_ot; F.hnv = s_nv; F.hnt = s_nt;
-        F.mesh_vol = fabs(mv); F.hull_vol = s_vol; F.err = s_err;
-        frags[f] = F;
-    }
+    jobs[f] = J;
 }
 
 // surfaces for the Hausdorff pairs: pair f = (hull of fragment f, fragment f)
@@ -117,13 +89,21 @@ __global__ void k_eval_finish(const CutResult* __restrict__ cuts, const FragInfo
 struct EvalWork {
     float4* planes; CutResult* cuts; FragInfo* frags; HDSurf* surfs; HDPrep* preps;
     char* dirs; int* i4; float* pmax; float* hd;
+    HullJob* jobs; HullState* states; int* hctl; int* wbuf; int nwc;
 };
 
-static size_t eval_fixed_bytes(int n)
+static size_t eval_fixed_bytes(int n, int nwc)
 {
     return al256(sizeof(float4) * n) + al256(sizeof(CutResult) * n) + al256(sizeof(FragInfo) * 2 * n)
          + al256(sizeof(HDSurf) * 4 * n) + al256(sizeof(HDPrep) * 4 * n) + al256(hd_dir_bytes() * 4 * n)
-         + al256(sizeof(int) * 4) + 2 * al256(sizeof(float) * 2 * n);
+         + al256(sizeof(int) * 4) + 2 * al256(sizeof(float) * 2 * n)
+         + al256(sizeof(HullJob) * 2 * n) + al256(sizeof(HullState) * 2 * n) + al256(64)
+         + al256(hull_wrap_buf_bytes(nwc));
+}
+
+static int eval_wrap_ctas(gpu_ctx* ctx, int nv, int n)
+{
+    return hull_wrap_ctas(2LL * n * nv, ctx->n_sm);
 }
 
 static size_t eval_arena_bytes(int nv, int nt, int n)
@@ -138,8 +118,13 @@ static size_t eval_arena_bytes(int nv, int nt, int n)
     return per * (size_t)n;
 }
 
-static int eval_take(gpu_ctx* ctx, int n, EvalWork& W)
+static int eval_take(gpu_ctx* ctx, int n, int nwc, EvalWork& W)
 {
+    W.nwc = nwc;
+    W.jobs = pool_take<HullJob>(ctx, 2 * n);
+    W.states = pool_take<HullState>(ctx, 2 * n);
+    W.hctl = pool_take<int>(ctx, 16);
+    W.wbuf = (int*)pool_take<char>(ctx, hull_wrap_buf_bytes(nwc));
     W.planes = pool_take<float4>(ctx, n);
     W.cuts = pool_take<CutResult>(ctx, n);
     W.frags = pool_take<FragInfo>(ctx, 2 * n);
@@ -169,9 +154,11 @@ static void eval_launch(gpu_ctx* ctx, const float* d_v, int nv, const int* d_t, 
     mark(0);
     launch_cut_planes(d_v, nv, d_t, nt, W.planes, n, ctx->d_arena, W.cuts, s);
     mark(1);
-    k_frag_hull<<<2 * n, HULL_NT, 0, s>>>(W.cuts, n, ctx->d_arena, W.frags);
+    k_frag_jobs<<<(2 * n + 127) / 128, 128, 0, s>>>(W.cuts, n, W.jobs);
+    launch_hull_jobs(W.jobs, 2 * n, W.states, W.frags, ctx->d_arena, ctx->d_arena, W.hctl, W.wbuf, W.nwc,
+                     nullptr, s);
     mark(2);
-    ctx->launches += 3;
+    ctx->launches += 6;
     const bool hd = flags & CUACD_EVAL_HAUSDORFF;
     if (hd) {
         k_make_surfs<<<(2 * n + 127) / 128, 128, 0, s>>>(W.cuts, W.frags, 2 * n, W.surfs);
@@ -216,10 +203,11 @@ extern "C" int cuacd_eval_candidates_device(gpu_ctx_t ctx, const float* d_verts,
     if (hd_min_samples < 0) hd_min_samples = 1000;
     CK(cudaSetDevice(ctx->device));
     cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
-    int rc = pool_begin(ctx, eval_fixed_bytes(n_planes) + eval_arena_bytes(nv, nt, n_planes));
+    const int nwc = eval_wrap_ctas(ctx, nv, n_planes);
+    int rc = pool_begin(ctx, eval_fixed_bytes(n_planes, nwc) + eval_arena_bytes(nv, nt, n_planes));
     if (rc) return rc;
     EvalWork W;
-    if (eval_take(ctx, n_planes, W)) return ctx_fail(ctx, KERR_HEAP_OOM, "pool too small");
+    if (eval_take(ctx, n_planes, nwc, W)) return ctx_fail(ctx, KERR_HEAP_OOM, "pool too small");
     CK(cudaMemcpyAsync(W.planes, d_planes, sizeof(float4) * n_planes, cudaMemcpyDeviceToDevice, s));
     eval_launch(ctx, d_verts, nv, d_tris, nt, n_planes, flags, hd_resolution, hd_min_samples, hd_total, W, d_out, s);
     CK(cudaGetLastError());
@@ -239,16 +227,17 @@ extern "C" int cuacd_eval_candidates(gpu_ctx_t ctx, const float* verts, int nv, 
     if (hd_min_samples < 0) hd_min_samples = 1000;
     CK(cudaSetDevice(ctx->device));
     size_t extra = 0;
+    const int nwc = eval_wrap_ctas(ctx, nv, n_planes);
     for (int attempt = 0; attempt < 4; attempt++) {
         size_t need = al256(12 * (size_t)nv) + al256(12 * (size_t)nt) + al256(sizeof(cuacd_cand_result) * n_planes)
-                    + eval_fixed_bytes(n_planes) + eval_arena_bytes(nv, nt, n_planes) + extra;
+                    + eval_fixed_bytes(n_planes, nwc) + eval_arena_bytes(nv, nt, n_planes) + extra;
         int rc = pool_begin(ctx, need);
         if (rc) return rc;
         float* dv = pool_take<float>(ctx, 3 * (size_t)nv);
         int* dt = pool_take<int>(ctx, 3 * (size_t)nt);
         cuacd_cand_result* dout = pool_take<cuacd_cand_result>(ctx, n_planes);
         EvalWork W;
-        if (eval_take(ctx, n_planes, W)) return ctx_fail(ctx, KERR_HEAP_OOM, "pool too small");
+        if (eval_take(ctx, n_planes, nwc, W)) return ctx_fail(ctx, KERR_HEAP_OOM, "pool too small");
         cudaStream_t s = ctx->stream;
         CK(cudaMemcpyAsync(dv, verts, 12 * (size_t)nv, cudaMemcpyHostToDevice, s));
         CK(cudaMemcpyAsync(dt, tris, 12 * (size_t)nt, cudaMemcpyHostToDevice, s));
@@ -259,7 +248,8 @@ extern "C" int cuacd_eval_candidates(gpu_ctx_t ctx, const float* verts, int nv, 
         rc = sync_and_check(ctx, "eval_candidates");
         if (rc) return rc;
         bool oom = false;
-        for (int i = 0; i < n_planes; i++) if (out[i].err & (KERR_HEAP_OOM | KERR_PC_SCRATCH_OOM | KERR_HD_SCRATCH_OOM)) oom = true;
+        for (int i = 0; i < n_planes; i++)
+            if (out[i].err & (KERR_HEAP_OOM | KERR_PC_SCRATCH_OOM | KERR_HD_SCRATCH_OOM)) oom = true;
         if (!oom) return 0;
         if (ctx->fixed) return ctx_fail(ctx, KERR_HEAP_OOM, "device pool too small for this evaluation");
         extra = (ctx->cap) * 2;       // grow and retry

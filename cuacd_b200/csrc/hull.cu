@@ -1,0 +1,224 @@
+// hull.cu — kernels and launcher of the batched hull pipeline (hull.cuh):
+// set-up (one CTA per cloud), shares of the wrap grid, persistent wrapping
+// (up to one CTA per SM; each CTA wraps its home cloud, then helps others),
+// output (one CTA per cloud).
+#include "context.cuh"
+#include "hull.cuh"
+#include "launch.h"
+
+__global__ void __launch_bounds__(HULL_NT)
+k_hull_setup(const HullJob* __restrict__ jobs, int n_jobs, Arena* scratch, HullState* states, int* ctl)
+{
+    __shared__ HullSetupShared sh;
+    __shared__ char* s_scr;
+    __shared__ int s_err;
+    const int j = blockIdx.x;
+    if (j >= n_jobs) return;
+    const HullJob J = jobs[j];
+    HullState* S = &states[j];
+    double mv = 0.0;
+    if (J.tris && J.nt > 0 && J.n > 0) mv = block_mesh_signed_volume(J.pts, J.n, J.tris, J.nt, sh.dsh);
+    if (threadIdx.x == 0) {
+        S->n = J.n; S->n_faces = 0; S->err = 0; S->active = 0; S->q_pending = 0;
+        for (int k = 0; k < 8; k++) S->stats[k] = 0;
+        s_err = 0; s_scr = nullptr;
+        if (J.n >= 4) {
+            s_scr = (char*)arena_alloc(scratch, hull_scratch_bytes(J.n), &s_err);
+            if (!s_scr) S->err = s_err | KERR_BT_POOL_EXHAUST;
+        }
+    }
+    __syncthreads();
+    if (s_scr) hull_setup_cta(J.pts, J.n, s_scr, S, sh);
+    if (threadIdx.x == 0) {
+        S->mesh_vol = fabs(mv);
+        if (s_scr && S->active) atomicAdd(&ctl[0], 1);
+    }
+}
+
+// Prefix of the active hulls' point counts (wrap-grid shares), one CTA.
+__global__ void __launch_bounds__(1024)
+k_hull_assign(HullState* states, int n_jobs, long long* total)
+{
+    __shared__ long long part[1024 / 32];
+    __shared__ long long carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (int base = 0; base < n_jobs; base += 1024) {
+        const int j = base + threadIdx.x;
+        long long w = (j < n_jobs && states[j].active) ? (long long)states[j].n : 0;
+        long long x = w;                                  // inclusive warp scan
+        #pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            long long y = __shfl_up_sync(FULL_MASK, x, o);
+            if ((threadIdx.x & 31) >= o) x += y;
+        }
+        if ((threadIdx.x & 31) == 31) part[threadIdx.x >> 5] = x;
+        __syncthreads();
+        if (threadIdx.x < 32) {
+            long long p = part[threadIdx.x], q = p;
+            #pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                long long y = __shfl_up_sync(FULL_MASK, q, o);
+                if (threadIdx.x >= o) q += y;
+            }
+            part[threadIdx.x] = q - p;                    // exclusive over warps
+        }
+        __syncthreads();
+        if (j < n_jobs) states[j].wbase = carry + part[threadIdx.x >> 5] + x - w;
+        __syncthreads();
+        if (threadIdx.x == 1023) carry += part[31] + x;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *total = carry;
+}
+
+__global__ void __launch_bounds__(HULL_NT, 1)
+k_hull_wrap(HullState* states, int n_jobs, int* ctl, const long long* total, int* wbuf)
+{
+    __shared__ HullWrapShared sh;
+    extern __shared__ int wsm_dyn[];                      // HULL_WRAP_DSMEM bytes
+    __shared__ int s_h0, s_go;
+    if (threadIdx.x == 0) {
+        // one reader decides for the whole CTA: other CTAs may finish the
+        // last hull while this one starts
+        s_go = *(volatile int*)&ctl[0] > 0;
+        // home hull: the active hull whose share holds this CTA's point
+        const long long W = *total;
+        const long long t = ((2LL * blockIdx.x + 1) * W) / (2LL * gridDim.x);
+        int lo = 0, hi = n_jobs - 1;
+        while (lo < hi) {                                 // last j with wbase[j] <= t
+            int mid = (lo + hi + 1) >> 1;
+            if (states[mid].wbase <= t) lo = mid; else hi = mid - 1;
+        }
+        s_h0 = lo;
+    }
+    __syncthreads();
+    if (!s_go) return;
+    hull_wrap_grid(states, n_jobs, s_h0, ctl, wbuf, sh, wsm_dyn);
+}
+
+__global__ void __launch_bounds__(HULL_NT)
+k_hull_output(const HullJob* __restrict__ jobs, HullState* states, int n_jobs, Arena* out, const int* ctl,
+              HullRes* res, unsigned long long* stats)
+{
+    __shared__ HullOutShared sh;
+    __shared__ float* s_ov;
+    __shared__ int* s_ot;
+    __shared__ int s_mhv, s_mht, s_aerr, s_nv, s_nt, s_oerr;
+    __shared__ float s_vol;
+    const int j = blockIdx.x;
+    if (j >= n_jobs) return;
+    const HullJob J = jobs[j];
+    HullState* S = &states[j];
+    if (threadIdx.x == 0) {
+        if (J.n >= 4 && S->active) atomicOr(&S->err, ctl[1] ? ctl[1] : KERR_TIMEOUT);   // not finished
+        s_aerr = 0;
+        s_ov = J.out_v; s_ot = J.out_t; s_mhv = J.max_hv; s_mht = J.max_ht;
+        if (!J.out_v && J.n >= 4 && S->err == 0) {
+            s_ov = (float*)arena_alloc(out, 12ull * J.n, &s_aerr);
+            s_ot = (int*)arena_alloc(out, 12ull * (2 * J.n + 4), &s_aerr);
+            s_mhv = J.n; s_mht = 2 * J.n + 4;
+        }
+        s_nv = 0; s_nt = 0; s_vol = 0.f; s_oerr = 0;
+    }
+    __syncthreads();
+    if (s_aerr) {
+        if (threadIdx.x == 0) { HullRes r; memset(&r, 0, sizeof(r)); r.mesh_vol = S->mesh_vol; r.err = s_aerr; res[j] = r; }
+        return;
+    }
+    hull_output_cta(J.pts, S, s_ov, s_ot, s_mhv, s_mht, &s_nv, &s_nt, &s_vol, &s_oerr, sh);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        HullRes r;
+        r.hv = s_nv > 0 ? s_ov : nullptr; r.ht = s_nt > 0 ? s_ot : nullptr;
+        r.hnv = s_nv; r.hnt = s_nt;
+        r.mesh_vol = S->mesh_vol; r.hull_vol = s_vol;
+        r.err = s_oerr | S->err;
+        res[j] = r;
+    }
+    if (stats && threadIdx.x < 8)
+        stats[8 * (size_t)j + threadIdx.x] = threadIdx.x == 2 ? (unsigned long long)S->n_faces : S->stats[threadIdx.x];
+}
+
+size_t hull_wrap_buf_bytes(int n_wrap_ctas)
+{
+    return (size_t)n_wrap_ctas * (HULL_NT / 32) * 2 * HULL_SGCAP * sizeof(int);
+}
+
+// Opt in to the wrap kernel's dynamic shared memory (once per process and
+// device) and return its resident CTAs per SM.
+static int hull_wrap_per_sm()
+{
+    static int cached[64] = {0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) dev = 0;
+    if (cached[dev] <= 0) {
+        cudaFuncSetAttribute(k_hull_wrap, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HULL_WRAP_DSMEM);
+        int b = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_hull_wrap, HULL_NT, HULL_WRAP_DSMEM) != cudaSuccess || b < 1)
+            b = 1;
+        cached[dev] = b;
+    }
+    return cached[dev];
+}
+
+// Wrap grid size: about one warp per 256 points of the batch, at most the
+// resident CTAs of the whole device.
+int hull_wrap_ctas(long long total_points, int n_sm)
+{
+    long long c = (total_points + 4095) / 4096;
+    const long long cap = (long long)n_sm * hull_wrap_per_sm();
+    if (c < 1) c = 1;
+    if (c > cap) c = cap;
+    return (int)c;
+}
+
+void launch_hull_jobs(const HullJob* d_jobs, int n_jobs, HullState* d_states, HullRes* d_res, Arena* scratch,
+                      Arena* out, int* d_ctl, int* d_wbuf, int n_wrap_ctas, unsigned long long* d_stats,
+                      cudaStream_t s)
+{
+    if (n_jobs <= 0) return;
+    cudaMemsetAsync(d_ctl, 0, 4 * sizeof(int), s);
+    k_hull_setup<<<n_jobs, HULL_NT, 0, s>>>(d_jobs, n_jobs, scratch, d_states, d_ctl);
+    k_hull_assign<<<1, 1024, 0, s>>>(d_states, n_jobs, (long long*)(d_ctl + 2));
+    hull_wrap_per_sm();                                   // dynamic shared memory opt-in
+    k_hull_wrap<<<n_wrap_ctas, HULL_NT, HULL_WRAP_DSMEM, s>>>(d_states, n_jobs, d_ctl, (const long long*)(d_ctl + 2),
+                                                             d_wbuf);
+    k_hull_output<<<n_jobs, HULL_NT, 0, s>>>(d_jobs, d_states, n_jobs, out, d_ctl, d_res, d_stats);
+}
+
+// Jobs for clouds packed back to back (offsets), outputs in fixed slots.
+__global__ void k_jobs_from_offsets(const float* pts, const int* offsets, int n, float* out_v, int* out_t,
+                                    int max_hv, int max_ht, HullJob* jobs)
+{
+    int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    HullJob J;
+    J.pts = pts + 3 * (size_t)offsets[j]; J.n = offsets[j + 1] - offsets[j];
+    J.tris = nullptr; J.nt = 0;
+    J.out_v = out_v + 3 * (size_t)j * max_hv; J.out_t = out_t + 3 * (size_t)j * max_ht;
+    J.max_hv = max_hv; J.max_ht = max_ht;
+    jobs[j] = J;
+}
+
+__global__ void k_unpack_results(const HullRes* res, int n, int* out_nv, int* out_nt, float* out_vol, int* out_err)
+{
+    int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    HullRes r = res[j];
+    out_nv[j] = r.hnv; out_nt[j] = r.hnt;
+    if (out_vol) out_vol[j] = r.hull_vol;
+    if (out_err) out_err[j] = r.err;
+}
+
+void launch_jobs_from_offsets(const float* d_pts, const int* d_off, int n, float* d_v, int* d_t, int max_hv,
+                              int max_ht, HullJob* d_jobs, cudaStream_t s)
+{
+    if (n > 0) k_jobs_from_offsets<<<(n + 127) / 128, 128, 0, s>>>(d_pts, d_off, n, d_v, d_t, max_hv, max_ht, d_jobs);
+}
+
+void launch_unpack_results(const HullRes* d_res, int n, int* d_nv, int* d_nt, float* d_vol, int* d_err, cudaStream_t s)
+{
+    if (n > 0) k_unpack_results<<<(n + 127) / 128, 128, 0, s>>>(d_res, n, d_nv, d_nt, d_vol, d_err);
+}

@@ -1,24 +1,27 @@
-// hull.cuh — exact convex hull of a point cloud, one CTA per cloud (sm_100a).
+// hull.cuh — exact convex hulls of point clouds, batched (sm_100a).
 //
 // Replaces the reference's warp D&C hull (cuda/hull_dandc.cuh:1678-1861) and
-// its k-DOP prefilter (cuda/kdop_hull.cuh:49-398) with one exact algorithm:
+// its k-DOP prefilter (cuda/kdop_hull.cuh:49-398) with one exact algorithm,
+// run as three launches over a batch of clouds (kernels in hull.cu):
 //
-//   1. quantise onto the reference grid (hull_dandc.cuh:1351-1411): per-axis
-//      step span/10216, axes permuted to (med,max,min), sign flip when
-//      (medAx+1)%3 != maxAx, truncation toward zero; IEEE-rounded divisions.
-//      Grid coordinates are |q| <= 5109, stored as exact floats.
-//   2. bucket the points by a 12-bit Morton code and build an implicit binary
-//      BVH over leaves of HULL_LEAF points (bounding boxes in grid units).
-//   3. gift wrapping over polygon faces, one thread per frontier edge: the
-//      next face around edge (u,v) is found by branch-and-bound over the BVH
-//      (a box is skipped when no corner lies strictly beyond the current
-//      plane).  Orientation tests run in FP32 with a static error bound and
-//      fall back to exact FP64 (all grid predicates are < 2^46 in magnitude,
-//      so FP64 is exact) near zero.  Coplanar points are merged into one
-//      polygon face; faces with more than HULL_SMALL_S coplanar points are
-//      finished cooperatively by the whole CTA.
-//   4. canonical output: corners in ascending input index; each face fanned
-//      from its smallest corner; triangles grouped by first vertex and sorted.
+//   1. set-up, one CTA per cloud: quantise onto the reference grid
+//      (hull_dandc.cuh:1351-1411: per-axis step span/10216, axes permuted to
+//      (med,max,min), sign flip when (medAx+1)%3 != maxAx, truncation toward
+//      zero, IEEE-rounded divisions; |q| <= 5109, stored as exact floats);
+//      bucket by a 12-bit Morton code; implicit binary BVH over leaves of
+//      HULL_LEAF points with per-leaf oriented boxes; the first face; the
+//      frontier queue.
+//   2. wrapping, a persistent grid: every warp takes frontier edges from any
+//      cloud's queue.  The next face around edge (u,v) is found by a
+//      depth-first branch-and-bound over the BVH that tightens the plane as
+//      leaves are scanned.  Orientation tests run in FP32 with a static error
+//      bound and fall back to exact FP64 near zero (grid predicates are
+//      < 2^46, so FP64 is exact).  Coplanar points are merged into one polygon
+//      face.  New faces go to a face hash set, their edges to an edge hash
+//      set, unmatched edges to the queue.
+//   3. output, one CTA per cloud: corners in ascending input index; each face
+//      fanned from its smallest corner; triangles grouped by first vertex and
+//      sorted; FP64 volume.
 //
 // Duplicate grid points resolve to the smallest input index, as the
 // reference's (y,x,z,index) sort keeps the first (warp_sort.cuh:237-244).
@@ -30,21 +33,15 @@
 #define HULL_SMALL_S  24
 #define HULL_MORTON_BITS 4            // bits per axis for the bucket sort
 #define HULL_CELLS    (1 << (3 * HULL_MORTON_BITS))
-#define HULL_WSM      (HULL_CELLS / (HULL_NT / 32))   // shared ints per warp while wrapping
-#define HULL_WQ       160                          // of which: node stack
+#define HULL_WSM      1024                         // shared ints per warp while wrapping (dynamic)
+#define HULL_WQ       704                          // of which: node stack
 #define HULL_WL       (HULL_WSM - HULL_WQ)         //           kept-leaf list
-
-struct HullOut {
-    float* verts;     // hull corner coordinates (input floats), cap max_hv
-    int*   tris;      // triangles, cap max_ht
-    int*   vidx;      // optional: input index of each corner (nullable)
-    int    max_hv, max_ht;
-};
+#define HULL_WRAP_DSMEM ((size_t)(HULL_NT / 32) * HULL_WSM * sizeof(int))
 
 // Per-cloud scratch layout (bytes computed on the host by hull_scratch_bytes).
 struct HullCaps {
     int n, m_leaves, P;      // points, leaves, leaf slots (pow2)
-    int hcap, ccap, fcap, fr_cap, eh, fh, bq_cap;
+    int hcap, ccap, fcap, fr_cap, eh, fh;
 };
 
 __host__ __device__ inline int hull_pow2(int x) { int p = 1; while (p < x) p <<= 1; return p; }
@@ -64,31 +61,11 @@ __host__ __device__ inline HullCaps hull_caps(int n)
     c.fr_cap = 6 * h + 64;
     c.eh = hull_pow2(2 * c.ccap);
     c.fh = hull_pow2(2 * c.fcap);
-    c.bq_cap = 1024;
     return c;
 }
 
 __host__ __device__ inline size_t hull_align(size_t x) { return (x + 255) & ~(size_t)255; }
 
-__host__ __device__ inline size_t hull_scratch_bytes(int n)
-{
-    HullCaps c = hull_caps(n);
-    size_t b = 0;
-    b += hull_align(sizeof(float4) * (size_t)(n > 0 ? n : 1));        // pts
-    b += hull_align(sizeof(float4) * 2 * (size_t)(2 * c.P));          // node lo/hi
-    b += hull_align(sizeof(unsigned long long) * (size_t)c.eh);       // edge set
-    b += hull_align(sizeof(unsigned long long) * (size_t)c.fh);       // face keys
-    b += hull_align(sizeof(int2) * (size_t)c.fcap);                   // faces
-    b += hull_align(sizeof(int) * (size_t)c.ccap);                    // corners
-    b += hull_align(sizeof(int2) * 2 * (size_t)c.fr_cap);             // frontier x2
-    b += hull_align(sizeof(int4) * (size_t)c.bq_cap);                 // big-face queue
-    b += hull_align(sizeof(int) * (size_t)(n > 0 ? n : 1));           // S / per-point flags
-    b += hull_align(sizeof(int) * (size_t)(n > 0 ? n : 1));           // positions
-    b += hull_align(sizeof(int) * (size_t)(n > 0 ? n : 1) * 2);       // owner count/fill
-    b += hull_align(sizeof(float4) * 4 * (size_t)c.P);                // leaf OBBs
-    b += hull_align(sizeof(int) * (HULL_NT / 32) * (2 * (size_t)(n + 2) + 3 * (size_t)c.P)); // per-warp buffers
-    return b;
-}
 
 // ---------------------------------------------------------------------------
 // exact grid geometry
@@ -559,41 +536,106 @@ static __device__ __forceinline__ bool hset_has(const unsigned long long* tab, i
 }
 
 // ---------------------------------------------------------------------------
-// the CTA hull
+// batched hull pipeline: setup (one CTA per hull), wrapping (a persistent
+// grid whose warps take frontier edges from any hull's queue), output (one
+// CTA per hull).  Per-hull state lives in global memory (HullState).
 // ---------------------------------------------------------------------------
-struct HullShared {
+struct HullJob {               // one hull to build (device pointers)
+    const float* pts; int n;   // the cloud, AoS xyz
+    const int* tris; int nt;   // optional: mesh triangles over pts (mesh volume)
+    float* out_v; int* out_t;  // null: outputs are taken from the output arena
+    int max_hv, max_ht;        //       (capacities n and 2n+4)
+};
+
+struct HullRes {               // per job
+    float* hv; int* ht; int hnv, hnt;
+    double mesh_vol;           // |signed volume| of (pts, tris), 0 without tris
+    float hull_vol; int err;
+};
+
+struct HullState {             // per hull, global memory
+    float4* P4; float4* nlo; float4* nhi; float4* obb;
+    unsigned long long* eset; unsigned long long* fset; unsigned long long* Q;
+    int2* faces; int* corners; int* Sbuf; int* posn; int* ocnt;
+    int n, P, m_leaves, eh, fh, fcap, ccap, qcap;
+    int q_head, q_tail, q_pending, n_faces, n_corners, err;
+    int active;                // 1 while its frontier queue has work
+    int lock;                  // guards Sbuf/posn/ocnt while wrapping (large faces)
+    long long wbase;           // wrap-grid share: prefix of the active hulls' point counts
+    double mesh_vol;
+    unsigned long long stats[8];   // leaves kept by wraps, wraps, faces, points
+                                   // tested by wraps, set-up cycles, wraps on
+                                   // the hull's own lists, faces on the hull's
+                                   // own buffers, large faces
+};
+
+__host__ __device__ inline size_t hull_scratch_bytes(int n)
+{
+    HullCaps c = hull_caps(n);
+    size_t nn = (size_t)(n > 0 ? n : 1);
+    size_t b = 0;
+    b += hull_align(sizeof(float4) * nn);                             // pts
+    b += hull_align(sizeof(float4) * 2 * (size_t)(2 * c.P));          // node lo/hi
+    b += hull_align(sizeof(unsigned long long) * (size_t)c.eh);       // edge set
+    b += hull_align(sizeof(unsigned long long) * (size_t)c.fh);       // face keys
+    b += hull_align(sizeof(int2) * (size_t)c.fcap);                   // faces
+    b += hull_align(sizeof(int) * (size_t)c.ccap);                    // corners
+    b += hull_align(sizeof(unsigned long long) * 2 * (size_t)c.fr_cap); // frontier queue
+    b += hull_align(sizeof(int) * nn);                                // coplanar set (set-up)
+    b += hull_align(sizeof(int) * nn);                                // output positions
+    b += hull_align(sizeof(int) * nn * 2);                            // owner count / fill
+    b += hull_align(sizeof(float4) * 4 * (size_t)c.P);                // leaf OBBs
+    return b;
+}
+
+// Per-warp global lists of the wrapping grid, sized for clouds of up to
+// n_max points: coplanar set and polygon (n_max + 2 each), node stack (2P)
+// and leaf list (P).
+__host__ __device__ inline size_t hull_warp_bytes(int n_max)
+{
+    HullCaps c = hull_caps(n_max > 4 ? n_max : 4);
+    return hull_align(sizeof(int) * (2 * (size_t)(n_max + 2) + 3 * (size_t)c.P));
+}
+
+struct HullSetupShared {
     float mn[3], mx[3];
     float cen[3], inv[3];
     int ax[3];
     unsigned long long lexmin;
-    int n_faces, n_corners, n_front, n_next, n_big, err;
+    int n_faces, n_corners, err;
     int n_S;
     int red_id[HULL_NT / 32];
     int scan[33];
     double dsh[33];
-    HullWarp ws[HULL_NT / 32];
-    int cells[HULL_CELLS];           // bucket sort
-    int wsm[HULL_NT / 32][HULL_WSM]; // per-warp node stack + leaf list
-    unsigned long long stats[8];   // leaves kept by wraps, wraps, faces, points
-                                   // tested by wraps, setup / wrap / output
-                                   // cycles, large faces
+    int cells[HULL_CELLS];
 };
 
-// Build one hull.  All HULL_NT threads call.  `pts` are the input floats
-// (AoS xyz) of this cloud; `scratch` holds hull_scratch_bytes(n).
-// Writes the hull into `out` and returns (via *o_nv, *o_nt, *o_vol from
-// thread 0) the counts and FP64 volume; error bits go to *err_word.
-static __device__ void hull_cta(const float* __restrict__ pts, int n, char* scratch,
-                         HullOut out, int* o_nv, int* o_nt, float* o_vol, int* err_word,
-                         HullShared& sh)
+struct HullWrapShared {
+    HullWarp ws[HULL_NT / 32];
+};
+
+struct HullOutShared {
+    int scan[33];
+    double dsh[33];
+};
+
+static __device__ __forceinline__ HullCtx hull_ctx(const HullState& S)
+{
+    HullCtx H;
+    H.pts = S.P4; H.nlo = S.nlo; H.nhi = S.nhi; H.obb = S.obb; H.m = S.n; H.P = S.P; H.nleaf = S.m_leaves;
+    return H;
+}
+
+// Set-up of one hull (all HULL_NT threads): quantise and bucket-sort the
+// points, build the BVH and the leaf boxes, clear the tables, build the
+// first face and seed the frontier queue.  Writes the hull's state to *S;
+// S->active = 1 when the queue holds work.  `scratch` holds
+// hull_scratch_bytes(n) bytes.
+static __device__ void hull_setup_cta(const float* __restrict__ pts, int n, char* scratch, HullState* S,
+                                      HullSetupShared& sh)
 {
     const int tid = threadIdx.x;
     const long long t_begin = clock64();
-    if (tid == 0) { sh.err = 0; }
-    if (n < 4) {
-        if (tid == 0) { *o_nv = 0; *o_nt = 0; if (o_vol) *o_vol = 0.f; }
-        return;
-    }
     HullCaps C = hull_caps(n);
     char* p = scratch;
     float4* P4 = (float4*)p;            p += hull_align(sizeof(float4) * (size_t)n);
@@ -603,15 +645,22 @@ static __device__ void hull_cta(const float* __restrict__ pts, int n, char* scra
     unsigned long long* fset = (unsigned long long*)p; p += hull_align(sizeof(unsigned long long) * (size_t)C.fh);
     int2* faces = (int2*)p;             p += hull_align(sizeof(int2) * (size_t)C.fcap);
     int* corners = (int*)p;             p += hull_align(sizeof(int) * (size_t)C.ccap);
-    int2* front0 = (int2*)p;
-    int2* front1 = front0 + C.fr_cap;   p += hull_align(sizeof(int2) * 2 * (size_t)C.fr_cap);
-    int4* bigq = (int4*)p;              p += hull_align(sizeof(int4) * (size_t)C.bq_cap);
+    unsigned long long* Q = (unsigned long long*)p; p += hull_align(sizeof(unsigned long long) * 2 * (size_t)C.fr_cap);
     int* Sbuf = (int*)p;                p += hull_align(sizeof(int) * (size_t)n);
     int* posn = (int*)p;                p += hull_align(sizeof(int) * (size_t)n);
-    int* ocnt = (int*)p;                p += hull_align(sizeof(int) * (size_t)n * 2);  // owner counts, fill
-    int* ofill = ocnt + n;
-    float4* obb = (float4*)p;           p += hull_align(sizeof(float4) * 4 * (size_t)C.P);
-    int* wbuf = (int*)p;                                 // per warp: S (n+2) then polygon (n+2)
+    int* ocnt = (int*)p;                p += hull_align(sizeof(int) * (size_t)n * 2);
+    float4* obb = (float4*)p;
+    const int qcap = 2 * C.fr_cap;
+    if (tid == 0) {
+        S->P4 = P4; S->nlo = nlo; S->nhi = nhi; S->obb = obb; S->eset = eset; S->fset = fset; S->Q = Q;
+        S->faces = faces; S->corners = corners; S->Sbuf = Sbuf; S->posn = posn; S->ocnt = ocnt;
+        S->n = n; S->P = C.P; S->m_leaves = C.m_leaves; S->eh = C.eh; S->fh = C.fh; S->fcap = C.fcap;
+        S->ccap = C.ccap; S->qcap = qcap;
+        S->q_head = 0; S->q_tail = 0; S->q_pending = 0; S->n_faces = 0; S->n_corners = 0; S->err = 0;
+        S->active = 0; S->lock = 0;
+        for (int k = 0; k < 8; k++) S->stats[k] = 0;
+        sh.err = 0;
+    }
 
     // ---- 1. bounding box and quantisation parameters
     {
@@ -773,8 +822,7 @@ static __device__ void hull_cta(const float* __restrict__ pts, int n, char* scra
     // ---- 4. tables
     for (int i = tid; i < C.eh; i += HULL_NT) eset[i] = ~0ull;
     for (int i = tid; i < C.fh; i += HULL_NT) fset[i] = ~0ull;
-    if (tid == 0) { sh.n_faces = 0; sh.n_corners = 0; sh.n_front = 0; sh.n_next = 0; sh.n_big = 0; sh.lexmin = ~0ull; }
-    if (tid < 8) sh.stats[tid] = 0;
+    if (tid == 0) { sh.n_faces = 0; sh.n_corners = 0; sh.lexmin = ~0ull; }
     __syncthreads();
     HullCtx H; H.pts = P4; H.nlo = nlo; H.nhi = nhi; H.obb = obb; H.m = n; H.P = C.P; H.nleaf = C.m_leaves;
 
@@ -865,7 +913,6 @@ static __device__ void hull_cta(const float* __restrict__ pts, int n, char* scra
             if (u >= 0) { if (s_cstart < C.ccap) corners[s_cstart] = v; s_k = 1; }
         }
         __syncthreads();
-        if (tid == 0) sh.stats[3]++;
         for (int guard = 0; guard <= ns + 1; guard++) {
             int cur = s_cur;
             if (tid == 0) {
@@ -925,7 +972,7 @@ static __device__ void hull_cta(const float* __restrict__ pts, int n, char* scra
     };
 
     // ---- 5. first face (cooperative, thread 0 finds the plane)
-    unsigned st_pts = 0, st_cop = 0, st_64 = 0, st_wraps = 0, st_small = 0, st_leaves = 0;
+    unsigned st_pts = 0, st_cop = 0, st_64 = 0;
     if (tid == 0) {
         int c = hull_wrap(H, p0, 0, 0, 1, p0 / HULL_LEAF, st_pts, st_64);
         double nx = 0, ny = 0, nz = 0;
@@ -956,23 +1003,14 @@ static __device__ void hull_cta(const float* __restrict__ pts, int n, char* scra
         s_face_ok = ok;
     }
     __syncthreads();
-    if (!s_face_ok) {
-        if (tid == 0) { *o_nv = 0; *o_nt = 0; if (o_vol) *o_vol = 0.f; }
-        return;                                      // degenerate: collinear input
-    }
+    if (!s_face_ok) return;                          // degenerate: collinear input (no faces, no error)
     coop_face(-1, -1, s_N[0], s_N[1], s_N[2], p0);
 
-    // ---- 6. wrapping: each warp pops a frontier edge (u,v) from a CTA queue,
-    // finds the face across it, and pushes the new face's edges whose twins
-    // are not registered yet.  No CTA-wide rounds; every wait is bounded.
-    const long long t_wrap = clock64();
-    unsigned long long* Q = (unsigned long long*)front0;   // 2*fr_cap slots
-    const int qcap = 2 * C.fr_cap;
-    __shared__ int q_head, q_tail, q_pending;
+    // ---- 6. frontier queue: every edge of the first face whose twin is unknown
     for (int i = tid; i < qcap; i += HULL_NT) Q[i] = ~0ull;
     __syncthreads();
     if (tid == 0) {
-        q_head = 0; q_tail = 0; q_pending = 0;
+        int qt = 0;
         const int nf0 = min(sh.n_faces, C.fcap);
         for (int f = 0; f < nf0; f++) {
             int2 F = faces[f];
@@ -984,158 +1022,270 @@ static __device__ void hull_cta(const float* __restrict__ pts, int n, char* scra
             int2 F = faces[f];
             for (int i = 0; i < F.y; i++) {
                 int u = corners[F.x + i], v = corners[F.x + (i + 1) % F.y];
-                if (!hset_has(eset, C.eh, ekey(v, u)) && q_tail < qcap) { Q[q_tail++] = ekey(u, v); q_pending++; }
+                if (!hset_has(eset, C.eh, ekey(v, u)) && qt < qcap) Q[qt++] = ekey(u, v);
             }
         }
+        S->q_tail = qt; S->q_pending = qt;
+        S->n_faces = sh.n_faces; S->n_corners = sh.n_corners; S->err = sh.err;
+        S->active = (qt > 0 && sh.err == 0) ? 1 : 0;
+        S->stats[4] = (unsigned long long)(clock64() - t_begin);
     }
     __syncthreads();
-    {
-        const int lane = tid & 31, warp = tid >> 5;
-        HullWarp& W = sh.ws[warp];
-        int* Sg = wbuf + (size_t)warp * (2 * (size_t)(n + 2) + 3 * (size_t)C.P);
-        int* Pg = Sg + (n + 2);
-        int* const gq = Pg + (n + 2);                    // global lists: 2P + P ints
-        WarpLists Ls, Lg;
-        Ls.q = sh.wsm[warp]; Ls.leaf = sh.wsm[warp] + HULL_WQ; Ls.qcap = HULL_WQ; Ls.lcap = HULL_WL;
-        Lg.q = gq; Lg.leaf = gq + 2 * C.P; Lg.qcap = 2 * C.P; Lg.lcap = C.P;
-        __syncwarp();
-        for (;;) {
-            int idx = -1;
-            if (lane == 0) {
-                int spin = 0;
-                for (; spin < (1 << 24); spin++) {
-                    int h = *(volatile int*)&q_head, t = *(volatile int*)&q_tail;
-                    if (h < t) {
-                        if (atomicCAS(&q_head, h, h + 1) == h) { idx = h; break; }
-                        continue;
-                    }
-                    if (*(volatile int*)&q_pending == 0 || *(volatile int*)&sh.err) { idx = -2; break; }
-                    __nanosleep(32);
-                }
-                if (idx == -1) { atomicOr(&sh.err, KERR_TIMEOUT); idx = -2; }
-            }
-            idx = __shfl_sync(FULL_MASK, idx, 0);
-            if (idx == -2) break;
-            unsigned long long key = ~0ull;
-            bool skip = false;
-            if (lane == 0) {
-                for (int spin = 0; spin < (1 << 22); spin++) {
-                    key = atomicAdd(&Q[idx], 0ull);
-                    if (key != ~0ull) break;
-                    __nanosleep(32);
-                }
-                if (key == ~0ull) atomicOr(&sh.err, KERR_TIMEOUT);
-                else skip = hset_has(eset, C.eh, ekey((int)(key & 0xffffffffu), (int)(key >> 32)));
-            }
-            key = __shfl_sync(FULL_MASK, key, 0);
-            skip = __shfl_sync(FULL_MASK, skip, 0);
-            if (key != ~0ull && !skip) {
-                const int u = (int)(key >> 32), v = (int)(key & 0xffffffffu);
-                int nl = 0;
-                WarpLists L = Ls;
-                int c = warp_wrap(H, u, v, L, lane, &nl, st_pts, st_64);
-                if (c == -2) {                               // shared lists too small: global ones
-                    L = Lg;
-                    c = warp_wrap(H, u, v, L, lane, &nl, st_pts, st_64);
-                }
-                st_leaves += nl;
-                const float4 pu = P4[u], pv = P4[v];
-                const int dx = (int)(pv.x - pu.x), dy = (int)(pv.y - pu.y), dz = (int)(pv.z - pu.z);
-                int ns = 0;
-                double nx = 0, ny = 0, nz = 0;
-                bool serial = (c == -2);
-                if (serial) {
-                    // the warp queues overflowed: serial search on lane 0
-                    int cc = -1;
-                    if (lane == 0) cc = hull_wrap(H, u, dx, dy, dz, u / HULL_LEAF, st_pts, st_64);
-                    c = __shfl_sync(FULL_MASK, cc, 0);
-                }
-                if (c >= 0) {
-                    float4 pc = P4[c];
-                    double ex = pc.x - pu.x, ey = pc.y - pu.y, ez = pc.z - pu.z;
-                    nx = ey * dz - ez * dy; ny = ez * dx - ex * dz; nz = ex * dy - ey * dx;
-                    if (serial) {
-                        int nn = 0;
-                        if (lane == 0) {
-                            nn = hull_coplanar(H, u, nx, ny, nz, Sg, n, st_cop, st_64);
-                            for (int i = 0; i < nn && i < HULL_SMALL_S; i++) W.S[i] = Sg[i];
-                        }
-                        ns = __shfl_sync(FULL_MASK, nn, 0);
-                        __syncwarp();
-                    } else {
-                        ns = warp_coplanar(H, pu, nx, ny, nz, W, L, nl, lane, HULL_SMALL_S, st_cop, st_64);
-                    }
-                }
-                int k = -1;
-                const int* poly = Pg;
-                if (c >= 0 && ns > HULL_SMALL_S) {
-                    k = warp_big_polygon(H, u, v, nx, ny, nz, L.leaf, serial ? -ns : nl, Sg, Pg, lane, st_cop, st_64);
-                    if (lane == 0) atomicAdd(&sh.stats[7], 1ull);
-                } else if (c >= 0) {
-                    if (lane == 0) {
-                        if (ns == 3) { Pg[0] = v; Pg[1] = u; Pg[2] = c; k = 3; }
-                        else k = hull_small_polygon(H, W.S, ns, nx, ny, nz, v, u, Pg);
-                    }
-                    k = __shfl_sync(FULL_MASK, k, 0);
-                }
-                __syncwarp();
-                // register the face: lane 0 claims it (face key = its smallest
-                // corner and the next one), then the lanes insert its edges and
-                // queue those whose twin is not known yet
-                int fs = -1;
-                if (lane == 0) {
-                    st_wraps++;
-                    if (c < 0 || k < 3) atomicOr(&sh.err, KERR_BT_EXTRACT_FAIL);
-                    else {
-                        int mi = 0;
-                        for (int i = 1; i < k; i++) if (pidx(P4[poly[i]]) < pidx(P4[poly[mi]])) mi = i;
-                        int ins = hset_insert(fset, C.fh, ekey(poly[mi], poly[(mi + 1) % k]));
-                        if (ins == 1) {
-                            st_small++;
-                            int cs = atomicAdd(&sh.n_corners, k);
-                            int f = atomicAdd(&sh.n_faces, 1);
-                            if (cs + k <= C.ccap && f < C.fcap) { faces[f] = make_int2(cs, k); fs = cs; }
-                            else atomicOr(&sh.err, KERR_BT_POOL_EXHAUST);
-                        } else if (ins < 0) atomicOr(&sh.err, KERR_BT_POOL_EXHAUST);
-                    }
-                }
-                fs = __shfl_sync(FULL_MASK, fs, 0);
-                if (fs >= 0) {
-                    for (int i = lane; i < k; i += 32) {
-                        corners[fs + i] = poly[i];
-                        if (hset_insert(eset, C.eh, ekey(poly[i], poly[(i + 1) % k])) < 0)
-                            atomicOr(&sh.err, KERR_BT_POOL_EXHAUST);
-                    }
-                    for (int i = lane; i < k; i += 32) {
-                        int x = poly[i], y = poly[(i + 1) % k];
-                        if (!hset_has(eset, C.eh, ekey(y, x))) {
-                            atomicAdd(&q_pending, 1);
-                            int slot = atomicAdd(&q_tail, 1);
-                            if (slot < qcap) atomicExch(&Q[slot], ekey(x, y));
-                            else { atomicOr(&sh.err, KERR_BT_POOL_EXHAUST); atomicSub(&q_pending, 1); }
-                        }
-                    }
-                }
-            }
-            __syncwarp();
-            if (lane == 0) atomicSub(&q_pending, 1);
-        }
-    }
-    if ((tid & 31) == 0) {
-        atomicAdd(&sh.stats[0], (unsigned long long)st_leaves);
-        atomicAdd(&sh.stats[1], (unsigned long long)st_wraps);
-    }
-    atomicAdd(&sh.stats[3], (unsigned long long)st_pts);
-    __syncthreads();
-    const long long t_out = clock64();
-    if (tid == 0) {
-        sh.stats[2] = (unsigned long long)sh.n_faces;
-        sh.stats[4] = (unsigned long long)(t_wrap - t_begin);
-        sh.stats[5] = (unsigned long long)(t_out - t_wrap);
-    }
+}
 
+#define HULL_SGCAP 4096   // per-warp coplanar set and polygon (ints each); larger faces use the hull's own buffers
+
+// The hull's own buffers Sbuf/posn/ocnt are free while it is being wrapped;
+// a warp that needs them for a large face or a long leaf list takes this
+// lock (bounded wait; a timeout marks the hull failed).
+static __device__ bool hull_lock(HullState* S, int lane)
+{
+    int ok = 0;
+    if (lane == 0) {
+        for (int spin = 0; spin < (1 << 22); spin++) {
+            if (atomicCAS(&S->lock, 0, 1) == 0) { ok = 1; break; }
+            __nanosleep(64);
+        }
+        if (!ok) atomicOr(&S->err, KERR_TIMEOUT);
+        __threadfence();
+    }
+    return __shfl_sync(FULL_MASK, ok, 0) != 0;
+}
+
+static __device__ void hull_unlock(HullState* S, int lane)
+{
+    __syncwarp();
+    if (lane == 0) { __threadfence(); atomicExch(&S->lock, 0); }
+    __syncwarp();
+}
+
+// Wrap about frontier edge (u, v) of hull S and register the face found
+// (whole warp): the first point hit, the face's coplanar points, its
+// polygon; a new face is inserted in the face set, its edges in the edge
+// set, and those whose twin is not known yet go to the frontier queue.
+static __device__ void hull_wrap_edge(HullState* S, int u, int v, HullWarp& W, const WarpLists Ls,
+                                      int* Sg, int* Pg, int lane, unsigned& st_pts, unsigned& st_cop,
+                                      unsigned& st_64)
+{
+    const HullCtx H = hull_ctx(*S);
+    const float4* P4 = H.pts;
+    int nl = 0;
+    WarpLists L = Ls;
+    bool locked = false;
+    int c = warp_wrap(H, u, v, L, lane, &nl, st_pts, st_64);
+    if (c == -2) {                                   // shared lists too small: the hull's own
+        locked = hull_lock(S, lane);
+        if (!locked) return;
+        if (lane == 0) atomicAdd(&S->stats[5], 1ull);
+        L.q = S->ocnt; L.leaf = S->ocnt + 2 * S->P; L.qcap = 2 * S->P; L.lcap = S->P;
+        c = warp_wrap(H, u, v, L, lane, &nl, st_pts, st_64);
+        if (c == -2) {                               // cannot happen: 2P + P hold the whole tree
+            if (lane == 0) atomicOr(&S->err, KERR_BT_WARP_OOM);
+            hull_unlock(S, lane);
+            return;
+        }
+    }
+    if (lane == 0) { atomicAdd(&S->stats[0], (unsigned long long)nl); atomicAdd(&S->stats[1], 1ull); }
+    const float4 pu = P4[u], pv = P4[v];
+    const int dx = (int)(pv.x - pu.x), dy = (int)(pv.y - pu.y), dz = (int)(pv.z - pu.z);
+    int ns = 0;
+    double nx = 0, ny = 0, nz = 0;
+    if (c >= 0) {
+        float4 pc = P4[c];
+        double ex = pc.x - pu.x, ey = pc.y - pu.y, ez = pc.z - pu.z;
+        nx = ey * dz - ez * dy; ny = ez * dx - ex * dz; nz = ex * dy - ey * dx;
+        ns = warp_coplanar(H, pu, nx, ny, nz, W, L, nl, lane, HULL_SMALL_S, st_cop, st_64);
+    }
+    int k = -1;
+    const int* poly = Pg;
+    if (c >= 0 && ns > HULL_SMALL_S) {
+        int* bS = Sg; int* bP = Pg;
+        if (ns + 2 > HULL_SGCAP) {                   // large face: the hull's own buffers
+            if (!locked) { locked = hull_lock(S, lane); if (!locked) return; }
+            if (lane == 0) atomicAdd(&S->stats[6], 1ull);
+            bS = S->Sbuf; bP = S->posn;
+        }
+        k = warp_big_polygon(H, u, v, nx, ny, nz, L.leaf, nl, bS, bP, lane, st_cop, st_64);
+        poly = bP;
+        if (lane == 0) atomicAdd(&S->stats[7], 1ull);
+    } else if (c >= 0) {
+        if (lane == 0) {
+            if (ns == 3) { Pg[0] = v; Pg[1] = u; Pg[2] = c; k = 3; }
+            else k = hull_small_polygon(H, W.S, ns, nx, ny, nz, v, u, Pg);
+        }
+        k = __shfl_sync(FULL_MASK, k, 0);
+    }
+    __syncwarp();
+    // register the face: lane 0 claims it (face key = its smallest corner and
+    // the next one), then the lanes insert its edges and queue the new ones
+    int fs = -1;
+    if (lane == 0) {
+        if (c < 0 || k < 3) atomicOr(&S->err, KERR_BT_EXTRACT_FAIL);
+        else {
+            int mi = 0;
+            for (int i = 1; i < k; i++) if (pidx(P4[poly[i]]) < pidx(P4[poly[mi]])) mi = i;
+            int ins = hset_insert(S->fset, S->fh, ekey(poly[mi], poly[(mi + 1) % k]));
+            if (ins == 1) {
+                int cs = atomicAdd(&S->n_corners, k);
+                int f = atomicAdd(&S->n_faces, 1);
+                if (cs + k <= S->ccap && f < S->fcap) { S->faces[f] = make_int2(cs, k); fs = cs; }
+                else atomicOr(&S->err, KERR_BT_POOL_EXHAUST);
+            } else if (ins < 0) atomicOr(&S->err, KERR_BT_POOL_EXHAUST);
+        }
+    }
+    fs = __shfl_sync(FULL_MASK, fs, 0);
+    if (fs >= 0) {
+        unsigned long long* eset = S->eset;
+        const int eh = S->eh, qcap = S->qcap;
+        for (int i = lane; i < k; i += 32) {
+            S->corners[fs + i] = poly[i];
+            if (hset_insert(eset, eh, ekey(poly[i], poly[(i + 1) % k])) < 0) atomicOr(&S->err, KERR_BT_POOL_EXHAUST);
+        }
+        for (int i = lane; i < k; i += 32) {
+            int x = poly[i], y = poly[(i + 1) % k];
+            if (!hset_has(eset, eh, ekey(y, x))) {
+                atomicAdd(&S->q_pending, 1);
+                int slot = atomicAdd(&S->q_tail, 1);
+                if (slot < qcap) atomicExch(&S->Q[slot], ekey(x, y));
+                else { atomicOr(&S->err, KERR_BT_POOL_EXHAUST); atomicSub(&S->q_pending, 1); }
+            }
+        }
+    }
+    if (locked) hull_unlock(S, lane);
+}
+
+// Persistent wrapping (all HULL_NT threads of every CTA of the grid).  Each
+// CTA has a home hull (h0): the CTAs are shared out over the active hulls in
+// proportion to their point counts, so a hull's BVH and points stay in the
+// L1 of the few SMs that wrap it.  A warp takes frontier edges from its
+// current hull, waits (backing off) while that hull still has edges in
+// flight, and moves to another hull with queued edges once it is done.
+// ctl[0] counts the hulls still wrapping; a hull is done when its last
+// queued edge is done.  Every wait is bounded: ctl[1] collects KERR_TIMEOUT.
+static __device__ void hull_wrap_grid(HullState* states, int n_jobs, int h0, int* ctl, int* wbuf,
+                                      HullWrapShared& sh, int* wsm)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int gw = blockIdx.x * (HULL_NT / 32) + warp;
+    HullWarp& W = sh.ws[warp];
+    int* Sg = wbuf + (size_t)gw * 2 * HULL_SGCAP;
+    int* Pg = Sg + HULL_SGCAP;
+    WarpLists Ls;
+    Ls.q = wsm + (size_t)warp * HULL_WSM; Ls.leaf = Ls.q + HULL_WQ; Ls.qcap = HULL_WQ; Ls.lcap = HULL_WL;
+    unsigned st_pts = 0, st_cop = 0, st_64 = 0;
+    int h = h0;
+    int idle = 0;
+    unsigned nap = 64;
+    for (;;) {
+        int idx = -1;
+        if (lane == 0) {
+            HullState* S = &states[h];
+            if (*(volatile int*)&S->active) {
+                int hd = *(volatile int*)&S->q_head;
+                const int tl = *(volatile int*)&S->q_tail;
+                while (hd < tl) {
+                    int prev = atomicCAS(&S->q_head, hd, hd + 1);
+                    if (prev == hd) { idx = hd; break; }
+                    hd = prev;
+                }
+            }
+        }
+        // lane 0 reads the shared words and broadcasts: every lane takes the
+        // same branch
+        int done = 0, stay = 0;
+        if (lane == 0 && idx < 0) {
+            done = *(volatile int*)&ctl[0] <= 0;
+            stay = *(volatile int*)&states[h].active;
+        }
+        idx = __shfl_sync(FULL_MASK, idx, 0);
+        done = __shfl_sync(FULL_MASK, done, 0);
+        stay = __shfl_sync(FULL_MASK, stay, 0);
+        if (idx < 0) {
+            if (done) break;                                         // every hull is done
+            if (stay) {                                              // edges in flight: stay
+                if (++idle > (1 << 20)) { if (lane == 0) atomicOr(&ctl[1], KERR_TIMEOUT); break; }
+                __nanosleep(nap);
+                nap = min(2 * nap, 2048u);
+                continue;
+            }
+            int found = -1;
+            for (int base = 1; base <= n_jobs && found < 0; base += 32) {   // warp-uniform trip count
+                const int off = base + lane;
+                const int cand = off <= n_jobs ? (h + off) % n_jobs : -1;
+                bool av = false;
+                if (cand >= 0) {
+                    const HullState* C = &states[cand];
+                    av = *(volatile const int*)&C->active &&
+                         *(volatile const int*)&C->q_head < *(volatile const int*)&C->q_tail;
+                }
+                const unsigned b = __ballot_sync(FULL_MASK, av);
+                if (b) found = __shfl_sync(FULL_MASK, cand, __ffs(b) - 1);      // same on every lane
+            }
+            if (found >= 0) { h = found; idle = 0; nap = 64; continue; }
+            if (++idle > (1 << 20)) { if (lane == 0) atomicOr(&ctl[1], KERR_TIMEOUT); break; }
+            __nanosleep(nap);                           // back off: idle warps must not flood L2
+            nap = min(2 * nap, 8192u);
+            continue;
+        }
+        idle = 0; nap = 64;
+        HullState* S = &states[h];
+        unsigned long long key = ~0ull;
+        int skip = 0;
+        if (lane == 0) {
+            for (int spin = 0; spin < (1 << 22); spin++) {
+                key = atomicAdd(&S->Q[idx], 0ull);
+                if (key != ~0ull) break;
+                __nanosleep(32);
+            }
+            if (key == ~0ull) atomicOr(&S->err, KERR_TIMEOUT);
+            else skip = (*(volatile int*)&S->err != 0) ||
+                        hset_has(S->eset, S->eh, ekey((int)(key & 0xffffffffu), (int)(key >> 32)));
+        }
+        key = __shfl_sync(FULL_MASK, key, 0);
+        skip = __shfl_sync(FULL_MASK, skip, 0);
+        if (key != ~0ull && !skip) {
+            const unsigned p0 = st_pts;
+            hull_wrap_edge(S, (int)(key >> 32), (int)(key & 0xffffffffu), W, Ls, Sg, Pg, lane, st_pts, st_cop, st_64);
+            unsigned d = st_pts - p0;
+            #pragma unroll
+            for (int o = 16; o > 0; o >>= 1) d += __shfl_xor_sync(FULL_MASK, d, o);
+            if (lane == 0) atomicAdd(&S->stats[3], (unsigned long long)d);
+        }
+        __syncwarp();
+        if (lane == 0) {
+            if (atomicSub(&S->q_pending, 1) == 1) {                   // this hull is complete
+                atomicExch(&S->active, 0);
+                __threadfence();
+                atomicSub(&ctl[0], 1);
+            }
+        }
+    }
+}
+
+// Output of one wrapped hull (all HULL_NT threads): corners in ascending
+// input index, each face fanned from its smallest corner, triangles grouped
+// by that corner and sorted; FP64 volume.  A hull without faces (fewer than
+// 4 points, or collinear) gives empty output; a failed hull only its error.
+static __device__ void hull_output_cta(const float* __restrict__ pts, const HullState* S, float* out_v, int* out_t,
+                                       int max_hv, int max_ht, int* o_nv, int* o_nt, float* o_vol, int* o_err,
+                                       HullOutShared& sh)
+{
+    const int tid = threadIdx.x;
+    const int n = S->n;
+    const int err0 = S->err;
+    if (n < 4 || S->n_faces == 0 || err0) {          // nothing built, or failed: no buffers touched
+        if (tid == 0) { *o_nv = 0; *o_nt = 0; *o_vol = 0.f; *o_err = err0; }
+        return;
+    }
+    if (tid == 0) *o_err = 0;
+    const float4* P4 = S->P4;
+    const int2* faces = S->faces;
+    const int* corners = S->corners;
+    int* posn = S->posn;
+    int* ocnt = S->ocnt;
+    int* ofill = ocnt + n;
     // ---- 7. canonical output
-    const int nfaces = min(sh.n_faces, C.fcap);
+    const int nfaces = min(S->n_faces, S->fcap);
     // mark corners by input index
     for (int i = tid; i < n; i += HULL_NT) { posn[i] = 0; ocnt[i] = 0; ofill[i] = 0; }
     __syncthreads();
@@ -1180,7 +1330,7 @@ static __device__ void hull_cta(const float* __restrict__ pts, int n, char* scra
         __syncthreads();
     }
     const int nt_out = s_carry;
-    bool fits = nv_out <= out.max_hv && nt_out <= out.max_ht && !sh.err;
+    bool fits = nv_out <= max_hv && nt_out <= max_ht && !err0;
     if (fits) {
         for (int f = tid; f < nfaces; f += HULL_NT) {
             int2 F = faces[f];
@@ -1189,9 +1339,9 @@ static __device__ void hull_cta(const float* __restrict__ pts, int n, char* scra
             int owner = posn[pidx(P4[corners[F.x + mi]])];
             int slot = ocnt[owner] + atomicAdd(&ofill[owner], k - 2);
             for (int i = 1; i + 1 < k; i++, slot++) {
-                out.tris[3 * slot]     = owner;
-                out.tris[3 * slot + 1] = posn[pidx(P4[corners[F.x + (mi + i) % k]])];
-                out.tris[3 * slot + 2] = posn[pidx(P4[corners[F.x + (mi + i + 1) % k]])];
+                out_t[3 * slot]     = owner;
+                out_t[3 * slot + 1] = posn[pidx(P4[corners[F.x + (mi + i) % k]])];
+                out_t[3 * slot + 2] = posn[pidx(P4[corners[F.x + (mi + i + 1) % k]])];
             }
         }
         __syncthreads();
@@ -1199,35 +1349,27 @@ static __device__ void hull_cta(const float* __restrict__ pts, int n, char* scra
         for (int o = tid; o < nv_out; o += HULL_NT) {
             int a = ocnt[o], b = (o + 1 < nv_out) ? ocnt[o + 1] : nt_out;
             for (int i = a + 1; i < b; i++) {
-                int k1 = out.tris[3 * i + 1], k2 = out.tris[3 * i + 2];
+                int k1 = out_t[3 * i + 1], k2 = out_t[3 * i + 2];
                 int j = i - 1;
-                while (j >= a && (out.tris[3 * j + 1] > k1 || (out.tris[3 * j + 1] == k1 && out.tris[3 * j + 2] > k2))) {
-                    out.tris[3 * (j + 1) + 1] = out.tris[3 * j + 1];
-                    out.tris[3 * (j + 1) + 2] = out.tris[3 * j + 2];
+                while (j >= a && (out_t[3 * j + 1] > k1 || (out_t[3 * j + 1] == k1 && out_t[3 * j + 2] > k2))) {
+                    out_t[3 * (j + 1) + 1] = out_t[3 * j + 1];
+                    out_t[3 * (j + 1) + 2] = out_t[3 * j + 2];
                     j--;
                 }
-                out.tris[3 * (j + 1) + 1] = k1; out.tris[3 * (j + 1) + 2] = k2;
+                out_t[3 * (j + 1) + 1] = k1; out_t[3 * (j + 1) + 2] = k2;
             }
         }
         for (int i = tid; i < n; i += HULL_NT) {
             int pos = posn[i];
             if (pos >= 0) {
-                out.verts[3 * pos] = pts[3 * i]; out.verts[3 * pos + 1] = pts[3 * i + 1]; out.verts[3 * pos + 2] = pts[3 * i + 2];
-                if (out.vidx) out.vidx[pos] = i;
+                out_v[3 * pos] = pts[3 * i]; out_v[3 * pos + 1] = pts[3 * i + 1]; out_v[3 * pos + 2] = pts[3 * i + 2];
             }
         }
         __syncthreads();
-        double vol = block_mesh_signed_volume(out.verts, nv_out, out.tris, nt_out, sh.dsh);
-        if (tid == 0) {
-            *o_nv = nv_out; *o_nt = nt_out; if (o_vol) *o_vol = (float)fabs(vol);
-            sh.stats[6] = (unsigned long long)(clock64() - t_out);
-        }
+        double vol = block_mesh_signed_volume(out_v, nv_out, out_t, nt_out, sh.dsh);
+        if (tid == 0) { *o_nv = nv_out; *o_nt = nt_out; *o_vol = (float)fabs(vol); }
     } else {
-        if (tid == 0) {
-            *o_nv = 0; *o_nt = 0; if (o_vol) *o_vol = 0.f;
-            int e = sh.err ? sh.err : KERR_BT_HEAP_OUTPUT;
-            atomicOr(err_word, e);
-        }
+        if (tid == 0) { *o_nv = 0; *o_nt = 0; *o_vol = 0.f; *o_err = err0 ? err0 : KERR_BT_HEAP_OUTPUT; }
     }
     __syncthreads();
 }

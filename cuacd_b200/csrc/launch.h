@@ -35,3 +35,16 @@ void launch_components(const HDSurf* d_meshes, int n, Arena* scratch, Arena* out
 struct gpu_ctx;
 int concave_planes_device(gpu_ctx* ctx, const float* d_v, int nv, const int* d_t, int nt, int K, float eps,
                           float thr, char* scr, size_t cap, float4* out_host, int* out_count, cudaStream_t s);
+
+// hull.cu
+struct HullJob;
+struct HullRes;
+struct HullState;
+size_t hull_wrap_buf_bytes(int n_wrap_ctas);
+int hull_wrap_ctas(long long total_points, int n_sm);
+void launch_hull_jobs(const HullJob* d_jobs, int n_jobs, HullState* d_states, HullRes* d_res, Arena* scratch,
+                      Arena* out, int* d_ctl, int* d_wbuf, int n_wrap_ctas, unsigned long long* d_stats,
+                      cudaStream_t s);
+void launch_jobs_from_offsets(const float* d_pts, const int* d_off, int n, float* d_v, int* d_t, int max_hv,
+                              int max_ht, HullJob* d_jobs, cudaStream_t s);
+void launch_unpack_results(const HullRes* d_res, int n, int* d_nv, int* d_nt, float* d_vol, int* d_err, cudaStream_t s);

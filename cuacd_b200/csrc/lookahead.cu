@@ -16,7 +16,8 @@
 //   4. `depth` expansion levels: level 0 cuts each cutting part with `width`
 //      axis cuts + its edge planes, level d > 0 cuts the worst part of every
 //      surviving item with `width2` axis cuts (la_expand.cu:65-340); every new
-//      fragment gets its volume and exact hull (la_hull, :357-424); the item
+//      fragment gets its volume and exact hull (la_hull, :357-424; the
+//      batched hull pipeline of hull.cu); the item
 //      records its worst rv cost per level (la_sort_and_record,
 //      la_refine.cu:359-409); a part too small on every axis ends its branch
 //      as a leaf padded with zero costs (la_expand.cu:155-174);
@@ -25,8 +26,9 @@
 //      (la_evaluate, la_refine.cu:418-527);
 //   6. the part is replaced by the two halves of its winning level-0 item
 //      (la_apply_cuts, la_lifecycle.cu:151-261), whose hulls are already known.
-// Cuts and hulls run as device jobs in waves: fragments go to an output arena
-// kept for the iteration, scratch to a second arena reset between waves.
+// Cuts and hulls run as device jobs in waves: fragments and hulls go to an
+// output arena kept for the iteration, scratch to a second arena reset
+// between waves.
 // The branch-and-bound pruning of the last level (la_hull's rough-hull bound)
 // only skips provably dominated items and is not needed for the result; the
 // quick levels (quick_depth) and the merge-hulls post-pass are not part of
@@ -49,11 +51,7 @@ struct CutJob {
     int axis, slice, cpa, _pad;     // axis >= 0: axis-aligned cut computed on the part's bbox
 };
 
-struct FragRes {                    // per fragment: hull + volumes
-    float* hv; int* ht; int hnv, hnt;
-    double mesh_vol;
-    float hull_vol; int err;
-};
+typedef HullRes FragRes;            // per fragment: hull + volumes
 
 __global__ void __launch_bounds__(CUT_NT)
 k_cut_jobs(const CutJob* __restrict__ jobs, int j0, int j1, Arena* scratch, Arena* out, float min_edge_dist,
@@ -110,67 +108,34 @@ k_cut_jobs(const CutJob* __restrict__ jobs, int j0, int j1, Arena* scratch, Aren
     cut_cta(J.v, J.nv, J.t, J.nt, p.x, p.y, p.z, p.w, scratch, none, &res[j], sh, out);
 }
 
-// Hull + mesh volume of one fragment into *dst (whole CTA).  Hull scratch
-// from `scratch`, hull vertices/triangles from `out`.
-static __device__ void frag_hull_cta(const float* v, int nv, const int* t, int nt, bool empty,
-                                     Arena* scratch, Arena* out, FragRes* dst, HullShared& sh)
+// Hull jobs for fragments f0..f1 (2 per cut, empty when the cut produced
+// no split) into jobs[f - f0].
+__global__ void k_cut_frag_jobs(const CutResult* __restrict__ cuts, int f0, int f1, HullJob* jobs)
 {
-    __shared__ char* s_scr;
-    __shared__ float* s_ov;
-    __shared__ int* s_ot;
-    __shared__ int s_err, s_nv, s_nt;
-    __shared__ float s_vol;
-    if (threadIdx.x == 0) {
-        s_err = 0; s_scr = nullptr; s_ov = nullptr; s_ot = nullptr;
-        if (!empty) {
-            s_scr = (char*)arena_alloc(scratch, hull_scratch_bytes(nv), &s_err);
-            s_ov = (float*)arena_alloc(out, 12ull * nv, &s_err);
-            s_ot = (int*)arena_alloc(out, 12ull * (2 * nv + 4), &s_err);
-        }
-    }
-    __syncthreads();
-    FragRes F;
-    memset(&F, 0, sizeof(F));
-    if (empty || s_err || !s_scr || !s_ov || !s_ot) {
-        if (threadIdx.x == 0) { F.err = s_err; *dst = F; }
-        return;
-    }
-    double mv = block_mesh_signed_volume(v, nv, t, nt, sh.dsh);
-    HullOut o; o.verts = s_ov; o.tris = s_ot; o.vidx = nullptr; o.max_hv = nv; o.max_ht = 2 * nv + 4;
-    hull_cta(v, nv, s_scr, o, &s_nv, &s_nt, &s_vol, &s_err, sh);
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        F.hv = s_ov; F.ht = s_ot; F.hnv = s_nv; F.hnt = s_nt;
-        F.mesh_vol = fabs(mv); F.hull_vol = s_vol; F.err = s_err;
-        *dst = F;
-    }
-}
-
-// Hull + volume of fragment f (2 per job), fragments f0..f1 of this wave.
-__global__ void __launch_bounds__(HULL_NT)
-k_hull_jobs(const CutResult* __restrict__ cuts, int f0, int f1, Arena* scratch, Arena* out, FragRes* frags)
-{
-    __shared__ HullShared sh;
-    const int f = f0 + blockIdx.x;
+    const int f = f0 + blockIdx.x * blockDim.x + threadIdx.x;
     if (f >= f1) return;
     const CutResult& C = cuts[f >> 1];
     const int side = f & 1;
-    const float* v = side ? C.nv : C.pv;
-    const int* t = side ? C.nt : C.pt;
-    const int nv = side ? C.nnv : C.npv, nt = side ? C.nnt : C.npt;
-    const bool empty = C.err != 0 || nv <= 0 || nt <= 0 || C.npv <= 0 || C.nnv <= 0;
-    frag_hull_cta(v, nv, t, nt, empty, scratch, out, &frags[f], sh);
+    const bool empty = C.err != 0 || C.npv <= 0 || C.nnv <= 0;
+    HullJob J;
+    memset(&J, 0, sizeof(J));
+    if (!empty) {
+        J.pts = side ? C.nv : C.pv; J.n = side ? C.nnv : C.npv;
+        J.tris = side ? C.nt : C.pt; J.nt = side ? C.nnt : C.npt;
+    }
+    jobs[f - f0] = J;
 }
 
-// Hull + volume of meshes f0..f1 (connected components of split parts).
-__global__ void __launch_bounds__(HULL_NT)
-k_hull_surfs(const HDSurf* __restrict__ meshes, int f0, int f1, Arena* scratch, Arena* out, FragRes* frags)
+// Hull jobs for meshes f0..f1 (connected components of split parts).
+__global__ void k_surf_jobs(const HDSurf* __restrict__ meshes, int f0, int f1, HullJob* jobs)
 {
-    __shared__ HullShared sh;
-    const int f = f0 + blockIdx.x;
+    const int f = f0 + blockIdx.x * blockDim.x + threadIdx.x;
     if (f >= f1) return;
     const HDSurf m = meshes[f];
-    frag_hull_cta(m.v, m.nv, m.t, m.nt, m.nv <= 0 || m.nt <= 0, scratch, out, &frags[f], sh);
+    HullJob J;
+    memset(&J, 0, sizeof(J));
+    if (m.nv > 0 && m.nt > 0) { J.pts = m.v; J.n = m.nv; J.tris = m.t; J.nt = m.nt; }
+    jobs[f - f0] = J;
 }
 
 __global__ void k_mesh_volumes(const HDSurf* meshes, int n, double* out)
@@ -240,6 +205,32 @@ struct Lookahead {
     HDSurf* d_surfs = nullptr; int surf_cap = 0;
     CompResult* d_cres = nullptr;
     FragRes* d_frags = nullptr; int frag_cap = 0;
+    // hull pipeline: jobs/states (frag_cap each), control words, wrap lists
+    HullJob* d_hjobs = nullptr; HullState* d_hstates = nullptr; int* d_hctl = nullptr; int* d_wbuf = nullptr;
+    int nwc = 1; size_t wbuf_bytes = 0;
+
+    // Hulls of jobs [0, n) already in d_hjobs, results into res[0, n); waves
+    // keep the per-hull scratch within the scratch arena.
+    int run_hulls(const std::vector<int>& sizes, FragRes* res)
+    {
+        const int n = (int)sizes.size();
+        int f = 0;
+        while (f < n) {
+            size_t acc = 0; int f1 = f;
+            while (f1 < n) {
+                size_t e = al256(hull_scratch_bytes(sizes[f1] > 4 ? sizes[f1] : 4)) + 256;
+                if (f1 > f && acc + e > scr_cap) break;
+                acc += e; f1++;
+            }
+            reset_scr();
+            launch_hull_jobs(d_hjobs + f, f1 - f, d_hstates + f, res + f, d_scr, d_out, d_hctl, d_wbuf, nwc,
+                             nullptr, s);
+            ctx->launches += 5;
+            f = f1;
+        }
+        CK(cudaGetLastError());
+        return 0;
+    }
 
     void reset_out() { launch_arena_reset(d_out, out_base, out_cap, s); }
     void reset_scr() { launch_arena_reset(d_scr, scr_base, scr_cap, s); }
@@ -271,23 +262,17 @@ struct Lookahead {
         CK(cudaMemcpyAsync(cuts.data(), d_cuts, sizeof(CutResult) * n, cudaMemcpyDeviceToHost, s));
         CK(cudaStreamSynchronize(s));
         for (auto& c : cuts) if (c.err & (KERR_HEAP_OOM | KERR_PC_SCRATCH_OOM | KERR_PC_POOL_OOM)) return KERR_HEAP_OOM;
-        // hull waves by exact fragment sizes
-        int f = 0;
-        while (f < 2 * n) {
-            size_t acc = 0; int f1 = f;
-            while (f1 < 2 * n) {
-                const CutResult& c = cuts[f1 >> 1];
-                int fv = (f1 & 1) ? c.nnv : c.npv;
-                size_t e = hull_scratch_bytes(fv > 0 ? fv : 1) + 4096;
-                if (f1 > f && acc + e > scr_cap) break;
-                acc += e; f1++;
-            }
-            reset_scr();
-            k_hull_jobs<<<f1 - f, HULL_NT, 0, s>>>(d_cuts, f, f1, d_scr, d_out, d_fr);
-            ctx->launches += 2;
-            f = f1;
+        // hulls of all fragments (exact sizes known now)
+        std::vector<int> sizes(2 * n);
+        for (int f = 0; f < 2 * n; f++) {
+            const CutResult& c = cuts[f >> 1];
+            const bool empty = c.err != 0 || c.npv <= 0 || c.nnv <= 0;
+            sizes[f] = empty ? 0 : ((f & 1) ? c.nnv : c.npv);
         }
-        CK(cudaGetLastError());
+        k_cut_frag_jobs<<<(2 * n + 127) / 128, 128, 0, s>>>(d_cuts, 0, 2 * n, d_hjobs);
+        ctx->launches += 1;
+        int rh = run_hulls(sizes, d_fr);
+        if (rh) return rh;
         CK(cudaMemcpyAsync(frags.data(), d_fr, sizeof(FragRes) * 2 * n, cudaMemcpyDeviceToHost, s));
         CK(cudaStreamSynchronize(s));
         for (auto& r : frags) if (r.err & (KERR_HEAP_OOM | KERR_BT_POOL_EXHAUST)) return KERR_HEAP_OOM;
@@ -364,20 +349,12 @@ int Lookahead::split_components(std::vector<HPart>& parts, const std::vector<int
             std::vector<HDSurf> hs(cn);
             for (int k = 0; k < cn; k++) hs[k] = {comps[c0 + k].v, comps[c0 + k].t, comps[c0 + k].nv, comps[c0 + k].nt};
             CK(cudaMemcpyAsync(d_surfs, hs.data(), sizeof(HDSurf) * cn, cudaMemcpyHostToDevice, s));
-            int f = 0;
-            while (f < cn) {
-                size_t acc = 0; int f1 = f;
-                while (f1 < cn) {
-                    size_t e = hull_scratch_bytes(hs[f1].nv > 0 ? hs[f1].nv : 1) + 4096;
-                    if (f1 > f && acc + e > scr_cap) break;
-                    acc += e; f1++;
-                }
-                reset_scr();
-                k_hull_surfs<<<f1 - f, HULL_NT, 0, s>>>(d_surfs, f, f1, d_scr, d_out, d_frags);
-                ctx->launches += 2;
-                f = f1;
-            }
-            CK(cudaGetLastError());
+            k_surf_jobs<<<(cn + 127) / 128, 128, 0, s>>>(d_surfs, 0, cn, d_hjobs);
+            ctx->launches += 1;
+            std::vector<int> sizes(cn);
+            for (int k = 0; k < cn; k++) sizes[k] = hs[k].nv;
+            int rh = run_hulls(sizes, d_frags);
+            if (rh) return rh;
             CK(cudaMemcpyAsync(fr.data() + c0, d_frags, sizeof(FragRes) * cn, cudaMemcpyDeviceToHost, s));
             CK(cudaStreamSynchronize(s));
         }
@@ -450,11 +427,14 @@ extern "C" int lookahead_decompose(gpu_ctx_t ctx, const float* verts, int nv, co
     size_t mesh_bytes = 12 * ((size_t)nv + nt);
     size_t max_jobs = (size_t)max_n_cutting * tw_max;
     for (int d = 1; d < depth; d++) max_jobs *= width2;
+    const size_t hjob_cap = std::max<size_t>(2 * max_jobs, 2 * 4096);
     size_t fixed = al256(sizeof(CutJob) * max_jobs) + al256(sizeof(CutResult) * max_jobs) + al256(sizeof(FragRes) * 2 * max_jobs)
                  + al256(2 * sizeof(Arena)) + al256(mesh_bytes) + al256(12 * ((size_t)hull_nv + hull_nt))
                  + al256(sizeof(HDSurf) * 2 * 4096) + al256(sizeof(HDPrep) * 2 * 4096) + al256(hd_dir_bytes() * 2 * 4096)
                  + al256(64) + al256(sizeof(float) * 2 * 4096) + al256(sizeof(double) * 4096)
-                 + al256(sizeof(CompResult) * 2 * 4096);
+                 + al256(sizeof(CompResult) * 2 * 4096)
+                 + al256(sizeof(HullJob) * hjob_cap) + al256(sizeof(HullState) * hjob_cap) + al256(64)
+                 + al256(hull_wrap_buf_bytes(hull_wrap_ctas(1LL << 40, ctx->n_sm)));
     size_t out_cap = std::max<size_t>((size_t)1 << 30, 8 * mesh_bytes * std::min<size_t>(max_jobs, 512));
     size_t scr_cap = std::max<size_t>((size_t)2 << 30, hull_scratch_bytes(nv) * 64);
     int rc = pool_begin(ctx, fixed + out_cap + scr_cap + (1 << 20));
@@ -474,6 +454,10 @@ extern "C" int lookahead_decompose(gpu_ctx_t ctx, const float* verts, int nv, co
     float* d_pmax = pool_take<float>(ctx, 2 * 4096);
     double* d_vols = pool_take<double>(ctx, 4096);
     CompResult* d_cres = pool_take<CompResult>(ctx, 2 * 4096);
+    HullJob* d_hjobs = pool_take<HullJob>(ctx, hjob_cap);
+    HullState* d_hstates = pool_take<HullState>(ctx, hjob_cap);
+    int* d_hctl = pool_take<int>(ctx, 16);
+    int* d_wbuf = (int*)pool_take<char>(ctx, hull_wrap_buf_bytes(hull_wrap_ctas(1LL << 40, ctx->n_sm)));
     char* out_base = pool_take<char>(ctx, out_cap);
     char* scr_base = pool_take<char>(ctx, scr_cap);
     if (!scr_base) return ctx_fail(ctx, KERR_HEAP_OOM, "pool carve failed");
@@ -483,6 +467,7 @@ extern "C" int lookahead_decompose(gpu_ctx_t ctx, const float* verts, int nv, co
     L.min_edge = std::min(threshold * 0.25f, 0.015f);
     L.d_surfs = d_surfs; L.surf_cap = 2 * 4096; L.d_cres = d_cres;
     L.d_frags = d_frags; L.frag_cap = (int)std::min<size_t>(2 * max_jobs, 1 << 30);
+    L.d_hjobs = d_hjobs; L.d_hstates = d_hstates; L.d_hctl = d_hctl; L.d_wbuf = d_wbuf; L.nwc = hull_wrap_ctas(1LL << 40, ctx->n_sm);
     CK(cudaMemcpyAsync(d_v0, verts, 12 * (size_t)nv, cudaMemcpyHostToDevice, s));
     CK(cudaMemcpyAsync(d_t0, tris, 12 * (size_t)nt, cudaMemcpyHostToDevice, s));
     if (hull_nv) CK(cudaMemcpyAsync(d_hv0, hull_verts, 12 * (size_t)hull_nv, cudaMemcpyHostToDevice, s));

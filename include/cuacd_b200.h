@@ -218,9 +218,10 @@ int cuacd_hull_batch_device(gpu_ctx_t ctx, const float* d_pts,
                             int* d_out_errors, void* stream);
 
 /* Diagnostic: exact hulls of a batch of clouds (host pointers) with the
- * hull kernel's work counters, 8 per cloud: BVH leaves kept by the wraps,
+ * hull kernels' work counters, 8 per cloud: BVH leaves kept by the wraps,
  * wraps, faces, points tested by the wraps, SM cycles spent in set-up (sort,
- * BVH, first face), in wrapping and in output, large faces. */
+ * BVH, first face), wraps that needed the cloud's own node lists, faces
+ * built in the cloud's own buffers, large faces. */
 int cuacd_hull_stats(gpu_ctx_t ctx, const float* pts, int total_pts,
                      const int* offsets, int n_hulls, int* out_nv, int* out_nt,
                      float* out_vol, unsigned long long* out_stats);
