@@ -52,3 +52,50 @@ static __device__ __forceinline__ int lower_bound_u64(const unsigned long long* 
     while (lo < hi) { int m = (lo + hi) >> 1; if (a[m] < k) lo = m + 1; else hi = m; }
     return lo;
 }
+
+// Stable LSD radix sort of n 64-bit keys by bits [lo_bit, lo_bit + nbits),
+// 8 bits per pass (whole CTA of NT threads).  `tmp` holds n keys; the
+// result is in `keys`.  `cnt` needs 256 * NT/32 ints of shared memory, `sh`
+// 34 ints.  Per pass: per-warp digit counts over contiguous segments, one
+// CTA scan (digit-major, warp-minor), then a stable scatter ranked with
+// __match_any_sync inside each 32-key chunk.
+template <int NT>
+static __device__ void cta_radix_sort_u64(unsigned long long* keys, unsigned long long* tmp, int n, int lo_bit,
+                                          int nbits, int* cnt, int* sh)
+{
+    constexpr int NW = NT / 32;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int seg = (n + NW - 1) / NW;
+    const int b = min(n, w * seg), e = min(n, b + seg);
+    unsigned long long* src = keys;
+    unsigned long long* dst = tmp;
+    int passes = 0;
+    for (int s = lo_bit; s < lo_bit + nbits; s += 8) {
+        for (int c = threadIdx.x; c < 256 * NW; c += NT) cnt[c] = 0;
+        __syncthreads();
+        for (int i = b + lane; i < e; i += 32) atomicAdd(&cnt[(int)((src[i] >> s) & 255ull) * NW + w], 1);
+        __syncthreads();
+        cta_scan_inplace(cnt, 256 * NW, sh);
+        for (int base = b; base < e; base += 32) {          // warp-uniform trip count
+            const int i = base + lane;
+            unsigned long long k = 0;
+            int d = -1;
+            if (i < e) { k = src[i]; d = (int)((k >> s) & 255ull); }
+            const unsigned m = __match_any_sync(FULL_MASK, d);
+            const int rank = __popc(m & ((1u << lane) - 1u));
+            int p = 0;
+            if (d >= 0) p = cnt[d * NW + w] + rank;
+            __syncwarp();
+            if (d >= 0 && rank == 0) cnt[d * NW + w] += __popc(m);
+            __syncwarp();
+            if (d >= 0) dst[p] = k;
+        }
+        __syncthreads();
+        unsigned long long* t = src; src = dst; dst = t;
+        passes++;
+    }
+    if (passes & 1) {
+        for (int i = threadIdx.x; i < n; i += NT) keys[i] = src[i];
+        __syncthreads();
+    }
+}

@@ -6,7 +6,7 @@
 #include "launch.h"
 
 // One CTA per surface: budget, offsets, BVH.  Scratch from the arena.
-__global__ void __launch_bounds__(HD_NT)
+__global__ void __launch_bounds__(HD_PREP_NT)
 k_hd_prep(const HDSurf* __restrict__ surfs, int n_surf, Arena* arena, float resolution, int min_samples,
           int total_override, HDPrep* preps, int* err)
 {
@@ -111,7 +111,7 @@ void launch_hausdorff_stages(const HDSurf* d_surfs, int n_pairs, Arena* arena, f
                              int total, HDPrep* d_preps, void* d_dirs, int* d_i2, float* d_pmax, int* d_err,
                              int n_sm, cudaStream_t s, const std::function<void(int)>& after)
 {
-    if (n_pairs > 0) k_hd_prep<<<2 * n_pairs, HD_NT, 0, s>>>(d_surfs, 2 * n_pairs, arena, resolution, min_samples, total, d_preps, d_err);
+    if (n_pairs > 0) k_hd_prep<<<2 * n_pairs, HD_PREP_NT, 0, s>>>(d_surfs, 2 * n_pairs, arena, resolution, min_samples, total, d_preps, d_err);
     after(0);
     if (n_pairs > 0) k_hd_plan<<<1, 32, 0, s>>>(d_surfs, d_preps, n_pairs, (HDDir*)d_dirs, d_i2, d_i2 + 1, d_pmax);
     after(1);

@@ -30,6 +30,7 @@
 #include "cta_util.cuh"
 
 #define HD_NT     256
+#define HD_PREP_NT 1024           // threads of the per-surface prep CTA
 #define HD_LEAF   4
 #define HD_CHUNK  1024
 #define HD_STACK  48
@@ -195,13 +196,14 @@ __host__ __device__ inline size_t hd_prep_bytes(int nt)
 
 struct HDShared {
     int scan[34];
-    long long fx[HD_NT / 32];
-    float bb[6][HD_NT / 32];
+    long long fx[HD_PREP_NT / 32];
+    float bb[6][HD_PREP_NT / 32];
     float lo[3], hi[3];
     long long fxsum;
+    int cnt[256 * (HD_PREP_NT / 32)];     // radix-sort digit counts
 };
 
-// Prep one surface.  All HD_NT threads call.
+// Prep one surface.  All HD_PREP_NT threads call.
 static __device__ void hd_prep_cta(HDSurf S, char* scratch, float resolution, int min_samples, int total_override,
                             HDPrep* out, HDShared& sh)
 {
@@ -223,7 +225,7 @@ static __device__ void hd_prep_cta(HDSurf S, char* scratch, float resolution, in
     // ---- areas (fixed point) and bbox of the triangles' vertices
     long long fx = 0;
     float lo[3] = {3.4e38f, 3.4e38f, 3.4e38f}, hi[3] = {-3.4e38f, -3.4e38f, -3.4e38f};
-    for (int t = tid; t < nt; t += HD_NT) {
+    for (int t = tid; t < nt; t += HD_PREP_NT) {
         int a = S.t[3 * t], b = S.t[3 * t + 1], c = S.t[3 * t + 2];
         float ar = hd_area(S.v, a, b, c);
         fx += __double2ll_rn(ldexp((double)ar, 36));
@@ -237,11 +239,11 @@ static __device__ void hd_prep_cta(HDSurf S, char* scratch, float resolution, in
     __syncthreads();
     if (tid == 0) {
         long long s = 0;
-        for (int i = 0; i < HD_NT / 32; i++) s += sh.fx[i];
+        for (int i = 0; i < HD_PREP_NT / 32; i++) s += sh.fx[i];
         sh.fxsum = s;
         for (int k = 0; k < 3; k++) {
             float a = 3.4e38f, b = -3.4e38f;
-            for (int i = 0; i < HD_NT / 32; i++) { a = fminf(a, sh.bb[k][i]); b = fmaxf(b, sh.bb[3 + k][i]); }
+            for (int i = 0; i < HD_PREP_NT / 32; i++) { a = fminf(a, sh.bb[k][i]); b = fmaxf(b, sh.bb[3 + k][i]); }
             sh.lo[k] = a; sh.hi[k] = b;
         }
     }
@@ -251,7 +253,7 @@ static __device__ void hd_prep_cta(HDSurf S, char* scratch, float resolution, in
     if (res < min_samples) res = min_samples;
     float area = (float)total;
     // ---- per-triangle counts -> offsets
-    for (int t = tid; t < nt; t += HD_NT) {
+    for (int t = tid; t < nt; t += HD_PREP_NT) {
         int a = S.t[3 * t], b = S.t[3 * t + 1], c = S.t[3 * t + 2];
         P.offsets[t] = hd_tri_count(hd_area(S.v, a, b, c), t, nt, res, area);
     }
@@ -261,7 +263,7 @@ static __device__ void hd_prep_cta(HDSurf S, char* scratch, float resolution, in
     // ---- Morton order of centroids
     float ext[3], inv[3];
     for (int k = 0; k < 3; k++) { ext[k] = sh.hi[k] - sh.lo[k]; inv[k] = ext[k] > 0.f ? 1023.0f / ext[k] : 0.f; }
-    for (int t = tid; t < nt; t += HD_NT) {
+    for (int t = tid; t < nt; t += HD_PREP_NT) {
         int a = S.t[3 * t], b = S.t[3 * t + 1], c = S.t[3 * t + 2];
         unsigned m = 0;
         unsigned q[3];
@@ -274,10 +276,12 @@ static __device__ void hd_prep_cta(HDSurf S, char* scratch, float resolution, in
         P.keys[t] = ((unsigned long long)m << 32) | (unsigned)t;
     }
     __syncthreads();
-    cta_sort_u64(P.keys, nt);
+    // stable radix sort by the 30-bit code (bits 32..61); the leaf triangle
+    // array (48 bytes per slot, written below) is its second buffer
+    cta_radix_sort_u64<HD_PREP_NT>(P.keys, (unsigned long long*)P.tri, nt, 32, 30, sh.cnt, sh.scan);
     // ---- triangles in leaf order; empty slots become far-away degenerate points
     const int nslot = P.nleaf * HD_LEAF;
-    for (int i = tid; i < nslot; i += HD_NT) {
+    for (int i = tid; i < nslot; i += HD_PREP_NT) {
         float4 A, B, C;
         if (i < nt) {
             int t = (int)(P.keys[i] & 0xffffffffu);
@@ -292,7 +296,7 @@ static __device__ void hd_prep_cta(HDSurf S, char* scratch, float resolution, in
     }
     __syncthreads();
     // ---- leaf boxes, then internal nodes holding both child boxes
-    for (int l = tid; l < P.P; l += HD_NT) {
+    for (int l = tid; l < P.P; l += HD_PREP_NT) {
         float4 blo = make_float4(3.4e38f, 3.4e38f, 3.4e38f, 0.f), bhi = make_float4(-3.4e38f, -3.4e38f, -3.4e38f, 0.f);
         if (l < P.nleaf) {
             for (int j = 0; j < HD_LEAF; j++) {
@@ -311,7 +315,7 @@ static __device__ void hd_prep_cta(HDSurf S, char* scratch, float resolution, in
     // node n (1 <= n < P) children 2n, 2n+1; boxes of level below live in
     // lbox (leaves) or in the parents' child slots already written.
     for (int width = P.P >> 1; width >= 1; width >>= 1) {
-        for (int j = tid; j < width; j += HD_NT) {
+        for (int j = tid; j < width; j += HD_PREP_NT) {
             int n = width + j;
             int cl = 2 * n, cr = 2 * n + 1;
             float4 llo, lhi, rlo, rhi;
