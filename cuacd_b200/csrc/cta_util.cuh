@@ -4,20 +4,49 @@
 #include "common.cuh"
 
 // In-place exclusive scan of n ints (any n), whole CTA.  Returns the total.
-// `sh` needs 34 ints of shared memory.
+// `sh` needs 34 ints of shared memory.  Each warp owns a contiguous segment:
+// pass 1 sums it, one CTA scan of the warp sums gives the segment offsets,
+// pass 2 scans the segment 32 values at a time with a running carry, so the
+// CTA meets three barriers whatever n is.
 static __device__ int cta_scan_inplace(int* data, int n, int* sh)
 {
-    int carry = 0;
-    for (int base = 0; base < n; base += blockDim.x) {
-        int i = base + threadIdx.x;
-        int v = (i < n) ? data[i] : 0;
-        int tot;
-        int ex = block_exclusive_scan(v, sh, &tot);
-        if (i < n) data[i] = carry + ex;
-        carry += tot;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    const int seg = ((n + nw - 1) / nw + 31) & ~31;
+    const int b = min(n, w * seg), e = min(n, b + seg);
+    int sum = 0;
+    for (int i = b + lane; i < e; i += 32) sum += data[i];
+    #pragma unroll
+    for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(FULL_MASK, sum, o);
+    __syncthreads();                                   // sh may still be in use by the caller
+    if (lane == 0) sh[w] = sum;
+    __syncthreads();
+    if (w == 0) {
+        int v = lane < nw ? sh[lane] : 0, x = v;
+        #pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int y = __shfl_up_sync(FULL_MASK, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane < nw) sh[lane] = x - v;               // exclusive segment offsets
+        if (lane == 31) sh[32] = x;                    // total
     }
     __syncthreads();
-    return carry;
+    int carry = sh[w];
+    const int total = sh[32];
+    for (int base = b; base < e; base += 32) {         // warp-uniform trip count
+        const int i = base + lane;
+        const int v = i < e ? data[i] : 0;
+        int x = v;
+        #pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int y = __shfl_up_sync(FULL_MASK, x, o);
+            if (lane >= o) x += y;
+        }
+        if (i < e) data[i] = carry + x - v;
+        carry += __shfl_sync(FULL_MASK, x, 31);
+    }
+    __syncthreads();
+    return total;
 }
 
 // Bitonic sort of keys[0..n) ascending; the array must hold next_pow2(n)

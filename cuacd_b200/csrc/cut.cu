@@ -1,5 +1,6 @@
 // cut.cu — plane-cut kernels (built with -fmad=false, see cut.cuh) and the
 // gpu_test_plane_cut entry point.
+#include <vector>
 #include "context.cuh"
 #include "cut.cuh"
 #include "launch.h"
@@ -15,7 +16,7 @@ k_cut_one(const float* __restrict__ v, int nv, const int* __restrict__ t, int nt
 
 // Many planes on one mesh; fragments go to the arena.  Degenerate planes
 // (all-zero normal) produce an empty result.
-__global__ void __launch_bounds__(CUT_NT)
+__global__ void __launch_bounds__(CUT_NT, 1)
 k_cut_planes(const float* __restrict__ v, int nv, const int* __restrict__ t, int nt,
              const float4* __restrict__ planes, int n_planes, Arena* arena, CutResult* res)
 {
@@ -95,5 +96,47 @@ extern "C" int gpu_test_plane_cut(gpu_ctx_t ctx, const float* vertices, int n_ve
     if (r.nnv) CK(cudaMemcpy(out_neg_verts, r.nv, 12 * (size_t)r.nnv, cudaMemcpyDeviceToHost));
     if (r.nnt) CK(cudaMemcpy(out_neg_tris, r.nt, 12 * (size_t)r.nnt, cudaMemcpyDeviceToHost));
     *out_n_pv = r.npv; *out_n_pt = r.npt; *out_n_nv = r.nnv; *out_n_nt = r.nnt;
+    return 0;
+}
+
+// Diagnostic: cut one mesh by n planes (k_cut_planes, fragments into the
+// arena) and report per plane 8 ints: crossing edges, boundary edges, loops,
+// cap triangles, then SM cycles / 64 of the crossing, split, boundary and
+// cap+output phases.
+extern "C" int cuacd_cut_stats(gpu_ctx_t ctx, const float* verts, int nv, const int* tris, int nt,
+                               const float* planes, int n_planes, int* out_stats)
+{
+    if (!ctx) return -1;
+    if (n_planes <= 0) return 0;
+    if (nv <= 0 || nt <= 0) return ctx_fail(ctx, KERR_MESH_INVALID, "empty mesh");
+    for (int i = 0; i < 3 * nt; i++)
+        if (tris[i] < 0 || tris[i] >= nv) return ctx_fail(ctx, KERR_MESH_INVALID, "triangle index out of range");
+    CK(cudaSetDevice(ctx->device));
+    size_t need = al256(12 * (size_t)nv) + al256(12 * (size_t)nt) + al256(16 * (size_t)n_planes)
+                + al256(sizeof(CutResult) * (size_t)n_planes) + cut_scratch_bytes(nv, nt) * (size_t)n_planes;
+    int rc = pool_begin(ctx, need);
+    if (rc) return rc;
+    float* d_v = pool_take<float>(ctx, 3 * (size_t)nv);
+    int* d_t = pool_take<int>(ctx, 3 * (size_t)nt);
+    float4* d_p = pool_take<float4>(ctx, n_planes);
+    CutResult* d_res = pool_take<CutResult>(ctx, n_planes);
+    if (!d_res) return ctx_fail(ctx, KERR_HEAP_OOM, "pool carve failed");
+    cudaStream_t s = ctx->stream;
+    CK(cudaMemcpyAsync(d_v, verts, 12 * (size_t)nv, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(d_t, tris, 12 * (size_t)nt, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(d_p, planes, 16 * (size_t)n_planes, cudaMemcpyHostToDevice, s));
+    launch_arena_reset(ctx->d_arena, ctx->pool + ctx->carve, ctx->cap - ctx->carve, s);
+    launch_cut_planes(d_v, nv, d_t, nt, d_p, n_planes, ctx->d_arena, d_res, s);
+    ctx->launches += 2;
+    CK(cudaGetLastError());
+    std::vector<CutResult> r(n_planes);
+    CK(cudaMemcpyAsync(r.data(), d_res, sizeof(CutResult) * n_planes, cudaMemcpyDeviceToHost, s));
+    rc = sync_and_check(ctx, "cut_stats");
+    if (rc) return rc;
+    for (int i = 0; i < n_planes; i++) {
+        int* o = out_stats + 8 * i;
+        o[0] = r[i].n_cross; o[1] = r[i].n_boundary; o[2] = r[i].n_loops; o[3] = r[i].n_cap;
+        for (int k = 0; k < 4; k++) o[4 + k] = (int)r[i].cyc[k];
+    }
     return 0;
 }

@@ -39,6 +39,7 @@ struct CutResult {
     int err;
     int flags;                             // CUT_FLAG_* (set by callers that skip the cut)
     int _pad;
+    unsigned cyc[4];                       // SM cycles / 64: crossings, split, boundary, caps + output
 };
 
 #define CUT_FLAG_SMALL   1    // the part is too small on every axis to be cut
@@ -93,62 +94,77 @@ static __device__ __forceinline__ int cut_pt_in_tri(double px, double py, double
     return !(neg && pos);
 }
 
-// Ear clipping of one polygon by warp 0 (lane 0 drives; lanes scan).
-// Returns triangles appended to cap (lane 0's count).
-static __device__ int cut_ear_clip(const Cap2D& c, const int* poly, int n, int* prv, int* nxt, int* cap, int lane)
+// Ear clipping of one polygon by the whole CTA.  Every thread follows the
+// same serial walk (cur, remaining); the test of a convex candidate ear
+// against the polygon's remaining vertices is split over the CTA and
+// combined with __syncthreads_or, so the decisions -- and the triangles --
+// are those of the one-thread walk.  U/W hold the polygon's 2D coordinates
+// (FP64), prv/nxt its links.  Returns the triangle count.
+#define CUT_EAR_SM 1024     // polygons up to this size keep U/W/prv/nxt in shared memory
+static __device__ int cut_ear_clip_cta(const Cap2D& c, const int* poly, int n, double* U, double* W,
+                                       int* prv, int* nxt, int* cap)
 {
+    const int tid = threadIdx.x;
+    for (int i = tid; i < n; i += CUT_NT) {
+        prv[i] = (i + n - 1) % n; nxt[i] = (i + 1) % n;
+        U[i] = cU(c, poly[i]); W[i] = cW(c, poly[i]);
+    }
+    __syncthreads();
     int nc = 0;
-    for (int i = lane; i < n; i += 32) { prv[i] = (i + n - 1) % n; nxt[i] = (i + 1) % n; }
-    __syncwarp();
     int remaining = n, cur = 0, iter = 0;
     while (remaining > 3 && iter < remaining) {
         iter++;
-        int p = prv[cur], q = nxt[cur];
-        int vp = poly[p], vc = poly[cur], vn = poly[q];
-        double up = cU(c, vp), wp = cW(c, vp), uc = cU(c, vc), wc = cW(c, vc), un = cU(c, vn), wn = cW(c, vn);
-        double cr = (uc - up) * (wn - wp) - (wc - wp) * (un - up);
+        const int p = prv[cur], q = nxt[cur];
+        const double up = U[p], wp = W[p], uc = U[cur], wc = W[cur], un = U[q], wn = W[q];
+        const double cr = (uc - up) * (wn - wp) - (wc - wp) * (un - up);
         if (cr < -1e-9) { cur = q; continue; }
         bool clip;
         if (cr <= 1e-9) clip = true;
         else {
             int inside = 0;
-            for (int idx = lane; idx < n; idx += 32) {
+            for (int idx = tid; idx < n; idx += CUT_NT) {
                 if (idx == p || idx == cur || idx == q) continue;
                 if (nxt[prv[idx]] != idx) continue;
-                int vi = poly[idx];
-                double cu = cU(c, vi), cw = cW(c, vi);
+                const double cu = U[idx], cw = W[idx];
                 if (fabs(cu - up) + fabs(cw - wp) > 1e-6 &&
                     fabs(cu - uc) + fabs(cw - wc) > 1e-6 &&
                     fabs(cu - un) + fabs(cw - wn) > 1e-6 &&
                     cut_pt_in_tri(cu, cw, up, wp, uc, wc, un, wn)) inside = 1;
             }
-            clip = __ballot_sync(FULL_MASK, inside) == 0;
+            clip = __syncthreads_or(inside) == 0;
         }
         if (clip) {
-            if (lane == 0) {
-                cap[3 * nc] = vp; cap[3 * nc + 1] = vc; cap[3 * nc + 2] = vn;
+            if (tid == 0) {
+                cap[3 * nc] = poly[p]; cap[3 * nc + 1] = poly[cur]; cap[3 * nc + 2] = poly[q];
                 nxt[p] = q; prv[q] = p;
             }
             nc++;
-            __syncwarp();
+            __syncthreads();
             remaining--; cur = q; iter = 0;
         } else cur = q;
     }
     if (remaining == 3) {
-        int p = prv[cur], q = nxt[cur];
-        if (lane == 0) { cap[3 * nc] = poly[p]; cap[3 * nc + 1] = poly[cur]; cap[3 * nc + 2] = poly[q]; }
+        const int p = prv[cur], q = nxt[cur];
+        if (tid == 0) { cap[3 * nc] = poly[p]; cap[3 * nc + 1] = poly[cur]; cap[3 * nc + 2] = poly[q]; }
         nc++;
     }
-    __syncwarp();
+    __syncthreads();
     return nc;
 }
 
 // Caps from the directed boundary edges be[] (sorted by (a,b), packed a<<32|b).
-// Warp 0 only.  Returns n_cap >= 0 or -1 on failure.
+// Whole CTA: thread 0 traces the loops, nests them and bridges holes; the
+// ear clipping is CTA-wide.  gU/gW: 2*poly_cap doubles of global scratch for
+// polygons longer than CUT_EAR_SM.  Returns n_cap >= 0 or -1 on failure.
 static __device__ int cut_build_caps(const float* V, int n_all, const unsigned long long* be, int nb,
                               float pa, float pb, float pc, int* used, int* lv, int* ls, int* lsz,
-                              int* poly, int* tmp, int poly_cap, int* cap_out, int* n_loops_out, int lane)
+                              int* poly, int* tmp, int poly_cap, int* cap_out, int* n_loops_out,
+                              double* gU)
 {
+    const int tid = threadIdx.x;
+    __shared__ int s_nl, s_fail, s_pn;
+    __shared__ double s_U[CUT_EAR_SM], s_W[CUT_EAR_SM];
+    __shared__ int s_prv[CUT_EAR_SM], s_nxt[CUT_EAR_SM];
     Cap2D C; C.V = V;
     {
         float ax = fabsf(pa), ay = fabsf(pb), az = fabsf(pc);
@@ -157,7 +173,7 @@ static __device__ int cut_build_caps(const float* V, int n_all, const unsigned l
         else                      { C.pu = 0; C.pv = 1; }
     }
     int n_loops = 0, fail = 0;
-    if (lane == 0) {
+    if (tid == 0) {
         int lvi = 0;
         for (int i = 0; i < nb; i++) used[i] = 0;
         for (int st = 0; st < nb && !fail; st++) {
@@ -182,15 +198,17 @@ static __device__ int cut_build_caps(const float* V, int n_all, const unsigned l
             ls[n_loops] = start; lsz[n_loops] = lvi - start; n_loops++;
         }
         if (n_loops > 128) fail = 1;
+        s_nl = n_loops; s_fail = fail;
     }
-    n_loops = __shfl_sync(FULL_MASK, n_loops, 0);
-    fail = __shfl_sync(FULL_MASK, fail, 0);
+    __syncthreads();
+    n_loops = s_nl;
+    fail = s_fail;
     *n_loops_out = n_loops;
     if (fail) return -1;
     __shared__ int parent[128], is_hole[128], hidx[128];
     __shared__ double hmax[128];
     int n_cap = 0;
-    if (lane == 0) {
+    if (tid == 0) {
         for (int i = 0; i < n_loops; i++)
             if (cut_signed_area(C, lv + ls[i], lsz[i]) < 0) cut_reverse(lv + ls[i], lsz[i]);
         for (int i = 0; i < n_loops; i++) { parent[i] = -1; is_hole[i] = 0; }
@@ -230,15 +248,16 @@ static __device__ int cut_build_caps(const float* V, int n_all, const unsigned l
             }
             for (int i = 0; i < n_loops; i++) if (is_hole[i]) cut_reverse(lv + ls[i], lsz[i]);
         }
+        s_fail = fail;
     }
-    fail = __shfl_sync(FULL_MASK, fail, 0);
-    __syncwarp();
+    __syncthreads();
+    fail = s_fail;
     if (fail) return -1;
     int expected = 0;
     for (int oi = 0; oi < n_loops; oi++) {
         if (is_hole[oi] || lsz[oi] < 3) continue;
         int pn = 0;
-        if (lane == 0) {
+        if (tid == 0) {
             pn = lsz[oi];
             for (int i = 0; i < pn; i++) poly[i] = lv[ls[oi] + i];
             int nin = 0;
@@ -285,13 +304,19 @@ static __device__ int cut_build_caps(const float* V, int n_all, const unsigned l
                 for (int j = 0; j < k; j++) poly[j] = tmp[j];
                 pn = k;
             }
+            s_fail = fail; s_pn = pn;
         }
-        fail = __shfl_sync(FULL_MASK, fail, 0);
-        pn = __shfl_sync(FULL_MASK, pn, 0);
-        __syncwarp();
+        __syncthreads();
+        fail = s_fail;
+        pn = s_pn;
         if (fail) return -1;
         expected += pn - 2;
-        if (pn >= 3) n_cap += cut_ear_clip(C, poly, pn, tmp, tmp + poly_cap, cap_out + 3 * n_cap, lane);
+        if (pn >= 3) {
+            if (pn <= CUT_EAR_SM)
+                n_cap += cut_ear_clip_cta(C, poly, pn, s_U, s_W, s_prv, s_nxt, cap_out + 3 * n_cap);
+            else
+                n_cap += cut_ear_clip_cta(C, poly, pn, gU, gU + poly_cap, tmp, tmp + poly_cap, cap_out + 3 * n_cap);
+        }
     }
     if (n_cap < expected) return -1;
     return n_cap;
@@ -308,6 +333,8 @@ static __device__ void cut_cta(const float* __restrict__ verts, int nv, const in
 {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     Arena* const oarena = out_arena ? out_arena : arena;
+    long long tph[5];
+    tph[0] = clock64();
     __shared__ int s_err;
     if (tid == 0) s_err = 0;
     __syncthreads();
@@ -462,7 +489,8 @@ static __device__ void cut_cta(const float* __restrict__ verts, int nv, const in
     unsigned long long* ce = (unsigned long long*)sh.ptr[3];
     if (tid == 0) sh.cnt[3] = 0;
     __syncthreads();
-    for (int base = 0; base < nt; base += CUT_NT) {
+    // collection order does not matter: the keys are sorted next
+    for (int base = 0; base < nt; base += CUT_NT) {     // uniform trip count (warp shuffles)
         int t = base + tid;
         unsigned long long k[3]; int m = 0;
         if (t < nt) {
@@ -475,14 +503,19 @@ static __device__ void cut_cta(const float* __restrict__ verts, int nv, const in
                 }
             }
         }
-        int off = 0, tot = 0;
-        off = block_exclusive_scan(m, sh.scan, &tot);
-        int b0 = sh.cnt[3];
-        for (int j = 0; j < m; j++) ce[b0 + off + j] = k[j];
-        __syncthreads();
-        if (tid == 0) sh.cnt[3] += tot;
-        __syncthreads();
+        int x = m;                                      // warp inclusive scan of the counts
+        #pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int y = __shfl_up_sync(FULL_MASK, x, o);
+            if (lane >= o) x += y;
+        }
+        int wb = 0;
+        const int wt = __shfl_sync(FULL_MASK, x, 31);
+        if (lane == 31 && wt) wb = atomicAdd(&sh.cnt[3], wt);
+        wb = __shfl_sync(FULL_MASK, wb, 31);
+        for (int j = 0; j < m; j++) ce[wb + x - m + j] = k[j];
     }
+    __syncthreads();
     cta_sort_u64(ce, n_occ);
     // unique keys (sorted order) and the intersection vertex of each
     CUT_ALLOC(4, int, n_occ);                  // 1 where a new key starts
@@ -538,6 +571,7 @@ static __device__ void cut_cta(const float* __restrict__ verts, int nv, const in
         isect[i] = ni;
     }
     __syncthreads();
+    tph[1] = clock64();
     // ---------------- split: per-triangle piece counts then write in order
     CUT_ALLOC(9, int, nt);     // pos offsets
     CUT_ALLOC(10, int, nt);    // neg offsets
@@ -614,6 +648,7 @@ static __device__ void cut_cta(const float* __restrict__ verts, int nv, const in
     int* ntri = (int*)sh.ptr[12];
     for (int t = tid; t < nt; t += CUT_NT) split(t, 1, ptri, ntri, poff[t], noff[t]);
     __syncthreads();
+    tph[2] = clock64();
     // ---------------- boundary of the positive side among edges on the cut
     // key = min<<33 | max<<1 | (a > b)
     if (tid == 0) sh.cnt[5] = 0;
@@ -667,21 +702,21 @@ static __device__ void cut_cta(const float* __restrict__ verts, int nv, const in
     __syncthreads();
     const int nb = sh.cnt[7];
     cta_sort_u64(be, nb);
+    tph[3] = clock64();
     // ---------------- caps (warp 0)
     const int poly_cap = nb * 4 + 64;
     CUT_ALLOC(15, int, 4 * nb + 3 * poly_cap + 3 * poly_cap);
+    CUT_ALLOC(13, double, poly_cap > CUT_EAR_SM ? 2 * poly_cap : 1);   // ear-clip coordinates of long polygons
     __syncthreads();
     if (s_err) goto fail_out;
     {
         int* blk = (int*)sh.ptr[15];
         int* used = blk; int* lv = used + nb; int* ls = lv + nb; int* lsz = ls + nb;
         int* poly = lsz + nb; int* tmp = poly + poly_cap; int* capt = tmp + 2 * poly_cap;
-        if (warp == 0) {
-            int nl = 0;
-            int nc = (nb > 0) ? cut_build_caps(all, n_all, be, nb, pa, pb, pc, used, lv, ls, lsz, poly, tmp,
-                                               poly_cap, capt, &nl, lane) : 0;
-            if (lane == 0) { sh.ival[8] = nc; sh.ival[9] = nl; }
-        }
+        int nl = 0;
+        int nc = (nb > 0) ? cut_build_caps(all, n_all, be, nb, pa, pb, pc, used, lv, ls, lsz, poly, tmp,
+                                           poly_cap, capt, &nl, (double*)sh.ptr[13]) : 0;
+        if (tid == 0) { sh.ival[8] = nc; sh.ival[9] = nl; }
         __syncthreads();
     }
     {
@@ -778,6 +813,8 @@ static __device__ void cut_cta(const float* __restrict__ verts, int nv, const in
             res->nv = (float*)sh.ptr[8]; res->nt = (int*)sh.ptr[9]; res->nnv = sh.ival[4]; res->nnt = sh.ival[5];
             res->n_pos_tris = n_pos; res->n_neg_tris = n_neg; res->n_cap = n_cap;
             res->n_loops = sh.ival[9]; res->n_boundary = nb; res->n_cross = n_u;
+            tph[4] = clock64();
+            for (int k = 0; k < 4; k++) res->cyc[k] = (unsigned)((tph[k + 1] - tph[k]) >> 6);
         }
         return;
     }

@@ -226,6 +226,13 @@ int cuacd_hull_stats(gpu_ctx_t ctx, const float* pts, int total_pts,
                      const int* offsets, int n_hulls, int* out_nv, int* out_nt,
                      float* out_vol, unsigned long long* out_stats);
 
+/* Diagnostic (no counterpart in the reference): cut one mesh by n_planes
+ * planes and report 8 ints per plane: crossing edges, boundary edges, cap
+ * loops, cap triangles, and the SM cycles / 64 spent in the crossing,
+ * split, boundary and cap+output phases of the cut kernel. */
+int cuacd_cut_stats(gpu_ctx_t ctx, const float* verts, int nv, const int* tris, int nt,
+                    const float* planes, int n_planes, int* out_stats);
+
 /* Number of kernel launches issued by this context so far (a counter the
  * benchmark reads around its timed region). */
 unsigned long long cuacd_launch_count(gpu_ctx_t ctx);
