@@ -43,7 +43,7 @@ struct HDPrep {            // per-surface prep output
     int*    offsets;       // [nt+1] exclusive sample offsets (global scratch)
     float4* tri;           // [3 * nleaf * HD_LEAF] triangles in leaf order
     float4* node;          // [4 * P] child boxes per internal node (lo_l, hi_l, lo_r, hi_r)
-    unsigned long long* keys;   // [pow2(nt)] Morton|tri sort keys
+    unsigned long long* keys;   // [pow2(nt)] leaf order: (first sample) << 32 | triangle
     int n_samples, res, P, nleaf;
     float area;
     int _pad;
@@ -337,6 +337,22 @@ static __device__ void hd_prep_cta(HDSurf S, char* scratch, float resolution, in
     if (P.P == 1 && tid == 0) {      // single leaf: node 1's "children" are that leaf and an empty box
         P.node[4] = lbox[0]; P.node[5] = lbox[1];
         P.node[6] = make_float4(3.4e38f, 3.4e38f, 3.4e38f, 0.f); P.node[7] = make_float4(-3.4e38f, -3.4e38f, -3.4e38f, 0.f);
+    }
+    __syncthreads();
+    // sample enumeration in leaf (Morton) order, so neighbouring query
+    // threads take neighbouring samples: keys[i] <- (first sample of sorted
+    // triangle i) << 32 | triangle.  The leaf boxes are dead by now and hold
+    // the counts for the scan.
+    {
+        int* cnt_s = (int*)lbox;
+        for (int i = tid; i < nt; i += HD_PREP_NT) {
+            const int t = (int)(P.keys[i] & 0xffffffffull);
+            cnt_s[i] = P.offsets[t + 1] - P.offsets[t];
+        }
+        __syncthreads();
+        cta_scan_inplace(cnt_s, nt, sh.scan);
+        for (int i = tid; i < nt; i += HD_PREP_NT)
+            P.keys[i] = ((unsigned long long)(unsigned)cnt_s[i] << 32) | (P.keys[i] & 0xffffffffull);
     }
     if (tid == 0) { P.n_samples = n_samples; P.res = res; P.area = area; *out = P; }
     __syncthreads();
