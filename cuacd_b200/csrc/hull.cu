@@ -35,17 +35,32 @@ k_hull_setup(const HullJob* __restrict__ jobs, int n_jobs, Arena* scratch, HullS
     }
 }
 
-// Prefix of the active hulls' point counts (wrap-grid shares), one CTA.
+// Wrap-grid shares (one CTA): prefix of the active hulls' weights, a hull's
+// point count plus a floor.  With H active hulls and G > H wrap CTAs the
+// floor ceil(sum n / (G - H)) makes every share at least one CTA spacing
+// wide, so every hull has a home CTA from the start.
 __global__ void __launch_bounds__(1024)
-k_hull_assign(HullState* states, int n_jobs, long long* total)
+k_hull_assign(HullState* states, int n_jobs, int n_ctas, long long* total)
 {
     __shared__ long long part[1024 / 32];
-    __shared__ long long carry;
-    if (threadIdx.x == 0) carry = 0;
+    __shared__ long long carry, s_sum, s_floor;
+    __shared__ int s_h;
+    if (threadIdx.x == 0) { carry = 0; s_sum = 0; s_h = 0; }
     __syncthreads();
+    {
+        long long sn = 0; int h = 0;
+        for (int j = threadIdx.x; j < n_jobs; j += 1024)
+            if (states[j].active) { sn += states[j].n; h++; }
+        atomicAdd((unsigned long long*)&s_sum, (unsigned long long)sn);
+        atomicAdd(&s_h, h);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) s_floor = n_ctas > s_h ? (s_sum + (n_ctas - s_h) - 1) / (n_ctas - s_h) : 0;
+    __syncthreads();
+    const long long floor_w = s_floor;
     for (int base = 0; base < n_jobs; base += 1024) {
         const int j = base + threadIdx.x;
-        long long w = (j < n_jobs && states[j].active) ? (long long)states[j].n : 0;
+        long long w = (j < n_jobs && states[j].active) ? (long long)states[j].n + floor_w : 0;
         long long x = w;                                  // inclusive warp scan
         #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
@@ -163,11 +178,13 @@ static int hull_wrap_per_sm()
     return cached[dev];
 }
 
+static int hull_wrap_pts_per_cta() { return 4096; }
+
 // Wrap grid size: about one warp per 256 points of the batch, at most the
 // resident CTAs of the whole device.
 int hull_wrap_ctas(long long total_points, int n_sm)
 {
-    long long c = (total_points + 4095) / 4096;
+    long long c = (total_points + hull_wrap_pts_per_cta() - 1) / hull_wrap_pts_per_cta();
     const long long cap = (long long)n_sm * hull_wrap_per_sm();
     if (c < 1) c = 1;
     if (c > cap) c = cap;
@@ -181,7 +198,7 @@ void launch_hull_jobs(const HullJob* d_jobs, int n_jobs, HullState* d_states, Hu
     if (n_jobs <= 0) return;
     cudaMemsetAsync(d_ctl, 0, 4 * sizeof(int), s);
     k_hull_setup<<<n_jobs, HULL_NT, 0, s>>>(d_jobs, n_jobs, scratch, d_states, d_ctl);
-    k_hull_assign<<<1, 1024, 0, s>>>(d_states, n_jobs, (long long*)(d_ctl + 2));
+    k_hull_assign<<<1, 1024, 0, s>>>(d_states, n_jobs, n_wrap_ctas, (long long*)(d_ctl + 2));
     hull_wrap_per_sm();                                   // dynamic shared memory opt-in
     k_hull_wrap<<<n_wrap_ctas, HULL_NT, HULL_WRAP_DSMEM, s>>>(d_states, n_jobs, d_ctl, (const long long*)(d_ctl + 2),
                                                              d_wbuf);

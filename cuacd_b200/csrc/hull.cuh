@@ -37,6 +37,7 @@
 #define HULL_WQ       704                          // of which: node stack
 #define HULL_WL       (HULL_WSM - HULL_WQ)         //           kept-leaf list
 #define HULL_WRAP_DSMEM ((size_t)(HULL_NT / 32) * HULL_WSM * sizeof(int))
+#define HULL_SEEDS    1                            // seed faces (1..6) that start the wrapping
 
 // Per-cloud scratch layout (bytes computed on the host by hull_scratch_bytes).
 struct HullCaps {
@@ -272,11 +273,14 @@ static __device__ __forceinline__ void warp_best(int& ci, float4& cq, float4 a, 
 // Returns c (sorted id), -1 if all points are on the line, -2 if the warp
 // queues overflowed (the caller then uses the serial search).
 static __device__ int warp_wrap(const HullCtx& H, int u, int v, const WarpLists W, int lane, int* nleaf_out,
-                                unsigned& n_pts, unsigned& n64)
+                                unsigned& n_pts, unsigned& n64, const int* dir = nullptr)
 {
+    // dir: wrap about the line through u with this direction (v unused)
     const unsigned lt = (1u << lane) - 1u;
-    float4 a = H.pts[u], pv = H.pts[v];
-    const int dx = (int)(pv.x - a.x), dy = (int)(pv.y - a.y), dz = (int)(pv.z - a.z);
+    float4 a = H.pts[u], pv = dir ? a : H.pts[v];
+    const int dx = dir ? dir[0] : (int)(pv.x - a.x), dy = dir ? dir[1] : (int)(pv.y - a.y);
+    const int dz = dir ? dir[2] : (int)(pv.z - a.z);
+    if (dir) v = u;
     int ci = -1; float4 cq = a;
     double mx = 0, my = 0, mz = 0; float fx = 0, fy = 0, fz = 0;
     auto setm = [&]() {
@@ -333,12 +337,16 @@ static __device__ int warp_wrap(const HullCtx& H, int u, int v, const WarpLists 
         sp = base + 2 * nbi; nl += nbl;
         if (nl > scanned) {                             // scan the new leaves, tighten the plane
             const int total = (nl - scanned) * HULL_LEAF;
+            const int ci0 = ci;
             for (int i = lane; i < total; i += 32) {
                 int p = W.leaf[scanned + i / HULL_LEAF] * HULL_LEAF + (i % HULL_LEAF);
                 if (p < H.m) take(p);
             }
-            warp_best(ci, cq, a, dx, dy, dz, n64);
-            if (ci >= 0) setm();
+            // reduce only when some lane found a better point
+            if (__any_sync(FULL_MASK, ci != ci0)) {
+                warp_best(ci, cq, a, dx, dy, dz, n64);
+                if (ci >= 0) setm();
+            }
             scanned = nl;
         }
     }
@@ -564,9 +572,10 @@ struct HullState {             // per hull, global memory
     long long wbase;           // wrap-grid share: prefix of the active hulls' point counts
     double mesh_vol;
     unsigned long long stats[8];   // leaves kept by wraps, wraps, faces, points
-                                   // tested by wraps, set-up cycles, wraps on
-                                   // the hull's own lists, faces on the hull's
-                                   // own buffers, large faces
+                                   // tested by wraps, set-up cycles, device
+                                   // time (ns) of the first edge taken and of
+                                   // completion, large faces (+ 2^32 per wrap
+                                   // and 2^48 per face on the hull's own lists)
 };
 
 __host__ __device__ inline size_t hull_scratch_bytes(int n)
@@ -598,6 +607,7 @@ __host__ __device__ inline size_t hull_warp_bytes(int n_max)
 }
 
 struct HullSetupShared {
+    HullWarp ws[8];                    // coplanar points of the seed planes (one per seed warp)
     float mn[3], mx[3];
     float cen[3], inv[3];
     int ax[3];
@@ -826,31 +836,28 @@ static __device__ void hull_setup_cta(const float* __restrict__ pts, int n, char
     __syncthreads();
     HullCtx H; H.pts = P4; H.nlo = nlo; H.nhi = nhi; H.obb = obb; H.m = n; H.P = C.P; H.nleaf = C.m_leaves;
 
-    // lexmin (x,y,z,input index) -> first face seed
-    {
+    // extreme point for seed sd: lexicographic minimum of (s0*q[ax0],
+    // s1*q[ax1], s2*q[ax2], input index) -> sorted id
+    __shared__ int s_p0;
+    auto extreme = [&](int ax0, int s0, int ax1, int s1, int ax2, int s2) -> int {
+        if (tid == 0) { sh.lexmin = ~0ull; s_p0 = -1; }
+        __syncthreads();
         unsigned long long best = ~0ull;
         for (int i = tid; i < n; i += HULL_NT) {
             float4 q = P4[i];
-            // key (x, y, z, input index): duplicates resolve to the smaller index
-            unsigned long long k = ((unsigned long long)((int)q.x + 8192) << 50) |
-                                   ((unsigned long long)((int)q.y + 8192) << 36) |
-                                   ((unsigned long long)((int)q.z + 8192) << 22) |
-                                   (unsigned long long)(unsigned)pidx(q);
+            const int c0 = s0 * (int)comp(q, ax0), c1 = s1 * (int)comp(q, ax1), c2 = s2 * (int)comp(q, ax2);
+            // duplicates resolve to the smaller input index
+            unsigned long long k = ((unsigned long long)(c0 + 8192) << 50) | ((unsigned long long)(c1 + 8192) << 36) |
+                                   ((unsigned long long)(c2 + 8192) << 22) | (unsigned long long)(unsigned)pidx(q);
             if (k < best) best = k;
         }
         atomicMin(&sh.lexmin, best);
         __syncthreads();
-    }
-    // convert lexmin key back to a sorted id (find the point with that input index)
-    __shared__ int s_p0;
-    if (tid == 0) s_p0 = -1;
-    __syncthreads();
-    {
-        int want = (int)(sh.lexmin & ((1ull << 22) - 1));
+        const int want = (int)(sh.lexmin & ((1ull << 22) - 1));
         for (int i = tid; i < n; i += HULL_NT) if (pidx(P4[i]) == want) s_p0 = i;
         __syncthreads();
-    }
-    const int p0 = s_p0;
+        return s_p0;
+    };
 
     // ---- cooperative (large) face: collect S by scanning all points, walk
     // the polygon with CTA reductions, publish the face.  u<0: first face.
@@ -971,42 +978,83 @@ static __device__ void hull_setup_cta(const float* __restrict__ pts, int n, char
         __syncthreads();
     };
 
-    // ---- 5. first face (cooperative, thread 0 finds the plane)
+    // ---- 5. seed faces.  Each seed is an extreme point p (a vertex of the
+    // cloud's projection along d) and a direction d: wrapping a plane about
+    // the line (p, d) gives a hull edge (p, c), whose outward face normal is
+    // (c - p) x d; a collinear contact set is wrapped again about (p, c).
+    // Seed 0 (lexicographic minimum, d = z) always runs; more seeds start the
+    // wrapping from up to five more places, which shortens its longest
+    // chain.  One warp finds each seed's plane (warp-cooperative wraps over
+    // the output buffers, free until the output phase), then the CTA builds
+    // the seed faces in order; a face already found is dropped by the face set.
     unsigned st_pts = 0, st_cop = 0, st_64 = 0;
-    if (tid == 0) {
-        int c = hull_wrap(H, p0, 0, 0, 1, p0 / HULL_LEAF, st_pts, st_64);
-        double nx = 0, ny = 0, nz = 0;
-        int ok = c >= 0;
-        if (ok) {
-            float4 a = P4[p0], q = P4[c];
-            double ex = q.x - a.x, ey = q.y - a.y, ez = q.z - a.z;
-            nx = ey; ny = -ex; nz = 0;                      // (c - p0) x (0,0,1)
-            // collinear contact set? then wrap again about (p0, c)
-            int tmp[HULL_SMALL_S];
-            int cnt = hull_coplanar(H, p0, nx, ny, nz, tmp, HULL_SMALL_S, st_cop, st_64);
-            bool noncol = cnt > HULL_SMALL_S;
-            int ix = (int)ex, iy = (int)ey, iz = (int)ez;
-            for (int i = 0; i < cnt && i < HULL_SMALL_S && !noncol; i++)
-                if (!on_line(ix, iy, iz, a, P4[tmp[i]])) noncol = true;
-            if (!noncol) {
-                int c2 = hull_wrap(H, p0, ix, iy, iz, p0 / HULL_LEAF, st_pts, st_64);
-                if (c2 < 0) ok = 0;
-                else {
-                    float4 q2 = P4[c2];
-                    double fx = q2.x - a.x, fy = q2.y - a.y, fz = q2.z - a.z;
-                    nx = fy * ez - fz * ey; ny = fz * ex - fx * ez; nz = fx * ey - fy * ex;
-                    if (nx == 0 && ny == 0 && nz == 0) ok = 0;
-                }
-            }
-        }
-        s_N[0] = nx; s_N[1] = ny; s_N[2] = nz;
-        s_face_ok = ok;
+    const int seeds[6][9] = {
+        {0, 1, 1, 1, 2, 1, 0, 0, 1}, {0, -1, 1, -1, 2, 1, 0, 0, 1},
+        {1, 1, 0, -1, 2, 1, 0, 0, 1}, {1, -1, 0, 1, 2, 1, 0, 0, 1},
+        {2, 1, 1, 1, 0, 1, 1, 0, 0}, {2, -1, 1, -1, 0, 1, 1, 0, 0}};
+    const int n_seeds = n >= 64 ? HULL_SEEDS : 1;
+    __shared__ int s_sp[6], s_sok[6];
+    __shared__ double s_sN[6][3];
+    for (int sd = 0; sd < n_seeds; sd++) {
+        const int* S6 = seeds[sd];
+        const int pe = extreme(S6[0], S6[1], S6[2], S6[3], S6[4], S6[5]);
+        if (tid == 0) s_sp[sd] = pe;
     }
     __syncthreads();
-    if (!s_face_ok) return;                          // degenerate: collinear input (no faces, no error)
-    coop_face(-1, -1, s_N[0], s_N[1], s_N[2], p0);
+    {
+        const int warp = tid >> 5, lane = tid & 31;
+        if (warp < n_seeds) {
+            const int sd = warp;
+            const int p0 = s_sp[sd];
+            const int dir[3] = {seeds[sd][6], seeds[sd][7], seeds[sd][8]};
+            // lists: 3P ints per seed warp, seeds 0-3 in ocnt (2n), 4-5 in posn (n)
+            int* base = sd < 4 ? ocnt + (size_t)sd * 3 * C.P : posn + (size_t)(sd - 4) * 3 * C.P;
+            WarpLists L;
+            L.q = base; L.leaf = base + 2 * C.P; L.qcap = 2 * C.P; L.lcap = C.P;
+            int nl = 0;
+            int ok = p0 >= 0;
+            double nx = 0, ny = 0, nz = 0;
+            int c = ok ? warp_wrap(H, p0, p0, L, lane, &nl, st_pts, st_64, dir) : -1;
+            ok = c >= 0;
+            if (ok) {
+                const float4 a = P4[p0], q = P4[c];
+                const double ex = q.x - a.x, ey = q.y - a.y, ez = q.z - a.z;
+                nx = ey * dir[2] - ez * dir[1]; ny = ez * dir[0] - ex * dir[2]; nz = ex * dir[1] - ey * dir[0];
+                // collinear contact set? then wrap again about (p0, c)
+                const int ns = warp_coplanar(H, a, nx, ny, nz, sh.ws[sd], L, nl, lane, HULL_SMALL_S, st_cop, st_64);
+                int noncol = 0;
+                if (lane == 0) {
+                    noncol = ns > HULL_SMALL_S;
+                    const int ix = (int)ex, iy = (int)ey, iz = (int)ez;
+                    for (int i = 0; i < ns && i < HULL_SMALL_S && !noncol; i++)
+                        if (!on_line(ix, iy, iz, a, P4[sh.ws[sd].S[i]])) noncol = 1;
+                }
+                noncol = __shfl_sync(FULL_MASK, noncol, 0);
+                if (!noncol) {
+                    const int c2 = warp_wrap(H, p0, c, L, lane, &nl, st_pts, st_64);
+                    if (c2 < 0) ok = 0;
+                    else {
+                        const float4 q2 = P4[c2];
+                        const double fx = q2.x - a.x, fy = q2.y - a.y, fz = q2.z - a.z;
+                        nx = fy * ez - fz * ey; ny = fz * ex - fx * ez; nz = fx * ey - fy * ex;
+                        if (nx == 0 && ny == 0 && nz == 0) ok = 0;
+                    }
+                }
+            }
+            if (lane == 0) { s_sok[sd] = ok; s_sN[sd][0] = nx; s_sN[sd][1] = ny; s_sN[sd][2] = nz; }
+        }
+    }
+    __syncthreads();
+    for (int sd = 0; sd < n_seeds; sd++) {
+        if (!s_sok[sd]) {
+            if (sd == 0) return;                     // degenerate: collinear input (no faces, no error)
+            continue;
+        }
+        coop_face(-1, -1, s_sN[sd][0], s_sN[sd][1], s_sN[sd][2], s_sp[sd]);
+        if (sh.err) break;
+    }
 
-    // ---- 6. frontier queue: every edge of the first face whose twin is unknown
+    // ---- 6. frontier queue: every edge of the seed faces whose twin is unknown
     for (int i = tid; i < qcap; i += HULL_NT) Q[i] = ~0ull;
     __syncthreads();
     if (tid == 0) {
@@ -1031,6 +1079,14 @@ static __device__ void hull_setup_cta(const float* __restrict__ pts, int n, char
         S->stats[4] = (unsigned long long)(clock64() - t_begin);
     }
     __syncthreads();
+}
+
+// Device-wide clock (ns) for the per-hull wrap timestamps.
+static __device__ __forceinline__ unsigned long long hull_now()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
 }
 
 #define HULL_SGCAP 4096   // per-warp coplanar set and polygon (ints each); larger faces use the hull's own buffers
@@ -1076,7 +1132,7 @@ static __device__ void hull_wrap_edge(HullState* S, int u, int v, HullWarp& W, c
     if (c == -2) {                                   // shared lists too small: the hull's own
         locked = hull_lock(S, lane);
         if (!locked) return;
-        if (lane == 0) atomicAdd(&S->stats[5], 1ull);
+        if (lane == 0) atomicAdd(&S->stats[7], 1ull << 32);
         L.q = S->ocnt; L.leaf = S->ocnt + 2 * S->P; L.qcap = 2 * S->P; L.lcap = S->P;
         c = warp_wrap(H, u, v, L, lane, &nl, st_pts, st_64);
         if (c == -2) {                               // cannot happen: 2P + P hold the whole tree
@@ -1102,7 +1158,7 @@ static __device__ void hull_wrap_edge(HullState* S, int u, int v, HullWarp& W, c
         int* bS = Sg; int* bP = Pg;
         if (ns + 2 > HULL_SGCAP) {                   // large face: the hull's own buffers
             if (!locked) { locked = hull_lock(S, lane); if (!locked) return; }
-            if (lane == 0) atomicAdd(&S->stats[6], 1ull);
+            if (lane == 0) atomicAdd(&S->stats[7], 1ull << 48);
             bS = S->Sbuf; bP = S->posn;
         }
         k = warp_big_polygon(H, u, v, nx, ny, nz, L.leaf, nl, bS, bP, lane, st_cop, st_64);
@@ -1229,6 +1285,7 @@ static __device__ void hull_wrap_grid(HullState* states, int n_jobs, int h0, int
         }
         idle = 0; nap = 64;
         HullState* S = &states[h];
+        if (lane == 0 && idx == 0) S->stats[5] = hull_now();          // first edge taken
         unsigned long long key = ~0ull;
         int skip = 0;
         if (lane == 0) {
@@ -1254,6 +1311,7 @@ static __device__ void hull_wrap_grid(HullState* states, int n_jobs, int h0, int
         __syncwarp();
         if (lane == 0) {
             if (atomicSub(&S->q_pending, 1) == 1) {                   // this hull is complete
+                S->stats[6] = hull_now();
                 atomicExch(&S->active, 0);
                 __threadfence();
                 atomicSub(&ctl[0], 1);

@@ -201,6 +201,7 @@ struct Lookahead {
     char* scr_base; size_t scr_cap;       // scratch arena memory
     Arena* d_out; Arena* d_scr;           // device arena structs
     float min_edge = 0.0125f;
+    int debug = 0;                        // write the points of failed fragment hulls to files
     // buffers for the components pass
     HDSurf* d_surfs = nullptr; int surf_cap = 0;
     CompResult* d_cres = nullptr;
@@ -275,6 +276,21 @@ struct Lookahead {
         if (rh) return rh;
         CK(cudaMemcpyAsync(frags.data(), d_fr, sizeof(FragRes) * 2 * n, cudaMemcpyDeviceToHost, s));
         CK(cudaStreamSynchronize(s));
+        if (debug) {
+            static int n_dump = 0;
+            for (int f = 0; f < 2 * n && n_dump < 16; f++) {
+                if (!frags[f].err) continue;
+                const CutResult& c = cuts[f >> 1];
+                const int nvf = (f & 1) ? c.nnv : c.npv;
+                std::vector<float> pts(3 * (size_t)(nvf > 0 ? nvf : 1));
+                CK(cudaMemcpy(pts.data(), (f & 1) ? c.nv : c.pv, 12 * (size_t)nvf, cudaMemcpyDeviceToHost));
+                char name[64];
+                snprintf(name, sizeof(name), "cuacd_failed_hull_%d.f32", n_dump++);
+                FILE* fp = fopen(name, "wb");
+                if (fp) { fwrite(pts.data(), 12, (size_t)nvf, fp); fclose(fp); }
+                fprintf(stderr, "[la] fragment hull failed (0x%x), %d points written to %s\n", frags[f].err, nvf, name);
+            }
+        }
         for (auto& r : frags) if (r.err & (KERR_HEAP_OOM | KERR_BT_POOL_EXHAUST)) return KERR_HEAP_OOM;
         return 0;
     }
@@ -411,7 +427,7 @@ extern "C" int lookahead_decompose(gpu_ctx_t ctx, const float* verts, int nv, co
                                    int n_concave_edges, float concave_eps, float concave_threshold,
                                    int concave_iters, int merge_hulls, struct gpu_result* out)
 {
-    (void)quick_depth; (void)debug; (void)merge_hulls;
+    (void)quick_depth; (void)merge_hulls;
     if (!ctx || !out) return -1;
     out->parts = nullptr; out->nparts = 0;
     if (nv <= 0 || nt <= 0) return ctx_fail(ctx, KERR_MESH_INVALID, "empty mesh");
@@ -465,6 +481,7 @@ extern "C" int lookahead_decompose(gpu_ctx_t ctx, const float* verts, int nv, co
     L.ctx = ctx; L.s = s; L.out_base = out_base; L.out_cap = out_cap; L.scr_base = scr_base; L.scr_cap = scr_cap;
     L.d_out = d_arenas; L.d_scr = d_arenas + 1;
     L.min_edge = std::min(threshold * 0.25f, 0.015f);
+    L.debug = debug;
     L.d_surfs = d_surfs; L.surf_cap = 2 * 4096; L.d_cres = d_cres;
     L.d_frags = d_frags; L.frag_cap = (int)std::min<size_t>(2 * max_jobs, 1 << 30);
     L.d_hjobs = d_hjobs; L.d_hstates = d_hstates; L.d_hctl = d_hctl; L.d_wbuf = d_wbuf; L.nwc = hull_wrap_ctas(1LL << 40, ctx->n_sm);

@@ -220,8 +220,9 @@ int cuacd_hull_batch_device(gpu_ctx_t ctx, const float* d_pts,
 /* Diagnostic: exact hulls of a batch of clouds (host pointers) with the
  * hull kernels' work counters, 8 per cloud: BVH leaves kept by the wraps,
  * wraps, faces, points tested by the wraps, SM cycles spent in set-up (sort,
- * BVH, first face), wraps that needed the cloud's own node lists, faces
- * built in the cloud's own buffers, large faces. */
+ * BVH, first face), device clock (ns) when the wrapping took the cloud's
+ * first edge and when it finished, large faces (+ 2^32 per wrap on the
+ * cloud's own node lists, + 2^48 per face built in its own buffers). */
 int cuacd_hull_stats(gpu_ctx_t ctx, const float* pts, int total_pts,
                      const int* offsets, int n_hulls, int* out_nv, int* out_nt,
                      float* out_vol, unsigned long long* out_stats);
