@@ -311,14 +311,14 @@ def main():
     e2e_val = world_n * n * args.steps / e2e_s
 
     # roofline of the dominant stage
-    names = ["k_cut_planes", "k_frag_hull", "k_hd_prep", "k_hd_plan", "k_hd_query", "k_eval_finish"]
+    names = ["k_cut_planes", "hull_pipeline", "k_hd_prep", "k_hd_plan", "k_hd_query", "k_eval_finish"]
     dom = int(np.argmax(stage_ms))
     V, T = len(v), len(t)
     Vf = sum(r.nv[0] + r.nv[1] for r in host); Tf = sum(r.nt[0] + r.nt[1] for r in host)
     Hv = sum(r.hull_nv[0] + r.hull_nv[1] for r in host); Ht = sum(r.hull_nt[0] + r.hull_nt[1] for r in host)
     alg = {
         "k_cut_planes": 12 * (V + T) * n + 12 * (Vf + Tf),
-        "k_frag_hull": 12 * (Vf + Tf) + 12 * (Hv + Ht),
+        "hull_pipeline": 12 * (Vf + Tf) + 12 * (Hv + Ht),
         "k_hd_prep": 12 * (Vf + Tf) + 12 * (Hv + Ht),
         "k_hd_plan": 0,
         "k_hd_query": 12 * (Vf + Tf) + 12 * (Hv + Ht),
