@@ -98,6 +98,20 @@ _opt("gpu_result_free", None, [ctypes.POINTER(GpuResult)])
 _opt("cuacd_candidate_planes", _I, [_P, _P, _I, _P, _I, _I, _F, _F, _I, _F, _P, _P, _P])
 _opt("cuacd_profile_stages", _I, [_P, _I])
 _opt("cuacd_stage_times", _I, [_P, _P])
+_opt("cuacd_scorer_n_params", _I, [])
+_opt("cuacd_scorer_n_features", _I, [])
+_opt("cuacd_scorer_create", _I, [_P, ctypes.c_uint, ctypes.POINTER(_P)])
+_opt("cuacd_scorer_free", None, [_P])
+_opt("cuacd_scorer_set_params", _I, [_P, _P])
+_opt("cuacd_scorer_get_params", _I, [_P, _P])
+_opt("cuacd_scorer_set_normalizer", _I, [_P, _P, _P])
+_opt("cuacd_scorer_get_normalizer", _I, [_P, _P, _P])
+_opt("cuacd_candidate_features", _I, [_P, _P, _P, _I, _P, _I, _F, _P, _I, _P])
+_opt("cuacd_scorer_grad", _I, [_P, _P, _P, _P, _I, _P, _P])
+_opt("cuacd_scorer_train", _I, [_P, _P, _P, _P, _I, _I, _I, _F, _F, ctypes.c_uint, _P])
+_opt("cuacd_scorer_predict", _I, [_P, _P, _P, _I, _P])
+_opt("cuacd_eval_candidates_pruned", _I, [_P, _P, _P, _I, _P, _I, _F, _P, _I, _I, _F, _I, _I, _I, _F,
+                                          _P, _P, _P, _P])
 
 
 def _fn(name):

@@ -1,0 +1,786 @@
+// scorer.cu — learned candidate scorer: per-plane features, a 240-256-256-1
+// MLP in BF16 with FP32 accumulation on the tensor cores (mma.sync
+// m16n8k16), its training (MSE, AdamW) and the pruned evaluator that sends
+// only the best-predicted planes through the exact evaluator.
+//
+// Features of plane (n, d) on a part (230 used of SC_K = 240), positions
+// relative to the part's vertex centroid c, lengths scaled by R (half the
+// bounding-box diagonal):
+//   [0..3]    n, d + n.c (offset through the centroid) / R
+//   [4..35]   per side (positive, negative): vertex fraction, centroid (3),
+//             second moments (xx yy zz xy xz yz) (6), box min (3), max (3)
+//   [36..53]  part: centroid (3, absolute), second moments (6), box min (3),
+//             max (3), mesh volume, hull volume, rv cost
+//   [54..69]  histogram of the vertices' signed distances, 16 bins on [-R, R]
+//   [70..229] sketch: 80 vertices (index i*nv/80): signed distance to the
+//             plane / R and distance from the line (c, n) / R
+#include <vector>
+#include <algorithm>
+#include <random>
+#include <cmath>
+#include <cstring>
+#include <cuda_bf16.h>
+#include "context.cuh"
+#include "launch.h"
+
+#define SC_K      240          // padded feature width
+#define SC_NF     230          // features used
+#define SC_H      256          // hidden width
+#define SC_SKETCH 80
+#define SC_TSCALE 10.0f        // targets are scaled by this for the loss
+
+struct PartStats {             // per part, computed on the device
+    float c[3];                // vertex centroid
+    float m2[6];               // second moments about c
+    float lo[3], hi[3];        // box relative to c
+    float R;                   // half box diagonal
+    float mesh_vol, hull_vol, rv;
+};
+
+// ---------------------------------------------------------------------------
+// features
+// ---------------------------------------------------------------------------
+static __device__ __forceinline__ float sc_block_sum(float v, float* sh)
+{
+    v = warp_sum(v);
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    __syncthreads();
+    if (lane == 0) sh[w] = v;
+    __syncthreads();
+    float t = 0.f;
+    for (int i = 0; i < nw; i++) t += sh[i];
+    return t;
+}
+static __device__ __forceinline__ float sc_block_min(float v, float* sh)
+{
+    v = warp_min(v);
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    __syncthreads();
+    if (lane == 0) sh[w] = v;
+    __syncthreads();
+    float t = 3.4e38f;
+    for (int i = 0; i < nw; i++) t = fminf(t, sh[i]);
+    return t;
+}
+static __device__ __forceinline__ float sc_block_max(float v, float* sh)
+{
+    v = warp_max(v);
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    __syncthreads();
+    if (lane == 0) sh[w] = v;
+    __syncthreads();
+    float t = -3.4e38f;
+    for (int i = 0; i < nw; i++) t = fmaxf(t, sh[i]);
+    return t;
+}
+
+// One CTA: statistics of the part (v, t).
+__global__ void __launch_bounds__(256)
+k_part_stats(const float* __restrict__ v, int nv, const int* __restrict__ t, int nt, float hull_vol, PartStats* out)
+{
+    __shared__ float sh[8];
+    __shared__ double dsh[33];
+    float s[3] = {0.f, 0.f, 0.f};
+    for (int i = threadIdx.x; i < nv; i += 256) for (int k = 0; k < 3; k++) s[k] += v[3 * i + k];
+    float c[3];
+    for (int k = 0; k < 3; k++) c[k] = sc_block_sum(s[k], sh) / (float)(nv > 0 ? nv : 1);
+    float m[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, lo[3] = {3.4e38f, 3.4e38f, 3.4e38f}, hi[3] = {-3.4e38f, -3.4e38f, -3.4e38f};
+    for (int i = threadIdx.x; i < nv; i += 256) {
+        float x = v[3 * i] - c[0], y = v[3 * i + 1] - c[1], z = v[3 * i + 2] - c[2];
+        m[0] += x * x; m[1] += y * y; m[2] += z * z; m[3] += x * y; m[4] += x * z; m[5] += y * z;
+        lo[0] = fminf(lo[0], x); lo[1] = fminf(lo[1], y); lo[2] = fminf(lo[2], z);
+        hi[0] = fmaxf(hi[0], x); hi[1] = fmaxf(hi[1], y); hi[2] = fmaxf(hi[2], z);
+    }
+    PartStats P;
+    for (int k = 0; k < 3; k++) P.c[k] = c[k];
+    for (int k = 0; k < 6; k++) P.m2[k] = sc_block_sum(m[k], sh) / (float)(nv > 0 ? nv : 1);
+    for (int k = 0; k < 3; k++) { P.lo[k] = sc_block_min(lo[k], sh); P.hi[k] = sc_block_max(hi[k], sh); }
+    const double mv = fabs(block_mesh_signed_volume(v, nv, t, nt, dsh));
+    if (threadIdx.x == 0) {
+        float dx = P.hi[0] - P.lo[0], dy = P.hi[1] - P.lo[1], dz = P.hi[2] - P.lo[2];
+        P.R = 0.5f * sqrtf(dx * dx + dy * dy + dz * dz);
+        if (!(P.R > 0.f)) P.R = 1.f;
+        P.mesh_vol = (float)mv; P.hull_vol = hull_vol;
+        P.rv = part_cost_rv((double)hull_vol, mv);
+        *out = P;
+    }
+}
+
+// One CTA per plane: the feature row (SC_K floats, zero padded).
+__global__ void __launch_bounds__(256)
+k_cand_features(const float* __restrict__ v, int nv, const float4* __restrict__ planes, int n_planes,
+                const PartStats* __restrict__ stats, float* __restrict__ feat)
+{
+    __shared__ float sh[8];
+    __shared__ float hist[16];
+    const int p = blockIdx.x;
+    if (p >= n_planes) return;
+    const PartStats P = *stats;
+    const float4 pl = planes[p];
+    const float invR = 1.f / P.R;
+    float* f = feat + (size_t)p * SC_K;
+    if (threadIdx.x < 16) hist[threadIdx.x] = 0.f;
+    // per side: count, sum(3), second moments(6), box(6)
+    float cnt[2] = {0.f, 0.f}, sm[2][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
+    float mm[2][6] = {{0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f, 0.f, 0.f}};
+    float lo[2][3] = {{3.4e38f, 3.4e38f, 3.4e38f}, {3.4e38f, 3.4e38f, 3.4e38f}};
+    float hi[2][3] = {{-3.4e38f, -3.4e38f, -3.4e38f}, {-3.4e38f, -3.4e38f, -3.4e38f}};
+    __syncthreads();
+    for (int i = threadIdx.x; i < nv; i += 256) {
+        const float x = v[3 * i] - P.c[0], y = v[3 * i + 1] - P.c[1], z = v[3 * i + 2] - P.c[2];
+        const float sd = pl.x * v[3 * i] + pl.y * v[3 * i + 1] + pl.z * v[3 * i + 2] + pl.w;
+        int b = (int)floorf((sd * invR + 1.f) * 8.f);
+        b = min(15, max(0, b));
+        atomicAdd(&hist[b], 1.f);
+        if (sd == 0.f) continue;
+        const int s = sd > 0.f ? 0 : 1;
+        cnt[s] += 1.f; sm[s][0] += x; sm[s][1] += y; sm[s][2] += z;
+        mm[s][0] += x * x; mm[s][1] += y * y; mm[s][2] += z * z; mm[s][3] += x * y; mm[s][4] += x * z; mm[s][5] += y * z;
+        lo[s][0] = fminf(lo[s][0], x); lo[s][1] = fminf(lo[s][1], y); lo[s][2] = fminf(lo[s][2], z);
+        hi[s][0] = fmaxf(hi[s][0], x); hi[s][1] = fmaxf(hi[s][1], y); hi[s][2] = fmaxf(hi[s][2], z);
+    }
+    const float inv_nv = 1.f / (float)(nv > 0 ? nv : 1);
+    for (int s = 0; s < 2; s++) {
+        const float c = sc_block_sum(cnt[s], sh);
+        const float ic = c > 0.f ? 1.f / c : 0.f;
+        float o[16];
+        o[0] = c * inv_nv;
+        for (int k = 0; k < 3; k++) o[1 + k] = sc_block_sum(sm[s][k], sh) * ic * invR;
+        for (int k = 0; k < 6; k++) o[4 + k] = sc_block_sum(mm[s][k], sh) * ic * invR * invR;
+        for (int k = 0; k < 3; k++) {
+            const float a = sc_block_min(lo[s][k], sh), b = sc_block_max(hi[s][k], sh);
+            o[10 + k] = c > 0.f ? a * invR : 0.f;
+            o[13 + k] = c > 0.f ? b * invR : 0.f;
+        }
+        if (threadIdx.x == 0) for (int k = 0; k < 16; k++) f[4 + 16 * s + k] = o[k];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        f[0] = pl.x; f[1] = pl.y; f[2] = pl.z;
+        f[3] = (pl.w + pl.x * P.c[0] + pl.y * P.c[1] + pl.z * P.c[2]) * invR;
+        for (int k = 0; k < 3; k++) f[36 + k] = P.c[k];
+        for (int k = 0; k < 6; k++) f[39 + k] = P.m2[k] * invR * invR;
+        for (int k = 0; k < 3; k++) { f[45 + k] = P.lo[k] * invR; f[48 + k] = P.hi[k] * invR; }
+        f[51] = P.mesh_vol * invR * invR * invR; f[52] = P.hull_vol * invR * invR * invR; f[53] = P.rv * invR;
+        for (int k = 0; k < 16; k++) f[54 + k] = hist[k] * inv_nv;
+        for (int k = SC_NF; k < SC_K; k++) f[k] = 0.f;
+    }
+    if (threadIdx.x < SC_SKETCH) {
+        const int i = (int)(((long long)threadIdx.x * nv) / SC_SKETCH);
+        float sd = 0.f, rad = 0.f;
+        if (i < nv) {
+            const float x = v[3 * i] - P.c[0], y = v[3 * i + 1] - P.c[1], z = v[3 * i + 2] - P.c[2];
+            sd = pl.x * v[3 * i] + pl.y * v[3 * i + 1] + pl.z * v[3 * i + 2] + pl.w;
+            const float along = pl.x * x + pl.y * y + pl.z * z;
+            const float r2 = x * x + y * y + z * z - along * along;
+            rad = sqrtf(fmaxf(r2, 0.f));
+        }
+        f[70 + 2 * threadIdx.x] = sd * invR;
+        f[71 + 2 * threadIdx.x] = rad * invR;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// GEMM on the tensor cores: C[M x N] = alpha * op(A)[M x K] * op(B)[K x N]
+// (+ C if accumulate) (+ bias[j]) (* (mask(i,j) > 0)) (relu), BF16 operands,
+// FP32 accumulation.  A(i,k) = A[i*ar + k*ac], B(k,j) = B[k*br + j*bc], so
+// transposed operands need no copy.  Block tile 64 x 64, K step 32, four
+// warps of 32 x 32 (2 x 4 mma.sync m16n8k16 tiles each).
+// ---------------------------------------------------------------------------
+#define GM_BM 64
+#define GM_BN 64
+#define GM_BK 32
+#define GM_LD (GM_BK + 8)          // smem row pitch (bf16): rows stay 4-byte aligned, banks spread
+
+struct GemmArgs {
+    const __nv_bfloat16* A; long long ar, ac;
+    const __nv_bfloat16* B; long long br, bc;
+    float* Cf; __nv_bfloat16* Cb; int ldc;
+    int M, N, K;
+    const float* bias;
+    const __nv_bfloat16* mask; int ldm;
+    float alpha;
+    int relu, accumulate;
+};
+
+static __device__ __forceinline__ void mma_bf16_16816(float* d, const unsigned* a, const unsigned* b)
+{
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 "
+        "{%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+__global__ void __launch_bounds__(128)
+k_gemm_bf16(GemmArgs g)
+{
+    __shared__ __align__(16) __nv_bfloat16 As[GM_BM][GM_LD];
+    __shared__ __align__(16) __nv_bfloat16 Bs[GM_BN][GM_LD];     // B tile stored n-major (k contiguous)
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int m0 = blockIdx.y * GM_BM, n0 = blockIdx.x * GM_BN;
+    const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
+    const int gq = lane >> 2, tq = lane & 3;
+    float acc[2][4][4];
+    #pragma unroll
+    for (int i = 0; i < 2; i++)
+        #pragma unroll
+        for (int j = 0; j < 4; j++)
+            #pragma unroll
+            for (int k = 0; k < 4; k++) acc[i][j][k] = 0.f;
+    const __nv_bfloat16 zero = __float2bfloat16(0.f);
+    for (int k0 = 0; k0 < g.K; k0 += GM_BK) {
+        // stage the tiles; consecutive threads walk the operand's unit stride
+        for (int e = tid; e < GM_BM * GM_BK; e += 128) {
+            int r, c;
+            if (g.ac == 1) { r = e / GM_BK; c = e % GM_BK; } else { c = e / GM_BM; r = e % GM_BM; }
+            const int gi = m0 + r, gk = k0 + c;
+            As[r][c] = (gi < g.M && gk < g.K) ? g.A[gi * g.ar + gk * g.ac] : zero;
+        }
+        for (int e = tid; e < GM_BN * GM_BK; e += 128) {
+            int n, c;
+            if (g.br == 1) { n = e / GM_BK; c = e % GM_BK; } else { c = e / GM_BN; n = e % GM_BN; }
+            const int gj = n0 + n, gk = k0 + c;
+            Bs[n][c] = (gj < g.N && gk < g.K) ? g.B[gk * g.br + gj * g.bc] : zero;
+        }
+        __syncthreads();
+        #pragma unroll
+        for (int kk = 0; kk < GM_BK; kk += 16) {
+            unsigned af[2][4], bfr[4][2];
+            #pragma unroll
+            for (int i = 0; i < 2; i++) {
+                const int r = wm + 16 * i + gq;
+                af[i][0] = *(const unsigned*)&As[r][kk + 2 * tq];
+                af[i][1] = *(const unsigned*)&As[r + 8][kk + 2 * tq];
+                af[i][2] = *(const unsigned*)&As[r][kk + 2 * tq + 8];
+                af[i][3] = *(const unsigned*)&As[r + 8][kk + 2 * tq + 8];
+            }
+            #pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const int n = wn + 8 * j + gq;
+                bfr[j][0] = *(const unsigned*)&Bs[n][kk + 2 * tq];
+                bfr[j][1] = *(const unsigned*)&Bs[n][kk + 2 * tq + 8];
+            }
+            #pragma unroll
+            for (int i = 0; i < 2; i++)
+                #pragma unroll
+                for (int j = 0; j < 4; j++) mma_bf16_16816(acc[i][j], af[i], bfr[j]);
+        }
+        __syncthreads();
+    }
+    // epilogue
+    #pragma unroll
+    for (int i = 0; i < 2; i++)
+        #pragma unroll
+        for (int j = 0; j < 4; j++)
+            #pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const int r = m0 + wm + 16 * i + gq + (q >> 1) * 8;
+                const int c = n0 + wn + 8 * j + 2 * tq + (q & 1);
+                if (r >= g.M || c >= g.N) continue;
+                float x = g.alpha * acc[i][j][q];
+                const size_t o = (size_t)r * g.ldc + c;
+                if (g.accumulate && g.Cf) x += g.Cf[o];
+                if (g.bias) x += g.bias[c];
+                if (g.mask && !(__bfloat162float(g.mask[(size_t)r * g.ldm + c]) > 0.f)) x = 0.f;
+                if (g.relu) x = fmaxf(x, 0.f);
+                if (g.Cf) g.Cf[o] = x;
+                if (g.Cb) g.Cb[o] = __float2bfloat16(x);
+            }
+}
+
+static void gemm(const GemmArgs& g, cudaStream_t s)
+{
+    dim3 grid((g.N + GM_BN - 1) / GM_BN, (g.M + GM_BM - 1) / GM_BM);
+    if (g.M > 0 && g.N > 0) k_gemm_bf16<<<grid, 128, 0, s>>>(g);
+}
+
+__global__ void k_f32_to_bf16(const float* in, __nv_bfloat16* out, size_t n)
+{
+    size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = __float2bfloat16(in[i]);
+}
+
+// Rows idx[0..b) of X (fp32, SC_K wide), standardised by the scorer's
+// feature normaliser (nrm[k] = mean, nrm[SC_K + k] = 1 / std), into Xb
+// (bf16); targets likewise (scaled).
+__global__ void k_gather_rows(const float* X, const float* T, const int* idx, int b, const float* __restrict__ nrm,
+                              __nv_bfloat16* Xb, float* Tb)
+{
+    const int r = blockIdx.x;
+    if (r >= b) return;
+    const int src = idx ? idx[r] : r;
+    for (int k = threadIdx.x; k < SC_K; k += blockDim.x)
+        Xb[(size_t)r * SC_K + k] = __float2bfloat16((X[(size_t)src * SC_K + k] - nrm[k]) * nrm[SC_K + k]);
+    if (threadIdx.x == 0 && T) Tb[r] = T[src] * SC_TSCALE;
+}
+
+// dY = 2 (Y - T) / b (bf16 for the GEMMs, fp32 kept), loss = mean (Y - T)^2.
+__global__ void k_mse_grad(const float* Y, const float* T, int b, __nv_bfloat16* dYb, float* dYf, float* loss)
+{
+    __shared__ float sh[8];
+    float l = 0.f;
+    for (int i = threadIdx.x; i < b; i += blockDim.x) {
+        const float e = Y[i] - T[i];
+        l += e * e;
+        const float gr = 2.f * e / (float)b;
+        dYf[i] = gr;
+        dYb[i] = __float2bfloat16(gr);
+    }
+    l = sc_block_sum(l, sh);
+    if (threadIdx.x == 0) *loss = l / (float)b;
+}
+
+// Column sums of a b x n fp32 matrix (bias gradients).
+__global__ void k_colsum(const float* D, int b, int n, float* out)
+{
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    float s = 0.f;
+    for (int i = 0; i < b; i++) s += D[(size_t)i * n + j];
+    out[j] = s;
+}
+
+// AdamW on one flat parameter block (decoupled weight decay where decay=1).
+__global__ void k_adamw(float* p, const float* gr, float* m, float* v, __nv_bfloat16* pb, size_t n, float lr,
+                        float b1, float b2, float eps, float wd, float c1, float c2, int decay)
+{
+    size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float g = gr[i];
+    const float mi = b1 * m[i] + (1.f - b1) * g;
+    const float vi = b2 * v[i] + (1.f - b2) * g * g;
+    m[i] = mi; v[i] = vi;
+    float x = p[i];
+    if (decay) x -= lr * wd * x;
+    x -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+    p[i] = x;
+    if (pb) pb[i] = __float2bfloat16(x);
+}
+
+// ---------------------------------------------------------------------------
+// host: the scorer object
+// ---------------------------------------------------------------------------
+namespace {
+const size_t OFF_W1 = 0;
+const size_t OFF_B1 = OFF_W1 + (size_t)SC_K * SC_H;
+const size_t OFF_W2 = OFF_B1 + SC_H;
+const size_t OFF_B2 = OFF_W2 + (size_t)SC_H * SC_H;
+const size_t OFF_W3 = OFF_B2 + SC_H;
+const size_t OFF_B3 = OFF_W3 + SC_H;
+const size_t N_PARAMS = OFF_B3 + 1;
+}
+
+struct cuacd_scorer {
+    int device;
+    float* p32;                  // master parameters (fp32)
+    __nv_bfloat16* pb;           // bf16 copies for the GEMMs
+    float* g32;                  // gradients
+    float* nrm;                  // feature normaliser: mean[SC_K], 1/std[SC_K]
+    float* m; float* v;          // AdamW moments
+    int step;
+    // work buffers for batches of up to cap rows
+    int cap;
+    float* X; float* T;          // fp32 rows / targets (gathered from)
+    int n_rows_cap;
+    int* idx;
+    __nv_bfloat16 *Xb, *H1, *H2, *dYb, *dH2b, *dH1b;
+    float *Tb, *Y, *dYf, *dH2f, *dH1f, *loss;
+    // pruned-evaluation buffers
+    float* mv; int* mt; float4* mp; PartStats* st; float* feat;
+    size_t mv_cap, mt_cap, mp_cap;
+};
+
+static int sc_fail(gpu_ctx* ctx, int code, const char* msg) { return ctx_fail(ctx, code, "%s", msg); }
+
+#define SCK(call) do { cudaError_t _e = (call); if (_e != cudaSuccess) \
+    return ctx_fail(ctx, (int)_e, "%s failed: %s", #call, cudaGetErrorString(_e)); } while (0)
+
+static int sc_reserve(gpu_ctx* ctx, cuacd_scorer* s, int b)
+{
+    if (b <= s->cap) return 0;
+    int c = s->cap > 0 ? s->cap : 1024;
+    while (c < b) c *= 2;
+    cudaFree(s->idx); cudaFree(s->Xb); cudaFree(s->H1); cudaFree(s->H2); cudaFree(s->dYb); cudaFree(s->dH2b);
+    cudaFree(s->dH1b); cudaFree(s->Tb); cudaFree(s->Y); cudaFree(s->dYf); cudaFree(s->dH2f); cudaFree(s->dH1f);
+    SCK(cudaMalloc(&s->idx, sizeof(int) * c));
+    SCK(cudaMalloc(&s->Xb, sizeof(__nv_bfloat16) * (size_t)c * SC_K));
+    SCK(cudaMalloc(&s->H1, sizeof(__nv_bfloat16) * (size_t)c * SC_H));
+    SCK(cudaMalloc(&s->H2, sizeof(__nv_bfloat16) * (size_t)c * SC_H));
+    SCK(cudaMalloc(&s->dYb, sizeof(__nv_bfloat16) * c));
+    SCK(cudaMalloc(&s->dH2b, sizeof(__nv_bfloat16) * (size_t)c * SC_H));
+    SCK(cudaMalloc(&s->dH1b, sizeof(__nv_bfloat16) * (size_t)c * SC_H));
+    SCK(cudaMalloc(&s->Tb, sizeof(float) * c));
+    SCK(cudaMalloc(&s->Y, sizeof(float) * c));
+    SCK(cudaMalloc(&s->dYf, sizeof(float) * c));
+    SCK(cudaMalloc(&s->dH2f, sizeof(float) * (size_t)c * SC_H));
+    SCK(cudaMalloc(&s->dH1f, sizeof(float) * (size_t)c * SC_H));
+    s->cap = c;
+    return 0;
+}
+
+static GemmArgs gargs(const __nv_bfloat16* A, long long ar, long long ac, const __nv_bfloat16* B, long long br,
+                      long long bc, int M, int N, int K)
+{
+    GemmArgs g;
+    memset(&g, 0, sizeof(g));
+    g.A = A; g.ar = ar; g.ac = ac; g.B = B; g.br = br; g.bc = bc; g.M = M; g.N = N; g.K = K; g.alpha = 1.f;
+    return g;
+}
+
+// Forward of b gathered rows (s->Xb): H1, H2, Y (Y in target units x SC_TSCALE).
+static void sc_forward(cuacd_scorer* s, int b, cudaStream_t st)
+{
+    GemmArgs g = gargs(s->Xb, SC_K, 1, s->pb + OFF_W1, SC_H, 1, b, SC_H, SC_K);
+    g.bias = s->p32 + OFF_B1; g.relu = 1; g.Cb = s->H1; g.ldc = SC_H;
+    gemm(g, st);
+    g = gargs(s->H1, SC_H, 1, s->pb + OFF_W2, SC_H, 1, b, SC_H, SC_H);
+    g.bias = s->p32 + OFF_B2; g.relu = 1; g.Cb = s->H2; g.ldc = SC_H;
+    gemm(g, st);
+    g = gargs(s->H2, SC_H, 1, s->pb + OFF_W3, 1, 0, b, 1, SC_H);
+    g.bias = s->p32 + OFF_B3; g.Cf = s->Y; g.ldc = 1;
+    gemm(g, st);
+}
+
+// Loss and gradients of the gathered batch into s->g32.
+static void sc_backward(cuacd_scorer* s, int b, cudaStream_t st)
+{
+    k_mse_grad<<<1, 256, 0, st>>>(s->Y, s->Tb, b, s->dYb, s->dYf, s->loss);
+    // W3, b3
+    GemmArgs g = gargs(s->H2, 1, SC_H, s->dYb, 1, 0, SC_H, 1, b);
+    g.Cf = s->g32 + OFF_W3; g.ldc = 1;
+    gemm(g, st);
+    k_colsum<<<1, 32, 0, st>>>(s->dYf, b, 1, s->g32 + OFF_B3);
+    // dH2 = dY W3^T (H2 > 0)
+    g = gargs(s->dYb, 1, 0, s->pb + OFF_W3, 0, 1, b, SC_H, 1);
+    g.mask = s->H2; g.ldm = SC_H; g.Cf = s->dH2f; g.Cb = s->dH2b; g.ldc = SC_H;
+    gemm(g, st);
+    // W2, b2
+    g = gargs(s->H1, 1, SC_H, s->dH2b, SC_H, 1, SC_H, SC_H, b);
+    g.Cf = s->g32 + OFF_W2; g.ldc = SC_H;
+    gemm(g, st);
+    k_colsum<<<(SC_H + 127) / 128, 128, 0, st>>>(s->dH2f, b, SC_H, s->g32 + OFF_B2);
+    // dH1 = dH2 W2^T (H1 > 0)
+    g = gargs(s->dH2b, SC_H, 1, s->pb + OFF_W2, 1, SC_H, b, SC_H, SC_H);
+    g.mask = s->H1; g.ldm = SC_H; g.Cf = s->dH1f; g.Cb = s->dH1b; g.ldc = SC_H;
+    gemm(g, st);
+    // W1, b1
+    g = gargs(s->Xb, 1, SC_K, s->dH1b, SC_H, 1, SC_K, SC_H, b);
+    g.Cf = s->g32 + OFF_W1; g.ldc = SC_H;
+    gemm(g, st);
+    k_colsum<<<(SC_H + 127) / 128, 128, 0, st>>>(s->dH1f, b, SC_H, s->g32 + OFF_B1);
+}
+
+static void sc_adamw(cuacd_scorer* s, float lr, float wd, cudaStream_t st)
+{
+    s->step++;
+    const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+    const float c1 = 1.f - powf(b1, (float)s->step), c2 = 1.f - powf(b2, (float)s->step);
+    const size_t blocks[6][2] = {{OFF_W1, (size_t)SC_K * SC_H}, {OFF_B1, SC_H}, {OFF_W2, (size_t)SC_H * SC_H},
+                                 {OFF_B2, SC_H}, {OFF_W3, SC_H}, {OFF_B3, 1}};
+    for (int i = 0; i < 6; i++) {
+        const size_t o = blocks[i][0], n = blocks[i][1];
+        k_adamw<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(s->p32 + o, s->g32 + o, s->m + o, s->v + o, s->pb + o, n,
+                                                             lr, b1, b2, eps, wd, c1, c2, (i % 2) == 0);
+    }
+}
+
+static int sc_upload_rows(gpu_ctx* ctx, cuacd_scorer* s, const float* X, const float* T, int n)
+{
+    if (n > s->n_rows_cap) {
+        cudaFree(s->X); cudaFree(s->T);
+        SCK(cudaMalloc(&s->X, sizeof(float) * (size_t)n * SC_K));
+        SCK(cudaMalloc(&s->T, sizeof(float) * (size_t)(n > 0 ? n : 1)));
+        s->n_rows_cap = n;
+    }
+    SCK(cudaMemcpyAsync(s->X, X, sizeof(float) * (size_t)n * SC_K, cudaMemcpyHostToDevice, ctx->stream));
+    if (T) SCK(cudaMemcpyAsync(s->T, T, sizeof(float) * (size_t)n, cudaMemcpyHostToDevice, ctx->stream));
+    return 0;
+}
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" int cuacd_scorer_n_params(void) { return (int)N_PARAMS; }
+extern "C" int cuacd_scorer_n_features(void) { return SC_K; }
+
+extern "C" int cuacd_scorer_create(gpu_ctx_t ctx, unsigned seed, cuacd_scorer_t* out)
+{
+    if (!ctx || !out) return -1;
+    *out = nullptr;
+    SCK(cudaSetDevice(ctx->device));
+    cuacd_scorer* s = (cuacd_scorer*)calloc(1, sizeof(cuacd_scorer));
+    if (!s) return sc_fail(ctx, -1, "out of host memory");
+    s->device = ctx->device;
+    cudaError_t e = cudaMalloc(&s->p32, sizeof(float) * N_PARAMS);
+    if (!e) e = cudaMalloc(&s->pb, sizeof(__nv_bfloat16) * N_PARAMS);
+    if (!e) e = cudaMalloc(&s->g32, sizeof(float) * N_PARAMS);
+    if (!e) e = cudaMalloc(&s->m, sizeof(float) * N_PARAMS);
+    if (!e) e = cudaMalloc(&s->v, sizeof(float) * N_PARAMS);
+    if (!e) e = cudaMalloc(&s->loss, sizeof(float));
+    if (!e) e = cudaMalloc(&s->nrm, sizeof(float) * 2 * SC_K);
+    if (e) { cuacd_scorer_free(s); return ctx_fail(ctx, (int)e, "scorer allocation failed: %s", cudaGetErrorString(e)); }
+    // He-uniform weights, zero biases
+    std::vector<float> p(N_PARAMS, 0.f);
+    std::mt19937 rng(seed);
+    auto fill = [&](size_t off, int fan_in, size_t n) {
+        const float a = sqrtf(6.f / (float)fan_in);
+        std::uniform_real_distribution<float> U(-a, a);
+        for (size_t i = 0; i < n; i++) p[off + i] = U(rng);
+    };
+    fill(OFF_W1, SC_NF, (size_t)SC_K * SC_H);
+    for (int k = SC_NF; k < SC_K; k++) for (int j = 0; j < SC_H; j++) p[OFF_W1 + (size_t)k * SC_H + j] = 0.f;
+    fill(OFF_W2, SC_H, (size_t)SC_H * SC_H);
+    fill(OFF_W3, SC_H, SC_H);
+    *out = s;
+    std::vector<float> nrm(2 * SC_K, 0.f);
+    for (int k = 0; k < SC_K; k++) nrm[SC_K + k] = 1.f;
+    if (cuacd_scorer_set_normalizer(s, nrm.data(), nrm.data() + SC_K)) return ctx_fail(ctx, -1, "scorer set-up failed");
+    return cuacd_scorer_set_params(s, p.data());
+}
+
+extern "C" int cuacd_scorer_set_normalizer(cuacd_scorer_t s, const float* mean, const float* inv_std)
+{
+    if (!s || !mean || !inv_std) return -1;
+    if (cudaSetDevice(s->device)) return -1;
+    if (cudaMemcpy(s->nrm, mean, sizeof(float) * SC_K, cudaMemcpyHostToDevice)) return -1;
+    return cudaMemcpy(s->nrm + SC_K, inv_std, sizeof(float) * SC_K, cudaMemcpyHostToDevice) == cudaSuccess ? 0 : -1;
+}
+
+extern "C" int cuacd_scorer_get_normalizer(cuacd_scorer_t s, float* mean, float* inv_std)
+{
+    if (!s || !mean || !inv_std) return -1;
+    if (cudaSetDevice(s->device)) return -1;
+    if (cudaMemcpy(mean, s->nrm, sizeof(float) * SC_K, cudaMemcpyDeviceToHost)) return -1;
+    return cudaMemcpy(inv_std, s->nrm + SC_K, sizeof(float) * SC_K, cudaMemcpyDeviceToHost) == cudaSuccess ? 0 : -1;
+}
+
+extern "C" void cuacd_scorer_free(cuacd_scorer_t s)
+{
+    if (!s) return;
+    cudaSetDevice(s->device);
+    cudaFree(s->p32); cudaFree(s->pb); cudaFree(s->g32); cudaFree(s->m); cudaFree(s->v); cudaFree(s->loss);
+    cudaFree(s->nrm);
+    cudaFree(s->X); cudaFree(s->T); cudaFree(s->idx); cudaFree(s->Xb); cudaFree(s->H1); cudaFree(s->H2);
+    cudaFree(s->dYb); cudaFree(s->dH2b); cudaFree(s->dH1b); cudaFree(s->Tb); cudaFree(s->Y); cudaFree(s->dYf);
+    cudaFree(s->dH2f); cudaFree(s->dH1f); cudaFree(s->mv); cudaFree(s->mt); cudaFree(s->mp); cudaFree(s->st);
+    free(s);                     // s->feat points into s->mp
+    cudaGetLastError();          // a failed free must not surface in the next call's launch check
+}
+
+extern "C" int cuacd_scorer_set_params(cuacd_scorer_t s, const float* params)
+{
+    if (!s || !params) return -1;
+    if (cudaSetDevice(s->device)) return -1;
+    if (cudaMemcpy(s->p32, params, sizeof(float) * N_PARAMS, cudaMemcpyHostToDevice)) return -1;
+    k_f32_to_bf16<<<(unsigned)((N_PARAMS + 255) / 256), 256>>>(s->p32, s->pb, N_PARAMS);
+    if (cudaMemset(s->m, 0, sizeof(float) * N_PARAMS) || cudaMemset(s->v, 0, sizeof(float) * N_PARAMS)) return -1;
+    s->step = 0;
+    return cudaDeviceSynchronize() == cudaSuccess ? 0 : -1;
+}
+
+extern "C" int cuacd_scorer_get_params(cuacd_scorer_t s, float* params)
+{
+    if (!s || !params) return -1;
+    if (cudaSetDevice(s->device)) return -1;
+    return cudaMemcpy(params, s->p32, sizeof(float) * N_PARAMS, cudaMemcpyDeviceToHost) == cudaSuccess ? 0 : -1;
+}
+
+// Features of n planes on one part (host pointers), SC_K floats per plane.
+static int sc_features_device(gpu_ctx* ctx, cuacd_scorer* s, const float* verts, int nv, const int* tris, int nt,
+                              float hull_vol, const float* planes, int n, cudaStream_t st)
+{
+    auto grow = [&](void** p, size_t& cap, size_t need) -> int {
+        if (need <= cap) return 0;
+        cudaFree(*p);
+        SCK(cudaMalloc(p, need));
+        cap = need;
+        return 0;
+    };
+    if (grow((void**)&s->mv, s->mv_cap, 12 * (size_t)nv)) return -1;
+    if (grow((void**)&s->mt, s->mt_cap, 12 * (size_t)(nt > 0 ? nt : 1))) return -1;
+    const size_t plane_bytes = (16 * (size_t)n + 255) & ~(size_t)255;
+    if (grow((void**)&s->mp, s->mp_cap, plane_bytes + sizeof(float) * (size_t)n * SC_K)) return -1;
+    if (!s->st) SCK(cudaMalloc(&s->st, sizeof(PartStats)));
+    s->feat = (float*)((char*)s->mp + plane_bytes);
+    SCK(cudaMemcpyAsync(s->mv, verts, 12 * (size_t)nv, cudaMemcpyHostToDevice, st));
+    if (nt) SCK(cudaMemcpyAsync(s->mt, tris, 12 * (size_t)nt, cudaMemcpyHostToDevice, st));
+    SCK(cudaMemcpyAsync(s->mp, planes, 16 * (size_t)n, cudaMemcpyHostToDevice, st));
+    k_part_stats<<<1, 256, 0, st>>>(s->mv, nv, s->mt, nt, hull_vol, s->st);
+    k_cand_features<<<n, 256, 0, st>>>(s->mv, nv, s->mp, n, s->st, s->feat);
+    ctx->launches += 2;
+    SCK(cudaGetLastError());
+    return 0;
+}
+
+extern "C" int cuacd_candidate_features(gpu_ctx_t ctx, cuacd_scorer_t s, const float* verts, int nv, const int* tris,
+                                        int nt, float hull_vol, const float* planes, int n, float* out)
+{
+    if (!ctx || !s || !out) return -1;
+    if (n <= 0) return 0;
+    if (nv <= 0) return ctx_fail(ctx, KERR_MESH_INVALID, "empty mesh");
+    for (int i = 0; i < 3 * nt; i++) if (tris[i] < 0 || tris[i] >= nv) return ctx_fail(ctx, KERR_MESH_INVALID, "index out of range");
+    SCK(cudaSetDevice(ctx->device));
+    if (sc_features_device(ctx, s, verts, nv, tris, nt, hull_vol, planes, n, ctx->stream)) return -1;
+    SCK(cudaMemcpyAsync(out, s->feat, sizeof(float) * (size_t)n * SC_K, cudaMemcpyDeviceToHost, ctx->stream));
+    return sync_and_check(ctx, "candidate_features");
+}
+
+extern "C" int cuacd_scorer_grad(gpu_ctx_t ctx, cuacd_scorer_t s, const float* X, const float* T, int n,
+                                 float* loss, float* grads)
+{
+    if (!ctx || !s || !X || !T || n <= 0) return -1;
+    SCK(cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    if (sc_reserve(ctx, s, n) || sc_upload_rows(ctx, s, X, T, n)) return -1;
+    k_gather_rows<<<n, 64, 0, st>>>(s->X, s->T, nullptr, n, s->nrm, s->Xb, s->Tb);
+    sc_forward(s, n, st);
+    sc_backward(s, n, st);
+    ctx->launches += 13;
+    SCK(cudaGetLastError());
+    if (loss) SCK(cudaMemcpyAsync(loss, s->loss, sizeof(float), cudaMemcpyDeviceToHost, st));
+    if (grads) SCK(cudaMemcpyAsync(grads, s->g32, sizeof(float) * N_PARAMS, cudaMemcpyDeviceToHost, st));
+    return sync_and_check(ctx, "scorer_grad");
+}
+
+extern "C" int cuacd_scorer_train(gpu_ctx_t ctx, cuacd_scorer_t s, const float* X, const float* T, int n, int epochs,
+                                  int batch, float lr, float wd, unsigned seed, float* final_loss)
+{
+    if (!ctx || !s || !X || !T || n <= 0 || epochs <= 0 || batch <= 0) return -1;
+    SCK(cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    batch = std::min(batch, n);
+    if (sc_reserve(ctx, s, batch) || sc_upload_rows(ctx, s, X, T, n)) return -1;
+    std::vector<int> perm(n);
+    for (int i = 0; i < n; i++) perm[i] = i;
+    std::mt19937 rng(seed);
+    int* d_perm = nullptr;
+    SCK(cudaMalloc(&d_perm, sizeof(int) * (size_t)n));
+    double loss_sum = 0.0; int loss_cnt = 0;
+    std::vector<float> losses;
+    float* d_losses = nullptr;
+    const int steps_per_epoch = n / batch;
+    SCK(cudaMalloc(&d_losses, sizeof(float) * (size_t)(steps_per_epoch > 0 ? steps_per_epoch : 1)));
+    for (int ep = 0; ep < epochs; ep++) {
+        std::shuffle(perm.begin(), perm.end(), rng);
+        SCK(cudaMemcpyAsync(d_perm, perm.data(), sizeof(int) * (size_t)n, cudaMemcpyHostToDevice, st));
+        for (int b = 0; b < steps_per_epoch; b++) {
+            k_gather_rows<<<batch, 64, 0, st>>>(s->X, s->T, d_perm + (size_t)b * batch, batch, s->nrm, s->Xb,
+                                                 s->Tb);
+            sc_forward(s, batch, st);
+            sc_backward(s, batch, st);
+            sc_adamw(s, lr, wd, st);
+            cudaMemcpyAsync(d_losses + b, s->loss, sizeof(float), cudaMemcpyDeviceToDevice, st);
+            ctx->launches += 20;
+        }
+        if (ep == epochs - 1 && steps_per_epoch > 0) {
+            losses.resize(steps_per_epoch);
+            SCK(cudaMemcpyAsync(losses.data(), d_losses, sizeof(float) * steps_per_epoch, cudaMemcpyDeviceToHost, st));
+        }
+    }
+    int rc = sync_and_check(ctx, "scorer_train");
+    cudaFree(d_perm); cudaFree(d_losses);
+    if (rc) return rc;
+    for (float l : losses) { loss_sum += l; loss_cnt++; }
+    if (final_loss) *final_loss = loss_cnt ? (float)(loss_sum / loss_cnt) / (SC_TSCALE * SC_TSCALE) : 0.f;
+    return 0;
+}
+
+// Predicted scores of rows already gathered in s->Xb (device), into s->Y.
+static void sc_predict_rows(cuacd_scorer* s, int n, cudaStream_t st) { sc_forward(s, n, st); }
+
+extern "C" int cuacd_scorer_predict(gpu_ctx_t ctx, cuacd_scorer_t s, const float* X, int n, float* out)
+{
+    if (!ctx || !s || !X || !out) return -1;
+    if (n <= 0) return 0;
+    SCK(cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    if (sc_reserve(ctx, s, n) || sc_upload_rows(ctx, s, X, nullptr, n)) return -1;
+    k_gather_rows<<<n, 64, 0, st>>>(s->X, nullptr, nullptr, n, s->nrm, s->Xb, nullptr);
+    sc_predict_rows(s, n, st);
+    ctx->launches += 4;
+    SCK(cudaGetLastError());
+    std::vector<float> y(n);
+    SCK(cudaMemcpyAsync(y.data(), s->Y, sizeof(float) * (size_t)n, cudaMemcpyDeviceToHost, st));
+    int rc = sync_and_check(ctx, "scorer_predict");
+    if (rc) return rc;
+    for (int i = 0; i < n; i++) out[i] = y[i] / SC_TSCALE;
+    return 0;
+}
+
+// Surrogate-pruned evaluation of n planes on one mesh (host pointers; hull_vol
+// < 0 computes the part's hull volume here): the
+// network predicts every plane's score_full; the top_k lowest predictions,
+// plus every plane whose prediction lies within `margin` of the k-th (the
+// cases where the ranking is too close to trust), go through the exact
+// evaluator.  out[i] is the exact result of an evaluated plane; the others
+// get ok = 0 and scores of FLT_MAX.  out_pred (optional) receives the
+// predictions, out_evaluated (optional) 1/0 per plane; *out_n_evaluated the
+// count.
+extern "C" int cuacd_eval_candidates_pruned(gpu_ctx_t ctx, cuacd_scorer_t s, const float* verts, int nv,
+                                            const int* tris, int nt, float hull_vol, const float* planes,
+                                            int n_planes, int flags,
+                                            float hd_resolution, int hd_min_samples, int hd_total, int top_k,
+                                            float margin, cuacd_cand_result* out, float* out_pred,
+                                            int* out_evaluated, int* out_n_evaluated)
+{
+    if (!ctx || !s || !out) return -1;
+    if (out_n_evaluated) *out_n_evaluated = 0;
+    if (n_planes <= 0) return 0;
+    if (nv <= 0 || nt <= 0) return ctx_fail(ctx, KERR_MESH_INVALID, "empty mesh");
+    for (int i = 0; i < 3 * nt; i++)
+        if (tris[i] < 0 || tris[i] >= nv) return ctx_fail(ctx, KERR_MESH_INVALID, "triangle index out of range");
+    if (top_k <= 0) top_k = 1;
+    SCK(cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    if (hull_vol < 0.f) {       // the exact hull of the part's vertices
+        std::vector<float> hv(3 * (size_t)nv);
+        std::vector<int> ht(6 * (size_t)nv + 12);
+        int hnv = 0, hnt = 0, herr = 0;
+        const int off[2] = {0, nv};
+        int rc = gpu_kdop_hull(ctx, verts, nv, off, 1, nv, 2 * nv + 4, hv.data(), ht.data(), &hnv, &hnt,
+                               &hull_vol, &herr);
+        if (rc) return rc;
+    }
+    if (sc_features_device(ctx, s, verts, nv, tris, nt, hull_vol, planes, n_planes, st)) return -1;
+    if (sc_reserve(ctx, s, n_planes)) return -1;
+    k_gather_rows<<<n_planes, 64, 0, st>>>(s->feat, nullptr, nullptr, n_planes, s->nrm, s->Xb, nullptr);
+    sc_predict_rows(s, n_planes, st);
+    ctx->launches += 4;
+    SCK(cudaGetLastError());
+    std::vector<float> pred(n_planes);
+    SCK(cudaMemcpyAsync(pred.data(), s->Y, sizeof(float) * (size_t)n_planes, cudaMemcpyDeviceToHost, st));
+    int rc = sync_and_check(ctx, "scorer_predict");
+    if (rc) return rc;
+    for (int i = 0; i < n_planes; i++) pred[i] /= SC_TSCALE;
+    std::vector<int> order(n_planes);
+    for (int i = 0; i < n_planes; i++) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return pred[a] < pred[b]; });
+    const int k = std::min(top_k, n_planes);
+    const float kth = pred[order[k - 1]];
+    std::vector<int> sel;
+    for (int r = 0; r < n_planes; r++) {
+        const int i = order[r];
+        if (r < k || pred[i] <= kth + margin) sel.push_back(i);
+    }
+    std::sort(sel.begin(), sel.end());
+    std::vector<float> sp(4 * sel.size());
+    for (size_t j = 0; j < sel.size(); j++) memcpy(&sp[4 * j], planes + 4 * (size_t)sel[j], 16);
+    std::vector<cuacd_cand_result> res(sel.size());
+    rc = cuacd_eval_candidates(ctx, verts, nv, tris, nt, sp.data(), (int)sel.size(), flags, hd_resolution,
+                               hd_min_samples, hd_total, res.data());
+    if (rc) return rc;
+    for (int i = 0; i < n_planes; i++) {
+        cuacd_cand_result& r = out[i];
+        memset(&r, 0, sizeof(r));
+        r.score_rv = r.score_full = 3.402823466e38f;
+        if (out_evaluated) out_evaluated[i] = 0;
+        if (out_pred) out_pred[i] = pred[i];
+    }
+    for (size_t j = 0; j < sel.size(); j++) {
+        out[sel[j]] = res[j];
+        if (out_evaluated) out_evaluated[sel[j]] = 1;
+    }
+    if (out_n_evaluated) *out_n_evaluated = (int)sel.size();
+    return 0;
+}

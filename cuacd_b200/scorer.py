@@ -1,0 +1,278 @@
+"""Learned candidate scorer: a 240-256-256-1 MLP that predicts a plane's
+exact score (score_full: the worst part cost of the cut, Hausdorff
+included), relative to the mean over its part's planes, from features
+computed on the GPU; trained on the GPU by the library's own BF16
+tensor-core forward, backward and AdamW kernels.
+
+The exact evaluator stays the judge: `Scorer.eval_pruned` sends the
+top-k best-predicted planes, plus every plane predicted within `margin` of
+the k-th, through `cuacd_eval_candidates`; final part costs are always
+computed exactly.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+from . import CandResult, _fn, _as_f32, _as_i32, _ptr, cand_to_dict
+
+WEIGHTS_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "scorer_weights.npz")
+
+N_FEATURES = 240
+HIDDEN = 256
+T_SCALE = 10.0          # the network's raw output is T_SCALE x the predicted score
+
+
+def n_params():
+    return int(_fn("cuacd_scorer_n_params")())
+
+
+def unpack(params):
+    """Flat parameter vector -> dict W1 (240x256), b1, W2 (256x256), b2, W3 (256,), b3 (1,)."""
+    p = np.asarray(params)
+    k, h = N_FEATURES, HIDDEN
+    o = 0
+    out = {}
+    for name, shape in (("W1", (k, h)), ("b1", (h,)), ("W2", (h, h)), ("b2", (h,)), ("W3", (h,)), ("b3", (1,))):
+        n = int(np.prod(shape))
+        out[name] = p[o:o + n].reshape(shape)
+        o += n
+    assert o == len(p)
+    return out
+
+
+class Scorer:
+    """Device-resident scorer bound to one `Context`."""
+
+    def __init__(self, ctx, seed=0, params=None):
+        self._ctx = ctx
+        h = ctypes.c_void_p()
+        ctx._check(_fn("cuacd_scorer_create")(ctx.handle, ctypes.c_uint(seed), ctypes.byref(h)))
+        self._h = h
+        if params is not None:
+            self.set_params(params)
+
+    @classmethod
+    def load(cls, ctx, path=WEIGHTS_PATH):
+        with np.load(path) as z:
+            s = cls(ctx, params=z["params"].astype(np.float32))
+            s.set_normalizer(z["mean"], z["inv_std"])
+        return s
+
+    def save(self, path, **meta):
+        mean, inv_std = self.normalizer()
+        np.savez_compressed(path, params=self.params(), mean=mean, inv_std=inv_std, **meta)
+
+    def close(self):
+        if self._h:
+            _fn("cuacd_scorer_free")(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # -- parameters ----------------------------------------------------------
+    def params(self):
+        out = np.empty(n_params(), np.float32)
+        self._ctx._check(_fn("cuacd_scorer_get_params")(self._h, _ptr(out)))
+        return out
+
+    def set_params(self, params):
+        p = _as_f32(params).ravel()
+        if len(p) != n_params():
+            raise ValueError(f"expected {n_params()} parameters, got {len(p)}")
+        self._ctx._check(_fn("cuacd_scorer_set_params")(self._h, _ptr(p)))
+
+    def normalizer(self):
+        mean = np.empty(N_FEATURES, np.float32)
+        inv = np.empty(N_FEATURES, np.float32)
+        self._ctx._check(_fn("cuacd_scorer_get_normalizer")(self._h, _ptr(mean), _ptr(inv)))
+        return mean, inv
+
+    def set_normalizer(self, mean, inv_std):
+        m, i = _as_f32(mean).ravel(), _as_f32(inv_std).ravel()
+        if len(m) != N_FEATURES or len(i) != N_FEATURES:
+            raise ValueError(f"normaliser vectors must have {N_FEATURES} entries")
+        self._ctx._check(_fn("cuacd_scorer_set_normalizer")(self._h, _ptr(m), _ptr(i)))
+
+    def fit_normalizer(self, X):
+        """Standardise each feature by its mean and std over X (constant
+        features are zeroed)."""
+        X = np.asarray(X, np.float64)
+        mean, sd = X.mean(0), X.std(0)
+        inv = np.where(sd > 1e-6, 1.0 / np.maximum(sd, 1e-6), 0.0)
+        self.set_normalizer(mean.astype(np.float32), inv.astype(np.float32))
+
+    # -- features, training, prediction --------------------------------------
+    def features(self, verts, tris, planes, hull_vol):
+        v, t = _as_f32(verts).reshape(-1, 3), _as_i32(tris).reshape(-1, 3)
+        p = _as_f32(planes).reshape(-1, 4)
+        out = np.zeros((len(p), N_FEATURES), np.float32)
+        if len(p):
+            self._ctx._check(_fn("cuacd_candidate_features")(self._ctx.handle, self._h, _ptr(v), len(v), _ptr(t), len(t),
+                                                             float(hull_vol), _ptr(p), len(p), _ptr(out)))
+        return out
+
+    def grad(self, X, T):
+        """(scaled loss, flat gradients) of one batch: loss = mean((y_raw - 10 T)^2)."""
+        X, T = _as_f32(X).reshape(-1, N_FEATURES), _as_f32(T).ravel()
+        loss = np.zeros(1, np.float32)
+        g = np.empty(n_params(), np.float32)
+        self._ctx._check(_fn("cuacd_scorer_grad")(self._ctx.handle, self._h, _ptr(X), _ptr(T), len(X), _ptr(loss), _ptr(g)))
+        return float(loss[0]), g
+
+    def train(self, X, T, epochs=10, batch=256, lr=1e-3, wd=1e-4, seed=0):
+        """AdamW epochs on the device; returns the last epoch's mean (unscaled) MSE."""
+        X, T = _as_f32(X).reshape(-1, N_FEATURES), _as_f32(T).ravel()
+        out = np.zeros(1, np.float32)
+        self._ctx._check(_fn("cuacd_scorer_train")(self._ctx.handle, self._h, _ptr(X), _ptr(T), len(X), int(epochs),
+                                                   int(batch), float(lr), float(wd), ctypes.c_uint(seed), _ptr(out)))
+        return float(out[0])
+
+    def predict(self, X):
+        X = _as_f32(X).reshape(-1, N_FEATURES)
+        out = np.zeros(len(X), np.float32)
+        if len(X):
+            self._ctx._check(_fn("cuacd_scorer_predict")(self._ctx.handle, self._h, _ptr(X), len(X), _ptr(out)))
+        return out
+
+    def eval_pruned(self, verts, tris, planes, top_k=8, margin=0.0, hull_vol=-1.0, hausdorff=True,
+                    resolution=2000.0, min_samples=1000, total=0):
+        """Surrogate-pruned evaluation -> (results as dicts, predictions, evaluated mask).
+        Unevaluated planes have ok = 0 and scores of FLT_MAX."""
+        v, t = _as_f32(verts).reshape(-1, 3), _as_i32(tris).reshape(-1, 3)
+        p = _as_f32(planes).reshape(-1, 4)
+        n = len(p)
+        out = (CandResult * max(n, 1))()
+        pred = np.zeros(n, np.float32)
+        ev = np.zeros(n, np.int32)
+        ne = ctypes.c_int(0)
+        self._ctx._check(_fn("cuacd_eval_candidates_pruned")(
+            self._ctx.handle, self._h, _ptr(v), len(v), _ptr(t), len(t), float(hull_vol), _ptr(p), n,
+            1 if hausdorff else 0, float(resolution), int(min_samples), int(total), int(top_k), float(margin),
+            ctypes.cast(out, ctypes.c_void_p), _ptr(pred), _ptr(ev), ctypes.byref(ne)))
+        return [cand_to_dict(out[i]) for i in range(n)], pred, ev.astype(bool)
+
+
+def part_hull_volume(ctx, verts):
+    vol, _ = ctx.batch_hull_volume([_as_f32(verts).reshape(-1, 3)])
+    return float(vol[0])
+
+
+def candidate_set(ctx, verts, tris, n_concave_edges=16, width=3, max_concave=27):
+    """The planes one search level scores on a part: up to `max_concave`
+    concave-edge planes followed by `width` axis-aligned cuts (30 planes at
+    the defaults; zero planes of too-narrow axes dropped)."""
+    conc, axis, valid = ctx.candidate_planes(verts, tris, n_concave_edges=n_concave_edges, width=width)
+    planes = np.concatenate([conc.reshape(-1, 4)[:max_concave], axis.reshape(-1, 4)[valid]])
+    keep = np.any(planes[:, :3] != 0, axis=1)
+    return planes[keep]
+
+
+def exact_pairs(ctx, scorer, verts, tris, planes, **eval_kw):
+    """(features, targets, ok mask, exact results) of planes on one part.
+    The target is the exact score_full; a plane that leaves one side empty
+    (ok = 0) takes the worst score among the part's splitting planes, so it
+    ranks last."""
+    hv = part_hull_volume(ctx, verts)
+    X = scorer.features(verts, tris, planes, hv)
+    res = ctx.eval_candidates(verts, tris, planes, **eval_kw)
+    T = np.array([r["score_full"] for r in res], np.float32)
+    ok = np.array([bool(r["ok"]) and r["err"] == 0 for r in res])
+    T[~ok] = T[ok].max() if ok.any() else 1.0
+    return X, T, ok, res
+
+
+def training_meshes(n, seed):
+    """Seeded synthetic parts with concave creases (the kind the search
+    cuts): ridged displaced UV spheres and icospheres of varying resolution
+    and amplitude, and strongly displaced smooth icospheres, all normalised
+    to extent 2."""
+    from . import workloads as W
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        kind = i % 3
+        s = int(rng.integers(1 << 30))
+        if kind == 0:
+            n_lon = int(rng.choice([32, 48, 64, 96, 128]))
+            n_rings = int(rng.integers(12, 41))
+            v, t = W.candidate_mesh(n_lon, n_rings, float(rng.uniform(0.2, 0.5)), s)
+        elif kind == 1:
+            v, t = W.icosphere(int(rng.integers(3, 6)))
+            v, t = W.displaced_sphere(v, t, float(rng.uniform(0.2, 0.5)), s, n_terms=6, fmin=2.0, fmax=5.0,
+                                      ridged=True)
+        else:
+            v, t = W.icosphere(int(rng.integers(3, 5)))
+            v, t = W.displaced_sphere(v, t, float(rng.uniform(0.5, 0.7)), s, n_terms=8, fmin=1.0, fmax=6.0)
+        v = W.normalize_extent(v).astype(np.float32)
+        out.append((np.ascontiguousarray(v, np.float32), np.ascontiguousarray(t, np.int32)))
+    return out
+
+
+def centered(T, groups):
+    """Targets relative to their part's mean: the ranking within a part is
+    all the pruning uses, so the network is trained on that."""
+    T = np.asarray(T, np.float64)
+    mean = np.bincount(groups, T) / np.maximum(np.bincount(groups), 1)
+    return (T - mean[groups]).astype(np.float32)
+
+
+def build_dataset(ctx, scorer, meshes, halves=True, plane_set=None, **eval_kw):
+    """Exact (feature, score) pairs on each mesh's candidate planes
+    (`candidate_set(**plane_set)`) and, when `halves`, on the two parts its
+    best plane leaves (the next level's parts).  Returns X [n, 240], T [n],
+    and the part index of each row."""
+    Xs, Ts, G = [], [], []
+    g = 0
+    plane_set = plane_set or {}
+
+    def add(v, t):
+        nonlocal g
+        planes = candidate_set(ctx, v, t, **plane_set)
+        if len(planes) < 2:
+            return None
+        X, T, ok, res = exact_pairs(ctx, scorer, v, t, planes, **eval_kw)
+        if not ok.any():
+            return None
+        Xs.append(X)
+        Ts.append(T)
+        G.append(np.full(len(T), g, np.int32))
+        g += 1
+        return planes[int(np.argmin(np.where(ok, T, np.inf)))]
+
+    for v, t in meshes:
+        best = add(v, t)
+        if halves and best is not None:
+            pv, pt, nv_, nt_ = ctx.plane_cut(v, t, best)[:4]
+            for hv_, ht_ in ((pv, pt), (nv_, nt_)):
+                if len(ht_) >= 8:
+                    add(hv_, ht_)
+    return np.concatenate(Xs), np.concatenate(Ts), np.concatenate(G)
+
+
+def ranking_quality(pred, T, groups, k=8):
+    """Per part: does the model's top-k contain the exact best plane, and the
+    regret (best exact score within the top-k minus the best overall).
+    Returns (hit rate, mean regret, mean regret of a random top-k)."""
+    rng = np.random.default_rng(0)
+    hits, reg, rreg = [], [], []
+    for g in np.unique(groups):
+        m = groups == g
+        p, t = pred[m], T[m]
+        kk = min(k, len(t))
+        top = np.argsort(p, kind="stable")[:kk]
+        best = t.min()
+        hits.append(np.argmin(t) in top or t[top].min() == best)
+        reg.append(t[top].min() - best)
+        rreg.append(np.mean([t[rng.choice(len(t), kk, replace=False)].min() - best for _ in range(16)]))
+    return float(np.mean(hits)), float(np.mean(reg)), float(np.mean(rreg))

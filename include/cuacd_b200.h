@@ -247,6 +247,57 @@ unsigned long long cuacd_launch_count(gpu_ctx_t ctx);
 int cuacd_profile_stages(gpu_ctx_t ctx, int enable);
 int cuacd_stage_times(gpu_ctx_t ctx, float* ms_out);
 
+/* ---- learned candidate scorer (no counterpart in the reference) ---------- */
+
+/* A 240-256-256-1 MLP (BF16 operands, FP32 accumulation, ReLU) that
+ * predicts a candidate plane's score_full from cuacd_candidate_features.
+ * Parameters are FP32 master copies, flattened as W1[240][256], b1[256],
+ * W2[256][256], b2[256], W3[256], b3[1] (row k of W holds input k's
+ * weights).  The loss is the mean squared error of (prediction - target)
+ * scaled by 10. */
+typedef struct cuacd_scorer* cuacd_scorer_t;
+int  cuacd_scorer_n_params(void);
+int  cuacd_scorer_n_features(void);
+int  cuacd_scorer_create(gpu_ctx_t ctx, unsigned seed, cuacd_scorer_t* out);
+void cuacd_scorer_free(cuacd_scorer_t s);
+/* set_params also resets the optimizer state. */
+int  cuacd_scorer_set_params(cuacd_scorer_t s, const float* params);
+int  cuacd_scorer_get_params(cuacd_scorer_t s, float* params);
+/* Feature standardisation applied before the first layer, x' = (x - mean) *
+ * inv_std (n_features floats each; identity after create). */
+int  cuacd_scorer_set_normalizer(cuacd_scorer_t s, const float* mean, const float* inv_std);
+int  cuacd_scorer_get_normalizer(cuacd_scorer_t s, float* mean, float* inv_std);
+
+/* Feature rows (n_features floats each) of n planes on one part; hull_vol is
+ * the part's convex-hull volume. */
+int cuacd_candidate_features(gpu_ctx_t ctx, cuacd_scorer_t s, const float* verts, int nv,
+                             const int* tris, int nt, float hull_vol,
+                             const float* planes, int n, float* out);
+
+/* Loss and parameter gradients (n_params floats) of one batch of n rows. */
+int cuacd_scorer_grad(gpu_ctx_t ctx, cuacd_scorer_t s, const float* X, const float* T,
+                      int n, float* loss, float* grads);
+
+/* AdamW (beta 0.9/0.999, eps 1e-8, decoupled weight decay wd on weights)
+ * over `epochs` shuffled passes of n rows in batches of `batch`; rows stay
+ * on the device.  *final_loss: mean unscaled MSE over the last epoch. */
+int cuacd_scorer_train(gpu_ctx_t ctx, cuacd_scorer_t s, const float* X, const float* T,
+                       int n, int epochs, int batch, float lr, float wd,
+                       unsigned seed, float* final_loss);
+
+int cuacd_scorer_predict(gpu_ctx_t ctx, cuacd_scorer_t s, const float* X, int n, float* out);
+
+/* Surrogate-pruned evaluation: predicted scores for all planes, the exact
+ * evaluator (cuacd_eval_candidates) for the top_k best predictions plus every
+ * plane predicted within `margin` of the k-th.  Unevaluated planes get
+ * ok = 0 and scores FLT_MAX.  hull_vol < 0 computes the part's hull volume. */
+int cuacd_eval_candidates_pruned(gpu_ctx_t ctx, cuacd_scorer_t s, const float* verts, int nv,
+                                 const int* tris, int nt, float hull_vol,
+                                 const float* planes, int n_planes, int flags,
+                                 float hd_resolution, int hd_min_samples, int hd_total,
+                                 int top_k, float margin, cuacd_cand_result* out,
+                                 float* out_pred, int* out_evaluated, int* out_n_evaluated);
+
 /* ---- lookahead search (reference csrc/lookahead.h, csrc/heap.h) ---------- */
 
 struct gpu_part_result {
