@@ -1,21 +1,27 @@
-"""Benchmark: exact candidate evaluation (cut + hull + volume + Hausdorff).
+"""Benchmark: candidate scoring, surrogate-pruned vs exact.
 
 Workload (one step): the 40,960-triangle radially displaced sphere normalised
 to extent 2, scored on 30 candidate planes — 27 concave-edge planes (16
 concave edges, dihedral > 3.49 rad, cuda/la_concave.cu rule) + 3 axis
-midpoints — with the exact evaluator: cut with caps, both fragments' volume
-and exact hull, sampled Hausdorff fragment<->hull (2000 samples per unit
-area), part costs.  Metric: candidates scored per second.
+midpoints.  The exact evaluator cuts with caps, computes both fragments'
+volume and exact hull, the sampled Hausdorff distance fragment<->hull (2000
+samples per unit area) and the part costs.  The surrogate-pruned step ranks
+all 30 planes with the learned scorer (GPU feature rows + BF16 tensor-core
+MLP) and sends the top 8, plus every plane predicted within 0.005 of the
+8th, through the exact evaluator.  Metric: candidates scored per second.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
-value    device-resident throughput (mesh and planes already in HBM), CUDA
-         events on the evaluator's stream, L2 flushed (256 MiB write)
-         before every timed step; max over ranks for N > 1.
+value    surrogate-pruned throughput, device-resident (mesh and planes
+         already in HBM), CUDA events on the evaluator's stream, L2 flushed
+         (256 MiB write) before every timed step; max over ranks for N > 1.
+         "exact" holds the same numbers for the exact evaluator on all 30
+         planes; "pruning" the planes evaluated exactly and whether the
+         pruned step found the exact step's best plane.
 e2e      the same metric through the public C-ABI entry point with pinned
          host buffers (H2D of mesh+planes and D2H of the results per step).
 roofline dominant kernel's algorithmic bytes / its CUDA-event duration.
---impl reference: the CPU oracle port of the same path on all host cores
+--impl reference: the CPU oracle port of the exact path on all host cores
          (the reference has no CPU implementation of this path; its CPU
          baselines need sources absent from the reference tree).
 N > 1 runs independent replicas (the path does not shard across GPUs).
@@ -34,9 +40,10 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-METRIC = "candidates scored/s (exact: cut+hull+Hausdorff), config 3"
+METRIC = "candidates scored/s at tau=0.05 on 1 B200: surrogate-pruned vs exact (config 3)"
 UNIT = "candidates/s"
 N_EDGE, WIDTH = 27, 3
+TOP_K, MARGIN = 8, 0.005
 
 
 def peaks():
@@ -48,15 +55,16 @@ def peaks():
         return 6650.0, "fallback"
 
 
-def ncu_traffic(kernel):
-    """DRAM bytes per launch of `kernel` from the committed ncu summary
-    (profiles/roofline_traffic.txt), or None."""
+def ncu_traffic(kernel, planes):
+    """DRAM bytes per launch of `kernel` on a step of `planes` candidate
+    planes, from the committed ncu summary (profiles/roofline_traffic.txt:
+    lines "kernel planes bytes"), or None."""
     try:
         with open(os.path.join(ROOT, "profiles", "roofline_traffic.txt")) as f:
             for line in f:
                 parts = line.split()
-                if len(parts) >= 2 and parts[0] == kernel:
-                    return int(parts[1])
+                if len(parts) >= 3 and parts[0] == kernel and parts[1] == str(planes):
+                    return int(parts[2])
     except OSError:
         pass
     return None
@@ -78,7 +86,8 @@ def planes_for(ctx, v, t):
 
 def config(n_planes, v, t):
     return {"workload": "config3: 40,960-tri displaced UV sphere (extent 2, seed 2), "
-                        "30 planes (27 concave-edge + 3 axis midpoints), exact evaluator",
+                        "30 planes (27 concave-edge + 3 axis midpoints); learned scorer ranks all 30, "
+                        "exact evaluator on the top 8 (+ margin 0.005)",
             "mesh_tris": int(len(t)), "mesh_verts": int(len(v)), "planes_per_step": int(n_planes),
             "hausdorff_samples": "2000 per unit area, min 1000", "l2": "flushed between timed steps (256 MiB write)",
             "parallelism": "replicas"}
@@ -178,6 +187,34 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def _timed(step, stream, flush, steps, clocks=None):
+    """CUDA-event time (ms) of each of `steps` calls of step() on `stream`,
+    L2 flushed (untimed) before each."""
+    import torch
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    for i in range(steps):
+        flush.zero_()
+        ev[i][0].record(stream)
+        step()
+        ev[i][1].record(stream)
+    stream.synchronize()
+    return [a.elapsed_time(b) for a, b in ev]
+
+
+def _stage_ms(lib, ctx, step, flush):
+    """Per-stage times of the exact evaluator (median of 3 profiled steps)."""
+    lib.cuacd_profile_stages(ctx.handle, 1)
+    out = []
+    for _ in range(3):
+        flush.zero_()
+        step()
+        arr = (ctypes.c_float * 6)()
+        lib.cuacd_stage_times(ctx.handle, ctypes.cast(arr, ctypes.c_void_p))
+        out.append(list(arr))
+    lib.cuacd_profile_stages(ctx.handle, 0)
+    return np.median(np.array(out), axis=0).tolist()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -209,15 +246,18 @@ def main():
 
     import torch
     import cuacd_b200
+    from cuacd_b200 import scorer as S
     lib = cuacd_b200._lib
     lib.cuacd_profile_stages.argtypes = [ctypes.c_void_p, ctypes.c_int]
     lib.cuacd_stage_times.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
     dev = local
     torch.cuda.set_device(dev)
     ctx = cuacd_b200.Context(dev)
+    sc = S.Scorer.load(ctx)
     v, t = workload()
     planes = planes_for(ctx, v, t)
     n = len(planes)
+    hull_vol = S.part_hull_volume(ctx, v)     # every part of the search carries its hull
 
     # device-resident inputs
     dv = torch.from_numpy(v.reshape(-1)).cuda()
@@ -225,9 +265,14 @@ def main():
     dp = torch.from_numpy(planes.reshape(-1)).cuda()
     res_bytes = ctypes.sizeof(cuacd_b200.CandResult) * n
     dres = torch.empty(res_bytes, dtype=torch.uint8, device="cuda")
+    dres_p = torch.empty(res_bytes, dtype=torch.uint8, device="cuda")
+    dpred = torch.empty(n, dtype=torch.float32, device="cuda")
+    deval = torch.empty(n, dtype=torch.int32, device="cuda")
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     stream = torch.cuda.Stream(device=dev)
     fn_dev = cuacd_b200._fn("cuacd_eval_candidates_device")
+    fn_pdev = cuacd_b200._fn("cuacd_eval_candidates_pruned_device")
+    n_eval = ctypes.c_int(0)
 
     def step():
         rc = fn_dev(ctx.handle, ctypes.c_void_p(dv.data_ptr()), len(v), ctypes.c_void_p(dt.data_ptr()), len(t),
@@ -236,54 +281,65 @@ def main():
         if rc:
             raise RuntimeError(f"cuacd error {rc}: {lib.gpu_last_error(ctx.handle)}")
 
+    def step_pruned():
+        rc = fn_pdev(ctx.handle, sc._h, ctypes.c_void_p(dv.data_ptr()), len(v), ctypes.c_void_p(dt.data_ptr()),
+                     len(t), float(hull_vol), ctypes.c_void_p(dp.data_ptr()), n, 1, 2000.0, 1000, 0, TOP_K,
+                     float(MARGIN), ctypes.c_void_p(dres_p.data_ptr()), ctypes.c_void_p(dpred.data_ptr()),
+                     ctypes.c_void_p(deval.data_ptr()), ctypes.byref(n_eval), ctypes.c_void_p(stream.cuda_stream))
+        if rc:
+            raise RuntimeError(f"cuacd error {rc}: {lib.gpu_last_error(ctx.handle)}")
+
+    def results(buf):
+        host = (cuacd_b200.CandResult * n)()
+        hbuf = buf.cpu().numpy()                  # keep the host copy alive for the memmove
+        ctypes.memmove(host, hbuf.ctypes.data, res_bytes)
+        return host
+
     with torch.cuda.stream(stream):
         for _ in range(args.warmup):
             step()
+            step_pruned()
         stream.synchronize()
-        # correctness guard on the resident path
-        host = (cuacd_b200.CandResult * n)()
-        hbuf = dres.cpu().numpy()                 # keep the host copy alive for the memmove
-        ctypes.memmove(host, hbuf.ctypes.data, res_bytes)
-        n_ok = sum(r.ok for r in host)
-        if any(r.err for r in host):
+        # correctness guards on the resident paths
+        exact = results(dres)
+        pruned = results(dres_p)
+        if any(r.err for r in exact) or any(r.err for r in pruned):
             raise RuntimeError("device evaluation reported errors")
+        ev_mask = deval.cpu().numpy().astype(bool)
+        for i in np.nonzero(ev_mask)[0]:
+            if bytes(pruned[i]) != bytes(exact[i]):
+                raise RuntimeError(f"pruned result {i} differs from the exact evaluator")
+        n_ok = sum(r.ok for r in exact)
+        sx = np.array([r.score_full if r.ok else np.inf for r in exact])
+        sp = np.array([r.score_full if (r.ok and m) else np.inf for r, m in zip(pruned, ev_mask)])
+        quality = {"top_k": TOP_K, "margin": MARGIN, "planes_exact_per_step": int(ev_mask.sum()),
+                   "best_exact_score": float(sx.min()), "best_pruned_score": float(sp.min()),
+                   "same_best_plane": bool(np.argmin(sp) == np.argmin(sx))}
 
         if dist:
             dist.barrier()
         torch.cuda.synchronize()
-        launches0 = ctx.launch_count()
-        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        l0 = ctx.launch_count()
+        ms_exact = _timed(step, stream, flush, args.steps)
+        l1 = ctx.launch_count()
         with Clocks(dev) as clk:
-            for i in range(args.steps):
-                flush.zero_()                       # evict L2 (untimed)
-                ev[i][0].record(stream)
-                step()
-                ev[i][1].record(stream)
-            stream.synchronize()
-        launches = ctx.launch_count() - launches0
+            ms_pruned = _timed(step_pruned, stream, flush, args.steps)
+        l2 = ctx.launch_count()
         torch.cuda.synchronize()
         if dist:
             dist.barrier()
-        ms = [a.elapsed_time(b) for a, b in ev]
-        tot_ms = sum(ms)
-        # per-stage times (one profiled step, same stream, after the timed loop)
-        lib.cuacd_profile_stages(ctx.handle, 1)
-        stage_ms = []
-        for _ in range(3):
-            flush.zero_()
-            step()
-            arr = (ctypes.c_float * 6)()
-            lib.cuacd_stage_times(ctx.handle, ctypes.cast(arr, ctypes.c_void_p))
-            stage_ms.append(list(arr))
-        lib.cuacd_profile_stages(ctx.handle, 0)
-        stage_ms = np.median(np.array(stage_ms), axis=0).tolist()
+        stage_exact = _stage_ms(lib, ctx, step, flush)
+        stage_pruned = _stage_ms(lib, ctx, step_pruned, flush)
 
-    # e2e through the public host-pointer entry point with pinned buffers
+    # e2e through the public host-pointer entry points with pinned buffers
     pv = torch.from_numpy(v.reshape(-1)).pin_memory()
     pt = torch.from_numpy(t.reshape(-1).astype(np.int32)).pin_memory()
     pp = torch.from_numpy(planes.reshape(-1)).pin_memory()
     pres = torch.empty(res_bytes, dtype=torch.uint8).pin_memory()
+    ppred = torch.empty(n, dtype=torch.float32).pin_memory()
+    peval = torch.empty(n, dtype=torch.int32).pin_memory()
     fn_host = cuacd_b200._fn("cuacd_eval_candidates")
+    fn_phost = cuacd_b200._fn("cuacd_eval_candidates_pruned")
 
     def host_step():
         rc = fn_host(ctx.handle, ctypes.c_void_p(pv.data_ptr()), len(v), ctypes.c_void_p(pt.data_ptr()), len(t),
@@ -291,59 +347,82 @@ def main():
         if rc:
             raise RuntimeError(f"cuacd error {rc}")
 
-    for _ in range(args.warmup):
-        host_step()
-    e2e_times = []
-    for _ in range(args.steps):
-        flush.zero_(); torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        host_step()
-        e2e_times.append(time.perf_counter() - t0)
-    e2e_s = sum(e2e_times)
+    def host_step_pruned():
+        rc = fn_phost(ctx.handle, sc._h, ctypes.c_void_p(pv.data_ptr()), len(v), ctypes.c_void_p(pt.data_ptr()),
+                      len(t), float(hull_vol), ctypes.c_void_p(pp.data_ptr()), n, 1, 2000.0, 1000, 0, TOP_K,
+                      float(MARGIN), ctypes.c_void_p(pres.data_ptr()), ctypes.c_void_p(ppred.data_ptr()),
+                      ctypes.c_void_p(peval.data_ptr()), ctypes.byref(n_eval))
+        if rc:
+            raise RuntimeError(f"cuacd error {rc}")
 
-    # max over ranks
+    def wall(fn):
+        for _ in range(args.warmup):
+            fn()
+        tt = []
+        for _ in range(args.steps):
+            flush.zero_(); torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            fn()
+            tt.append(time.perf_counter() - t0)
+        return sum(tt)
+
+    e2e_exact_s = wall(host_step)
+    e2e_s = wall(host_step_pruned)
+
+    tot_ms, tot_exact_ms = sum(ms_pruned), sum(ms_exact)
     if dist:
-        tt = torch.tensor([tot_ms, e2e_s], device="cuda", dtype=torch.float64)
+        tt = torch.tensor([tot_ms, tot_exact_ms, e2e_s, e2e_exact_s], device="cuda", dtype=torch.float64)
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        tot_ms, e2e_s = float(tt[0]), float(tt[1])
+        tot_ms, tot_exact_ms, e2e_s, e2e_exact_s = [float(x) for x in tt]
     world_n = world
     value = world_n * n * args.steps / (tot_ms / 1000.0)
     e2e_val = world_n * n * args.steps / e2e_s
 
-    # roofline of the dominant stage
+    # roofline of the dominant stage of the pruned step's exact evaluation
     names = ["k_cut_planes", "hull_pipeline", "k_hd_prep", "k_hd_plan", "k_hd_query", "k_eval_finish"]
-    dom = int(np.argmax(stage_ms))
-    V, T = len(v), len(t)
-    Vf = sum(r.nv[0] + r.nv[1] for r in host); Tf = sum(r.nt[0] + r.nt[1] for r in host)
-    Hv = sum(r.hull_nv[0] + r.hull_nv[1] for r in host); Ht = sum(r.hull_nt[0] + r.hull_nt[1] for r in host)
-    alg = {
-        "k_cut_planes": 12 * (V + T) * n + 12 * (Vf + Tf),
-        "hull_pipeline": 12 * (Vf + Tf) + 12 * (Hv + Ht),
-        "k_hd_prep": 12 * (Vf + Tf) + 12 * (Hv + Ht),
-        "k_hd_plan": 0,
-        "k_hd_query": 12 * (Vf + Tf) + 12 * (Hv + Ht),
-        "k_eval_finish": 0,
-    }
-    peak, peak_kind = peaks()
-    achieved = alg[names[dom]] / (stage_ms[dom] / 1000.0) / 1e9
-    roof = {"bound": "hbm", "kernel": names[dom], "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "peak_source": peak_kind, "traffic": ncu_traffic(names[dom]),
-            "algorithmic_bytes": int(alg[names[dom]]),
-            "stage_ms": {k: round(x, 4) for k, x in zip(names, stage_ms)}}
+
+    def roofline(stage_ms, res, mask):
+        dom = int(np.argmax(stage_ms))
+        V, T = len(v), len(t)
+        sel = [r for r, m in zip(res, mask) if m]
+        k = len(sel)
+        Vf = sum(r.nv[0] + r.nv[1] for r in sel); Tf = sum(r.nt[0] + r.nt[1] for r in sel)
+        Hv = sum(r.hull_nv[0] + r.hull_nv[1] for r in sel); Ht = sum(r.hull_nt[0] + r.hull_nt[1] for r in sel)
+        alg = {
+            "k_cut_planes": 12 * (V + T) * k + 12 * (Vf + Tf),
+            "hull_pipeline": 12 * (Vf + Tf) + 12 * (Hv + Ht),
+            "k_hd_prep": 12 * (Vf + Tf) + 12 * (Hv + Ht),
+            "k_hd_plan": 0,
+            "k_hd_query": 12 * (Vf + Tf) + 12 * (Hv + Ht),
+            "k_eval_finish": 0,
+        }
+        peak, peak_kind = peaks()
+        achieved = alg[names[dom]] / (stage_ms[dom] / 1000.0) / 1e9
+        return {"bound": "hbm", "kernel": names[dom], "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": peak_kind,
+                "traffic": ncu_traffic(names[dom], k),
+                "algorithmic_bytes": int(alg[names[dom]]), "planes": k,
+                "stage_ms": {kk: round(x, 4) for kk, x in zip(names, stage_ms)}}
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world_n, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": tot_ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32 (exact int/f64 predicates)",
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 (exact int/f64 predicates); bf16 network",
             "data": "synthetic", "config": config(n, v, t),
-            "candidates_ok": int(n_ok), "gpu_launches": int(launches), "clocks": clk.summary(),
-            "roofline": roof,
+            "candidates_ok": int(n_ok), "gpu_launches": int(l2 - l1), "clocks": clk.summary(),
+            "pruning": quality,
+            "roofline": roofline(stage_pruned, pruned, ev_mask),
             "e2e": {"value": e2e_val, "unit": UNIT,
                     "h2d_bytes_per_step": int(v.nbytes + t.astype(np.int32).nbytes + planes.nbytes),
-                    "d2h_bytes_per_step": int(res_bytes)}}
+                    "d2h_bytes_per_step": int(res_bytes + 8 * n)},
+            "exact": {"value": world_n * n * args.steps / (tot_exact_ms / 1000.0),
+                      "ms_per_step": tot_exact_ms / args.steps, "gpu_launches": int(l1 - l0),
+                      "e2e": world_n * n * args.steps / e2e_exact_s,
+                      "roofline": roofline(stage_exact, exact, np.ones(n, bool))}}
     if rank == 0 and world_n == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(v, t, planes)
     if rank == 0:
         print(json.dumps(line), flush=True)
+    del sc
     ctx.close()
     if dist:
         dist.barrier()

@@ -95,6 +95,9 @@ _opt("lookahead_decompose", _I, [_P, _P, _I, _P, _I, _P, _I, _P, _I,
                                  _I, _I, _I, _F, _I, _I, _I, _I, _I, _I, _I,
                                  _I, _F, _F, _I, _I, ctypes.POINTER(GpuResult)])
 _opt("gpu_result_free", None, [ctypes.POINTER(GpuResult)])
+_opt("cuacd_lookahead_decompose_pruned", _I, [_P, _P, _I, _F, _I, _P, _P, _I, _P, _I, _P, _I, _P, _I,
+                                              _I, _I, _I, _F, _I, _I, _I, _I, _I, _I, _F, _F, _I,
+                                              ctypes.POINTER(GpuResult)])
 _opt("cuacd_candidate_planes", _I, [_P, _P, _I, _P, _I, _I, _F, _F, _I, _F, _P, _P, _P])
 _opt("cuacd_profile_stages", _I, [_P, _I])
 _opt("cuacd_stage_times", _I, [_P, _P])
@@ -110,6 +113,8 @@ _opt("cuacd_candidate_features", _I, [_P, _P, _P, _I, _P, _I, _F, _P, _I, _P])
 _opt("cuacd_scorer_grad", _I, [_P, _P, _P, _P, _I, _P, _P])
 _opt("cuacd_scorer_train", _I, [_P, _P, _P, _P, _I, _I, _I, _F, _F, ctypes.c_uint, _P])
 _opt("cuacd_scorer_predict", _I, [_P, _P, _P, _I, _P])
+_opt("cuacd_eval_candidates_pruned_device", _I, [_P, _P, _P, _I, _P, _I, _F, _P, _I, _I, _F, _I, _I, _I, _F,
+                                                 _P, _P, _P, _P, _P])
 _opt("cuacd_eval_candidates_pruned", _I, [_P, _P, _P, _I, _P, _I, _F, _P, _I, _I, _F, _I, _I, _I, _F,
                                           _P, _P, _P, _P])
 
@@ -363,9 +368,16 @@ class Context:
                             depth=2, quick_depth=0, max_n_cutting=16, verbose=0, debug=0,
                             decompose_components=False, no_decompose_components_per_iter=False,
                             n_concave_edges=32, concave_eps=0.005, concave_threshold=3.49,
-                            concave_iters=10, merge_hulls=False):
+                            concave_iters=10, merge_hulls=False, scorer=None, top_k=8, margin=0.0, beam=0):
         """Convex decomposition by lookahead tree search ->
-        [(verts, tris, hull_verts, hull_tris)] (cuacd/__init__.py:367-454)."""
+        [(verts, tris, hull_verts, hull_tris)] (cuacd/__init__.py:367-454).
+
+        With `scorer` (a cuacd_b200.scorer.Scorer), level 0 cuts only the
+        top_k planes of each cutting part by predicted score (plus those
+        within `margin` of the k-th); with `beam` > 0 only the `beam` level-0
+        cuts of each part with the lowest exact cost are expanded further.
+        `self.last_prune_stats` then holds (level-0 planes ranked, planes
+        cut, level-0 cuts expanded)."""
         verts = _as_f32(verts).reshape(-1, 3)
         tris = _as_i32(tris).reshape(-1, 3)
         if width2 is None:
@@ -376,12 +388,25 @@ class Context:
         hull = self.batch_hull_dandc_mesh([verts])[0]
         hv, ht = _as_f32(hull[0]), _as_i32(hull[1])
         res = GpuResult()
-        fn = _fn("lookahead_decompose")
-        self._check(fn(self._h, _ptr(verts), len(verts), _ptr(tris), len(tris), _ptr(hv), len(hv), _ptr(ht), len(ht),
-                       int(max_iters), int(width), int(width2), float(threshold), int(depth), int(quick_depth),
-                       int(max_n_cutting), int(verbose), int(debug), int(bool(decompose_components)),
-                       int(not no_decompose_components_per_iter), int(n_concave_edges), float(concave_eps),
-                       float(concave_threshold), int(concave_iters), int(bool(merge_hulls)), ctypes.byref(res)))
+        if scorer is None and not beam:
+            fn = _fn("lookahead_decompose")
+            self._check(fn(self._h, _ptr(verts), len(verts), _ptr(tris), len(tris), _ptr(hv), len(hv), _ptr(ht),
+                           len(ht), int(max_iters), int(width), int(width2), float(threshold), int(depth),
+                           int(quick_depth), int(max_n_cutting), int(verbose), int(debug),
+                           int(bool(decompose_components)), int(not no_decompose_components_per_iter),
+                           int(n_concave_edges), float(concave_eps), float(concave_threshold), int(concave_iters),
+                           int(bool(merge_hulls)), ctypes.byref(res)))
+        else:
+            st = (ctypes.c_ulonglong * 3)()
+            fn = _fn("cuacd_lookahead_decompose_pruned")
+            self._check(fn(self._h, scorer._h if scorer is not None else None, int(top_k), float(margin), int(beam),
+                           ctypes.cast(st, ctypes.c_void_p),
+                           _ptr(verts), len(verts), _ptr(tris), len(tris), _ptr(hv), len(hv), _ptr(ht), len(ht),
+                           int(max_iters), int(width), int(width2), float(threshold), int(depth),
+                           int(max_n_cutting), int(verbose), int(bool(decompose_components)),
+                           int(not no_decompose_components_per_iter), int(n_concave_edges), float(concave_eps),
+                           float(concave_threshold), int(concave_iters), ctypes.byref(res)))
+            self.last_prune_stats = (int(st[0]), int(st[1]), int(st[2]))
         out = []
         try:
             for i in range(res.nparts):

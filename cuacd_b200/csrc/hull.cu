@@ -20,7 +20,7 @@ k_hull_setup(const HullJob* __restrict__ jobs, int n_jobs, Arena* scratch, HullS
     if (J.tris && J.nt > 0 && J.n > 0) mv = block_mesh_signed_volume(J.pts, J.n, J.tris, J.nt, sh.dsh);
     if (threadIdx.x == 0) {
         S->n = J.n; S->n_faces = 0; S->err = 0; S->active = 0; S->q_pending = 0;
-        for (int k = 0; k < 8; k++) S->stats[k] = 0;
+        for (int k = 0; k < 8; k++) { S->stats[k] = 0; S->fail[k] = 0; }
         s_err = 0; s_scr = nullptr;
         if (J.n >= 4) {
             s_scr = (char*)arena_alloc(scratch, hull_scratch_bytes(J.n), &s_err);
@@ -151,8 +151,14 @@ k_hull_output(const HullJob* __restrict__ jobs, HullState* states, int n_jobs, A
         r.err = s_oerr | S->err;
         res[j] = r;
     }
-    if (stats && threadIdx.x < 8)
-        stats[8 * (size_t)j + threadIdx.x] = threadIdx.x == 2 ? (unsigned long long)S->n_faces : S->stats[threadIdx.x];
+    if (stats && threadIdx.x < 8) {
+        unsigned long long x = threadIdx.x == 2 ? (unsigned long long)S->n_faces : S->stats[threadIdx.x];
+        if (S->fail[0] && threadIdx.x >= 4) {       // failed hull: slots 4-7 hold the failure record
+            const int k = 2 * ((int)threadIdx.x - 4);
+            x = (unsigned long long)(unsigned)S->fail[k] | ((unsigned long long)(unsigned)S->fail[k + 1] << 32);
+        }
+        stats[8 * (size_t)j + threadIdx.x] = x;
+    }
 }
 
 size_t hull_wrap_buf_bytes(int n_wrap_ctas)

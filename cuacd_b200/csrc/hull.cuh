@@ -81,14 +81,18 @@ struct HullCtx {
 
 // Bounds of N.(x - a) over a leaf's points from its oriented box:
 // N.(c - a) -+ (sum_i h_i |N.e_i| + margin).  The margin covers the float
-// rounding of the stored centre and axes (|N|_1 * 1e-5 * (sum h + 1)).
+// rounding of the stored axes (|N|_1 * 1e-5 * (sum h + 1)).  c - a is formed
+// in FP64, where it is exact: the centre is not on the grid, and a float
+// difference would be off by up to half an ulp of |c - a| (5e-4 grid units),
+// more than the margin of a flat leaf lying in the plane -- its points would
+// then be cut from the face.
 static __device__ __forceinline__ bool leaf_obb(const HullCtx& H, int leaf, double nx, double ny, double nz,
                                                 float4 a, double* lo, double* hi)
 {
     float4 c = H.obb[4 * leaf];
     if (c.w == 0.f) return false;
     float4 e1 = H.obb[4 * leaf + 1], e2 = H.obb[4 * leaf + 2], e3 = H.obb[4 * leaf + 3];
-    double mid = nx * (double)(c.x - a.x) + ny * (double)(c.y - a.y) + nz * (double)(c.z - a.z);
+    double mid = nx * ((double)c.x - (double)a.x) + ny * ((double)c.y - (double)a.y) + nz * ((double)c.z - (double)a.z);
     double r = fabs(nx * e1.x + ny * e1.y + nz * e1.z) * e1.w + fabs(nx * e2.x + ny * e2.y + nz * e2.z) * e2.w
              + fabs(nx * e3.x + ny * e3.y + nz * e3.z) * e3.w;
     r += (fabs(nx) + fabs(ny) + fabs(nz)) * 1e-5 * ((double)e1.w + e2.w + e3.w + 1.0);
@@ -571,6 +575,7 @@ struct HullState {             // per hull, global memory
     int lock;                  // guards Sbuf/posn/ocnt while wrapping (large faces)
     long long wbase;           // wrap-grid share: prefix of the active hulls' point counts
     double mesh_vol;
+    int fail[8];               // first construction failure: site, u, v, c, ns, k, input index of u, of v
     unsigned long long stats[8];   // leaves kept by wraps, wraps, faces, points
                                    // tested by wraps, set-up cycles, device
                                    // time (ns) of the first edge taken and of
@@ -973,7 +978,13 @@ static __device__ void hull_setup_cta(const float* __restrict__ pts, int n, char
                     if (f < C.fcap) { faces[f] = make_int2(s_cstart, k); sh.n_corners = s_cstart + k; }
                     else sh.err |= KERR_BT_POOL_EXHAUST;
                 } else if (ins < 0) sh.err |= KERR_BT_POOL_EXHAUST;
-            } else if (!s_face_ok || s_cur >= 0) sh.err |= KERR_BT_EXTRACT_FAIL;
+            } else if (!s_face_ok || s_cur >= 0) {
+                sh.err |= KERR_BT_EXTRACT_FAIL;
+                if (S->fail[0] == 0) {
+                    S->fail[0] = 2; S->fail[1] = u; S->fail[2] = v; S->fail[3] = s_cur; S->fail[4] = ns;
+                    S->fail[5] = k; S->fail[6] = s_face_ok; S->fail[7] = anchor;
+                }
+            }
         }
         __syncthreads();
     };
@@ -1176,8 +1187,13 @@ static __device__ void hull_wrap_edge(HullState* S, int u, int v, HullWarp& W, c
     // the next one), then the lanes insert its edges and queue the new ones
     int fs = -1;
     if (lane == 0) {
-        if (c < 0 || k < 3) atomicOr(&S->err, KERR_BT_EXTRACT_FAIL);
-        else {
+        if (c < 0 || k < 3) {
+            atomicOr(&S->err, KERR_BT_EXTRACT_FAIL);
+            if (atomicCAS(&S->fail[0], 0, 1) == 0) {
+                S->fail[1] = u; S->fail[2] = v; S->fail[3] = c; S->fail[4] = ns; S->fail[5] = k;
+                S->fail[6] = pidx(P4[u]); S->fail[7] = pidx(P4[v]);
+            }
+        } else {
             int mi = 0;
             for (int i = 1; i < k; i++) if (pidx(P4[poly[i]]) < pidx(P4[poly[mi]])) mi = i;
             int ins = hset_insert(S->fset, S->fh, ekey(poly[mi], poly[(mi + 1) % k]));

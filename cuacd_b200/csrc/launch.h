@@ -48,3 +48,11 @@ void launch_hull_jobs(const HullJob* d_jobs, int n_jobs, HullState* d_states, Hu
 void launch_jobs_from_offsets(const float* d_pts, const int* d_off, int n, float* d_v, int* d_t, int max_hv,
                               int max_ht, HullJob* d_jobs, cudaStream_t s);
 void launch_unpack_results(const HullRes* d_res, int n, int* d_nv, int* d_nt, float* d_vol, int* d_err, cudaStream_t s);
+
+// scorer.cu
+struct cuacd_scorer;
+struct ScorerPart { const float* v; const int* t; int nv, nt; float hull_vol; int off, n; };
+// Predicted scores (score units) of planes d_planes[p.off, p.off + p.n) of
+// each part p into pred[0, n_rows) (host); synchronises `s`.
+int scorer_predict_parts(gpu_ctx* ctx, cuacd_scorer* sc, const ScorerPart* parts, int n_parts,
+                         const float4* d_planes, int n_rows, float* pred, cudaStream_t s);

@@ -53,19 +53,15 @@ struct CutJob {
 
 typedef HullRes FragRes;            // per fragment: hull + volumes
 
-__global__ void __launch_bounds__(CUT_NT)
-k_cut_jobs(const CutJob* __restrict__ jobs, int j0, int j1, Arena* scratch, Arena* out, float min_edge_dist,
-           CutResult* res)
+// The plane of cut job J, computed by the whole CTA into *s_plane / *s_flags
+// (la_axis_cut_candidate + la_expand's bbox rules, cuda/la_axis_cut.cuh:10-19,
+// cuda/la_expand.cu:155-199): an axis job cuts its part's bbox at slice /
+// (cpa + 1) inside a min_edge_dist margin; a part too small on every axis is
+// flagged SMALL, an axis too narrow NOPLANE; an explicit zero plane is NOPLANE.
+static __device__ void cut_job_plane(const CutJob& J, float min_edge_dist, float (*red)[CUT_NT / 32], float* s_lo,
+                                     float* s_hi, float4* s_plane, int* s_flags)
 {
-    __shared__ CutShared sh;
-    __shared__ float s_lo[3], s_hi[3];
-    __shared__ float4 s_plane;
-    __shared__ int s_flags;
-    __shared__ float red[6][CUT_NT / 32];
-    const int j = j0 + blockIdx.x;
-    if (j >= j1) return;
-    const CutJob J = jobs[j];
-    if (threadIdx.x == 0) { s_flags = 0; s_plane = J.plane; }
+    if (threadIdx.x == 0) { *s_flags = 0; *s_plane = J.plane; }
     if (J.axis >= 0) {
         float l[3] = {1e30f, 1e30f, 1e30f}, h[3] = {-1e30f, -1e30f, -1e30f};
         for (int i = threadIdx.x; i < J.nv; i += CUT_NT)
@@ -83,21 +79,36 @@ k_cut_jobs(const CutJob* __restrict__ jobs, int j0, int j1, Arena* scratch, Aren
             bool all_small = (s_hi[0] - s_lo[0] <= 2.f * min_edge_dist + eps) &&
                              (s_hi[1] - s_lo[1] <= 2.f * min_edge_dist + eps) &&
                              (s_hi[2] - s_lo[2] <= 2.f * min_edge_dist + eps);
-            if (all_small) s_flags = CUT_FLAG_SMALL | CUT_FLAG_NOPLANE;
+            if (all_small) *s_flags = CUT_FLAG_SMALL | CUT_FLAG_NOPLANE;
             else {
                 float lv = s_lo[J.axis] + min_edge_dist, hv = s_hi[J.axis] - min_edge_dist;
-                if (lv >= hv) s_flags = CUT_FLAG_NOPLANE;
+                if (lv >= hv) *s_flags = CUT_FLAG_NOPLANE;
                 else {
                     float frac = ((float)J.slice + 1.0f) / ((float)J.cpa + 1.0f);
                     float cut = fmaf(frac, hv - lv, lv);
-                    s_plane = make_float4(J.axis == 0 ? 1.f : 0.f, J.axis == 1 ? 1.f : 0.f, J.axis == 2 ? 1.f : 0.f, -cut);
+                    *s_plane = make_float4(J.axis == 0 ? 1.f : 0.f, J.axis == 1 ? 1.f : 0.f, J.axis == 2 ? 1.f : 0.f, -cut);
                 }
             }
         }
     } else if (threadIdx.x == 0 && J.plane.x == 0.f && J.plane.y == 0.f && J.plane.z == 0.f) {
-        s_flags = CUT_FLAG_NOPLANE;
+        *s_flags = CUT_FLAG_NOPLANE;
     }
     __syncthreads();
+}
+
+__global__ void __launch_bounds__(CUT_NT)
+k_cut_jobs(const CutJob* __restrict__ jobs, int j0, int j1, Arena* scratch, Arena* out, float min_edge_dist,
+           CutResult* res)
+{
+    __shared__ CutShared sh;
+    __shared__ float s_lo[3], s_hi[3];
+    __shared__ float4 s_plane;
+    __shared__ int s_flags;
+    __shared__ float red[6][CUT_NT / 32];
+    const int j = j0 + blockIdx.x;
+    if (j >= j1) return;
+    const CutJob J = jobs[j];
+    cut_job_plane(J, min_edge_dist, red, s_lo, s_hi, &s_plane, &s_flags);
     if (s_flags & CUT_FLAG_NOPLANE) {
         if (threadIdx.x == 0) { CutResult r; memset(&r, 0, sizeof(r)); r.flags = s_flags; res[j] = r; }
         return;
@@ -106,6 +117,22 @@ k_cut_jobs(const CutJob* __restrict__ jobs, int j0, int j1, Arena* scratch, Aren
     memset(&none, 0, sizeof(none));
     float4 p = s_plane;
     cut_cta(J.v, J.nv, J.t, J.nt, p.x, p.y, p.z, p.w, scratch, none, &res[j], sh, out);
+}
+
+// The planes and flags of jobs [0, n) without cutting (what k_cut_jobs would
+// cut with), for the learned scorer's ranking of level-0 candidates.
+__global__ void __launch_bounds__(CUT_NT)
+k_job_planes(const CutJob* __restrict__ jobs, int n, float min_edge_dist, float4* planes, int* flags)
+{
+    __shared__ float s_lo[3], s_hi[3];
+    __shared__ float4 s_plane;
+    __shared__ int s_flags;
+    __shared__ float red[6][CUT_NT / 32];
+    const int j = blockIdx.x;
+    if (j >= n) return;
+    const CutJob J = jobs[j];
+    cut_job_plane(J, min_edge_dist, red, s_lo, s_hi, &s_plane, &s_flags);
+    if (threadIdx.x == 0) { planes[j] = s_plane; flags[j] = s_flags; }
 }
 
 // Hull jobs for fragments f0..f1 (2 per cut, empty when the cut produced
@@ -200,6 +227,9 @@ struct Lookahead {
     char* out_base; size_t out_cap;       // output arena memory
     char* scr_base; size_t scr_cap;       // scratch arena memory
     Arena* d_out; Arena* d_scr;           // device arena structs
+    char* tmp_base; size_t tmp_cap;       // arena for the last level's fragments (reset per wave)
+    Arena* d_tmp;
+    Arena* d_cur = nullptr;               // where run_level / run_hulls write: d_out or d_tmp
     float min_edge = 0.0125f;
     int debug = 0;                        // write the points of failed fragment hulls to files
     // buffers for the components pass
@@ -224,7 +254,7 @@ struct Lookahead {
                 acc += e; f1++;
             }
             reset_scr();
-            launch_hull_jobs(d_hjobs + f, f1 - f, d_hstates + f, res + f, d_scr, d_out, d_hctl, d_wbuf, nwc,
+            launch_hull_jobs(d_hjobs + f, f1 - f, d_hstates + f, res + f, d_scr, d_cur, d_hctl, d_wbuf, nwc,
                              nullptr, s);
             ctx->launches += 5;
             f = f1;
@@ -234,6 +264,35 @@ struct Lookahead {
     }
 
     void reset_out() { launch_arena_reset(d_out, out_base, out_cap, s); }
+    void reset_tmp() { launch_arena_reset(d_tmp, tmp_base, tmp_cap, s); }
+
+    // The last level's fragments are only needed for their costs: its jobs
+    // run in waves whose output fits the temporary arena, reset per wave.
+    int run_last_level(const std::vector<CutJob>& jobs, std::vector<CutResult>& cuts, std::vector<FragRes>& frags,
+                       CutJob* d_jobs, CutResult* d_cuts, FragRes* d_fr)
+    {
+        cuts.clear(); frags.clear();
+        std::vector<CutResult> c1; std::vector<FragRes> f1;
+        size_t j = 0;
+        while (j < jobs.size()) {
+            size_t acc = 0, j1 = j;
+            while (j1 < jobs.size()) {
+                size_t e = 64 * ((size_t)jobs[j1].nv + jobs[j1].nt) + (64 << 10);
+                if (j1 > j && acc + e > tmp_cap) break;
+                acc += e; j1++;
+            }
+            std::vector<CutJob> part(jobs.begin() + j, jobs.begin() + j1);
+            reset_tmp();
+            d_cur = d_tmp;
+            int rc = run_level(part, c1, f1, d_jobs, d_cuts, d_fr);
+            d_cur = d_out;
+            if (rc) return rc;
+            cuts.insert(cuts.end(), c1.begin(), c1.end());
+            frags.insert(frags.end(), f1.begin(), f1.end());
+            j = j1;
+        }
+        return 0;
+    }
     void reset_scr() { launch_arena_reset(d_scr, scr_base, scr_cap, s); }
 
     // Run cut jobs then hull jobs; returns 0 or an error (OOM -> KERR_HEAP_OOM).
@@ -255,7 +314,7 @@ struct Lookahead {
                 acc += e; j1++;
             }
             reset_scr();
-            k_cut_jobs<<<j1 - j, CUT_NT, 0, s>>>(d_jobs, j, j1, d_scr, d_out, min_edge, d_cuts);
+            k_cut_jobs<<<j1 - j, CUT_NT, 0, s>>>(d_jobs, j, j1, d_scr, d_cur, min_edge, d_cuts);
             ctx->launches += 2;
             j = j1;
         }
@@ -418,16 +477,83 @@ extern "C" void gpu_result_free(struct gpu_result* r)
     r->parts = nullptr; r->nparts = 0;
 }
 
-extern "C" int lookahead_decompose(gpu_ctx_t ctx, const float* verts, int nv, const int* tris, int nt,
-                                   const float* hull_verts, int hull_nv, const int* hull_tris, int hull_nt,
-                                   int max_iters, int width, int width2, float threshold,
-                                   int depth, int quick_depth, int max_n_cutting,
-                                   int verbose, int debug, int decompose_components,
-                                   int decompose_components_per_iter,
-                                   int n_concave_edges, float concave_eps, float concave_threshold,
-                                   int concave_iters, int merge_hulls, struct gpu_result* out)
+struct Prune;
+static int prune_level0(gpu_ctx* ctx, Lookahead& L, const Prune& P, const std::vector<Item>& cur,
+                        std::vector<CutJob>& jobs, std::vector<std::pair<int, int>>& job_of, CutJob* d_jobs,
+                        float4* d_planes, int* d_flags);
+
+// Optional pruning.  With a scorer, it ranks each cutting part's level-0
+// planes and only the top_k (plus those predicted within `margin` of the
+// k-th) are cut; planes the cut would skip (no plane, part too small) are
+// always kept.  With beam > 0, only the `beam` level-0 items of each part
+// with the lowest exact level-0 cost are expanded further.  stats[0] +=
+// level-0 candidates ranked, stats[1] += those cut, stats[2] += level-0
+// items expanded.
+struct Prune { cuacd_scorer* sc; int top_k; float margin; int beam; unsigned long long* stats; };
+
+static int prune_level0(gpu_ctx* ctx, Lookahead& L, const Prune& P, const std::vector<Item>& cur,
+                        std::vector<CutJob>& jobs, std::vector<std::pair<int, int>>& job_of, CutJob* d_jobs,
+                        float4* d_planes, int* d_flags)
 {
-    (void)quick_depth; (void)merge_hulls;
+    const int n = (int)jobs.size();
+    if (n == 0) return 0;
+    cudaStream_t s = L.s;
+    CK(cudaMemcpyAsync(d_jobs, jobs.data(), sizeof(CutJob) * n, cudaMemcpyHostToDevice, s));
+    k_job_planes<<<n, CUT_NT, 0, s>>>(d_jobs, n, L.min_edge, d_planes, d_flags);
+    ctx->launches++;
+    CK(cudaGetLastError());
+    std::vector<int> flags(n);
+    CK(cudaMemcpyAsync(flags.data(), d_flags, sizeof(int) * n, cudaMemcpyDeviceToHost, s));
+    // one scorer part per item: its jobs are consecutive
+    std::vector<ScorerPart> sp;
+    for (int j = 0; j < n;) {
+        const int ii = job_of[j].first;
+        int j1 = j;
+        while (j1 < n && job_of[j1].first == ii) j1++;
+        const LPart& w = cur[ii].parts.back();
+        sp.push_back({w.v, w.t, w.nv, w.nt, (float)w.hull_vol, j, j1 - j});
+        j = j1;
+    }
+    std::vector<float> pred(n);
+    int rc = scorer_predict_parts(ctx, P.sc, sp.data(), (int)sp.size(), d_planes, n, pred.data(), s);
+    if (rc) return rc;
+    std::vector<char> keep(n, 0);
+    for (const ScorerPart& p : sp) {
+        std::vector<int> valid;
+        for (int k = p.off; k < p.off + p.n; k++) {
+            if (flags[k] & CUT_FLAG_NOPLANE) keep[k] = 1;     // skipped by the cut; keeps the small-part rule
+            else valid.push_back(k);
+        }
+        P.stats[0] += valid.size();
+        std::vector<float> key(valid.size());
+        for (size_t r = 0; r < valid.size(); r++) {
+            const float y = pred[valid[r]];
+            key[r] = y == y ? y : 3.402823466e38f;             // NaN ranks last
+        }
+        std::vector<int> order(valid.size());
+        for (size_t r = 0; r < valid.size(); r++) order[r] = (int)r;
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return key[a] < key[b]; });
+        const int k = std::min<int>(P.top_k, (int)valid.size());
+        const float kth = k > 0 ? key[order[k - 1]] : 0.f;
+        for (int r = 0; r < (int)order.size(); r++)
+            if (r < k || key[order[r]] <= kth + P.margin) { keep[valid[order[r]]] = 1; P.stats[1]++; }
+    }
+    std::vector<CutJob> kj;
+    std::vector<std::pair<int, int>> ko;
+    for (int j = 0; j < n; j++) if (keep[j]) { kj.push_back(jobs[j]); ko.push_back(job_of[j]); }
+    jobs.swap(kj);
+    job_of.swap(ko);
+    return 0;
+}
+
+static int lookahead_impl(gpu_ctx_t ctx, const float* verts, int nv, const int* tris, int nt,
+                          const float* hull_verts, int hull_nv, const int* hull_tris, int hull_nt,
+                          int max_iters, int width, int width2, float threshold,
+                          int depth, int max_n_cutting, int verbose, int debug, int decompose_components,
+                          int decompose_components_per_iter,
+                          int n_concave_edges, float concave_eps, float concave_threshold,
+                          int concave_iters, const Prune* prune, struct gpu_result* out)
+{
     if (!ctx || !out) return -1;
     out->parts = nullptr; out->nparts = 0;
     if (nv <= 0 || nt <= 0) return ctx_fail(ctx, KERR_MESH_INVALID, "empty mesh");
@@ -445,20 +571,31 @@ extern "C" int lookahead_decompose(gpu_ctx_t ctx, const float* verts, int nv, co
     for (int d = 1; d < depth; d++) max_jobs *= width2;
     const size_t hjob_cap = std::max<size_t>(2 * max_jobs, 2 * 4096);
     size_t fixed = al256(sizeof(CutJob) * max_jobs) + al256(sizeof(CutResult) * max_jobs) + al256(sizeof(FragRes) * 2 * max_jobs)
-                 + al256(2 * sizeof(Arena)) + al256(mesh_bytes) + al256(12 * ((size_t)hull_nv + hull_nt))
+                 + al256(sizeof(float4) * max_n_cutting * tw_max) + al256(sizeof(int) * max_n_cutting * tw_max)
+                 + al256(3 * sizeof(Arena)) + al256(mesh_bytes) + al256(12 * ((size_t)hull_nv + hull_nt))
                  + al256(sizeof(HDSurf) * 2 * 4096) + al256(sizeof(HDPrep) * 2 * 4096) + al256(hd_dir_bytes() * 2 * 4096)
                  + al256(64) + al256(sizeof(float) * 2 * 4096) + al256(sizeof(double) * 4096)
                  + al256(sizeof(CompResult) * 2 * 4096)
                  + al256(sizeof(HullJob) * hjob_cap) + al256(sizeof(HullState) * hjob_cap) + al256(64)
                  + al256(hull_wrap_buf_bytes(hull_wrap_ctas(1LL << 40, ctx->n_sm)));
-    size_t out_cap = std::max<size_t>((size_t)1 << 30, 8 * mesh_bytes * std::min<size_t>(max_jobs, 512));
+    // Output arena: the fragments and hulls of every level but the last.  The
+    // cutting parts of one iteration partition (part of) the mesh, so one
+    // level-0 candidate set outputs about 64 bytes per input vertex and
+    // triangle per plane; each further kept level multiplies by width2.
+    size_t lvl_bytes = (size_t)tw_max * 64 * ((size_t)nv + nt) * 5 / 4;
+    for (int d = 1; d + 1 < depth; d++) lvl_bytes *= width2;
+    size_t out_cap = std::min<size_t>(std::max<size_t>((size_t)1 << 30, lvl_bytes), (size_t)96 << 30);
+    size_t tmp_cap = std::min<size_t>(std::max<size_t>((size_t)1 << 30, (size_t)width2 * 64 * ((size_t)nv + nt) * 2),
+                                      (size_t)16 << 30);
     size_t scr_cap = std::max<size_t>((size_t)2 << 30, hull_scratch_bytes(nv) * 64);
-    int rc = pool_begin(ctx, fixed + out_cap + scr_cap + (1 << 20));
+    int rc = pool_begin(ctx, fixed + out_cap + tmp_cap + scr_cap + (1 << 20));
     if (rc) return rc;
     CutJob* d_jobs = pool_take<CutJob>(ctx, max_jobs);
+    float4* d_jplanes = pool_take<float4>(ctx, (size_t)max_n_cutting * tw_max);
+    int* d_jflags = pool_take<int>(ctx, (size_t)max_n_cutting * tw_max);
     CutResult* d_cuts = pool_take<CutResult>(ctx, max_jobs);
     FragRes* d_frags = pool_take<FragRes>(ctx, 2 * max_jobs);
-    Arena* d_arenas = pool_take<Arena>(ctx, 2);
+    Arena* d_arenas = pool_take<Arena>(ctx, 3);
     float* d_v0 = pool_take<float>(ctx, 3 * (size_t)nv);
     int* d_t0 = pool_take<int>(ctx, 3 * (size_t)nt);
     float* d_hv0 = pool_take<float>(ctx, 3 * (size_t)hull_nv);
@@ -476,10 +613,12 @@ extern "C" int lookahead_decompose(gpu_ctx_t ctx, const float* verts, int nv, co
     int* d_wbuf = (int*)pool_take<char>(ctx, hull_wrap_buf_bytes(hull_wrap_ctas(1LL << 40, ctx->n_sm)));
     char* out_base = pool_take<char>(ctx, out_cap);
     char* scr_base = pool_take<char>(ctx, scr_cap);
-    if (!scr_base) return ctx_fail(ctx, KERR_HEAP_OOM, "pool carve failed");
+    char* tmp_base = pool_take<char>(ctx, tmp_cap);
+    if (!scr_base || !tmp_base) return ctx_fail(ctx, KERR_HEAP_OOM, "pool carve failed");
     Lookahead L;
     L.ctx = ctx; L.s = s; L.out_base = out_base; L.out_cap = out_cap; L.scr_base = scr_base; L.scr_cap = scr_cap;
-    L.d_out = d_arenas; L.d_scr = d_arenas + 1;
+    L.d_out = d_arenas; L.d_scr = d_arenas + 1; L.d_tmp = d_arenas + 2; L.d_cur = L.d_out;
+    L.tmp_base = tmp_base; L.tmp_cap = tmp_cap;
     L.min_edge = std::min(threshold * 0.25f, 0.015f);
     L.debug = debug;
     L.d_surfs = d_surfs; L.surf_cap = 2 * 4096; L.d_cres = d_cres;
@@ -622,7 +761,13 @@ extern "C" int lookahead_decompose(gpu_ctx_t ctx, const float* verts, int nv, co
                     job_of.push_back({ii, ci});
                 }
             }
-            int lr = L.run_level(jobs, cuts, frs, d_jobs, d_cuts, d_frags);
+            if (d == 0 && prune && prune->sc) {
+                result = prune_level0(ctx, L, *prune, cur, jobs, job_of, d_jobs, d_jplanes, d_jflags);
+                if (result) break;
+            }
+            const bool last = d == depth - 1 && d > 0;
+            int lr = last ? L.run_last_level(jobs, cuts, frs, d_jobs, d_cuts, d_frags)
+                          : L.run_level(jobs, cuts, frs, d_jobs, d_cuts, d_frags);
             if (lr) { result = ctx_fail(ctx, lr, "lookahead level %d failed at iter %d (0x%x)", d, iter, lr); break; }
             std::vector<Item> next;
             std::vector<bool> small_done(cur.size(), false);
@@ -658,6 +803,19 @@ extern "C" int lookahead_decompose(gpu_ctx_t ctx, const float* verts, int nv, co
                 next.push_back(std::move(x));
             }
             if (result) break;
+            if (d == 0 && prune && prune->beam > 0 && depth > 1) {
+                std::vector<std::vector<int>> by_src(nc);
+                for (int k = 0; k < (int)next.size(); k++) by_src[next[k].src].push_back(k);
+                std::vector<char> keep(next.size(), 0);
+                for (auto& ks : by_src) {
+                    std::stable_sort(ks.begin(), ks.end(), [&](int a, int b) { return next[a].costs[0] < next[b].costs[0]; });
+                    for (int r = 0; r < (int)ks.size() && r < prune->beam; r++) keep[ks[r]] = 1;
+                }
+                std::vector<Item> kept;
+                for (size_t k = 0; k < next.size(); k++) if (keep[k]) kept.push_back(std::move(next[k]));
+                next.swap(kept);
+            }
+            if (d == 0 && prune) prune->stats[2] += next.size();
             cur.swap(next);
         }
         if (result) break;
@@ -744,4 +902,41 @@ extern "C" int lookahead_decompose(gpu_ctx_t ctx, const float* verts, int nv, co
     cudaStreamSynchronize(s);
     if (result) { gpu_result_free(out); return result; }
     return 0;
+}
+
+extern "C" int lookahead_decompose(gpu_ctx_t ctx, const float* verts, int nv, const int* tris, int nt,
+                                   const float* hull_verts, int hull_nv, const int* hull_tris, int hull_nt,
+                                   int max_iters, int width, int width2, float threshold,
+                                   int depth, int quick_depth, int max_n_cutting,
+                                   int verbose, int debug, int decompose_components,
+                                   int decompose_components_per_iter,
+                                   int n_concave_edges, float concave_eps, float concave_threshold,
+                                   int concave_iters, int merge_hulls, struct gpu_result* out)
+{
+    (void)quick_depth; (void)merge_hulls;
+    return lookahead_impl(ctx, verts, nv, tris, nt, hull_verts, hull_nv, hull_tris, hull_nt, max_iters, width, width2,
+                          threshold, depth, max_n_cutting, verbose, debug, decompose_components,
+                          decompose_components_per_iter, n_concave_edges, concave_eps, concave_threshold,
+                          concave_iters, nullptr, out);
+}
+
+extern "C" int cuacd_lookahead_decompose_pruned(gpu_ctx_t ctx, cuacd_scorer_t scorer, int top_k, float margin,
+                                                int beam, unsigned long long* out_stats,
+                                                const float* verts, int nv, const int* tris, int nt,
+                                                const float* hull_verts, int hull_nv, const int* hull_tris,
+                                                int hull_nt, int max_iters, int width, int width2, float threshold,
+                                                int depth, int max_n_cutting, int verbose,
+                                                int decompose_components, int decompose_components_per_iter,
+                                                int n_concave_edges, float concave_eps, float concave_threshold,
+                                                int concave_iters, struct gpu_result* out)
+{
+    if (!ctx) return -1;
+    unsigned long long st[3] = {0, 0, 0};
+    Prune P{scorer, top_k > 0 ? top_k : 1, margin, beam, st};
+    int rc = lookahead_impl(ctx, verts, nv, tris, nt, hull_verts, hull_nv, hull_tris, hull_nt, max_iters, width,
+                            width2, threshold, depth, max_n_cutting, verbose, 0, decompose_components,
+                            decompose_components_per_iter, n_concave_edges, concave_eps, concave_threshold,
+                            concave_iters, &P, out);
+    if (out_stats) for (int k = 0; k < 3; k++) out_stats[k] = st[k];
+    return rc;
 }

@@ -359,6 +359,67 @@ __global__ void k_adamw(float* p, const float* gr, float* m, float* v, __nv_bflo
 }
 
 // ---------------------------------------------------------------------------
+// pruning: selection of the planes that go through the exact evaluator
+// ---------------------------------------------------------------------------
+#define SC_SEL_MAX 1024
+
+// One CTA.  Rank of plane i = number of planes predicted lower (ties: lower
+// index first); selected when rank < k or prediction <= k-th + margin.
+// Writes the selected planes compacted in index order, pos[i] (slot in the
+// compacted list or -1), the count and the predictions in score units.
+__global__ void __launch_bounds__(256)
+k_select_planes(const float* __restrict__ Y, int n, int k, float margin, const float4* __restrict__ planes,
+                float4* __restrict__ sel_planes, int* __restrict__ pos, int* __restrict__ count,
+                float* __restrict__ pred)
+{
+    __shared__ float key[SC_SEL_MAX];
+    __shared__ unsigned char fl[SC_SEL_MAX];
+    __shared__ float kth;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const float y = Y[i] / SC_TSCALE;
+        key[i] = (y == y) ? y : 3.402823466e38f;        // NaN ranks last
+        if (pred) pred[i] = y;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const float ki = key[i];
+        int r = 0;
+        for (int j = 0; j < n; j++) r += (key[j] < ki) || (key[j] == ki && j < i);
+        if (r == k - 1) kth = ki;
+        fl[i] = r < k;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += blockDim.x) fl[i] |= key[i] <= kth + margin;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int c = 0;
+        for (int i = 0; i < n; i++) {
+            if (fl[i]) { sel_planes[c] = planes[i]; pos[i] = c++; }
+            else pos[i] = -1;
+        }
+        *count = c;
+    }
+}
+
+// out[i] = the exact result of plane i when it was evaluated, else ok = 0
+// and FLT_MAX scores.
+__global__ void k_scatter_results(const cuacd_cand_result* __restrict__ sub, const int* __restrict__ pos, int n,
+                                  cuacd_cand_result* __restrict__ out, int* __restrict__ evaluated)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int j = pos[i];
+    cuacd_cand_result r;
+    if (j >= 0) r = sub[j];
+    else {
+        memset(&r, 0, sizeof(r));
+        r.score_rv = r.score_full = 3.402823466e38f;
+    }
+    out[i] = r;
+    if (evaluated) evaluated[i] = j >= 0;
+}
+
+// ---------------------------------------------------------------------------
 // host: the scorer object
 // ---------------------------------------------------------------------------
 namespace {
@@ -389,6 +450,8 @@ struct cuacd_scorer {
     // pruned-evaluation buffers
     float* mv; int* mt; float4* mp; PartStats* st; float* feat;
     size_t mv_cap, mt_cap, mp_cap;
+    char* pr; size_t pr_cap;     // device pruning: selected planes, pos, count, sub-results
+    int* h_count;                // pinned
 };
 
 static int sc_fail(gpu_ctx* ctx, int code, const char* msg) { return ctx_fail(ctx, code, "%s", msg); }
@@ -564,6 +627,7 @@ extern "C" void cuacd_scorer_free(cuacd_scorer_t s)
     cudaFree(s->X); cudaFree(s->T); cudaFree(s->idx); cudaFree(s->Xb); cudaFree(s->H1); cudaFree(s->H2);
     cudaFree(s->dYb); cudaFree(s->dH2b); cudaFree(s->dH1b); cudaFree(s->Tb); cudaFree(s->Y); cudaFree(s->dYf);
     cudaFree(s->dH2f); cudaFree(s->dH1f); cudaFree(s->mv); cudaFree(s->mt); cudaFree(s->mp); cudaFree(s->st);
+    cudaFree(s->pr); cudaFreeHost(s->h_count);
     free(s);                     // s->feat points into s->mp
     cudaGetLastError();          // a failed free must not surface in the next call's launch check
 }
@@ -586,30 +650,73 @@ extern "C" int cuacd_scorer_get_params(cuacd_scorer_t s, float* params)
     return cudaMemcpy(params, s->p32, sizeof(float) * N_PARAMS, cudaMemcpyDeviceToHost) == cudaSuccess ? 0 : -1;
 }
 
+// Predicted scores of rows already gathered in s->Xb (device), into s->Y.
+static void sc_predict_rows(cuacd_scorer* s, int n, cudaStream_t st) { sc_forward(s, n, st); }
+
+static int sc_grow(gpu_ctx* ctx, void** p, size_t& cap, size_t need)
+{
+    if (need <= cap) return 0;
+    cudaFree(*p);
+    *p = nullptr;
+    cap = 0;
+    SCK(cudaMalloc(p, need));
+    cap = need;
+    return 0;
+}
+
+// Room for n planes and their feature rows in s->mp (s->feat follows the planes).
+static int sc_feature_buffers(gpu_ctx* ctx, cuacd_scorer* s, int n)
+{
+    const size_t plane_bytes = (16 * (size_t)n + 255) & ~(size_t)255;
+    if (sc_grow(ctx, (void**)&s->mp, s->mp_cap, plane_bytes + sizeof(float) * (size_t)n * SC_K)) return -1;
+    if (!s->st) SCK(cudaMalloc(&s->st, sizeof(PartStats)));
+    s->feat = (float*)((char*)s->mp + plane_bytes);
+    return 0;
+}
+
+// Part statistics and the feature rows of n planes (device pointers) into s->feat.
+static void sc_launch_features(gpu_ctx* ctx, cuacd_scorer* s, const float* d_v, int nv, const int* d_t, int nt,
+                               float hull_vol, const float4* d_planes, int n, cudaStream_t st)
+{
+    k_part_stats<<<1, 256, 0, st>>>(d_v, nv, d_t, nt, hull_vol, s->st);
+    k_cand_features<<<n, 256, 0, st>>>(d_v, nv, d_planes, n, s->st, s->feat);
+    ctx->launches += 2;
+}
+
 // Features of n planes on one part (host pointers), SC_K floats per plane.
 static int sc_features_device(gpu_ctx* ctx, cuacd_scorer* s, const float* verts, int nv, const int* tris, int nt,
                               float hull_vol, const float* planes, int n, cudaStream_t st)
 {
-    auto grow = [&](void** p, size_t& cap, size_t need) -> int {
-        if (need <= cap) return 0;
-        cudaFree(*p);
-        SCK(cudaMalloc(p, need));
-        cap = need;
-        return 0;
-    };
-    if (grow((void**)&s->mv, s->mv_cap, 12 * (size_t)nv)) return -1;
-    if (grow((void**)&s->mt, s->mt_cap, 12 * (size_t)(nt > 0 ? nt : 1))) return -1;
-    const size_t plane_bytes = (16 * (size_t)n + 255) & ~(size_t)255;
-    if (grow((void**)&s->mp, s->mp_cap, plane_bytes + sizeof(float) * (size_t)n * SC_K)) return -1;
-    if (!s->st) SCK(cudaMalloc(&s->st, sizeof(PartStats)));
-    s->feat = (float*)((char*)s->mp + plane_bytes);
+    if (sc_grow(ctx, (void**)&s->mv, s->mv_cap, 12 * (size_t)nv)) return -1;
+    if (sc_grow(ctx, (void**)&s->mt, s->mt_cap, 12 * (size_t)(nt > 0 ? nt : 1))) return -1;
+    if (sc_feature_buffers(ctx, s, n)) return -1;
     SCK(cudaMemcpyAsync(s->mv, verts, 12 * (size_t)nv, cudaMemcpyHostToDevice, st));
     if (nt) SCK(cudaMemcpyAsync(s->mt, tris, 12 * (size_t)nt, cudaMemcpyHostToDevice, st));
     SCK(cudaMemcpyAsync(s->mp, planes, 16 * (size_t)n, cudaMemcpyHostToDevice, st));
-    k_part_stats<<<1, 256, 0, st>>>(s->mv, nv, s->mt, nt, hull_vol, s->st);
-    k_cand_features<<<n, 256, 0, st>>>(s->mv, nv, s->mp, n, s->st, s->feat);
-    ctx->launches += 2;
+    sc_launch_features(ctx, s, s->mv, nv, s->mt, nt, hull_vol, s->mp, n, st);
     SCK(cudaGetLastError());
+    return 0;
+}
+
+int scorer_predict_parts(gpu_ctx* ctx, cuacd_scorer* s, const ScorerPart* parts, int n_parts,
+                         const float4* d_planes, int n_rows, float* pred, cudaStream_t st)
+{
+    if (n_rows <= 0) return 0;
+    if (sc_feature_buffers(ctx, s, n_rows) || sc_reserve(ctx, s, n_rows)) return -1;
+    for (int i = 0; i < n_parts; i++) {
+        const ScorerPart& p = parts[i];
+        if (p.n <= 0) continue;
+        k_part_stats<<<1, 256, 0, st>>>(p.v, p.nv, p.t, p.nt, p.hull_vol, s->st);
+        k_cand_features<<<p.n, 256, 0, st>>>(p.v, p.nv, d_planes + p.off, p.n, s->st, s->feat + (size_t)p.off * SC_K);
+        ctx->launches += 2;
+    }
+    k_gather_rows<<<n_rows, 64, 0, st>>>(s->feat, nullptr, nullptr, n_rows, s->nrm, s->Xb, nullptr);
+    sc_predict_rows(s, n_rows, st);
+    ctx->launches += 4;
+    SCK(cudaGetLastError());
+    SCK(cudaMemcpyAsync(pred, s->Y, sizeof(float) * (size_t)n_rows, cudaMemcpyDeviceToHost, st));
+    SCK(cudaStreamSynchronize(st));
+    for (int i = 0; i < n_rows; i++) pred[i] /= SC_TSCALE;
     return 0;
 }
 
@@ -686,8 +793,6 @@ extern "C" int cuacd_scorer_train(gpu_ctx_t ctx, cuacd_scorer_t s, const float* 
     return 0;
 }
 
-// Predicted scores of rows already gathered in s->Xb (device), into s->Y.
-static void sc_predict_rows(cuacd_scorer* s, int n, cudaStream_t st) { sc_forward(s, n, st); }
 
 extern "C" int cuacd_scorer_predict(gpu_ctx_t ctx, cuacd_scorer_t s, const float* X, int n, float* out)
 {
@@ -752,16 +857,20 @@ extern "C" int cuacd_eval_candidates_pruned(gpu_ctx_t ctx, cuacd_scorer_t s, con
     SCK(cudaMemcpyAsync(pred.data(), s->Y, sizeof(float) * (size_t)n_planes, cudaMemcpyDeviceToHost, st));
     int rc = sync_and_check(ctx, "scorer_predict");
     if (rc) return rc;
-    for (int i = 0; i < n_planes; i++) pred[i] /= SC_TSCALE;
+    std::vector<float> key(n_planes);
+    for (int i = 0; i < n_planes; i++) {
+        pred[i] /= SC_TSCALE;
+        key[i] = pred[i] == pred[i] ? pred[i] : 3.402823466e38f;     // NaN ranks last
+    }
     std::vector<int> order(n_planes);
     for (int i = 0; i < n_planes; i++) order[i] = i;
-    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return pred[a] < pred[b]; });
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return key[a] < key[b]; });
     const int k = std::min(top_k, n_planes);
-    const float kth = pred[order[k - 1]];
+    const float kth = key[order[k - 1]];
     std::vector<int> sel;
     for (int r = 0; r < n_planes; r++) {
         const int i = order[r];
-        if (r < k || pred[i] <= kth + margin) sel.push_back(i);
+        if (r < k || key[i] <= kth + margin) sel.push_back(i);
     }
     std::sort(sel.begin(), sel.end());
     std::vector<float> sp(4 * sel.size());
@@ -782,5 +891,54 @@ extern "C" int cuacd_eval_candidates_pruned(gpu_ctx_t ctx, cuacd_scorer_t s, con
         if (out_evaluated) out_evaluated[sel[j]] = 1;
     }
     if (out_n_evaluated) *out_n_evaluated = (int)sel.size();
+    return 0;
+}
+
+// Device-pointer form of the pruned evaluation on `stream`: features,
+// network, selection and the scatter of results all run on the device; the
+// call waits once, for the selected count, before it launches the exact
+// evaluator on the selected planes.  hull_vol must be the part's hull volume.
+extern "C" int cuacd_eval_candidates_pruned_device(gpu_ctx_t ctx, cuacd_scorer_t s, const float* d_verts, int nv,
+                                                   const int* d_tris, int nt, float hull_vol, const float* d_planes,
+                                                   int n_planes, int flags, float hd_resolution, int hd_min_samples,
+                                                   int hd_total, int top_k, float margin, cuacd_cand_result* d_out,
+                                                   float* d_pred, int* d_evaluated, int* out_n_evaluated,
+                                                   void* stream)
+{
+    if (!ctx || !s || !d_out) return -1;
+    if (out_n_evaluated) *out_n_evaluated = 0;
+    if (n_planes <= 0) return 0;
+    if (n_planes > SC_SEL_MAX) return ctx_fail(ctx, -1, "pruned evaluation takes at most %d planes", SC_SEL_MAX);
+    if (nv <= 0 || nt <= 0) return ctx_fail(ctx, KERR_MESH_INVALID, "empty mesh");
+    if (!(hull_vol >= 0.f)) return ctx_fail(ctx, -1, "hull_vol must be the part's hull volume");
+    if (top_k <= 0) top_k = 1;
+    const int k = std::min(top_k, n_planes);
+    SCK(cudaSetDevice(ctx->device));
+    cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+    auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    const size_t o_pos = al(16 * (size_t)n_planes), o_cnt = o_pos + al(4 * (size_t)n_planes), o_sub = o_cnt + 256;
+    if (sc_grow(ctx, (void**)&s->pr, s->pr_cap, o_sub + sizeof(cuacd_cand_result) * (size_t)n_planes)) return -1;
+    if (!s->h_count) SCK(cudaMallocHost(&s->h_count, sizeof(int)));
+    if (sc_feature_buffers(ctx, s, n_planes) || sc_reserve(ctx, s, n_planes)) return -1;
+    float4* sel = (float4*)s->pr;
+    int* pos = (int*)(s->pr + o_pos);
+    int* cnt = (int*)(s->pr + o_cnt);
+    cuacd_cand_result* sub = (cuacd_cand_result*)(s->pr + o_sub);
+    sc_launch_features(ctx, s, d_verts, nv, d_tris, nt, hull_vol, (const float4*)d_planes, n_planes, st);
+    k_gather_rows<<<n_planes, 64, 0, st>>>(s->feat, nullptr, nullptr, n_planes, s->nrm, s->Xb, nullptr);
+    sc_predict_rows(s, n_planes, st);
+    k_select_planes<<<1, 256, 0, st>>>(s->Y, n_planes, k, margin, (const float4*)d_planes, sel, pos, cnt, d_pred);
+    ctx->launches += 5;
+    SCK(cudaGetLastError());
+    SCK(cudaMemcpyAsync(s->h_count, cnt, sizeof(int), cudaMemcpyDeviceToHost, st));
+    SCK(cudaStreamSynchronize(st));
+    const int n_sel = *s->h_count;
+    int rc = cuacd_eval_candidates_device(ctx, d_verts, nv, d_tris, nt, (const float*)sel, n_sel, flags,
+                                          hd_resolution, hd_min_samples, hd_total, sub, st);
+    if (rc) return rc;
+    k_scatter_results<<<(n_planes + 127) / 128, 128, 0, st>>>(sub, pos, n_planes, d_out, d_evaluated);
+    ctx->launches += 1;
+    SCK(cudaGetLastError());
+    if (out_n_evaluated) *out_n_evaluated = n_sel;
     return 0;
 }

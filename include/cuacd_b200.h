@@ -222,7 +222,10 @@ int cuacd_hull_batch_device(gpu_ctx_t ctx, const float* d_pts,
  * wraps, faces, points tested by the wraps, SM cycles spent in set-up (sort,
  * BVH, first face), device clock (ns) when the wrapping took the cloud's
  * first edge and when it finished, large faces (+ 2^32 per wrap on the
- * cloud's own node lists, + 2^48 per face built in its own buffers). */
+ * cloud's own node lists, + 2^48 per face built in its own buffers).  For a
+ * cloud whose construction failed, slots 4-7 instead hold the first failure
+ * as pairs of 32-bit values (low, high): (site, u), (v, c), (coplanar count,
+ * corner count), and for a failed wrap the input indices of u and v. */
 int cuacd_hull_stats(gpu_ctx_t ctx, const float* pts, int total_pts,
                      const int* offsets, int n_hulls, int* out_nv, int* out_nt,
                      float* out_vol, unsigned long long* out_stats);
@@ -298,6 +301,19 @@ int cuacd_eval_candidates_pruned(gpu_ctx_t ctx, cuacd_scorer_t s, const float* v
                                  int top_k, float margin, cuacd_cand_result* out,
                                  float* out_pred, int* out_evaluated, int* out_n_evaluated);
 
+/* Device-pointer form on `stream` (at most 1024 planes): features, network,
+ * selection and the scatter of results run on the device; the call waits
+ * once for the selected count, then launches the exact evaluator on the
+ * selected planes and returns without synchronising.  d_pred and
+ * d_evaluated may be NULL; hull_vol must be the part's hull volume. */
+int cuacd_eval_candidates_pruned_device(gpu_ctx_t ctx, cuacd_scorer_t s, const float* d_verts, int nv,
+                                        const int* d_tris, int nt, float hull_vol,
+                                        const float* d_planes, int n_planes, int flags,
+                                        float hd_resolution, int hd_min_samples, int hd_total,
+                                        int top_k, float margin, cuacd_cand_result* d_out,
+                                        float* d_pred, int* d_evaluated, int* out_n_evaluated,
+                                        void* stream);
+
 /* ---- lookahead search (reference csrc/lookahead.h, csrc/heap.h) ---------- */
 
 struct gpu_part_result {
@@ -334,6 +350,26 @@ int lookahead_decompose(gpu_ctx_t ctx,
                         int n_concave_edges, float concave_eps,
                         float concave_threshold, int concave_iters,
                         int merge_hulls, struct gpu_result* out);
+
+/* lookahead_decompose with pruning (no counterpart in the reference).  With
+ * a scorer, it ranks each cutting part's level-0 planes and only the top_k,
+ * plus every plane predicted within `margin` of the k-th, are cut and scored
+ * exactly (scorer NULL: all are).  With beam > 0, only the `beam` level-0
+ * cuts of each part with the lowest exact level-0 cost are expanded to the
+ * next level.  Deeper levels, the choice of the cut and every part cost stay
+ * exact.  out_stats (optional, 3 values): level-0 planes ranked, planes cut,
+ * level-0 cuts expanded.  Other arguments as lookahead_decompose. */
+int cuacd_lookahead_decompose_pruned(gpu_ctx_t ctx, cuacd_scorer_t scorer, int top_k, float margin,
+                                     int beam, unsigned long long* out_stats,
+                                     const float* verts, int nv, const int* tris, int nt,
+                                     const float* hull_verts, int hull_nv,
+                                     const int* hull_tris, int hull_nt,
+                                     int max_iters, int width, int width2, float threshold,
+                                     int depth, int max_n_cutting, int verbose,
+                                     int decompose_components, int decompose_components_per_iter,
+                                     int n_concave_edges, float concave_eps,
+                                     float concave_threshold, int concave_iters,
+                                     struct gpu_result* out);
 
 #ifdef __cplusplus
 }

@@ -78,3 +78,18 @@ def test_kdop_caps(ctx):
     v, _ = W.candidate_mesh(64, 20)
     (hv, ht, vol), = ctx.batch_kdop_hull_mesh([v])
     assert 0 < len(hv) <= 4096 and len(ht) == 2 * len(hv) - 4
+
+
+def test_flat_leaves_in_face_plane(ctx, oracle):
+    """A fragment cloud (210 points of a lookahead cut of the ridged sphere
+    candidate_mesh(64, 24), with two axis-cut caps) whose BVH leaves lie flat
+    in hull faces: the leaf bound must keep their points on the face, or the
+    wrap loses them (the hull failed with an extraction error).  Also the
+    same cloud shuffled and in a batch with others."""
+    c = np.load(os.path.join(GOLDEN, "hull_flat_leaves.npy"))
+    rng = np.random.default_rng(0)
+    clouds = [c] + [c[rng.permutation(len(c))] for _ in range(3)] + W.hull_clouds(4, 1000, 0)
+    gpu = _gpu_hulls(ctx, clouds)
+    _check_exact(oracle, clouds, gpu)
+    vol, err = ctx.batch_hull_volume(clouds)
+    assert not err.any()

@@ -159,3 +159,41 @@ def test_ablation_trained_vs_random(ctx, S):
     random_hit = float(np.mean(np.minimum(8, sizes) / sizes))
     assert hit > random_hit + 0.15, (hit, random_hit)
     assert reg < 0.5 * rreg, (reg, rreg)
+
+
+def test_pruned_device_matches_host(ctx, S, part):
+    """The device-pointer pruned evaluation (selection and scatter on the
+    GPU) returns the host entry point's results, predictions and mask."""
+    import ctypes
+    import torch
+    import cuacd_b200
+    v, t = part
+    sc = S.Scorer(ctx, seed=4)
+    planes = S.candidate_set(ctx, v, t)
+    n = len(planes)
+    hv = S.part_hull_volume(ctx, v)
+    res, pred, ev = sc.eval_pruned(v, t, planes, top_k=5, margin=0.01, hull_vol=hv)
+    dv = torch.from_numpy(v.reshape(-1)).cuda()
+    dt = torch.from_numpy(t.reshape(-1).astype(np.int32)).cuda()
+    dp = torch.from_numpy(planes.reshape(-1)).cuda()
+    nb = ctypes.sizeof(cuacd_b200.CandResult) * n
+    dout = torch.zeros(nb, dtype=torch.uint8, device="cuda")
+    dpred = torch.zeros(n, dtype=torch.float32, device="cuda")
+    dev = torch.zeros(n, dtype=torch.int32, device="cuda")
+    ne = ctypes.c_int(0)
+    stream = torch.cuda.current_stream()
+    rc = cuacd_b200._fn("cuacd_eval_candidates_pruned_device")(
+        ctx.handle, sc._h, ctypes.c_void_p(dv.data_ptr()), len(v), ctypes.c_void_p(dt.data_ptr()), len(t),
+        float(hv), ctypes.c_void_p(dp.data_ptr()), n, 1, 2000.0, 1000, 0, 5, 0.01,
+        ctypes.c_void_p(dout.data_ptr()), ctypes.c_void_p(dpred.data_ptr()), ctypes.c_void_p(dev.data_ptr()),
+        ctypes.byref(ne), ctypes.c_void_p(stream.cuda_stream))
+    ctx._check(rc)
+    torch.cuda.synchronize()
+    host = (cuacd_b200.CandResult * n)()
+    buf = dout.cpu().numpy()
+    ctypes.memmove(host, buf.ctypes.data, nb)
+    got = [cuacd_b200.cand_to_dict(r) for r in host]
+    assert ne.value == int(ev.sum())
+    np.testing.assert_array_equal(dev.cpu().numpy().astype(bool), ev)
+    np.testing.assert_array_equal(dpred.cpu().numpy(), pred)
+    assert got == res
