@@ -95,6 +95,8 @@ _opt("lookahead_decompose", _I, [_P, _P, _I, _P, _I, _P, _I, _P, _I,
                                  _I, _I, _I, _F, _I, _I, _I, _I, _I, _I, _I,
                                  _I, _F, _F, _I, _I, ctypes.POINTER(GpuResult)])
 _opt("gpu_result_free", None, [ctypes.POINTER(GpuResult)])
+_opt("cuacd_lookahead_trace", _I, [_P, _P, _P, _I, _P, _P, _I, _P, _I, _P, _I, _P, _I,
+                                   _I, _I, _I, _F, _I, _I, _I, _F, _F, _I, ctypes.POINTER(GpuResult)])
 _opt("cuacd_lookahead_decompose_pruned", _I, [_P, _P, _I, _F, _I, _P, _P, _I, _P, _I, _P, _I, _P, _I,
                                               _I, _I, _I, _F, _I, _I, _I, _I, _I, _I, _F, _F, _I,
                                               ctypes.POINTER(GpuResult)])

@@ -134,6 +134,11 @@ static __device__ int cut_ear_clip_cta(const Cap2D& c, const int* poly, int n, d
             clip = __syncthreads_or(inside) == 0;
         }
         if (clip) {
+            // Reflex steps and a degenerate ear meet no barrier, so a lagging
+            // thread may still be reading nxt[]/prv[] of an earlier step of
+            // the walk (nxt[p] among them): wait before the links change, or
+            // it would follow another walk into another barrier.
+            __syncthreads();
             if (tid == 0) {
                 cap[3 * nc] = poly[p]; cap[3 * nc + 1] = poly[cur]; cap[3 * nc + 2] = poly[q];
                 nxt[p] = q; prv[q] = p;

@@ -56,3 +56,6 @@ struct ScorerPart { const float* v; const int* t; int nv, nt; float hull_vol; in
 // each part p into pred[0, n_rows) (host); synchronises `s`.
 int scorer_predict_parts(gpu_ctx* ctx, cuacd_scorer* sc, const ScorerPart* parts, int n_parts,
                          const float4* d_planes, int n_rows, float* pred, cudaStream_t s);
+// Feature rows of the last scorer_predict_parts call (n_rows x n_features floats) to the host.
+int scorer_copy_features(gpu_ctx* ctx, cuacd_scorer* sc, int n_rows, float* out, cudaStream_t s);
+int scorer_n_features();

@@ -489,7 +489,15 @@ static int prune_level0(gpu_ctx* ctx, Lookahead& L, const Prune& P, const std::v
 // with the lowest exact level-0 cost are expanded further.  stats[0] +=
 // level-0 candidates ranked, stats[1] += those cut, stats[2] += level-0
 // items expanded.
-struct Prune { cuacd_scorer* sc; int top_k; float margin; int beam; unsigned long long* stats; };
+struct Prune {
+    cuacd_scorer* sc; int top_k; float margin; int beam; unsigned long long* stats;
+    // trace mode (top_k <= 0 with a scorer): nothing is pruned; every level-0
+    // candidate's feature row is kept with its exact level-0 cost and its
+    // path cost (mean level cost of its best leaf), rows of n_features + 4
+    // floats: features, level-0 cost, path cost, part key, 1 if it has leaves
+    std::vector<float>* trace; size_t trace_cap; int iter;
+    mutable std::vector<float> tfeat; mutable std::vector<std::pair<int, int>> tkey;
+};
 
 static int prune_level0(gpu_ctx* ctx, Lookahead& L, const Prune& P, const std::vector<Item>& cur,
                         std::vector<CutJob>& jobs, std::vector<std::pair<int, int>>& job_of, CutJob* d_jobs,
@@ -517,6 +525,13 @@ static int prune_level0(gpu_ctx* ctx, Lookahead& L, const Prune& P, const std::v
     std::vector<float> pred(n);
     int rc = scorer_predict_parts(ctx, P.sc, sp.data(), (int)sp.size(), d_planes, n, pred.data(), s);
     if (rc) return rc;
+    if (P.top_k <= 0) {                                // trace: keep every job, remember its row
+        P.tfeat.resize((size_t)n * scorer_n_features());
+        rc = scorer_copy_features(ctx, P.sc, n, P.tfeat.data(), s);
+        if (rc) return rc;
+        P.tkey.assign(job_of.begin(), job_of.end());
+        return 0;
+    }
     std::vector<char> keep(n, 0);
     for (const ScorerPart& p : sp) {
         std::vector<int> valid;
@@ -734,6 +749,8 @@ static int lookahead_impl(gpu_ctx_t ctx, const float* verts, int nv, const int* 
             it.parts.push_back({p.v, p.t, p.nv, p.nt, p.mesh_vol, p.hull_vol, p.hv, p.ht, p.hnv, p.hnt});
             cur.push_back(it);
         }
+        std::vector<int> cur_src_of_item0(cur.size());  // level-0 item -> cutting part
+        for (size_t ii = 0; ii < cur.size(); ii++) cur_src_of_item0[ii] = cur[ii].src;
         std::vector<Item> level0;              // level-0 items by (src, cut) for apply
         std::vector<std::vector<int>> l0index(nc, std::vector<int>(tw0, -1));
         L.reset_out();
@@ -842,7 +859,24 @@ static int lookahead_impl(gpu_ctx_t ctx, const float* verts, int nv, const int* 
             float best = 1e30f; int bi = -1;
             for (int ci = 0; ci < tw0; ci++) if (cb[ci] < best) { best = cb[ci]; bi = ci; }
             best_cut[c] = bi;
+            if (prune && prune->trace && !prune->tkey.empty()) {
+                const int K = scorer_n_features();
+                for (size_t j = 0; j < prune->tkey.size(); j++) {
+                    if (cur_src_of_item0[prune->tkey[j].first] != c) continue;
+                    const int ci = prune->tkey[j].second;
+                    const int li = l0index[c][ci];
+                    if (li < 0 || level0[li].costs.empty()) continue;      // no split: not a candidate
+                    if (prune->trace->size() + K + 4 > prune->trace_cap) break;
+                    const float* f = prune->tfeat.data() + j * K;
+                    prune->trace->insert(prune->trace->end(), f, f + K);
+                    prune->trace->push_back(level0[li].costs[0]);
+                    prune->trace->push_back(cb[ci] < 1e30f ? cb[ci] : level0[li].costs[0]);
+                    prune->trace->push_back((float)(iter * 4096 + c));
+                    prune->trace->push_back(any ? 1.f : 0.f);
+                }
+            }
         }
+        if (prune) { prune->tkey.clear(); prune->tfeat.clear(); }
         // ---- 6. apply: the part becomes the two halves of its best level-0 item
         bool applied = false;
         std::vector<HPart> added;
@@ -939,4 +973,28 @@ extern "C" int cuacd_lookahead_decompose_pruned(gpu_ctx_t ctx, cuacd_scorer_t sc
                             concave_iters, &P, out);
     if (out_stats) for (int k = 0; k < 3; k++) out_stats[k] = st[k];
     return rc;
+}
+
+extern "C" int cuacd_lookahead_trace(gpu_ctx_t ctx, cuacd_scorer_t scorer, float* out_rows, int max_rows,
+                                     int* out_n_rows, const float* verts, int nv, const int* tris, int nt,
+                                     const float* hull_verts, int hull_nv, const int* hull_tris, int hull_nt,
+                                     int max_iters, int width, int width2, float threshold, int depth,
+                                     int max_n_cutting, int n_concave_edges, float concave_eps,
+                                     float concave_threshold, int concave_iters, struct gpu_result* out)
+{
+    if (!ctx) return -1;
+    if (!scorer || !out_rows || !out_n_rows || max_rows < 0) return ctx_fail(ctx, -1, "bad trace arguments");
+    *out_n_rows = 0;
+    const int W = scorer_n_features() + 4;
+    std::vector<float> rows;
+    unsigned long long st[3] = {0, 0, 0};
+    Prune P{scorer, 0, 0.f, 0, st, &rows, (size_t)max_rows * W, 0, {}, {}};
+    int rc = lookahead_impl(ctx, verts, nv, tris, nt, hull_verts, hull_nv, hull_tris, hull_nt, max_iters, width,
+                            width2, threshold, depth, max_n_cutting, 0, 0, 0, 1, n_concave_edges, concave_eps,
+                            concave_threshold, concave_iters, &P, out);
+    if (rc) return rc;
+    const int n = (int)(rows.size() / W);
+    memcpy(out_rows, rows.data(), sizeof(float) * (size_t)n * W);
+    *out_n_rows = n;
+    return 0;
 }

@@ -720,6 +720,16 @@ int scorer_predict_parts(gpu_ctx* ctx, cuacd_scorer* s, const ScorerPart* parts,
     return 0;
 }
 
+int scorer_copy_features(gpu_ctx* ctx, cuacd_scorer* s, int n_rows, float* out, cudaStream_t st)
+{
+    if (n_rows <= 0) return 0;
+    SCK(cudaMemcpyAsync(out, s->feat, sizeof(float) * (size_t)n_rows * SC_K, cudaMemcpyDeviceToHost, st));
+    SCK(cudaStreamSynchronize(st));
+    return 0;
+}
+
+int scorer_n_features() { return SC_K; }
+
 extern "C" int cuacd_candidate_features(gpu_ctx_t ctx, cuacd_scorer_t s, const float* verts, int nv, const int* tris,
                                         int nt, float hull_vol, const float* planes, int n, float* out)
 {

@@ -163,6 +163,30 @@ class Scorer:
         return [cand_to_dict(out[i]) for i in range(n)], pred, ev.astype(bool)
 
 
+def lookahead_trace(ctx, scorer, verts, tris, max_rows=200000, *, max_iters=100, width=30, width2=5,
+                    threshold=0.05, depth=2, max_n_cutting=16, n_concave_edges=32, concave_eps=0.005,
+                    concave_threshold=3.49, concave_iters=10):
+    """Exact lookahead_decompose recording every level-0 candidate: returns
+    (features [n, 240], level-0 cost [n], path cost [n], part key [n], n_parts)."""
+    from . import GpuResult
+    v, t = _as_f32(verts).reshape(-1, 3), _as_i32(tris).reshape(-1, 3)
+    hull = ctx.batch_hull_dandc_mesh([v])[0]
+    hv, ht = _as_f32(hull[0]), _as_i32(hull[1])
+    W = N_FEATURES + 4
+    rows = np.zeros((max_rows, W), np.float32)
+    n = ctypes.c_int(0)
+    res = GpuResult()
+    ctx._check(_fn("cuacd_lookahead_trace")(
+        ctx.handle, scorer._h, _ptr(rows), int(max_rows), ctypes.byref(n), _ptr(v), len(v), _ptr(t), len(t),
+        _ptr(hv), len(hv), _ptr(ht), len(ht), int(max_iters), int(width), int(width2), float(threshold), int(depth),
+        int(max_n_cutting), int(n_concave_edges), float(concave_eps), float(concave_threshold), int(concave_iters),
+        ctypes.byref(res)))
+    n_parts = res.nparts
+    _fn("gpu_result_free")(ctypes.byref(res))
+    r = rows[:n.value]
+    return r[:, :N_FEATURES], r[:, N_FEATURES], r[:, N_FEATURES + 1], r[:, N_FEATURES + 2].astype(np.int64), n_parts
+
+
 def part_hull_volume(ctx, verts):
     vol, _ = ctx.batch_hull_volume([_as_f32(verts).reshape(-1, 3)])
     return float(vol[0])
@@ -178,15 +202,18 @@ def candidate_set(ctx, verts, tris, n_concave_edges=16, width=3, max_concave=27)
     return planes[keep]
 
 
-def exact_pairs(ctx, scorer, verts, tris, planes, **eval_kw):
+def exact_pairs(ctx, scorer, verts, tris, planes, target="full", **eval_kw):
     """(features, targets, ok mask, exact results) of planes on one part.
-    The target is the exact score_full; a plane that leaves one side empty
-    (ok = 0) takes the worst score among the part's splitting planes, so it
-    ranks last."""
+    The target is the exact score_full (target "full") or score_rv ("rv",
+    evaluated without Hausdorff); a plane that leaves one side empty (ok = 0)
+    takes the worst score among the part's splitting planes, so it ranks
+    last."""
     hv = part_hull_volume(ctx, verts)
     X = scorer.features(verts, tris, planes, hv)
+    if target == "rv":
+        eval_kw = dict(eval_kw, hausdorff=False)
     res = ctx.eval_candidates(verts, tris, planes, **eval_kw)
-    T = np.array([r["score_full"] for r in res], np.float32)
+    T = np.array([r["score_full" if target == "full" else "score_rv"] for r in res], np.float32)
     ok = np.array([bool(r["ok"]) and r["err"] == 0 for r in res])
     T[~ok] = T[ok].max() if ok.any() else 1.0
     return X, T, ok, res
@@ -227,7 +254,7 @@ def centered(T, groups):
     return (T - mean[groups]).astype(np.float32)
 
 
-def build_dataset(ctx, scorer, meshes, halves=True, plane_set=None, **eval_kw):
+def build_dataset(ctx, scorer, meshes, halves=True, plane_set=None, target="full", **eval_kw):
     """Exact (feature, score) pairs on each mesh's candidate planes
     (`candidate_set(**plane_set)`) and, when `halves`, on the two parts its
     best plane leaves (the next level's parts).  Returns X [n, 240], T [n],
@@ -241,7 +268,7 @@ def build_dataset(ctx, scorer, meshes, halves=True, plane_set=None, **eval_kw):
         planes = candidate_set(ctx, v, t, **plane_set)
         if len(planes) < 2:
             return None
-        X, T, ok, res = exact_pairs(ctx, scorer, v, t, planes, **eval_kw)
+        X, T, ok, res = exact_pairs(ctx, scorer, v, t, planes, target=target, **eval_kw)
         if not ok.any():
             return None
         Xs.append(X)
@@ -258,6 +285,10 @@ def build_dataset(ctx, scorer, meshes, halves=True, plane_set=None, **eval_kw):
                 if len(ht_) >= 8:
                     add(hv_, ht_)
     return np.concatenate(Xs), np.concatenate(Ts), np.concatenate(G)
+
+
+RV_WEIGHTS_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "scorer_rv_weights.npz")
+PATH_WEIGHTS_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "scorer_path_weights.npz")
 
 
 def ranking_quality(pred, T, groups, k=8):

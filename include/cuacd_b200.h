@@ -371,6 +371,21 @@ int cuacd_lookahead_decompose_pruned(gpu_ctx_t ctx, cuacd_scorer_t scorer, int t
                                      float concave_threshold, int concave_iters,
                                      struct gpu_result* out);
 
+/* Exact lookahead_decompose that also records, for every level-0 candidate
+ * that splits its part, the scorer's feature row followed by 4 floats: the
+ * exact level-0 cost, the path cost the search ranks it by (mean level cost
+ * of its best descendant leaf), a part key (iteration * 4096 + cutting-part
+ * index) and 1 if the part's candidates had leaves (else the path cost is the
+ * level-0 cost).  Up to max_rows rows of n_features + 4 floats go to
+ * out_rows; *out_n_rows receives the count.  The training pairs of the
+ * scorer's path-cost target (no counterpart in the reference). */
+int cuacd_lookahead_trace(gpu_ctx_t ctx, cuacd_scorer_t scorer, float* out_rows, int max_rows,
+                          int* out_n_rows, const float* verts, int nv, const int* tris, int nt,
+                          const float* hull_verts, int hull_nv, const int* hull_tris, int hull_nt,
+                          int max_iters, int width, int width2, float threshold, int depth,
+                          int max_n_cutting, int n_concave_edges, float concave_eps,
+                          float concave_threshold, int concave_iters, struct gpu_result* out);
+
 #ifdef __cplusplus
 }
 #endif
