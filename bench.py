@@ -24,6 +24,9 @@ roofline dominant kernel's algorithmic bytes / its CUDA-event duration.
 --impl reference: the CPU oracle port of the exact path on all host cores
          (the reference has no CPU implementation of this path; its CPU
          baselines need sources absent from the reference tree).
+search   whole lookahead searches on six ridged spheres through the host API:
+         meshes/s exact vs pruned (learned level-0 ranking + exact beam),
+         part counts and the largest part cost of each.
 N > 1 runs independent replicas (the path does not shard across GPUs).
 """
 import argparse
@@ -140,6 +143,62 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+SEARCH_TOP_K, SEARCH_BEAM = 48, 8
+
+
+def search_meshes():
+    """Search sample: six ridged displaced spheres (UV 64x24, 96x32, 128x40
+    and icospheres of 5,120-20,480 triangles), extent 2; their creases give
+    the concave-edge planes the search ranks."""
+    from cuacd_b200 import workloads as W
+    out = [W.candidate_mesh(64, 24), W.candidate_mesh(96, 32, 0.35, seed=5), W.candidate_mesh(128, 40, 0.4, seed=7)]
+    for lvl, amp, sd in ((4, 0.35, 1), (4, 0.45, 2), (5, 0.4, 3)):
+        v, t = W.icosphere(lvl)
+        v, t = W.displaced_sphere(v, t, amp, sd, n_terms=6, fmin=2.0, fmax=5.0, ridged=True)
+        out.append((W.normalize_extent(v).astype(np.float32), t))
+    return out
+
+
+def part_cost_max(parts):
+    """Largest rv cost of the returned parts (FP64 volumes of part and hull)."""
+    worst = 0.0
+    for v, t, hv, ht in parts:
+        def vol(V, T):
+            V = V.astype(np.float64)
+            return abs(float(np.einsum("ij,ij->i", V[T[:, 0]], np.cross(V[T[:, 1]], V[T[:, 2]])).sum()) / 6.0)
+        g = max(vol(hv, ht) - vol(v, t), 0.0) if len(ht) else 0.0
+        worst = max(worst, 0.3 * np.cbrt(3.0 / (4.0 * np.pi) * g))
+    return worst
+
+
+def search_leg(ctx, scorer, untrained):
+    """Whole lookahead searches (tau 0.05, width 30/5, depth 2, 32 concave
+    edges) on the search sample through the host API, exact and pruned (the
+    level-0 scorer keeps the top 48 planes of each part, the exact search
+    then expands the 8 best level-0 cuts).  One untimed pass of each mode
+    first (pools grow to size).  Ablations: the same beam without the
+    scorer, and the same pruning with an untrained (random) network."""
+    kw = dict(width=30, width2=5, depth=2, threshold=0.05, max_iters=100)
+    modes = {"exact": {}, "pruned": {"scorer": scorer, "top_k": SEARCH_TOP_K, "beam": SEARCH_BEAM},
+             "beam_only": {"beam": SEARCH_BEAM},
+             "untrained": {"scorer": untrained, "top_k": SEARCH_TOP_K, "beam": SEARCH_BEAM}}
+    meshes = search_meshes()
+    out = {}
+    for name, extra in modes.items():
+        for v, t in meshes[:2]:
+            ctx.lookahead_decompose(v, t, **kw, **extra)
+        t0 = time.perf_counter()
+        parts = [ctx.lookahead_decompose(v, t, **kw, **extra) for v, t in meshes]
+        dt = time.perf_counter() - t0
+        out[name] = {"meshes_per_s": len(meshes) / dt, "s": dt, "parts": int(sum(len(p) for p in parts)),
+                     "max_rv_cost": float(max(part_cost_max(p) for p in parts))}
+    out["speedup"] = out["exact"]["s"] / out["pruned"]["s"]
+    out["parts_ratio"] = out["pruned"]["parts"] / max(out["exact"]["parts"], 1)
+    out["workload"] = (f"{len(meshes)} ridged displaced spheres (3,072-20,480 tris), tau 0.05, width 30/5, "
+                       f"depth 2, 32 concave edges; pruned = learned top-{SEARCH_TOP_K} + beam {SEARCH_BEAM}")
+    return out
+
+
 def cpu_baseline(v, t, planes, budget_s=20.0):
     """Oracle port on all host cores over a bounded sample of the workload."""
     from oracle import oracle as O
@@ -222,6 +281,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-search", action="store_true", help="skip the whole-search comparison")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -418,6 +478,9 @@ def main():
                       "ms_per_step": tot_exact_ms / args.steps, "gpu_launches": int(l1 - l0),
                       "e2e": world_n * n * args.steps / e2e_exact_s,
                       "roofline": roofline(stage_exact, exact, np.ones(n, bool))}}
+    if not args.no_search:
+        with S.Scorer.load(ctx, S.RV_WEIGHTS_PATH) as rv, S.Scorer(ctx, seed=1) as raw:
+            line["search"] = search_leg(ctx, rv, raw)
     if rank == 0 and world_n == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(v, t, planes)
     if rank == 0:

@@ -64,3 +64,54 @@ def test_displaced_sphere(ctx, oracle):
         # each part's hull is the exact hull of its vertices
         vi, tri, hvol = oracle.hull(pv)
         np.testing.assert_array_equal(hv, pv[vi])
+
+
+def _rv_costs(parts):
+    out = []
+    for v, t, hv, ht in parts:
+        def vol(V, T):
+            V = V.astype(np.float64)
+            return abs(float(np.einsum("ij,ij->i", V[T[:, 0]], np.cross(V[T[:, 1]], V[T[:, 2]])).sum()) / 6.0)
+        g = max(vol(hv, ht) - vol(v, t), 0.0)
+        out.append(0.3 * np.cbrt(3.0 / (4.0 * np.pi) * g))
+    return out
+
+
+def _ridged(lvl, amp, seed):
+    v, t = W.icosphere(lvl)
+    v, t = W.displaced_sphere(v, t, amp, seed, n_terms=6, fmin=2.0, fmax=5.0, ridged=True)
+    return W.normalize_extent(v).astype(np.float32), t
+
+
+def test_pruned_search_quality(ctx, oracle):
+    """Learned level-0 pruning (top 48 of each part's planes by the trained
+    scorer, then the exact search expands its 8 best level-0 cuts): the parts
+    stay watertight, keep the volume, end below tau, and their count stays
+    within 10 % of the exact search's over three ridged meshes."""
+    from cuacd_b200 import scorer as S
+    rv = S.Scorer.load(ctx, S.RV_WEIGHTS_PATH)
+    kw = dict(width=30, width2=5, depth=2, threshold=0.05, max_iters=100)
+    meshes = [W.candidate_mesh(64, 24), _ridged(4, 0.35, 1), W.candidate_mesh(96, 32, 0.35, seed=5)]
+    n_exact = n_pruned = 0
+    for v, t in meshes:
+        pe = ctx.lookahead_decompose(v, t, **kw)
+        pp = ctx.lookahead_decompose(v, t, scorer=rv, top_k=48, beam=8, **kw)
+        ranked, cut, expanded = ctx.last_prune_stats
+        assert cut < 0.5 * ranked and expanded <= cut
+        n_exact += len(pe)
+        n_pruned += len(pp)
+        total = oracle.mesh_volume(v, t)
+        assert abs(sum(oracle.mesh_volume(pv, pt) for pv, pt, _, _ in pp) - total) / total < 1e-4
+        assert all(is_watertight(pt) for _, pt, _, _ in pp)
+        assert max(_rv_costs(pp)) < 0.05
+    assert n_pruned <= 1.10 * n_exact, (n_pruned, n_exact)
+
+
+def test_beam_only_search(ctx):
+    """Exact beam (no scorer): only the 4 best level-0 cuts of each part are
+    expanded; every part still ends below tau."""
+    v, t = _ridged(4, 0.35, 1)
+    pp = ctx.lookahead_decompose(v, t, width=30, width2=5, depth=2, threshold=0.05, beam=4)
+    ranked, cut, expanded = ctx.last_prune_stats
+    assert ranked == 0 and cut == 0 and expanded > 0
+    assert max(_rv_costs(pp)) < 0.05

@@ -197,3 +197,18 @@ def test_pruned_device_matches_host(ctx, S, part):
     np.testing.assert_array_equal(dev.cpu().numpy().astype(bool), ev)
     np.testing.assert_array_equal(dpred.cpu().numpy(), pred)
     assert got == res
+
+
+def test_search_scorer_ranks_level0(ctx, S):
+    """The trained level-0 scorer on held-out parts (seeds unseen in
+    training), over the search's level-0 planes (32 concave edges, 30 axis
+    cuts): its top 48 contains the plane with the lowest exact rv cost far
+    more often than 48 random planes do."""
+    sc = S.Scorer.load(ctx, S.RV_WEIGHTS_PATH)
+    plane_set = {"n_concave_edges": 32, "width": 30, "max_concave": 128}
+    X, T, G = S.build_dataset(ctx, sc, S.training_meshes(12, 4242), plane_set=plane_set, target="rv")
+    hit, reg, rreg = S.ranking_quality(sc.predict(X), T, G, k=48)
+    sizes = np.bincount(G)
+    random_hit = float(np.mean(np.minimum(48, sizes) / sizes))
+    assert hit > random_hit + 0.3, (hit, random_hit)
+    assert reg < 0.25 * rreg, (reg, rreg)
