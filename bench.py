@@ -358,6 +358,7 @@ def main():
     with torch.cuda.stream(stream):
         for _ in range(args.warmup):
             step()
+        for _ in range(args.warmup):
             step_pruned()
         stream.synchronize()
         # correctness guards on the resident paths
