@@ -71,6 +71,11 @@ extern "C" void gpu_destroy(gpu_ctx_t ctx)
     cudaStreamSynchronize(ctx->stream);
     if (ctx->pool) cudaFree(ctx->pool);
     if (ctx->d_arena) cudaFree(ctx->d_arena);
+    for (int i = 0; i < 3; i++) {
+        if (ctx->aux[i]) cudaStreamDestroy(ctx->aux[i]);
+        if (ctx->join_ev[i]) cudaEventDestroy(ctx->join_ev[i]);
+    }
+    if (ctx->fork_ev) cudaEventDestroy(ctx->fork_ev);
     cudaStreamDestroy(ctx->stream);
     free(ctx);
 }

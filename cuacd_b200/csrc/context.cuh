@@ -29,6 +29,9 @@ struct gpu_ctx {
     int            profile;            // record stage events in the evaluator
     cudaEvent_t    ev[8];              // stage boundaries of the last evaluation
     int            n_ev;
+    int            eval_groups;        // plane groups evaluated concurrently (0: default)
+    cudaStream_t   aux[3];             // streams of groups 1..3 (created on first use)
+    cudaEvent_t    fork_ev, join_ev[3];
     char           last_error[256];
 };
 
