@@ -176,7 +176,7 @@ def search_leg(ctx, scorer, untrained):
     edges) on the search sample through the host API, exact and pruned (the
     level-0 scorer keeps the top 48 planes of each part, the exact search
     then expands the 8 best level-0 cuts).  One untimed pass of each mode
-    first (pools grow to size).  Ablations: the same beam without the
+    over the sample first (pools grow to size).  Ablations: the same beam without the
     scorer, and the same pruning with an untrained (random) network."""
     kw = dict(width=30, width2=5, depth=2, threshold=0.05, max_iters=100)
     modes = {"exact": {}, "pruned": {"scorer": scorer, "top_k": SEARCH_TOP_K, "beam": SEARCH_BEAM},
@@ -185,7 +185,7 @@ def search_leg(ctx, scorer, untrained):
     meshes = search_meshes()
     out = {}
     for name, extra in modes.items():
-        for v, t in meshes[:2]:
+        for v, t in meshes:                       # untimed: the pools grow to the largest mesh's needs
             ctx.lookahead_decompose(v, t, **kw, **extra)
         t0 = time.perf_counter()
         parts = [ctx.lookahead_decompose(v, t, **kw, **extra) for v, t in meshes]

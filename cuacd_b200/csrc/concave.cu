@@ -17,11 +17,14 @@
 // Axis cuts replace la_axis_cut_candidate + la_expand's plane placement
 // (cuda/la_axis_cut.cuh:10-19, cuda/la_expand.cu:129-199).
 #include <cmath>
+#include <vector>
 #include "context.cuh"
 #include "cta_util.cuh"
 #include "launch.h"
 
 #define CC_NT 256
+
+static cudaStream_t s_of(gpu_ctx* ctx) { return ctx->stream; }
 
 struct ConcaveParams {
     int K;              // n_concave_edges
@@ -56,14 +59,17 @@ static __device__ int cc_face_normal(const float* v, const int* t, int f, float*
     return 1;
 }
 
-// One CTA per mesh.  keys: scratch of next_pow2(3*nt) u64; flags: 3*nt ints;
-// res: 4*K ints.  Writes up to 4K planes and the count.
-__global__ void __launch_bounds__(CC_NT)
-k_concave_planes(const float* __restrict__ v, int nv, const int* __restrict__ t, int nt, ConcaveParams P,
-                 unsigned long long* keys, int* flags, int* res, float4* out, int* out_count)
+// One CTA per mesh.  keys, tmp: 3*nt u64 each; flags: 3*nt ints; res: 4*K
+// ints.  Writes up to 4K planes and the count.  The directed edges are
+// ordered by a stable LSD radix sort of their 64-bit keys (8 passes of 8
+// bits; the keys are distinct, so the order is the keys' total order).
+static __device__ void concave_cta(const float* __restrict__ v, int nv, const int* __restrict__ t, int nt,
+                                   const ConcaveParams& P, unsigned long long* keys, unsigned long long* tmp,
+                                   int* flags, int* res, float4* out, int* out_count)
 {
     __shared__ int scan[34];
     __shared__ int s_nres;
+    __shared__ int cnt[256 * (CC_NT / 32)];
     const int tid = threadIdx.x;
     const int nd = 3 * nt;
     if (nt < 2 || P.K <= 0) { if (tid == 0) *out_count = 0; return; }
@@ -74,7 +80,7 @@ k_concave_planes(const float* __restrict__ v, int nv, const int* __restrict__ t,
         keys[i] = ((unsigned long long)lo << 43) | ((unsigned long long)hi << 22) | (unsigned long long)f;
     }
     __syncthreads();
-    cta_sort_u64(keys, nd);
+    cta_radix_sort_u64<CC_NT>(keys, tmp, nd, 0, 64, cnt, scan);
     const unsigned long long EDGE = ~((1ull << 22) - 1);
     for (int i = tid; i < nd; i += CC_NT) {
         int valid = 0;
@@ -176,6 +182,26 @@ k_concave_planes(const float* __restrict__ v, int nv, const int* __restrict__ t,
     (void)nv;
 }
 
+__global__ void __launch_bounds__(CC_NT)
+k_concave_planes(const float* __restrict__ v, int nv, const int* __restrict__ t, int nt, ConcaveParams P,
+                 unsigned long long* keys, unsigned long long* tmp, int* flags, int* res, float4* out, int* out_count)
+{
+    concave_cta(v, nv, t, nt, P, keys, tmp, flags, res, out, out_count);
+}
+
+// Several meshes, one CTA each (the lookahead's cutting parts).
+struct ConcaveJob {
+    const float* v; const int* t; int nv, nt;
+    unsigned long long* keys; unsigned long long* tmp; int* flags; int* res; float4* out; int* count;
+};
+__global__ void __launch_bounds__(CC_NT)
+k_concave_planes_batch(const ConcaveJob* __restrict__ jobs, int n_jobs, ConcaveParams P)
+{
+    if ((int)blockIdx.x >= n_jobs) return;
+    const ConcaveJob J = jobs[blockIdx.x];
+    concave_cta(J.v, J.nv, J.t, J.nt, P, J.keys, J.tmp, J.flags, J.res, J.out, J.count);
+}
+
 // Axis cuts: bbox reduction, then plane cut_idx of `width` per thread.
 __global__ void __launch_bounds__(CC_NT)
 k_axis_planes(const float* __restrict__ v, int nv, int width, float min_edge_dist, float4* out, int* valid)
@@ -223,9 +249,9 @@ extern "C" int cuacd_candidate_planes(gpu_ctx_t ctx, const float* verts, int nv,
     for (int i = 0; i < 3 * nt; i++) if (tris[i] < 0 || tris[i] >= nv) return ctx_fail(ctx, KERR_MESH_INVALID, "index out of range");
     CK(cudaSetDevice(ctx->device));
     int nd = 3 * nt;
-    int N = 1; while (N < nd) N <<= 1;
+    int N = nd > 0 ? nd : 1;
     int K = n_concave_edges;
-    size_t need = al256(12 * (size_t)nv) + al256(12 * (size_t)(nt > 0 ? nt : 1)) + al256(8 * (size_t)N)
+    size_t need = al256(12 * (size_t)nv) + al256(12 * (size_t)(nt > 0 ? nt : 1)) + 2 * al256(8 * (size_t)N)
                 + al256(4 * (size_t)(nd > 0 ? nd : 1)) + al256(16 * (size_t)(4 * K + 1)) + al256(16 * (size_t)(4 * K + width + 1))
                 + 2 * al256(4 * (size_t)(width + 2));
     int rc = pool_begin(ctx, need);
@@ -233,6 +259,7 @@ extern "C" int cuacd_candidate_planes(gpu_ctx_t ctx, const float* verts, int nv,
     float* dv = pool_take<float>(ctx, 3 * (size_t)nv);
     int* dt = pool_take<int>(ctx, 3 * (size_t)(nt > 0 ? nt : 1));
     unsigned long long* dk = pool_take<unsigned long long>(ctx, N);
+    unsigned long long* dk2 = pool_take<unsigned long long>(ctx, N);
     int* df = pool_take<int>(ctx, nd > 0 ? nd : 1);
     int* dr = pool_take<int>(ctx, 4 * (K + 1));
     float4* dp = pool_take<float4>(ctx, 4 * K + width + 1);
@@ -242,7 +269,7 @@ extern "C" int cuacd_candidate_planes(gpu_ctx_t ctx, const float* verts, int nv,
     if (nt) CK(cudaMemcpyAsync(dt, tris, 12 * (size_t)nt, cudaMemcpyHostToDevice, s));
     CK(cudaMemsetAsync(dc, 0, 4 * (size_t)(width + 2), s));
     ConcaveParams P = concave_params(K, concave_eps, concave_threshold);
-    k_concave_planes<<<1, CC_NT, 0, s>>>(dv, nv, dt, nt, P, dk, df, dr, dp, dc);
+    k_concave_planes<<<1, CC_NT, 0, s>>>(dv, nv, dt, nt, P, dk, dk2, df, dr, dp, dc);
     if (width > 0) k_axis_planes<<<1, CC_NT, 0, s>>>(dv, nv, width, min_edge_dist, dp + 4 * K, dc + 1);
     ctx->launches += 1 + (width > 0);
     CK(cudaGetLastError());
@@ -259,37 +286,67 @@ extern "C" int cuacd_candidate_planes(gpu_ctx_t ctx, const float* verts, int nv,
     return 0;
 }
 
-// Concave-edge planes of a device-resident mesh, scratch carved from
-// [scr, scr+cap); the planes (at most 4*K) land in out_host.  Synchronises
-// the stream.  Used by the lookahead search for each cutting part.
-int concave_planes_device(gpu_ctx* ctx, const float* d_v, int nv, const int* d_t, int nt, int K, float eps,
-                          float thr, char* scr, size_t cap, float4* out_host, int* out_count, cudaStream_t s)
+// Concave-edge planes of device-resident meshes, one CTA each, scratch
+// carved from [scr, scr+cap) (in waves when it does not hold them all); the
+// planes (at most 4*K per mesh) land in out[i].  Synchronises the stream.
+// Used by the lookahead search for its cutting parts.
+int concave_planes_device_batch(gpu_ctx* ctx, int n, const float* const* d_v, const int* nv, const int* const* d_t,
+                                const int* nt, int K, float eps, float thr, char* scr, size_t cap,
+                                std::vector<std::vector<float4>>& out)
 {
-    *out_count = 0;
-    if (K <= 0 || nt < 2) return 0;
-    if (nv >= (1 << 21) || nt >= (1 << 22)) return ctx_fail(ctx, KERR_MESH_INVALID, "mesh too large for edge keys");
-    const int nd = 3 * nt;
-    int N = 1; while (N < nd) N <<= 1;
-    size_t need = al256(8 * (size_t)N) + al256(4 * (size_t)nd) + al256(4 * (size_t)(4 * (K + 1)))
-                + al256(16 * (size_t)(4 * K + 1)) + al256(16);
-    if (need > cap) return ctx_fail(ctx, KERR_HEAP_OOM, "concave planes need %zu scratch bytes, have %zu", need, cap);
-    char* p = scr;
-    unsigned long long* dk = (unsigned long long*)p; p += al256(8 * (size_t)N);
-    int* df = (int*)p; p += al256(4 * (size_t)nd);
-    int* dr = (int*)p; p += al256(4 * (size_t)(4 * (K + 1)));
-    float4* dp = (float4*)p; p += al256(16 * (size_t)(4 * K + 1));
-    int* dc = (int*)p;
-    CK(cudaMemsetAsync(dc, 0, 16, s));
+    out.assign(n, std::vector<float4>());
+    if (K <= 0 || n <= 0) return 0;
     ConcaveParams P = concave_params(K, eps, thr);
-    k_concave_planes<<<1, CC_NT, 0, s>>>(d_v, nv, d_t, nt, P, dk, df, dr, dp, dc);
-    ctx->launches += 1;
-    CK(cudaGetLastError());
-    int cnt = 0;
-    CK(cudaMemcpyAsync(&cnt, dc, sizeof(int), cudaMemcpyDeviceToHost, s));
-    CK(cudaStreamSynchronize(s));
-    if (cnt > 4 * K) return ctx_fail(ctx, KERR_MESH_INVALID, "concave plane count %d above %d", cnt, 4 * K);
-    if (cnt > 0) CK(cudaMemcpyAsync(out_host, dp, 16 * (size_t)cnt, cudaMemcpyDeviceToHost, s));
-    CK(cudaStreamSynchronize(s));
-    *out_count = cnt;
+    auto part_bytes = [&](int i) -> size_t {
+        const size_t nd = 3 * (size_t)(nt[i] > 0 ? nt[i] : 1);
+        return 2 * al256(8 * nd) + al256(4 * nd) + al256(4 * (size_t)(4 * (K + 1))) + al256(16 * (size_t)(4 * K + 1))
+             + al256(16);
+    };
+    const size_t job_bytes = al256(sizeof(ConcaveJob) * (size_t)n);
+    if (job_bytes >= cap) return ctx_fail(ctx, KERR_HEAP_OOM, "concave planes: scratch too small");
+    ConcaveJob* d_jobs = (ConcaveJob*)scr;
+    int i0 = 0;
+    while (i0 < n) {
+        std::vector<ConcaveJob> jobs;
+        char* p = scr + job_bytes;
+        int i1 = i0;
+        while (i1 < n) {
+            const size_t b = part_bytes(i1);
+            if ((size_t)(p - scr) + b > cap) break;
+            ConcaveJob J;
+            const size_t nd = 3 * (size_t)(nt[i1] > 0 ? nt[i1] : 1);
+            J.v = d_v[i1]; J.t = d_t[i1]; J.nv = nv[i1]; J.nt = nt[i1];
+            J.keys = (unsigned long long*)p; p += al256(8 * nd);
+            J.tmp = (unsigned long long*)p; p += al256(8 * nd);
+            J.flags = (int*)p; p += al256(4 * nd);
+            J.res = (int*)p; p += al256(4 * (size_t)(4 * (K + 1)));
+            J.out = (float4*)p; p += al256(16 * (size_t)(4 * K + 1));
+            J.count = (int*)p; p += al256(16);
+            if (nv[i1] >= (1 << 21) || nt[i1] >= (1 << 22))
+                return ctx_fail(ctx, KERR_MESH_INVALID, "mesh too large for edge keys");
+            jobs.push_back(J);
+            i1++;
+        }
+        if (i1 == i0) return ctx_fail(ctx, KERR_HEAP_OOM, "concave planes need %zu scratch bytes, have %zu",
+                                      part_bytes(i0) + job_bytes, cap);
+        const int m = i1 - i0;
+        CK(cudaMemcpyAsync(d_jobs, jobs.data(), sizeof(ConcaveJob) * m, cudaMemcpyHostToDevice, s_of(ctx)));
+        k_concave_planes_batch<<<m, CC_NT, 0, s_of(ctx)>>>(d_jobs, m, P);
+        ctx->launches += 1;
+        CK(cudaGetLastError());
+        std::vector<int> cnt(m);
+        for (int k = 0; k < m; k++)
+            CK(cudaMemcpyAsync(&cnt[k], jobs[k].count, sizeof(int), cudaMemcpyDeviceToHost, s_of(ctx)));
+        CK(cudaStreamSynchronize(s_of(ctx)));
+        for (int k = 0; k < m; k++) {
+            if (cnt[k] > 4 * K) return ctx_fail(ctx, KERR_MESH_INVALID, "concave plane count %d above %d", cnt[k], 4 * K);
+            out[i0 + k].resize(cnt[k]);
+            if (cnt[k] > 0)
+                CK(cudaMemcpyAsync(out[i0 + k].data(), jobs[k].out, 16 * (size_t)cnt[k], cudaMemcpyDeviceToHost,
+                                   s_of(ctx)));
+        }
+        CK(cudaStreamSynchronize(s_of(ctx)));
+        i0 = i1;
+    }
     return 0;
 }

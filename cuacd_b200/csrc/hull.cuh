@@ -37,7 +37,9 @@
 #define HULL_WQ       704                          // of which: node stack
 #define HULL_WL       (HULL_WSM - HULL_WQ)         //           kept-leaf list
 #define HULL_WRAP_DSMEM ((size_t)(HULL_NT / 32) * HULL_WSM * sizeof(int))
-#define HULL_SEEDS    1                            // seed faces (1..6) that start the wrapping
+#define HULL_SEEDS    1                            // seed faces (1..6) that start the wrapping; 6 seeds
+                                                   // measured slower (7.3 vs 6.4 ms hull stage, config 3):
+                                                   // their set-up costs more than the shorter chains save
 
 // Per-cloud scratch layout (bytes computed on the host by hull_scratch_bytes).
 struct HullCaps {

@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <functional>
+#include <vector>
 #include "common.cuh"
 
 struct CutResult;
@@ -33,8 +34,9 @@ void launch_components(const HDSurf* d_meshes, int n, Arena* scratch, Arena* out
 
 // concave.cu
 struct gpu_ctx;
-int concave_planes_device(gpu_ctx* ctx, const float* d_v, int nv, const int* d_t, int nt, int K, float eps,
-                          float thr, char* scr, size_t cap, float4* out_host, int* out_count, cudaStream_t s);
+int concave_planes_device_batch(gpu_ctx* ctx, int n, const float* const* d_v, const int* nv, const int* const* d_t,
+                                const int* nt, int K, float eps, float thr, char* scr, size_t cap,
+                                std::vector<std::vector<float4>>& out);
 
 // hull.cu
 struct HullJob;

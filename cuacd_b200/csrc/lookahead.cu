@@ -35,6 +35,7 @@
 // this engine and are ignored.
 #include <vector>
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -669,13 +670,27 @@ static int lookahead_impl(gpu_ctx_t ctx, const float* verts, int nv, const int* 
     std::vector<CutJob> jobs;
     std::vector<CutResult> cuts;
     std::vector<FragRes> frs;
+    // verbose >= 2: wall time per phase (the stream is drained at each mark)
+    double tph[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    auto tnow = [&]() { cudaStreamSynchronize(s); return std::chrono::steady_clock::now(); };
+    std::chrono::steady_clock::time_point tmark = std::chrono::steady_clock::now();
+    auto tacc = [&](int k) {
+        if (verbose < 2) return;
+        auto t = tnow();
+        tph[k] += std::chrono::duration<double>(t - tmark).count();
+        tmark = t;
+    };
+    int n_iters_run = 0;
     for (int iter = 0; iter < max_iters && result == 0; iter++) {
+        n_iters_run++;
+        tacc(7);
         // ---- 0. split parts made of several connected components
         //      (dc_pre_eval / dc_post_cuts, csrc/lookahead.c:329-347, :909-925)
         if (decompose_components_per_iter) {
             result = L.split_components(parts, unchecked(), cc_counter);
             if (result) break;
         }
+        tacc(0);
         // ---- 1. Hausdorff of parts below tau
         {
             std::vector<int> need;
@@ -721,26 +736,27 @@ static int lookahead_impl(gpu_ctx_t ctx, const float* verts, int nv, const int* 
         for (int i = 0; i < (int)order.size(); i++) if (full(order[i]) >= threshold) { first_above = i; break; }
         int start = std::max(first_above, (int)order.size() - max_n_cutting);
         for (int i = start; i < (int)order.size(); i++) if (full(order[i]) >= threshold) cutting.push_back(order[i]);
-        if (verbose) fprintf(stderr, "[la] iter %d: parts=%zu cutting=%zu\n", iter, parts.size(), cutting.size());
+        if (verbose == 1 || verbose >= 3) fprintf(stderr, "[la] iter %d: parts=%zu cutting=%zu\n", iter, parts.size(), cutting.size());
         if (cutting.empty()) break;
         const int nc = (int)cutting.size();
+        tacc(1);
         // ---- 3. concave-edge planes per cutting part
         std::vector<std::vector<float4>> eplanes(nc);
-        if (K > 0 && iter < concave_iters) {
+        if (K > 0 && iter < concave_iters) {      // all cutting parts in one launch
+            std::vector<const float*> pv(nc); std::vector<const int*> pt(nc);
+            std::vector<int> pnv(nc), pnt(nc);
             for (int c = 0; c < nc; c++) {
                 const HPart& p = parts[cutting[c]];
-                if (p.nt < 2) continue;
-                float4 pl[1024]; int cnt = 0;
-                rc = concave_planes_device(ctx, p.v, p.nv, p.t, p.nt, K, concave_eps, concave_threshold,
-                                           L.scr_base, L.scr_cap, pl, &cnt, s);
-                if (rc) { result = rc; break; }
-                eplanes[c].assign(pl, pl + cnt);
+                pv[c] = p.v; pt[c] = p.t; pnv[c] = p.nv; pnt[c] = p.nt;
             }
-            if (result) break;
+            rc = concave_planes_device_batch(ctx, nc, pv.data(), pnv.data(), pt.data(), pnt.data(), K, concave_eps,
+                                             concave_threshold, L.scr_base, L.scr_cap, eplanes);
+            if (rc) { result = rc; break; }
         }
         int n_edge = 0;
         for (auto& e : eplanes) n_edge = std::max(n_edge, (int)e.size());
         const int tw0 = width + n_edge;
+        tacc(2);
         // ---- 4. expansion levels
         std::vector<Item> cur, leaves, extra;
         for (int c = 0; c < nc; c++) {
@@ -781,10 +797,12 @@ static int lookahead_impl(gpu_ctx_t ctx, const float* verts, int nv, const int* 
             if (d == 0 && prune && prune->sc) {
                 result = prune_level0(ctx, L, *prune, cur, jobs, job_of, d_jobs, d_jplanes, d_jflags);
                 if (result) break;
+                tacc(3);
             }
             const bool last = d == depth - 1 && d > 0;
             int lr = last ? L.run_last_level(jobs, cuts, frs, d_jobs, d_cuts, d_frags)
                           : L.run_level(jobs, cuts, frs, d_jobs, d_cuts, d_frags);
+            tacc(d == 0 ? 4 : 5);
             if (lr) { result = ctx_fail(ctx, lr, "lookahead level %d failed at iter %d (0x%x)", d, iter, lr); break; }
             std::vector<Item> next;
             std::vector<bool> small_done(cur.size(), false);
@@ -877,6 +895,7 @@ static int lookahead_impl(gpu_ctx_t ctx, const float* verts, int nv, const int* 
             }
         }
         if (prune) { prune->tkey.clear(); prune->tfeat.clear(); }
+        tacc(6);
         // ---- 6. apply: the part becomes the two halves of its best level-0 item
         bool applied = false;
         std::vector<HPart> added;
@@ -908,6 +927,11 @@ static int lookahead_impl(gpu_ctx_t ctx, const float* verts, int nv, const int* 
         CK(cudaStreamSynchronize(s));
         if (!applied) break;
     }
+    tacc(7);
+    if (verbose >= 2)
+        fprintf(stderr, "[la] %d iterations, seconds: components %.4f hausdorff %.4f concave %.4f prune %.4f "
+                "level0 %.4f deeper %.4f bookkeeping %.4f apply %.4f\n", n_iters_run, tph[0], tph[1], tph[2],
+                tph[3], tph[4], tph[5], tph[6], tph[7]);
     // ---- post-pass components (csrc/lookahead.c:969-985); with the per-iteration
     //      pass on, only the pieces of the last iteration's cuts are left
     if (result == 0 && (decompose_components || decompose_components_per_iter))
