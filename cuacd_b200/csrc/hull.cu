@@ -4,35 +4,13 @@
 // output (one CTA per cloud).
 #include "context.cuh"
 #include "hull.cuh"
+#include "hull_kernels.cuh"
 #include "launch.h"
 
 __global__ void __launch_bounds__(HULL_NT)
 k_hull_setup(const HullJob* __restrict__ jobs, int n_jobs, Arena* scratch, HullState* states, int* ctl)
 {
-    __shared__ HullSetupShared sh;
-    __shared__ char* s_scr;
-    __shared__ int s_err;
-    const int j = blockIdx.x;
-    if (j >= n_jobs) return;
-    const HullJob J = jobs[j];
-    HullState* S = &states[j];
-    double mv = 0.0;
-    if (J.tris && J.nt > 0 && J.n > 0) mv = block_mesh_signed_volume(J.pts, J.n, J.tris, J.nt, sh.dsh);
-    if (threadIdx.x == 0) {
-        S->n = J.n; S->n_faces = 0; S->err = 0; S->active = 0; S->q_pending = 0;
-        for (int k = 0; k < 8; k++) { S->stats[k] = 0; S->fail[k] = 0; }
-        s_err = 0; s_scr = nullptr;
-        if (J.n >= 4) {
-            s_scr = (char*)arena_alloc(scratch, hull_scratch_bytes(J.n), &s_err);
-            if (!s_scr) S->err = s_err | KERR_BT_POOL_EXHAUST;
-        }
-    }
-    __syncthreads();
-    if (s_scr) hull_setup_cta(J.pts, J.n, s_scr, S, sh);
-    if (threadIdx.x == 0) {
-        S->mesh_vol = fabs(mv);
-        if (s_scr && S->active) atomicAdd(&ctl[0], 1);
-    }
+    hull_setup_body(jobs, n_jobs, scratch, states, ctl);
 }
 
 // Wrap-grid shares (one CTA): prefix of the active hulls' weights, a hull's
@@ -42,123 +20,21 @@ k_hull_setup(const HullJob* __restrict__ jobs, int n_jobs, Arena* scratch, HullS
 __global__ void __launch_bounds__(1024)
 k_hull_assign(HullState* states, int n_jobs, int n_ctas, long long* total)
 {
-    __shared__ long long part[1024 / 32];
-    __shared__ long long carry, s_sum, s_floor;
-    __shared__ int s_h;
-    if (threadIdx.x == 0) { carry = 0; s_sum = 0; s_h = 0; }
-    __syncthreads();
-    {
-        long long sn = 0; int h = 0;
-        for (int j = threadIdx.x; j < n_jobs; j += 1024)
-            if (states[j].active) { sn += states[j].n; h++; }
-        atomicAdd((unsigned long long*)&s_sum, (unsigned long long)sn);
-        atomicAdd(&s_h, h);
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) s_floor = n_ctas > s_h ? (s_sum + (n_ctas - s_h) - 1) / (n_ctas - s_h) : 0;
-    __syncthreads();
-    const long long floor_w = s_floor;
-    for (int base = 0; base < n_jobs; base += 1024) {
-        const int j = base + threadIdx.x;
-        long long w = (j < n_jobs && states[j].active) ? (long long)states[j].n + floor_w : 0;
-        long long x = w;                                  // inclusive warp scan
-        #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            long long y = __shfl_up_sync(FULL_MASK, x, o);
-            if ((threadIdx.x & 31) >= o) x += y;
-        }
-        if ((threadIdx.x & 31) == 31) part[threadIdx.x >> 5] = x;
-        __syncthreads();
-        if (threadIdx.x < 32) {
-            long long p = part[threadIdx.x], q = p;
-            #pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                long long y = __shfl_up_sync(FULL_MASK, q, o);
-                if (threadIdx.x >= o) q += y;
-            }
-            part[threadIdx.x] = q - p;                    // exclusive over warps
-        }
-        __syncthreads();
-        if (j < n_jobs) states[j].wbase = carry + part[threadIdx.x >> 5] + x - w;
-        __syncthreads();
-        if (threadIdx.x == 1023) carry += part[31] + x;
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) *total = carry;
+    hull_assign_body(states, n_jobs, n_ctas, total);
 }
 
 __global__ void __launch_bounds__(HULL_NT, 1)
 k_hull_wrap(HullState* states, int n_jobs, int* ctl, const long long* total, int* wbuf)
 {
-    __shared__ HullWrapShared sh;
     extern __shared__ int wsm_dyn[];                      // HULL_WRAP_DSMEM bytes
-    __shared__ int s_h0, s_go;
-    if (threadIdx.x == 0) {
-        // one reader decides for the whole CTA: other CTAs may finish the
-        // last hull while this one starts
-        s_go = *(volatile int*)&ctl[0] > 0;
-        // home hull: the active hull whose share holds this CTA's point
-        const long long W = *total;
-        const long long t = ((2LL * blockIdx.x + 1) * W) / (2LL * gridDim.x);
-        int lo = 0, hi = n_jobs - 1;
-        while (lo < hi) {                                 // last j with wbase[j] <= t
-            int mid = (lo + hi + 1) >> 1;
-            if (states[mid].wbase <= t) lo = mid; else hi = mid - 1;
-        }
-        s_h0 = lo;
-    }
-    __syncthreads();
-    if (!s_go) return;
-    hull_wrap_grid(states, n_jobs, s_h0, ctl, wbuf, sh, wsm_dyn);
+    hull_wrap_body(states, n_jobs, ctl, total, wbuf, wsm_dyn);
 }
 
 __global__ void __launch_bounds__(HULL_NT)
 k_hull_output(const HullJob* __restrict__ jobs, HullState* states, int n_jobs, Arena* out, const int* ctl,
               HullRes* res, unsigned long long* stats)
 {
-    __shared__ HullOutShared sh;
-    __shared__ float* s_ov;
-    __shared__ int* s_ot;
-    __shared__ int s_mhv, s_mht, s_aerr, s_nv, s_nt, s_oerr;
-    __shared__ float s_vol;
-    const int j = blockIdx.x;
-    if (j >= n_jobs) return;
-    const HullJob J = jobs[j];
-    HullState* S = &states[j];
-    if (threadIdx.x == 0) {
-        if (J.n >= 4 && S->active) atomicOr(&S->err, ctl[1] ? ctl[1] : KERR_TIMEOUT);   // not finished
-        s_aerr = 0;
-        s_ov = J.out_v; s_ot = J.out_t; s_mhv = J.max_hv; s_mht = J.max_ht;
-        if (!J.out_v && J.n >= 4 && S->err == 0) {
-            s_ov = (float*)arena_alloc(out, 12ull * J.n, &s_aerr);
-            s_ot = (int*)arena_alloc(out, 12ull * (2 * J.n + 4), &s_aerr);
-            s_mhv = J.n; s_mht = 2 * J.n + 4;
-        }
-        s_nv = 0; s_nt = 0; s_vol = 0.f; s_oerr = 0;
-    }
-    __syncthreads();
-    if (s_aerr) {
-        if (threadIdx.x == 0) { HullRes r; memset(&r, 0, sizeof(r)); r.mesh_vol = S->mesh_vol; r.err = s_aerr; res[j] = r; }
-        return;
-    }
-    hull_output_cta(J.pts, S, s_ov, s_ot, s_mhv, s_mht, &s_nv, &s_nt, &s_vol, &s_oerr, sh);
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        HullRes r;
-        r.hv = s_nv > 0 ? s_ov : nullptr; r.ht = s_nt > 0 ? s_ot : nullptr;
-        r.hnv = s_nv; r.hnt = s_nt;
-        r.mesh_vol = S->mesh_vol; r.hull_vol = s_vol;
-        r.err = s_oerr | S->err;
-        res[j] = r;
-    }
-    if (stats && threadIdx.x < 8) {
-        unsigned long long x = threadIdx.x == 2 ? (unsigned long long)S->n_faces : S->stats[threadIdx.x];
-        if (S->fail[0] && threadIdx.x >= 4) {       // failed hull: slots 4-7 hold the failure record
-            const int k = 2 * ((int)threadIdx.x - 4);
-            x = (unsigned long long)(unsigned)S->fail[k] | ((unsigned long long)(unsigned)S->fail[k + 1] << 32);
-        }
-        stats[8 * (size_t)j + threadIdx.x] = x;
-    }
+    hull_output_body(jobs, states, n_jobs, out, ctl, res, stats);
 }
 
 size_t hull_wrap_buf_bytes(int n_wrap_ctas)

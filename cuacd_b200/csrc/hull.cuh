@@ -1098,7 +1098,11 @@ static __device__ void hull_setup_cta(const float* __restrict__ pts, int n, char
 static __device__ __forceinline__ unsigned long long hull_now()
 {
     unsigned long long t;
+#ifdef __CUDA_ARCH__
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+#else
+    t = (unsigned long long)clock64();      // host builds of the device code (CPU emulation in the tests)
+#endif
     return t;
 }
 

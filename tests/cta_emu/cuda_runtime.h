@@ -160,3 +160,13 @@ template <class T> T atomicMax(T* p, T v)
 }
 template <class T> T atomicCAS(T* p, T c, T v) { std::atomic_ref<T>(*p).compare_exchange_strong(c, v); return c; }
 template <class T> T atomicExch(T* p, T v) { return std::atomic_ref<T>(*p).exchange(v); }
+
+// IEEE round-to-nearest float intrinsics: the host's float operations round
+// the same way when built with -ffp-contract=off.
+inline float __fdiv_rn(float a, float b) { return a / b; }
+inline float __fadd_rn(float a, float b) { return a + b; }
+inline float __fsub_rn(float a, float b) { return a - b; }
+inline float __fmul_rn(float a, float b) { return a * b; }
+inline int __float2int_rz(float x) { return (int)x; }
+template <class T> T __ldcg(const T* p) { return std::atomic_ref<T>(*const_cast<T*>(p)).load(); }
+template <class T> T atomicSub(T* p, T v) { return std::atomic_ref<T>(*p).fetch_sub(v); }

@@ -78,3 +78,56 @@ def test_ear_clipping_race_case(emu_cut, tmp_path, oracle):
     rows, reports = run(emu_cut, tmp_path, v, t, planes)
     assert not reports, reports[:5]
     check(oracle, v, t, planes, rows)
+
+
+@pytest.fixture(scope="module")
+def emu_hull(tmp_path_factory):
+    if shutil.which("g++") is None:
+        pytest.skip("g++ not available")
+    out = str(tmp_path_factory.mktemp("emuh") / "emu_hull")
+    r = subprocess.run(["g++", "-std=c++20", "-O2", "-pthread", "-ffp-contract=off", "-I", EMU,
+                        os.path.join(EMU, "emu_hull.cpp"), "-o", out], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-2000:]
+    return out
+
+
+def run_hulls(emu_hull, tmp_path, clouds):
+    path = str(tmp_path / "clouds.bin")
+    with open(path, "wb") as f:
+        np.array([len(clouds)] + [len(c) for c in clouds], np.int32).tofile(f)
+        for c in clouds:
+            np.ascontiguousarray(c, np.float32).tofile(f)
+    r = subprocess.run([emu_hull, path], capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0, r.stderr[-2000:]
+    reports = [l for l in r.stderr.splitlines() if l.startswith("[emu]")]
+    lines = r.stdout.splitlines()
+    out = []
+    for i in range(0, len(lines), 3):
+        h = lines[i].split()
+        err, nv, nt = int(h[3]), int(h[5]), int(h[7])
+        v = np.array(lines[i + 1].split(), np.float32).reshape(nv, 3)
+        t = np.array(lines[i + 2].split(), np.int32).reshape(nt, 3)
+        out.append((err, v, t))
+    return out, reports
+
+
+def test_hull_pipeline_emulated(emu_hull, tmp_path, oracle):
+    """The batched hull pipeline's set-up, wrap and output code (one wrap CTA
+    for every cloud) raises no divergent barrier or warp misuse and builds
+    the oracle's hulls: uniform clouds, a fragment of a cut (a large flat cap
+    face), flat leaves lying in faces, duplicated points and a grid with many
+    coplanar points."""
+    rng = np.random.default_rng(4)
+    v, t = W.candidate_mesh(32, 12, 0.35, seed=3)
+    frag = oracle.plane_cut(v, t, np.array([0.6, 0.0, 0.8, -0.2], np.float32))[0]
+    dup = rng.uniform(-1, 1, (200, 3)).astype(np.float32)
+    dup = np.concatenate([dup, dup[:40]])
+    g = np.stack(np.meshgrid(*[np.linspace(-1, 1, 6)] * 3), -1).reshape(-1, 3).astype(np.float32)
+    clouds = W.hull_clouds(3, 600, 0) + [frag, np.load(os.path.join(GOLDEN, "hull_flat_leaves.npy")), dup, g]
+    got, reports = run_hulls(emu_hull, tmp_path, clouds)
+    assert not reports, reports[:5]
+    for c, (err, hv, ht) in zip(clouds, got):
+        vi, tri, vol = oracle.hull(c)
+        assert err == 0
+        np.testing.assert_array_equal(hv, c[vi])
+        np.testing.assert_array_equal(ht, tri)
