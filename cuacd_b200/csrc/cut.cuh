@@ -136,15 +136,17 @@ static __device__ int cut_ear_clip_cta(const Cap2D& c, const int* poly, int n, d
         if (clip) {
             // Reflex steps and a degenerate ear meet no barrier, so a lagging
             // thread may still be reading nxt[]/prv[] of an earlier step of
-            // the walk (nxt[p] among them): wait before the links change, or
-            // it would follow another walk into another barrier.
-            __syncthreads();
-            if (tid == 0) {
-                cap[3 * nc] = poly[p]; cap[3 * nc + 1] = poly[cur]; cap[3 * nc + 2] = poly[q];
-                nxt[p] = q; prv[q] = p;
-            }
+            // the walk (nxt[p] among them): a degenerate ear waits before the
+            // links change, or that thread would follow another walk into
+            // another barrier (a tested ear already met __syncthreads_or).
+            // Every thread then writes the same two links itself, so its own
+            // next reads see them without a second barrier; no thread can
+            // write the next clip's links before all have met that clip's
+            // barrier.
+            if (cr <= 1e-9) __syncthreads();
+            if (tid == 0) { cap[3 * nc] = poly[p]; cap[3 * nc + 1] = poly[cur]; cap[3 * nc + 2] = poly[q]; }
+            nxt[p] = q; prv[q] = p;
             nc++;
-            __syncthreads();
             remaining--; cur = q; iter = 0;
         } else cur = q;
     }
