@@ -363,6 +363,29 @@ static __device__ int warp_wrap(const HullCtx& H, int u, int v, const WarpLists 
 // Points of the kept leaves lying on the plane through a with outward normal
 // N (all points satisfy N.(q-a) <= 0).  Leaves whose box stays below the
 // plane are skipped first.  Returns the count; the first `cap` ids go to W.S.
+// Does any point of the kept leaves lie on the plane (a, N) but off the line
+// through a with integer direction e?  (Whole warp; the answer is uniform.)
+static __device__ bool warp_any_off_line(const HullCtx& H, const WarpLists L, int nl, float4 a, double nx, double ny,
+                                         double nz, int ex, int ey, int ez, int lane, unsigned& n64)
+{
+    const float fx = (float)nx, fy = (float)ny, fz = (float)nz;
+    const int total = nl * HULL_LEAF;
+    bool any = false;
+    for (int base = 0; base < total && !any; base += 32) {
+        const int i = base + lane;
+        bool off = false;
+        if (i < total) {
+            const int p = L.leaf[i / HULL_LEAF] * HULL_LEAF + (i % HULL_LEAF);
+            if (p < H.m) {
+                const float4 q = H.pts[p];
+                off = plane_sign(nx, ny, nz, fx, fy, fz, a, q, n64) == 0 && !on_line(ex, ey, ez, a, q);
+            }
+        }
+        any = __any_sync(FULL_MASK, off);
+    }
+    return any;
+}
+
 static __device__ int warp_coplanar(const HullCtx& H, float4 a, double nx, double ny, double nz, HullWarp& W,
                                     const WarpLists L, int nl, int lane, int cap, unsigned& n_pts, unsigned& n64)
 {
@@ -1035,14 +1058,17 @@ static __device__ void hull_setup_cta(const float* __restrict__ pts, int n, char
                 nx = ey * dir[2] - ez * dir[1]; ny = ez * dir[0] - ex * dir[2]; nz = ex * dir[1] - ey * dir[0];
                 // collinear contact set? then wrap again about (p0, c)
                 const int ns = warp_coplanar(H, a, nx, ny, nz, sh.ws[sd], L, nl, lane, HULL_SMALL_S, st_cop, st_64);
+                // (a large contact set may still be collinear: duplicates of
+                // p0 or c, or points along the line)
+                const int ix = (int)ex, iy = (int)ey, iz = (int)ez;
                 int noncol = 0;
-                if (lane == 0) {
-                    noncol = ns > HULL_SMALL_S;
-                    const int ix = (int)ex, iy = (int)ey, iz = (int)ez;
-                    for (int i = 0; i < ns && i < HULL_SMALL_S && !noncol; i++)
-                        if (!on_line(ix, iy, iz, a, P4[sh.ws[sd].S[i]])) noncol = 1;
+                if (ns > HULL_SMALL_S) noncol = warp_any_off_line(H, L, nl, a, nx, ny, nz, ix, iy, iz, lane, st_64);
+                else {
+                    if (lane == 0)
+                        for (int i = 0; i < ns && !noncol; i++)
+                            if (!on_line(ix, iy, iz, a, P4[sh.ws[sd].S[i]])) noncol = 1;
+                    noncol = __shfl_sync(FULL_MASK, noncol, 0);
                 }
-                noncol = __shfl_sync(FULL_MASK, noncol, 0);
                 if (!noncol) {
                     const int c2 = warp_wrap(H, p0, c, L, lane, &nl, st_pts, st_64);
                     if (c2 < 0) ok = 0;

@@ -31,8 +31,9 @@
 // between waves.
 // The branch-and-bound pruning of the last level (la_hull's rough-hull bound)
 // only skips provably dominated items and is not needed for the result; the
-// quick levels (quick_depth) and the merge-hulls post-pass are not part of
-// this engine and are ignored.
+// quick levels (quick_depth) are not part of this engine and are ignored.
+// merge_hulls runs the merge-hulls post-pass (merge_hulls_pass) after the
+// last iteration.
 #include <vector>
 #include <algorithm>
 #include <chrono>
@@ -173,6 +174,143 @@ __global__ void k_mesh_volumes(const HDSurf* meshes, int n, double* out)
     if (i >= n) return;
     double v = block_mesh_signed_volume(meshes[i].v, meshes[i].nv, meshes[i].t, meshes[i].nt, sh);
     if (threadIdx.x == 0) out[i] = fabs(v);
+}
+
+// ---------------------------------------------------------------------------
+// merge-hulls post-pass kernels (cuda/postprocess_merge.cu:41-679)
+// ---------------------------------------------------------------------------
+// Axis-aligned box of every mesh: out[6i..6i+5] = min xyz, max xyz.
+__global__ void __launch_bounds__(256) k_mesh_boxes(const HDSurf* __restrict__ meshes, int n, float* out)
+{
+    __shared__ float red[6][8];
+    const int i = blockIdx.x;
+    if (i >= n) return;
+    const HDSurf M = meshes[i];
+    float l[3] = {1e30f, 1e30f, 1e30f}, h[3] = {-1e30f, -1e30f, -1e30f};
+    for (int v = threadIdx.x; v < M.nv; v += 256)
+        for (int k = 0; k < 3; k++) { const float x = M.v[3 * v + k]; l[k] = fminf(l[k], x); h[k] = fmaxf(h[k], x); }
+    for (int k = 0; k < 3; k++) { l[k] = warp_min(l[k]); h[k] = warp_max(h[k]); }
+    if ((threadIdx.x & 31) == 0) for (int k = 0; k < 3; k++) { red[k][threadIdx.x >> 5] = l[k]; red[3 + k][threadIdx.x >> 5] = h[k]; }
+    __syncthreads();
+    if (threadIdx.x < 6) {
+        const int k = threadIdx.x;
+        float r = k < 3 ? 1e30f : -1e30f;
+        for (int w = 0; w < 8; w++) r = k < 3 ? fminf(r, red[k][w]) : fmaxf(r, red[k][w]);
+        out[6 * i + k] = r;
+    }
+}
+
+// One merge candidate: parts a and b (meshes and hulls), where its buffers live.
+struct MergeJob {
+    const float* av; const int* at; int anv, ant;      // part a's mesh
+    const float* bv; const int* bt; int bnv, bnt;      // part b's mesh
+    const float* ahv; const int* aht; int ahnv, ahnt;  // hulls
+    const float* bhv; int bhnv;
+    float* cat_pts;                                    // ahnv + bhnv points (hull vertices of a, then b)
+    float* mv; int* mt;                                // concatenated mesh (filtered triangles)
+    int* mnt;                                          // filtered triangle count
+};
+
+// Hull vertices of a then b, one CTA per candidate.
+__global__ void __launch_bounds__(256) k_merge_cat_points(const MergeJob* __restrict__ jobs, int n)
+{
+    const int j = blockIdx.x;
+    if (j >= n) return;
+    const MergeJob J = jobs[j];
+    for (int i = threadIdx.x; i < 3 * J.ahnv; i += 256) J.cat_pts[i] = J.ahv[i];
+    for (int i = threadIdx.x; i < 3 * J.bhnv; i += 256) J.cat_pts[3 * J.ahnv + i] = J.bhv[i];
+}
+
+// The concatenated mesh of a and b for the merged part's Hausdorff test:
+// vertices of a then b; triangles of a then b (b's indices offset), minus
+// those whose three vertices lie within 1e-3 of the shared plane -- a face
+// plane of a's hull with every vertex of a's hull on or below it and every
+// vertex of b's hull on it (la_merge_find_shared_plane_warp, cuda/merge.cuh;
+// the lowest such face of a's hull, where the reference takes the first lane
+// to find one).  Triangles keep their input order.  One CTA per candidate.
+__global__ void __launch_bounds__(256) k_merge_cat_mesh(const MergeJob* __restrict__ jobs, int n)
+{
+    __shared__ int s_face;
+    __shared__ float4 s_plane;
+    __shared__ int scan[34];
+    const int j = blockIdx.x;
+    if (j >= n) return;
+    const MergeJob J = jobs[j];
+    const float tol = 1e-3f;
+    if (threadIdx.x == 0) s_face = 0x7fffffff;
+    __syncthreads();
+    for (int f = threadIdx.x; f < J.ahnt; f += 256) {
+        const int ia = J.aht[3 * f], ib = J.aht[3 * f + 1], ic = J.aht[3 * f + 2];
+        const float ax = J.ahv[3 * ia], ay = J.ahv[3 * ia + 1], az = J.ahv[3 * ia + 2];
+        const float e1x = J.ahv[3 * ib] - ax, e1y = J.ahv[3 * ib + 1] - ay, e1z = J.ahv[3 * ib + 2] - az;
+        const float e2x = J.ahv[3 * ic] - ax, e2y = J.ahv[3 * ic + 1] - ay, e2z = J.ahv[3 * ic + 2] - az;
+        float nx = e1y * e2z - e1z * e2y, ny = e1z * e2x - e1x * e2z, nz = e1x * e2y - e1y * e2x;
+        const float len = sqrtf(nx * nx + ny * ny + nz * nz);
+        if (len < 1e-20f) continue;
+        const float inv = 1.0f / len;
+        nx *= inv; ny *= inv; nz *= inv;
+        const float d = nx * ax + ny * ay + nz * az;
+        bool ok = true;
+        for (int k = 0; k < J.ahnv && ok; k++) ok = nx * J.ahv[3 * k] + ny * J.ahv[3 * k + 1] + nz * J.ahv[3 * k + 2] - d <= tol;
+        for (int k = 0; k < J.bhnv && ok; k++) ok = fabsf(nx * J.bhv[3 * k] + ny * J.bhv[3 * k + 1] + nz * J.bhv[3 * k + 2] - d) <= tol;
+        if (ok) { atomicMin(&s_face, f); }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && s_face != 0x7fffffff) {
+        const int f = s_face;
+        const int ia = J.aht[3 * f], ib = J.aht[3 * f + 1], ic = J.aht[3 * f + 2];
+        const float ax = J.ahv[3 * ia], ay = J.ahv[3 * ia + 1], az = J.ahv[3 * ia + 2];
+        const float e1x = J.ahv[3 * ib] - ax, e1y = J.ahv[3 * ib + 1] - ay, e1z = J.ahv[3 * ib + 2] - az;
+        const float e2x = J.ahv[3 * ic] - ax, e2y = J.ahv[3 * ic + 1] - ay, e2z = J.ahv[3 * ic + 2] - az;
+        float nx = e1y * e2z - e1z * e2y, ny = e1z * e2x - e1x * e2z, nz = e1x * e2y - e1y * e2x;
+        const float inv = 1.0f / sqrtf(nx * nx + ny * ny + nz * nz);
+        nx *= inv; ny *= inv; nz *= inv;
+        s_plane = make_float4(nx, ny, nz, nx * ax + ny * ay + nz * az);
+    }
+    __syncthreads();
+    const bool has_plane = s_face != 0x7fffffff;
+    const float4 P = s_plane;
+    for (int i = threadIdx.x; i < 3 * J.anv; i += 256) J.mv[i] = J.av[i];
+    for (int i = threadIdx.x; i < 3 * J.bnv; i += 256) J.mv[3 * J.anv + i] = J.bv[i];
+    // keep flags in input order, then an exclusive scan gives each kept triangle its slot
+    const int nt = J.ant + J.bnt;
+    int written = 0;
+    for (int base = 0; base < nt; base += 256) {
+        const int t = base + threadIdx.x;
+        int keep = 0, i0 = 0, i1 = 0, i2 = 0;
+        if (t < nt) {
+            const bool inb = t >= J.ant;
+            const float* V = inb ? J.bv : J.av;
+            const int* T = inb ? J.bt + 3 * (t - J.ant) : J.at + 3 * t;
+            i0 = T[0]; i1 = T[1]; i2 = T[2];
+            keep = 1;
+            if (has_plane) {
+                const float s0 = P.x * V[3 * i0] + P.y * V[3 * i0 + 1] + P.z * V[3 * i0 + 2] - P.w;
+                const float s1 = P.x * V[3 * i1] + P.y * V[3 * i1 + 1] + P.z * V[3 * i1 + 2] - P.w;
+                const float s2 = P.x * V[3 * i2] + P.y * V[3 * i2 + 1] + P.z * V[3 * i2 + 2] - P.w;
+                if (fabsf(s0) <= tol && fabsf(s1) <= tol && fabsf(s2) <= tol) keep = 0;
+            }
+            if (inb) { i0 += J.anv; i1 += J.anv; i2 += J.anv; }
+        }
+        int tot;
+        const int ex = block_exclusive_scan(keep, scan, &tot);
+        if (keep) { J.mt[3 * (written + ex)] = i0; J.mt[3 * (written + ex) + 1] = i1; J.mt[3 * (written + ex) + 2] = i2; }
+        written += tot;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *J.mnt = written;
+}
+
+// The merged part's mesh: vertices of a then b, triangles of a then b with
+// b's indices offset (la_merge_apply, cuda/postprocess_merge.cu:520-620).
+__global__ void __launch_bounds__(256) k_merge_concat(const float* av, const int* at, int anv, int ant, const float* bv,
+                                                      const int* bt, int bnv, int bnt, float* ov, int* ot)
+{
+    const int i = blockIdx.x * 256 + threadIdx.x;
+    if (i < 3 * anv) ov[i] = av[i];
+    if (i < 3 * bnv) ov[3 * anv + i] = bv[i];
+    if (i < 3 * ant) ot[i] = at[i];
+    if (i < 3 * bnt) ot[3 * ant + i] = bt[i] + anv;
 }
 
 // ---------------------------------------------------------------------------
@@ -478,6 +616,192 @@ extern "C" void gpu_result_free(struct gpu_result* r)
     r->parts = nullptr; r->nparts = 0;
 }
 
+// Merge-hulls post-pass (cuda/postprocess_merge.cu:41-679, driven as in
+// csrc/lookahead.c:987-1063).  For every pair of parts (p1 > p2) of the same
+// connected component: reject when the sum of their hull-minus-mesh gaps
+// already costs tau or more, or when their boxes are tau/2 or more apart;
+// else the exact hull of both hulls' vertices gives the merged rv cost, and
+// below tau the sampled Hausdorff distance between that hull and both meshes
+// (less the triangles lying in a shared face plane) raises it to
+// max(rv, H).  Then one greedy round: the cheapest pair below tau merges, its
+// two parts leave the pool, repeat; each merged part is both meshes
+// concatenated with the merged hull.  Costs use the reference's FP32 forms.
+static int merge_hulls_pass(gpu_ctx* ctx, Lookahead& L, std::vector<HPart>& parts, float tau, HDSurf* d_surfs,
+                            HDPrep* d_preps, char* d_dirs, int* d_i4, float* d_pmax)
+{
+    cudaStream_t s = L.s;
+    const int P = (int)parts.size();
+    const float pi_f = 3.14159265358979f;
+    auto rv_of = [&](float gap) { return 0.3f * cbrtf((3.0f / (4.0f * pi_f)) * gap); };
+    // boxes of every part's mesh
+    std::vector<float> box(6 * (size_t)P);
+    for (int b = 0; b < P; b += 1024) {                // d_pmax holds 8192 floats: 6 per part
+        const int m = std::min(1024, P - b);
+        std::vector<HDSurf> sf(m);
+        for (int k = 0; k < m; k++) sf[k] = {parts[b + k].v, parts[b + k].t, parts[b + k].nv, parts[b + k].nt};
+        CK(cudaMemcpyAsync(d_surfs, sf.data(), sizeof(HDSurf) * m, cudaMemcpyHostToDevice, s));
+        k_mesh_boxes<<<m, 256, 0, s>>>(d_surfs, m, d_pmax);
+        ctx->launches++;
+        CK(cudaMemcpyAsync(box.data() + 6 * (size_t)b, d_pmax, sizeof(float) * 6 * m, cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+    }
+    // candidates surviving the quick rejects (reference order of pair indices)
+    std::vector<std::pair<int, int>> cand;
+    for (int p1 = 1; p1 < P; p1++)
+        for (int p2 = 0; p2 < p1; p2++) {
+            const HPart& A = parts[p1]; const HPart& B = parts[p2];
+            if (A.cc_id != 0 && B.cc_id != 0 && A.cc_id != B.cc_id) continue;
+            const float msum = (float)A.mesh_vol + (float)B.mesh_vol;
+            if (rv_of(fmaxf((float)A.hull_vol + (float)B.hull_vol - msum, 0.0f)) >= tau) continue;
+            const float* a = &box[6 * (size_t)p1]; const float* b = &box[6 * (size_t)p2];
+            float g2 = 0.f;
+            for (int k = 0; k < 3; k++) { const float g = fmaxf(0.0f, fmaxf(a[k] - b[3 + k], b[k] - a[3 + k])); g2 += g * g; }
+            if (g2 >= (tau * 0.5f) * (tau * 0.5f)) continue;
+            cand.push_back({p1, p2});
+        }
+    std::vector<float> cost(cand.size(), 1e30f);
+    std::vector<FragRes> mres(cand.size());
+    L.reset_out();                                   // the search's fragments are no longer needed
+    const int CH = std::min(2048, L.frag_cap);
+    for (size_t c0 = 0; c0 < cand.size(); c0 += CH) {
+        const int m = (int)std::min<size_t>(CH, cand.size() - c0);
+        // device buffers for this chunk
+        size_t pts = 0, mv = 0, mt = 0;
+        for (int k = 0; k < m; k++) {
+            const HPart& A = parts[cand[c0 + k].first]; const HPart& B = parts[cand[c0 + k].second];
+            pts += 3 * (size_t)(A.hnv + B.hnv); mv += 3 * (size_t)(A.nv + B.nv); mt += 3 * (size_t)(A.nt + B.nt);
+        }
+        char* blk = nullptr;
+        const size_t bj = al256(sizeof(MergeJob) * m), bp = al256(4 * pts), bv = al256(4 * mv), bt = al256(4 * mt);
+        const size_t bn = al256(4 * (size_t)m);
+        CK(cudaMallocAsync((void**)&blk, bj + bp + bv + bt + bn, s));
+        MergeJob* d_jobs = (MergeJob*)blk;
+        float* d_pts = (float*)(blk + bj); float* d_mv = (float*)(blk + bj + bp); int* d_mt = (int*)(blk + bj + bp + bv);
+        int* d_mnt = (int*)(blk + bj + bp + bv + bt);
+        std::vector<MergeJob> jobs(m);
+        std::vector<HullJob> hj(m);
+        std::vector<int> sizes(m);
+        size_t op = 0, ov = 0, ot = 0;
+        for (int k = 0; k < m; k++) {
+            const HPart& A = parts[cand[c0 + k].first]; const HPart& B = parts[cand[c0 + k].second];
+            MergeJob& J = jobs[k];
+            J.av = A.v; J.at = A.t; J.anv = A.nv; J.ant = A.nt;
+            J.bv = B.v; J.bt = B.t; J.bnv = B.nv; J.bnt = B.nt;
+            J.ahv = A.hv; J.aht = A.ht; J.ahnv = A.hnv; J.ahnt = A.hnt;
+            J.bhv = B.hv; J.bhnv = B.hnv;
+            J.cat_pts = d_pts + op; J.mv = d_mv + ov; J.mt = d_mt + ot; J.mnt = d_mnt + k;
+            HullJob& H = hj[k];
+            memset(&H, 0, sizeof(H));
+            H.pts = J.cat_pts; H.n = A.hnv + B.hnv;
+            sizes[k] = H.n;
+            op += 3 * (size_t)(A.hnv + B.hnv); ov += 3 * (size_t)(A.nv + B.nv); ot += 3 * (size_t)(A.nt + B.nt);
+        }
+        CK(cudaMemcpyAsync(d_jobs, jobs.data(), sizeof(MergeJob) * m, cudaMemcpyHostToDevice, s));
+        k_merge_cat_points<<<m, 256, 0, s>>>(d_jobs, m);
+        CK(cudaMemcpyAsync(L.d_hjobs, hj.data(), sizeof(HullJob) * m, cudaMemcpyHostToDevice, s));
+        ctx->launches++;
+        int rh = L.run_hulls(sizes, L.d_frags);
+        if (rh) { cudaFreeAsync(blk, s); return rh; }
+        std::vector<FragRes> fr(m);
+        CK(cudaMemcpyAsync(fr.data(), L.d_frags, sizeof(FragRes) * m, cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        std::vector<int> hd_idx;                        // candidates that go on to the Hausdorff test
+        for (int k = 0; k < m; k++) {
+            const HPart& A = parts[cand[c0 + k].first]; const HPart& B = parts[cand[c0 + k].second];
+            mres[c0 + k] = fr[k];
+            if (fr[k].err || fr[k].hnt == 0) { if (fr[k].err & (KERR_HEAP_OOM | KERR_BT_POOL_EXHAUST)) { cudaFreeAsync(blk, s); return ctx_fail(ctx, KERR_HEAP_OOM, "merge hulls: pool exhausted"); } continue; }
+            const float msum = (float)A.mesh_vol + (float)B.mesh_vol;
+            const float rv = rv_of(fmaxf(fr[k].hull_vol - msum, 0.0f));
+            cost[c0 + k] = rv;
+            if (rv < tau) hd_idx.push_back(k);
+        }
+        if (!hd_idx.empty()) {
+            k_merge_cat_mesh<<<m, 256, 0, s>>>(d_jobs, m);
+            ctx->launches++;
+            std::vector<int> mnt(m);
+            CK(cudaMemcpyAsync(mnt.data(), d_mnt, sizeof(int) * m, cudaMemcpyDeviceToHost, s));
+            CK(cudaStreamSynchronize(s));
+            std::vector<int> keep;                      // no triangle left: Hausdorff 0 (reference)
+            for (int k : hd_idx) if (mnt[k] > 0) keep.push_back(k);
+            hd_idx.swap(keep);
+            for (size_t b = 0; b < hd_idx.size(); b += 4096) {
+                const int q = (int)std::min<size_t>(4096, hd_idx.size() - b);
+                std::vector<HDSurf> sf(2 * q);
+                std::vector<int> with(q, 1);
+                for (int r = 0; r < q; r++) {
+                    const int k = hd_idx[b + r];
+                    const MergeJob& J = jobs[k];
+                    sf[2 * r] = {fr[k].hv, fr[k].ht, fr[k].hnv, fr[k].hnt};
+                    sf[2 * r + 1] = {J.mv, J.mt, J.anv + J.bnv, mnt[k]};
+                }
+                CK(cudaMemcpyAsync(d_surfs, sf.data(), sizeof(HDSurf) * 2 * q, cudaMemcpyHostToDevice, s));
+                CK(cudaMemsetAsync(d_i4, 0, 16 * sizeof(int), s));
+                L.reset_scr();
+                launch_hausdorff_pairs(d_surfs, q, L.d_scr, 2000.f, 1000, 0, d_preps, d_dirs, d_i4, d_pmax, d_i4 + 2,
+                                       ctx->n_sm, s);
+                launch_hd_sqrt(d_pmax, q, d_pmax + 4096, 1, s);
+                ctx->launches += 5;
+                std::vector<float> h(q);
+                int herr = 0;
+                CK(cudaMemcpyAsync(h.data(), d_pmax + 4096, sizeof(float) * q, cudaMemcpyDeviceToHost, s));
+                CK(cudaMemcpyAsync(&herr, d_i4 + 2, sizeof(int), cudaMemcpyDeviceToHost, s));
+                CK(cudaStreamSynchronize(s));
+                if (herr) { cudaFreeAsync(blk, s); return ctx_fail(ctx, herr, "merge hulls: Hausdorff failed (0x%x)", herr); }
+                for (int r = 0; r < q; r++) {
+                    const int k = hd_idx[b + r];
+                    if (with[r]) cost[c0 + k] = fmaxf(cost[c0 + k], h[r]);
+                }
+            }
+        }
+        // merged hulls of pairs that may still merge stay in the output arena;
+        // the chunk's own buffers go
+        CK(cudaFreeAsync(blk, s));
+    }
+    // greedy matching: cheapest pair below tau first (ties: lower pair index)
+    std::vector<int> order;
+    for (size_t k = 0; k < cand.size(); k++) if (cost[k] < tau) order.push_back((int)k);
+    auto pair_index = [&](int k) { const int p1 = cand[k].first, p2 = cand[k].second; return (long long)p1 * (p1 - 1) / 2 + p2; };
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+        return cost[a] < cost[b] || (cost[a] == cost[b] && pair_index(a) < pair_index(b));
+    });
+    std::vector<char> used(P, 0), dead(P, 0);
+    for (int k : order) {
+        const int p1 = cand[k].first, p2 = cand[k].second;
+        if (used[p1] || used[p2]) continue;
+        used[p1] = used[p2] = 1;
+        const HPart A = parts[p1], B = parts[p2];
+        const FragRes& H = mres[k];
+        HPart M;
+        const int nv = A.nv + B.nv, nt = A.nt + B.nt;
+        const size_t b0 = al256(12 * (size_t)nv), b1 = al256(12 * (size_t)nt), b2 = al256(12 * (size_t)H.hnv);
+        const size_t b3 = al256(12 * (size_t)H.hnt);
+        char* blk = nullptr;
+        CK(cudaMallocAsync((void**)&blk, b0 + b1 + b2 + b3 + 256, s));
+        M.block = blk;
+        M.v = (float*)blk; M.t = (int*)(blk + b0); M.hv = (float*)(blk + b0 + b1); M.ht = (int*)(blk + b0 + b1 + b2);
+        M.nv = nv; M.nt = nt; M.hnv = H.hnv; M.hnt = H.hnt;
+        const int big = 3 * std::max(std::max(A.nv, B.nv), std::max(A.nt, B.nt));
+        k_merge_concat<<<(big + 255) / 256, 256, 0, s>>>(A.v, A.t, A.nv, A.nt, B.v, B.t, B.nv, B.nt, M.v, M.t);
+        ctx->launches++;
+        CK(cudaMemcpyAsync(M.hv, H.hv, 12 * (size_t)H.hnv, cudaMemcpyDeviceToDevice, s));
+        CK(cudaMemcpyAsync(M.ht, H.ht, 12 * (size_t)H.hnt, cudaMemcpyDeviceToDevice, s));
+        M.mesh_vol = (double)((float)A.mesh_vol + (float)B.mesh_vol);
+        M.hull_vol = H.hull_vol;
+        M.hd = 0.0;                                    // la_merge_apply resets it
+        M.cc_id = A.cc_id ? A.cc_id : B.cc_id;
+        M.checked = true;
+        L.free_part(parts[p1]);
+        L.free_part(parts[p2]);
+        parts[p1] = M;
+        dead[p2] = 1;
+    }
+    std::vector<HPart> kept;
+    for (int i = 0; i < P; i++) if (!dead[i]) kept.push_back(parts[i]);
+    parts.swap(kept);
+    CK(cudaStreamSynchronize(s));
+    return 0;
+}
+
 struct Prune;
 static int prune_level0(gpu_ctx* ctx, Lookahead& L, const Prune& P, const std::vector<Item>& cur,
                         std::vector<CutJob>& jobs, std::vector<std::pair<int, int>>& job_of, CutJob* d_jobs,
@@ -568,7 +892,7 @@ static int lookahead_impl(gpu_ctx_t ctx, const float* verts, int nv, const int* 
                           int depth, int max_n_cutting, int verbose, int debug, int decompose_components,
                           int decompose_components_per_iter,
                           int n_concave_edges, float concave_eps, float concave_threshold,
-                          int concave_iters, const Prune* prune, struct gpu_result* out)
+                          int concave_iters, int merge_hulls, const Prune* prune, struct gpu_result* out)
 {
     if (!ctx || !out) return -1;
     out->parts = nullptr; out->nparts = 0;
@@ -936,6 +1260,10 @@ static int lookahead_impl(gpu_ctx_t ctx, const float* verts, int nv, const int* 
     //      pass on, only the pieces of the last iteration's cuts are left
     if (result == 0 && (decompose_components || decompose_components_per_iter))
         result = L.split_components(parts, unchecked(), cc_counter);
+    // ---- merge-hulls post-pass (csrc/lookahead.c:987-1063, cuda/postprocess_merge.cu:41-679):
+    //      one greedy round of pairwise merges whose merged cost stays below tau
+    if (result == 0 && merge_hulls && parts.size() >= 2)
+        result = merge_hulls_pass(ctx, L, parts, threshold, d_surfs, d_preps, d_dirs, d_i4, d_pmax);
     // ---- results (host copies)
     if (result == 0) {
         out->parts = (gpu_part_result*)calloc(parts.size() > 0 ? parts.size() : 1, sizeof(gpu_part_result));
@@ -975,7 +1303,7 @@ extern "C" int lookahead_decompose(gpu_ctx_t ctx, const float* verts, int nv, co
     return lookahead_impl(ctx, verts, nv, tris, nt, hull_verts, hull_nv, hull_tris, hull_nt, max_iters, width, width2,
                           threshold, depth, max_n_cutting, verbose, debug, decompose_components,
                           decompose_components_per_iter, n_concave_edges, concave_eps, concave_threshold,
-                          concave_iters, nullptr, out);
+                          concave_iters, merge_hulls, nullptr, out);
 }
 
 extern "C" int cuacd_lookahead_decompose_pruned(gpu_ctx_t ctx, cuacd_scorer_t scorer, int top_k, float margin,
@@ -994,7 +1322,7 @@ extern "C" int cuacd_lookahead_decompose_pruned(gpu_ctx_t ctx, cuacd_scorer_t sc
     int rc = lookahead_impl(ctx, verts, nv, tris, nt, hull_verts, hull_nv, hull_tris, hull_nt, max_iters, width,
                             width2, threshold, depth, max_n_cutting, verbose, 0, decompose_components,
                             decompose_components_per_iter, n_concave_edges, concave_eps, concave_threshold,
-                            concave_iters, &P, out);
+                            concave_iters, 0, &P, out);
     if (out_stats) for (int k = 0; k < 3; k++) out_stats[k] = st[k];
     return rc;
 }
@@ -1015,7 +1343,7 @@ extern "C" int cuacd_lookahead_trace(gpu_ctx_t ctx, cuacd_scorer_t scorer, float
     Prune P{scorer, 0, 0.f, 0, st, &rows, (size_t)max_rows * W, 0, {}, {}};
     int rc = lookahead_impl(ctx, verts, nv, tris, nt, hull_verts, hull_nv, hull_tris, hull_nt, max_iters, width,
                             width2, threshold, depth, max_n_cutting, 0, 0, 0, 1, n_concave_edges, concave_eps,
-                            concave_threshold, concave_iters, &P, out);
+                            concave_threshold, concave_iters, 0, &P, out);
     if (rc) return rc;
     const int n = (int)(rows.size() / W);
     memcpy(out_rows, rows.data(), sizeof(float) * (size_t)n * W);

@@ -338,7 +338,9 @@ struct gpu_result {
 /* Replaces gpu_result_free (csrc/heap.h:85). */
 void gpu_result_free(struct gpu_result* result);
 
-/* Replaces lookahead_decompose (csrc/lookahead.h:28-43). */
+/* Replaces lookahead_decompose (csrc/lookahead.h:28-43).  quick_depth is
+ * accepted and ignored; merge_hulls runs the merge-hulls post-pass
+ * (cuda/postprocess_merge.cu:41-679). */
 int lookahead_decompose(gpu_ctx_t ctx,
                         const float* verts, int nv, const int* tris, int nt,
                         const float* hull_verts, int hull_nv,

@@ -115,15 +115,18 @@ def test_hull_pipeline_emulated(emu_hull, tmp_path, oracle):
     """The batched hull pipeline's set-up, wrap and output code (one wrap CTA
     for every cloud) raises no divergent barrier or warp misuse and builds
     the oracle's hulls: uniform clouds, a fragment of a cut (a large flat cap
-    face), flat leaves lying in faces, duplicated points and a grid with many
-    coplanar points."""
+    face), flat leaves lying in faces, duplicated points, a grid with many
+    coplanar points, and clouds with 34 points on their lexicographic minimum
+    (a collinear first contact set)."""
     rng = np.random.default_rng(4)
     v, t = W.candidate_mesh(32, 12, 0.35, seed=3)
     frag = oracle.plane_cut(v, t, np.array([0.6, 0.0, 0.8, -0.2], np.float32))[0]
     dup = rng.uniform(-1, 1, (200, 3)).astype(np.float32)
     dup = np.concatenate([dup, dup[:40]])
     g = np.stack(np.meshgrid(*[np.linspace(-1, 1, 6)] * 3), -1).reshape(-1, 3).astype(np.float32)
-    clouds = W.hull_clouds(3, 600, 0) + [frag, np.load(os.path.join(GOLDEN, "hull_flat_leaves.npy")), dup, g]
+    dc = np.load(os.path.join(GOLDEN, "hull_dup_corner.npz"))
+    clouds = W.hull_clouds(3, 600, 0) + [frag, np.load(os.path.join(GOLDEN, "hull_flat_leaves.npy")), dup, g,
+                                         dc["c0"], dc["c1"]]
     got, reports = run_hulls(emu_hull, tmp_path, clouds)
     assert not reports, reports[:5]
     for c, (err, hv, ht) in zip(clouds, got):

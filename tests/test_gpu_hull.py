@@ -93,3 +93,13 @@ def test_flat_leaves_in_face_plane(ctx, oracle):
     _check_exact(oracle, clouds, gpu)
     vol, err = ctx.batch_hull_volume(clouds)
     assert not err.any()
+
+
+def test_duplicated_extreme_point(ctx, oracle):
+    """Two part clouds of a search (355 and 390 points) where 34 points
+    quantise onto the lexicographic minimum, so the first seed's contact set
+    is more than 24 points on one line: the seed must wrap again instead of
+    taking them for a face (the hull came out empty, with no error)."""
+    g = np.load(os.path.join(GOLDEN, "hull_dup_corner.npz"))
+    clouds = [g["c0"], g["c1"]]
+    _check_exact(oracle, clouds, _gpu_hulls(ctx, clouds))

@@ -115,3 +115,31 @@ def test_beam_only_search(ctx):
     ranked, cut, expanded = ctx.last_prune_stats
     assert ranked == 0 and cut == 0 and expanded > 0
     assert max(_rv_costs(pp)) < 0.05
+
+
+def test_merge_hulls_pass(ctx, oracle):
+    """merge_hulls (cuda/postprocess_merge.cu): one greedy round of pairwise
+    merges.  Fewer parts, the same total volume, every merged part below tau,
+    and each merged part's hull is the exact hull of its vertices."""
+    v, t = W.candidate_mesh(64, 24)
+    kw = dict(width=30, width2=5, depth=2, threshold=0.05, n_concave_edges=16)
+    plain = ctx.lookahead_decompose(v, t, **kw)
+    merged = ctx.lookahead_decompose(v, t, merge_hulls=True, **kw)
+    assert len(merged) < len(plain)
+    total = oracle.mesh_volume(v, t)
+    assert abs(sum(oracle.mesh_volume(pv, pt) for pv, pt, _, _ in merged) - total) / total < 1e-4
+    plain_keys = {(len(pv), len(pt)) for pv, pt, _, _ in plain}
+    n_new = 0
+    for pv, pt, hv, ht in merged:
+        assert is_watertight(pt)
+        vi, tri, hvol = oracle.hull(pv)
+        if (len(pv), len(pt)) in plain_keys:         # untouched part: its own exact hull
+            np.testing.assert_array_equal(np.unique(hv, axis=0), np.unique(pv[vi], axis=0))
+        else:
+            # merged part: the hull of both parts' hull vertices (each found on
+            # its own part's quantisation grid), so corners that only the
+            # merged grid resolves may be missing; the volume agrees
+            n_new += 1
+            assert len(hv) > 0 and abs(oracle.mesh_volume(hv, ht) - hvol) <= 1e-3 * hvol
+            assert max(_rv_costs([(pv, pt, hv, ht)])) < 0.05
+    assert n_new == len(plain) - len(merged)
