@@ -28,7 +28,7 @@
 #include "common.cuh"
 #include "cta_util.cuh"
 
-#define CUT_NT  256
+#define CUT_NT  512
 #define CUT_EPS 1e-6f
 
 struct CutResult {
@@ -179,26 +179,66 @@ static __device__ int cut_build_caps(const float* V, int n_all, const unsigned l
         else if (ay >= az)        { C.pu = 0; C.pv = 2; }
         else                      { C.pu = 0; C.pv = 1; }
     }
+    // Loops, orientation and nesting are serial decisions of thread 0.  When
+    // the boundary fits the ear-clipping arrays (nb <= CUT_EAR_SM) they are
+    // borrowed first: the CTA stages each edge's start-vertex coordinates
+    // (s_U/s_W), the first edge leaving its end vertex (s_nxt) and a used
+    // flag (s_prv), so thread 0 walks shared memory instead of binary
+    // searches and scattered vertex loads; le[k] (in `used`) is the edge
+    // whose start vertex is lv[k] (shared memory: thread 0 would otherwise
+    // wait on L2 for every element it has just written).  Same values, same
+    // order: same result.
+    const bool fast = nb <= CUT_EAR_SM;
+    __shared__ int s_le[CUT_EAR_SM];
+    int* le = fast ? s_le : used;
+    if (fast) {
+        for (int i = tid; i < nb; i += CUT_NT) {
+            const int a = (int)(be[i] >> 32), b = (int)(be[i] & 0xffffffffu);
+            s_U[i] = (a >= 0 && a < n_all) ? cU(C, a) : 0.0;
+            s_W[i] = (a >= 0 && a < n_all) ? cW(C, a) : 0.0;
+            s_nxt[i] = lower_bound_u64(be, nb, (unsigned long long)(unsigned)b << 32);
+            s_prv[i] = 0;
+        }
+        __syncthreads();
+    }
+    auto LU = [&](int k) -> double { return fast ? s_U[le[k]] : cU(C, lv[k]); };
+    auto LW = [&](int k) -> double { return fast ? s_W[le[k]] : cW(C, lv[k]); };
+    auto loop_area = [&](int start, int m) -> double {      // cut_signed_area of lv[start .. start+m)
+        double a = 0.0;
+        for (int i = 0; i < m; i++) {
+            const int j = (i + 1) % m;
+            a += LU(start + i) * LW(start + j) - LU(start + j) * LW(start + i);
+        }
+        return a * 0.5;
+    };
+    auto loop_reverse = [&](int start, int m) { cut_reverse(lv + start, m); if (fast) cut_reverse(le + start, m); };
     int n_loops = 0, fail = 0;
     if (tid == 0) {
         int lvi = 0;
-        for (int i = 0; i < nb; i++) used[i] = 0;
+        if (!fast) for (int i = 0; i < nb; i++) used[i] = 0;
         for (int st = 0; st < nb && !fail; st++) {
-            if (used[st]) continue;
+            if (fast ? s_prv[st] : used[st]) continue;
             int first = (int)(be[st] >> 32), cur = (int)(be[st] & 0xffffffffu);
             if (first < 0 || first >= n_all || cur < 0 || cur >= n_all) { fail = 1; break; }
-            used[st] = 1;
+            int ce = st;
+            if (fast) { s_prv[st] = 1; le[lvi] = st; } else used[st] = 1;
             int start = lvi;
             lv[lvi++] = first;
             int guard = nb + 2;
             while (cur != first && guard-- > 0) {
                 if (lvi >= nb) { fail = 1; break; }
-                lv[lvi++] = cur;
-                int lo = lower_bound_u64(be, nb, (unsigned long long)(unsigned)cur << 32);
+                lv[lvi] = cur;
                 int found = -1;
-                for (int k = lo; k < nb && (int)(be[k] >> 32) == cur; k++) if (!used[k]) { found = k; break; }
+                if (fast) {
+                    for (int k = s_nxt[ce]; k < nb && (int)(be[k] >> 32) == cur; k++) if (!s_prv[k]) { found = k; break; }
+                } else {
+                    int lo = lower_bound_u64(be, nb, (unsigned long long)(unsigned)cur << 32);
+                    for (int k = lo; k < nb && (int)(be[k] >> 32) == cur; k++) if (!used[k]) { found = k; break; }
+                }
                 if (found < 0) { fail = 1; break; }
-                used[found] = 1;
+                if (fast) { s_prv[found] = 1; le[lvi] = found; } else used[found] = 1;
+                lvi++;
+                ce = found;
                 cur = (int)(be[found] & 0xffffffffu);
             }
             if (fail || cur != first) { fail = 1; break; }
@@ -217,27 +257,26 @@ static __device__ int cut_build_caps(const float* V, int n_all, const unsigned l
     int n_cap = 0;
     if (tid == 0) {
         for (int i = 0; i < n_loops; i++)
-            if (cut_signed_area(C, lv + ls[i], lsz[i]) < 0) cut_reverse(lv + ls[i], lsz[i]);
+            if (loop_area(ls[i], lsz[i]) < 0) loop_reverse(ls[i], lsz[i]);
         for (int i = 0; i < n_loops; i++) { parent[i] = -1; is_hole[i] = 0; }
         for (int i = 0; i < n_loops; i++) {
             if (lsz[i] < 3) continue;
-            int vi = lv[ls[i]];
-            double pu_ = cU(C, vi), pv_ = cW(C, vi);
+            double pu_ = LU(ls[i]), pv_ = LW(ls[i]);
             double best_area = 1e300;
             for (int j = 0; j < n_loops; j++) {
                 if (j == i || lsz[j] < 3) continue;
-                const int* lp = lv + ls[j];
+                const int lp = ls[j];
                 int m = lsz[j], crossings = 0;
                 for (int k = 0; k < m; k++) {
                     int kn = (k + 1) % m;
-                    double ay = cW(C, lp[k]), by = cW(C, lp[kn]);
+                    double ay = LW(lp + k), by = LW(lp + kn);
                     if ((ay <= pv_) == (by <= pv_)) continue;
-                    double ax = cU(C, lp[k]), bx = cU(C, lp[kn]);
+                    double ax = LU(lp + k), bx = LU(lp + kn);
                     double t = (pv_ - ay) / (by - ay);
                     if (ax + t * (bx - ax) > pu_) crossings++;
                 }
                 if (crossings & 1) {
-                    double a = fabs(cut_signed_area(C, lp, m));
+                    double a = fabs(loop_area(lp, m));
                     if (a < best_area) { best_area = a; parent[i] = j; }
                 }
             }
@@ -253,7 +292,7 @@ static __device__ int cut_build_caps(const float* V, int n_all, const unsigned l
                 is_hole[i] = depth & 1;
                 if (!is_hole[i] && depth >= 2) parent[i] = -1;
             }
-            for (int i = 0; i < n_loops; i++) if (is_hole[i]) cut_reverse(lv + ls[i], lsz[i]);
+            for (int i = 0; i < n_loops; i++) if (is_hole[i]) loop_reverse(ls[i], lsz[i]);
         }
         s_fail = fail;
     }
@@ -264,9 +303,13 @@ static __device__ int cut_build_caps(const float* V, int n_all, const unsigned l
     for (int oi = 0; oi < n_loops; oi++) {
         if (is_hole[oi] || lsz[oi] < 3) continue;
         int pn = 0;
+        {                                                    // the outer loop, copied by the CTA
+            const int o = ls[oi], m = lsz[oi];
+            for (int i = tid; i < m; i += CUT_NT) poly[i] = lv[o + i];
+            __syncthreads();
+        }
         if (tid == 0) {
             pn = lsz[oi];
-            for (int i = 0; i < pn; i++) poly[i] = lv[ls[oi] + i];
             int nin = 0;
             for (int i = 0; i < n_loops && nin < 128; i++) {
                 if (parent[i] != oi || lsz[i] < 3) continue;
