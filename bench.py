@@ -27,6 +27,7 @@ roofline dominant kernel's algorithmic bytes / its CUDA-event duration.
 search   whole lookahead searches on six ridged spheres through the host API:
          meshes/s exact vs pruned (learned level-0 ranking + exact beam),
          part counts and the largest part cost of each.
+config4  the same on a 64-mesh sample of config 4's uneven batch.
 N > 1 runs independent replicas (the path does not shard across GPUs).
 """
 import argparse
@@ -196,6 +197,29 @@ def search_leg(ctx, scorer, untrained):
     out["parts_ratio"] = out["pruned"]["parts"] / max(out["exact"]["parts"], 1)
     out["workload"] = (f"{len(meshes)} ridged displaced spheres (3,072-20,480 tris), tau 0.05, width 30/5, "
                        f"depth 2, 32 concave edges; pruned = learned top-{SEARCH_TOP_K} + beam {SEARCH_BEAM}")
+    return out
+
+
+def config4_leg(ctx, scorer):
+    """Config 4 sample: the 64 meshes with index 0 or 5 mod 16 of the 512
+    uneven synthetic meshes (500 to 200,000 triangles; displaced icospheres
+    and unions of 2-6 boxes, seed 3), whole searches with config 4's
+    parameters (tau 0.05, width 30/5, depth 2, 16 concave edges), exact and
+    pruned; one untimed pass first."""
+    from cuacd_b200 import workloads as W
+    meshes = W.batch_meshes(512, 500, 200_000, seed=3, select={i for i in range(512) if i % 16 in (0, 5)})
+    kw = dict(width=30, width2=5, depth=2, threshold=0.05, max_iters=100, n_concave_edges=16)
+    out = {}
+    for name, extra in (("exact", {}), ("pruned", {"scorer": scorer, "top_k": SEARCH_TOP_K, "beam": SEARCH_BEAM})):
+        for v, t in meshes:
+            ctx.lookahead_decompose(v, t, **kw, **extra)
+        t0 = time.perf_counter()
+        parts = [ctx.lookahead_decompose(v, t, **kw, **extra) for v, t in meshes]
+        dt = time.perf_counter() - t0
+        out[name] = {"meshes_per_s": len(meshes) / dt, "s": dt, "parts": int(sum(len(p) for p in parts)),
+                     "max_rv_cost": float(max(part_cost_max(p) for p in parts))}
+    out["workload"] = (f"config 4 sample: {len(meshes)} of the 512 meshes (index 0 or 5 mod 16), "
+                       f"{min(len(t) for _, t in meshes)}-{max(len(t) for _, t in meshes)} tris")
     return out
 
 
@@ -482,6 +506,7 @@ def main():
     if not args.no_search:
         with S.Scorer.load(ctx, S.RV_WEIGHTS_PATH) as rv, S.Scorer(ctx, seed=1) as raw:
             line["search"] = search_leg(ctx, rv, raw)
+            line["config4"] = config4_leg(ctx, rv)
     if rank == 0 and world_n == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(v, t, planes)
     if rank == 0:

@@ -180,9 +180,8 @@ def candidate_mesh(n_lon=256, n_rings=80, amplitude=0.35, seed=2):
     return normalize_extent(v).astype(np.float32), t
 
 
-def random_boxes_mesh(n_boxes, target_tris, rng):
-    """Union of n_boxes disjoint random boxes (rejection sampled in [-1,1]^3)
-    as one multi-shell mesh with about target_tris triangles."""
+def _sample_boxes(n_boxes, rng):
+    """Up to n_boxes disjoint random boxes (rejection sampled in [-1,1]^3)."""
     boxes = []
     for _ in range(200 * n_boxes):
         if len(boxes) == n_boxes:
@@ -193,6 +192,10 @@ def random_boxes_mesh(n_boxes, target_tris, rng):
         if any(np.all(lo < b[1] + 0.02) and np.all(b[0] < hi + 0.02) for b in boxes):
             continue
         boxes.append((lo, hi))
+    return boxes
+
+
+def _boxes_mesh(boxes, target_tris):
     per = max(12, target_tris // max(len(boxes), 1))
     sub = max(1, int(round((per / 12.0) ** 0.5)))
     vs, ts, off = [], [], 0
@@ -204,19 +207,34 @@ def random_boxes_mesh(n_boxes, target_tris, rng):
     return np.concatenate(vs), np.concatenate(ts).astype(np.int32)
 
 
-def batch_meshes(n_meshes=512, tmin=500, tmax=200_000, seed=3):
+def random_boxes_mesh(n_boxes, target_tris, rng):
+    """Union of n_boxes disjoint random boxes (rejection sampled in [-1,1]^3)
+    as one multi-shell mesh with about target_tris triangles."""
+    return _boxes_mesh(_sample_boxes(n_boxes, rng), target_tris)
+
+
+def batch_meshes(n_meshes=512, tmin=500, tmax=200_000, seed=3, select=None):
     """Uneven batch: triangle counts log-uniform in [tmin, tmax]; even
     indices are displaced spheres, odd ones unions of 2-6 random boxes.
-    All meshes are normalised to extent 2."""
+    All meshes are normalised to extent 2.  `select` (indices) builds only
+    those meshes -- the random draws of the others are still made, so a
+    selected mesh is the same as in the full batch."""
     rng = np.random.default_rng(seed)
     out = []
     for i in range(n_meshes):
         target = int(np.exp(rng.uniform(np.log(tmin), np.log(tmax))))
+        keep = select is None or i in select
         if i % 2 == 0:
             lvl = max(1, int(round(np.log(max(target, 80) / 20.0) / np.log(4.0))))
+            sd = int(rng.integers(1 << 30))
+            if not keep:
+                continue
             v, t = icosphere(min(lvl, 7))
-            v, t = displaced_sphere(v, t, 0.3, int(rng.integers(1 << 30)))
+            v, t = displaced_sphere(v, t, 0.3, sd)
         else:
-            v, t = random_boxes_mesh(int(rng.integers(2, 7)), target, rng)
+            boxes = _sample_boxes(int(rng.integers(2, 7)), rng)
+            if not keep:
+                continue
+            v, t = _boxes_mesh(boxes, target)
         out.append((normalize_extent(v).astype(np.float32), t))
     return out
