@@ -16,8 +16,11 @@ _lib = None
 
 
 def build():
-    """Compile the oracle with its Makefile (gcc only)."""
+    """Compile the oracle with its Makefile (gcc only), and the reference's
+    own GPU path into oracle/_ref with Makefile.ref where the reference tree
+    is present (it skips itself otherwise)."""
     subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    subprocess.run(["make", "-s", "-j8", "-C", _HERE, "-f", "Makefile.ref"], check=True)
 
 
 class CandResult(ctypes.Structure):
