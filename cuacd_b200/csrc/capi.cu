@@ -122,7 +122,7 @@ static int launch_hull_batch(gpu_ctx* ctx, const float* d_pts, const int* d_off,
                              int* d_nv, int* d_nt, float* d_vol, int* d_err, cudaStream_t s,
                              unsigned long long* d_stats = nullptr)
 {
-    const int nwc = hull_wrap_ctas((long long)n_hulls * max_pts, ctx->n_sm);
+    const int nwc = hull_wrap_ctas(hull_wrap_points(n_hulls, max_pts), ctx->n_sm);
     HullJob* jobs = pool_take<HullJob>(ctx, n_hulls);
     HullState* states = pool_take<HullState>(ctx, n_hulls);
     HullRes* res = pool_take<HullRes>(ctx, n_hulls);
@@ -159,7 +159,7 @@ static int hull_common(gpu_ctx_t ctx, const float* pts, int total_pts, const int
     size_t need = al256(sizeof(float) * 3 * (size_t)total_pts) + al256(sizeof(int) * (size_t)(n_hulls + 1))
                 + al256(sizeof(float) * 3 * (size_t)n_hulls * max_hv) + al256(sizeof(int) * 3 * (size_t)n_hulls * max_ht)
                 + 4 * al256(sizeof(int) * (size_t)n_hulls)
-                + hull_batch_need(n_hulls, max_pts, hull_wrap_ctas((long long)n_hulls * max_pts, ctx->n_sm))
+                + hull_batch_need(n_hulls, max_pts, hull_wrap_ctas(hull_wrap_points(n_hulls, max_pts), ctx->n_sm))
                 + al256(64 * (size_t)n_hulls);
     int rc = pool_begin(ctx, need);
     if (rc) return rc;
@@ -215,7 +215,7 @@ extern "C" int cuacd_hull_batch_device(gpu_ctx_t ctx, const float* d_pts, const 
     if (n_hulls <= 0) return 0;
     if (max_pts >= (1 << 22)) return ctx_fail(ctx, KERR_MESH_INVALID, "more than 2^22 points in one cloud");
     CK(cudaSetDevice(ctx->device));
-    int rc = pool_begin(ctx, hull_batch_need(n_hulls, max_pts, hull_wrap_ctas((long long)n_hulls * max_pts, ctx->n_sm)));
+    int rc = pool_begin(ctx, hull_batch_need(n_hulls, max_pts, hull_wrap_ctas(hull_wrap_points(n_hulls, max_pts), ctx->n_sm)));
     if (rc) return rc;
     return launch_hull_batch(ctx, d_pts, d_offsets, n_hulls, max_pts, max_hv, max_ht, d_v, d_t, d_nv, d_nt,
                              d_vol, d_err, stream ? (cudaStream_t)stream : ctx->stream);

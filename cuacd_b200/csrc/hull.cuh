@@ -33,8 +33,15 @@
 #define HULL_SMALL_S  24
 #define HULL_MORTON_BITS 4            // bits per axis for the bucket sort
 #define HULL_CELLS    (1 << (3 * HULL_MORTON_BITS))
-#define HULL_WSM      1024                         // shared ints per warp while wrapping (dynamic)
-#define HULL_WQ       704                          // of which: node stack
+// Shared ints per warp while wrapping (dynamic) and, of which, the node
+// stack; the rest is the kept-leaf list.  (The CPU emulation of the tests
+// builds with much smaller lists to drive the overflow paths.)
+#ifndef HULL_WSM
+#define HULL_WSM      1024
+#endif
+#ifndef HULL_WQ
+#define HULL_WQ       704
+#endif
 #define HULL_WL       (HULL_WSM - HULL_WQ)         //           kept-leaf list
 #define HULL_WRAP_DSMEM ((size_t)(HULL_NT / 32) * HULL_WSM * sizeof(int))
 #define HULL_SEEDS    1                            // seed faces (1..6) that start the wrapping; 6 seeds
@@ -320,7 +327,10 @@ static __device__ int warp_wrap(const HullCtx& H, int u, int v, const WarpLists 
     if (lane == 0) W.q[0] = 1;
     __syncwarp();
     while (sp > 0) {
-        const int batch = min(32, sp);
+        // pop at most as many nodes as the stack has room for children of
+        // (a step grows the stack by at most the nodes it pops)
+        const int batch = min(min(32, sp), W.qcap - sp);
+        if (batch <= 0) return -2;
         const int base = sp - batch;
         const int node = lane < batch ? W.q[base + lane] : 0;
         __syncwarp();                                   // all pops read before pushes overwrite
@@ -336,6 +346,31 @@ static __device__ int warp_wrap(const HullCtx& H, int u, int v, const WarpLists 
         }
         const unsigned bl = __ballot_sync(FULL_MASK, kl), bi = __ballot_sync(FULL_MASK, ki);
         const int nbl = __popc(bl), nbi = __popc(bi);
+        if (nl + nbl > W.lcap && ci >= 0) {
+            // Leaf list full: drop the recorded leaves that the current
+            // plane now prunes.  Their points were scanned already
+            // (scanned == nl here), and a point of the final face is never
+            // strictly beyond an earlier plane, so none of them can be on
+            // it.  In place: an entry moves to a position <= its own, after
+            // every lane has read its entry of the chunk.
+            int nk = 0;
+            for (int b0 = 0; b0 < nl; b0 += 32) {
+                const int j = b0 + lane;
+                int lf = 0;
+                bool keep = false;
+                if (j < nl) {
+                    lf = W.leaf[j];
+                    keep = !(box_min(mx, my, mz, H.nlo[lf + H.P], H.nhi[lf + H.P], a) > 0.0);
+                    double olo, ohi;
+                    if (keep && leaf_obb(H, lf, mx, my, mz, a, &olo, &ohi) && olo > 0.0) keep = false;
+                }
+                const unsigned bk = __ballot_sync(FULL_MASK, keep);
+                if (keep) W.leaf[nk + __popc(bk & lt)] = lf;
+                nk += __popc(bk);
+                __syncwarp();
+            }
+            nl = nk; scanned = nk;
+        }
         if (nl + nbl > W.lcap || base + 2 * nbi > W.qcap) return -2;
         if (kl) W.leaf[nl + __popc(bl & lt)] = node - H.P;
         if (ki) { int p = base + 2 * __popc(bi & lt); W.q[p] = 2 * node; W.q[p + 1] = 2 * node + 1; }

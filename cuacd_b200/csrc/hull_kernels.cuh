@@ -81,24 +81,32 @@ static __device__ void hull_assign_body(HullState* states, int n_jobs, int n_cta
 static __device__ void hull_wrap_body(HullState* states, int n_jobs, int* ctl, const long long* total, int* wbuf, int* wsm_dyn)
 {
     __shared__ HullWrapShared sh;
-    __shared__ int s_h0, s_go;
-    if (threadIdx.x == 0) {
-        // one reader decides for the whole CTA: other CTAs may finish the
-        // last hull while this one starts
-        s_go = *(volatile int*)&ctl[0] > 0;
-        // home hull: the active hull whose share holds this CTA's point
+    __shared__ int s_h0[HULL_NT / 32], s_go;
+    // one reader decides for the whole CTA: other CTAs may finish the last
+    // hull while this one starts
+    if (threadIdx.x == 0) s_go = *(volatile int*)&ctl[0] > 0;
+    // Home hull of each warp: the active hull whose share holds the warp's
+    // point.  With at most one hull per CTA the point is the CTA's (all its
+    // warps wrap one hull, whose BVH stays in that SM's L1); with more hulls
+    // than CTAs it is the warp's own, so many small clouds start at once
+    // instead of queueing behind one home hull per CTA.
+    if (threadIdx.x < HULL_NT / 32) {
         const long long W = *total;
-        const long long t = ((2LL * blockIdx.x + 1) * W) / (2LL * gridDim.x);
+        const bool per_warp = n_jobs > (int)gridDim.x;
+        const long long pos = per_warp ? 2LL * ((long long)blockIdx.x * (HULL_NT / 32) + threadIdx.x) + 1
+                                       : 2LL * blockIdx.x + 1;
+        const long long den = per_warp ? 2LL * gridDim.x * (HULL_NT / 32) : 2LL * gridDim.x;
+        const long long t = (pos * W) / den;
         int lo = 0, hi = n_jobs - 1;
         while (lo < hi) {                                 // last j with wbase[j] <= t
             int mid = (lo + hi + 1) >> 1;
             if (states[mid].wbase <= t) lo = mid; else hi = mid - 1;
         }
-        s_h0 = lo;
+        s_h0[threadIdx.x] = lo;
     }
     __syncthreads();
     if (!s_go) return;
-    hull_wrap_grid(states, n_jobs, s_h0, ctl, wbuf, sh, wsm_dyn);
+    hull_wrap_grid(states, n_jobs, s_h0[threadIdx.x >> 5], ctl, wbuf, sh, wsm_dyn);
 }
 static __device__ void hull_output_body(const HullJob* __restrict__ jobs, HullState* states, int n_jobs, Arena* out, const int* ctl,
               HullRes* res, unsigned long long* stats)

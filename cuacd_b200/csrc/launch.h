@@ -44,6 +44,13 @@ struct HullRes;
 struct HullState;
 size_t hull_wrap_buf_bytes(int n_wrap_ctas);
 int hull_wrap_ctas(long long total_points, int n_sm);
+// Points that size the wrap grid of a batch of n_hulls clouds of at most
+// max_pts points: small clouds count as 256 points each, so a batch of many
+// tiny clouds still gets about one warp per cloud.
+inline long long hull_wrap_points(int n_hulls, int max_pts)
+{
+    return (long long)n_hulls * (max_pts > 256 ? max_pts : 256);
+}
 void launch_hull_jobs(const HullJob* d_jobs, int n_jobs, HullState* d_states, HullRes* d_res, Arena* scratch,
                       Arena* out, int* d_ctl, int* d_wbuf, int n_wrap_ctas, unsigned long long* d_stats,
                       cudaStream_t s);

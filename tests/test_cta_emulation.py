@@ -80,15 +80,27 @@ def test_ear_clipping_race_case(emu_cut, tmp_path, oracle):
     check(oracle, v, t, planes, rows)
 
 
-@pytest.fixture(scope="module")
-def emu_hull(tmp_path_factory):
+def _build_emu_hull(tmp_path_factory, defines=()):
     if shutil.which("g++") is None:
         pytest.skip("g++ not available")
     out = str(tmp_path_factory.mktemp("emuh") / "emu_hull")
-    r = subprocess.run(["g++", "-std=c++20", "-O2", "-pthread", "-ffp-contract=off", "-I", EMU,
+    r = subprocess.run(["g++", "-std=c++20", "-O2", "-pthread", "-ffp-contract=off", *defines, "-I", EMU,
                         os.path.join(EMU, "emu_hull.cpp"), "-o", out], capture_output=True, text=True)
     assert r.returncode == 0, r.stderr[-2000:]
     return out
+
+
+@pytest.fixture(scope="module")
+def emu_hull(tmp_path_factory):
+    return _build_emu_hull(tmp_path_factory)
+
+
+@pytest.fixture(scope="module")
+def emu_hull_small_lists(tmp_path_factory):
+    """The same pipeline with 64 shared ints per warp (a 40-node stack and a
+    24-leaf list) instead of 1,024, so that wraps hit the stack limiter,
+    the leaf-list compaction and the fall-back to the hull's own lists."""
+    return _build_emu_hull(tmp_path_factory, ["-DHULL_WSM=64", "-DHULL_WQ=40"])
 
 
 def run_hulls(emu_hull, tmp_path, clouds):
@@ -128,6 +140,26 @@ def test_hull_pipeline_emulated(emu_hull, tmp_path, oracle):
     clouds = W.hull_clouds(3, 600, 0) + [frag, np.load(os.path.join(GOLDEN, "hull_flat_leaves.npy")), dup, g,
                                          dc["c0"], dc["c1"]]
     got, reports = run_hulls(emu_hull, tmp_path, clouds)
+    assert not reports, reports[:5]
+    for c, (err, hv, ht) in zip(clouds, got):
+        vi, tri, vol = oracle.hull(c)
+        assert err == 0
+        np.testing.assert_array_equal(hv, c[vi])
+        np.testing.assert_array_equal(ht, tri)
+
+
+def test_hull_overflow_paths_emulated(emu_hull_small_lists, tmp_path, oracle):
+    """With small per-warp lists, sphere shells and uniform clouds (many
+    leaves kept near each wrapping plane) still give the oracle's hulls, with
+    no divergent barrier or warp misuse, through the stack limiter, the
+    compaction of the kept-leaf list and the hull's own (locked) lists."""
+    rng = np.random.default_rng(5)
+    shells = []
+    for n in (1500, 3000):
+        d = rng.normal(size=(n, 3))
+        shells.append((d / np.linalg.norm(d, axis=1, keepdims=True) * rng.uniform(0.98, 1.0, (n, 1))).astype(np.float32))
+    clouds = shells + W.hull_clouds(2, 2000, 6)
+    got, reports = run_hulls(emu_hull_small_lists, tmp_path, clouds)
     assert not reports, reports[:5]
     for c, (err, hv, ht) in zip(clouds, got):
         vi, tri, vol = oracle.hull(c)
