@@ -215,11 +215,11 @@ class Context:
     # -- hulls --------------------------------------------------------------
     @staticmethod
     def _pack(pts_list):
-        arrs = [_as_f32(p).reshape(-1, 3) for p in pts_list]
-        packed = np.ascontiguousarray(np.concatenate(arrs, axis=0)) if arrs else np.zeros((0, 3), np.float32)
+        arrs = [p if (type(p) is np.ndarray and p.dtype == np.float32 and p.ndim == 2 and p.shape[1] == 3)
+                else np.asarray(p, dtype=np.float32).reshape(-1, 3) for p in pts_list]
+        packed = np.concatenate(arrs, axis=0) if arrs else np.zeros((0, 3), np.float32)
         off = np.zeros(len(arrs) + 1, dtype=np.int32)
-        for i, a in enumerate(arrs):
-            off[i + 1] = off[i] + len(a)
+        np.cumsum([len(a) for a in arrs], out=off[1:])
         return arrs, packed, off
 
     def _hull(self, pts_list, max_hv=None, max_ht=None):
