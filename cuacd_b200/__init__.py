@@ -84,6 +84,8 @@ def _opt(name, res, args):
 
 _opt("gpu_test_hausdorff", _I, [_P, _P, _I, _P, _I, _P, _I, _P, _I, _P])
 _opt("cuacd_hausdorff", _I, [_P, _P, _I, _P, _I, _P, _I, _P, _I, _F, _I, _I, _P])
+_opt("cuacd_hausdorff_batch", _I, [_P, _I, _P, _P, _P, _P, _P, _P, _P, _P, _F, _I, _I, _P])
+_opt("cuacd_hausdorff_batch_device", _I, [_P, _I, _P, _P, _P, _P, _P, _P, _P, _P, _F, _I, _I, _P, _P])
 _opt("gpu_test_plane_cut", _I, [_P, _P, _I, _P, _I, _F, _F, _F, _F,
                                 _P, _I, _P, _I, _P, _I, _P, _I, _P, _P, _P, _P])
 _opt("gpu_test_warp_sort", _I, [_P, _P, _I, _P, _I])
@@ -301,6 +303,28 @@ class Context:
                                            _ptr(bv), len(bv), _ptr(bt), len(bt),
                                            float(resolution), int(min_samples), int(total), _ptr(out)))
         return float(out[0])
+
+    def hausdorff_batch(self, pairs, resolution=2000.0, min_samples=1000, total=0):
+        """Sampled Hausdorff distance of each (a_verts, a_tris, b_verts, b_tris)
+        pair, all pairs in one batch -> float32[n]."""
+        n = len(pairs)
+        if n == 0:
+            return np.empty(0, np.float32)
+
+        def pack(items):
+            vs = [_as_f32(x[0]).reshape(-1, 3) for x in items]
+            ts = [_as_i32(x[1]).reshape(-1, 3) for x in items]
+            voff = np.zeros(n + 1, np.int32); np.cumsum([len(v) for v in vs], out=voff[1:])
+            toff = np.zeros(n + 1, np.int32); np.cumsum([len(t) for t in ts], out=toff[1:])
+            return (np.ascontiguousarray(np.concatenate(vs)), voff, np.ascontiguousarray(np.concatenate(ts)), toff)
+
+        av, avo, at, ato = pack([(p[0], p[1]) for p in pairs])
+        bv, bvo, bt, bto = pack([(p[2], p[3]) for p in pairs])
+        out = np.zeros(n, np.float32)
+        self._check(_fn("cuacd_hausdorff_batch")(self._h, n, _ptr(av), _ptr(avo), _ptr(at), _ptr(ato),
+                                                 _ptr(bv), _ptr(bvo), _ptr(bt), _ptr(bto), float(resolution),
+                                                 int(min_samples), int(total), _ptr(out)))
+        return out
 
     def plane_cut(self, verts, tris, plane):
         """Cut a closed mesh by plane (a,b,c,d) -> (pos_v, pos_t, neg_v, neg_t)."""

@@ -1,6 +1,8 @@
 // hausdorff.cu — Hausdorff kernels and the gpu_test_hausdorff /
 // cuacd_hausdorff entry points.
+#include <algorithm>
 #include <mutex>
+#include <vector>
 #include "context.cuh"
 #include "hausdorff.cuh"
 #include "launch.h"
@@ -298,6 +300,132 @@ extern "C" int gpu_test_hausdorff(gpu_ctx_t ctx, const float* hull_verts, int hu
 {
     return cuacd_hausdorff(ctx, hull_verts, hull_nv, hull_tris, hull_nt, mesh_verts, mesh_nv, mesh_tris, mesh_nt,
                            2000.f, 1000, 0, out_hausdorff);
+}
+
+// ---------------------------------------------------------------------------
+// Batched Hausdorff distance: n_pairs (A_i, B_i) pairs in one launch of each
+// stage (the reference runs such a batch as one block per pair in
+// bench/hausdorff_bench.cu:253-345 and, inside the search, in
+// la_hausdorff_parts).  Meshes are packed back to back: vertex offsets
+// voff[n+1], triangle offsets toff[n+1], triangle indices local to their mesh.
+// ---------------------------------------------------------------------------
+static int hd_batch_check(gpu_ctx* ctx, int n_pairs, const int* voff, const int* toff, const char* which,
+                          int* max_nt)
+{
+    *max_nt = 0;
+    if (voff[0] != 0 || toff[0] != 0) return ctx_fail(ctx, KERR_MESH_INVALID, "mesh %s: offsets must start at 0", which);
+    for (int i = 0; i < n_pairs; i++) {
+        if (voff[i + 1] < voff[i] || toff[i + 1] < toff[i])
+            return ctx_fail(ctx, KERR_MESH_INVALID, "mesh %s %d: decreasing offsets", which, i);
+        *max_nt = std::max(*max_nt, toff[i + 1] - toff[i]);
+    }
+    return 0;
+}
+
+static int hd_batch_run(gpu_ctx* ctx, int n_pairs, const float* dav, const int* a_voff, const int* dat,
+                        const int* a_toff, const float* dbv, const int* b_voff, const int* dbt, const int* b_toff,
+                        int max_a, int max_b, float resolution, int min_samples, int total, float* d_out,
+                        cudaStream_t s)
+{
+    HDSurf* dsurf = pool_take<HDSurf>(ctx, 2 * (size_t)n_pairs);
+    HDPrep* dprep = pool_take<HDPrep>(ctx, 2 * (size_t)n_pairs);
+    char* ddirs = pool_take<char>(ctx, 2 * (size_t)n_pairs * sizeof(HDDir));
+    int* di = pool_take<int>(ctx, 4);
+    float* dmax = pool_take<float>(ctx, (size_t)n_pairs);
+    if (!dsurf || !dprep || !ddirs || !di || !dmax) return ctx_fail(ctx, KERR_HEAP_OOM, "hausdorff batch: pool too small");
+    std::vector<HDSurf> hs(2 * (size_t)n_pairs);
+    for (int i = 0; i < n_pairs; i++) {
+        hs[2 * i] = {dav + 3 * (size_t)a_voff[i], dat + 3 * (size_t)a_toff[i], a_voff[i + 1] - a_voff[i],
+                     a_toff[i + 1] - a_toff[i]};
+        hs[2 * i + 1] = {dbv + 3 * (size_t)b_voff[i], dbt + 3 * (size_t)b_toff[i], b_voff[i + 1] - b_voff[i],
+                         b_toff[i + 1] - b_toff[i]};
+    }
+    CK(cudaMemcpyAsync(dsurf, hs.data(), sizeof(HDSurf) * hs.size(), cudaMemcpyHostToDevice, s));
+    CK(cudaMemsetAsync(di, 0, 4 * sizeof(int), s));
+    launch_arena_reset(ctx->d_arena, ctx->pool + ctx->carve, ctx->cap - ctx->carve, s);
+    launch_hausdorff_pairs(dsurf, n_pairs, ctx->d_arena, resolution, min_samples, total, dprep, ddirs, di, dmax,
+                           di + 2, sm_count(ctx), s);
+    launch_hd_sqrt(dmax, n_pairs, d_out, 1, s);
+    ctx->launches += 5;
+    CK(cudaGetLastError());
+    int herr = 0;
+    CK(cudaMemcpyAsync(&herr, di + 2, sizeof(int), cudaMemcpyDeviceToHost, s));
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return ctx_fail(ctx, (int)e, "hausdorff batch: %s", cudaGetErrorString(e));
+    if (herr) return ctx_fail(ctx, herr, "hausdorff batch failed (error word 0x%x)", herr);
+    (void)max_a; (void)max_b;
+    return 0;
+}
+
+static size_t hd_batch_pool_bytes(int n_pairs, int max_a, int max_b)
+{
+    return al256(sizeof(HDSurf) * 2 * (size_t)n_pairs) + al256(sizeof(HDPrep) * 2 * (size_t)n_pairs)
+         + al256(sizeof(HDDir) * 2 * (size_t)n_pairs) + al256(sizeof(int) * 4) + al256(sizeof(float) * (size_t)n_pairs)
+         + hd_pairs_scratch_bytes(n_pairs, max_a, max_b) + (1 << 20);
+}
+
+extern "C" int cuacd_hausdorff_batch(gpu_ctx_t ctx, int n_pairs,
+                                     const float* a_verts, const int* a_voff, const int* a_tris, const int* a_toff,
+                                     const float* b_verts, const int* b_voff, const int* b_tris, const int* b_toff,
+                                     float resolution, int min_samples, int total, float* out_hausdorff)
+{
+    if (!ctx) return -1;
+    if (n_pairs <= 0) return 0;
+    int max_a = 0, max_b = 0;
+    int rc = hd_batch_check(ctx, n_pairs, a_voff, a_toff, "a", &max_a);
+    if (!rc) rc = hd_batch_check(ctx, n_pairs, b_voff, b_toff, "b", &max_b);
+    if (rc) return rc;
+    for (int i = 0; i < n_pairs; i++) {
+        for (int k = 3 * a_toff[i]; k < 3 * a_toff[i + 1]; k++)
+            if (a_tris[k] < 0 || a_tris[k] >= a_voff[i + 1] - a_voff[i])
+                return ctx_fail(ctx, KERR_MESH_INVALID, "mesh a %d: index out of range", i);
+        for (int k = 3 * b_toff[i]; k < 3 * b_toff[i + 1]; k++)
+            if (b_tris[k] < 0 || b_tris[k] >= b_voff[i + 1] - b_voff[i])
+                return ctx_fail(ctx, KERR_MESH_INVALID, "mesh b %d: index out of range", i);
+    }
+    if (resolution <= 0.f) resolution = 2000.f;
+    if (min_samples < 0) min_samples = 1000;
+    CK(cudaSetDevice(ctx->device));
+    const size_t anv = a_voff[n_pairs], ant = a_toff[n_pairs], bnv = b_voff[n_pairs], bnt = b_toff[n_pairs];
+    size_t need = al256(12 * anv) + al256(12 * ant) + al256(12 * bnv) + al256(12 * bnt)
+                + al256(sizeof(float) * (size_t)n_pairs) + hd_batch_pool_bytes(n_pairs, max_a, max_b);
+    rc = pool_begin(ctx, need);
+    if (rc) return rc;
+    float* dav = pool_take<float>(ctx, 3 * anv); int* dat = pool_take<int>(ctx, 3 * ant);
+    float* dbv = pool_take<float>(ctx, 3 * bnv); int* dbt = pool_take<int>(ctx, 3 * bnt);
+    float* dout = pool_take<float>(ctx, (size_t)n_pairs);
+    cudaStream_t s = ctx->stream;
+    if (anv) CK(cudaMemcpyAsync(dav, a_verts, 12 * anv, cudaMemcpyHostToDevice, s));
+    if (ant) CK(cudaMemcpyAsync(dat, a_tris, 12 * ant, cudaMemcpyHostToDevice, s));
+    if (bnv) CK(cudaMemcpyAsync(dbv, b_verts, 12 * bnv, cudaMemcpyHostToDevice, s));
+    if (bnt) CK(cudaMemcpyAsync(dbt, b_tris, 12 * bnt, cudaMemcpyHostToDevice, s));
+    rc = hd_batch_run(ctx, n_pairs, dav, a_voff, dat, a_toff, dbv, b_voff, dbt, b_toff, max_a, max_b, resolution,
+                      min_samples, total, dout, s);
+    if (rc) return rc;
+    CK(cudaMemcpy(out_hausdorff, dout, sizeof(float) * (size_t)n_pairs, cudaMemcpyDeviceToHost));
+    return 0;
+}
+
+extern "C" int cuacd_hausdorff_batch_device(gpu_ctx_t ctx, int n_pairs,
+                                            const float* d_a_verts, const int* a_voff, const int* d_a_tris,
+                                            const int* a_toff, const float* d_b_verts, const int* b_voff,
+                                            const int* d_b_tris, const int* b_toff, float resolution,
+                                            int min_samples, int total, float* d_out, void* stream)
+{
+    if (!ctx) return -1;
+    if (n_pairs <= 0) return 0;
+    int max_a = 0, max_b = 0;
+    int rc = hd_batch_check(ctx, n_pairs, a_voff, a_toff, "a", &max_a);
+    if (!rc) rc = hd_batch_check(ctx, n_pairs, b_voff, b_toff, "b", &max_b);
+    if (rc) return rc;
+    if (resolution <= 0.f) resolution = 2000.f;
+    if (min_samples < 0) min_samples = 1000;
+    CK(cudaSetDevice(ctx->device));
+    rc = pool_begin(ctx, hd_batch_pool_bytes(n_pairs, max_a, max_b));
+    if (rc) return rc;
+    return hd_batch_run(ctx, n_pairs, d_a_verts, a_voff, d_a_tris, a_toff, d_b_verts, b_voff, d_b_tris, b_toff,
+                        max_a, max_b, resolution, min_samples, total, d_out,
+                        stream ? (cudaStream_t)stream : ctx->stream);
 }
 
 // ---------------------------------------------------------------------------

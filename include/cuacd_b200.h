@@ -184,6 +184,27 @@ int cuacd_hausdorff(gpu_ctx_t ctx,
                     float resolution, int min_samples, int total,
                     float* out_hausdorff);
 
+/* Batched Hausdorff distance of n_pairs mesh pairs (A_i, B_i), each stage
+ * launched once for the whole batch.  Replaces the reference's batch of
+ * hausdorff_block calls, one block per pair (bench/hausdorff_bench.cu:253-345;
+ * la_hausdorff_parts in cuda/la_lifecycle.cu), with the sampling rule of
+ * gpu_test_hausdorff (csrc/test.h:96-102).  Meshes are packed back to back:
+ * vertex offsets voff[n_pairs+1] and triangle offsets toff[n_pairs+1] (host
+ * arrays, starting at 0), triangle indices local to their mesh.  Host
+ * variant: host arrays in, out_hausdorff[n_pairs] on the host.  Device
+ * variant: vertex/triangle arrays and d_out on the device, offsets on the
+ * host, work on `stream` (NULL: the context's), synchronised before return;
+ * the caller guarantees the indices are in range. */
+int cuacd_hausdorff_batch(gpu_ctx_t ctx, int n_pairs,
+                          const float* a_verts, const int* a_voff, const int* a_tris, const int* a_toff,
+                          const float* b_verts, const int* b_voff, const int* b_tris, const int* b_toff,
+                          float resolution, int min_samples, int total, float* out_hausdorff);
+int cuacd_hausdorff_batch_device(gpu_ctx_t ctx, int n_pairs,
+                                 const float* d_a_verts, const int* a_voff, const int* d_a_tris,
+                                 const int* a_toff, const float* d_b_verts, const int* b_voff,
+                                 const int* d_b_tris, const int* b_toff, float resolution,
+                                 int min_samples, int total, float* d_out, void* stream);
+
 /* Allocation-free Hausdorff distance (no counterpart in the reference).
  * For callers that cannot allocate device memory — plugins inside a host
  * framework that owns all device allocations, or code where cudaMalloc is

@@ -48,3 +48,22 @@ def test_small_brute_sizes(ctx, oracle):
     g = ctx.hausdorff(tet_v, tet_t, v, t)
     o = oracle.hausdorff(tet_v, tet_t, v, t)
     assert abs(g - o) < HD_ATOL
+
+
+def test_batch_matches_single_pairs(ctx, oracle):
+    """cuacd_hausdorff_batch: every pair of a mixed batch gets the distance
+    the single-pair entry point gives it (same samples, exact maximum), and
+    the oracle's within 1e-5; repeated identical pairs agree."""
+    v, t = W.hausdorff_sphere(level=3)
+    (hv, ht, _), = ctx.batch_hull_dandc_mesh([v])
+    iv, it = W.icosphere(2)
+    a = box_mesh([-1, -1, -1], [1, 1, 1]); b = box_mesh([-0.5, -0.5, -0.5], [0.5, 0.5, 0.5])
+    cv, ct = W.candidate_mesh(32, 12, 0.35, seed=3)
+    (chv, cht, _), = ctx.batch_hull_dandc_mesh([cv])
+    pairs = [(hv, ht, v, t), (*a, *b), (iv.astype(np.float32), it, *a), (chv, cht, cv, ct)] + [(hv, ht, v, t)] * 5
+    got = ctx.hausdorff_batch(pairs)
+    for i, p in enumerate(pairs):
+        single = ctx.hausdorff(*p)
+        assert got[i] == np.float32(single), (i, got[i], single)
+        assert abs(got[i] - oracle.hausdorff(*p)) < HD_ATOL, i
+    assert np.all(got[4:] == got[0])
