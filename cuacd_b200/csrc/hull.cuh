@@ -323,8 +323,15 @@ static __device__ int warp_wrap(const HullCtx& H, int u, int v, const WarpLists 
     // pruned against it.  Every leaf not pruned when reached is recorded:
     // a point on the final plane is never strictly below an earlier (less
     // rotated) plane, so the list holds the final face's points.
-    int sp = 1, nl = 0, scanned = 0;
-    if (lane == 0) W.q[0] = 1;
+    // The sweep starts from the tree level with min(32, P) nodes (fewer if
+    // the stack is short) rather than the root: the levels above it hold fewer nodes than lanes, and walking
+    // them costs dependent steps with idle lanes.  A box contains its
+    // children's boxes, so a node the root walk would prune has every
+    // descendant pruned here too; only the order of the visits changes.
+    int d0 = 1;
+    while (d0 < 32 && d0 < H.P && 4 * d0 <= W.qcap) d0 <<= 1;
+    int sp = d0, nl = 0, scanned = 0;
+    if (lane < d0) W.q[lane] = d0 + lane;
     __syncwarp();
     while (sp > 0) {
         // pop at most as many nodes as the stack has room for children of
