@@ -270,6 +270,23 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def replica_max(totals, dist, device):
+    """Per-rank totals (times) -> their maximum over the ranks: N replicas
+    finish when the slowest one does.  Without a process group, unchanged."""
+    if dist is None:
+        return [float(x) for x in totals]
+    import torch
+    tt = torch.tensor([float(x) for x in totals], device=device, dtype=torch.float64)
+    dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    return [float(x) for x in tt]
+
+
+def replica_rate(world, units_per_rank, seconds):
+    """Whole-job throughput of `world` replicas that each processed
+    `units_per_rank` units, the slowest in `seconds`."""
+    return world * units_per_rank / seconds
+
+
 def _timed(step, stream, flush, steps, clocks=None):
     """CUDA-event time (ms) of each of `steps` calls of step() on `stream`,
     L2 flushed (untimed) before each."""
@@ -454,14 +471,11 @@ def main():
     e2e_exact_s = wall(host_step)
     e2e_s = wall(host_step_pruned)
 
-    tot_ms, tot_exact_ms = sum(ms_pruned), sum(ms_exact)
-    if dist:
-        tt = torch.tensor([tot_ms, tot_exact_ms, e2e_s, e2e_exact_s], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        tot_ms, tot_exact_ms, e2e_s, e2e_exact_s = [float(x) for x in tt]
+    tot_ms, tot_exact_ms, e2e_s, e2e_exact_s = replica_max(
+        [sum(ms_pruned), sum(ms_exact), e2e_s, e2e_exact_s], dist, "cuda")
     world_n = world
-    value = world_n * n * args.steps / (tot_ms / 1000.0)
-    e2e_val = world_n * n * args.steps / e2e_s
+    value = replica_rate(world_n, n * args.steps, tot_ms / 1000.0)
+    e2e_val = replica_rate(world_n, n * args.steps, e2e_s)
 
     # roofline of the dominant stage of the pruned step's exact evaluation
     names = ["k_cut_planes", "hull_pipeline", "k_hd_prep", "k_hd_plan", "k_hd_query", "k_eval_finish"]
@@ -499,9 +513,9 @@ def main():
             "e2e": {"value": e2e_val, "unit": UNIT,
                     "h2d_bytes_per_step": int(v.nbytes + t.astype(np.int32).nbytes + planes.nbytes),
                     "d2h_bytes_per_step": int(res_bytes + 8 * n)},
-            "exact": {"value": world_n * n * args.steps / (tot_exact_ms / 1000.0),
+            "exact": {"value": replica_rate(world_n, n * args.steps, tot_exact_ms / 1000.0),
                       "ms_per_step": tot_exact_ms / args.steps, "gpu_launches": int(l1 - l0),
-                      "e2e": world_n * n * args.steps / e2e_exact_s,
+                      "e2e": replica_rate(world_n, n * args.steps, e2e_exact_s),
                       "roofline": roofline(stage_exact, exact, np.ones(n, bool))}}
     if not args.no_search:
         with S.Scorer.load(ctx, S.RV_WEIGHTS_PATH) as rv, S.Scorer(ctx, seed=1) as raw:
