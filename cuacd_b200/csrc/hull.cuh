@@ -713,6 +713,16 @@ static __device__ __forceinline__ HullCtx hull_ctx(const HullState& S)
 // first face and seed the frontier queue.  Writes the hull's state to *S;
 // S->active = 1 when the queue holds work.  `scratch` holds
 // hull_scratch_bytes(n) bytes.
+// Set every entry of a table of 64-bit words to ~0 (all HULL_NT threads);
+// n even and the table 16-byte aligned, so two entries go per store.
+static __device__ __forceinline__ void cta_fill_ones64(unsigned long long* tab, int n, int tid)
+{
+    ulonglong2* t2 = reinterpret_cast<ulonglong2*>(tab);
+    ulonglong2 ones;
+    ones.x = ~0ull; ones.y = ~0ull;
+    for (int i = tid; i < (n >> 1); i += HULL_NT) t2[i] = ones;
+}
+
 static __device__ void hull_setup_cta(const float* __restrict__ pts, int n, char* scratch, HullState* S,
                                       HullSetupShared& sh)
 {
@@ -902,8 +912,8 @@ static __device__ void hull_setup_cta(const float* __restrict__ pts, int n, char
         __syncthreads();
     }
     // ---- 4. tables
-    for (int i = tid; i < C.eh; i += HULL_NT) eset[i] = ~0ull;
-    for (int i = tid; i < C.fh; i += HULL_NT) fset[i] = ~0ull;
+    cta_fill_ones64(eset, C.eh, tid);                // sizes even (powers of two), 256-byte aligned
+    cta_fill_ones64(fset, C.fh, tid);
     if (tid == 0) { sh.n_faces = 0; sh.n_corners = 0; sh.lexmin = ~0ull; }
     __syncthreads();
     HullCtx H; H.pts = P4; H.nlo = nlo; H.nhi = nhi; H.obb = obb; H.m = n; H.P = C.P; H.nleaf = C.m_leaves;
@@ -1136,7 +1146,7 @@ static __device__ void hull_setup_cta(const float* __restrict__ pts, int n, char
     }
 
     // ---- 6. frontier queue: every edge of the seed faces whose twin is unknown
-    for (int i = tid; i < qcap; i += HULL_NT) Q[i] = ~0ull;
+    cta_fill_ones64(Q, qcap, tid);                   // qcap = 2 * fr_cap, even
     __syncthreads();
     if (tid == 0) {
         int qt = 0;

@@ -32,6 +32,7 @@ using std::min;
 #define __align__(x) alignas(x)
 struct float4 { float x, y, z, w; };
 struct int2 { int x, y; };
+struct alignas(16) ulonglong2 { unsigned long long x, y; };
 struct dim3 { unsigned x = 0, y = 0, z = 0; };
 inline float4 make_float4(float a, float b, float c, float d) { return {a, b, c, d}; }
 inline int2 make_int2(int a, int b) { return {a, b}; }
