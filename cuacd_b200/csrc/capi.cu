@@ -294,6 +294,90 @@ extern "C" int gpu_test_mesh_volume(gpu_ctx_t ctx, const float* verts, int n_ver
 }
 
 // ---------------------------------------------------------------------------
+// Allocation throughput of the device arena on the workload of the
+// reference's heap benchmark (bench/malloc_test_bench.cu:76-125, an
+// mstress-style loop): `grid` blocks of 32 threads; thread 0 of each makes
+// `iters` allocations of log-uniform sizes in [size_min, size_max]
+// (xorshift32 draws, seeded per block) and keeps each in one of `slots`
+// per-block slots.  The arena has no single free: the memory of a whole run
+// is released by resetting the arena before the next one, as every
+// evaluation and every lookahead wave does.  Allocations that do not fit are
+// counted in fail.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned bench_xorshift32(unsigned& r)
+{
+    r ^= r << 13; r ^= r >> 17; r ^= r << 5;
+    return r;
+}
+
+__global__ void k_arena_mstress(Arena* a, void** slots, int n_slots, int iters, unsigned size_min, unsigned size_max,
+                                float ln_min, float ln_delta, int* fail)
+{
+    if (threadIdx.x != 0) return;
+    unsigned r = (unsigned)(blockIdx.x + 1) * 2654435761u;
+    void** mine = slots + (size_t)blockIdx.x * n_slots;
+    int nf = 0;
+    for (int i = 0; i < iters; i++) {
+        const int slot = (int)(bench_xorshift32(r) % (unsigned)n_slots);
+        const float u = (float)(bench_xorshift32(r) >> 8) * (1.0f / 16777216.0f);
+        unsigned sz = (unsigned)expf(ln_min + u * ln_delta);
+        sz = min(max(sz, size_min), size_max);
+        void* p = arena_alloc(a, sz, nullptr);
+        if (!p) nf++;
+        mine[slot] = p;
+    }
+    if (nf) atomicAdd(fail, nf);
+}
+
+extern "C" int cuacd_arena_bench(gpu_ctx_t ctx, int grid, int iters, int slots, unsigned size_min, unsigned size_max,
+                                 unsigned long long arena_bytes, int warmup, int measure, float* out_mean_ms,
+                                 float* out_std_ms, int* out_fail)
+{
+    if (!ctx || grid <= 0 || iters <= 0 || slots <= 0 || size_min == 0 || size_max < size_min || measure <= 0)
+        return -1;
+    CK(cudaSetDevice(ctx->device));
+    const size_t slot_bytes = sizeof(void*) * (size_t)grid * slots;
+    int rc = pool_begin(ctx, al256(slot_bytes) + al256(sizeof(int)) + arena_bytes + 4096);
+    if (rc) return rc;
+    void** d_slots = pool_take<void*>(ctx, (size_t)grid * slots);
+    int* d_fail = pool_take<int>(ctx, 1);
+    cudaStream_t s = ctx->stream;
+    const float ln_min = logf((float)size_min), ln_delta = logf((float)size_max) - ln_min;
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    std::vector<float> ms;
+    int fail = 0;
+    for (int run = 0; run < warmup + measure; run++) {
+        launch_arena_reset(ctx->d_arena, ctx->pool + ctx->carve, ctx->cap - ctx->carve, s);
+        CK(cudaMemsetAsync(d_slots, 0, slot_bytes, s));
+        CK(cudaMemsetAsync(d_fail, 0, sizeof(int), s));
+        CK(cudaEventRecord(e0, s));
+        k_arena_mstress<<<grid, 32, 0, s>>>(ctx->d_arena, d_slots, slots, iters, size_min, size_max, ln_min,
+                                            ln_delta, d_fail);
+        CK(cudaEventRecord(e1, s));
+        CK(cudaEventSynchronize(e1));
+        CK(cudaGetLastError());
+        float t = 0.f;
+        CK(cudaEventElapsedTime(&t, e0, e1));
+        if (run >= warmup) ms.push_back(t);
+        CK(cudaMemcpy(&fail, d_fail, sizeof(int), cudaMemcpyDeviceToHost));
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    double m = 0.0, v = 0.0;
+    for (float t : ms) m += t;
+    m /= ms.size();
+    for (float t : ms) v += (t - m) * (t - m);
+    v /= ms.size();
+    if (out_mean_ms) *out_mean_ms = (float)m;
+    if (out_std_ms) *out_std_ms = (float)sqrt(v);
+    if (out_fail) *out_fail = fail;
+    ctx->launches += (unsigned long long)(warmup + measure) * 2;
+    return 0;
+}
+
+// ---------------------------------------------------------------------------
 // entry points implemented in the remaining translation units
 // ---------------------------------------------------------------------------
 

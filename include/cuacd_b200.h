@@ -184,6 +184,18 @@ int cuacd_hausdorff(gpu_ctx_t ctx,
                     float resolution, int min_samples, int total,
                     float* out_hausdorff);
 
+/* Diagnostic: allocation throughput of the device arena that replaces the
+ * reference's device heap (heap_alloc/heap_free, cuda/allocator.cuh:110-362),
+ * on the workload of its heap benchmark (bench/malloc_test_bench.cu:76-125):
+ * `grid` blocks, thread 0 of each makes `iters` allocations of log-uniform
+ * sizes in [size_min, size_max] into `slots` per-block slots.  The arena
+ * frees by whole-arena reset, once per run (arena_bytes of pool).  Reports
+ * the mean and deviation of the kernel time over `measure` runs after
+ * `warmup`, and the allocations of the last run that did not fit. */
+int cuacd_arena_bench(gpu_ctx_t ctx, int grid, int iters, int slots, unsigned size_min, unsigned size_max,
+                      unsigned long long arena_bytes, int warmup, int measure, float* out_mean_ms,
+                      float* out_std_ms, int* out_fail);
+
 /* Batched Hausdorff distance of n_pairs mesh pairs (A_i, B_i), each stage
  * launched once for the whole batch.  Replaces the reference's batch of
  * hausdorff_block calls, one block per pair (bench/hausdorff_bench.cu:253-345;
