@@ -104,3 +104,11 @@ static int sync_and_check(gpu_ctx* ctx, const char* what)
     if (e != cudaSuccess) return ctx_fail(ctx, (int)e, "%s: %s", what, cudaGetErrorString(e));
     return 0;
 }
+
+// eval.cu: exact evaluation of the planes a selection keeps, the cut of
+// every plane overlapping the caller's selection work on stream s.
+struct EvalPrecut;
+int eval_precut_begin(gpu_ctx* ctx, const float* d_v, int nv, const int* d_t, int nt, const float4* d_planes, int n,
+                      EvalPrecut& P, cudaStream_t s);
+int eval_precut_finish(gpu_ctx* ctx, EvalPrecut& P, const int* d_pos, int n_sel, int flags, float res, int mins,
+                       int total, cuacd_cand_result* d_out, cudaStream_t s);

@@ -85,6 +85,16 @@ __global__ void k_eval_finish(const CutResult* __restrict__ cuts, const FragInfo
     out[i] = r;
 }
 
+// cuts[pos[i]] = all[i] for every plane i a selection kept (pos[i] >= 0).
+__global__ void k_gather_cuts(const CutResult* __restrict__ all, const int* __restrict__ pos, int n,
+                              CutResult* __restrict__ cuts)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int j = pos[i];
+    if (j >= 0) cuts[j] = all[i];
+}
+
 // ---------------------------------------------------------------------------
 // workspace and launch sequence (shared by the host and device entry points)
 // ---------------------------------------------------------------------------
@@ -146,16 +156,12 @@ static int sm_count_dev(int dev)
     return n > 0 ? n : 148;
 }
 
-// All launches of one evaluation of n planes (already in W.planes) on
-// stream s.  The caller resets the arena first.
-static void eval_launch(gpu_ctx* ctx, const float* d_v, int nv, const int* d_t, int nt, int n, int flags,
-                        float res, int mins, int total, EvalWork& W, cuacd_cand_result* d_out, cudaStream_t s)
+// The stages after the cut (hulls, Hausdorff, part costs) of n planes whose
+// cut results are in W.cuts, on stream s.
+static void eval_launch_after_cut(gpu_ctx* ctx, int n, int flags, float res, int mins, int total, EvalWork& W,
+                                  cuacd_cand_result* d_out, cudaStream_t s)
 {
     auto mark = [&](int i) { if (ctx->profile) { cudaEventRecord(ctx->ev[i], s); ctx->n_ev = i + 1; } };
-    cudaMemsetAsync(W.i4, 0, 4 * sizeof(int), s);
-    mark(0);
-    launch_cut_planes(d_v, nv, d_t, nt, W.planes, n, ctx->d_arena, W.cuts, s);
-    mark(1);
     k_frag_jobs<<<(2 * n + 127) / 128, 128, 0, s>>>(W.cuts, n, W.jobs);
     launch_hull_jobs(W.jobs, 2 * n, W.states, W.frags, ctx->d_arena, ctx->d_arena, W.hctl, W.wbuf, W.nwc,
                      nullptr, s);
@@ -172,6 +178,19 @@ static void eval_launch(gpu_ctx* ctx, const float* d_v, int nv, const int* d_t, 
     k_eval_finish<<<(n + 127) / 128, 128, 0, s>>>(W.cuts, W.frags, W.hd, n, hd ? 1 : 0, W.i4 + 2, d_out);
     mark(6);
     ctx->launches += 1;
+}
+
+// All launches of one evaluation of n planes (already in W.planes) on
+// stream s.  The caller resets the arena first.
+static void eval_launch(gpu_ctx* ctx, const float* d_v, int nv, const int* d_t, int nt, int n, int flags,
+                        float res, int mins, int total, EvalWork& W, cuacd_cand_result* d_out, cudaStream_t s)
+{
+    auto mark = [&](int i) { if (ctx->profile) { cudaEventRecord(ctx->ev[i], s); ctx->n_ev = i + 1; } };
+    cudaMemsetAsync(W.i4, 0, 4 * sizeof(int), s);
+    mark(0);
+    launch_cut_planes(d_v, nv, d_t, nt, W.planes, n, ctx->d_arena, W.cuts, s);
+    mark(1);
+    eval_launch_after_cut(ctx, n, flags, res, mins, total, W, d_out, s);
 }
 
 // ---------------------------------------------------------------------------
@@ -249,6 +268,59 @@ static int eval_run(gpu_ctx* ctx, const float* d_v, int nv, const int* d_t, int 
     }
     CK(cudaGetLastError());
     return 0;
+}
+
+// ---------------------------------------------------------------------------
+// Evaluation of the planes a selection keeps, with the cut of every plane
+// overlapping the selection itself (the surrogate-pruned evaluator): the
+// cuts of all n planes run on the context's auxiliary stream while the
+// caller ranks the planes on s; then s waits for them, gathers the kept
+// planes' cut results and runs the remaining stages on those alone.  The
+// cut of a plane does not depend on which others are cut, so every kept
+// plane's result equals the one the exact evaluator gives it.
+// ---------------------------------------------------------------------------
+int eval_precut_begin(gpu_ctx* ctx, const float* d_v, int nv, const int* d_t, int nt, const float4* d_planes, int n,
+                      EvalPrecut& P, cudaStream_t s)
+{
+    P.n = n;
+    P.nwc = eval_wrap_ctas(ctx, nv, n);
+    if (eval_aux_ready(ctx, 2)) return -1;
+    int rc = pool_begin(ctx, eval_fixed_bytes(n, P.nwc) + al256(sizeof(CutResult) * (size_t)n)
+                             + eval_arena_bytes(nv, nt, n));
+    if (rc) return rc;
+    P.W = new EvalWork;
+    if (eval_take(ctx, n, P.nwc, *P.W)) return ctx_fail(ctx, KERR_HEAP_OOM, "pool too small");
+    P.all_cuts = pool_take<CutResult>(ctx, n);
+    if (!P.all_cuts) return ctx_fail(ctx, KERR_HEAP_OOM, "pool too small");
+    cudaStream_t a = ctx->aux[0];
+    launch_arena_reset(ctx->d_arena, ctx->pool + ctx->carve, ctx->cap - ctx->carve, s);
+    CK(cudaMemsetAsync(P.W->i4, 0, 4 * sizeof(int), s));
+    CK(cudaEventRecord(ctx->fork_ev, s));
+    CK(cudaStreamWaitEvent(a, ctx->fork_ev, 0));
+    CK(cudaMemcpyAsync(P.W->planes, d_planes, sizeof(float4) * (size_t)n, cudaMemcpyDeviceToDevice, a));
+    launch_cut_planes(d_v, nv, d_t, nt, P.W->planes, n, ctx->d_arena, P.all_cuts, a);
+    CK(cudaEventRecord(ctx->join_ev[0], a));
+    ctx->launches += 2;
+    CK(cudaGetLastError());
+    return 0;
+}
+
+int eval_precut_finish(gpu_ctx* ctx, EvalPrecut& P, const int* d_pos, int n_sel, int flags, float res, int mins,
+                       int total, cuacd_cand_result* d_out, cudaStream_t s)
+{
+    CK(cudaStreamWaitEvent(s, ctx->join_ev[0], 0));
+    int rc = 0;
+    if (n_sel > 0) {
+        if (res <= 0.f) res = 2000.f;
+        if (mins < 0) mins = 1000;
+        k_gather_cuts<<<(P.n + 127) / 128, 128, 0, s>>>(P.all_cuts, d_pos, P.n, P.W->cuts);
+        ctx->launches += 1;
+        eval_launch_after_cut(ctx, n_sel, flags, res, mins, total, *P.W, d_out, s);
+        if (cudaGetLastError() != cudaSuccess) rc = ctx_fail(ctx, -1, "pruned evaluation launch failed");
+    }
+    delete P.W;
+    P.W = nullptr;
+    return rc;
 }
 
 extern "C" int cuacd_profile_stages(gpu_ctx_t ctx, int enable)

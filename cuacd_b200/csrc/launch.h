@@ -68,3 +68,9 @@ int scorer_predict_parts(gpu_ctx* ctx, cuacd_scorer* sc, const ScorerPart* parts
 // Feature rows of the last scorer_predict_parts call (n_rows x n_features floats) to the host.
 int scorer_copy_features(gpu_ctx* ctx, cuacd_scorer* sc, int n_rows, float* out, cudaStream_t s);
 int scorer_n_features();
+
+// eval.cu: exact evaluation of the planes a selection keeps, the cut of all
+// planes overlapping the selection (eval_precut_begin / eval_precut_finish,
+// declared in context.cuh)
+struct EvalWork;
+struct EvalPrecut { EvalWork* W = nullptr; CutResult* all_cuts = nullptr; int n = 0, nwc = 0; };

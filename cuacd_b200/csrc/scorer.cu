@@ -452,6 +452,7 @@ struct cuacd_scorer {
     size_t mv_cap, mt_cap, mp_cap;
     char* pr; size_t pr_cap;     // device pruning: selected planes, pos, count, sub-results
     int* h_count;                // pinned
+    char* hx; size_t hx_cap;     // host-pointer pruning: staged mesh, planes and results
 };
 
 static int sc_fail(gpu_ctx* ctx, int code, const char* msg) { return ctx_fail(ctx, code, "%s", msg); }
@@ -627,7 +628,7 @@ extern "C" void cuacd_scorer_free(cuacd_scorer_t s)
     cudaFree(s->X); cudaFree(s->T); cudaFree(s->idx); cudaFree(s->Xb); cudaFree(s->H1); cudaFree(s->H2);
     cudaFree(s->dYb); cudaFree(s->dH2b); cudaFree(s->dH1b); cudaFree(s->Tb); cudaFree(s->Y); cudaFree(s->dYf);
     cudaFree(s->dH2f); cudaFree(s->dH1f); cudaFree(s->mv); cudaFree(s->mt); cudaFree(s->mp); cudaFree(s->st);
-    cudaFree(s->pr); cudaFreeHost(s->h_count);
+    cudaFree(s->pr); cudaFreeHost(s->h_count); cudaFree(s->hx);
     free(s);                     // s->feat points into s->mp
     cudaGetLastError();          // a failed free must not surface in the next call's launch check
 }
@@ -857,50 +858,54 @@ extern "C" int cuacd_eval_candidates_pruned(gpu_ctx_t ctx, cuacd_scorer_t s, con
                                &hull_vol, &herr);
         if (rc) return rc;
     }
-    if (sc_features_device(ctx, s, verts, nv, tris, nt, hull_vol, planes, n_planes, st)) return -1;
-    if (sc_reserve(ctx, s, n_planes)) return -1;
-    k_gather_rows<<<n_planes, 64, 0, st>>>(s->feat, nullptr, nullptr, n_planes, s->nrm, s->Xb, nullptr);
-    sc_predict_rows(s, n_planes, st);
-    ctx->launches += 4;
-    SCK(cudaGetLastError());
-    std::vector<float> pred(n_planes);
-    SCK(cudaMemcpyAsync(pred.data(), s->Y, sizeof(float) * (size_t)n_planes, cudaMemcpyDeviceToHost, st));
-    int rc = sync_and_check(ctx, "scorer_predict");
+    // Stage the mesh and planes in the scorer's own device buffers and run
+    // the device-pointer form (features, network, selection and the exact
+    // evaluation of the kept planes, whose cuts overlap the ranking).
+    if (n_planes > SC_SEL_MAX) return ctx_fail(ctx, -1, "pruned evaluation takes at most %d planes", SC_SEL_MAX);
+    auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    const size_t o_t = al(12 * (size_t)nv), o_p = o_t + al(12 * (size_t)nt), o_r = o_p + al(16 * (size_t)n_planes);
+    const size_t o_y = o_r + al(sizeof(cuacd_cand_result) * (size_t)n_planes), o_e = o_y + al(4 * (size_t)n_planes);
+    if (sc_grow(ctx, (void**)&s->hx, s->hx_cap, o_e + al(4 * (size_t)n_planes))) return -1;
+    float* dv = (float*)s->hx;
+    int* dt = (int*)(s->hx + o_t);
+    float* dp = (float*)(s->hx + o_p);
+    cuacd_cand_result* dres = (cuacd_cand_result*)(s->hx + o_r);
+    float* dpred = (float*)(s->hx + o_y);
+    int* deval = (int*)(s->hx + o_e);
+    SCK(cudaMemcpyAsync(dv, verts, 12 * (size_t)nv, cudaMemcpyHostToDevice, st));
+    SCK(cudaMemcpyAsync(dt, tris, 12 * (size_t)nt, cudaMemcpyHostToDevice, st));
+    SCK(cudaMemcpyAsync(dp, planes, 16 * (size_t)n_planes, cudaMemcpyHostToDevice, st));
+    int n_eval = 0;
+    int rc = cuacd_eval_candidates_pruned_device(ctx, s, dv, nv, dt, nt, hull_vol, dp, n_planes, flags,
+                                                 hd_resolution, hd_min_samples, hd_total, top_k, margin, dres, dpred,
+                                                 deval, &n_eval, st);
     if (rc) return rc;
-    std::vector<float> key(n_planes);
-    for (int i = 0; i < n_planes; i++) {
-        pred[i] /= SC_TSCALE;
-        key[i] = pred[i] == pred[i] ? pred[i] : 3.402823466e38f;     // NaN ranks last
-    }
-    std::vector<int> order(n_planes);
-    for (int i = 0; i < n_planes; i++) order[i] = i;
-    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return key[a] < key[b]; });
-    const int k = std::min(top_k, n_planes);
-    const float kth = key[order[k - 1]];
-    std::vector<int> sel;
-    for (int r = 0; r < n_planes; r++) {
-        const int i = order[r];
-        if (r < k || key[i] <= kth + margin) sel.push_back(i);
-    }
-    std::sort(sel.begin(), sel.end());
-    std::vector<float> sp(4 * sel.size());
-    for (size_t j = 0; j < sel.size(); j++) memcpy(&sp[4 * j], planes + 4 * (size_t)sel[j], 16);
-    std::vector<cuacd_cand_result> res(sel.size());
-    rc = cuacd_eval_candidates(ctx, verts, nv, tris, nt, sp.data(), (int)sel.size(), flags, hd_resolution,
-                               hd_min_samples, hd_total, res.data());
+    SCK(cudaMemcpyAsync(out, dres, sizeof(cuacd_cand_result) * (size_t)n_planes, cudaMemcpyDeviceToHost, st));
+    if (out_pred) SCK(cudaMemcpyAsync(out_pred, dpred, 4 * (size_t)n_planes, cudaMemcpyDeviceToHost, st));
+    std::vector<int> evl(n_planes);
+    SCK(cudaMemcpyAsync(evl.data(), deval, 4 * (size_t)n_planes, cudaMemcpyDeviceToHost, st));
+    rc = sync_and_check(ctx, "eval_candidates_pruned");
     if (rc) return rc;
+    if (out_n_evaluated) *out_n_evaluated = n_eval;
+    if (out_evaluated) memcpy(out_evaluated, evl.data(), 4 * (size_t)n_planes);
+    // An arena too small for this mesh: evaluate the kept planes again
+    // through the host entry point, which grows the pool and retries.
+    std::vector<int> kept;
+    bool oom = false;
     for (int i = 0; i < n_planes; i++) {
-        cuacd_cand_result& r = out[i];
-        memset(&r, 0, sizeof(r));
-        r.score_rv = r.score_full = 3.402823466e38f;
-        if (out_evaluated) out_evaluated[i] = 0;
-        if (out_pred) out_pred[i] = pred[i];
+        if (!evl[i]) continue;
+        kept.push_back(i);
+        if (out[i].err & (KERR_HEAP_OOM | KERR_PC_SCRATCH_OOM | KERR_HD_SCRATCH_OOM)) oom = true;
     }
-    for (size_t j = 0; j < sel.size(); j++) {
-        out[sel[j]] = res[j];
-        if (out_evaluated) out_evaluated[sel[j]] = 1;
+    if (oom) {
+        std::vector<float> sp(4 * kept.size());
+        for (size_t j = 0; j < kept.size(); j++) memcpy(&sp[4 * j], planes + 4 * (size_t)kept[j], 16);
+        std::vector<cuacd_cand_result> res(kept.size());
+        rc = cuacd_eval_candidates(ctx, verts, nv, tris, nt, sp.data(), (int)kept.size(), flags, hd_resolution,
+                                   hd_min_samples, hd_total, res.data());
+        if (rc) return rc;
+        for (size_t j = 0; j < kept.size(); j++) out[kept[j]] = res[j];
     }
-    if (out_n_evaluated) *out_n_evaluated = (int)sel.size();
     return 0;
 }
 
@@ -934,6 +939,15 @@ extern "C" int cuacd_eval_candidates_pruned_device(gpu_ctx_t ctx, cuacd_scorer_t
     int* pos = (int*)(s->pr + o_pos);
     int* cnt = (int*)(s->pr + o_cnt);
     cuacd_cand_result* sub = (cuacd_cand_result*)(s->pr + o_sub);
+    // Outside stage profiling the cuts of all planes run on a second stream
+    // while the network ranks them (the profiled stages stay one serial
+    // pipeline, timed per stage).
+    const bool overlap = !ctx->profile;
+    EvalPrecut P;
+    if (overlap) {
+        int rc = eval_precut_begin(ctx, d_verts, nv, d_tris, nt, (const float4*)d_planes, n_planes, P, st);
+        if (rc) { delete P.W; return rc; }
+    }
     sc_launch_features(ctx, s, d_verts, nv, d_tris, nt, hull_vol, (const float4*)d_planes, n_planes, st);
     k_gather_rows<<<n_planes, 64, 0, st>>>(s->feat, nullptr, nullptr, n_planes, s->nrm, s->Xb, nullptr);
     sc_predict_rows(s, n_planes, st);
@@ -943,8 +957,9 @@ extern "C" int cuacd_eval_candidates_pruned_device(gpu_ctx_t ctx, cuacd_scorer_t
     SCK(cudaMemcpyAsync(s->h_count, cnt, sizeof(int), cudaMemcpyDeviceToHost, st));
     SCK(cudaStreamSynchronize(st));
     const int n_sel = *s->h_count;
-    int rc = cuacd_eval_candidates_device(ctx, d_verts, nv, d_tris, nt, (const float*)sel, n_sel, flags,
-                                          hd_resolution, hd_min_samples, hd_total, sub, st);
+    int rc = overlap ? eval_precut_finish(ctx, P, pos, n_sel, flags, hd_resolution, hd_min_samples, hd_total, sub, st)
+                     : cuacd_eval_candidates_device(ctx, d_verts, nv, d_tris, nt, (const float*)sel, n_sel, flags,
+                                                    hd_resolution, hd_min_samples, hd_total, sub, st);
     if (rc) return rc;
     k_scatter_results<<<(n_planes + 127) / 128, 128, 0, st>>>(sub, pos, n_planes, d_out, d_evaluated);
     ctx->launches += 1;

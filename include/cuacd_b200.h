@@ -323,10 +323,13 @@ int cuacd_scorer_train(gpu_ctx_t ctx, cuacd_scorer_t s, const float* X, const fl
 
 int cuacd_scorer_predict(gpu_ctx_t ctx, cuacd_scorer_t s, const float* X, int n, float* out);
 
-/* Surrogate-pruned evaluation: predicted scores for all planes, the exact
- * evaluator (cuacd_eval_candidates) for the top_k best predictions plus every
+/* Surrogate-pruned evaluation (at most 1024 planes): predicted scores for
+ * all planes, the exact evaluator for the top_k best predictions plus every
  * plane predicted within `margin` of the k-th.  Unevaluated planes get
- * ok = 0 and scores FLT_MAX.  hull_vol < 0 computes the part's hull volume. */
+ * ok = 0 and scores FLT_MAX.  hull_vol < 0 computes the part's hull volume.
+ * Runs the device-pointer form on staged copies of the inputs; kept planes
+ * that meet a full arena are evaluated again through cuacd_eval_candidates,
+ * which grows the pool. */
 int cuacd_eval_candidates_pruned(gpu_ctx_t ctx, cuacd_scorer_t s, const float* verts, int nv,
                                  const int* tris, int nt, float hull_vol,
                                  const float* planes, int n_planes, int flags,
@@ -335,9 +338,10 @@ int cuacd_eval_candidates_pruned(gpu_ctx_t ctx, cuacd_scorer_t s, const float* v
                                  float* out_pred, int* out_evaluated, int* out_n_evaluated);
 
 /* Device-pointer form on `stream` (at most 1024 planes): features, network,
- * selection and the scatter of results run on the device; the call waits
- * once for the selected count, then launches the exact evaluator on the
- * selected planes and returns without synchronising.  d_pred and
+ * selection and the scatter of results run on the device, and the cuts of
+ * all planes run on a second stream while the network ranks them; the call
+ * waits once for the selected count, then launches the remaining exact
+ * stages on the selected planes and returns without synchronising.  d_pred and
  * d_evaluated may be NULL; hull_vol must be the part's hull volume. */
 int cuacd_eval_candidates_pruned_device(gpu_ctx_t ctx, cuacd_scorer_t s, const float* d_verts, int nv,
                                         const int* d_tris, int nt, float hull_vol,
