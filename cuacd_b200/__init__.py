@@ -86,6 +86,7 @@ _opt("gpu_test_hausdorff", _I, [_P, _P, _I, _P, _I, _P, _I, _P, _I, _P])
 _opt("cuacd_hausdorff", _I, [_P, _P, _I, _P, _I, _P, _I, _P, _I, _F, _I, _I, _P])
 _opt("cuacd_hausdorff_batch", _I, [_P, _I, _P, _P, _P, _P, _P, _P, _P, _P, _F, _I, _I, _P])
 _opt("cuacd_hausdorff_batch_device", _I, [_P, _I, _P, _P, _P, _P, _P, _P, _P, _P, _F, _I, _I, _P, _P])
+_opt("gpu_mesh_audit", _I, [_P, _P, _I, _P, _I, ctypes.POINTER(ctypes.c_uint)])
 _opt("gpu_test_plane_cut", _I, [_P, _P, _I, _P, _I, _F, _F, _F, _F,
                                 _P, _I, _P, _I, _P, _I, _P, _I, _P, _P, _P, _P])
 _opt("gpu_test_warp_sort", _I, [_P, _P, _I, _P, _I])
@@ -132,6 +133,10 @@ def _fn(name):
 
 def native_library_path():
     return _LIB_PATH
+
+
+# verdict bits of gpu_mesh_audit (cuda/mesh_audit.cuh:21-26 in the reference)
+MAV_DEGEN_TRI, MAV_BAD_INDEX, MAV_OPEN_EDGE, MAV_NONMANIFOLD, MAV_FLIPPED = 1, 2, 4, 8, 16
 
 
 def _as_f32(a):
@@ -209,7 +214,25 @@ class Context:
 
     # -- out of scope in this engine ---------------------------------------
     def check_mesh(self, verts, tris):
-        raise NotImplementedError("check_mesh (mesh audit) is outside the candidate-evaluation path")
+        """Topology audit on the GPU (cuacd/__init__.py:124-152): a dict of
+        booleans and the raw verdict bitmask -- watertight (no edge used by
+        one triangle), manifold (none used by more than two), oriented (no
+        edge used twice in one direction, no degenerate triangle),
+        needs_remesh (any flag), degenerate, bad_index, flags."""
+        v = _as_f32(verts).reshape(-1, 3)
+        t = _as_i32(tris).reshape(-1, 3)
+        flags = ctypes.c_uint(0)
+        self._check(_fn("gpu_mesh_audit")(self._h, _ptr(v), len(v), _ptr(t), len(t), ctypes.byref(flags)))
+        f = int(flags.value)
+        return {
+            "watertight": not (f & MAV_OPEN_EDGE),
+            "manifold": not (f & MAV_NONMANIFOLD),
+            "oriented": not (f & (MAV_FLIPPED | MAV_DEGEN_TRI)),
+            "needs_remesh": bool(f),
+            "degenerate": bool(f & MAV_DEGEN_TRI),
+            "bad_index": bool(f & MAV_BAD_INDEX),
+            "flags": f,
+        }
 
     def preprocess(self, verts, tris, resolution=64):
         raise NotImplementedError("preprocess (remeshing) is outside the candidate-evaluation path")

@@ -104,6 +104,20 @@ int gpu_test_plane_cut(gpu_ctx_t ctx,
                        int* out_n_pv, int* out_n_pt,
                        int* out_n_nv, int* out_n_nt);
 
+/* Replaces gpu_mesh_audit (csrc/test.h:124-132): topology audit of a
+ * triangle mesh, *out_flags = a bitmask of the reference's verdict bits
+ * (cuda/mesh_audit.cuh:21-26): a zero-area or repeated-index triangle, an
+ * index outside [0, n_verts) (that triangle is skipped), an edge used by one
+ * triangle, by more than two, or by two in the same direction. */
+#define CUACD_MAV_OK          0u
+#define CUACD_MAV_DEGEN_TRI   (1u << 0)
+#define CUACD_MAV_BAD_INDEX   (1u << 1)
+#define CUACD_MAV_OPEN_EDGE   (1u << 2)
+#define CUACD_MAV_NONMANIFOLD (1u << 3)
+#define CUACD_MAV_FLIPPED     (1u << 4)
+int gpu_mesh_audit(gpu_ctx_t ctx, const float* verts, int n_verts, const int* tris, int n_tris,
+                   unsigned int* out_flags);
+
 /* Replaces gpu_test_postprocess_dc (csrc/postprocess.h:20-27): split a mesh
  * into its vertex-connected components.  Component c's vertices go to
  * out_verts[c*max_verts_per*3 ...] and its triangles (component-local

@@ -199,3 +199,45 @@ def components(verts, tris, max_comp=4096):
         vo += cnv[c]
         to += cnt[c]
     return out
+
+
+def mesh_audit(verts, tris):
+    """Verdict bits of the reference's mesh audit (cuda/mesh_audit.cuh:92-157):
+    1 a repeated-index or exactly zero-area triangle (FP32 cross product,
+    no fused operations), 2 an index outside [0, nv) (that triangle is
+    skipped), 4 an edge used by one triangle, 8 by more than two, 16 by two
+    in the same direction."""
+    v = np.asarray(verts, np.float32).reshape(-1, 3)
+    t = np.asarray(tris, np.int64).reshape(-1, 3)
+    nv = len(v)
+    flags = 0
+    bad = ((t < 0) | (t >= nv)).any(axis=1)
+    if bad.any():
+        flags |= 2
+    t = t[~bad]
+    if len(t) == 0:
+        return flags
+    a, b, c = t[:, 0], t[:, 1], t[:, 2]
+    rep = (a == b) | (b == c) | (a == c)
+    ab = (v[b] - v[a]).astype(np.float32)
+    ac = (v[c] - v[a]).astype(np.float32)
+    nx = ab[:, 1] * ac[:, 2] - ab[:, 2] * ac[:, 1]
+    ny = ab[:, 2] * ac[:, 0] - ab[:, 0] * ac[:, 2]
+    nz = ab[:, 0] * ac[:, 1] - ab[:, 1] * ac[:, 0]
+    zero = (nx * nx + ny * ny + nz * nz) <= np.float32(0.0)
+    if (rep | zero).any():
+        flags |= 1
+    e0 = np.concatenate([a, b, c])
+    e1 = np.concatenate([b, c, a])
+    lo, hi = np.minimum(e0, e1), np.maximum(e0, e1)
+    key = lo * (1 << 32) + hi
+    uk, inv = np.unique(key, return_inverse=True)
+    tot = np.bincount(inv, minlength=len(uk))
+    fwd = np.bincount(inv, weights=(e0 < e1).astype(np.int64), minlength=len(uk)).astype(np.int64)
+    if (tot == 1).any():
+        flags |= 4
+    if (tot > 2).any():
+        flags |= 8
+    if ((tot == 2) & ((fwd == 2) | (fwd == 0))).any():
+        flags |= 16
+    return flags

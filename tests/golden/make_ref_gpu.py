@@ -12,6 +12,7 @@ this library's CUDA path (GPU) with the reference's results.
 
 usage (on a machine with a B200, after `make -f oracle/Makefile.ref`):
     python tests/golden/make_ref_gpu.py [out.npz]
+    python tests/golden/make_ref_gpu.py --audit [out.npz]   (mesh-audit verdicts: ref_gpu_audit.npz)
 """
 import importlib.machinery
 import importlib.util
@@ -83,6 +84,46 @@ def hausdorff_meshes():
 
 def lookahead_meshes():
     return [W.candidate_mesh(64, 24), W.candidate_mesh(96, 32, 0.35, seed=5)]
+
+
+def audit_cases():
+    """(name, verts, tris) for the topology audit: closed meshes and the
+    same meshes broken in each way the verdict bits name."""
+    v, t = W.candidate_mesh(64, 24)
+    t = t.astype(np.int32)
+    bv, bt = W.box((-1, -0.5, -0.25), (1, 0.5, 0.25), 3)
+    rng = np.random.default_rng(30)
+    mv, mt = W.random_boxes_mesh(4, 3000, rng)
+    big = [m for m in W.batch_meshes(512, 500, 200_000, seed=3, select={i for i in range(512) if i % 16 in (0, 5)})
+           if len(m[1]) == 327680][0]
+    flip = t.copy(); flip[100] = flip[100][[0, 2, 1]]
+    extra_v = np.concatenate([v, np.array([[3.0, 3.0, 3.0]], np.float32)])
+    nonman = np.concatenate([t, np.array([[t[0, 0], t[0, 1], len(v)]], np.int32)])
+    col_v = np.concatenate([v, np.array([[0, 0, 0], [1, 1, 1], [2, 2, 2]], np.float32)])
+    collinear = np.concatenate([t, np.array([[len(v), len(v) + 1, len(v) + 2]], np.int32)])
+    rep = np.concatenate([t, np.array([[5, 5, 6]], np.int32)])
+    bad = np.concatenate([t, np.array([[0, 1, len(v)]], np.int32)])
+    neg = np.concatenate([t, np.array([[0, -1, 2]], np.int32)])
+    dup = np.concatenate([t, t[:1]])
+    bflip = big[1].astype(np.int32).copy(); bflip[5000] = bflip[5000][[1, 0, 2]]
+    return [("sphere", v, t), ("box", bv, bt.astype(np.int32)), ("boxes", mv, mt.astype(np.int32)),
+            ("open", v, t[:-1]), ("flipped", v, flip), ("nonmanifold", extra_v, nonman),
+            ("collinear", col_v, collinear), ("repeated_index", v, rep), ("bad_index", v, bad),
+            ("negative_index", v, neg), ("duplicate_triangle", v, dup), ("big_sphere", big[0], big[1].astype(np.int32)),
+            ("big_flipped", big[0], bflip)]
+
+
+def main_audit(out_path):
+    """The reference's `_gpu.mesh_audit` verdict on every audit case."""
+    g = load_ref()
+    rec = {}
+    for name, v, t in audit_cases():
+        v = np.ascontiguousarray(v, np.float32)
+        t = np.ascontiguousarray(t, np.int32)
+        rec[name] = np.array([g.mesh_audit(v.ctypes.data, len(v), t.ctypes.data, len(t))], np.uint32)
+        print(name, int(rec[name][0]), flush=True)
+    g.destroy()
+    np.savez_compressed(out_path, **rec)
 
 
 LOOKAHEAD_KW = dict(max_iters=100, width=30, width2=5, threshold=0.05, depth=2, quick_depth=0,
@@ -238,4 +279,7 @@ def main(out_path):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else os.path.join(HERE, "ref_gpu.npz"))
+    if len(sys.argv) > 1 and sys.argv[1] == "--audit":
+        main_audit(sys.argv[2] if len(sys.argv) > 2 else os.path.join(HERE, "ref_gpu_audit.npz"))
+    else:
+        main(sys.argv[1] if len(sys.argv) > 1 else os.path.join(HERE, "ref_gpu.npz"))
