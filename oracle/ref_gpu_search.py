@@ -17,7 +17,8 @@ triangles, parts, seconds and the largest part rv cost, for the reference,
 this library's exact search and its pruned search (learned level-0 top-48 +
 exact beam 8).  Measurement infrastructure only; writes one JSON file.
 
-usage:  python oracle/ref_gpu_search.py out.json
+usage:  python oracle/ref_gpu_search.py out.json [--full]
+        (--full: all 512 meshes of config 4 instead of the 64-mesh sample)
 """
 import json
 import os
@@ -38,7 +39,9 @@ from cuacd_b200 import workloads as W  # noqa: E402
 KW = dict(max_iters=100, width=30, width2=5, threshold=0.05, depth=2, quick_depth=0, max_n_cutting=16)
 
 
-def samples():
+def samples(full=False):
+    if full:                                          # all 512 meshes of config 4
+        return {"search": (B.search_meshes(), 32), "config4_full": (W.batch_meshes(512, 500, 200_000, seed=3), 16)}
     c4 = W.batch_meshes(512, 500, 200_000, seed=3, select={i for i in range(512) if i % 16 in (0, 5)})
     return {"search": (B.search_meshes(), 32), "config4": (c4, 16)}
 
@@ -67,8 +70,8 @@ def ref_search(g, v, t, n_edges):
     return parts, dt
 
 
-def main(out_path):
-    S = samples()
+def main(out_path, full=False):
+    S = samples(full)
     rec = {"settings": {**KW, "n_concave_edges": {k: e for k, (_, e) in S.items()}}}
     g = MR.load_ref()
     for v, t in S["search"][0]:                       # untimed pass
@@ -76,7 +79,11 @@ def main(out_path):
     for name, (meshes, ne) in S.items():
         rows = []
         for v, t in meshes:
-            parts, dt = ref_search(g, v, t, ne)
+            try:
+                parts, dt = ref_search(g, v, t, ne)
+            except Exception as e:                    # record a failed search and go on
+                rows.append({"tris": int(len(t)), "parts": 0, "s": 0.0, "max_rv": 0.0, "error": str(e)[:200]})
+                continue
             rows.append({"tris": int(len(t)), "parts": len(parts), "s": dt, "max_rv": B.part_cost_max(parts)})
         rec[f"reference_{name}"] = rows
         print("reference", name, sum(r["s"] for r in rows), "s", sum(r["parts"] for r in rows), "parts", flush=True)
@@ -93,7 +100,11 @@ def main(out_path):
                 rows = []
                 for v, t in meshes:
                     t0 = time.perf_counter()
-                    parts = ctx.lookahead_decompose(v, t, **KW, n_concave_edges=ne, **extra)
+                    try:
+                        parts = ctx.lookahead_decompose(v, t, **KW, n_concave_edges=ne, **extra)
+                    except RuntimeError as e:
+                        rows.append({"tris": int(len(t)), "parts": 0, "s": 0.0, "max_rv": 0.0, "error": str(e)[:200]})
+                        continue
                     dt = time.perf_counter() - t0
                     rows.append({"tris": int(len(t)), "parts": len(parts), "s": dt, "max_rv": B.part_cost_max(parts)})
                 rec[f"{mname}_{name}"] = rows
@@ -103,4 +114,4 @@ def main(out_path):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1])
+    main(sys.argv[1], full="--full" in sys.argv[2:])
