@@ -54,6 +54,34 @@ __global__ void k_make_surfs(const CutResult* __restrict__ cuts, const FragInfo*
     surfs[2 * f + 1] = B;
 }
 
+// The same pairs built in two steps, so that the fragments' Hausdorff prep
+// can start before their hulls exist: the fragment surfaces (2f+1) from the
+// cut alone, then the hull surfaces (2f) -- empty when the hull failed, which
+// leaves the pair without queries, as k_make_surfs does.
+__global__ void k_make_frag_surfs(const CutResult* __restrict__ cuts, int n_frag, HDSurf* surfs)
+{
+    int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= n_frag) return;
+    const CutResult& C = cuts[f >> 1];
+    const bool ok = C.err == 0 && C.npv > 0 && C.nnv > 0;
+    HDSurf B;
+    if (f & 1) { B.v = C.nv; B.t = C.nt; B.nv = ok ? C.nnv : 0; B.nt = ok ? C.nnt : 0; }
+    else       { B.v = C.pv; B.t = C.pt; B.nv = ok ? C.npv : 0; B.nt = ok ? C.npt : 0; }
+    surfs[2 * f + 1] = B;
+}
+
+__global__ void k_make_hull_surfs(const CutResult* __restrict__ cuts, const FragInfo* __restrict__ frags, int n_frag,
+                                  HDSurf* surfs)
+{
+    int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= n_frag) return;
+    const CutResult& C = cuts[f >> 1];
+    const FragInfo& F = frags[f];
+    const bool ok = F.err == 0 && F.hnt > 0 && C.npv > 0 && C.nnv > 0;
+    HDSurf A = {F.hv, F.ht, ok ? F.hnv : 0, ok ? F.hnt : 0};
+    surfs[2 * f] = A;
+}
+
 __global__ void k_eval_finish(const CutResult* __restrict__ cuts, const FragInfo* __restrict__ frags,
                               const float* __restrict__ hd, int n_cand, int with_hd, const int* arena_err,
                               cuacd_cand_result* out)
@@ -156,19 +184,42 @@ static int sm_count_dev(int dev)
     return n > 0 ? n : 148;
 }
 
+static int eval_aux_ready(gpu_ctx* ctx, int G);
+
 // The stages after the cut (hulls, Hausdorff, part costs) of n planes whose
 // cut results are in W.cuts, on stream s.
 static void eval_launch_after_cut(gpu_ctx* ctx, int n, int flags, float res, int mins, int total, EvalWork& W,
-                                  cuacd_cand_result* d_out, cudaStream_t s)
+                                  cuacd_cand_result* d_out, cudaStream_t s, bool may_overlap)
 {
     auto mark = [&](int i) { if (ctx->profile) { cudaEventRecord(ctx->ev[i], s); ctx->n_ev = i + 1; } };
+    const bool hd = flags & CUACD_EVAL_HAUSDORFF;
+    // Outside stage profiling (whose events describe one serial pipeline),
+    // the fragments' Hausdorff prep runs on a second stream beside the hull
+    // pipeline: it needs only the cut.
+    const bool overlap = hd && may_overlap && !ctx->profile && eval_aux_ready(ctx, 3) == 0;
     k_frag_jobs<<<(2 * n + 127) / 128, 128, 0, s>>>(W.cuts, n, W.jobs);
+    if (overlap) {
+        cudaStream_t a = ctx->aux[1];
+        k_make_frag_surfs<<<(2 * n + 127) / 128, 128, 0, s>>>(W.cuts, 2 * n, W.surfs);
+        cudaEventRecord(ctx->fork_ev, s);
+        cudaStreamWaitEvent(a, ctx->fork_ev, 0);
+        launch_hd_prep_subset(W.surfs, 2 * n, 1, 2, ctx->d_arena, res, mins, total, W.preps, W.i4 + 2, a);
+        cudaEventRecord(ctx->join_ev[1], a);
+        ctx->launches += 2;
+    }
     launch_hull_jobs(W.jobs, 2 * n, W.states, W.frags, ctx->d_arena, ctx->d_arena, W.hctl, W.wbuf, W.nwc,
                      nullptr, s);
     mark(2);
     ctx->launches += 6;
-    const bool hd = flags & CUACD_EVAL_HAUSDORFF;
-    if (hd) {
+    if (hd && overlap) {
+        k_make_hull_surfs<<<(2 * n + 127) / 128, 128, 0, s>>>(W.cuts, W.frags, 2 * n, W.surfs);
+        launch_hd_prep_subset(W.surfs, 2 * n, 0, 2, ctx->d_arena, res, mins, total, W.preps, W.i4 + 2, s);
+        cudaStreamWaitEvent(s, ctx->join_ev[1], 0);
+        launch_hd_plan_query(W.surfs, 2 * n, W.preps, W.dirs, W.i4, W.pmax, sm_count_dev(ctx->device), s,
+                             [](int) {});
+        launch_hd_sqrt(W.pmax, 2 * n, W.hd, 1, s);
+        ctx->launches += 5;
+    } else if (hd) {
         k_make_surfs<<<(2 * n + 127) / 128, 128, 0, s>>>(W.cuts, W.frags, 2 * n, W.surfs);
         launch_hausdorff_stages(W.surfs, 2 * n, ctx->d_arena, res, mins, total, W.preps, W.dirs, W.i4, W.pmax,
                                 W.i4 + 2, sm_count_dev(ctx->device), s, [&](int k) { mark(3 + k); });
@@ -183,14 +234,15 @@ static void eval_launch_after_cut(gpu_ctx* ctx, int n, int flags, float res, int
 // All launches of one evaluation of n planes (already in W.planes) on
 // stream s.  The caller resets the arena first.
 static void eval_launch(gpu_ctx* ctx, const float* d_v, int nv, const int* d_t, int nt, int n, int flags,
-                        float res, int mins, int total, EvalWork& W, cuacd_cand_result* d_out, cudaStream_t s)
+                        float res, int mins, int total, EvalWork& W, cuacd_cand_result* d_out, cudaStream_t s,
+                        bool may_overlap)
 {
     auto mark = [&](int i) { if (ctx->profile) { cudaEventRecord(ctx->ev[i], s); ctx->n_ev = i + 1; } };
     cudaMemsetAsync(W.i4, 0, 4 * sizeof(int), s);
     mark(0);
     launch_cut_planes(d_v, nv, d_t, nt, W.planes, n, ctx->d_arena, W.cuts, s);
     mark(1);
-    eval_launch_after_cut(ctx, n, flags, res, mins, total, W, d_out, s);
+    eval_launch_after_cut(ctx, n, flags, res, mins, total, W, d_out, s, may_overlap);
 }
 
 // ---------------------------------------------------------------------------
@@ -260,7 +312,7 @@ static int eval_run(gpu_ctx* ctx, const float* d_v, int nv, const int* d_t, int 
         cudaStream_t sg = g == 0 ? s : ctx->aux[g - 1];
         if (g > 0) CK(cudaStreamWaitEvent(sg, ctx->fork_ev, 0));
         CK(cudaMemcpyAsync(W[g].planes, d_planes + o, sizeof(float4) * m, cudaMemcpyDeviceToDevice, sg));
-        eval_launch(ctx, d_v, nv, d_t, nt, m, flags, res, mins, total, W[g], d_out + o, sg);
+        eval_launch(ctx, d_v, nv, d_t, nt, m, flags, res, mins, total, W[g], d_out + o, sg, G == 1);
     }
     for (int g = 1; g < G; g++) {
         CK(cudaEventRecord(ctx->join_ev[g - 1], ctx->aux[g - 1]));
@@ -315,7 +367,7 @@ int eval_precut_finish(gpu_ctx* ctx, EvalPrecut& P, const int* d_pos, int n_sel,
         if (mins < 0) mins = 1000;
         k_gather_cuts<<<(P.n + 127) / 128, 128, 0, s>>>(P.all_cuts, d_pos, P.n, P.W->cuts);
         ctx->launches += 1;
-        eval_launch_after_cut(ctx, n_sel, flags, res, mins, total, *P.W, d_out, s);
+        eval_launch_after_cut(ctx, n_sel, flags, res, mins, total, *P.W, d_out, s, true);
         if (cudaGetLastError() != cudaSuccess) rc = ctx_fail(ctx, -1, "pruned evaluation launch failed");
     }
     delete P.W;

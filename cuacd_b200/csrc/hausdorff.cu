@@ -8,13 +8,15 @@
 #include "launch.h"
 
 // One CTA per surface: budget, offsets, BVH.  Scratch from the arena.
+// Surface i = first + blockIdx.x * step (a subset of the surfaces can be
+// prepared while the rest are still being built).
 __global__ void __launch_bounds__(HD_PREP_NT)
 k_hd_prep(const HDSurf* __restrict__ surfs, int n_surf, Arena* arena, float resolution, int min_samples,
-          int total_override, HDPrep* preps, int* err)
+          int total_override, HDPrep* preps, int* err, int first = 0, int step = 1)
 {
     __shared__ HDShared sh;
     __shared__ char* s_scr;
-    int i = blockIdx.x;
+    int i = first + (int)blockIdx.x * step;
     if (i >= n_surf) return;
     HDSurf S = surfs[i];
     if (threadIdx.x == 0) {
@@ -218,6 +220,25 @@ void launch_hausdorff_stages(const HDSurf* d_surfs, int n_pairs, Arena* arena, f
 {
     if (n_pairs > 0) k_hd_prep<<<2 * n_pairs, HD_PREP_NT, 0, s>>>(d_surfs, 2 * n_pairs, arena, resolution, min_samples, total, d_preps, d_err);
     after(0);
+    if (n_pairs > 0) k_hd_plan<<<1, 32, 0, s>>>(d_surfs, d_preps, n_pairs, (HDDir*)d_dirs, d_i2, d_i2 + 1, d_pmax);
+    after(1);
+    if (n_pairs > 0) k_hd_query<<<n_sm * 8, HD_NT, 0, s>>>(d_surfs, d_preps, (const HDDir*)d_dirs, 2 * n_pairs, d_i2, d_i2 + 1, d_pmax);
+    after(2);
+}
+
+// The stages split for overlap: prep of surfaces first, first + step, ...
+// (below 2 * n_pairs), and plan + queries once every surface is prepared.
+void launch_hd_prep_subset(const HDSurf* d_surfs, int n_pairs, int first, int step, Arena* arena, float resolution,
+                           int min_samples, int total, HDPrep* d_preps, int* d_err, cudaStream_t s)
+{
+    const int n = (2 * n_pairs - first + step - 1) / step;
+    if (n > 0) k_hd_prep<<<n, HD_PREP_NT, 0, s>>>(d_surfs, 2 * n_pairs, arena, resolution, min_samples, total, d_preps,
+                                                 d_err, first, step);
+}
+
+void launch_hd_plan_query(const HDSurf* d_surfs, int n_pairs, HDPrep* d_preps, void* d_dirs, int* d_i2,
+                          float* d_pmax, int n_sm, cudaStream_t s, const std::function<void(int)>& after)
+{
     if (n_pairs > 0) k_hd_plan<<<1, 32, 0, s>>>(d_surfs, d_preps, n_pairs, (HDDir*)d_dirs, d_i2, d_i2 + 1, d_pmax);
     after(1);
     if (n_pairs > 0) k_hd_query<<<n_sm * 8, HD_NT, 0, s>>>(d_surfs, d_preps, (const HDDir*)d_dirs, 2 * n_pairs, d_i2, d_i2 + 1, d_pmax);

@@ -27,6 +27,10 @@ void launch_hausdorff_stages(const HDSurf* d_surfs, int n_pairs, Arena* arena, f
                              int total, HDPrep* d_preps, void* d_dirs, int* d_i2, float* d_pmax, int* d_err,
                              int n_sm, cudaStream_t s, const std::function<void(int)>& after);
 void launch_hd_sqrt(const float* pmax, int n, float* out, int stride_floats, cudaStream_t s);
+void launch_hd_prep_subset(const HDSurf* d_surfs, int n_pairs, int first, int step, Arena* arena, float resolution,
+                           int min_samples, int total, HDPrep* d_preps, int* d_err, cudaStream_t s);
+void launch_hd_plan_query(const HDSurf* d_surfs, int n_pairs, HDPrep* d_preps, void* d_dirs, int* d_i2,
+                          float* d_pmax, int n_sm, cudaStream_t s, const std::function<void(int)>& after);
 
 // components.cu
 struct CompResult;
