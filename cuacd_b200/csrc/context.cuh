@@ -112,3 +112,4 @@ int eval_precut_begin(gpu_ctx* ctx, const float* d_v, int nv, const int* d_t, in
                       EvalPrecut& P, cudaStream_t s);
 int eval_precut_finish(gpu_ctx* ctx, EvalPrecut& P, const int* d_pos, int n_sel, int flags, float res, int mins,
                        int total, cuacd_cand_result* d_out, cudaStream_t s);
+void eval_precut_release(EvalPrecut& P);      // frees the work set (finish does it too)

@@ -357,6 +357,12 @@ int eval_precut_begin(gpu_ctx* ctx, const float* d_v, int nv, const int* d_t, in
     return 0;
 }
 
+void eval_precut_release(EvalPrecut& P)
+{
+    delete P.W;
+    P.W = nullptr;
+}
+
 int eval_precut_finish(gpu_ctx* ctx, EvalPrecut& P, const int* d_pos, int n_sel, int flags, float res, int mins,
                        int total, cuacd_cand_result* d_out, cudaStream_t s)
 {
@@ -370,8 +376,7 @@ int eval_precut_finish(gpu_ctx* ctx, EvalPrecut& P, const int* d_pos, int n_sel,
         eval_launch_after_cut(ctx, n_sel, flags, res, mins, total, *P.W, d_out, s, true);
         if (cudaGetLastError() != cudaSuccess) rc = ctx_fail(ctx, -1, "pruned evaluation launch failed");
     }
-    delete P.W;
-    P.W = nullptr;
+    eval_precut_release(P);
     return rc;
 }
 

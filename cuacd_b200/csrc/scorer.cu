@@ -944,9 +944,13 @@ extern "C" int cuacd_eval_candidates_pruned_device(gpu_ctx_t ctx, cuacd_scorer_t
     // pipeline, timed per stage).
     const bool overlap = !ctx->profile;
     EvalPrecut P;
+    struct Release {                   // the work set of an overlapped evaluation, on every return path
+        EvalPrecut& p;
+        ~Release() { eval_precut_release(p); }
+    } release{P};
     if (overlap) {
         int rc = eval_precut_begin(ctx, d_verts, nv, d_tris, nt, (const float4*)d_planes, n_planes, P, st);
-        if (rc) { delete P.W; return rc; }
+        if (rc) return rc;
     }
     sc_launch_features(ctx, s, d_verts, nv, d_tris, nt, hull_vol, (const float4*)d_planes, n_planes, st);
     k_gather_rows<<<n_planes, 64, 0, st>>>(s->feat, nullptr, nullptr, n_planes, s->nrm, s->Xb, nullptr);
