@@ -74,6 +74,23 @@ def ncu_traffic(kernel, planes):
     return None
 
 
+def ncu_counters(stage):
+    """Issue efficiency, cache hit rates and DRAM throughput of the stage's
+    main kernel from the committed ncu summary (profiles/roofline_traffic.txt:
+    lines "counters stage kernel l2 l1 issue warps dram"), or None."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "roofline_traffic.txt")) as f:
+            for line in f:
+                p = line.split()
+                if len(p) == 8 and p[0] == "counters" and p[1] == stage:
+                    return {"kernel": p[2], "l2_hit_pct": float(p[3]), "l1_hit_pct": float(p[4]),
+                            "issue_active_pct": float(p[5]), "warps_active_pct": float(p[6]),
+                            "dram_throughput_pct": float(p[7]), "source": "profiles/eval_config3_kernels_full.md"}
+    except (OSError, ValueError):
+        pass
+    return None
+
+
 def workload():
     from cuacd_b200 import workloads as W
     v, t = W.candidate_mesh()
@@ -499,7 +516,7 @@ def main():
         achieved = alg[names[dom]] / (stage_ms[dom] / 1000.0) / 1e9
         return {"bound": "hbm", "kernel": names[dom], "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_source": peak_kind,
-                "traffic": ncu_traffic(names[dom], k),
+                "traffic": ncu_traffic(names[dom], k), "ncu_counters": ncu_counters(names[dom]),
                 "algorithmic_bytes": int(alg[names[dom]]), "planes": k,
                 "stage_ms": {kk: round(x, 4) for kk, x in zip(names, stage_ms)}}
 
