@@ -85,15 +85,29 @@ def ncu_counters(stage):
                 if len(p) == 8 and p[0] == "counters" and p[1] == stage:
                     return {"kernel": p[2], "l2_hit_pct": float(p[3]), "l1_hit_pct": float(p[4]),
                             "issue_active_pct": float(p[5]), "warps_active_pct": float(p[6]),
-                            "dram_throughput_pct": float(p[7]), "source": "profiles/eval_config3_kernels_full.md"}
+                            "dram_throughput_pct": float(p[7])}
     except (OSError, ValueError):
         pass
     return None
 
 
+def workloads():
+    """The seeded workload generators (cuacd_b200/workloads.py, plain numpy),
+    loaded by path: the reference arm must not import the package, whose
+    import maps this library's shared object into the process."""
+    import importlib.util
+    name = "_cuacd_workloads"
+    if name in sys.modules:
+        return sys.modules[name]
+    spec = importlib.util.spec_from_file_location(name, os.path.join(ROOT, "cuacd_b200", "workloads.py"))
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
 def workload():
-    from cuacd_b200 import workloads as W
-    v, t = W.candidate_mesh()
+    v, t = workloads().candidate_mesh()
     return v, t
 
 
@@ -168,7 +182,7 @@ def search_meshes():
     """Search sample: six ridged displaced spheres (UV 64x24, 96x32, 128x40
     and icospheres of 5,120-20,480 triangles), extent 2; their creases give
     the concave-edge planes the search ranks."""
-    from cuacd_b200 import workloads as W
+    W = workloads()
     out = [W.candidate_mesh(64, 24), W.candidate_mesh(96, 32, 0.35, seed=5), W.candidate_mesh(128, 40, 0.4, seed=7)]
     for lvl, amp, sd in ((4, 0.35, 1), (4, 0.45, 2), (5, 0.4, 3)):
         v, t = W.icosphere(lvl)
@@ -217,14 +231,17 @@ def search_leg(ctx, scorer, untrained):
     return out
 
 
+def config4_sample():
+    return workloads().batch_meshes(512, 500, 200_000, seed=3, select={i for i in range(512) if i % 16 in (0, 5)})
+
+
 def config4_leg(ctx, scorer):
     """Config 4 sample: the 64 meshes with index 0 or 5 mod 16 of the 512
     uneven synthetic meshes (500 to 200,000 triangles; displaced icospheres
     and unions of 2-6 boxes, seed 3), whole searches with config 4's
     parameters (tau 0.05, width 30/5, depth 2, 16 concave edges), exact and
     pruned; one untimed pass first."""
-    from cuacd_b200 import workloads as W
-    meshes = W.batch_meshes(512, 500, 200_000, seed=3, select={i for i in range(512) if i % 16 in (0, 5)})
+    meshes = config4_sample()
     kw = dict(width=30, width2=5, depth=2, threshold=0.05, max_iters=100, n_concave_edges=16)
     out = {}
     for name, extra in (("exact", {}), ("pruned", {"scorer": scorer, "top_k": SEARCH_TOP_K, "beam": SEARCH_BEAM})):
@@ -240,40 +257,85 @@ def config4_leg(ctx, scorer):
     return out
 
 
+def oracle_planes(v, t):
+    """The same 30 planes as the library's GPU generator, from the oracle
+    (the GPU path is bit-exact to it)."""
+    from oracle import oracle as O
+    return np.ascontiguousarray(np.concatenate(
+        [O.concave_planes(v, t, 16, 0.005, 3.49)[:N_EDGE],
+         np.stack([O.axis_plane(v, WIDTH, i, 0.0125) for i in range(WIDTH)])]).astype(np.float32))
+
+
 def cpu_baseline(v, t, planes, budget_s=20.0):
-    """Oracle port on all host cores over a bounded sample of the workload."""
+    """Oracle port on all host cores over a bounded sample of the workload:
+    whole 30-plane steps until about budget_s/2 seconds have passed."""
     from oracle import oracle as O
     cores = os.cpu_count() or 1
-    n = min(len(planes), max(cores, 8))
     t0 = time.perf_counter()
     done = 0
     while True:
-        O.eval_candidates(v, t, planes[:n], hausdorff=True, threads=cores)
-        done += n
+        O.eval_candidates(v, t, planes, hausdorff=True, threads=cores)
+        done += len(planes)
         if time.perf_counter() - t0 > budget_s * 0.5 or done >= 4 * len(planes):
             break
     dt = time.perf_counter() - t0
     return {"value": done / dt, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"{done} candidates ({n} planes per pass) of the same workload, "
+            "sample": f"{done} candidates ({len(planes)} planes per step) of the same workload, "
                       f"oracle (FP64/exact C) with {cores} threads"}
 
 
+def cpu_hull_baseline(clouds, budget_s=10.0):
+    """Oracle hulls (exact int64 on the quantised grid) of the config-1
+    clouds on all host cores (one cloud per thread; ctypes releases the GIL)."""
+    from concurrent.futures import ThreadPoolExecutor
+    from oracle import oracle as O
+    cores = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    done = 0
+    with ThreadPoolExecutor(cores) as ex:
+        while True:
+            list(ex.map(O.hull, clouds))
+            done += len(clouds)
+            if time.perf_counter() - t0 > budget_s * 0.5:
+                break
+    dt = time.perf_counter() - t0
+    return {"value": done / dt, "unit": "clouds/s", "cores": cores, "kind": "port",
+            "sample": f"{done} clouds of 1,000 points (the config-1 batch, whole passes), oracle with {cores} threads"}
+
+
+def cpu_hausdorff_baseline(a, b, total=20000):
+    """Oracle Hausdorff (FP64, brute force nearest triangle) of the config-2
+    pair on all host cores, `total` samples per direction."""
+    from oracle import oracle as O
+    cores = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    O.hausdorff(*a, *b, total=total, threads=cores)
+    dt = time.perf_counter() - t0
+    return {"value": 2 * total / dt, "unit": "samples/s", "cores": cores, "kind": "port",
+            "sample": f"{total} samples per direction (of the 10^6 of a step), oracle with {cores} threads"}
+
+
 def run_reference(args, rank, world):
+    """The reference arm.  The reference implements this path only in CUDA
+    (its CPU baselines need sources absent from its tree), so the line's
+    value is the oracle port of the path (the reference's algorithm in
+    FP64/exact C) on all host cores, on the same 30 planes of the same mesh.
+    The reference's own GPU path, built unmodified from its sources into
+    oracle/_ref, is timed beside it in a child process (its own extension
+    loaded, nothing of this library) under "reference_gpu"."""
     if rank != 0:
         return
     from oracle import oracle as O
     v, t = workload()
-    planes = np.ascontiguousarray(np.concatenate(
-        [O.concave_planes(v, t, 16, 0.005, 3.49)[:N_EDGE],
-         np.stack([O.axis_plane(v, WIDTH, i, 0.0125) for i in range(WIDTH)])]).astype(np.float32))
+    planes = oracle_planes(v, t)
+    n = len(planes)
     cores = os.cpu_count() or 1
-    n = min(len(planes), max(cores, 8))
     for _ in range(args.warmup):
-        O.eval_candidates(v, t, planes[:n], hausdorff=True, threads=cores)
+        O.eval_candidates(v, t, planes, hausdorff=True, threads=cores)
     times = []
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        O.eval_candidates(v, t, planes[:n], hausdorff=True, threads=cores)
+        O.eval_candidates(v, t, planes, hausdorff=True, threads=cores)
         times.append(time.perf_counter() - t0)
     total = sum(times)
     val = n * args.steps / total
@@ -282,9 +344,369 @@ def run_reference(args, rank, world):
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": config(n, v, t), "impl": "reference",
             "cpu_baseline": {"value": val, "unit": UNIT, "cores": cores, "kind": "port",
-                             "sample": f"{n} of the 30 planes per step, oracle with {cores} threads"},
+                             "sample": f"all {n} planes per step, oracle with {cores} threads"},
             "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if not args.no_reference_gpu:
+        line["reference_gpu"] = reference_gpu(args)
     print(json.dumps(line), flush=True)
+
+
+REF_DIR = os.path.join(ROOT, "oracle", "_ref")
+
+
+def reference_gpu(args):
+    """Run the reference's GPU legs in a child process; its JSON or why not."""
+    if not os.path.exists(os.path.join(REF_DIR, "_gpu.so")):
+        return {"unavailable": "the reference's GPU build (oracle/_ref) is absent"}
+    cmd = [sys.executable, os.path.abspath(__file__), "--ref-gpu-child", "--steps", str(args.steps),
+           "--warmup", str(args.warmup)]
+    if args.no_search:
+        cmd.append("--no-search")
+    try:
+        r = subprocess.run(cmd, capture_output=True, text=True, timeout=600)
+    except subprocess.TimeoutExpired:
+        return {"unavailable": "the reference's GPU legs ran past 600 s"}
+    lines = [x for x in r.stdout.splitlines() if x.startswith("{")]
+    if r.returncode != 0 or not lines:
+        return {"unavailable": f"reference GPU child exited {r.returncode}: {r.stderr.strip()[-300:]}"}
+    return json.loads(lines[-1])
+
+
+def load_ref_gpu():
+    """The reference's CPython extension (oracle/_ref/_gpu.so) with its
+    fatbin, initialised on device 0 as its Python wrapper does."""
+    import importlib.machinery
+    import importlib.util
+    loader = importlib.machinery.ExtensionFileLoader("_gpu", os.path.join(REF_DIR, "_gpu.so"))
+    spec = importlib.util.spec_from_loader("_gpu", loader)
+    g = importlib.util.module_from_spec(spec)
+    loader.exec_module(g)
+    with open(os.path.join(REF_DIR, "kernels.fatbin"), "rb") as f:
+        g.set_fatbin(f.read())
+    g.init(0, 0)
+    return g
+
+
+def _ref_hull_call(g, clouds, kdop):
+    """One call of the reference's hull entry point over a batch of clouds,
+    with the output caps its wrapper uses (cuacd/__init__.py:203-205,289-290)."""
+    n = len(clouds)
+    packed = np.ascontiguousarray(np.concatenate(clouds), np.float32)
+    off = np.zeros(n + 1, np.int32)
+    off[1:] = np.cumsum([len(c) for c in clouds])
+    if kdop:
+        mhv, mht = 4096, 8192
+    else:
+        mhv, mht = max(len(c) for c in clouds), max(max(2 * len(c) - 4 for c in clouds), 4)
+    ov = np.empty(n * mhv * 3, np.float32)
+    ot = np.empty(n * mht * 3, np.int32)
+    onv, ont, err = (np.empty(n, np.int32) for _ in range(3))
+    ovol = np.empty(n, np.float32)
+    if kdop:
+        g.kdop_hull(packed.ctypes.data, len(packed), off.ctypes.data, n, mhv, mht, ov.ctypes.data, ot.ctypes.data,
+                    onv.ctypes.data, ont.ctypes.data, ovol.ctypes.data, err.ctypes.data)
+    else:
+        g.hull_dandc(packed.ctypes.data, len(packed), off.ctypes.data, n, max(len(c) for c in clouds), mhv, mht,
+                     ov.ctypes.data, ot.ctypes.data, onv.ctypes.data, ont.ctypes.data, err.ctypes.data)
+    out = []
+    for i in range(n):
+        hv = ov[i * mhv * 3:(i * mhv + onv[i]) * 3].reshape(-1, 3)
+        ht = ot[i * mht * 3:(i * mht + ont[i]) * 3].reshape(-1, 3)
+        out.append((hv, ht, float(ovol[i])))
+    return out, err
+
+
+def _fp32_volume(v, t):
+    """The reference wrapper's host-side hull volume (cuacd/__init__.py:222-231)."""
+    a, b, c = v[t[:, 0]], v[t[:, 1]], v[t[:, 2]]
+    return abs(float(np.einsum("ij,ij->i", a, np.cross(b, c)).sum()) / 6.0)
+
+
+def _ref_eval_candidate(g, v, t, p, caps):
+    """One candidate through the reference's GPU entry points, the steps of
+    its la_expand/la_hull (cuda/la_expand.cu:65-424) plus the per-part
+    Hausdorff the full score needs: the cut with caps (test_plane_cut), the
+    k-DOP hull and volume of both fragments (one kdop_hull call), both
+    fragments' volumes (one batch_mesh_volume call), and the Hausdorff
+    distance of each fragment to its hull (two test_hausdorff calls)."""
+    pv, pt, nvv, ntt, vcap, tcap = caps
+    a, b, c, d = (float(x) for x in p)
+    n_pv, n_pt, n_nv, n_nt = g.test_plane_cut(v.ctypes.data, len(v), t.ctypes.data, len(t), a, b, c, d,
+                                              pv.ctypes.data, vcap, pt.ctypes.data, tcap,
+                                              nvv.ctypes.data, vcap, ntt.ctypes.data, tcap)
+    if n_pt == 0 or n_nt == 0:
+        return False
+    frags = [(pv[:3 * n_pv].reshape(-1, 3), pt[:3 * n_pt].reshape(-1, 3)),
+             (nvv[:3 * n_nv].reshape(-1, 3), ntt[:3 * n_nt].reshape(-1, 3))]
+    hulls, _ = _ref_hull_call(g, [f[0] for f in frags], kdop=True)
+    allv = np.ascontiguousarray(np.concatenate([f[0] for f in frags]))
+    allt = np.ascontiguousarray(np.concatenate([f[1] for f in frags]))
+    toff = np.array([0, n_pt, n_pt + n_nt], np.int32)
+    voff = np.array([0, n_pv, n_pv + n_nv], np.int32)
+    vols = np.empty(2, np.float32)
+    g.batch_mesh_volume(allv.ctypes.data, len(allv), allt.ctypes.data, len(allt), toff.ctypes.data,
+                        voff.ctypes.data, 2, vols.ctypes.data)
+    out = np.zeros(1, np.float32)
+    for (fv, ft), (hv, ht, _) in zip(frags, hulls):
+        fv, ft = np.ascontiguousarray(fv), np.ascontiguousarray(ft)
+        hv, ht = np.ascontiguousarray(hv), np.ascontiguousarray(ht)
+        g.test_hausdorff(hv.ctypes.data, len(hv), ht.ctypes.data, len(ht), fv.ctypes.data, len(fv),
+                         ft.ctypes.data, len(ft), out.ctypes.data)
+    return True
+
+
+def _ref_lookahead(g, v, t, n_edges):
+    """The reference's lookahead_decompose as its Python wrapper drives it
+    (cuacd/__init__.py:367-454): scipy hull of the input with outward
+    winding, then the extension call; returns the parts as arrays."""
+    import scipy.spatial
+    v = np.ascontiguousarray(v, np.float32)
+    t = np.ascontiguousarray(t, np.int32)
+    h = scipy.spatial.ConvexHull(v)
+    hv = np.ascontiguousarray(h.points, np.float32)
+    ht = np.ascontiguousarray(h.simplices, np.int32)
+    cen = hv.mean(0)
+    nrm = np.cross(hv[ht[:, 1]] - hv[ht[:, 0]], hv[ht[:, 2]] - hv[ht[:, 0]])
+    inward = (nrm * (hv[ht[:, 0]] - cen)).sum(1) < 0
+    ht[inward] = ht[inward][:, [0, 2, 1]]
+    raw = g.lookahead_decompose(v.ctypes.data, len(v), t.ctypes.data, len(t), hv.ctypes.data, len(hv),
+                                ht.ctypes.data, len(ht), 100, 30, 5, 0.05, 2, 0, 16, 0, 0,
+                                n_concave_edges=n_edges)
+    parts = []
+    for vb, tb, nv, nt, hvb, htb, hnv, hnt, _, _ in raw:
+        parts.append((np.frombuffer(vb, np.float32).reshape(nv, 3), np.frombuffer(tb, np.int32).reshape(nt, 3),
+                      np.frombuffer(hvb, np.float32).reshape(hnv, 3), np.frombuffer(htb, np.int32).reshape(hnt, 3)))
+    return parts
+
+
+def ref_gpu_child(args):
+    """The reference's own GPU path (built unmodified from its sources) on
+    the bench's workloads, through its CPython extension, wall clock per
+    call as its synchronous entry points return.  Prints one JSON line."""
+    from oracle import oracle as O
+    W = workloads()
+    g = load_ref_gpu()
+    out = {"build": "eliphatfs/cuacd sources, nvcc -O3 --use_fast_math sm_100 (its setup.py flags), "
+                    "run through its _gpu extension"}
+    # config 3: 30 candidates per step
+    v, t = workload()
+    v = np.ascontiguousarray(v, np.float32)
+    t = np.ascontiguousarray(t, np.int32)
+    planes = oracle_planes(v, t)
+    vcap, tcap = len(v) + 2 * len(t), 3 * len(t) + 64
+    caps = (np.empty(vcap * 3, np.float32), np.empty(tcap * 3, np.int32), np.empty(vcap * 3, np.float32),
+            np.empty(tcap * 3, np.int32), vcap, tcap)
+    for _ in range(args.warmup):
+        for p in planes:
+            _ref_eval_candidate(g, v, t, p, caps)
+    with Clocks(0) as clk:
+        times = []
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            ok = sum(_ref_eval_candidate(g, v, t, p, caps) for p in planes)
+            times.append(time.perf_counter() - t0)
+    out["config3"] = {"value": len(planes) * args.steps / sum(times), "unit": UNIT,
+                      "ms_per_step": 1000 * sum(times) / args.steps, "candidates_ok": int(ok),
+                      "steps": args.steps, "warmup": args.warmup, "clocks": clk.summary(),
+                      "workload": "the same 30 planes of the 40,960-tri sphere; per candidate test_plane_cut + "
+                                  "kdop_hull (both fragments) + batch_mesh_volume + 2 test_hausdorff"}
+    # config 1: 256 x 1,000-point clouds, batch_hull_volume's steps
+    clouds = W.hull_clouds(256, 1000, 0)
+    def c1():
+        hulls, _ = _ref_hull_call(g, clouds, kdop=False)
+        return [_fp32_volume(hv, ht) for hv, ht, _ in hulls]
+    for _ in range(args.warmup):
+        c1()
+    with Clocks(0) as clk:
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            c1()
+        dt = time.perf_counter() - t0
+    out["config1"] = {"value": len(clouds) * args.steps / dt, "unit": "clouds/s", "ms_per_step": 1000 * dt / args.steps,
+                      "clocks": clk.summary(),
+                      "workload": "256 x 1,000 uniform points (seed 0): hull_dandc + FP32 host volumes, "
+                                  "as its batch_hull_volume"}
+    # config 2: the 20,480-tri sphere against its hull, at the reference's
+    # own sample rule (HD_RESOLUTION 2000 is a plain #define in its source)
+    sv, st = W.hausdorff_sphere(level=5)
+    (hv, ht, _), = _ref_hull_call(g, [sv], kdop=False)[0]
+    hv, ht = np.ascontiguousarray(hv), np.ascontiguousarray(ht)
+    sv, st = np.ascontiguousarray(sv, np.float32), np.ascontiguousarray(st, np.int32)
+    n_samp = O.hd_sample_count(hv, ht) + O.hd_sample_count(sv, st)
+    res = np.zeros(1, np.float32)
+    def c2():
+        g.test_hausdorff(hv.ctypes.data, len(hv), ht.ctypes.data, len(ht), sv.ctypes.data, len(sv),
+                         st.ctypes.data, len(st), res.ctypes.data)
+    for _ in range(args.warmup):
+        c2()
+    with Clocks(0) as clk:
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            c2()
+        dt = time.perf_counter() - t0
+    out["config2"] = {"value": n_samp * args.steps / dt, "unit": "samples/s", "ms_per_step": 1000 * dt / args.steps,
+                      "samples_per_step": int(n_samp), "hausdorff": float(res[0]), "clocks": clk.summary(),
+                      "workload": "20,480-tri displaced icosphere (seed 1) vs its hull, both directions, "
+                                  "the reference's 2000-per-unit-area rule (its resolution is fixed in source)"}
+    if not args.no_search:
+        meshes = config4_sample()
+        for vv, tt in meshes[:4]:                    # untimed: the pools grow
+            _ref_lookahead(g, vv, tt, 16)
+        with Clocks(0) as clk:
+            t0 = time.perf_counter()
+            parts = [_ref_lookahead(g, vv, tt, 16) for vv, tt in meshes]
+            dt = time.perf_counter() - t0
+        out["config4"] = {"meshes_per_s": len(meshes) / dt, "s": dt, "parts": int(sum(len(p) for p in parts)),
+                          "parts_per_mesh": [len(p) for p in parts],
+                          "max_rv_cost": float(max(part_cost_max(p) for p in parts)), "clocks": clk.summary(),
+                          "workload": "the 64-mesh config-4 sample, tau 0.05, width 30/5, depth 2, 16 concave edges"}
+    g.destroy()
+    print(json.dumps(out), flush=True)
+
+
+def config1_leg(ctx, stream, flush, args):
+    """Config 1: exact hulls and volumes of 256 clouds x 1,000 uniform points
+    (seed 0) in one batch.  value: device-resident (cuacd_hull_batch_device,
+    inputs in HBM), CUDA events, L2 flushed before each step; e2e: the public
+    Context.batch_hull_volume with host arrays."""
+    import torch
+    import cuacd_b200
+    W = workloads()
+    clouds = W.hull_clouds(256, 1000, 0)
+    n, k = len(clouds), 1000
+    packed = np.ascontiguousarray(np.concatenate(clouds), np.float32)
+    off = np.arange(0, n * k + 1, k, dtype=np.int32)
+    mht = 2 * k - 4
+    d_pts = torch.from_numpy(packed.reshape(-1)).cuda()
+    d_off = torch.from_numpy(off).cuda()
+    d_v = torch.empty(n * k * 3, dtype=torch.float32, device="cuda")
+    d_t = torch.empty(n * mht * 3, dtype=torch.int32, device="cuda")
+    d_nv, d_nt, d_err = (torch.empty(n, dtype=torch.int32, device="cuda") for _ in range(3))
+    d_vol = torch.empty(n, dtype=torch.float32, device="cuda")
+    fn = cuacd_b200._fn("cuacd_hull_batch_device")
+    P = lambda x: ctypes.c_void_p(x.data_ptr())
+
+    def step():
+        rc = fn(ctx.handle, P(d_pts), P(d_off), n, k, k, mht, P(d_v), P(d_t), P(d_nv), P(d_nt), P(d_vol), P(d_err),
+                ctypes.c_void_p(stream.cuda_stream))
+        if rc:
+            raise RuntimeError(f"cuacd error {rc}")
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            step()
+        stream.synchronize()
+        if int(d_err.abs().sum()):
+            raise RuntimeError("config 1: hull errors")
+        l0 = ctx.launch_count()
+        ms = _timed(step, stream, flush, args.steps)
+        launches = ctx.launch_count() - l0
+    nv, nt = int(d_nv.sum()), int(d_nt.sum())
+    vols = d_vol.cpu().numpy()
+
+    def e2e():
+        ctx.batch_hull_volume(clouds)
+    for _ in range(args.warmup):
+        e2e()
+    tt = []
+    for _ in range(args.steps):
+        flush.zero_(); torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e2e()
+        tt.append(time.perf_counter() - t0)
+    alg = 12 * n * k + 12 * (nv + nt)
+    avg = sum(ms) / len(ms)
+    peak, peak_kind = peaks()
+    achieved = alg / (avg / 1000.0) / 1e9
+    out = {"value": n * args.steps / (sum(ms) / 1000.0), "unit": "clouds/s", "ms_per_step": avg,
+           "gpu_launches": int(launches),
+           "workload": "config1: 256 clouds x 1,000 float32 points uniform in [-1,1]^3 (seed 0), "
+                       "exact hull index sets + volumes, one batch per step",
+           "hull_verts": nv, "hull_tris": nt, "volume_sum": float(vols.sum()),
+           "roofline": {"bound": "hbm", "kernel": "hull_pipeline", "achieved": achieved, "peak": peak,
+                        "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
+                        "traffic": ncu_traffic("config1_hull", n), "algorithmic_bytes": int(alg)},
+           "e2e": {"value": n * args.steps / sum(tt), "unit": "clouds/s",
+                   "h2d_bytes_per_step": int(packed.nbytes + off.nbytes), "d2h_bytes_per_step": int(16 * n)}}
+    if not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_hull_baseline(clouds)
+    return out
+
+
+C2_SAMPLES = 10 ** 6
+
+
+def config2_leg(ctx, stream, flush, args):
+    """Config 2: sampled Hausdorff distance between the 20,480-triangle
+    displaced icosphere (seed 1) and its exact hull, 10^6 samples per
+    surface per direction.  value: device-resident
+    (cuacd_hausdorff_batch_device), samples/s over both directions, CUDA
+    events, L2 flushed; e2e: Context.hausdorff with host arrays.  Also timed
+    at the reference's own sample rule (2000 per unit area, min 1000)."""
+    import torch
+    import cuacd_b200
+    W = workloads()
+    sv, st = W.hausdorff_sphere(level=5)
+    (hv, ht, _), = ctx.batch_hull_dandc_mesh([sv])
+    a = (np.ascontiguousarray(hv, np.float32), np.ascontiguousarray(ht, np.int32))
+    b = (np.ascontiguousarray(sv, np.float32), np.ascontiguousarray(st, np.int32))
+    dav, dat = torch.from_numpy(a[0].reshape(-1)).cuda(), torch.from_numpy(a[1].reshape(-1)).cuda()
+    dbv, dbt = torch.from_numpy(b[0].reshape(-1)).cuda(), torch.from_numpy(b[1].reshape(-1)).cuda()
+    avo = np.array([0, len(a[0])], np.int32); ato = np.array([0, len(a[1])], np.int32)
+    bvo = np.array([0, len(b[0])], np.int32); bto = np.array([0, len(b[1])], np.int32)
+    d_out = torch.zeros(1, dtype=torch.float32, device="cuda")
+    fn = cuacd_b200._fn("cuacd_hausdorff_batch_device")
+    P = lambda x: ctypes.c_void_p(x.data_ptr())
+    H = lambda x: ctypes.c_void_p(x.ctypes.data)
+
+    def run(total):
+        def step():
+            rc = fn(ctx.handle, 1, P(dav), H(avo), P(dat), H(ato), P(dbv), H(bvo), P(dbt), H(bto),
+                    2000.0, 1000, total, P(d_out), ctypes.c_void_p(stream.cuda_stream))
+            if rc:
+                raise RuntimeError(f"cuacd error {rc}")
+        with torch.cuda.stream(stream):
+            for _ in range(args.warmup):
+                step()
+            stream.synchronize()
+            l0 = ctx.launch_count()
+            ms = _timed(step, stream, flush, args.steps)
+            return ms, ctx.launch_count() - l0, float(d_out.item())
+
+    ms, launches, h = run(C2_SAMPLES)
+    n_samp = 2 * C2_SAMPLES
+    ms_rule, _, h_rule = run(0)
+
+    def e2e():
+        ctx.hausdorff(*a, *b, total=C2_SAMPLES)
+    for _ in range(args.warmup):
+        e2e()
+    tt = []
+    for _ in range(args.steps):
+        flush.zero_(); torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e2e()
+        tt.append(time.perf_counter() - t0)
+    avg = sum(ms) / len(ms)
+    alg = 12 * (len(a[0]) + len(a[1]) + len(b[0]) + len(b[1]))
+    peak, peak_kind = peaks()
+    achieved = alg / (avg / 1000.0) / 1e9
+    out = {"value": n_samp * args.steps / (sum(ms) / 1000.0), "unit": "samples/s", "ms_per_step": avg,
+           "gpu_launches": int(launches), "hausdorff": h,
+           "workload": "config2: 20,480-tri displaced icosphere (radius 1+0.25*sum of 8 sines, seed 1) vs its "
+                       "exact hull, 10^6 samples per surface, both directions",
+           "roofline": {"bound": "hbm", "kernel": "k_hd_prep+k_hd_query", "achieved": achieved, "peak": peak,
+                        "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
+                        "traffic": None, "algorithmic_bytes": int(alg),
+                        "note": "the samples are generated on chip: the meshes are the only bytes, so the "
+                                "query is issue/latency-bound, not HBM-bound"},
+           "e2e": {"value": n_samp * args.steps / sum(tt), "unit": "samples/s",
+                   "h2d_bytes_per_step": int(sum(x.nbytes for x in a + b)), "d2h_bytes_per_step": 4},
+           "reference_rule": {"ms_per_step": sum(ms_rule) / len(ms_rule), "hausdorff": h_rule,
+                              "note": "2000 samples per unit area, min 1000 (cuda/hausdorff.cuh:380-382)"}}
+    if not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_hausdorff_baseline(a, b)
+    return out
 
 
 def replica_max(totals, dist, device):
@@ -340,8 +762,14 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-search", action="store_true", help="skip the whole-search comparison")
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="reference arm: skip the reference's own GPU legs")
+    ap.add_argument("--ref-gpu-child", action="store_true", help=argparse.SUPPRESS)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.ref_gpu_child:
+        ref_gpu_child(args)
+        return
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -534,6 +962,8 @@ def main():
                       "ms_per_step": tot_exact_ms / args.steps, "gpu_launches": int(l1 - l0),
                       "e2e": replica_rate(world_n, n * args.steps, e2e_exact_s),
                       "roofline": roofline(stage_exact, exact, np.ones(n, bool))}}
+    line["config1"] = config1_leg(ctx, stream, flush, args)
+    line["config2"] = config2_leg(ctx, stream, flush, args)
     if not args.no_search:
         with S.Scorer.load(ctx, S.RV_WEIGHTS_PATH) as rv, S.Scorer(ctx, seed=1) as raw:
             line["search"] = search_leg(ctx, rv, raw)

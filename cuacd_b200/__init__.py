@@ -148,7 +148,7 @@ def _as_i32(a):
 
 
 def _ptr(a):
-    return ctypes.c_void_p(a.ctypes.data)
+    return ctypes.c_void_p(None if a is None else a.ctypes.data)
 
 
 class Context:
@@ -247,15 +247,16 @@ class Context:
         np.cumsum([len(a) for a in arrs], out=off[1:])
         return arrs, packed, off
 
-    def _hull(self, pts_list, max_hv=None, max_ht=None):
+    def _hull(self, pts_list, max_hv=None, max_ht=None, meshes=True):
         arrs, packed, off = self._pack(pts_list)
         n = len(arrs)
         ns = [len(a) for a in arrs]
         max_pts = max(ns)
         max_hv = max_pts if max_hv is None else max_hv
         max_ht = max(max(2 * k - 4 for k in ns), 4) if max_ht is None else max_ht
-        ov = np.empty(n * max(max_hv, 1) * 3, np.float32)
-        ot = np.empty(n * max(max_ht, 1) * 3, np.int32)
+        # volumes only: the hull meshes stay on the device (no copy back)
+        ov = np.empty(n * max(max_hv, 1) * 3, np.float32) if meshes else None
+        ot = np.empty(n * max(max_ht, 1) * 3, np.int32) if meshes else None
         onv = np.empty(n, np.int32)
         ont = np.empty(n, np.int32)
         vol = np.empty(n, np.float32)
@@ -270,7 +271,7 @@ class Context:
         `algo` is accepted for compatibility and ignored."""
         if len(pts_list) == 0:
             return np.empty(0, np.float32), np.empty(0, np.int32)
-        _, _, onv, ont, vol, err, _, _ = self._hull(pts_list)
+        _, _, onv, ont, vol, err, _, _ = self._hull(pts_list, meshes=False)
         vol = np.where((onv > 0) & (ont > 0), vol, 0.0).astype(np.float32)
         return vol, err
 

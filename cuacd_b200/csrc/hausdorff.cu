@@ -465,6 +465,7 @@ extern "C" int cuacd_hausdorff_batch_device(gpu_ctx_t ctx, int n_pairs,
 // that first call before any stream capture.
 // ---------------------------------------------------------------------------
 #define CUACD_HD_NOALLOC_BYTES (32ull << 20)
+#define CUACD_HD_NOALLOC_MAX_TRIS (1 << 20)
 static __device__ __align__(256) char g_hd_noalloc_scratch[CUACD_HD_NOALLOC_BYTES];
 
 // Layout of the static block: [Arena | 2 HDSurf | 2 HDPrep | 2 HDDir |
@@ -488,6 +489,35 @@ __global__ void k_hd_noalloc_setup(char* base, const float* av, int anv, const i
     M[0] = 0.f; M[1] = 0.f;
 }
 
+// Every triangle index must lie in [0, nv).  The allocating entry points
+// check this on the host; here the indices are device memory, so a grid scan
+// does it: a surface with a bad index gets the error word set and its
+// triangle count zeroed before any kernel reads through its indices.
+__global__ void k_hd_noalloc_check(char* base, const int* at, int ant, int anv, const int* bt, int bnt, int bnv)
+{
+    HDSurf* S = (HDSurf*)(base + 256);
+    int* I = (int*)(base + 1024);
+    const long long na = 3ll * ant, n = na + 3ll * bnt;
+    for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+        const bool in_a = k < na;
+        const int x = in_a ? at[k] : bt[k - na];
+        if (x < 0 || x >= (in_a ? anv : bnv)) {
+            atomicOr(&I[2], KERR_MESH_INVALID);
+            S[in_a ? 0 : 1].nt = 0;
+        }
+    }
+}
+
+// sqrt of the pair's squared maximum, or NaN when any kernel of the call set
+// the error word (bad index, scratch overflow): never a silent 0.
+__global__ void k_hd_noalloc_finish(const char* base, float* out)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const int err = ((const int*)(base + 1024))[2];
+    const float m = ((const float*)(base + 1088))[0];
+    *out = err ? __int_as_float(0x7fc00000) : sqrtf(m);
+}
+
 static char* g_noalloc_base[64];
 static std::mutex g_noalloc_mu;
 
@@ -497,6 +527,9 @@ extern "C" int cuacd_hausdorff_noalloc(const float* d_av, int anv, const int* d_
                                        float* d_out, void* stream)
 {
     if (anv < 0 || ant < 0 || bnv < 0 || bnt < 0 || !d_out) return CUACD_NOALLOC_BAD_ARGS;
+    // No surface above this many triangles can fit the block; rejecting them
+    // first keeps the sizing arithmetic below far from int overflow.
+    if (ant > CUACD_HD_NOALLOC_MAX_TRIS || bnt > CUACD_HD_NOALLOC_MAX_TRIS) return CUACD_NOALLOC_TOO_LARGE;
     size_t need = NOALLOC_HDR + hd_prep_bytes(ant) + hd_prep_bytes(bnt) + 8 * 256;
     if (need > CUACD_HD_NOALLOC_BYTES) return CUACD_NOALLOC_TOO_LARGE;
     int dev = 0;
@@ -520,6 +553,11 @@ extern "C" int cuacd_hausdorff_noalloc(const float* d_av, int anv, const int* d_
     cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
     cudaStream_t s = (cudaStream_t)stream;
     k_hd_noalloc_setup<<<1, 32, 0, s>>>(base, d_av, anv, d_at, ant, d_bv, bnv, d_bt, bnt);
+    if (ant + bnt > 0) {
+        const long long n = 3ll * ((long long)ant + bnt);
+        const int blocks = (int)std::min<long long>((n + 255) / 256, 4ll * (n_sm > 0 ? n_sm : 148));
+        k_hd_noalloc_check<<<blocks, 256, 0, s>>>(base, d_at, ant, anv, d_bt, bnt, bnv);
+    }
     HDSurf* surfs = (HDSurf*)(base + 256);
     HDPrep* preps = (HDPrep*)(base + 384);
     void* dirs = (void*)(base + 768);
@@ -527,7 +565,7 @@ extern "C" int cuacd_hausdorff_noalloc(const float* d_av, int anv, const int* d_
     float* pmax = (float*)(base + 1088);
     launch_hausdorff_pairs(surfs, 1, (Arena*)base, resolution, min_samples, total, preps, dirs, i4, pmax, i4 + 2,
                            n_sm > 0 ? n_sm : 148, s);
-    launch_hd_sqrt(pmax, 1, d_out, 1, s);
+    k_hd_noalloc_finish<<<1, 32, 0, s>>>(base, d_out);
     e = cudaGetLastError();
     return e == cudaSuccess ? 0 : (int)e;
 }

@@ -179,8 +179,10 @@ static __device__ __forceinline__ unsigned hd_expand10(unsigned v)
 }
 
 __host__ __device__ inline int hd_nleaf(int nt) { int l = (nt + HD_LEAF - 1) / HD_LEAF; return l < 1 ? 1 : l; }
-__host__ __device__ inline int hd_P(int nt) { int l = hd_nleaf(nt); int p = 1; while (p < l) p <<= 1; return p; }
-__host__ __device__ inline int hd_keycap(int nt) { int p = 1; while (p < nt) p <<= 1; return p; }
+// Powers of two stop at 2^30: an int shift past it would wrap to zero and the
+// loop would never end.  Callers bound nt far below that before sizing.
+__host__ __device__ inline int hd_P(int nt) { int l = hd_nleaf(nt); int p = 1; while (p < l && p < (1 << 30)) p <<= 1; return p; }
+__host__ __device__ inline int hd_keycap(int nt) { int p = 1; while (p < nt && p < (1 << 30)) p <<= 1; return p; }
 
 // Scratch bytes for one surface's prep.
 __host__ __device__ inline size_t hd_prep_bytes(int nt)

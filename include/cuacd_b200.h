@@ -241,11 +241,18 @@ int cuacd_hausdorff_batch_device(gpu_ctx_t ctx, int n_pairs,
  * does not synchronise.  Scratch is a static 32 MiB device array held by
  * every GPU that loads this library until exit; all calls share it, so calls
  * whose work overlaps on the GPU race.  The first call on a device looks up
- * the array's device address; make it before any stream capture.  Returns 0,
+ * the array's device address and keeps it for the life of the process;
+ * make that first call before any stream capture, and do not use the entry
+ * point on a device after cudaDeviceReset (the kept address is stale).
+ * Every triangle index must lie in [0, nv) of its surface; a device-side scan
+ * checks this before any kernel reads through the indices.  Returns 0,
  * CUACD_NOALLOC_TOO_LARGE when the two surfaces' prep data would not fit
  * (two surfaces of up to 161,000 triangles each fit; the exact test is the
- * sum of both surfaces' per-triangle prep sizes), CUACD_NOALLOC_BAD_ARGS, or
- * a CUDA error code. */
+ * sum of both surfaces' per-triangle prep sizes; more than 2^20 triangles on
+ * a surface is refused before any sizing), CUACD_NOALLOC_BAD_ARGS, or a CUDA
+ * error code.  A failure found on the device (an index out of range, scratch
+ * overflow) cannot be returned by a call that does not synchronise: *d_out
+ * is then NaN, never a distance. */
 #define CUACD_NOALLOC_TOO_LARGE (-2)
 #define CUACD_NOALLOC_BAD_ARGS  (-3)
 int cuacd_hausdorff_noalloc(const float* d_a_verts, int a_nv,

@@ -20,7 +20,8 @@ def build():
     own GPU path into oracle/_ref with Makefile.ref where the reference tree
     is present (it skips itself otherwise)."""
     subprocess.run(["make", "-s", "-C", _HERE], check=True)
-    subprocess.run(["make", "-s", "-j8", "-C", _HERE, "-f", "Makefile.ref"], check=True)
+    ref = os.environ.get("CUACD_REFERENCE_TREE", "/root/reference")
+    subprocess.run(["make", "-s", "-j8", "-C", _HERE, "-f", "Makefile.ref", f"REF={ref}"], check=True)
 
 
 class CandResult(ctypes.Structure):
@@ -134,6 +135,13 @@ def hd_samples(verts, tris, resolution=2000.0, min_samples=1000, total=0):
     lib().orc_hd_samples(v.ctypes.data, len(v), t.ctypes.data, len(t),
                          resolution, min_samples, total, out.ctypes.data, n)
     return out[:n]
+
+
+def hd_sample_count(verts, tris, resolution=2000.0, min_samples=1000, total=0):
+    """Samples the reference's rule draws on one surface (cuda/hausdorff.cuh:380-382)."""
+    v, t = _f32(verts), _i32(tris)
+    return int(lib().orc_hd_sample_count(v.ctypes.data, len(v), t.ctypes.data, len(t),
+                                         resolution, min_samples, total))
 
 
 def hausdorff(av, at, bv, bt, resolution=2000.0, min_samples=1000, total=0, threads=1):

@@ -9,7 +9,7 @@ need either).
   hausdorff_ref.npz   the reference's golden Hausdorff pairs and CoACD values
                       (tests/data/hausdorff_coacd_ref.npz in the reference).
 
-usage: python tests/golden/make_golden.py [path/to/reference]
+usage: python tests/golden/make_golden.py path/to/reference
 """
 import os
 import sys
@@ -63,7 +63,9 @@ def clouds():
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) < 2:
+        sys.exit("usage: make_golden.py <path of the reference tree>")
+    ref = sys.argv[1]
     cl, names = clouds()
     rec = {"names": np.array(names)}
     for i, c in enumerate(cl):
