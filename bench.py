@@ -244,13 +244,31 @@ def config4_leg(ctx, scorer):
     meshes = config4_sample()
     kw = dict(width=30, width2=5, depth=2, threshold=0.05, max_iters=100, n_concave_edges=16)
     out = {}
+    per_mesh = {}
     for name, extra in (("exact", {}), ("pruned", {"scorer": scorer, "top_k": SEARCH_TOP_K, "beam": SEARCH_BEAM})):
         for v, t in meshes:
             ctx.lookahead_decompose(v, t, **kw, **extra)
         t0 = time.perf_counter()
         parts = [ctx.lookahead_decompose(v, t, **kw, **extra) for v, t in meshes]
         dt = time.perf_counter() - t0
+        per_mesh[name] = parts
         out[name] = {"meshes_per_s": len(meshes) / dt, "s": dt, "parts": int(sum(len(p) for p in parts)),
+                     "parts_per_mesh": [len(p) for p in parts],
+                     "max_rv_cost": float(max(part_cost_max(p) for p in parts))}
+    # the same searches as one batch (cuacd_lookahead_decompose_batch): the
+    # levels of all 64 meshes share their launches; the parts must be the
+    # per-mesh calls' parts
+    for name, extra in (("batch_exact", {}),
+                        ("batch_pruned", {"scorer": scorer, "top_k": SEARCH_TOP_K, "beam": SEARCH_BEAM})):
+        ctx.lookahead_decompose_batch(meshes[:8], **kw, **extra)
+        t0 = time.perf_counter()
+        parts = ctx.lookahead_decompose_batch(meshes, **kw, **extra)
+        dt = time.perf_counter() - t0
+        ref = per_mesh[name.split("_")[1]]
+        same = all(len(a) == len(b) and all(np.array_equal(x, y) for pa, pb in zip(a, b) for x, y in zip(pa, pb))
+                   for a, b in zip(parts, ref))
+        out[name] = {"meshes_per_s": len(meshes) / dt, "s": dt, "parts": int(sum(len(p) for p in parts)),
+                     "same_parts_as_per_mesh_calls": bool(same), "stats": list(ctx.last_search_stats),
                      "max_rv_cost": float(max(part_cost_max(p) for p in parts))}
     out["workload"] = (f"config 4 sample: {len(meshes)} of the 512 meshes (index 0 or 5 mod 16), "
                        f"{min(len(t) for _, t in meshes)}-{max(len(t) for _, t in meshes)} tris")

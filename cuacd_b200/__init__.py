@@ -103,6 +103,9 @@ _opt("cuacd_lookahead_trace", _I, [_P, _P, _P, _I, _P, _P, _I, _P, _I, _P, _I, _
 _opt("cuacd_lookahead_decompose_pruned", _I, [_P, _P, _I, _F, _I, _P, _P, _I, _P, _I, _P, _I, _P, _I,
                                               _I, _I, _I, _F, _I, _I, _I, _I, _I, _I, _F, _F, _I,
                                               ctypes.POINTER(GpuResult)])
+_opt("cuacd_lookahead_decompose_batch", _I, [_P, _I, _P, _P, _P, _P, _P, _P, _P, _P,
+                                             _I, _I, _I, _F, _I, _I, _I, _I, _I, _I, _I, _F, _F, _I, _I, _I,
+                                             _P, _I, _F, _I, _P, _P])
 _opt("cuacd_candidate_planes", _I, [_P, _P, _I, _P, _I, _I, _F, _F, _I, _F, _P, _P, _P])
 _opt("cuacd_profile_stages", _I, [_P, _I])
 _opt("cuacd_stage_times", _I, [_P, _P])
@@ -457,18 +460,80 @@ class Context:
                            int(not no_decompose_components_per_iter), int(n_concave_edges), float(concave_eps),
                            float(concave_threshold), int(concave_iters), ctypes.byref(res)))
             self.last_prune_stats = (int(st[0]), int(st[1]), int(st[2]))
+        return _take_parts(res)
+
+    def lookahead_decompose_batch(self, meshes, *, max_iters=100, width=60, width2=5, threshold=0.05,
+                                  depth=2, quick_depth=0, max_n_cutting=16, verbose=0,
+                                  decompose_components=False, no_decompose_components_per_iter=False,
+                                  n_concave_edges=32, concave_eps=0.005, concave_threshold=3.49,
+                                  concave_iters=10, merge_hulls=False, branch_and_bound=True,
+                                  scorer=None, top_k=8, margin=0.0, beam=0):
+        """lookahead_decompose of every (verts, tris) of `meshes` in one
+        search whose levels share their launches -> one part list per mesh,
+        each equal to what lookahead_decompose of that mesh alone returns
+        (the same scorer / top_k / margin / beam pruning when given).
+        `self.last_search_stats`: level-0 planes ranked, planes cut, level-0
+        cuts expanded, fragment hulls built, items cut off by the
+        branch-and-bound, iterations run."""
+        if len(meshes) == 0:
+            return []
+        total_width = width + 4 * n_concave_edges
+        if total_width >= 512:
+            raise ValueError(f"width + 4*n_concave_edges must be < 512 (got {total_width})")
+        vs = [_as_f32(v).reshape(-1, 3) for v, _ in meshes]
+        ts = [_as_i32(t).reshape(-1, 3) for _, t in meshes]
+        hulls = self.batch_hull_dandc_mesh(vs)
+        hvs = [_as_f32(h[0]).reshape(-1, 3) for h in hulls]
+        hts = [_as_i32(h[1]).reshape(-1, 3) for h in hulls]
+
+        def pack(arrs, dtype):
+            off = np.zeros(len(arrs) + 1, np.int32)
+            np.cumsum([len(a) for a in arrs], out=off[1:])
+            cat = np.ascontiguousarray(np.concatenate(arrs).astype(dtype, copy=False)) if arrs else np.zeros((0, 3), dtype)
+            return cat, off
+
+        V, Vo = pack(vs, np.float32)
+        T, To = pack(ts, np.int32)
+        HV, HVo = pack(hvs, np.float32)
+        HT, HTo = pack(hts, np.int32)
+        n = len(meshes)
+        res = (GpuResult * n)()
+        st = (ctypes.c_ulonglong * 8)()
+        fn = _fn("cuacd_lookahead_decompose_batch")
+        self._check(fn(self._h, n, _ptr(V), _ptr(Vo), _ptr(T), _ptr(To), _ptr(HV), _ptr(HVo), _ptr(HT), _ptr(HTo),
+                       int(max_iters), int(width), int(width2), float(threshold), int(depth), int(quick_depth),
+                       int(max_n_cutting), int(verbose), int(bool(decompose_components)),
+                       int(not no_decompose_components_per_iter), int(n_concave_edges), float(concave_eps),
+                       float(concave_threshold), int(concave_iters), int(bool(merge_hulls)),
+                       int(bool(branch_and_bound)), scorer._h if scorer is not None else None, int(top_k),
+                       float(margin), int(beam), ctypes.cast(st, ctypes.c_void_p),
+                       ctypes.cast(res, ctypes.c_void_p)))
+        self.last_search_stats = tuple(int(x) for x in st[:6])
         out = []
         try:
-            for i in range(res.nparts):
-                p = res.parts[i]
-                v = np.ctypeslib.as_array(p.verts, (p.nv * 3,)).reshape(p.nv, 3).copy() if p.nv else np.zeros((0, 3), np.float32)
-                t = np.ctypeslib.as_array(p.tris, (p.nt * 3,)).reshape(p.nt, 3).copy() if p.nt else np.zeros((0, 3), np.int32)
-                hv_ = np.ctypeslib.as_array(p.hull_verts, (p.hull_nv * 3,)).reshape(p.hull_nv, 3).copy() if p.hull_nv else np.zeros((0, 3), np.float32)
-                ht_ = np.ctypeslib.as_array(p.hull_tris, (p.hull_nt * 3,)).reshape(p.hull_nt, 3).copy() if p.hull_nt else np.zeros((0, 3), np.int32)
-                out.append((v, t, hv_, ht_))
+            for i in range(n):
+                out.append(_take_parts(res[i], free=False))
         finally:
-            _fn("gpu_result_free")(ctypes.byref(res))
+            for i in range(n):
+                _fn("gpu_result_free")(ctypes.byref(res[i]))
         return out
+
+
+def _take_parts(res, free=True):
+    """Copy a gpu_result's parts into numpy arrays (and free it)."""
+    out = []
+    try:
+        for i in range(res.nparts):
+            p = res.parts[i]
+            v = np.ctypeslib.as_array(p.verts, (p.nv * 3,)).reshape(p.nv, 3).copy() if p.nv else np.zeros((0, 3), np.float32)
+            t = np.ctypeslib.as_array(p.tris, (p.nt * 3,)).reshape(p.nt, 3).copy() if p.nt else np.zeros((0, 3), np.int32)
+            hv_ = np.ctypeslib.as_array(p.hull_verts, (p.hull_nv * 3,)).reshape(p.hull_nv, 3).copy() if p.hull_nv else np.zeros((0, 3), np.float32)
+            ht_ = np.ctypeslib.as_array(p.hull_tris, (p.hull_nt * 3,)).reshape(p.hull_nt, 3).copy() if p.hull_nt else np.zeros((0, 3), np.int32)
+            out.append((v, t, hv_, ht_))
+    finally:
+        if free:
+            _fn("gpu_result_free")(ctypes.byref(res))
+    return out
 
 
 def cand_to_dict(r):

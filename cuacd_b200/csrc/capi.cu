@@ -60,6 +60,17 @@ extern "C" int gpu_init(gpu_ctx_t* out, int device_ordinal, size_t pool_bytes)
         cudaFree(ctx->d_arena); cudaStreamDestroy(ctx->stream); free(ctx); return (int)e;
     }
     ctx->cap = want;
+    cudaMemPoolProps props;
+    memset(&props, 0, sizeof(props));
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    e = cudaMemPoolCreate(&ctx->parts_pool, &props);
+    if (e != cudaSuccess) {
+        cudaFree(ctx->pool); cudaFree(ctx->d_arena); cudaStreamDestroy(ctx->stream); free(ctx); return (int)e;
+    }
+    unsigned long long keep = ~0ull;
+    cudaMemPoolSetAttribute(ctx->parts_pool, cudaMemPoolAttrReleaseThreshold, &keep);
     *out = ctx;
     return 0;
 }
@@ -77,6 +88,7 @@ extern "C" void gpu_destroy(gpu_ctx_t ctx)
     }
     if (ctx->fork_ev) cudaEventDestroy(ctx->fork_ev);
     cudaStreamDestroy(ctx->stream);
+    if (ctx->parts_pool) cudaMemPoolDestroy(ctx->parts_pool);
     free(ctx);
 }
 

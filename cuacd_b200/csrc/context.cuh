@@ -32,6 +32,9 @@ struct gpu_ctx {
     int            eval_groups;        // plane groups evaluated concurrently (0: default)
     cudaStream_t   aux[3];             // streams of groups 1..3 (created on first use)
     cudaEvent_t    fork_ev, join_ev[3];
+    cudaMemPool_t  parts_pool;         // stream-ordered allocations of search parts; keeps what it
+                                       // reserved (release threshold: never), so a search does not
+                                       // return memory to the driver at every synchronisation
     char           last_error[256];
 };
 

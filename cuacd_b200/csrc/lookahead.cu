@@ -29,11 +29,18 @@
 // Cuts and hulls run as device jobs in waves: fragments and hulls go to an
 // output arena kept for the iteration, scratch to a second arena reset
 // between waves.
-// The branch-and-bound pruning of the last level (la_hull's rough-hull bound)
-// only skips provably dominated items and is not needed for the result; the
-// quick levels (quick_depth) are not part of this engine and are ignored.
+//   4b. `quick_depth` quick levels after the full ones (la_expand_quick,
+//      la_refine.cu:52-351): each item's worst part is cut at its box midpoint
+//      on the three axes and the most even volume split makes its one child;
+//   4c. branch and bound on the last level (la_compute_best_ub + la_hull's
+//      rough-hull bound, la_expand.cu:380-457): an item whose new fragment's
+//      rough hull (exact hull of its extreme points along 40 directions)
+//      already leaves a volume gap too large to beat the best path bound of
+//      its cutting part gets no exact hulls and is not evaluated.
 // merge_hulls runs the merge-hulls post-pass (merge_hulls_pass) after the
-// last iteration.
+// last iteration.  A batch of meshes runs as one search whose levels share
+// their launches (cuacd_lookahead_decompose_batch); every choice is per part,
+// so each mesh's parts are those of a search of that mesh alone.
 #include <vector>
 #include <algorithm>
 #include <chrono>
@@ -82,7 +89,13 @@ static __device__ void cut_job_plane(const CutJob& J, float min_edge_dist, float
                              (s_hi[1] - s_lo[1] <= 2.f * min_edge_dist + eps) &&
                              (s_hi[2] - s_lo[2] <= 2.f * min_edge_dist + eps);
             if (all_small) *s_flags = CUT_FLAG_SMALL | CUT_FLAG_NOPLANE;
-            else {
+            else if (J.cpa < 0) {       // quick level: the box midpoint (la_expand_quick, cuda/la_refine.cu:151-159)
+                if (s_hi[J.axis] - s_lo[J.axis] <= 2.f * min_edge_dist + eps) *s_flags = CUT_FLAG_NOPLANE;
+                else {
+                    const float mid = (s_lo[J.axis] + s_hi[J.axis]) * 0.5f;
+                    *s_plane = make_float4(J.axis == 0 ? 1.f : 0.f, J.axis == 1 ? 1.f : 0.f, J.axis == 2 ? 1.f : 0.f, -mid);
+                }
+            } else {
                 float lv = s_lo[J.axis] + min_edge_dist, hv = s_hi[J.axis] - min_edge_dist;
                 if (lv >= hv) *s_flags = CUT_FLAG_NOPLANE;
                 else {
@@ -139,13 +152,14 @@ k_job_planes(const CutJob* __restrict__ jobs, int n, float min_edge_dist, float4
 
 // Hull jobs for fragments f0..f1 (2 per cut, empty when the cut produced
 // no split) into jobs[f - f0].
-__global__ void k_cut_frag_jobs(const CutResult* __restrict__ cuts, int f0, int f1, HullJob* jobs)
+__global__ void k_cut_frag_jobs(const CutResult* __restrict__ cuts, int f0, int f1, HullJob* jobs,
+                                const unsigned char* __restrict__ skip = nullptr)
 {
     const int f = f0 + blockIdx.x * blockDim.x + threadIdx.x;
     if (f >= f1) return;
     const CutResult& C = cuts[f >> 1];
     const int side = f & 1;
-    const bool empty = C.err != 0 || C.npv <= 0 || C.nnv <= 0;
+    const bool empty = C.err != 0 || C.npv <= 0 || C.nnv <= 0 || (skip && skip[f >> 1]);
     HullJob J;
     memset(&J, 0, sizeof(J));
     if (!empty) {
@@ -174,6 +188,88 @@ __global__ void k_mesh_volumes(const HDSurf* meshes, int n, double* out)
     if (i >= n) return;
     double v = block_mesh_signed_volume(meshes[i].v, meshes[i].nv, meshes[i].t, meshes[i].nt, sh);
     if (threadIdx.x == 0) out[i] = fabs(v);
+}
+
+// ---------------------------------------------------------------------------
+// branch-and-bound rough hulls (la_hull's bound, cuda/la_expand.cu:380-401 with
+// kdop_hull_block's step 3b, cuda/kdop_hull.cuh:184-213): the exact hull of a
+// fragment's extreme points along LA_ROUGH_DIRS directions lies inside the
+// fragment's hull, so its volume bounds the hull volume from below.
+// ---------------------------------------------------------------------------
+#define LA_ROUGH_DIRS 40
+#define LA_ROUGH_PTS (2 * LA_ROUGH_DIRS)
+#define LA_ROUGH_MIN_NV 1024       // smaller fragments get their exact hull directly (kdop_hull.cuh:95)
+
+// Direction k of a Fibonacci lattice on the upper half sphere.
+static __device__ __forceinline__ float3 rough_dir(int k)
+{
+    const float z = 1.0f - ((float)k + 0.5f) / (float)LA_ROUGH_DIRS;
+    const float r = sqrtf(fmaxf(0.f, 1.0f - z * z));
+    const float phi = 2.39996322972865332f * (float)k;          // golden angle
+    return make_float3(r * cosf(phi), r * sinf(phi), z);
+}
+
+// Order-preserving map of a float to 32 unsigned bits.
+static __device__ __forceinline__ unsigned long long ord32(float f)
+{
+    const unsigned u = __float_as_uint(f);
+    return (u & 0x80000000u) ? (unsigned long long)(~u) : (unsigned long long)(u | 0x80000000u);
+}
+
+// One CTA (256 threads) per fragment: its extreme vertex along +-each
+// direction (ties: the smallest index), written as LA_ROUGH_PTS points.
+__global__ void __launch_bounds__(256) k_rough_points(const HDSurf* __restrict__ frags, int n, float* out)
+{
+    __shared__ unsigned long long best[LA_ROUGH_PTS];
+    const int i = blockIdx.x;
+    if (i >= n) return;
+    const HDSurf F = frags[i];
+    for (int k = threadIdx.x; k < LA_ROUGH_PTS; k += 256) best[k] = 0ull;
+    __syncthreads();
+    for (int g = 0; g < LA_ROUGH_DIRS; g += 8) {
+        float3 d[8];
+        for (int k = 0; k < 8; k++) d[k] = rough_dir(g + k);
+        unsigned long long hi[8], lo[8];
+        for (int k = 0; k < 8; k++) { hi[k] = 0ull; lo[k] = 0ull; }
+        for (int v = threadIdx.x; v < F.nv; v += 256) {
+            const float x = F.v[3 * v], y = F.v[3 * v + 1], z = F.v[3 * v + 2];
+            const unsigned long long tag = 0xffffffffull - (unsigned)v;     // larger for smaller indices
+            for (int k = 0; k < 8; k++) {
+                const float t = fmaf(d[k].x, x, fmaf(d[k].y, y, d[k].z * z));
+                const unsigned long long a = (ord32(t) << 32) | tag, b = (ord32(-t) << 32) | tag;
+                hi[k] = a > hi[k] ? a : hi[k];
+                lo[k] = b > lo[k] ? b : lo[k];
+            }
+        }
+        for (int k = 0; k < 8; k++) {
+            for (int o = 16; o > 0; o >>= 1) {
+                const unsigned long long a = __shfl_xor_sync(FULL_MASK, hi[k], o);
+                const unsigned long long b = __shfl_xor_sync(FULL_MASK, lo[k], o);
+                hi[k] = a > hi[k] ? a : hi[k];
+                lo[k] = b > lo[k] ? b : lo[k];
+            }
+            if ((threadIdx.x & 31) == 0) {
+                atomicMax(&best[2 * (g + k)], hi[k]);
+                atomicMax(&best[2 * (g + k) + 1], lo[k]);
+            }
+        }
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < LA_ROUGH_PTS; k += 256) {
+        const int v = F.nv > 0 ? (int)(0xffffffffull - (best[k] & 0xffffffffull)) : 0;
+        for (int c = 0; c < 3; c++) out[(size_t)i * 3 * LA_ROUGH_PTS + 3 * k + c] = F.nv > 0 ? F.v[3 * v + c] : 0.f;
+    }
+}
+
+// Hull jobs over the rough point clouds.
+__global__ void k_rough_jobs(const float* pts, int n, HullJob* jobs)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    HullJob J;
+    memset(&J, 0, sizeof(J));
+    J.pts = pts + (size_t)i * 3 * LA_ROUGH_PTS; J.n = LA_ROUGH_PTS;
+    jobs[i] = J;
 }
 
 // ---------------------------------------------------------------------------
@@ -326,6 +422,7 @@ struct HPart {                 // a part of the decomposition (persistent storag
     char* block;               // owning allocation (nullptr: caller's input)
     int cc_id = 0;             // source connected component (0: not assigned)
     bool checked = false;      // already known to be one connected component
+    int mesh = 0;              // input mesh of a batch the part belongs to
 };
 
 struct LPart {                 // a part inside a search item (arena or persistent)
@@ -405,13 +502,24 @@ struct Lookahead {
     void reset_out() { launch_arena_reset(d_out, out_base, out_cap, s); }
     void reset_tmp() { launch_arena_reset(d_tmp, tmp_base, tmp_cap, s); }
 
+    // Branch-and-bound buffers (2 per job): rough-hull sources, points, mesh
+    // volumes, and the per-job skip mask of the fragment hulls.
+    HDSurf* d_bnb_surf = nullptr; float* d_bnb_pts = nullptr; double* d_bnb_mvol = nullptr;
+    unsigned char* d_skip = nullptr;
+    int bnb_cap = 0;                                 // fragments the rough-hull buffers hold
+    unsigned long long n_hulls = 0, n_pruned = 0;    // fragment hulls built, items pruned
+
     // The last level's fragments are only needed for their costs: its jobs
     // run in waves whose output fits the temporary arena, reset per wave.
+    // bound / pruned as in run_level.
     int run_last_level(const std::vector<CutJob>& jobs, std::vector<CutResult>& cuts, std::vector<FragRes>& frags,
-                       CutJob* d_jobs, CutResult* d_cuts, FragRes* d_fr)
+                       CutJob* d_jobs, CutResult* d_cuts, FragRes* d_fr, const std::vector<float>* bound = nullptr,
+                       std::vector<char>* pruned = nullptr)
     {
         cuts.clear(); frags.clear();
+        if (pruned) pruned->clear();
         std::vector<CutResult> c1; std::vector<FragRes> f1;
+        std::vector<float> b1; std::vector<char> p1;
         size_t j = 0;
         while (j < jobs.size()) {
             size_t acc = 0, j1 = j;
@@ -421,29 +529,28 @@ struct Lookahead {
                 acc += e; j1++;
             }
             std::vector<CutJob> part(jobs.begin() + j, jobs.begin() + j1);
+            if (bound) b1.assign(bound->begin() + j, bound->begin() + j1);
             reset_tmp();
             d_cur = d_tmp;
-            int rc = run_level(part, c1, f1, d_jobs, d_cuts, d_fr);
+            int rc = run_level(part, c1, f1, d_jobs, d_cuts, d_fr, bound ? &b1 : nullptr, pruned ? &p1 : nullptr);
             d_cur = d_out;
             if (rc) return rc;
             cuts.insert(cuts.end(), c1.begin(), c1.end());
             frags.insert(frags.end(), f1.begin(), f1.end());
+            if (pruned) pruned->insert(pruned->end(), p1.begin(), p1.end());
             j = j1;
         }
         return 0;
     }
     void reset_scr() { launch_arena_reset(d_scr, scr_base, scr_cap, s); }
 
-    // Run cut jobs then hull jobs; returns 0 or an error (OOM -> KERR_HEAP_OOM).
-    int run_level(const std::vector<CutJob>& jobs, std::vector<CutResult>& cuts, std::vector<FragRes>& frags,
-                  CutJob* d_jobs, CutResult* d_cuts, FragRes* d_fr)
+    // Cut jobs [0, n) into waves of the scratch arena; results to the host.
+    int run_cuts(const std::vector<CutJob>& jobs, std::vector<CutResult>& cuts, CutJob* d_jobs, CutResult* d_cuts)
     {
         const int n = (int)jobs.size();
         cuts.assign(n, CutResult());
-        frags.assign(2 * n, FragRes());
         if (n == 0) return 0;
         CK(cudaMemcpyAsync(d_jobs, jobs.data(), sizeof(CutJob) * n, cudaMemcpyHostToDevice, s));
-        // cut waves by a scratch estimate
         int j = 0;
         while (j < n) {
             size_t acc = 0; int j1 = j;
@@ -461,14 +568,96 @@ struct Lookahead {
         CK(cudaMemcpyAsync(cuts.data(), d_cuts, sizeof(CutResult) * n, cudaMemcpyDeviceToHost, s));
         CK(cudaStreamSynchronize(s));
         for (auto& c : cuts) if (c.err & (KERR_HEAP_OOM | KERR_PC_SCRATCH_OOM | KERR_PC_POOL_OOM)) return KERR_HEAP_OOM;
+        return 0;
+    }
+
+    // Branch and bound over the cut results of one level: bound[j] is job j's
+    // rv budget (the best bound on its source part's path sum less the job's
+    // item's own partial sum; >= 1e29: none).  A job whose fragment (of more
+    // than LA_ROUGH_MIN_NV vertices) already has a rough-hull volume gap above
+    // the gap that budget allows -- any gap when the budget is <= 0 -- is
+    // pruned: its item cannot beat the bound (la_hull, cuda/la_expand.cu:380-401).
+    int bnb_prune(const std::vector<CutResult>& cuts, const std::vector<float>& bound, std::vector<char>& pruned,
+                  FragRes* d_fr)
+    {
+        const int n = (int)cuts.size();
+        pruned.assign(n, 0);
+        std::vector<HDSurf> src;
+        std::vector<int> src_job;
+        for (int j = 0; j < n; j++) {
+            const CutResult& c = cuts[j];
+            if (bound[j] >= 1e29f || c.err || c.npv <= 0 || c.nnv <= 0) continue;
+            if (c.npv > LA_ROUGH_MIN_NV) { src.push_back({c.pv, c.pt, c.npv, c.npt}); src_job.push_back(j); }
+            if (c.nnv > LA_ROUGH_MIN_NV) { src.push_back({c.nv, c.nt, c.nnv, c.nnt}); src_job.push_back(j); }
+        }
+        const int m = (int)src.size();
+        if (m == 0) return 0;
+        std::vector<FragRes> fr(m);
+        std::vector<double> mv(m);
+        for (int b = 0; b < m; b += bnb_cap) {                  // chunks of the rough-hull buffers
+            const int q = std::min(bnb_cap, m - b);
+            CK(cudaMemcpyAsync(d_bnb_surf, src.data() + b, sizeof(HDSurf) * q, cudaMemcpyHostToDevice, s));
+            k_rough_points<<<q, 256, 0, s>>>(d_bnb_surf, q, d_bnb_pts);
+            k_mesh_volumes<<<q, 256, 0, s>>>(d_bnb_surf, q, d_bnb_mvol);
+            k_rough_jobs<<<(q + 127) / 128, 128, 0, s>>>(d_bnb_pts, q, d_hjobs);
+            ctx->launches += 3;
+            CK(cudaGetLastError());
+            std::vector<int> sizes(q, LA_ROUGH_PTS);
+            int rh = run_hulls(sizes, d_fr);
+            if (rh) return rh;
+            CK(cudaMemcpyAsync(fr.data() + b, d_fr, sizeof(FragRes) * q, cudaMemcpyDeviceToHost, s));
+            CK(cudaMemcpyAsync(mv.data() + b, d_bnb_mvol, sizeof(double) * q, cudaMemcpyDeviceToHost, s));
+            CK(cudaStreamSynchronize(s));
+        }
+        const double pi = 3.14159265358979;
+        for (int k = 0; k < m; k++) {
+            if (fr[k].err || fr[k].hnt <= 0) continue;          // no rough hull (degenerate points): no bound
+            const int j = src_job[k];
+            const double thr = bound[j];
+            bool cut_off;
+            if (thr <= 0.0) cut_off = true;
+            else {
+                const double r = thr / 0.3;
+                const double gap_thr = r * r * r * (4.0 * pi / 3.0);
+                // a relative slack keeps the bound item's own children (whose gap
+                // can equal the budget's) clear of rounding in the budget
+                cut_off = std::max((double)fr[k].hull_vol - mv[k], 0.0) > gap_thr * (1.0 + 1e-4) + 1e-12;
+            }
+            if (cut_off) pruned[j] = 1;
+        }
+        for (int j = 0; j < n; j++) n_pruned += pruned[j] ? 1 : 0;
+        return 0;
+    }
+
+    // Run cut jobs then hull jobs; returns 0 or an error (OOM -> KERR_HEAP_OOM).
+    // With `bound`, jobs that branch and bound cuts off get no fragment hulls
+    // and are flagged in *pruned.
+    int run_level(const std::vector<CutJob>& jobs, std::vector<CutResult>& cuts, std::vector<FragRes>& frags,
+                  CutJob* d_jobs, CutResult* d_cuts, FragRes* d_fr, const std::vector<float>* bound = nullptr,
+                  std::vector<char>* pruned = nullptr)
+    {
+        const int n = (int)jobs.size();
+        cuts.assign(n, CutResult());
+        frags.assign(2 * n, FragRes());
+        if (pruned) pruned->assign(n, 0);
+        if (n == 0) return 0;
+        int rc = run_cuts(jobs, cuts, d_jobs, d_cuts);
+        if (rc) return rc;
+        const bool use_bnb = bound && pruned;
+        if (use_bnb) {
+            rc = bnb_prune(cuts, *bound, *pruned, d_fr);
+            if (rc) return rc;
+            CK(cudaMemcpyAsync(d_skip, pruned->data(), (size_t)n, cudaMemcpyHostToDevice, s));
+        }
         // hulls of all fragments (exact sizes known now)
         std::vector<int> sizes(2 * n);
         for (int f = 0; f < 2 * n; f++) {
             const CutResult& c = cuts[f >> 1];
-            const bool empty = c.err != 0 || c.npv <= 0 || c.nnv <= 0;
+            const bool empty = c.err != 0 || c.npv <= 0 || c.nnv <= 0 || (use_bnb && (*pruned)[f >> 1]);
             sizes[f] = empty ? 0 : ((f & 1) ? c.nnv : c.npv);
+            n_hulls += empty ? 0 : 1;
         }
-        k_cut_frag_jobs<<<(2 * n + 127) / 128, 128, 0, s>>>(d_cuts, 0, 2 * n, d_hjobs);
+        k_cut_frag_jobs<<<(2 * n + 127) / 128, 128, 0, s>>>(d_cuts, 0, 2 * n, d_hjobs, use_bnb ? d_skip : nullptr);
         ctx->launches += 1;
         int rh = run_hulls(sizes, d_fr);
         if (rh) return rh;
@@ -500,7 +689,7 @@ struct Lookahead {
         size_t b0 = al256(12 * (size_t)nv), b1 = al256(12 * (size_t)nt), b2 = al256(12 * (size_t)hnv);
         size_t b3 = al256(12 * (size_t)hnt);
         char* blk = nullptr;
-        CK(cudaMallocAsync((void**)&blk, b0 + b1 + b2 + b3 + 256, s));
+        CK(cudaMallocFromPoolAsync((void**)&blk, b0 + b1 + b2 + b3 + 256, ctx->parts_pool, s));
         p.block = blk;
         p.v = (float*)blk; p.t = (int*)(blk + b0); p.hv = (float*)(blk + b0 + b1); p.ht = (int*)(blk + b0 + b1 + b2);
         p.nv = nv; p.nt = nt; p.hnv = hnv; p.hnt = hnt;
@@ -512,7 +701,7 @@ struct Lookahead {
     }
     void free_part(HPart& p) { if (p.block) cudaFreeAsync(p.block, s); p.block = nullptr; }
 
-    int split_components(std::vector<HPart>& parts, const std::vector<int>& idx, int& cc_counter);
+    int split_components(std::vector<HPart>& parts, const std::vector<int>& idx, std::vector<int>& cc_counter);
 };
 
 // Replace every part of `idx` that has several connected components by its
@@ -520,7 +709,7 @@ struct Lookahead {
 // + la_hull_decomp, csrc/lookahead.c:329-347 and :909-925).  The first
 // component takes the part's slot, the others are appended
 // (la_lifecycle.cu:384-406); cc ids follow la_lifecycle.cu:363-378.
-int Lookahead::split_components(std::vector<HPart>& parts, const std::vector<int>& idx, int& cc_counter)
+int Lookahead::split_components(std::vector<HPart>& parts, const std::vector<int>& idx, std::vector<int>& cc_counter)
 {
     size_t gi = 0;
     while (gi < idx.size()) {
@@ -579,8 +768,9 @@ int Lookahead::split_components(std::vector<HPart>& parts, const std::vector<int
             if (cr[k].n <= 0) continue;
             const int slot = idx[gi + k];
             const int parent_cc = parts[slot].cc_id;
-            const int base_cc = cc_counter;
-            if (parent_cc == 0) cc_counter += cr[k].n;
+            const int mesh = parts[slot].mesh;
+            const int base_cc = cc_counter[mesh];
+            if (parent_cc == 0) cc_counter[mesh] += cr[k].n;
             std::vector<HPart> made(cr[k].n);
             for (int j = 0; j < cr[k].n; j++, c++) {
                 HPart& p = made[j];
@@ -592,6 +782,7 @@ int Lookahead::split_components(std::vector<HPart>& parts, const std::vector<int
                 p.hd = -1;
                 p.checked = true;
                 p.cc_id = parent_cc ? parent_cc : base_cc + j + 1;
+                p.mesh = mesh;
             }
             free_part(parts[slot]);
             parts[slot] = made[0];
@@ -674,7 +865,7 @@ static int merge_hulls_pass(gpu_ctx* ctx, Lookahead& L, std::vector<HPart>& part
         char* blk = nullptr;
         const size_t bj = al256(sizeof(MergeJob) * m), bp = al256(4 * pts), bv = al256(4 * mv), bt = al256(4 * mt);
         const size_t bn = al256(4 * (size_t)m);
-        CK(cudaMallocAsync((void**)&blk, bj + bp + bv + bt + bn, s));
+        CK(cudaMallocFromPoolAsync((void**)&blk, bj + bp + bv + bt + bn, ctx->parts_pool, s));
         MergeJob* d_jobs = (MergeJob*)blk;
         float* d_pts = (float*)(blk + bj); float* d_mv = (float*)(blk + bj + bp); int* d_mt = (int*)(blk + bj + bp + bv);
         int* d_mnt = (int*)(blk + bj + bp + bv + bt);
@@ -776,7 +967,7 @@ static int merge_hulls_pass(gpu_ctx* ctx, Lookahead& L, std::vector<HPart>& part
         const size_t b0 = al256(12 * (size_t)nv), b1 = al256(12 * (size_t)nt), b2 = al256(12 * (size_t)H.hnv);
         const size_t b3 = al256(12 * (size_t)H.hnt);
         char* blk = nullptr;
-        CK(cudaMallocAsync((void**)&blk, b0 + b1 + b2 + b3 + 256, s));
+        CK(cudaMallocFromPoolAsync((void**)&blk, b0 + b1 + b2 + b3 + 256, ctx->parts_pool, s));
         M.block = blk;
         M.v = (float*)blk; M.t = (int*)(blk + b0); M.hv = (float*)(blk + b0 + b1); M.ht = (int*)(blk + b0 + b1 + b2);
         M.nv = nv; M.nt = nt; M.hnv = H.hnv; M.hnt = H.hnt;
@@ -790,6 +981,7 @@ static int merge_hulls_pass(gpu_ctx* ctx, Lookahead& L, std::vector<HPart>& part
         M.hd = 0.0;                                    // la_merge_apply resets it
         M.cc_id = A.cc_id ? A.cc_id : B.cc_id;
         M.checked = true;
+        M.mesh = A.mesh;
         L.free_part(parts[p1]);
         L.free_part(parts[p2]);
         parts[p1] = M;
@@ -886,60 +1078,126 @@ static int prune_level0(gpu_ctx* ctx, Lookahead& L, const Prune& P, const std::v
     return 0;
 }
 
-static int lookahead_impl(gpu_ctx_t ctx, const float* verts, int nv, const int* tris, int nt,
-                          const float* hull_verts, int hull_nv, const int* hull_tris, int hull_nt,
-                          int max_iters, int width, int width2, float threshold,
-                          int depth, int max_n_cutting, int verbose, int debug, int decompose_components,
-                          int decompose_components_per_iter,
-                          int n_concave_edges, float concave_eps, float concave_threshold,
-                          int concave_iters, int merge_hulls, const Prune* prune, struct gpu_result* out)
+// One input mesh of a batch: the mesh and its convex hull (host pointers).
+struct MeshIn { const float* v; int nv; const int* t; int nt; const float* hv; int hnv; const int* ht; int hnt; };
+
+struct SearchParams {
+    int max_iters, width, width2; float threshold; int depth, quick_depth, max_n_cutting, verbose, debug;
+    int decompose_components, decompose_components_per_iter, n_concave_edges;
+    float concave_eps, concave_threshold; int concave_iters, merge_hulls, bnb;
+};
+
+// Branch-and-bound budgets of the last level's jobs.  Per source part, the
+// best bound on a path sum over the current items: partial sum plus the
+// worst (latest) level cost for every level left, since a part's volume gap
+// never grows when it is cut (la_compute_best_ub, cuda/la_expand.cu:434-457).
+// The bound is taken per source part: the reference takes one minimum over
+// the items of every cutting part, which lets one part's bound cut off all
+// of another part's leaves and send that part to its greedy fallback.
+// A job's budget is that bound less its item's partial sum (1e30: none).
+static std::vector<float> bnb_budgets(const std::vector<Item>& cur, int n_src, int total_levels,
+                                      const std::vector<std::pair<int, int>>& job_of)
 {
-    if (!ctx || !out) return -1;
-    out->parts = nullptr; out->nparts = 0;
-    if (nv <= 0 || nt <= 0) return ctx_fail(ctx, KERR_MESH_INVALID, "empty mesh");
-    if (width < 1 || width2 < 1 || depth < 1 || depth > 4 || max_n_cutting < 1 || n_concave_edges < 0 || n_concave_edges > 256)
+    std::vector<double> ub(n_src, 1e30);
+    for (const Item& it : cur) {
+        const int nl = (int)it.costs.size();
+        if (nl <= 0) continue;
+        double ps = 0;
+        for (float c : it.costs) ps += c;
+        ub[it.src] = std::min(ub[it.src], ps + (double)it.costs.back() * (total_levels - nl));
+    }
+    std::vector<float> b(job_of.size(), 1e30f);
+    for (size_t j = 0; j < job_of.size(); j++) {
+        const Item& it = cur[job_of[j].first];
+        const int nl = (int)it.costs.size();
+        if (ub[it.src] >= 1e29 || nl <= 0 || nl >= total_levels) continue;
+        double ps = 0;
+        for (float c : it.costs) ps += c;
+        b[j] = (float)(ub[it.src] - ps);
+    }
+    return b;
+}
+
+// Search statistics of a call (cuacd_lookahead_decompose_batch's out_stats).
+enum { ST_RANKED = 0, ST_CUT = 1, ST_EXPANDED = 2, ST_HULLS = 3, ST_PRUNED = 4, ST_ITERS = 5, ST_N = 8 };
+
+// The lookahead search over a group of meshes at once.  Every decision is
+// per part, so each mesh gets exactly the parts a search of it alone gets;
+// what the group shares are the launches: one cut wave and one hull wave
+// per level serve the cutting parts of every mesh still running.
+static int search_group(gpu_ctx_t ctx, int n_mesh, const MeshIn* M, const SearchParams& P, const Prune* prune,
+                        unsigned long long* st, struct gpu_result* outs)
+{
+    if (!ctx || !outs) return -1;
+    for (int m = 0; m < n_mesh; m++) { outs[m].parts = nullptr; outs[m].nparts = 0; }
+    if (n_mesh <= 0) return 0;
+    if (n_mesh > 2048) return ctx_fail(ctx, KERR_MESH_INVALID, "more than 2048 meshes in one search group");
+    if (P.width < 1 || P.width2 < 1 || P.depth < 1 || P.depth > 4 || P.quick_depth < 0 || P.quick_depth > 4 ||
+        P.max_n_cutting < 1 || P.n_concave_edges < 0 || P.n_concave_edges > 256)
         return ctx_fail(ctx, KERR_MESH_INVALID, "bad search parameters");
-    for (int i = 0; i < 3 * nt; i++) if (tris[i] < 0 || tris[i] >= nv) return ctx_fail(ctx, KERR_MESH_INVALID, "index out of range");
-    for (int i = 0; i < 3 * hull_nt; i++) if (hull_tris[i] < 0 || hull_tris[i] >= hull_nv) return ctx_fail(ctx, KERR_MESH_INVALID, "hull index out of range");
+    size_t sum_v = 0, sum_t = 0, sum_hv = 0, sum_ht = 0;
+    int max_nv = 0;
+    for (int m = 0; m < n_mesh; m++) {
+        const MeshIn& I = M[m];
+        if (I.nv <= 0 || I.nt <= 0) return ctx_fail(ctx, KERR_MESH_INVALID, "mesh %d: empty mesh", m);
+        if (I.hnv < 0 || I.hnt < 0) return ctx_fail(ctx, KERR_MESH_INVALID, "mesh %d: negative hull size", m);
+        for (int i = 0; i < 3 * I.nt; i++)
+            if (I.t[i] < 0 || I.t[i] >= I.nv) return ctx_fail(ctx, KERR_MESH_INVALID, "mesh %d: index out of range", m);
+        for (int i = 0; i < 3 * I.hnt; i++)
+            if (I.ht[i] < 0 || I.ht[i] >= I.hnv)
+                return ctx_fail(ctx, KERR_MESH_INVALID, "mesh %d: hull index out of range", m);
+        sum_v += I.nv; sum_t += I.nt; sum_hv += I.hnv; sum_ht += I.hnt;
+        max_nv = std::max(max_nv, I.nv);
+    }
     CK(cudaSetDevice(ctx->device));
     cudaStream_t s = ctx->stream;
-    const int K = n_concave_edges;
-    const int tw_max = width + 4 * K;
-    // ---- pool: fixed buffers + output arena + scratch arena
-    size_t mesh_bytes = 12 * ((size_t)nv + nt);
-    size_t max_jobs = (size_t)max_n_cutting * tw_max;
-    for (int d = 1; d < depth; d++) max_jobs *= width2;
+    const int K = P.n_concave_edges;
+    const int tw_max = P.width + 4 * K;
+    const int total_levels = P.depth + P.quick_depth;
+    const size_t n_cut_cap = (size_t)P.max_n_cutting * n_mesh;
+    // ---- pool: fixed buffers + output arena + scratch arena + temporary arena
+    size_t items_last = n_cut_cap * tw_max;             // items after the full levels
+    for (int d = 1; d < P.depth; d++) items_last *= P.width2;
+    const size_t max_jobs = items_last * (P.quick_depth > 0 ? 3 : 1);
     const size_t hjob_cap = std::max<size_t>(2 * max_jobs, 2 * 4096);
+    const size_t bnb_cap = std::min<size_t>(hjob_cap, 16384);
     size_t fixed = al256(sizeof(CutJob) * max_jobs) + al256(sizeof(CutResult) * max_jobs) + al256(sizeof(FragRes) * 2 * max_jobs)
-                 + al256(sizeof(float4) * max_n_cutting * tw_max) + al256(sizeof(int) * max_n_cutting * tw_max)
-                 + al256(3 * sizeof(Arena)) + al256(mesh_bytes) + al256(12 * ((size_t)hull_nv + hull_nt))
+                 + al256(sizeof(float4) * n_cut_cap * tw_max) + al256(sizeof(int) * n_cut_cap * tw_max)
+                 + al256(3 * sizeof(Arena)) + al256(12 * (sum_v + sum_t)) + al256(12 * (sum_hv + sum_ht))
                  + al256(sizeof(HDSurf) * 2 * 4096) + al256(sizeof(HDPrep) * 2 * 4096) + al256(hd_dir_bytes() * 2 * 4096)
                  + al256(64) + al256(sizeof(float) * 2 * 4096) + al256(sizeof(double) * 4096)
                  + al256(sizeof(CompResult) * 2 * 4096)
                  + al256(sizeof(HullJob) * hjob_cap) + al256(sizeof(HullState) * hjob_cap) + al256(64)
-                 + al256(hull_wrap_buf_bytes(hull_wrap_ctas(1LL << 40, ctx->n_sm)));
-    // Output arena: the fragments and hulls of every level but the last.  The
-    // cutting parts of one iteration partition (part of) the mesh, so one
-    // level-0 candidate set outputs about 64 bytes per input vertex and
-    // triangle per plane; each further kept level multiplies by width2.
-    size_t lvl_bytes = (size_t)tw_max * 64 * ((size_t)nv + nt) * 5 / 4;
-    for (int d = 1; d + 1 < depth; d++) lvl_bytes *= width2;
-    size_t out_cap = std::min<size_t>(std::max<size_t>((size_t)1 << 30, lvl_bytes), (size_t)96 << 30);
-    size_t tmp_cap = std::min<size_t>(std::max<size_t>((size_t)1 << 30, (size_t)width2 * 64 * ((size_t)nv + nt) * 2),
+                 + al256(hull_wrap_buf_bytes(hull_wrap_ctas(1LL << 40, ctx->n_sm)))
+                 + al256(sizeof(HDSurf) * bnb_cap) + al256(sizeof(float) * 3 * LA_ROUGH_PTS * bnb_cap)
+                 + al256(sizeof(double) * bnb_cap) + al256(max_jobs);
+    // Output arena: the fragments and hulls of every level whose items outlive
+    // it.  A level-0 candidate set outputs about 64 bytes per input vertex and
+    // triangle per plane; a further level multiplies that by width2 at most.
+    const size_t lvl0 = (size_t)tw_max * 64 * (sum_v + sum_t) * 5 / 4;
+    size_t kept = 0, mult = 1;
+    const int kept_full = P.quick_depth > 0 ? P.depth : P.depth - 1;
+    for (int d = 0; d < kept_full; d++) { kept += mult; mult *= P.width2; }
+    if (P.quick_depth > 1) kept += (size_t)(P.quick_depth - 1) * (mult / P.width2 > 0 ? mult / P.width2 : 1);
+    size_t free_b = 0, total_b = 0;
+    cudaMemGetInfo(&free_b, &total_b);
+    const size_t out_limit = std::max<size_t>((size_t)1 << 30, std::min<size_t>((size_t)96 << 30, free_b / 2));
+    size_t out_cap = std::min<size_t>(std::max<size_t>((size_t)1 << 30, lvl0 * std::max<size_t>(kept, 1)), out_limit);
+    size_t tmp_cap = std::min<size_t>(std::max<size_t>((size_t)1 << 30, (size_t)P.width2 * 64 * (sum_v + sum_t) * 2),
                                       (size_t)16 << 30);
-    size_t scr_cap = std::max<size_t>((size_t)2 << 30, hull_scratch_bytes(nv) * 64);
+    size_t scr_cap = std::max<size_t>((size_t)2 << 30, hull_scratch_bytes(max_nv) * 64);
     int rc = pool_begin(ctx, fixed + out_cap + tmp_cap + scr_cap + (1 << 20));
     if (rc) return rc;
     CutJob* d_jobs = pool_take<CutJob>(ctx, max_jobs);
-    float4* d_jplanes = pool_take<float4>(ctx, (size_t)max_n_cutting * tw_max);
-    int* d_jflags = pool_take<int>(ctx, (size_t)max_n_cutting * tw_max);
+    float4* d_jplanes = pool_take<float4>(ctx, n_cut_cap * tw_max);
+    int* d_jflags = pool_take<int>(ctx, n_cut_cap * tw_max);
     CutResult* d_cuts = pool_take<CutResult>(ctx, max_jobs);
     FragRes* d_frags = pool_take<FragRes>(ctx, 2 * max_jobs);
     Arena* d_arenas = pool_take<Arena>(ctx, 3);
-    float* d_v0 = pool_take<float>(ctx, 3 * (size_t)nv);
-    int* d_t0 = pool_take<int>(ctx, 3 * (size_t)nt);
-    float* d_hv0 = pool_take<float>(ctx, 3 * (size_t)hull_nv);
-    int* d_ht0 = pool_take<int>(ctx, 3 * (size_t)hull_nt);
+    float* d_v0 = pool_take<float>(ctx, 3 * sum_v);
+    int* d_t0 = pool_take<int>(ctx, 3 * sum_t);
+    float* d_hv0 = pool_take<float>(ctx, 3 * sum_hv);
+    int* d_ht0 = pool_take<int>(ctx, 3 * sum_ht);
     HDSurf* d_surfs = pool_take<HDSurf>(ctx, 2 * 4096);
     HDPrep* d_preps = pool_take<HDPrep>(ctx, 2 * 4096);
     char* d_dirs = pool_take<char>(ctx, hd_dir_bytes() * 2 * 4096);
@@ -951,6 +1209,10 @@ static int lookahead_impl(gpu_ctx_t ctx, const float* verts, int nv, const int* 
     HullState* d_hstates = pool_take<HullState>(ctx, hjob_cap);
     int* d_hctl = pool_take<int>(ctx, 16);
     int* d_wbuf = (int*)pool_take<char>(ctx, hull_wrap_buf_bytes(hull_wrap_ctas(1LL << 40, ctx->n_sm)));
+    HDSurf* d_bnb_surf = pool_take<HDSurf>(ctx, bnb_cap);
+    float* d_bnb_pts = pool_take<float>(ctx, 3 * LA_ROUGH_PTS * bnb_cap);
+    double* d_bnb_mvol = pool_take<double>(ctx, bnb_cap);
+    unsigned char* d_skip = pool_take<unsigned char>(ctx, max_jobs);
     char* out_base = pool_take<char>(ctx, out_cap);
     char* scr_base = pool_take<char>(ctx, scr_cap);
     char* tmp_base = pool_take<char>(ctx, tmp_cap);
@@ -959,36 +1221,53 @@ static int lookahead_impl(gpu_ctx_t ctx, const float* verts, int nv, const int* 
     L.ctx = ctx; L.s = s; L.out_base = out_base; L.out_cap = out_cap; L.scr_base = scr_base; L.scr_cap = scr_cap;
     L.d_out = d_arenas; L.d_scr = d_arenas + 1; L.d_tmp = d_arenas + 2; L.d_cur = L.d_out;
     L.tmp_base = tmp_base; L.tmp_cap = tmp_cap;
-    L.min_edge = std::min(threshold * 0.25f, 0.015f);
-    L.debug = debug;
+    L.min_edge = std::min(P.threshold * 0.25f, 0.015f);
+    L.debug = P.debug;
     L.d_surfs = d_surfs; L.surf_cap = 2 * 4096; L.d_cres = d_cres;
     L.d_frags = d_frags; L.frag_cap = (int)std::min<size_t>(2 * max_jobs, 1 << 30);
     L.d_hjobs = d_hjobs; L.d_hstates = d_hstates; L.d_hctl = d_hctl; L.d_wbuf = d_wbuf; L.nwc = hull_wrap_ctas(1LL << 40, ctx->n_sm);
-    CK(cudaMemcpyAsync(d_v0, verts, 12 * (size_t)nv, cudaMemcpyHostToDevice, s));
-    CK(cudaMemcpyAsync(d_t0, tris, 12 * (size_t)nt, cudaMemcpyHostToDevice, s));
-    if (hull_nv) CK(cudaMemcpyAsync(d_hv0, hull_verts, 12 * (size_t)hull_nv, cudaMemcpyHostToDevice, s));
-    if (hull_nt) CK(cudaMemcpyAsync(d_ht0, hull_tris, 12 * (size_t)hull_nt, cudaMemcpyHostToDevice, s));
-    // ---- initial part: the mesh and the caller's hull (la_initialize, la_lifecycle.cu:18-81)
+    L.d_bnb_surf = d_bnb_surf; L.d_bnb_pts = d_bnb_pts; L.d_bnb_mvol = d_bnb_mvol; L.d_skip = d_skip;
+    L.bnb_cap = (int)bnb_cap;
+    // ---- initial parts: each mesh and the caller's hull (la_initialize, la_lifecycle.cu:18-81)
     std::vector<HPart> parts;
     {
-        HDSurf m[2] = {{d_v0, d_t0, nv, nt}, {d_hv0, d_ht0, hull_nv, hull_nt}};
-        CK(cudaMemcpyAsync(d_surfs, m, sizeof(m), cudaMemcpyHostToDevice, s));
-        k_mesh_volumes<<<2, 256, 0, s>>>(d_surfs, 2, d_vols);
-        ctx->launches++;
-        double vols[2];
-        CK(cudaMemcpyAsync(vols, d_vols, sizeof(vols), cudaMemcpyDeviceToHost, s));
-        CK(cudaStreamSynchronize(s));
-        HPart p;
-        p.v = d_v0; p.t = d_t0; p.nv = nv; p.nt = nt;
-        p.hv = d_hv0; p.ht = d_ht0; p.hnv = hull_nv; p.hnt = hull_nt;
-        p.mesh_vol = vols[0]; p.hull_vol = vols[1]; p.hd = -1; p.block = nullptr;
-        parts.push_back(p);
+        size_t ov = 0, ot = 0, ohv = 0, oht = 0;
+        std::vector<HDSurf> sf(2 * (size_t)n_mesh);
+        for (int m = 0; m < n_mesh; m++) {
+            const MeshIn& I = M[m];
+            CK(cudaMemcpyAsync(d_v0 + 3 * ov, I.v, 12 * (size_t)I.nv, cudaMemcpyHostToDevice, s));
+            CK(cudaMemcpyAsync(d_t0 + 3 * ot, I.t, 12 * (size_t)I.nt, cudaMemcpyHostToDevice, s));
+            if (I.hnv) CK(cudaMemcpyAsync(d_hv0 + 3 * ohv, I.hv, 12 * (size_t)I.hnv, cudaMemcpyHostToDevice, s));
+            if (I.hnt) CK(cudaMemcpyAsync(d_ht0 + 3 * oht, I.ht, 12 * (size_t)I.hnt, cudaMemcpyHostToDevice, s));
+            HPart p;
+            p.v = d_v0 + 3 * ov; p.t = d_t0 + 3 * ot; p.nv = I.nv; p.nt = I.nt;
+            p.hv = d_hv0 + 3 * ohv; p.ht = d_ht0 + 3 * oht; p.hnv = I.hnv; p.hnt = I.hnt;
+            p.hd = -1; p.block = nullptr; p.mesh = m;
+            parts.push_back(p);
+            sf[2 * m] = {p.v, p.t, p.nv, p.nt};
+            sf[2 * m + 1] = {p.hv, p.ht, p.hnv, p.hnt};
+            ov += I.nv; ot += I.nt; ohv += I.hnv; oht += I.hnt;
+        }
+        for (int b = 0; b < 2 * n_mesh; b += 4096) {
+            const int q = std::min(4096, 2 * n_mesh - b);
+            std::vector<double> vols(q);
+            CK(cudaMemcpyAsync(d_surfs, sf.data() + b, sizeof(HDSurf) * q, cudaMemcpyHostToDevice, s));
+            k_mesh_volumes<<<q, 256, 0, s>>>(d_surfs, q, d_vols);
+            ctx->launches++;
+            CK(cudaMemcpyAsync(vols.data(), d_vols, sizeof(double) * q, cudaMemcpyDeviceToHost, s));
+            CK(cudaStreamSynchronize(s));
+            for (int k = 0; k < q; k++) {
+                HPart& p = parts[(b + k) >> 1];
+                if (((b + k) & 1) == 0) p.mesh_vol = vols[k]; else p.hull_vol = vols[k];
+            }
+        }
     }
     int result = 0;
-    int cc_counter = 0;
+    std::vector<int> cc_counter(n_mesh, 0);
+    std::vector<char> done(n_mesh, 0);
     auto unchecked = [&]() {
         std::vector<int> u;
-        for (int i = 0; i < (int)parts.size(); i++) if (!parts[i].checked) u.push_back(i);
+        for (int i = 0; i < (int)parts.size(); i++) if (!parts[i].checked && !done[parts[i].mesh]) u.push_back(i);
         return u;
     };
     std::vector<CutJob> jobs;
@@ -999,18 +1278,21 @@ static int lookahead_impl(gpu_ctx_t ctx, const float* verts, int nv, const int* 
     auto tnow = [&]() { cudaStreamSynchronize(s); return std::chrono::steady_clock::now(); };
     std::chrono::steady_clock::time_point tmark = std::chrono::steady_clock::now();
     auto tacc = [&](int k) {
-        if (verbose < 2) return;
+        if (P.verbose < 2) return;
         auto t = tnow();
         tph[k] += std::chrono::duration<double>(t - tmark).count();
         tmark = t;
     };
     int n_iters_run = 0;
-    for (int iter = 0; iter < max_iters && result == 0; iter++) {
+    for (int iter = 0; iter < P.max_iters && result == 0; iter++) {
+        bool any_active = false;
+        for (int m = 0; m < n_mesh; m++) any_active |= !done[m];
+        if (!any_active) break;
         n_iters_run++;
         tacc(7);
         // ---- 0. split parts made of several connected components
         //      (dc_pre_eval / dc_post_cuts, csrc/lookahead.c:329-347, :909-925)
-        if (decompose_components_per_iter) {
+        if (P.decompose_components_per_iter) {
             result = L.split_components(parts, unchecked(), cc_counter);
             if (result) break;
         }
@@ -1019,7 +1301,8 @@ static int lookahead_impl(gpu_ctx_t ctx, const float* verts, int nv, const int* 
         {
             std::vector<int> need;
             for (int i = 0; i < (int)parts.size(); i++)
-                if (parts[i].hd < 0 && parts[i].hnt > 0 && cost_rv(parts[i].hull_vol, parts[i].mesh_vol) < threshold)
+                if (!done[parts[i].mesh] && parts[i].hd < 0 && parts[i].hnt > 0 &&
+                    cost_rv(parts[i].hull_vol, parts[i].mesh_vol) < P.threshold)
                     need.push_back(i);
             for (size_t b = 0; b < need.size(); b += 4096) {
                 int m = (int)std::min<size_t>(4096, need.size() - b);
@@ -1033,7 +1316,7 @@ static int lookahead_impl(gpu_ctx_t ctx, const float* verts, int nv, const int* 
                 CK(cudaMemsetAsync(d_i4, 0, 16 * sizeof(int), s));
                 L.reset_scr();
                 launch_hausdorff_pairs(d_surfs, m, L.d_scr, 2000.f, 1000, 0, d_preps, d_dirs, d_i4, d_pmax, d_i4 + 2,
-                                       148, s);
+                                       ctx->n_sm, s);
                 launch_hd_sqrt(d_pmax, m, d_pmax + 4096, 1, s);
                 ctx->launches += 5;
                 std::vector<float> h(m);
@@ -1046,42 +1329,49 @@ static int lookahead_impl(gpu_ctx_t ctx, const float* verts, int nv, const int* 
             }
             if (result) break;
         }
-        // ---- 2. cutting parts (costliest first, la_sort_and_count_cutting)
-        std::vector<int> order(parts.size());
-        for (size_t i = 0; i < parts.size(); i++) order[i] = (int)i;
+        // ---- 2. cutting parts of every running mesh (costliest first, la_sort_and_count_cutting)
         auto full = [&](int i) {
             const HPart& p = parts[i];
             float rv = cost_rv(p.hull_vol, p.mesh_vol);
             return std::max(rv, p.hd > 0 ? (float)p.hd : 0.f);
         };
-        std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return full(a) < full(b); });
+        std::vector<std::vector<int>> of_mesh(n_mesh);
+        for (int i = 0; i < (int)parts.size(); i++) if (!done[parts[i].mesh]) of_mesh[parts[i].mesh].push_back(i);
         std::vector<int> cutting;
-        int first_above = (int)order.size();
-        for (int i = 0; i < (int)order.size(); i++) if (full(order[i]) >= threshold) { first_above = i; break; }
-        int start = std::max(first_above, (int)order.size() - max_n_cutting);
-        for (int i = start; i < (int)order.size(); i++) if (full(order[i]) >= threshold) cutting.push_back(order[i]);
-        if (verbose == 1 || verbose >= 3) fprintf(stderr, "[la] iter %d: parts=%zu cutting=%zu\n", iter, parts.size(), cutting.size());
+        for (int m = 0; m < n_mesh; m++) {
+            if (done[m]) continue;
+            std::vector<int>& order = of_mesh[m];
+            std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return full(a) < full(b); });
+            int first_above = (int)order.size();
+            for (int i = 0; i < (int)order.size(); i++) if (full(order[i]) >= P.threshold) { first_above = i; break; }
+            const int start = std::max(first_above, (int)order.size() - P.max_n_cutting);
+            size_t before = cutting.size();
+            for (int i = start; i < (int)order.size(); i++) if (full(order[i]) >= P.threshold) cutting.push_back(order[i]);
+            if (cutting.size() == before) done[m] = 1;           // nothing above tau: this mesh is finished
+        }
+        if (P.verbose == 1 || P.verbose >= 3)
+            fprintf(stderr, "[la] iter %d: parts=%zu cutting=%zu\n", iter, parts.size(), cutting.size());
         if (cutting.empty()) break;
         const int nc = (int)cutting.size();
         tacc(1);
         // ---- 3. concave-edge planes per cutting part
         std::vector<std::vector<float4>> eplanes(nc);
-        if (K > 0 && iter < concave_iters) {      // all cutting parts in one launch
+        if (K > 0 && iter < P.concave_iters) {      // all cutting parts in one launch
             std::vector<const float*> pv(nc); std::vector<const int*> pt(nc);
             std::vector<int> pnv(nc), pnt(nc);
             for (int c = 0; c < nc; c++) {
                 const HPart& p = parts[cutting[c]];
                 pv[c] = p.v; pt[c] = p.t; pnv[c] = p.nv; pnt[c] = p.nt;
             }
-            rc = concave_planes_device_batch(ctx, nc, pv.data(), pnv.data(), pt.data(), pnt.data(), K, concave_eps,
-                                             concave_threshold, L.scr_base, L.scr_cap, eplanes);
+            rc = concave_planes_device_batch(ctx, nc, pv.data(), pnv.data(), pt.data(), pnt.data(), K, P.concave_eps,
+                                             P.concave_threshold, L.scr_base, L.scr_cap, eplanes);
             if (rc) { result = rc; break; }
         }
         int n_edge = 0;
         for (auto& e : eplanes) n_edge = std::max(n_edge, (int)e.size());
-        const int tw0 = width + n_edge;
+        const int tw0 = P.width + n_edge;
         tacc(2);
-        // ---- 4. expansion levels
+        // ---- 4. expansion levels: `depth` full levels, then `quick_depth` quick ones
         std::vector<Item> cur, leaves, extra;
         for (int c = 0; c < nc; c++) {
             Item it; it.src = c; it.cut0 = -1;
@@ -1094,8 +1384,29 @@ static int lookahead_impl(gpu_ctx_t ctx, const float* verts, int nv, const int* 
         std::vector<Item> level0;              // level-0 items by (src, cut) for apply
         std::vector<std::vector<int>> l0index(nc, std::vector<int>(tw0, -1));
         L.reset_out();
-        for (int d = 0; d < depth && !cur.empty() && result == 0; d++) {
-            const int wd = d == 0 ? width : width2;
+        // a part too small on every axis ends its branch as a leaf padded with
+        // zero costs (la_expand.cu:155-174, la_refine.cu:103-118)
+        auto small_leaf = [&](const Item& it, int d, int ci) {
+            Item x = it;
+            if (d == 0) x.cut0 = ci;
+            while ((int)x.costs.size() < total_levels) x.costs.push_back(0.f);
+            x.leaf_small = true;
+            extra.push_back(x);
+        };
+        // the item that replaces its worst part by the two fragments of cut j
+        auto child = [&](const Item& it, int d, int ci, const CutResult& c, const FragRes& a, const FragRes& b) {
+            Item x;
+            x.src = it.src; x.cut0 = d == 0 ? ci : it.cut0;
+            x.parts.assign(it.parts.begin(), it.parts.end() - 1);
+            x.parts.push_back({c.pv, c.pt, c.npv, c.npt, a.mesh_vol, (double)a.hull_vol, a.hv, a.ht, a.hnv, a.hnt});
+            x.parts.push_back({c.nv, c.nt, c.nnv, c.nnt, b.mesh_vol, (double)b.hull_vol, b.hv, b.ht, b.hnv, b.hnt});
+            std::stable_sort(x.parts.begin(), x.parts.end(), [](const LPart& p, const LPart& q) { return cost_rv(p) < cost_rv(q); });
+            x.costs = it.costs;
+            x.costs.push_back(cost_rv(x.parts.back()));
+            return x;
+        };
+        for (int d = 0; d < P.depth && !cur.empty() && result == 0; d++) {
+            const int wd = d == 0 ? P.width : P.width2;
             jobs.clear();
             std::vector<std::pair<int, int>> job_of;   // (item, cut idx)
             for (int ii = 0; ii < (int)cur.size(); ii++) {
@@ -1123,8 +1434,13 @@ static int lookahead_impl(gpu_ctx_t ctx, const float* verts, int nv, const int* 
                 if (result) break;
                 tacc(3);
             }
-            const bool last = d == depth - 1 && d > 0;
-            int lr = last ? L.run_last_level(jobs, cuts, frs, d_jobs, d_cuts, d_frags)
+            const bool last = d == total_levels - 1 && d > 0;
+            const bool bnb = last && P.bnb;
+            std::vector<float> budget;
+            std::vector<char> pruned;
+            if (bnb) budget = bnb_budgets(cur, nc, total_levels, job_of);
+            int lr = last ? L.run_last_level(jobs, cuts, frs, d_jobs, d_cuts, d_frags, bnb ? &budget : nullptr,
+                                             bnb ? &pruned : nullptr)
                           : L.run_level(jobs, cuts, frs, d_jobs, d_cuts, d_frags);
             tacc(d == 0 ? 4 : 5);
             if (lr) { result = ctx_fail(ctx, lr, "lookahead level %d failed at iter %d (0x%x)", d, iter, lr); break; }
@@ -1135,34 +1451,21 @@ static int lookahead_impl(gpu_ctx_t ctx, const float* verts, int nv, const int* 
                 const Item& it = cur[ii];
                 const CutResult& c = cuts[j];
                 if (c.flags & CUT_FLAG_SMALL) {
-                    if (!small_done[ii]) {
-                        small_done[ii] = true;
-                        Item x = it;
-                        if (d == 0) x.cut0 = ci;
-                        while ((int)x.costs.size() < depth) x.costs.push_back(0.f);
-                        x.leaf_small = true;
-                        extra.push_back(x);
-                    }
+                    if (!small_done[ii]) { small_done[ii] = true; small_leaf(it, d, ci); }
                     continue;
                 }
                 if (c.flags & CUT_FLAG_NOPLANE) continue;
                 if (c.err || c.npv == 0 || c.nnv == 0) continue;
+                if (bnb && pruned[j]) continue;            // cannot beat its source part's bound
                 const FragRes& a = frs[2 * j];
                 const FragRes& b = frs[2 * j + 1];
                 if (a.err || b.err) { result = ctx_fail(ctx, a.err | b.err, "fragment hull failed (0x%x)", a.err | b.err); break; }
-                Item x;
-                x.src = it.src; x.cut0 = d == 0 ? ci : it.cut0;
-                x.parts.assign(it.parts.begin(), it.parts.end() - 1);
-                x.parts.push_back({c.pv, c.pt, c.npv, c.npt, a.mesh_vol, (double)a.hull_vol, a.hv, a.ht, a.hnv, a.hnt});
-                x.parts.push_back({c.nv, c.nt, c.nnv, c.nnt, b.mesh_vol, (double)b.hull_vol, b.hv, b.ht, b.hnv, b.hnt});
-                std::stable_sort(x.parts.begin(), x.parts.end(), [](const LPart& p, const LPart& q) { return cost_rv(p) < cost_rv(q); });
-                x.costs = it.costs;
-                x.costs.push_back(cost_rv(x.parts.back()));
+                Item x = child(it, d, ci, c, a, b);
                 if (d == 0) { l0index[x.src][ci] = (int)level0.size(); level0.push_back(x); }
                 next.push_back(std::move(x));
             }
             if (result) break;
-            if (d == 0 && prune && prune->beam > 0 && depth > 1) {
+            if (d == 0 && prune && prune->beam > 0 && total_levels > 1) {
                 std::vector<std::vector<int>> by_src(nc);
                 for (int k = 0; k < (int)next.size(); k++) by_src[next[k].src].push_back(k);
                 std::vector<char> keep(next.size(), 0);
@@ -1170,11 +1473,113 @@ static int lookahead_impl(gpu_ctx_t ctx, const float* verts, int nv, const int* 
                     std::stable_sort(ks.begin(), ks.end(), [&](int a, int b) { return next[a].costs[0] < next[b].costs[0]; });
                     for (int r = 0; r < (int)ks.size() && r < prune->beam; r++) keep[ks[r]] = 1;
                 }
-                std::vector<Item> kept;
-                for (size_t k = 0; k < next.size(); k++) if (keep[k]) kept.push_back(std::move(next[k]));
-                next.swap(kept);
+                std::vector<Item> kept_items;
+                for (size_t k = 0; k < next.size(); k++) if (keep[k]) kept_items.push_back(std::move(next[k]));
+                next.swap(kept_items);
             }
             if (d == 0 && prune) prune->stats[2] += next.size();
+            cur.swap(next);
+        }
+        // quick levels (la_expand_quick, cuda/la_refine.cu:52-351): each item's
+        // worst part is cut at its box midpoint on each axis; the cut with the
+        // most even volume split (max / sum, first axis on ties) makes the
+        // item's one child.  The three cuts are made in the temporary arena to
+        // compare them, then the chosen one again where its level keeps it.
+        for (int q = 0; q < P.quick_depth && !cur.empty() && result == 0; q++) {
+            const int d = P.depth + q;
+            const int ni = (int)cur.size();
+            jobs.clear();
+            for (int ii = 0; ii < ni; ii++) {
+                const LPart& w = cur[ii].parts.back();
+                for (int a = 0; a < 3; a++) {
+                    CutJob J;
+                    J.v = w.v; J.t = w.t; J.nv = w.nv; J.nt = w.nt; J._pad = 0;
+                    J.axis = a; J.slice = 0; J.cpa = -1; J.plane = make_float4(0, 0, 0, 0);
+                    jobs.push_back(J);
+                }
+            }
+            std::vector<int> choice(ni, -1);
+            std::vector<char> is_small(ni, 0);
+            {
+                std::vector<double> bal(jobs.size(), 1e30);
+                size_t j = 0;
+                while (j < jobs.size() && result == 0) {
+                    size_t acc = 0, j1 = j;
+                    while (j1 < jobs.size()) {
+                        size_t e = 64 * ((size_t)jobs[j1].nv + jobs[j1].nt) + (64 << 10);
+                        if (j1 > j && acc + e > L.tmp_cap) break;
+                        acc += e; j1++;
+                    }
+                    std::vector<CutJob> part(jobs.begin() + j, jobs.begin() + j1);
+                    std::vector<CutResult> c1;
+                    L.reset_tmp();
+                    L.d_cur = L.d_tmp;
+                    int lr = L.run_cuts(part, c1, d_jobs, d_cuts);
+                    if (lr) { L.d_cur = L.d_out; result = ctx_fail(ctx, lr, "quick level %d failed at iter %d (0x%x)", q, iter, lr); break; }
+                    std::vector<HDSurf> src;
+                    std::vector<size_t> src_job;
+                    for (size_t k = 0; k < c1.size(); k++) {
+                        const CutResult& c = c1[k];
+                        if (c.flags & CUT_FLAG_SMALL) is_small[(j + k) / 3] = 1;
+                        if ((c.flags & CUT_FLAG_NOPLANE) || c.err || c.npv <= 0 || c.nnv <= 0) continue;
+                        src.push_back({c.pv, c.pt, c.npv, c.npt});
+                        src.push_back({c.nv, c.nt, c.nnv, c.nnt});
+                        src_job.push_back(j + k);
+                    }
+                    std::vector<double> vol(src.size());
+                    for (size_t b = 0; b < src.size(); b += bnb_cap) {
+                        const int m = (int)std::min<size_t>(bnb_cap, src.size() - b);
+                        CK(cudaMemcpyAsync(d_bnb_surf, src.data() + b, sizeof(HDSurf) * m, cudaMemcpyHostToDevice, s));
+                        k_mesh_volumes<<<m, 256, 0, s>>>(d_bnb_surf, m, d_bnb_mvol);
+                        ctx->launches++;
+                        CK(cudaMemcpyAsync(vol.data() + b, d_bnb_mvol, sizeof(double) * m, cudaMemcpyDeviceToHost, s));
+                        CK(cudaStreamSynchronize(s));
+                    }
+                    for (size_t k = 0; k < src_job.size(); k++) {
+                        const double vp = vol[2 * k], vn = vol[2 * k + 1];
+                        bal[src_job[k]] = std::max(vp, vn) / (vp + vn + 1e-10);
+                    }
+                    L.d_cur = L.d_out;
+                    j = j1;
+                }
+                if (result) break;
+                for (int ii = 0; ii < ni; ii++) {
+                    double best = 1e30;
+                    for (int a = 0; a < 3; a++)
+                        if (bal[3 * ii + a] < best) { best = bal[3 * ii + a]; choice[ii] = a; }
+                }
+            }
+            // the chosen cuts, kept where their level's items live
+            std::vector<CutJob> cj;
+            std::vector<std::pair<int, int>> job_of;
+            for (int ii = 0; ii < ni; ii++) {
+                if (is_small[ii]) { small_leaf(cur[ii], d, 0); continue; }
+                if (choice[ii] < 0) continue;                // no axis splits it: the item ends here
+                cj.push_back(jobs[3 * ii + choice[ii]]);
+                job_of.push_back({ii, 0});
+            }
+            const bool last = d == total_levels - 1;
+            const bool bnb = last && P.bnb;
+            std::vector<float> budget;
+            std::vector<char> pruned;
+            if (bnb) budget = bnb_budgets(cur, nc, total_levels, job_of);
+            int lr = last ? L.run_last_level(cj, cuts, frs, d_jobs, d_cuts, d_frags, bnb ? &budget : nullptr,
+                                             bnb ? &pruned : nullptr)
+                          : L.run_level(cj, cuts, frs, d_jobs, d_cuts, d_frags);
+            tacc(5);
+            if (lr) { result = ctx_fail(ctx, lr, "quick level %d failed at iter %d (0x%x)", q, iter, lr); break; }
+            std::vector<Item> next;
+            for (size_t j = 0; j < cj.size(); j++) {
+                const Item& it = cur[job_of[j].first];
+                const CutResult& c = cuts[j];
+                if ((c.flags & (CUT_FLAG_SMALL | CUT_FLAG_NOPLANE)) || c.err || c.npv == 0 || c.nnv == 0) continue;
+                if (bnb && pruned[j]) continue;
+                const FragRes& a = frs[2 * j];
+                const FragRes& b = frs[2 * j + 1];
+                if (a.err || b.err) { result = ctx_fail(ctx, a.err | b.err, "fragment hull failed (0x%x)", a.err | b.err); break; }
+                next.push_back(child(it, d, 0, c, a, b));
+            }
+            if (result) break;
             cur.swap(next);
         }
         if (result) break;
@@ -1202,15 +1607,15 @@ static int lookahead_impl(gpu_ctx_t ctx, const float* verts, int nv, const int* 
             for (int ci = 0; ci < tw0; ci++) if (cb[ci] < best) { best = cb[ci]; bi = ci; }
             best_cut[c] = bi;
             if (prune && prune->trace && !prune->tkey.empty()) {
-                const int K = scorer_n_features();
+                const int KF = scorer_n_features();
                 for (size_t j = 0; j < prune->tkey.size(); j++) {
                     if (cur_src_of_item0[prune->tkey[j].first] != c) continue;
                     const int ci = prune->tkey[j].second;
                     const int li = l0index[c][ci];
                     if (li < 0 || level0[li].costs.empty()) continue;      // no split: not a candidate
-                    if (prune->trace->size() + K + 4 > prune->trace_cap) break;
-                    const float* f = prune->tfeat.data() + j * K;
-                    prune->trace->insert(prune->trace->end(), f, f + K);
+                    if (prune->trace->size() + KF + 4 > prune->trace_cap) break;
+                    const float* f = prune->tfeat.data() + j * KF;
+                    prune->trace->insert(prune->trace->end(), f, f + KF);
                     prune->trace->push_back(level0[li].costs[0]);
                     prune->trace->push_back(cb[ci] < 1e30f ? cb[ci] : level0[li].costs[0]);
                     prune->trace->push_back((float)(iter * 4096 + c));
@@ -1221,9 +1626,11 @@ static int lookahead_impl(gpu_ctx_t ctx, const float* verts, int nv, const int* 
         if (prune) { prune->tkey.clear(); prune->tfeat.clear(); }
         tacc(6);
         // ---- 6. apply: the part becomes the two halves of its best level-0 item
-        bool applied = false;
+        std::vector<char> applied(n_mesh, 0), had(n_mesh, 0);
         std::vector<HPart> added;
         for (int c = 0; c < nc; c++) {
+            const int mesh = parts[cutting[c]].mesh;
+            had[mesh] = 1;
             int bi = best_cut[c];
             if (bi < 0) continue;
             int li = l0index[c][bi];
@@ -1239,55 +1646,87 @@ static int lookahead_impl(gpu_ctx_t ctx, const float* verts, int nv, const int* 
                 p.mesh_vol = std::min(q.mesh_vol, q.hull_vol);   // la_hull_decomp clamp (la_lifecycle.cu:294-297)
                 p.hd = -1;
                 p.cc_id = parts[cutting[c]].cc_id;             // cut pieces inherit (la_expand.cu:253-258)
+                p.mesh = mesh;
             }
             if (result) break;
             L.free_part(parts[cutting[c]]);
             parts[cutting[c]] = nw[0];
             added.push_back(nw[1]);
-            applied = true;
+            applied[mesh] = 1;
         }
         for (auto& p : added) parts.push_back(p);
         if (result) break;
         CK(cudaStreamSynchronize(s));
-        if (!applied) break;
+        for (int m = 0; m < n_mesh; m++) if (had[m] && !applied[m]) done[m] = 1;   // no cut applied: finished
     }
     tacc(7);
-    if (verbose >= 2)
+    if (P.verbose >= 2)
         fprintf(stderr, "[la] %d iterations, seconds: components %.4f hausdorff %.4f concave %.4f prune %.4f "
                 "level0 %.4f deeper %.4f bookkeeping %.4f apply %.4f\n", n_iters_run, tph[0], tph[1], tph[2],
                 tph[3], tph[4], tph[5], tph[6], tph[7]);
+    if (st) { st[ST_HULLS] += L.n_hulls; st[ST_PRUNED] += L.n_pruned; st[ST_ITERS] += n_iters_run; }
     // ---- post-pass components (csrc/lookahead.c:969-985); with the per-iteration
     //      pass on, only the pieces of the last iteration's cuts are left
-    if (result == 0 && (decompose_components || decompose_components_per_iter))
+    if (result == 0 && (P.decompose_components || P.decompose_components_per_iter)) {
+        std::fill(done.begin(), done.end(), 0);
         result = L.split_components(parts, unchecked(), cc_counter);
+    }
     // ---- merge-hulls post-pass (csrc/lookahead.c:987-1063, cuda/postprocess_merge.cu:41-679):
-    //      one greedy round of pairwise merges whose merged cost stays below tau
-    if (result == 0 && merge_hulls && parts.size() >= 2)
-        result = merge_hulls_pass(ctx, L, parts, threshold, d_surfs, d_preps, d_dirs, d_i4, d_pmax);
-    // ---- results (host copies)
+    //      one greedy round of pairwise merges whose merged cost stays below tau, per mesh
+    if (result == 0 && P.merge_hulls) {
+        std::vector<HPart> merged;
+        for (int m = 0; m < n_mesh && result == 0; m++) {
+            std::vector<HPart> mine;
+            for (auto& p : parts) if (p.mesh == m) mine.push_back(p);
+            if (mine.size() >= 2)
+                result = merge_hulls_pass(ctx, L, mine, P.threshold, d_surfs, d_preps, d_dirs, d_i4, d_pmax);
+            merged.insert(merged.end(), mine.begin(), mine.end());
+        }
+        if (result == 0) parts.swap(merged);
+    }
+    // ---- results (host copies), per mesh in part order
     if (result == 0) {
-        out->parts = (gpu_part_result*)calloc(parts.size() > 0 ? parts.size() : 1, sizeof(gpu_part_result));
-        out->nparts = (int)parts.size();
+        std::vector<int> count(n_mesh, 0);
+        for (auto& p : parts) count[p.mesh]++;
+        for (int m = 0; m < n_mesh; m++) {
+            outs[m].parts = (gpu_part_result*)calloc(count[m] > 0 ? count[m] : 1, sizeof(gpu_part_result));
+            outs[m].nparts = 0;
+        }
         for (size_t i = 0; i < parts.size() && result == 0; i++) {
             const HPart& p = parts[i];
-            gpu_part_result& r = out->parts[i];
+            gpu_part_result& r = outs[p.mesh].parts[outs[p.mesh].nparts++];
             r.nv = p.nv; r.nt = p.nt; r.hull_nv = p.hnv; r.hull_nt = p.hnt;
             r.verts = (float*)malloc(12 * (size_t)(p.nv > 0 ? p.nv : 1));
             r.tris = (int*)malloc(12 * (size_t)(p.nt > 0 ? p.nt : 1));
             r.hull_verts = (float*)malloc(12 * (size_t)(p.hnv > 0 ? p.hnv : 1));
             r.hull_tris = (int*)malloc(12 * (size_t)(p.hnt > 0 ? p.hnt : 1));
             r.mesh_vol = (float)p.mesh_vol; r.hull_vol = (float)p.hull_vol; r.hausdorff = (float)std::max(p.hd, 0.0);
-            cudaError_t e1 = cudaMemcpy(r.verts, p.v, 12 * (size_t)p.nv, cudaMemcpyDeviceToHost);
-            cudaError_t e2 = cudaMemcpy(r.tris, p.t, 12 * (size_t)p.nt, cudaMemcpyDeviceToHost);
-            cudaError_t e3 = p.hnv ? cudaMemcpy(r.hull_verts, p.hv, 12 * (size_t)p.hnv, cudaMemcpyDeviceToHost) : cudaSuccess;
-            cudaError_t e4 = p.hnt ? cudaMemcpy(r.hull_tris, p.ht, 12 * (size_t)p.hnt, cudaMemcpyDeviceToHost) : cudaSuccess;
+            cudaError_t e1 = cudaMemcpyAsync(r.verts, p.v, 12 * (size_t)p.nv, cudaMemcpyDeviceToHost, s);
+            cudaError_t e2 = cudaMemcpyAsync(r.tris, p.t, 12 * (size_t)p.nt, cudaMemcpyDeviceToHost, s);
+            cudaError_t e3 = p.hnv ? cudaMemcpyAsync(r.hull_verts, p.hv, 12 * (size_t)p.hnv, cudaMemcpyDeviceToHost, s) : cudaSuccess;
+            cudaError_t e4 = p.hnt ? cudaMemcpyAsync(r.hull_tris, p.ht, 12 * (size_t)p.hnt, cudaMemcpyDeviceToHost, s) : cudaSuccess;
             if (e1 || e2 || e3 || e4) result = ctx_fail(ctx, -1, "result copy failed");
         }
+        if (cudaStreamSynchronize(s) != cudaSuccess && result == 0) result = ctx_fail(ctx, -1, "result copy failed");
     }
     for (auto& p : parts) L.free_part(p);
     cudaStreamSynchronize(s);
-    if (result) { gpu_result_free(out); return result; }
+    if (result) { for (int m = 0; m < n_mesh; m++) gpu_result_free(&outs[m]); return result; }
     return 0;
+}
+
+static SearchParams search_params(int max_iters, int width, int width2, float threshold, int depth, int quick_depth,
+                                  int max_n_cutting, int verbose, int debug, int decompose_components,
+                                  int decompose_components_per_iter, int n_concave_edges, float concave_eps,
+                                  float concave_threshold, int concave_iters, int merge_hulls, int bnb)
+{
+    SearchParams P;
+    P.max_iters = max_iters; P.width = width; P.width2 = width2; P.threshold = threshold; P.depth = depth;
+    P.quick_depth = quick_depth; P.max_n_cutting = max_n_cutting; P.verbose = verbose; P.debug = debug;
+    P.decompose_components = decompose_components; P.decompose_components_per_iter = decompose_components_per_iter;
+    P.n_concave_edges = n_concave_edges; P.concave_eps = concave_eps; P.concave_threshold = concave_threshold;
+    P.concave_iters = concave_iters; P.merge_hulls = merge_hulls; P.bnb = bnb;
+    return P;
 }
 
 extern "C" int lookahead_decompose(gpu_ctx_t ctx, const float* verts, int nv, const int* tris, int nt,
@@ -1299,11 +1738,12 @@ extern "C" int lookahead_decompose(gpu_ctx_t ctx, const float* verts, int nv, co
                                    int n_concave_edges, float concave_eps, float concave_threshold,
                                    int concave_iters, int merge_hulls, struct gpu_result* out)
 {
-    (void)quick_depth; (void)merge_hulls;
-    return lookahead_impl(ctx, verts, nv, tris, nt, hull_verts, hull_nv, hull_tris, hull_nt, max_iters, width, width2,
-                          threshold, depth, max_n_cutting, verbose, debug, decompose_components,
-                          decompose_components_per_iter, n_concave_edges, concave_eps, concave_threshold,
-                          concave_iters, merge_hulls, nullptr, out);
+    if (!ctx || !out) return -1;
+    MeshIn m{verts, nv, tris, nt, hull_verts, hull_nv, hull_tris, hull_nt};
+    SearchParams P = search_params(max_iters, width, width2, threshold, depth, quick_depth, max_n_cutting, verbose,
+                                   debug, decompose_components, decompose_components_per_iter, n_concave_edges,
+                                   concave_eps, concave_threshold, concave_iters, merge_hulls, 1);
+    return search_group(ctx, 1, &m, P, nullptr, nullptr, out);
 }
 
 extern "C" int cuacd_lookahead_decompose_pruned(gpu_ctx_t ctx, cuacd_scorer_t scorer, int top_k, float margin,
@@ -1316,14 +1756,72 @@ extern "C" int cuacd_lookahead_decompose_pruned(gpu_ctx_t ctx, cuacd_scorer_t sc
                                                 int n_concave_edges, float concave_eps, float concave_threshold,
                                                 int concave_iters, struct gpu_result* out)
 {
-    if (!ctx) return -1;
+    if (!ctx || !out) return -1;
     unsigned long long st[3] = {0, 0, 0};
-    Prune P{scorer, top_k > 0 ? top_k : 1, margin, beam, st};
-    int rc = lookahead_impl(ctx, verts, nv, tris, nt, hull_verts, hull_nv, hull_tris, hull_nt, max_iters, width,
-                            width2, threshold, depth, max_n_cutting, verbose, 0, decompose_components,
-                            decompose_components_per_iter, n_concave_edges, concave_eps, concave_threshold,
-                            concave_iters, 0, &P, out);
+    Prune PR{scorer, top_k > 0 ? top_k : 1, margin, beam, st};
+    MeshIn m{verts, nv, tris, nt, hull_verts, hull_nv, hull_tris, hull_nt};
+    SearchParams P = search_params(max_iters, width, width2, threshold, depth, 0, max_n_cutting, verbose, 0,
+                                   decompose_components, decompose_components_per_iter, n_concave_edges, concave_eps,
+                                   concave_threshold, concave_iters, 0, 1);
+    int rc = search_group(ctx, 1, &m, P, &PR, nullptr, out);
     if (out_stats) for (int k = 0; k < 3; k++) out_stats[k] = st[k];
+    return rc;
+}
+
+extern "C" int cuacd_lookahead_decompose_batch(gpu_ctx_t ctx, int n_meshes,
+                                               const float* verts, const int* vert_off,
+                                               const int* tris, const int* tri_off,
+                                               const float* hull_verts, const int* hull_vert_off,
+                                               const int* hull_tris, const int* hull_tri_off,
+                                               int max_iters, int width, int width2, float threshold,
+                                               int depth, int quick_depth, int max_n_cutting, int verbose,
+                                               int decompose_components, int decompose_components_per_iter,
+                                               int n_concave_edges, float concave_eps, float concave_threshold,
+                                               int concave_iters, int merge_hulls, int branch_and_bound,
+                                               cuacd_scorer_t scorer, int top_k, float margin, int beam,
+                                               unsigned long long* out_stats, struct gpu_result* out)
+{
+    if (!ctx || !out || n_meshes < 0) return -1;
+    if (n_meshes == 0) return 0;
+    if (!verts || !vert_off || !tris || !tri_off || !hull_verts || !hull_vert_off || !hull_tris || !hull_tri_off)
+        return ctx_fail(ctx, KERR_MESH_INVALID, "null mesh arrays");
+    std::vector<MeshIn> M(n_meshes);
+    for (int m = 0; m < n_meshes; m++) {
+        if (vert_off[m + 1] < vert_off[m] || tri_off[m + 1] < tri_off[m] || hull_vert_off[m + 1] < hull_vert_off[m] ||
+            hull_tri_off[m + 1] < hull_tri_off[m])
+            return ctx_fail(ctx, KERR_MESH_INVALID, "mesh %d: decreasing offsets", m);
+        M[m] = {verts + 3 * (size_t)vert_off[m], vert_off[m + 1] - vert_off[m], tris + 3 * (size_t)tri_off[m],
+                tri_off[m + 1] - tri_off[m], hull_verts + 3 * (size_t)hull_vert_off[m],
+                hull_vert_off[m + 1] - hull_vert_off[m], hull_tris + 3 * (size_t)hull_tri_off[m],
+                hull_tri_off[m + 1] - hull_tri_off[m]};
+    }
+    for (int m = 0; m < n_meshes; m++) { out[m].parts = nullptr; out[m].nparts = 0; }
+    unsigned long long pst[3] = {0, 0, 0};
+    Prune PR{scorer, top_k > 0 ? top_k : 1, margin, beam, pst};
+    const bool use_prune = scorer != nullptr || beam > 0;
+    SearchParams P = search_params(max_iters, width, width2, threshold, depth, quick_depth, max_n_cutting, verbose,
+                                   0, decompose_components, decompose_components_per_iter, n_concave_edges,
+                                   concave_eps, concave_threshold, concave_iters, merge_hulls, branch_and_bound);
+    unsigned long long st[ST_N] = {0, 0, 0, 0, 0, 0, 0, 0};
+    // groups of consecutive meshes: the level output of a group's cutting parts
+    // must fit one output arena
+    const size_t group_elems = (size_t)3 << 20;
+    const int group_meshes = 256;
+    int g = 0, rc = 0;
+    while (g < n_meshes && rc == 0) {
+        size_t acc = 0;
+        int g1 = g;
+        while (g1 < n_meshes && g1 - g < group_meshes) {
+            const size_t e = (size_t)M[g1].nv + M[g1].nt;
+            if (g1 > g && acc + e > group_elems) break;
+            acc += e; g1++;
+        }
+        rc = search_group(ctx, g1 - g, M.data() + g, P, use_prune ? &PR : nullptr, st, out + g);
+        g = g1;
+    }
+    if (rc) { for (int m = 0; m < n_meshes; m++) gpu_result_free(&out[m]); }
+    st[ST_RANKED] = pst[0]; st[ST_CUT] = pst[1]; st[ST_EXPANDED] = pst[2];
+    if (out_stats) for (int k = 0; k < ST_N; k++) out_stats[k] = st[k];
     return rc;
 }
 
@@ -1340,10 +1838,12 @@ extern "C" int cuacd_lookahead_trace(gpu_ctx_t ctx, cuacd_scorer_t scorer, float
     const int W = scorer_n_features() + 4;
     std::vector<float> rows;
     unsigned long long st[3] = {0, 0, 0};
-    Prune P{scorer, 0, 0.f, 0, st, &rows, (size_t)max_rows * W, 0, {}, {}};
-    int rc = lookahead_impl(ctx, verts, nv, tris, nt, hull_verts, hull_nv, hull_tris, hull_nt, max_iters, width,
-                            width2, threshold, depth, max_n_cutting, 0, 0, 0, 1, n_concave_edges, concave_eps,
-                            concave_threshold, concave_iters, 0, &P, out);
+    Prune PR{scorer, 0, 0.f, 0, st, &rows, (size_t)max_rows * W, 0, {}, {}};
+    MeshIn m{verts, nv, tris, nt, hull_verts, hull_nv, hull_tris, hull_nt};
+    // no branch and bound: every level-0 candidate's path cost is traced
+    SearchParams P = search_params(max_iters, width, width2, threshold, depth, 0, max_n_cutting, 0, 0, 0, 1,
+                                   n_concave_edges, concave_eps, concave_threshold, concave_iters, 0, 0);
+    int rc = search_group(ctx, 1, &m, P, &PR, nullptr, out);
     if (rc) return rc;
     const int n = (int)(rows.size() / W);
     memcpy(out_rows, rows.data(), sizeof(float) * (size_t)n * W);

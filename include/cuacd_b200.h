@@ -396,8 +396,11 @@ struct gpu_result {
 /* Replaces gpu_result_free (csrc/heap.h:85). */
 void gpu_result_free(struct gpu_result* result);
 
-/* Replaces lookahead_decompose (csrc/lookahead.h:28-43).  quick_depth is
- * accepted and ignored; merge_hulls runs the merge-hulls post-pass
+/* Replaces lookahead_decompose (csrc/lookahead.h:28-43).  quick_depth adds
+ * the reference's quick levels after the `depth` full ones
+ * (cuda/la_refine.cu:52-351); the last level runs the reference's branch and
+ * bound (cuda/la_expand.cu:380-457), with the path bound taken per cutting
+ * part; merge_hulls runs the merge-hulls post-pass
  * (cuda/postprocess_merge.cu:41-679). */
 int lookahead_decompose(gpu_ctx_t ctx,
                         const float* verts, int nv, const int* tris, int nt,
@@ -430,6 +433,33 @@ int cuacd_lookahead_decompose_pruned(gpu_ctx_t ctx, cuacd_scorer_t scorer, int t
                                      int n_concave_edges, float concave_eps,
                                      float concave_threshold, int concave_iters,
                                      struct gpu_result* out);
+
+/* lookahead_decompose over a batch of meshes (no counterpart in the
+ * reference, whose call takes one mesh).  Mesh m is vertices
+ * [vert_off[m], vert_off[m+1]) and triangles [tri_off[m], tri_off[m+1]) of
+ * the packed arrays, with indices relative to its own first vertex; its
+ * convex hull likewise (hull_vert_off / hull_tri_off).  The meshes are
+ * searched together -- every level's cuts and hulls of all meshes still
+ * running go out as shared launches -- and every choice stays per part, so
+ * out[m] holds exactly the parts a lookahead_decompose of mesh m alone
+ * returns (with the same scorer, top_k, margin and beam as
+ * cuacd_lookahead_decompose_pruned when scorer != NULL or beam > 0).
+ * branch_and_bound = 0 turns the last level's bound off.  out_stats
+ * (optional, 8 values): level-0 planes ranked, planes cut, level-0 cuts
+ * expanded, fragment hulls built, items cut off by the bound, iterations
+ * run, 0, 0.  out: n_meshes results, each freed with gpu_result_free. */
+int cuacd_lookahead_decompose_batch(gpu_ctx_t ctx, int n_meshes,
+                                    const float* verts, const int* vert_off,
+                                    const int* tris, const int* tri_off,
+                                    const float* hull_verts, const int* hull_vert_off,
+                                    const int* hull_tris, const int* hull_tri_off,
+                                    int max_iters, int width, int width2, float threshold,
+                                    int depth, int quick_depth, int max_n_cutting, int verbose,
+                                    int decompose_components, int decompose_components_per_iter,
+                                    int n_concave_edges, float concave_eps, float concave_threshold,
+                                    int concave_iters, int merge_hulls, int branch_and_bound,
+                                    cuacd_scorer_t scorer, int top_k, float margin, int beam,
+                                    unsigned long long* out_stats, struct gpu_result* out);
 
 /* Exact lookahead_decompose that also records, for every level-0 candidate
  * that splits its part, the scorer's feature row followed by 4 floats: the
