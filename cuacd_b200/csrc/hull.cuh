@@ -63,8 +63,11 @@ __host__ __device__ inline HullCaps hull_caps(int n)
     c.m_leaves = (n + HULL_LEAF - 1) / HULL_LEAF;
     if (c.m_leaves < 1) c.m_leaves = 1;
     c.P = hull_pow2(c.m_leaves);
+    // every point may be a hull vertex (a convex cloud, such as the vertices
+    // of a fine sphere, has all of them on its hull); clouds are limited to
+    // 2^22 points, which keeps every table below within int range
     int h = n < 4 ? 4 : n;
-    if (h > 65536) h = 65536;
+    if (h > (1 << 22)) h = 1 << 22;
     c.hcap = h;
     c.ccap = 6 * h + 64;
     c.fcap = 2 * h + 8;

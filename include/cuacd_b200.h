@@ -118,6 +118,14 @@ int gpu_test_plane_cut(gpu_ctx_t ctx,
 int gpu_mesh_audit(gpu_ctx_t ctx, const float* verts, int n_verts, const int* tris, int n_tris,
                    unsigned int* out_flags);
 
+/* Stands in for gpu_preprocess (csrc/preprocess.h:17-24), the PaMO remesh
+ * of the reference's front end, which this library does not build: it
+ * writes NULL / 0 to the outputs and returns -1 with the reason in
+ * gpu_last_error, so the reference's CPython module links unchanged and its
+ * preprocess() raises RuntimeError. */
+int gpu_preprocess(gpu_ctx_t ctx, const float* verts, int nv, const int* tris, int nt,
+                   int resolution, float** out_verts, int* out_nv, int** out_tris, int* out_nt);
+
 /* Replaces gpu_test_postprocess_dc (csrc/postprocess.h:20-27): split a mesh
  * into its vertex-connected components.  Component c's vertices go to
  * out_verts[c*max_verts_per*3 ...] and its triangles (component-local

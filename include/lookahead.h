@@ -1,0 +1,3 @@
+/* Reference header name (csrc/lookahead.h) mapped onto this library's C ABI,
+ * so the reference's csrc/module.c builds unchanged against it. */
+#include "cuacd_b200.h"

@@ -15,13 +15,21 @@ _LIB_PATH = os.path.join(_HERE, "libcuacd_oracle.so")
 _lib = None
 
 
+def reference_tree():
+    """Where the reference tree lies in this checkout's machine (the
+    CUACD_REFERENCE_TREE variable, else its mount point), or None."""
+    ref = os.environ.get("CUACD_REFERENCE_TREE", "/root/reference")
+    return ref if os.path.exists(os.path.join(ref, "cuda", "mm.cu")) else None
+
+
 def build():
     """Compile the oracle with its Makefile (gcc only), and the reference's
     own GPU path into oracle/_ref with Makefile.ref where the reference tree
     is present (it skips itself otherwise)."""
     subprocess.run(["make", "-s", "-C", _HERE], check=True)
-    ref = os.environ.get("CUACD_REFERENCE_TREE", "/root/reference")
-    subprocess.run(["make", "-s", "-j8", "-C", _HERE, "-f", "Makefile.ref", f"REF={ref}"], check=True)
+    ref = reference_tree()
+    if ref:
+        subprocess.run(["make", "-s", "-j8", "-C", _HERE, "-f", "Makefile.ref", f"REF={ref}"], check=True)
 
 
 class CandResult(ctypes.Structure):

@@ -10,9 +10,11 @@ small .npz.  The fixture is committed (tests/golden/ref_gpu.npz); the tests
 regenerate the inputs from the same seeds and compare the oracle (CPU) and
 this library's CUDA path (GPU) with the reference's results.
 
-usage (on a machine with a B200, after `make -f oracle/Makefile.ref`):
+usage (on a machine with a B200, after `make -f oracle/Makefile.ref REF=...`):
     python tests/golden/make_ref_gpu.py [out.npz]
-    python tests/golden/make_ref_gpu.py --audit [out.npz]   (mesh-audit verdicts: ref_gpu_audit.npz)
+    python tests/golden/make_ref_gpu.py --audit [out.npz]    (mesh-audit verdicts: ref_gpu_audit.npz)
+    python tests/golden/make_ref_gpu.py --concave [out.npz]  (concave-edge planes: ref_gpu_concave.npz)
+    python tests/golden/make_ref_gpu.py --search [out.npz]   (config-4 sample searches: ref_gpu_search.npz)
 """
 import importlib.machinery
 import importlib.util
@@ -25,7 +27,18 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.join(HERE, "..", "..")
 sys.path.insert(0, ROOT)
-from cuacd_b200 import workloads as W  # noqa: E402
+
+
+def _workloads():
+    """cuacd_b200/workloads.py (plain numpy) loaded by path, so that this
+    process, which runs the reference, never maps this library."""
+    spec = importlib.util.spec_from_file_location("_cuacd_workloads", os.path.join(ROOT, "cuacd_b200", "workloads.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+W = _workloads()
 
 REF_DIR = os.path.join(ROOT, "oracle", "_ref")
 
@@ -278,8 +291,105 @@ def main(out_path):
     print("wrote", out_path, os.path.getsize(out_path), "bytes")
 
 
+CONCAVE_KW = dict(eps=0.005, threshold=3.49)
+
+
+def concave_cases():
+    """(name, verts, tris, n_concave_edges): the config-3 sphere with its 16
+    sampled edges, the six ridged spheres of the search sample with 16 and
+    with 32, and the first displaced sphere of the config-4 sample (smooth:
+    no edge passes the dihedral test)."""
+    import bench as B
+    v3, t3 = W.candidate_mesh()
+    out = [("config3", v3, t3, 16)]
+    for k, (v, t) in enumerate(B.search_meshes()):
+        out += [(f"search{k}_16", v, t, 16), (f"search{k}_32", v, t, 32)]
+    c4 = W.batch_meshes(512, 500, 200_000, seed=3, select={0})
+    out.append(("config4_0", c4[0][0], c4[0][1], 16))
+    return [(n, np.ascontiguousarray(v, np.float32), np.ascontiguousarray(t, np.int32), e) for n, v, t, e in out]
+
+
+def main_concave(out_path):
+    """The planes the reference's la_find_concave_edges emits for each case,
+    through oracle/_ref/ref_concave.so (its kernel launched on a one-part
+    decomposition state, its own context set-up)."""
+    import ctypes
+    lib = ctypes.CDLL(os.path.join(REF_DIR, "ref_concave.so"))
+    P, I, F = ctypes.c_void_p, ctypes.c_int, ctypes.c_float
+    lib.gpu_set_fatbin.argtypes = [P, ctypes.c_size_t]
+    lib.gpu_init.argtypes = [ctypes.POINTER(P), I, ctypes.c_size_t]
+    lib.ref_concave_planes.argtypes = [P, P, I, P, I, I, F, F, P, ctypes.POINTER(I), ctypes.POINTER(I)]
+    with open(os.path.join(REF_DIR, "kernels.fatbin"), "rb") as f:
+        fat = f.read()
+    fat_buf = ctypes.create_string_buffer(fat, len(fat))
+    lib.gpu_set_fatbin(fat_buf, len(fat))
+    ctx = P()
+    rc = lib.gpu_init(ctypes.byref(ctx), 0, 2 << 30)
+    assert rc == 0, rc
+    rec = {}
+    for name, v, t, ne in concave_cases():
+        out = np.zeros((4 * ne, 4), np.float32)
+        n, err = I(0), I(0)
+        rc = lib.ref_concave_planes(ctx, v.ctypes.data, len(v), t.ctypes.data, len(t), ne, CONCAVE_KW["eps"],
+                                    CONCAVE_KW["threshold"], out.ctypes.data, ctypes.byref(n), ctypes.byref(err))
+        assert rc == 0 and err.value == 0, (name, rc, err.value)
+        rec[f"{name}_planes"] = out[:n.value].copy()
+        rec[f"{name}_n_edges"] = np.array([ne], np.int32)
+        print(name, n.value, "planes", flush=True)
+    np.savez_compressed(out_path, **rec)
+
+
+def main_search(out_path):
+    """Per mesh of config 4's 64-mesh sample: the reference's part count and
+    its largest part rv cost (FP64 volumes) under config 4's settings."""
+    g = load_ref()
+    c4 = W.batch_meshes(512, 500, 200_000, seed=3, select={i for i in range(512) if i % 16 in (0, 5)})
+    parts, worst = [], []
+    for v, t in c4:
+        raw = ref_lookahead_parts(g, v, t)
+        parts.append(len(raw))
+        w = 0.0
+        for pv, pt, hv, ht in raw:
+            gap = max(abs(vol64(hv, ht)) - abs(vol64(pv, pt)), 0.0) if len(ht) else 0.0
+            w = max(w, 0.3 * np.cbrt(3.0 / (4.0 * np.pi) * gap))
+        worst.append(w)
+    g.destroy()
+    np.savez_compressed(out_path, parts=np.array(parts, np.int32), max_rv=np.array(worst),
+                        tris=np.array([len(t) for _, t in c4], np.int32))
+    print("parts", sum(parts), "max rv", max(worst), flush=True)
+
+
+def ref_lookahead_parts(g, v, t):
+    """The reference's lookahead_decompose as its wrapper drives it, with
+    LOOKAHEAD_KW; the parts as (verts, tris, hull verts, hull tris)."""
+    import scipy.spatial
+    v = np.ascontiguousarray(v, np.float32)
+    t = np.ascontiguousarray(t, np.int32)
+    h = scipy.spatial.ConvexHull(v)
+    hv = np.ascontiguousarray(h.points, np.float32)
+    ht = np.ascontiguousarray(h.simplices, np.int32)
+    cen = hv.mean(0)
+    nrm = np.cross(hv[ht[:, 1]] - hv[ht[:, 0]], hv[ht[:, 2]] - hv[ht[:, 0]])
+    inward = (nrm * (hv[ht[:, 0]] - cen)).sum(1) < 0
+    ht[inward] = ht[inward][:, [0, 2, 1]]
+    kw = LOOKAHEAD_KW
+    raw = g.lookahead_decompose(v.ctypes.data, len(v), t.ctypes.data, len(t), hv.ctypes.data, len(hv),
+                                ht.ctypes.data, len(ht), kw["max_iters"], kw["width"], kw["width2"],
+                                kw["threshold"], kw["depth"], kw["quick_depth"], kw["max_n_cutting"], 0, 0,
+                                n_concave_edges=kw["n_concave_edges"])
+    out = []
+    for vb, tb, nv, nt, hvb, htb, hnv, hnt, _, _ in raw:
+        out.append((np.frombuffer(vb, np.float32).reshape(nv, 3), np.frombuffer(tb, np.int32).reshape(nt, 3),
+                    np.frombuffer(hvb, np.float32).reshape(hnv, 3), np.frombuffer(htb, np.int32).reshape(hnt, 3)))
+    return out
+
+
 if __name__ == "__main__":
     if len(sys.argv) > 1 and sys.argv[1] == "--audit":
         main_audit(sys.argv[2] if len(sys.argv) > 2 else os.path.join(HERE, "ref_gpu_audit.npz"))
+    elif len(sys.argv) > 1 and sys.argv[1] == "--concave":
+        main_concave(sys.argv[2] if len(sys.argv) > 2 else os.path.join(HERE, "ref_gpu_concave.npz"))
+    elif len(sys.argv) > 1 and sys.argv[1] == "--search":
+        main_search(sys.argv[2] if len(sys.argv) > 2 else os.path.join(HERE, "ref_gpu_search.npz"))
     else:
         main(sys.argv[1] if len(sys.argv) > 1 else os.path.join(HERE, "ref_gpu.npz"))

@@ -103,3 +103,30 @@ def test_duplicated_extreme_point(ctx, oracle):
     g = np.load(os.path.join(GOLDEN, "hull_dup_corner.npz"))
     clouds = [g["c0"], g["c1"]]
     _check_exact(oracle, clouds, _gpu_hulls(ctx, clouds))
+
+
+def test_hull_above_65536_vertices(ctx):
+    """A convex cloud whose hull has more than 65,536 vertices (the 163,842
+    vertices of a level-7 icosphere: 79,206 on the hull grid), directly and
+    as a fragment of the evaluator: the same vertex sets and sizes as the
+    oracle (tests/golden/hull_big.npz, made by make_big_hull.py), never a
+    truncated hull."""
+    d = np.load(os.path.join(GOLDEN, "hull_big.npz"))
+    v, t = W.icosphere(7)
+    v = v.astype(np.float32)
+    (hv, ht, vol), = ctx.batch_hull_dandc_mesh([v])
+    first = {}
+    for i, p in enumerate(map(tuple, v.tolist())):
+        first.setdefault(p, i)
+    idx = np.sort(np.array([first[tuple(p)] for p in hv.tolist()], np.int32))
+    assert len(idx) > 65536
+    np.testing.assert_array_equal(idx, np.sort(d["ico7_idx"]))
+    assert len(ht) == 2 * len(hv) - 4
+    r = ctx.eval_candidates(v, t, d["cut_plane"], hausdorff=False)[0]
+    assert r["err"] == 0 and r["ok"] == int(d["cut_ok"])
+    assert tuple(r["nv"]) == tuple(d["cut_nv"]) and tuple(r["nt"]) == tuple(d["cut_nt"])
+    assert tuple(r["hull_nv"]) == tuple(d["cut_hull_nv"]) and tuple(r["hull_nt"]) == tuple(d["cut_hull_nt"])
+    assert max(r["hull_nv"]) > 65536
+    for s in range(2):
+        assert abs(r["hull_vol"][s] - d["cut_hull_vol"][s]) <= VOL_RTOL * d["cut_hull_vol"][s]
+        assert abs(r["mesh_vol"][s] - d["cut_mesh_vol"][s]) <= VOL_RTOL * d["cut_mesh_vol"][s]

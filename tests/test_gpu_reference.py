@@ -75,3 +75,31 @@ def test_lookahead_part_count(ctx, k):
     hv = ctx.batch_mesh_volume([p[2] for p in parts], [p[3] for p in parts])
     rv = 0.3 * np.cbrt(3.0 / (4.0 * np.pi) * np.maximum(hv.astype(np.float64) - vol, 0.0))
     assert rv.max() < M.LOOKAHEAD_KW["threshold"] + 1e-6, rv.max()
+
+
+def _max_rv(parts):
+    worst = 0.0
+    for pv, pt, hv, ht in parts:
+        gap = max(abs(M.vol64(hv, ht)) - abs(M.vol64(pv, pt)), 0.0) if len(ht) else 0.0
+        worst = max(worst, 0.3 * np.cbrt(3.0 / (4.0 * np.pi) * gap))
+    return worst
+
+
+def test_config4_sample_searches_match_reference(ctx):
+    """Config 4's 64-mesh sample (displaced spheres and unions of boxes,
+    540-327,680 triangles) with config 4's settings, as one batched search:
+    per mesh at most 10 % more parts than the reference's own search
+    (tests/golden/ref_gpu_search.npz, recorded on a B200), every part at or
+    below tau (north-star acceptance), and the same total."""
+    import os
+    d = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "ref_gpu_search.npz"))
+    meshes = M.W.batch_meshes(512, 500, 200_000, seed=3, select={i for i in range(512) if i % 16 in (0, 5)})
+    assert [len(t) for _, t in meshes] == d["tris"].tolist()
+    kw = dict(M.LOOKAHEAD_KW)
+    kw.pop("quick_depth")
+    res = ctx.lookahead_decompose_batch(meshes, **kw)
+    counts = np.array([len(p) for p in res])
+    assert (counts <= 1.1 * d["parts"]).all(), (counts, d["parts"])
+    assert abs(int(counts.sum()) - int(d["parts"].sum())) <= 0.1 * d["parts"].sum()
+    for p in res:
+        assert _max_rv(p) <= M.LOOKAHEAD_KW["threshold"] + 1e-6

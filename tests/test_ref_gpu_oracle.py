@@ -1,6 +1,10 @@
 """The oracle against the reference's own GPU outputs on the same seeded
 inputs: hull vertex sets (D&C and k-DOP paths), mesh volumes, plane-cut
-topology and fragment volumes, sampled Hausdorff distances."""
+topology and fragment volumes, sampled Hausdorff distances, concave-edge
+planes (tests/golden/ref_gpu_concave.npz)."""
+import functools
+import os
+
 import numpy as np
 import pytest
 
@@ -48,3 +52,32 @@ def test_hausdorff(oracle):
         hv, ht = REF[f"hd{k}_hull_v"], REF[f"hd{k}_hull_t"]
         o = oracle.hausdorff(hv, ht, v, t, threads=8)
         assert abs(o - float(REF[f"hd{k}_dist"][0])) < RC.HD_ATOL, k
+
+
+CONCAVE = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "ref_gpu_concave.npz"))
+
+
+@functools.lru_cache(maxsize=1)
+def _concave_cases():
+    return {c[0]: c for c in M.concave_cases()}
+
+
+@pytest.mark.parametrize("case", list(_concave_cases()))
+def test_concave_planes_match_reference(oracle, case):
+    """The planes the reference's own kernel (la_find_concave_edges,
+    cuda/la_concave.cu:48-363) emitted for the case, recorded on a B200, as
+    a multiset against the oracle's: the same number of planes, each oracle
+    plane matched to its own reference plane within 1e-6 per coefficient
+    (the reference computes them with fast-math FP32, so the last bits
+    differ; its emission order is atomic, so only the multiset counts)."""
+    name, v, t, ne = _concave_cases()[case]
+    ref = CONCAVE[f"{name}_planes"]
+    ours = oracle.concave_planes(v, t, ne, M.CONCAVE_KW["eps"], M.CONCAVE_KW["threshold"])
+    assert len(ours) == len(ref)
+    used = np.zeros(len(ref), bool)
+    for p in ours:
+        d = np.abs(ref - p).max(axis=1)
+        d[used] = np.inf
+        j = int(np.argmin(d))
+        assert d[j] <= 1e-6, (case, p, ref[j])
+        used[j] = True
