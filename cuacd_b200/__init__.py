@@ -106,6 +106,9 @@ _opt("cuacd_lookahead_decompose_pruned", _I, [_P, _P, _I, _F, _I, _P, _P, _I, _P
 _opt("cuacd_lookahead_decompose_batch", _I, [_P, _I, _P, _P, _P, _P, _P, _P, _P, _P,
                                              _I, _I, _I, _F, _I, _I, _I, _I, _I, _I, _I, _F, _F, _I, _I, _I,
                                              _P, _I, _F, _I, _P, _P])
+_opt("cuacd_hull_set_tuning", _I, [_P, _I, _I, _I])
+_opt("cuacd_hull_get_tuning", _I, [_P, _I, ctypes.POINTER(_I), ctypes.POINTER(_I)])
+_opt("cuacd_device_info", _I, [_P, ctypes.c_char_p, _I, ctypes.POINTER(_I)])
 _opt("cuacd_candidate_planes", _I, [_P, _P, _I, _P, _I, _I, _F, _F, _I, _F, _P, _P, _P])
 _opt("cuacd_profile_stages", _I, [_P, _I])
 _opt("cuacd_stage_times", _I, [_P, _P])
@@ -172,6 +175,9 @@ class Context:
             raise RuntimeError(f"cuacd error {rc}: gpu_init failed")
         self._h = h
         self._alive = True
+        # launch shapes tuned for this device by cuacd_b200.autotune, if stored
+        from . import autotune
+        autotune.apply_stored(self)
 
     # -- lifecycle ---------------------------------------------------------
     def close(self):

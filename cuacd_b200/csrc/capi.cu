@@ -93,6 +93,16 @@ extern "C" void gpu_destroy(gpu_ctx_t ctx)
 }
 
 extern "C" const char* gpu_last_error(gpu_ctx_t ctx) { return ctx ? ctx->last_error : "no context"; }
+
+extern "C" int cuacd_device_info(gpu_ctx_t ctx, char* name, int cap, int* n_sm)
+{
+    if (!ctx) return -1;
+    cudaDeviceProp prop;
+    CK(cudaGetDeviceProperties(&prop, ctx->device));
+    if (name && cap > 0) { strncpy(name, prop.name, (size_t)cap - 1); name[cap - 1] = 0; }
+    if (n_sm) *n_sm = ctx->n_sm;
+    return 0;
+}
 extern "C" int gpu_heap_compact(gpu_ctx_t ctx) { (void)ctx; return 0; }
 extern "C" size_t gpu_pool_usage(gpu_ctx_t ctx)
 {
@@ -134,7 +144,7 @@ static int launch_hull_batch(gpu_ctx* ctx, const float* d_pts, const int* d_off,
                              int* d_nv, int* d_nt, float* d_vol, int* d_err, cudaStream_t s,
                              unsigned long long* d_stats = nullptr)
 {
-    const int nwc = hull_wrap_ctas(hull_wrap_points(n_hulls, max_pts), ctx->n_sm);
+    const int nwc = hull_wrap_ctas(hull_wrap_points(n_hulls, max_pts), ctx->n_sm, max_pts);
     HullJob* jobs = pool_take<HullJob>(ctx, n_hulls);
     HullState* states = pool_take<HullState>(ctx, n_hulls);
     HullRes* res = pool_take<HullRes>(ctx, n_hulls);
@@ -145,7 +155,7 @@ static int launch_hull_batch(gpu_ctx* ctx, const float* d_pts, const int* d_off,
     if (!scratch) return ctx_fail(ctx, KERR_HEAP_OOM, "hull scratch does not fit the pool");
     launch_arena_reset(ctx->d_arena, scratch, scr_bytes, s);
     launch_jobs_from_offsets(d_pts, d_off, n_hulls, d_v, d_t, max_hv, max_ht, jobs, s);
-    launch_hull_jobs(jobs, n_hulls, states, res, ctx->d_arena, ctx->d_arena, ctl, wbuf, nwc, d_stats, s);
+    launch_hull_jobs(jobs, n_hulls, states, res, ctx->d_arena, ctx->d_arena, ctl, wbuf, nwc, d_stats, s, max_pts);
     launch_unpack_results(res, n_hulls, d_nv, d_nt, d_vol, d_err, s);
     ctx->launches += 6;
     CK(cudaGetLastError());
@@ -171,7 +181,7 @@ static int hull_common(gpu_ctx_t ctx, const float* pts, int total_pts, const int
     size_t need = al256(sizeof(float) * 3 * (size_t)total_pts) + al256(sizeof(int) * (size_t)(n_hulls + 1))
                 + al256(sizeof(float) * 3 * (size_t)n_hulls * max_hv) + al256(sizeof(int) * 3 * (size_t)n_hulls * max_ht)
                 + 4 * al256(sizeof(int) * (size_t)n_hulls)
-                + hull_batch_need(n_hulls, max_pts, hull_wrap_ctas(hull_wrap_points(n_hulls, max_pts), ctx->n_sm))
+                + hull_batch_need(n_hulls, max_pts, hull_wrap_ctas(hull_wrap_points(n_hulls, max_pts), ctx->n_sm, max_pts))
                 + al256(64 * (size_t)n_hulls);
     int rc = pool_begin(ctx, need);
     if (rc) return rc;
@@ -227,7 +237,7 @@ extern "C" int cuacd_hull_batch_device(gpu_ctx_t ctx, const float* d_pts, const 
     if (n_hulls <= 0) return 0;
     if (max_pts >= (1 << 22)) return ctx_fail(ctx, KERR_MESH_INVALID, "more than 2^22 points in one cloud");
     CK(cudaSetDevice(ctx->device));
-    int rc = pool_begin(ctx, hull_batch_need(n_hulls, max_pts, hull_wrap_ctas(hull_wrap_points(n_hulls, max_pts), ctx->n_sm)));
+    int rc = pool_begin(ctx, hull_batch_need(n_hulls, max_pts, hull_wrap_ctas(hull_wrap_points(n_hulls, max_pts), ctx->n_sm, max_pts)));
     if (rc) return rc;
     return launch_hull_batch(ctx, d_pts, d_offsets, n_hulls, max_pts, max_hv, max_ht, d_v, d_t, d_nv, d_nt,
                              d_vol, d_err, stream ? (cudaStream_t)stream : ctx->stream);

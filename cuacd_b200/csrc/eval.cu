@@ -130,6 +130,7 @@ struct EvalWork {
     float4* planes; CutResult* cuts; FragInfo* frags; HDSurf* surfs; HDPrep* preps;
     char* dirs; int* i4; float* pmax; float* hd;
     HullJob* jobs; HullState* states; int* hctl; int* wbuf; int nwc;
+    int max_pts;                       // largest fragment possible: the parent's vertex count
 };
 
 static size_t eval_fixed_bytes(int n, int nwc)
@@ -143,7 +144,7 @@ static size_t eval_fixed_bytes(int n, int nwc)
 
 static int eval_wrap_ctas(gpu_ctx* ctx, int nv, int n)
 {
-    return hull_wrap_ctas(2LL * n * nv, ctx->n_sm);
+    return hull_wrap_ctas(2LL * n * nv, ctx->n_sm, nv);
 }
 
 static size_t eval_arena_bytes(int nv, int nt, int n)
@@ -158,8 +159,9 @@ static size_t eval_arena_bytes(int nv, int nt, int n)
     return per * (size_t)n;
 }
 
-static int eval_take(gpu_ctx* ctx, int n, int nwc, EvalWork& W)
+static int eval_take(gpu_ctx* ctx, int n, int nwc, EvalWork& W, int max_pts)
 {
+    W.max_pts = max_pts;
     W.nwc = nwc;
     W.jobs = pool_take<HullJob>(ctx, 2 * n);
     W.states = pool_take<HullState>(ctx, 2 * n);
@@ -208,7 +210,7 @@ static void eval_launch_after_cut(gpu_ctx* ctx, int n, int flags, float res, int
         ctx->launches += 2;
     }
     launch_hull_jobs(W.jobs, 2 * n, W.states, W.frags, ctx->d_arena, ctx->d_arena, W.hctl, W.wbuf, W.nwc,
-                     nullptr, s);
+                     nullptr, s, W.max_pts);
     mark(2);
     ctx->launches += 6;
     if (hd && overlap) {
@@ -283,7 +285,7 @@ static int eval_groups_take(gpu_ctx* ctx, int nv, int n, int G, EvalWork* W)
 {
     for (int g = 0; g < G; g++) {
         int o, m; group_range(n, G, g, &o, &m);
-        if (eval_take(ctx, m, eval_wrap_ctas(ctx, nv, m), W[g])) return -1;
+        if (eval_take(ctx, m, eval_wrap_ctas(ctx, nv, m), W[g], nv)) return -1;
     }
     return 0;
 }
@@ -341,7 +343,7 @@ int eval_precut_begin(gpu_ctx* ctx, const float* d_v, int nv, const int* d_t, in
                              + eval_arena_bytes(nv, nt, n));
     if (rc) return rc;
     P.W = new EvalWork;
-    if (eval_take(ctx, n, P.nwc, *P.W)) return ctx_fail(ctx, KERR_HEAP_OOM, "pool too small");
+    if (eval_take(ctx, n, P.nwc, *P.W, nv)) return ctx_fail(ctx, KERR_HEAP_OOM, "pool too small");
     P.all_cuts = pool_take<CutResult>(ctx, n);
     if (!P.all_cuts) return ctx_fail(ctx, KERR_HEAP_OOM, "pool too small");
     cudaStream_t a = ctx->aux[0];

@@ -2,15 +2,17 @@
 // set-up (one CTA per cloud), shares of the wrap grid, persistent wrapping
 // (up to one CTA per SM; each CTA wraps its home cloud, then helps others),
 // output (one CTA per cloud).
+#include <mutex>
 #include "context.cuh"
 #include "hull.cuh"
 #include "hull_kernels.cuh"
 #include "launch.h"
 
 __global__ void __launch_bounds__(HULL_NT)
-k_hull_setup(const HullJob* __restrict__ jobs, int n_jobs, Arena* scratch, HullState* states, int* ctl)
+k_hull_setup(const HullJob* __restrict__ jobs, int n_jobs, Arena* scratch, HullState* states, int* ctl,
+             int seed_min_n)
 {
-    hull_setup_body(jobs, n_jobs, scratch, states, ctl);
+    hull_setup_body(jobs, n_jobs, scratch, states, ctl, seed_min_n);
 }
 
 // Wrap-grid shares (one CTA): prefix of the active hulls' weights, a hull's
@@ -60,13 +62,58 @@ static int hull_wrap_per_sm()
     return cached[dev];
 }
 
-static int hull_wrap_pts_per_cta() { return 4096; }
+// Tuned launch shape per size class of a batch's largest cloud (< 4,096
+// points, < 65,536, larger): points of the batch per wrap CTA (so warps per
+// cloud) and the cloud size from which wrapping starts at HULL_SEEDS seed
+// faces.  Per device; the defaults hold until cuacd_hull_set_tuning (the
+// autotuner, cuacd_b200/autotune.py) replaces them.
+struct HullTune { int pts_per_cta, seed_min_n; };
+static HullTune g_hull_tune[64][HULL_TUNE_CLASSES] = {};
+static std::mutex g_hull_tune_mu;
 
-// Wrap grid size: about one warp per 256 points of the batch, at most the
-// resident CTAs of the whole device.
-int hull_wrap_ctas(long long total_points, int n_sm)
+static int cur_device()
 {
-    long long c = (total_points + hull_wrap_pts_per_cta() - 1) / hull_wrap_pts_per_cta();
+    int dev = 0;
+    cudaGetDevice(&dev);
+    return dev >= 0 && dev < 64 ? dev : 0;
+}
+
+int hull_size_class(int max_pts) { return max_pts < 4096 ? 0 : (max_pts < 65536 ? 1 : 2); }
+
+static HullTune hull_tune(int cls)
+{
+    std::lock_guard<std::mutex> lock(g_hull_tune_mu);
+    HullTune t = g_hull_tune[cur_device()][cls];
+    if (t.pts_per_cta <= 0) t.pts_per_cta = 4096;
+    if (t.seed_min_n <= 0) t.seed_min_n = 1 << 30;
+    return t;
+}
+
+extern "C" int cuacd_hull_set_tuning(gpu_ctx_t ctx, int size_class, int pts_per_cta, int seed_min_n)
+{
+    if (!ctx || size_class < 0 || size_class >= HULL_TUNE_CLASSES || pts_per_cta < 0 || seed_min_n < 0) return -1;
+    cudaSetDevice(ctx->device);
+    std::lock_guard<std::mutex> lock(g_hull_tune_mu);
+    g_hull_tune[ctx->device >= 0 && ctx->device < 64 ? ctx->device : 0][size_class] = {pts_per_cta, seed_min_n};
+    return 0;
+}
+
+extern "C" int cuacd_hull_get_tuning(gpu_ctx_t ctx, int size_class, int* pts_per_cta, int* seed_min_n)
+{
+    if (!ctx || size_class < 0 || size_class >= HULL_TUNE_CLASSES || !pts_per_cta || !seed_min_n) return -1;
+    cudaSetDevice(ctx->device);
+    const HullTune t = hull_tune(size_class);
+    *pts_per_cta = t.pts_per_cta; *seed_min_n = t.seed_min_n;
+    return 0;
+}
+
+// Wrap grid size: total_points / the tuned points per CTA of the class of
+// max_pts (default 4,096: about one warp per 256 points), at most the
+// resident CTAs of the whole device.
+int hull_wrap_ctas(long long total_points, int n_sm, int max_pts)
+{
+    const int ppc = hull_tune(hull_size_class(max_pts)).pts_per_cta;
+    long long c = (total_points + ppc - 1) / ppc;
     const long long cap = (long long)n_sm * hull_wrap_per_sm();
     if (c < 1) c = 1;
     if (c > cap) c = cap;
@@ -75,11 +122,12 @@ int hull_wrap_ctas(long long total_points, int n_sm)
 
 void launch_hull_jobs(const HullJob* d_jobs, int n_jobs, HullState* d_states, HullRes* d_res, Arena* scratch,
                       Arena* out, int* d_ctl, int* d_wbuf, int n_wrap_ctas, unsigned long long* d_stats,
-                      cudaStream_t s)
+                      cudaStream_t s, int max_pts)
 {
     if (n_jobs <= 0) return;
+    const int seed_min_n = hull_tune(hull_size_class(max_pts)).seed_min_n;
     cudaMemsetAsync(d_ctl, 0, 4 * sizeof(int), s);
-    k_hull_setup<<<n_jobs, HULL_NT, 0, s>>>(d_jobs, n_jobs, scratch, d_states, d_ctl);
+    k_hull_setup<<<n_jobs, HULL_NT, 0, s>>>(d_jobs, n_jobs, scratch, d_states, d_ctl, seed_min_n);
     k_hull_assign<<<1, 1024, 0, s>>>(d_states, n_jobs, n_wrap_ctas, (long long*)(d_ctl + 2));
     hull_wrap_per_sm();                                   // dynamic shared memory opt-in
     k_hull_wrap<<<n_wrap_ctas, HULL_NT, HULL_WRAP_DSMEM, s>>>(d_states, n_jobs, d_ctl, (const long long*)(d_ctl + 2),

@@ -44,9 +44,9 @@
 #endif
 #define HULL_WL       (HULL_WSM - HULL_WQ)         //           kept-leaf list
 #define HULL_WRAP_DSMEM ((size_t)(HULL_NT / 32) * HULL_WSM * sizeof(int))
-#define HULL_SEEDS    1                            // seed faces (1..6) that start the wrapping; 6 seeds
-                                                   // measured slower (7.3 vs 6.4 ms hull stage, config 3):
-                                                   // their set-up costs more than the shorter chains save
+#define HULL_SEEDS    6                            // seed faces that start the wrapping of a cloud of at
+                                                   // least seed_min_n points (the tuned size class decides;
+                                                   // smaller clouds start from one)
 
 // Per-cloud scratch layout (bytes computed on the host by hull_scratch_bytes).
 struct HullCaps {
@@ -727,7 +727,7 @@ static __device__ __forceinline__ void cta_fill_ones64(unsigned long long* tab, 
 }
 
 static __device__ void hull_setup_cta(const float* __restrict__ pts, int n, char* scratch, HullState* S,
-                                      HullSetupShared& sh)
+                                      HullSetupShared& sh, int seed_min_n = 1 << 30)
 {
     const int tid = threadIdx.x;
     const long long t_begin = clock64();
@@ -1083,7 +1083,7 @@ static __device__ void hull_setup_cta(const float* __restrict__ pts, int n, char
         {0, 1, 1, 1, 2, 1, 0, 0, 1}, {0, -1, 1, -1, 2, 1, 0, 0, 1},
         {1, 1, 0, -1, 2, 1, 0, 0, 1}, {1, -1, 0, 1, 2, 1, 0, 0, 1},
         {2, 1, 1, 1, 0, 1, 1, 0, 0}, {2, -1, 1, -1, 0, 1, 1, 0, 0}};
-    const int n_seeds = n >= 64 ? HULL_SEEDS : 1;
+    const int n_seeds = (n >= 64 && n >= seed_min_n) ? HULL_SEEDS : 1;
     __shared__ int s_sp[6], s_sok[6];
     __shared__ double s_sN[6][3];
     for (int sd = 0; sd < n_seeds; sd++) {

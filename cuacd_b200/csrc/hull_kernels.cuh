@@ -5,7 +5,8 @@
 #pragma once
 #include "hull.cuh"
 
-static __device__ void hull_setup_body(const HullJob* __restrict__ jobs, int n_jobs, Arena* scratch, HullState* states, int* ctl)
+static __device__ void hull_setup_body(const HullJob* __restrict__ jobs, int n_jobs, Arena* scratch, HullState* states, int* ctl,
+                                       int seed_min_n = 1 << 30)
 {
     __shared__ HullSetupShared sh;
     __shared__ char* s_scr;
@@ -26,7 +27,7 @@ static __device__ void hull_setup_body(const HullJob* __restrict__ jobs, int n_j
         }
     }
     __syncthreads();
-    if (s_scr) hull_setup_cta(J.pts, J.n, s_scr, S, sh);
+    if (s_scr) hull_setup_cta(J.pts, J.n, s_scr, S, sh, seed_min_n);
     if (threadIdx.x == 0) {
         S->mesh_vol = fabs(mv);
         if (s_scr && S->active) atomicAdd(&ctl[0], 1);

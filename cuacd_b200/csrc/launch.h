@@ -47,7 +47,11 @@ struct HullJob;
 struct HullRes;
 struct HullState;
 size_t hull_wrap_buf_bytes(int n_wrap_ctas);
-int hull_wrap_ctas(long long total_points, int n_sm);
+#define HULL_TUNE_CLASSES 3
+int hull_size_class(int max_pts);
+// Wrap CTAs for a batch of total_points points whose largest cloud has
+// max_pts (its size class picks the tuned points per CTA).
+int hull_wrap_ctas(long long total_points, int n_sm, int max_pts = 1 << 30);
 // Points that size the wrap grid of a batch of n_hulls clouds of at most
 // max_pts points: small clouds count as 256 points each, so a batch of many
 // tiny clouds still gets about one warp per cloud.
@@ -57,7 +61,7 @@ inline long long hull_wrap_points(int n_hulls, int max_pts)
 }
 void launch_hull_jobs(const HullJob* d_jobs, int n_jobs, HullState* d_states, HullRes* d_res, Arena* scratch,
                       Arena* out, int* d_ctl, int* d_wbuf, int n_wrap_ctas, unsigned long long* d_stats,
-                      cudaStream_t s);
+                      cudaStream_t s, int max_pts);
 void launch_jobs_from_offsets(const float* d_pts, const int* d_off, int n, float* d_v, int* d_t, int max_hv,
                               int max_ht, HullJob* d_jobs, cudaStream_t s);
 void launch_unpack_results(const HullRes* d_res, int n, int* d_nv, int* d_nt, float* d_vol, int* d_err, cudaStream_t s);

@@ -489,9 +489,11 @@ struct Lookahead {
                 if (f1 > f && acc + e > scr_cap) break;
                 acc += e; f1++;
             }
+            long long pts = 0; int mx = 0;
+            for (int k = f; k < f1; k++) { pts += std::max(sizes[k], 256); mx = std::max(mx, sizes[k]); }
             reset_scr();
-            launch_hull_jobs(d_hjobs + f, f1 - f, d_hstates + f, res + f, d_scr, d_cur, d_hctl, d_wbuf, nwc,
-                             nullptr, s);
+            launch_hull_jobs(d_hjobs + f, f1 - f, d_hstates + f, res + f, d_scr, d_cur, d_hctl, d_wbuf,
+                             std::min(nwc, hull_wrap_ctas(pts, ctx->n_sm, mx)), nullptr, s, mx);
             ctx->launches += 5;
             f = f1;
         }

@@ -292,6 +292,21 @@ int cuacd_hull_stats(gpu_ctx_t ctx, const float* pts, int total_pts,
                      const int* offsets, int n_hulls, int* out_nv, int* out_nt,
                      float* out_vol, unsigned long long* out_stats);
 
+/* Launch-shape tuning of the batched hull pipeline (no counterpart in the
+ * reference, whose launch shapes are fixed: csrc/lookahead.c:572-573,
+ * 606-607).  Per device and per size class of a batch's largest cloud
+ * (0: < 4,096 points, 1: < 65,536, 2: larger): pts_per_cta = points of the
+ * batch per wrap CTA, i.e. how many warps share a cloud (0: the default
+ * 4,096); seed_min_n = clouds of at least this many points start wrapping
+ * from six seed faces instead of one (0: never).  cuacd_b200/autotune.py
+ * sweeps both with CUDA-event timing and stores the best per device. */
+int cuacd_hull_set_tuning(gpu_ctx_t ctx, int size_class, int pts_per_cta, int seed_min_n);
+int cuacd_hull_get_tuning(gpu_ctx_t ctx, int size_class, int* pts_per_cta, int* seed_min_n);
+
+/* The context's device: its name (NUL-terminated, at most cap bytes) and
+ * streaming multiprocessor count (no counterpart in the reference). */
+int cuacd_device_info(gpu_ctx_t ctx, char* name, int cap, int* n_sm);
+
 /* Diagnostic (no counterpart in the reference): cut one mesh by n_planes
  * planes and report 8 ints per plane: crossing edges, boundary edges, cap
  * loops, cap triangles, and the SM cycles / 64 spent in the crossing,
