@@ -1,6 +1,7 @@
 // scorer.cu — learned candidate scorer: per-plane features, a 240-256-256-1
-// MLP in BF16 with FP32 accumulation on the tensor cores (mma.sync
-// m16n8k16), its training (MSE, AdamW) and the pruned evaluator that sends
+// MLP in BF16 with FP32 accumulation on the 5th-generation tensor cores
+// (tcgen05.mma, accumulators in tensor memory), its training (MSE, AdamW) and
+// the pruned evaluator that sends
 // only the best-predicted planes through the exact evaluator.
 //
 // Features of plane (n, d) on a part (230 used of SC_K = 240), positions
@@ -181,16 +182,23 @@ k_cand_features(const float* __restrict__ v, int nv, const float4* __restrict__ 
 }
 
 // ---------------------------------------------------------------------------
-// GEMM on the tensor cores: C[M x N] = alpha * op(A)[M x K] * op(B)[K x N]
-// (+ C if accumulate) (+ bias[j]) (* (mask(i,j) > 0)) (relu), BF16 operands,
-// FP32 accumulation.  A(i,k) = A[i*ar + k*ac], B(k,j) = B[k*br + j*bc], so
-// transposed operands need no copy.  Block tile 64 x 64, K step 32, four
-// warps of 32 x 32 (2 x 4 mma.sync m16n8k16 tiles each).
+// GEMM on the 5th-generation tensor cores (tcgen05): C[M x N] = alpha *
+// op(A)[M x K] * op(B)[K x N] (+ C if accumulate) (+ bias[j]) (* (mask(i,j) >
+// 0)) (relu), BF16 operands, FP32 accumulation in tensor memory.  A(i,k) =
+// A[i*ar + k*ac], B(k,j) = B[k*br + j*bc], so transposed operands need no
+// copy: the CTA stages each 64-wide K slab of its 128 x 128 output tile into
+// shared memory in the K-major core-matrix layout of UMMA (8 rows x 16 bytes
+// per core matrix, no swizzle), one elected thread issues four
+// tcgen05.mma.cta_group::1.kind::f16 (M 128, N 128, K 16) into a 128-column
+// TMEM accumulator and commits them to an mbarrier, and after the last slab
+// the four warps read their 32 accumulator lanes each with tcgen05.ld for
+// the fused epilogue.  Every wait is bounded: a wait that gives up records
+// KERR_TIMEOUT in *err and the CTA still frees its tensor memory.
 // ---------------------------------------------------------------------------
-#define GM_BM 64
-#define GM_BN 64
-#define GM_BK 32
-#define GM_LD (GM_BK + 8)          // smem row pitch (bf16): rows stay 4-byte aligned, banks spread
+#define GM_BM 128
+#define GM_BN 128
+#define GM_BK 64
+#define GM_NT 128
 
 struct GemmArgs {
     const __nv_bfloat16* A; long long ar, ac;
@@ -201,84 +209,145 @@ struct GemmArgs {
     const __nv_bfloat16* mask; int ldm;
     float alpha;
     int relu, accumulate;
+    int* err;
 };
 
-static __device__ __forceinline__ void mma_bf16_16816(float* d, const unsigned* a, const unsigned* b)
+static __device__ __forceinline__ unsigned smem_addr(const void* p)
 {
-    asm volatile(
-        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 "
-        "{%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
-        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+    return (unsigned)__cvta_generic_to_shared(p);
 }
 
-__global__ void __launch_bounds__(128)
-k_gemm_bf16(GemmArgs g)
+// Shared-memory matrix descriptor of a K-major, unswizzled operand slab
+// (tcgen05 descriptor format: start, leading and stride byte offsets in 16 B
+// units, version 1 at bits 46-47, layout type 0 = no swizzle).
+static __device__ __forceinline__ unsigned long long umma_desc(unsigned addr, unsigned lbo, unsigned sbo)
 {
-    __shared__ __align__(16) __nv_bfloat16 As[GM_BM][GM_LD];
-    __shared__ __align__(16) __nv_bfloat16 Bs[GM_BN][GM_LD];     // B tile stored n-major (k contiguous)
+    return (unsigned long long)((addr >> 4) & 0x3FFF) | ((unsigned long long)((lbo >> 4) & 0x3FFF) << 16) |
+           ((unsigned long long)((sbo >> 4) & 0x3FFF) << 32) | (1ull << 46);
+}
+
+// Instruction descriptor of kind::f16: FP32 accumulator, BF16 A and B, both
+// K-major, N >> 3 at bits 17-22, M >> 4 at bits 24-28.
+static __host__ __device__ constexpr unsigned umma_idesc_bf16(int m, int n)
+{
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((unsigned)(n >> 3) << 17) | ((unsigned)(m >> 4) << 24);
+}
+
+// Bounded wait for the mbarrier phase `parity`; false when it gave up.
+static __device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity)
+{
+    for (int it = 0; it < (1 << 24); it++) {
+        unsigned done;
+        asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+                     " selp.u32 %0, 1, 0, p;\n}\n" : "=r"(done) : "r"(bar), "r"(parity) : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+// Element (r, k) of a 128-row, 64-wide K-major slab: core matrix
+// (k / 8, r / 8) of 128 bytes, row r % 8 at 16 bytes, column k % 8.
+static __device__ __forceinline__ int slab_index(int r, int k)
+{
+    return (((k >> 3) * (GM_BM / 8) + (r >> 3)) << 6) + ((r & 7) << 3) + (k & 7);
+}
+
+__global__ void __launch_bounds__(GM_NT)
+k_gemm_umma(GemmArgs g)
+{
+    __shared__ __align__(128) __nv_bfloat16 As[GM_BM * GM_BK];
+    __shared__ __align__(128) __nv_bfloat16 Bs[GM_BN * GM_BK];
+    __shared__ __align__(8) unsigned long long s_bar;
+    __shared__ unsigned s_tmem;
+    __shared__ int s_fail;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int m0 = blockIdx.y * GM_BM, n0 = blockIdx.x * GM_BN;
-    const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
-    const int gq = lane >> 2, tq = lane & 3;
-    float acc[2][4][4];
-    #pragma unroll
-    for (int i = 0; i < 2; i++)
-        #pragma unroll
-        for (int j = 0; j < 4; j++)
-            #pragma unroll
-            for (int k = 0; k < 4; k++) acc[i][j][k] = 0.f;
+    const unsigned bar = smem_addr(&s_bar);
+    if (warp == 0) {                                  // 128 fp32 columns of tensor memory
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     :: "r"(smem_addr(&s_tmem)), "r"(GM_BN) : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0) {
+        s_fail = 0;
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(bar), "r"(1) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const unsigned tmem = s_tmem;
     const __nv_bfloat16 zero = __float2bfloat16(0.f);
-    for (int k0 = 0; k0 < g.K; k0 += GM_BK) {
-        // stage the tiles; consecutive threads walk the operand's unit stride
-        for (int e = tid; e < GM_BM * GM_BK; e += 128) {
+    constexpr unsigned idesc = umma_idesc_bf16(GM_BM, GM_BN);
+    const unsigned a0 = smem_addr(As), b0 = smem_addr(Bs);
+    unsigned phase = 0;
+    bool issued = false;
+    for (int k0 = 0; k0 < g.K && !s_fail; k0 += GM_BK) {
+        // stage the slabs (zero outside the matrices); consecutive threads
+        // walk the operand's unit stride
+        for (int e = tid; e < GM_BM * GM_BK; e += GM_NT) {
             int r, c;
             if (g.ac == 1) { r = e / GM_BK; c = e % GM_BK; } else { c = e / GM_BM; r = e % GM_BM; }
             const int gi = m0 + r, gk = k0 + c;
-            As[r][c] = (gi < g.M && gk < g.K) ? g.A[gi * g.ar + gk * g.ac] : zero;
+            As[slab_index(r, c)] = (gi < g.M && gk < g.K) ? g.A[gi * g.ar + gk * g.ac] : zero;
         }
-        for (int e = tid; e < GM_BN * GM_BK; e += 128) {
+        for (int e = tid; e < GM_BN * GM_BK; e += GM_NT) {
             int n, c;
             if (g.br == 1) { n = e / GM_BK; c = e % GM_BK; } else { c = e / GM_BN; n = e % GM_BN; }
             const int gj = n0 + n, gk = k0 + c;
-            Bs[n][c] = (gj < g.N && gk < g.K) ? g.B[gk * g.br + gj * g.bc] : zero;
+            Bs[slab_index(n, c)] = (gj < g.N && gk < g.K) ? g.B[gk * g.br + gj * g.bc] : zero;
         }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // generic stores -> tensor-core reads
         __syncthreads();
-        #pragma unroll
-        for (int kk = 0; kk < GM_BK; kk += 16) {
-            unsigned af[2][4], bfr[4][2];
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             #pragma unroll
-            for (int i = 0; i < 2; i++) {
-                const int r = wm + 16 * i + gq;
-                af[i][0] = *(const unsigned*)&As[r][kk + 2 * tq];
-                af[i][1] = *(const unsigned*)&As[r + 8][kk + 2 * tq];
-                af[i][2] = *(const unsigned*)&As[r][kk + 2 * tq + 8];
-                af[i][3] = *(const unsigned*)&As[r + 8][kk + 2 * tq + 8];
+            for (int kk = 0; kk < GM_BK / 16; kk++) {
+                // K chunk pair (2kk, 2kk+1): leading offset = one chunk of
+                // 16 core matrices, stride offset = one core matrix
+                const unsigned off = (unsigned)(2 * kk * (GM_BM / 8) * 128);
+                const unsigned long long ad = umma_desc(a0 + off, (GM_BM / 8) * 128, 128);
+                const unsigned long long bd = umma_desc(b0 + off, (GM_BN / 8) * 128, 128);
+                const unsigned acc = (k0 > 0 || kk > 0) ? 1u : 0u;
+                asm volatile("{\n .reg .pred p;\n setp.ne.u32 p, %4, 0;\n"
+                             " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n"
+                             :: "r"(tmem), "l"(ad), "l"(bd), "r"(idesc), "r"(acc) : "memory");
             }
-            #pragma unroll
-            for (int j = 0; j < 4; j++) {
-                const int n = wn + 8 * j + gq;
-                bfr[j][0] = *(const unsigned*)&Bs[n][kk + 2 * tq];
-                bfr[j][1] = *(const unsigned*)&Bs[n][kk + 2 * tq + 8];
-            }
-            #pragma unroll
-            for (int i = 0; i < 2; i++)
-                #pragma unroll
-                for (int j = 0; j < 4; j++) mma_bf16_16816(acc[i][j], af[i], bfr[j]);
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                         :: "r"(bar) : "memory");
         }
-        __syncthreads();
+        issued = true;
+        // a wait that gives up waits once more (bounded) for the MMAs in
+        // flight before the CTA stops and frees its tensor memory
+        if (!mbar_wait(bar, phase) && !mbar_wait(bar, phase) && lane == 0) atomicOr(&s_fail, 1);
+        phase ^= 1u;
+        __syncthreads();                               // the slabs are free again
     }
-    // epilogue
-    #pragma unroll
-    for (int i = 0; i < 2; i++)
-        #pragma unroll
-        for (int j = 0; j < 4; j++)
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (s_fail) {
+        if (tid == 0 && g.err) atomicOr(g.err, KERR_TIMEOUT);
+    } else if (issued) {
+        // epilogue: warp w owns accumulator lanes (rows) 32w .. 32w + 31
+        const int r = m0 + 32 * warp + lane;
+        for (int c0 = 0; c0 < GM_BN; c0 += 32) {
+            unsigned v[32];
+            const unsigned taddr = tmem + ((unsigned)(32 * warp) << 16) + (unsigned)c0;
+            asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+                         "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+                         "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+                         : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+                           "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
+                           "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]),
+                           "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]),
+                           "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+                         : "r"(taddr));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (r >= g.M) continue;
             #pragma unroll
-            for (int q = 0; q < 4; q++) {
-                const int r = m0 + wm + 16 * i + gq + (q >> 1) * 8;
-                const int c = n0 + wn + 8 * j + 2 * tq + (q & 1);
-                if (r >= g.M || c >= g.N) continue;
-                float x = g.alpha * acc[i][j][q];
+            for (int q = 0; q < 32; q++) {
+                const int c = n0 + c0 + q;
+                if (c >= g.N) break;
+                float x = g.alpha * __uint_as_float(v[q]);
                 const size_t o = (size_t)r * g.ldc + c;
                 if (g.accumulate && g.Cf) x += g.Cf[o];
                 if (g.bias) x += g.bias[c];
@@ -287,12 +356,19 @@ k_gemm_bf16(GemmArgs g)
                 if (g.Cf) g.Cf[o] = x;
                 if (g.Cb) g.Cb[o] = __float2bfloat16(x);
             }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(GM_BN) : "memory");
 }
 
-static void gemm(const GemmArgs& g, cudaStream_t s)
+static void gemm(GemmArgs g, int* err, cudaStream_t s)
 {
+    g.err = err;
     dim3 grid((g.N + GM_BN - 1) / GM_BN, (g.M + GM_BM - 1) / GM_BM);
-    if (g.M > 0 && g.N > 0) k_gemm_bf16<<<grid, 128, 0, s>>>(g);
+    if (g.M > 0 && g.N > 0) k_gemm_umma<<<grid, GM_NT, 0, s>>>(g);
 }
 
 __global__ void k_f32_to_bf16(const float* in, __nv_bfloat16* out, size_t n)
@@ -447,6 +523,7 @@ struct cuacd_scorer {
     int* idx;
     __nv_bfloat16 *Xb, *H1, *H2, *dYb, *dH2b, *dH1b;
     float *Tb, *Y, *dYf, *dH2f, *dH1f, *loss;
+    int* gerr;                   // error word of the tensor-core GEMMs (KERR_TIMEOUT)
     // pruned-evaluation buffers
     float* mv; int* mt; float4* mp; PartStats* st; float* feat;
     size_t mv_cap, mt_cap, mp_cap;
@@ -497,13 +574,13 @@ static void sc_forward(cuacd_scorer* s, int b, cudaStream_t st)
 {
     GemmArgs g = gargs(s->Xb, SC_K, 1, s->pb + OFF_W1, SC_H, 1, b, SC_H, SC_K);
     g.bias = s->p32 + OFF_B1; g.relu = 1; g.Cb = s->H1; g.ldc = SC_H;
-    gemm(g, st);
+    gemm(g, s->gerr, st);
     g = gargs(s->H1, SC_H, 1, s->pb + OFF_W2, SC_H, 1, b, SC_H, SC_H);
     g.bias = s->p32 + OFF_B2; g.relu = 1; g.Cb = s->H2; g.ldc = SC_H;
-    gemm(g, st);
+    gemm(g, s->gerr, st);
     g = gargs(s->H2, SC_H, 1, s->pb + OFF_W3, 1, 0, b, 1, SC_H);
     g.bias = s->p32 + OFF_B3; g.Cf = s->Y; g.ldc = 1;
-    gemm(g, st);
+    gemm(g, s->gerr, st);
 }
 
 // Loss and gradients of the gathered batch into s->g32.
@@ -513,25 +590,25 @@ static void sc_backward(cuacd_scorer* s, int b, cudaStream_t st)
     // W3, b3
     GemmArgs g = gargs(s->H2, 1, SC_H, s->dYb, 1, 0, SC_H, 1, b);
     g.Cf = s->g32 + OFF_W3; g.ldc = 1;
-    gemm(g, st);
+    gemm(g, s->gerr, st);
     k_colsum<<<1, 32, 0, st>>>(s->dYf, b, 1, s->g32 + OFF_B3);
     // dH2 = dY W3^T (H2 > 0)
     g = gargs(s->dYb, 1, 0, s->pb + OFF_W3, 0, 1, b, SC_H, 1);
     g.mask = s->H2; g.ldm = SC_H; g.Cf = s->dH2f; g.Cb = s->dH2b; g.ldc = SC_H;
-    gemm(g, st);
+    gemm(g, s->gerr, st);
     // W2, b2
     g = gargs(s->H1, 1, SC_H, s->dH2b, SC_H, 1, SC_H, SC_H, b);
     g.Cf = s->g32 + OFF_W2; g.ldc = SC_H;
-    gemm(g, st);
+    gemm(g, s->gerr, st);
     k_colsum<<<(SC_H + 127) / 128, 128, 0, st>>>(s->dH2f, b, SC_H, s->g32 + OFF_B2);
     // dH1 = dH2 W2^T (H1 > 0)
     g = gargs(s->dH2b, SC_H, 1, s->pb + OFF_W2, 1, SC_H, b, SC_H, SC_H);
     g.mask = s->H1; g.ldm = SC_H; g.Cf = s->dH1f; g.Cb = s->dH1b; g.ldc = SC_H;
-    gemm(g, st);
+    gemm(g, s->gerr, st);
     // W1, b1
     g = gargs(s->Xb, 1, SC_K, s->dH1b, SC_H, 1, SC_K, SC_H, b);
     g.Cf = s->g32 + OFF_W1; g.ldc = SC_H;
-    gemm(g, st);
+    gemm(g, s->gerr, st);
     k_colsum<<<(SC_H + 127) / 128, 128, 0, st>>>(s->dH1f, b, SC_H, s->g32 + OFF_B1);
 }
 
@@ -582,6 +659,8 @@ extern "C" int cuacd_scorer_create(gpu_ctx_t ctx, unsigned seed, cuacd_scorer_t*
     if (!e) e = cudaMalloc(&s->m, sizeof(float) * N_PARAMS);
     if (!e) e = cudaMalloc(&s->v, sizeof(float) * N_PARAMS);
     if (!e) e = cudaMalloc(&s->loss, sizeof(float));
+    if (!e) e = cudaMalloc(&s->gerr, sizeof(int));
+    if (!e) e = cudaMemset(s->gerr, 0, sizeof(int));
     if (!e) e = cudaMalloc(&s->nrm, sizeof(float) * 2 * SC_K);
     if (e) { cuacd_scorer_free(s); return ctx_fail(ctx, (int)e, "scorer allocation failed: %s", cudaGetErrorString(e)); }
     // He-uniform weights, zero biases
@@ -624,7 +703,7 @@ extern "C" void cuacd_scorer_free(cuacd_scorer_t s)
     if (!s) return;
     cudaSetDevice(s->device);
     cudaFree(s->p32); cudaFree(s->pb); cudaFree(s->g32); cudaFree(s->m); cudaFree(s->v); cudaFree(s->loss);
-    cudaFree(s->nrm);
+    cudaFree(s->gerr); cudaFree(s->nrm);
     cudaFree(s->X); cudaFree(s->T); cudaFree(s->idx); cudaFree(s->Xb); cudaFree(s->H1); cudaFree(s->H2);
     cudaFree(s->dYb); cudaFree(s->dH2b); cudaFree(s->dH1b); cudaFree(s->Tb); cudaFree(s->Y); cudaFree(s->dYf);
     cudaFree(s->dH2f); cudaFree(s->dH1f); cudaFree(s->mv); cudaFree(s->mt); cudaFree(s->mp); cudaFree(s->st);
@@ -699,6 +778,18 @@ static int sc_features_device(gpu_ctx* ctx, cuacd_scorer* s, const float* verts,
     return 0;
 }
 
+// After a synchronisation: a tensor-core wait of the GEMMs that gave up
+// (error word set) fails the call, and the word is cleared.
+static int sc_check_gemm(gpu_ctx* ctx, cuacd_scorer* s, cudaStream_t st)
+{
+    int e = 0;
+    SCK(cudaMemcpyAsync(&e, s->gerr, sizeof(int), cudaMemcpyDeviceToHost, st));
+    SCK(cudaStreamSynchronize(st));
+    if (!e) return 0;
+    SCK(cudaMemsetAsync(s->gerr, 0, sizeof(int), st));
+    return ctx_fail(ctx, e, "scorer GEMM: a tensor-core wait gave up (0x%x)", e);
+}
+
 int scorer_predict_parts(gpu_ctx* ctx, cuacd_scorer* s, const ScorerPart* parts, int n_parts,
                          const float4* d_planes, int n_rows, float* pred, cudaStream_t st)
 {
@@ -717,6 +808,7 @@ int scorer_predict_parts(gpu_ctx* ctx, cuacd_scorer* s, const ScorerPart* parts,
     SCK(cudaGetLastError());
     SCK(cudaMemcpyAsync(pred, s->Y, sizeof(float) * (size_t)n_rows, cudaMemcpyDeviceToHost, st));
     SCK(cudaStreamSynchronize(st));
+    if (sc_check_gemm(ctx, s, st)) return -1;
     for (int i = 0; i < n_rows; i++) pred[i] /= SC_TSCALE;
     return 0;
 }
@@ -758,7 +850,8 @@ extern "C" int cuacd_scorer_grad(gpu_ctx_t ctx, cuacd_scorer_t s, const float* X
     SCK(cudaGetLastError());
     if (loss) SCK(cudaMemcpyAsync(loss, s->loss, sizeof(float), cudaMemcpyDeviceToHost, st));
     if (grads) SCK(cudaMemcpyAsync(grads, s->g32, sizeof(float) * N_PARAMS, cudaMemcpyDeviceToHost, st));
-    return sync_and_check(ctx, "scorer_grad");
+    int rc = sync_and_check(ctx, "scorer_grad");
+    return rc ? rc : sc_check_gemm(ctx, s, st);
 }
 
 extern "C" int cuacd_scorer_train(gpu_ctx_t ctx, cuacd_scorer_t s, const float* X, const float* T, int n, int epochs,
@@ -798,6 +891,7 @@ extern "C" int cuacd_scorer_train(gpu_ctx_t ctx, cuacd_scorer_t s, const float* 
     }
     int rc = sync_and_check(ctx, "scorer_train");
     cudaFree(d_perm); cudaFree(d_losses);
+    if (!rc) rc = sc_check_gemm(ctx, s, st);
     if (rc) return rc;
     for (float l : losses) { loss_sum += l; loss_cnt++; }
     if (final_loss) *final_loss = loss_cnt ? (float)(loss_sum / loss_cnt) / (SC_TSCALE * SC_TSCALE) : 0.f;
@@ -819,6 +913,7 @@ extern "C" int cuacd_scorer_predict(gpu_ctx_t ctx, cuacd_scorer_t s, const float
     std::vector<float> y(n);
     SCK(cudaMemcpyAsync(y.data(), s->Y, sizeof(float) * (size_t)n, cudaMemcpyDeviceToHost, st));
     int rc = sync_and_check(ctx, "scorer_predict");
+    if (!rc) rc = sc_check_gemm(ctx, s, st);
     if (rc) return rc;
     for (int i = 0; i < n; i++) out[i] = y[i] / SC_TSCALE;
     return 0;
