@@ -10,9 +10,9 @@
 
 __global__ void __launch_bounds__(HULL_NT)
 k_hull_setup(const HullJob* __restrict__ jobs, int n_jobs, Arena* scratch, HullState* states, int* ctl,
-             int seed_min_n)
+             int seed_min_n, int retry_round)
 {
-    hull_setup_body(jobs, n_jobs, scratch, states, ctl, seed_min_n);
+    hull_setup_body(jobs, n_jobs, scratch, states, ctl, seed_min_n, retry_round);
 }
 
 // Wrap-grid shares (one CTA): prefix of the active hulls' weights, a hull's
@@ -34,9 +34,9 @@ k_hull_wrap(HullState* states, int n_jobs, int* ctl, const long long* total, int
 
 __global__ void __launch_bounds__(HULL_NT)
 k_hull_output(const HullJob* __restrict__ jobs, HullState* states, int n_jobs, Arena* out, const int* ctl,
-              HullRes* res, unsigned long long* stats)
+              HullRes* res, unsigned long long* stats, int retry_round)
 {
-    hull_output_body(jobs, states, n_jobs, out, ctl, res, stats);
+    hull_output_body(jobs, states, n_jobs, out, ctl, res, stats, retry_round);
 }
 
 size_t hull_wrap_buf_bytes(int n_wrap_ctas)
@@ -126,13 +126,20 @@ void launch_hull_jobs(const HullJob* d_jobs, int n_jobs, HullState* d_states, Hu
 {
     if (n_jobs <= 0) return;
     const int seed_min_n = hull_tune(hull_size_class(max_pts)).seed_min_n;
-    cudaMemsetAsync(d_ctl, 0, 4 * sizeof(int), s);
-    k_hull_setup<<<n_jobs, HULL_NT, 0, s>>>(d_jobs, n_jobs, scratch, d_states, d_ctl, seed_min_n);
-    k_hull_assign<<<1, 1024, 0, s>>>(d_states, n_jobs, n_wrap_ctas, (long long*)(d_ctl + 2));
     hull_wrap_per_sm();                                   // dynamic shared memory opt-in
-    k_hull_wrap<<<n_wrap_ctas, HULL_NT, HULL_WRAP_DSMEM, s>>>(d_states, n_jobs, d_ctl, (const long long*)(d_ctl + 2),
-                                                             d_wbuf);
-    k_hull_output<<<n_jobs, HULL_NT, 0, s>>>(d_jobs, d_states, n_jobs, out, d_ctl, d_res, d_stats);
+    // round 0 builds every cloud with first-attempt tables; round 1 (only
+    // launched when a cloud of the batch can outgrow them) rebuilds the
+    // clouds whose tables overflowed at full capacity -- its kernels return
+    // at once when there are none
+    const int rounds = max_pts > HULL_FIRST_CAP ? 2 : 1;
+    for (int r = 0; r < rounds; r++) {
+        cudaMemsetAsync(d_ctl, 0, 4 * sizeof(int), s);
+        k_hull_setup<<<n_jobs, HULL_NT, 0, s>>>(d_jobs, n_jobs, scratch, d_states, d_ctl, seed_min_n, r);
+        k_hull_assign<<<1, 1024, 0, s>>>(d_states, n_jobs, n_wrap_ctas, (long long*)(d_ctl + 2));
+        k_hull_wrap<<<n_wrap_ctas, HULL_NT, HULL_WRAP_DSMEM, s>>>(d_states, n_jobs, d_ctl,
+                                                                 (const long long*)(d_ctl + 2), d_wbuf);
+        k_hull_output<<<n_jobs, HULL_NT, 0, s>>>(d_jobs, d_states, n_jobs, out, d_ctl, d_res, d_stats, r);
+    }
 }
 
 // Jobs for clouds packed back to back (offsets), outputs in fixed slots.

@@ -56,17 +56,32 @@ struct HullCaps {
 
 __host__ __device__ inline int hull_pow2(int x) { int p = 1; while (p < x) p <<= 1; return p; }
 
-__host__ __device__ inline HullCaps hull_caps(int n)
+// Hull vertex capacity of the first attempt at an n-point cloud: every
+// point up to HULL_FIRST_CAP points, beyond that a quarter of them (at least
+// HULL_FIRST_CAP).  Fragments of meshes have far fewer hull vertices than
+// points (a 20,000-point sphere fragment about 2,800), so their edge set,
+// face set and frontier queue -- cleared at set-up, probed while wrapping --
+// start four times smaller; a cloud whose hull outgrows them (a convex
+// cloud, such as the vertices of a fine sphere, has every point on its hull)
+// is built again with h = n in the same launch sequence.
+#define HULL_FIRST_CAP 4096
+__host__ __device__ inline int hull_first_cap(int n)
+{
+    if (n <= HULL_FIRST_CAP) return n;
+    return n / 4 > HULL_FIRST_CAP ? n / 4 : HULL_FIRST_CAP;
+}
+
+// Table capacities of an n-point cloud built with room for h hull vertices.
+// Clouds are limited to 2^22 points, which keeps every table within int range.
+__host__ __device__ inline HullCaps hull_caps(int n, int h)
 {
     HullCaps c;
     c.n = n;
     c.m_leaves = (n + HULL_LEAF - 1) / HULL_LEAF;
     if (c.m_leaves < 1) c.m_leaves = 1;
     c.P = hull_pow2(c.m_leaves);
-    // every point may be a hull vertex (a convex cloud, such as the vertices
-    // of a fine sphere, has all of them on its hull); clouds are limited to
-    // 2^22 points, which keeps every table below within int range
-    int h = n < 4 ? 4 : n;
+    if (h > n) h = n;
+    if (h < 4) h = 4;
     if (h > (1 << 22)) h = 1 << 22;
     c.hcap = h;
     c.ccap = 6 * h + 64;
@@ -640,6 +655,8 @@ struct HullState {             // per hull, global memory
     unsigned long long* eset; unsigned long long* fset; unsigned long long* Q;
     int2* faces; int* corners; int* Sbuf; int* posn; int* ocnt;
     int n, P, m_leaves, eh, fh, fcap, ccap, qcap;
+    int hcap;                  // hull vertex capacity its tables were sized for
+    int retry;                 // 1: its tables overflowed on the first attempt; build again at h = n
     int q_head, q_tail, q_pending, n_faces, n_corners, err;
     int active;                // 1 while its frontier queue has work
     int lock;                  // guards Sbuf/posn/ocnt while wrapping (large faces)
@@ -653,9 +670,10 @@ struct HullState {             // per hull, global memory
                                    // and 2^48 per face on the hull's own lists)
 };
 
-__host__ __device__ inline size_t hull_scratch_bytes(int n)
+// Scratch of one attempt at an n-point cloud with room for h hull vertices.
+__host__ __device__ inline size_t hull_attempt_bytes(int n, int h)
 {
-    HullCaps c = hull_caps(n);
+    HullCaps c = hull_caps(n, h);
     size_t nn = (size_t)(n > 0 ? n : 1);
     size_t b = 0;
     b += hull_align(sizeof(float4) * nn);                             // pts
@@ -672,12 +690,20 @@ __host__ __device__ inline size_t hull_scratch_bytes(int n)
     return b;
 }
 
+// Scratch a cloud may use over both attempts (the first one's stays
+// allocated while the second runs): what callers reserve per cloud.
+__host__ __device__ inline size_t hull_scratch_bytes(int n)
+{
+    const int h1 = hull_first_cap(n);
+    return hull_align(hull_attempt_bytes(n, h1)) + (h1 < n ? hull_align(hull_attempt_bytes(n, n)) : 0);
+}
+
 // Per-warp global lists of the wrapping grid, sized for clouds of up to
 // n_max points: coplanar set and polygon (n_max + 2 each), node stack (2P)
 // and leaf list (P).
 __host__ __device__ inline size_t hull_warp_bytes(int n_max)
 {
-    HullCaps c = hull_caps(n_max > 4 ? n_max : 4);
+    HullCaps c = hull_caps(n_max > 4 ? n_max : 4, n_max);
     return hull_align(sizeof(int) * (2 * (size_t)(n_max + 2) + 3 * (size_t)c.P));
 }
 
@@ -727,11 +753,11 @@ static __device__ __forceinline__ void cta_fill_ones64(unsigned long long* tab, 
 }
 
 static __device__ void hull_setup_cta(const float* __restrict__ pts, int n, char* scratch, HullState* S,
-                                      HullSetupShared& sh, int seed_min_n = 1 << 30)
+                                      HullSetupShared& sh, int seed_min_n = 1 << 30, int hcap = 1 << 30)
 {
     const int tid = threadIdx.x;
     const long long t_begin = clock64();
-    HullCaps C = hull_caps(n);
+    HullCaps C = hull_caps(n, hcap);
     char* p = scratch;
     float4* P4 = (float4*)p;            p += hull_align(sizeof(float4) * (size_t)n);
     float4* nlo = (float4*)p;           p += hull_align(sizeof(float4) * 2 * (size_t)(2 * C.P));
@@ -750,7 +776,7 @@ static __device__ void hull_setup_cta(const float* __restrict__ pts, int n, char
         S->P4 = P4; S->nlo = nlo; S->nhi = nhi; S->obb = obb; S->eset = eset; S->fset = fset; S->Q = Q;
         S->faces = faces; S->corners = corners; S->Sbuf = Sbuf; S->posn = posn; S->ocnt = ocnt;
         S->n = n; S->P = C.P; S->m_leaves = C.m_leaves; S->eh = C.eh; S->fh = C.fh; S->fcap = C.fcap;
-        S->ccap = C.ccap; S->qcap = qcap;
+        S->ccap = C.ccap; S->qcap = qcap; S->hcap = C.hcap;
         S->q_head = 0; S->q_tail = 0; S->q_pending = 0; S->n_faces = 0; S->n_corners = 0; S->err = 0;
         S->active = 0; S->lock = 0;
         for (int k = 0; k < 8; k++) S->stats[k] = 0;

@@ -5,8 +5,10 @@
 #pragma once
 #include "hull.cuh"
 
+// retry_round 0: every cloud, first-attempt capacities (hull_first_cap);
+// retry_round 1: only the clouds whose tables overflowed, at h = n.
 static __device__ void hull_setup_body(const HullJob* __restrict__ jobs, int n_jobs, Arena* scratch, HullState* states, int* ctl,
-                                       int seed_min_n = 1 << 30)
+                                       int seed_min_n = 1 << 30, int retry_round = 0)
 {
     __shared__ HullSetupShared sh;
     __shared__ char* s_scr;
@@ -15,19 +17,25 @@ static __device__ void hull_setup_body(const HullJob* __restrict__ jobs, int n_j
     if (j >= n_jobs) return;
     const HullJob J = jobs[j];
     HullState* S = &states[j];
+    if (retry_round && !S->retry) {              // built on the first attempt: nothing to do
+        if (threadIdx.x == 0) S->active = 0;
+        return;
+    }
+    const int hcap = retry_round ? J.n : hull_first_cap(J.n);
     double mv = 0.0;
     if (J.tris && J.nt > 0 && J.n > 0) mv = block_mesh_signed_volume(J.pts, J.n, J.tris, J.nt, sh.dsh);
     if (threadIdx.x == 0) {
-        S->n = J.n; S->n_faces = 0; S->err = 0; S->active = 0; S->q_pending = 0;
+        S->n = J.n; S->n_faces = 0; S->err = 0; S->active = 0; S->q_pending = 0; S->hcap = hcap;
+        if (!retry_round) S->retry = 0;
         for (int k = 0; k < 8; k++) { S->stats[k] = 0; S->fail[k] = 0; }
         s_err = 0; s_scr = nullptr;
         if (J.n >= 4) {
-            s_scr = (char*)arena_alloc(scratch, hull_scratch_bytes(J.n), &s_err);
+            s_scr = (char*)arena_alloc(scratch, hull_attempt_bytes(J.n, hcap), &s_err);
             if (!s_scr) S->err = s_err | KERR_BT_POOL_EXHAUST;
         }
     }
     __syncthreads();
-    if (s_scr) hull_setup_cta(J.pts, J.n, s_scr, S, sh, seed_min_n);
+    if (s_scr) hull_setup_cta(J.pts, J.n, s_scr, S, sh, seed_min_n, hcap);
     if (threadIdx.x == 0) {
         S->mesh_vol = fabs(mv);
         if (s_scr && S->active) atomicAdd(&ctl[0], 1);
@@ -110,12 +118,12 @@ static __device__ void hull_wrap_body(HullState* states, int n_jobs, int* ctl, c
     hull_wrap_grid(states, n_jobs, s_h0[threadIdx.x >> 5], ctl, wbuf, sh, wsm_dyn);
 }
 static __device__ void hull_output_body(const HullJob* __restrict__ jobs, HullState* states, int n_jobs, Arena* out, const int* ctl,
-              HullRes* res, unsigned long long* stats)
+              HullRes* res, unsigned long long* stats, int retry_round = 0)
 {
     __shared__ HullOutShared sh;
     __shared__ float* s_ov;
     __shared__ int* s_ot;
-    __shared__ int s_mhv, s_mht, s_aerr, s_nv, s_nt, s_oerr;
+    __shared__ int s_mhv, s_mht, s_aerr, s_nv, s_nt, s_oerr, s_skip;
     __shared__ float s_vol;
     const int j = blockIdx.x;
     if (j >= n_jobs) return;
@@ -123,6 +131,19 @@ static __device__ void hull_output_body(const HullJob* __restrict__ jobs, HullSt
     HullState* S = &states[j];
     if (threadIdx.x == 0) {
         if (J.n >= 4 && S->active) atomicOr(&S->err, ctl[1] ? ctl[1] : KERR_TIMEOUT);   // not finished
+        // a first attempt whose tables overflowed (and not for want of
+        // arena memory) is built again at full capacity: no output yet
+        const int e = S->err;
+        s_skip = retry_round ? !S->retry : 0;
+        if (!retry_round && J.n >= 4 && S->hcap < J.n && (e & KERR_BT_POOL_EXHAUST) && !(e & KERR_HEAP_OOM)) {
+            S->retry = 1;
+            s_skip = 1;
+        }
+        if (retry_round) S->retry = 0;
+    }
+    __syncthreads();
+    if (s_skip) return;
+    if (threadIdx.x == 0) {
         s_aerr = 0;
         s_ov = J.out_v; s_ot = J.out_t; s_mhv = J.max_hv; s_mht = J.max_ht;
         if (!J.out_v && J.n >= 4 && S->err == 0) {

@@ -226,11 +226,13 @@ static __device__ __forceinline__ unsigned long long umma_desc(unsigned addr, un
            ((unsigned long long)((sbo >> 4) & 0x3FFF) << 32) | (1ull << 46);
 }
 
-// Instruction descriptor of kind::f16: FP32 accumulator, BF16 A and B, both
-// K-major, N >> 3 at bits 17-22, M >> 4 at bits 24-28.
-static __host__ __device__ constexpr unsigned umma_idesc_bf16(int m, int n)
+// Instruction descriptor of kind::f16: FP32 accumulator, BF16 A and B, A /
+// B MN-major when a_mn / b_mn (bits 15 / 16, else K-major), N >> 3 at bits
+// 17-22, M >> 4 at bits 24-28.
+static __host__ __device__ constexpr unsigned umma_idesc_bf16(int m, int n, int a_mn, int b_mn)
 {
-    return (1u << 4) | (1u << 7) | (1u << 10) | ((unsigned)(n >> 3) << 17) | ((unsigned)(m >> 4) << 24);
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((unsigned)a_mn << 15) | ((unsigned)b_mn << 16) |
+           ((unsigned)(n >> 3) << 17) | ((unsigned)(m >> 4) << 24);
 }
 
 // Bounded wait for the mbarrier phase `parity`; false when it gave up.
@@ -245,11 +247,69 @@ static __device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity)
     return false;
 }
 
-// Element (r, k) of a 128-row, 64-wide K-major slab: core matrix
+// Element (r, k) of a 128-row, 64-wide slab.  K-major: core matrix
 // (k / 8, r / 8) of 128 bytes, row r % 8 at 16 bytes, column k % 8.
+// MN-major: the same core matrices, each holding 8 K rows of 8 consecutive
+// r.  Either way the leading byte offset (next 8 K) is 16 core matrices and
+// the stride byte offset (next 8 rows) one.
 static __device__ __forceinline__ int slab_index(int r, int k)
 {
     return (((k >> 3) * (GM_BM / 8) + (r >> 3)) << 6) + ((r & 7) << 3) + (k & 7);
+}
+static __device__ __forceinline__ int slab_index_mn(int r, int k)
+{
+    return (((k >> 3) * (GM_BM / 8) + (r >> 3)) << 6) + ((k & 7) << 3) + (r & 7);
+}
+
+// How an operand X(r, k) = X[r*rs + k*ks] is staged: 2 = MN-major with
+// 16-byte loads along r, 1 = K-major with 16-byte loads along k, 0 =
+// K-major element by element.
+static __host__ __device__ __forceinline__ int stage_mode(long long rs, long long ks, int K)
+{
+    if (ks == 1 && rs % 8 == 0) return 1;
+    if (rs == 1 && (ks % 8 == 0 || K == 1)) return 2;
+    return 0;
+}
+
+// Stage rows [r0, r0 + 128) x K columns [k0, k0 + 64) of X (R x K, zero
+// outside) into a slab (all GM_NT threads).
+static __device__ __forceinline__ void stage_slab(__nv_bfloat16* slab, const __nv_bfloat16* __restrict__ X, long long rs,
+                                                  long long ks, int R, int K, int r0, int k0, int mode, int tid)
+{
+    const __nv_bfloat16 zero = __float2bfloat16(0.f);
+    if (mode == 1) {                                       // 8 consecutive k of one row per load
+        for (int e = tid; e < GM_BM * (GM_BK / 8); e += GM_NT) {
+            const int r = e / (GM_BK / 8), c = 8 * (e % (GM_BK / 8));
+            const int gr = r0 + r, gk = k0 + c;
+            uint4 v;
+            if (gr < R && gk + 7 < K) v = *reinterpret_cast<const uint4*>(X + gr * rs + gk);
+            else {
+                __nv_bfloat16 t[8];
+                for (int q = 0; q < 8; q++) t[q] = (gr < R && gk + q < K) ? X[gr * rs + (gk + q)] : zero;
+                v = *reinterpret_cast<const uint4*>(t);
+            }
+            *reinterpret_cast<uint4*>(slab + slab_index(r, c)) = v;
+        }
+    } else if (mode == 2) {                                // 8 consecutive r of one k per load
+        for (int e = tid; e < (GM_BM / 8) * GM_BK; e += GM_NT) {
+            const int r = 8 * (e % (GM_BM / 8)), k = e / (GM_BM / 8);
+            const int gr = r0 + r, gk = k0 + k;
+            uint4 v;
+            if (gk < K && gr + 7 < R) v = *reinterpret_cast<const uint4*>(X + gr + gk * ks);
+            else {
+                __nv_bfloat16 t[8];
+                for (int q = 0; q < 8; q++) t[q] = (gk < K && gr + q < R) ? X[(gr + q) + gk * ks] : zero;
+                v = *reinterpret_cast<const uint4*>(t);
+            }
+            *reinterpret_cast<uint4*>(slab + slab_index_mn(r, k)) = v;
+        }
+    } else {
+        for (int e = tid; e < GM_BM * GM_BK; e += GM_NT) {
+            const int r = e / GM_BK, c = e % GM_BK;
+            const int gr = r0 + r, gk = k0 + c;
+            slab[slab_index(r, c)] = (gr < R && gk < K) ? X[gr * rs + gk * ks] : zero;
+        }
+    }
 }
 
 __global__ void __launch_bounds__(GM_NT)
@@ -277,26 +337,17 @@ k_gemm_umma(GemmArgs g)
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const unsigned tmem = s_tmem;
-    const __nv_bfloat16 zero = __float2bfloat16(0.f);
-    constexpr unsigned idesc = umma_idesc_bf16(GM_BM, GM_BN);
+    // A(i, k) = A[i*ar + k*ac]; B as an N x K operand: B(j, k) = B[j*bc + k*br]
+    const int amode = stage_mode(g.ar, g.ac, g.K), bmode = stage_mode(g.bc, g.br, g.K);
+    const unsigned idesc = umma_idesc_bf16(GM_BM, GM_BN, amode == 2, bmode == 2);
     const unsigned a0 = smem_addr(As), b0 = smem_addr(Bs);
     unsigned phase = 0;
     bool issued = false;
     for (int k0 = 0; k0 < g.K && !s_fail; k0 += GM_BK) {
-        // stage the slabs (zero outside the matrices); consecutive threads
-        // walk the operand's unit stride
-        for (int e = tid; e < GM_BM * GM_BK; e += GM_NT) {
-            int r, c;
-            if (g.ac == 1) { r = e / GM_BK; c = e % GM_BK; } else { c = e / GM_BM; r = e % GM_BM; }
-            const int gi = m0 + r, gk = k0 + c;
-            As[slab_index(r, c)] = (gi < g.M && gk < g.K) ? g.A[gi * g.ar + gk * g.ac] : zero;
-        }
-        for (int e = tid; e < GM_BN * GM_BK; e += GM_NT) {
-            int n, c;
-            if (g.br == 1) { n = e / GM_BK; c = e % GM_BK; } else { c = e / GM_BN; n = e % GM_BN; }
-            const int gj = n0 + n, gk = k0 + c;
-            Bs[slab_index(n, c)] = (gj < g.N && gk < g.K) ? g.B[gk * g.br + gj * g.bc] : zero;
-        }
+        // stage the slabs (zero outside the matrices) with 16-byte loads
+        // along whichever of the operand's dimensions is contiguous
+        stage_slab(As, g.A, g.ar, g.ac, g.M, g.K, m0, k0, amode, tid);
+        stage_slab(Bs, g.B, g.bc, g.br, g.N, g.K, n0, k0, bmode, tid);
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // generic stores -> tensor-core reads
         __syncthreads();
         if (tid == 0) {

@@ -89,17 +89,23 @@ int main(int argc, char** argv)
     std::vector<HullState> states(n_jobs);
     memset(states.data(), 0, sizeof(HullState) * n_jobs);
     std::vector<HullRes> res(n_jobs);
-    int ctl[4] = {0, 0, 0, 0};
-    long long total = 0;
-    for (int j = 0; j < n_jobs; j++)
-        run_cta("setup", HULL_NT, j, n_jobs, [&]() { hull_setup_body(jobs.data(), n_jobs, &scratch, states.data(), ctl); });
-    run_cta("assign", 1024, 0, 1, [&]() { hull_assign_body(states.data(), n_jobs, 1, &total); });
     std::vector<int> wbuf((HULL_NT / 32) * 2 * HULL_SGCAP);
     std::vector<int> wsm(HULL_WRAP_DSMEM / sizeof(int));
-    run_cta("wrap", HULL_NT, 0, 1, [&]() { hull_wrap_body(states.data(), n_jobs, ctl, &total, wbuf.data(), wsm.data()); });
-    for (int j = 0; j < n_jobs; j++)
-        run_cta("output", HULL_NT, j, n_jobs,
-                [&]() { hull_output_body(jobs.data(), states.data(), n_jobs, &out, ctl, res.data(), nullptr); });
+    // the launcher's two rounds: first-attempt tables, then full-size tables
+    // for the clouds whose tables overflowed
+    for (int round = 0; round < 2; round++) {
+        int ctl[4] = {0, 0, 0, 0};
+        long long total = 0;
+        for (int j = 0; j < n_jobs; j++)
+            run_cta("setup", HULL_NT, j, n_jobs,
+                    [&]() { hull_setup_body(jobs.data(), n_jobs, &scratch, states.data(), ctl, 1 << 30, round); });
+        run_cta("assign", 1024, 0, 1, [&]() { hull_assign_body(states.data(), n_jobs, 1, &total); });
+        run_cta("wrap", HULL_NT, 0, 1,
+                [&]() { hull_wrap_body(states.data(), n_jobs, ctl, &total, wbuf.data(), wsm.data()); });
+        for (int j = 0; j < n_jobs; j++)
+            run_cta("output", HULL_NT, j, n_jobs,
+                    [&]() { hull_output_body(jobs.data(), states.data(), n_jobs, &out, ctl, res.data(), nullptr, round); });
+    }
     for (int j = 0; j < n_jobs; j++) {
         const HullRes& r = res[j];
         printf("hull %d: err %d nv %d nt %d vol %.9g\n", j, r.err, r.hnv, r.hnt, (double)r.hull_vol);
