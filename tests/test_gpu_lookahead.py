@@ -143,3 +143,43 @@ def test_merge_hulls_pass(ctx, oracle):
             assert len(hv) > 0 and abs(oracle.mesh_volume(hv, ht) - hvol) <= 1e-3 * hvol
             assert max(_rv_costs([(pv, pt, hv, ht)])) < 0.05
     assert n_new == len(plain) - len(merged)
+
+
+def test_merge_hulls_pairs_match_oracle(ctx, oracle):
+    """Which pairs the merge-hulls pass merges, and the parts it makes,
+    against the pass restated on the CPU (oracle/merge_ref.py) from the same
+    search's parts before merging: same matched pairs in the same order, and
+    each merged part is both meshes concatenated with the exact hull of both
+    hulls' vertices.  A candidate whose cost lies within 1e-4 of tau or of
+    another candidate's would make the greedy order depend on the last bits
+    of FP32 sums; none may occur here."""
+    from oracle import merge_ref as MR
+    kw = dict(width=30, width2=5, depth=2, threshold=0.05, n_concave_edges=16)
+    n_merged = 0
+    for v, t in (W.candidate_mesh(64, 24), W.candidate_mesh(96, 32, 0.35, seed=5)):
+        plain = ctx.lookahead_decompose(v, t, **kw)
+        merged = ctx.lookahead_decompose(v, t, merge_hulls=True, **kw)
+        matches, costs = MR.merge_pass(plain, 0.05, oracle)
+        c = sorted(costs.values())
+        assert all(abs(x - 0.05) > 1e-4 for x in c)
+        assert all(b - a > 1e-4 or a >= 0.05 for a, b in zip(c, c[1:]))
+        partner = {p1: p2 for p1, p2 in matches}
+        dead = {p2 for _, p2 in matches}
+        expect = []
+        for i, p in enumerate(plain):
+            if i in dead:
+                continue
+            if i in partner:
+                a, b = p, plain[partner[i]]
+                pts = np.concatenate([a[2], b[2]]).astype(np.float32)
+                vidx, tris, _ = oracle.hull(pts)
+                expect.append((np.concatenate([a[0], b[0]]), np.concatenate([a[1], b[1] + len(a[0])]),
+                               pts[vidx], tris))
+            else:
+                expect.append(p)
+        assert len(merged) == len(expect), (len(merged), len(expect), matches)
+        for got, exp in zip(merged, expect):
+            for x, y in zip(got, exp):
+                np.testing.assert_array_equal(x, y)
+        n_merged += len(matches)
+    assert n_merged > 0
