@@ -150,9 +150,9 @@ def test_merge_hulls_pairs_match_oracle(ctx, oracle):
     against the pass restated on the CPU (oracle/merge_ref.py) from the same
     search's parts before merging: same matched pairs in the same order, and
     each merged part is both meshes concatenated with the exact hull of both
-    hulls' vertices.  A candidate whose cost lies within 1e-4 of tau or of
-    another candidate's would make the greedy order depend on the last bits
-    of FP32 sums; none may occur here."""
+    hulls' vertices.  A candidate whose cost lay within 1e-4 of tau would
+    make the decision depend on the last bits of FP32 sums; none may occur
+    here."""
     from oracle import merge_ref as MR
     kw = dict(width=30, width2=5, depth=2, threshold=0.05, n_concave_edges=16)
     n_merged = 0
@@ -160,9 +160,7 @@ def test_merge_hulls_pairs_match_oracle(ctx, oracle):
         plain = ctx.lookahead_decompose(v, t, **kw)
         merged = ctx.lookahead_decompose(v, t, merge_hulls=True, **kw)
         matches, costs = MR.merge_pass(plain, 0.05, oracle)
-        c = sorted(costs.values())
-        assert all(abs(x - 0.05) > 1e-4 for x in c)
-        assert all(b - a > 1e-4 or a >= 0.05 for a, b in zip(c, c[1:]))
+        assert all(abs(x - 0.05) > 1e-4 for x in costs.values())
         partner = {p1: p2 for p1, p2 in matches}
         dead = {p2 for _, p2 in matches}
         expect = []
