@@ -113,14 +113,15 @@ static __device__ void cut_job_plane(const CutJob& J, float min_edge_dist, float
 
 __global__ void __launch_bounds__(CUT_NT)
 k_cut_jobs(const CutJob* __restrict__ jobs, int j0, int j1, Arena* scratch, Arena* out, float min_edge_dist,
-           CutResult* res)
+           CutResult* res, const int* __restrict__ order = nullptr)
 {
     __shared__ CutShared sh;
     __shared__ float s_lo[3], s_hi[3];
     __shared__ float4 s_plane;
     __shared__ int s_flags;
     __shared__ float red[6][CUT_NT / 32];
-    const int j = j0 + blockIdx.x;
+    // order: the wave's jobs largest first, so the longest cuts start first
+    const int j = order ? order[j0 + blockIdx.x] : j0 + blockIdx.x;
     if (j >= j1) return;
     const CutJob J = jobs[j];
     cut_job_plane(J, min_edge_dist, red, s_lo, s_hi, &s_plane, &s_flags);
@@ -509,6 +510,7 @@ struct Lookahead {
     HDSurf* d_bnb_surf = nullptr; float* d_bnb_pts = nullptr; double* d_bnb_mvol = nullptr;
     unsigned char* d_skip = nullptr;
     int bnb_cap = 0;                                 // fragments the rough-hull buffers hold
+    int* d_order = nullptr;                          // cut jobs, largest first per wave (max_jobs)
     unsigned long long n_hulls = 0, n_pruned = 0;    // fragment hulls built, items pruned
 
     // The last level's fragments are only needed for their costs: its jobs
@@ -553,6 +555,11 @@ struct Lookahead {
         cuts.assign(n, CutResult());
         if (n == 0) return 0;
         CK(cudaMemcpyAsync(d_jobs, jobs.data(), sizeof(CutJob) * n, cudaMemcpyHostToDevice, s));
+        // waves by the scratch estimate; inside a wave the CTAs take the jobs
+        // largest first (longest-processing-time order: the block scheduler
+        // hands out blocks in index order, so the tail is the short cuts)
+        std::vector<int> order(n);
+        std::vector<std::pair<int, int>> waves;
         int j = 0;
         while (j < n) {
             size_t acc = 0; int j1 = j;
@@ -561,10 +568,18 @@ struct Lookahead {
                 if (j1 > j && acc + e > scr_cap) break;
                 acc += e; j1++;
             }
-            reset_scr();
-            k_cut_jobs<<<j1 - j, CUT_NT, 0, s>>>(d_jobs, j, j1, d_scr, d_cur, min_edge, d_cuts);
-            ctx->launches += 2;
+            for (int k = j; k < j1; k++) order[k] = k;
+            std::stable_sort(order.begin() + j, order.begin() + j1,
+                             [&](int a, int b) { return jobs[a].nt > jobs[b].nt; });
+            waves.push_back({j, j1});
             j = j1;
+        }
+        CK(cudaMemcpyAsync(d_order, order.data(), sizeof(int) * n, cudaMemcpyHostToDevice, s));
+        for (const auto& w : waves) {
+            reset_scr();
+            k_cut_jobs<<<w.second - w.first, CUT_NT, 0, s>>>(d_jobs, w.first, w.second, d_scr, d_cur, min_edge, d_cuts,
+                                                            d_order);
+            ctx->launches += 2;
         }
         CK(cudaGetLastError());
         CK(cudaMemcpyAsync(cuts.data(), d_cuts, sizeof(CutResult) * n, cudaMemcpyDeviceToHost, s));
@@ -1172,7 +1187,7 @@ static int search_group(gpu_ctx_t ctx, int n_mesh, const MeshIn* M, const Search
                  + al256(sizeof(HullJob) * hjob_cap) + al256(sizeof(HullState) * hjob_cap) + al256(64)
                  + al256(hull_wrap_buf_bytes(hull_wrap_ctas(1LL << 40, ctx->n_sm)))
                  + al256(sizeof(HDSurf) * bnb_cap) + al256(sizeof(float) * 3 * LA_ROUGH_PTS * bnb_cap)
-                 + al256(sizeof(double) * bnb_cap) + al256(max_jobs);
+                 + al256(sizeof(double) * bnb_cap) + al256(max_jobs) + al256(sizeof(int) * max_jobs);
     // Output arena: the fragments and hulls of every level whose items outlive
     // it.  A level-0 candidate set outputs about 64 bytes per input vertex and
     // triangle per plane; a further level multiplies that by width2 at most.
@@ -1215,6 +1230,7 @@ static int search_group(gpu_ctx_t ctx, int n_mesh, const MeshIn* M, const Search
     float* d_bnb_pts = pool_take<float>(ctx, 3 * LA_ROUGH_PTS * bnb_cap);
     double* d_bnb_mvol = pool_take<double>(ctx, bnb_cap);
     unsigned char* d_skip = pool_take<unsigned char>(ctx, max_jobs);
+    int* d_order = pool_take<int>(ctx, max_jobs);
     char* out_base = pool_take<char>(ctx, out_cap);
     char* scr_base = pool_take<char>(ctx, scr_cap);
     char* tmp_base = pool_take<char>(ctx, tmp_cap);
@@ -1230,6 +1246,7 @@ static int search_group(gpu_ctx_t ctx, int n_mesh, const MeshIn* M, const Search
     L.d_hjobs = d_hjobs; L.d_hstates = d_hstates; L.d_hctl = d_hctl; L.d_wbuf = d_wbuf; L.nwc = hull_wrap_ctas(1LL << 40, ctx->n_sm);
     L.d_bnb_surf = d_bnb_surf; L.d_bnb_pts = d_bnb_pts; L.d_bnb_mvol = d_bnb_mvol; L.d_skip = d_skip;
     L.bnb_cap = (int)bnb_cap;
+    L.d_order = d_order;
     // ---- initial parts: each mesh and the caller's hull (la_initialize, la_lifecycle.cu:18-81)
     std::vector<HPart> parts;
     {
