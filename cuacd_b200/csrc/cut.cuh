@@ -159,124 +159,6 @@ static __device__ int cut_ear_clip_cta(const Cap2D& c, const int* poly, int n, d
     return nc;
 }
 
-// Ear clipping of a polygon that fits shared memory, walked by warp 0 with
-// the same serial decisions as cut_ear_clip_cta.  The polygon's vertices are
-// first bucketed into a G x G grid over their box (the whole CTA); a convex
-// candidate ear then tests only the vertices in the cells its triangle's box
-// covers, grown by the most a vertex can lie outside the triangle and still
-// pass the tolerant point-in-triangle test: with d_i >= -1e-10 for all three
-// edge functions and d_1 + d_2 + d_3 = cr, the vertex is an affine
-// combination of the corners with weights >= -1e-10 / cr, so it lies within
-// 2 (1e-10 / cr) x the triangle's span of its box.  Those cells hold every
-// vertex the full scan could find inside, so the decision is the full
-// scan's; a warp vote replaces the CTA barrier of each tested ear.
-#define CUT_EAR_G 32        // at most CUT_EAR_G x CUT_EAR_G grid cells
-static __device__ __forceinline__ int ear_cell(double x, double lo, double inv, int g)
-{
-    const double f = floor((x - lo) * inv);
-    return f < 0.0 ? 0 : (f >= (double)g ? g - 1 : (int)f);
-}
-static __device__ int cut_ear_clip_grid(const Cap2D& c, const int* poly, int n, double* U, double* W,
-                                        int* prv, int* nxt, int* cap)
-{
-    __shared__ int s_start[CUT_EAR_G * CUT_EAR_G + 1], s_fill[CUT_EAR_G * CUT_EAR_G];
-    __shared__ int s_items[CUT_EAR_SM];
-    __shared__ double s_red[4][CUT_NT / 32];
-    __shared__ double s_lo[2], s_inv[2];
-    __shared__ int s_g, s_nc;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    double lu = 1e300, hu = -1e300, lw = 1e300, hw = -1e300;
-    for (int i = tid; i < n; i += CUT_NT) {
-        prv[i] = (i + n - 1) % n; nxt[i] = (i + 1) % n;
-        const double u = cU(c, poly[i]), w = cW(c, poly[i]);
-        U[i] = u; W[i] = w;
-        lu = fmin(lu, u); hu = fmax(hu, u); lw = fmin(lw, w); hw = fmax(hw, w);
-    }
-    for (int o = 16; o > 0; o >>= 1) {
-        lu = fmin(lu, __shfl_xor_sync(FULL_MASK, lu, o)); hu = fmax(hu, __shfl_xor_sync(FULL_MASK, hu, o));
-        lw = fmin(lw, __shfl_xor_sync(FULL_MASK, lw, o)); hw = fmax(hw, __shfl_xor_sync(FULL_MASK, hw, o));
-    }
-    if (lane == 0) { s_red[0][warp] = lu; s_red[1][warp] = hu; s_red[2][warp] = lw; s_red[3][warp] = hw; }
-    __syncthreads();
-    if (tid == 0) {
-        for (int k = 1; k < CUT_NT / 32; k++) {
-            lu = fmin(lu, s_red[0][k]); hu = fmax(hu, s_red[1][k]); lw = fmin(lw, s_red[2][k]); hw = fmax(hw, s_red[3][k]);
-        }
-        lu = fmin(lu, s_red[0][0]); hu = fmax(hu, s_red[1][0]); lw = fmin(lw, s_red[2][0]); hw = fmax(hw, s_red[3][0]);
-        int g = (int)sqrt((double)n * 0.5);
-        g = g < 1 ? 1 : (g > CUT_EAR_G ? CUT_EAR_G : g);
-        s_g = g;
-        s_lo[0] = lu; s_lo[1] = lw;
-        s_inv[0] = hu > lu ? (double)g / (hu - lu) : 0.0;
-        s_inv[1] = hw > lw ? (double)g / (hw - lw) : 0.0;
-    }
-    __syncthreads();
-    const int G = s_g;
-    for (int k = tid; k <= G * G; k += CUT_NT) s_start[k] = 0;
-    __syncthreads();
-    for (int i = tid; i < n; i += CUT_NT)
-        atomicAdd(&s_start[1 + ear_cell(U[i], s_lo[0], s_inv[0], G) + G * ear_cell(W[i], s_lo[1], s_inv[1], G)], 1);
-    __syncthreads();
-    if (tid == 0)
-        for (int k = 0; k < G * G; k++) { s_start[k + 1] += s_start[k]; s_fill[k] = s_start[k]; }
-    __syncthreads();
-    for (int i = tid; i < n; i += CUT_NT)
-        s_items[atomicAdd(&s_fill[ear_cell(U[i], s_lo[0], s_inv[0], G) + G * ear_cell(W[i], s_lo[1], s_inv[1], G)], 1)] = i;
-    __syncthreads();
-    if (warp == 0) {
-        int nc = 0;
-        int remaining = n, cur = 0, iter = 0;
-        while (remaining > 3 && iter < remaining) {
-            iter++;
-            const int p = prv[cur], q = nxt[cur];
-            const double up = U[p], wp = W[p], uc = U[cur], wc = W[cur], un = U[q], wn = W[q];
-            const double cr = (uc - up) * (wn - wp) - (wc - wp) * (un - up);
-            if (cr < -1e-9) { cur = q; continue; }
-            bool clip;
-            if (cr <= 1e-9) clip = true;
-            else {
-                const double bu0 = fmin(up, fmin(uc, un)), bu1 = fmax(up, fmax(uc, un));
-                const double bw0 = fmin(wp, fmin(wc, wn)), bw1 = fmax(wp, fmax(wc, wn));
-                const double grow = 2.0 * (1e-10 / cr) * fmax(bu1 - bu0, bw1 - bw0) + 1e-12;
-                const int cx0 = ear_cell(bu0 - grow, s_lo[0], s_inv[0], G), cx1 = ear_cell(bu1 + grow, s_lo[0], s_inv[0], G);
-                const int cy0 = ear_cell(bw0 - grow, s_lo[1], s_inv[1], G), cy1 = ear_cell(bw1 + grow, s_lo[1], s_inv[1], G);
-                int inside = 0;
-                for (int cy = cy0; cy <= cy1; cy++)
-                    for (int cx = cx0; cx <= cx1; cx++) {
-                        const int cell = cx + G * cy;
-                        for (int k = s_start[cell] + lane; k < s_start[cell + 1]; k += 32) {
-                            const int idx = s_items[k];
-                            if (idx == p || idx == cur || idx == q) continue;
-                            if (nxt[prv[idx]] != idx) continue;
-                            const double cu = U[idx], cw = W[idx];
-                            if (fabs(cu - up) + fabs(cw - wp) > 1e-6 &&
-                                fabs(cu - uc) + fabs(cw - wc) > 1e-6 &&
-                                fabs(cu - un) + fabs(cw - wn) > 1e-6 &&
-                                cut_pt_in_tri(cu, cw, up, wp, uc, wc, un, wn)) inside = 1;
-                        }
-                    }
-                clip = !__any_sync(FULL_MASK, inside);
-            }
-            if (clip) {
-                if (lane == 0) { cap[3 * nc] = poly[p]; cap[3 * nc + 1] = poly[cur]; cap[3 * nc + 2] = poly[q]; }
-                __syncwarp();                      // every lane has read this step's links
-                nxt[p] = q; prv[q] = p;            // every lane writes the same two links
-                __syncwarp();
-                nc++;
-                remaining--; cur = q; iter = 0;
-            } else cur = q;
-        }
-        if (remaining == 3) {
-            const int p = prv[cur], q = nxt[cur];
-            if (lane == 0) { cap[3 * nc] = poly[p]; cap[3 * nc + 1] = poly[cur]; cap[3 * nc + 2] = poly[q]; }
-            nc++;
-        }
-        if (lane == 0) s_nc = nc;
-    }
-    __syncthreads();
-    return s_nc;
-}
-
 // Caps from the directed boundary edges be[] (sorted by (a,b), packed a<<32|b).
 // Whole CTA: thread 0 traces the loops, nests them and bridges holes; the
 // ear clipping is CTA-wide.  gU/gW: 2*poly_cap doubles of global scratch for
@@ -481,7 +363,7 @@ static __device__ int cut_build_caps(const float* V, int n_all, const unsigned l
         expected += pn - 2;
         if (pn >= 3) {
             if (pn <= CUT_EAR_SM)
-                n_cap += cut_ear_clip_grid(C, poly, pn, s_U, s_W, s_prv, s_nxt, cap_out + 3 * n_cap);
+                n_cap += cut_ear_clip_cta(C, poly, pn, s_U, s_W, s_prv, s_nxt, cap_out + 3 * n_cap);
             else
                 n_cap += cut_ear_clip_cta(C, poly, pn, gU, gU + poly_cap, tmp, tmp + poly_cap, cap_out + 3 * n_cap);
         }
