@@ -108,6 +108,8 @@ _opt("cuacd_lookahead_decompose_batch", _I, [_P, _I, _P, _P, _P, _P, _P, _P, _P,
                                              _P, _I, _F, _I, _P, _P])
 _opt("cuacd_hull_set_tuning", _I, [_P, _I, _I, _I])
 _opt("cuacd_hull_get_tuning", _I, [_P, _I, ctypes.POINTER(_I), ctypes.POINTER(_I)])
+_opt("cuacd_hull_set_table_limit", _I, [_P, _I, _I])
+_opt("cuacd_hull_get_table_limit", _I, [_P, _I, ctypes.POINTER(_I)])
 _opt("cuacd_device_info", _I, [_P, ctypes.c_char_p, _I, ctypes.POINTER(_I)])
 _opt("cuacd_candidate_planes", _I, [_P, _P, _I, _P, _I, _I, _F, _F, _I, _F, _P, _P, _P])
 _opt("cuacd_profile_stages", _I, [_P, _I])

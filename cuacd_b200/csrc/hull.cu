@@ -10,9 +10,9 @@
 
 __global__ void __launch_bounds__(HULL_NT)
 k_hull_setup(const HullJob* __restrict__ jobs, int n_jobs, Arena* scratch, HullState* states, int* ctl,
-             int seed_min_n, int retry_round)
+             int seed_min_n, int retry_round, int reduce_max_n)
 {
-    hull_setup_body(jobs, n_jobs, scratch, states, ctl, seed_min_n, retry_round);
+    hull_setup_body(jobs, n_jobs, scratch, states, ctl, seed_min_n, retry_round, reduce_max_n);
 }
 
 // Wrap-grid shares (one CTA): prefix of the active hulls' weights, a hull's
@@ -67,7 +67,7 @@ static int hull_wrap_per_sm()
 // cloud) and the cloud size from which wrapping starts at HULL_SEEDS seed
 // faces.  Per device; the defaults hold until cuacd_hull_set_tuning (the
 // autotuner, cuacd_b200/autotune.py) replaces them.
-struct HullTune { int pts_per_cta, seed_min_n; };
+struct HullTune { int pts_per_cta, seed_min_n, reduce_max_n; };
 static HullTune g_hull_tune[64][HULL_TUNE_CLASSES] = {};
 static std::mutex g_hull_tune_mu;
 
@@ -86,6 +86,7 @@ static HullTune hull_tune(int cls)
     HullTune t = g_hull_tune[cur_device()][cls];
     if (t.pts_per_cta <= 0) t.pts_per_cta = 4096;
     if (t.seed_min_n <= 0) t.seed_min_n = 1 << 30;
+    if (t.reduce_max_n <= 0) t.reduce_max_n = HULL_REDUCE_MAX_N;
     return t;
 }
 
@@ -94,7 +95,8 @@ extern "C" int cuacd_hull_set_tuning(gpu_ctx_t ctx, int size_class, int pts_per_
     if (!ctx || size_class < 0 || size_class >= HULL_TUNE_CLASSES || pts_per_cta < 0 || seed_min_n < 0) return -1;
     cudaSetDevice(ctx->device);
     std::lock_guard<std::mutex> lock(g_hull_tune_mu);
-    g_hull_tune[ctx->device >= 0 && ctx->device < 64 ? ctx->device : 0][size_class] = {pts_per_cta, seed_min_n};
+    HullTune& t = g_hull_tune[ctx->device >= 0 && ctx->device < 64 ? ctx->device : 0][size_class];
+    t.pts_per_cta = pts_per_cta; t.seed_min_n = seed_min_n;
     return 0;
 }
 
@@ -104,6 +106,23 @@ extern "C" int cuacd_hull_get_tuning(gpu_ctx_t ctx, int size_class, int* pts_per
     cudaSetDevice(ctx->device);
     const HullTune t = hull_tune(size_class);
     *pts_per_cta = t.pts_per_cta; *seed_min_n = t.seed_min_n;
+    return 0;
+}
+
+extern "C" int cuacd_hull_set_table_limit(gpu_ctx_t ctx, int size_class, int reduce_max_n)
+{
+    if (!ctx || size_class < 0 || size_class >= HULL_TUNE_CLASSES || reduce_max_n < 0) return -1;
+    cudaSetDevice(ctx->device);
+    std::lock_guard<std::mutex> lock(g_hull_tune_mu);
+    g_hull_tune[ctx->device >= 0 && ctx->device < 64 ? ctx->device : 0][size_class].reduce_max_n = reduce_max_n;
+    return 0;
+}
+
+extern "C" int cuacd_hull_get_table_limit(gpu_ctx_t ctx, int size_class, int* reduce_max_n)
+{
+    if (!ctx || size_class < 0 || size_class >= HULL_TUNE_CLASSES || !reduce_max_n) return -1;
+    cudaSetDevice(ctx->device);
+    *reduce_max_n = hull_tune(size_class).reduce_max_n;
     return 0;
 }
 
@@ -122,19 +141,22 @@ int hull_wrap_ctas(long long total_points, int n_sm, int max_pts)
 
 void launch_hull_jobs(const HullJob* d_jobs, int n_jobs, HullState* d_states, HullRes* d_res, Arena* scratch,
                       Arena* out, int* d_ctl, int* d_wbuf, int n_wrap_ctas, unsigned long long* d_stats,
-                      cudaStream_t s, int max_pts)
+                      cudaStream_t s, int max_pts, bool reduce)
 {
     if (n_jobs <= 0) return;
-    const int seed_min_n = hull_tune(hull_size_class(max_pts)).seed_min_n;
+    HullTune tune = hull_tune(hull_size_class(max_pts));
+    if (!reduce) tune.reduce_max_n = HULL_FIRST_CAP;
+    const int seed_min_n = tune.seed_min_n;
     hull_wrap_per_sm();                                   // dynamic shared memory opt-in
     // round 0 builds every cloud with first-attempt tables; round 1 (only
     // launched when a cloud of the batch can outgrow them) rebuilds the
     // clouds whose tables overflowed at full capacity -- its kernels return
     // at once when there are none
-    const int rounds = max_pts > HULL_FIRST_CAP ? 2 : 1;
+    const int rounds = max_pts > HULL_FIRST_CAP && tune.reduce_max_n > HULL_FIRST_CAP ? 2 : 1;
     for (int r = 0; r < rounds; r++) {
         cudaMemsetAsync(d_ctl, 0, 4 * sizeof(int), s);
-        k_hull_setup<<<n_jobs, HULL_NT, 0, s>>>(d_jobs, n_jobs, scratch, d_states, d_ctl, seed_min_n, r);
+        k_hull_setup<<<n_jobs, HULL_NT, 0, s>>>(d_jobs, n_jobs, scratch, d_states, d_ctl, seed_min_n, r,
+                                                tune.reduce_max_n);
         k_hull_assign<<<1, 1024, 0, s>>>(d_states, n_jobs, n_wrap_ctas, (long long*)(d_ctl + 2));
         k_hull_wrap<<<n_wrap_ctas, HULL_NT, HULL_WRAP_DSMEM, s>>>(d_states, n_jobs, d_ctl,
                                                                  (const long long*)(d_ctl + 2), d_wbuf);

@@ -64,10 +64,13 @@ __host__ __device__ inline int hull_pow2(int x) { int p = 1; while (p < x) p <<=
 // start four times smaller; a cloud whose hull outgrows them (a convex
 // cloud, such as the vertices of a fine sphere, has every point on its hull)
 // is built again with h = n in the same launch sequence.
+// Clouds above reduce_max_n points start at full size: large clouds are
+// often convex-ish (a whole input mesh), and a second attempt at them would
+// repeat most of the wrapping (the tuned size class sets the limit).
 #define HULL_FIRST_CAP 4096
-__host__ __device__ inline int hull_first_cap(int n)
+__host__ __device__ inline int hull_first_cap(int n, int reduce_max_n = 1 << 30)
 {
-    if (n <= HULL_FIRST_CAP) return n;
+    if (n <= HULL_FIRST_CAP || n > reduce_max_n) return n;
     return n / 4 > HULL_FIRST_CAP ? n / 4 : HULL_FIRST_CAP;
 }
 
@@ -692,9 +695,9 @@ __host__ __device__ inline size_t hull_attempt_bytes(int n, int h)
 
 // Scratch a cloud may use over both attempts (the first one's stays
 // allocated while the second runs): what callers reserve per cloud.
-__host__ __device__ inline size_t hull_scratch_bytes(int n)
+__host__ __device__ inline size_t hull_scratch_bytes(int n, int reduce_max_n = 1 << 30)
 {
-    const int h1 = hull_first_cap(n);
+    const int h1 = hull_first_cap(n, reduce_max_n);
     return hull_align(hull_attempt_bytes(n, h1)) + (h1 < n ? hull_align(hull_attempt_bytes(n, n)) : 0);
 }
 

@@ -8,7 +8,7 @@
 // retry_round 0: every cloud, first-attempt capacities (hull_first_cap);
 // retry_round 1: only the clouds whose tables overflowed, at h = n.
 static __device__ void hull_setup_body(const HullJob* __restrict__ jobs, int n_jobs, Arena* scratch, HullState* states, int* ctl,
-                                       int seed_min_n = 1 << 30, int retry_round = 0)
+                                       int seed_min_n = 1 << 30, int retry_round = 0, int reduce_max_n = 1 << 30)
 {
     __shared__ HullSetupShared sh;
     __shared__ char* s_scr;
@@ -21,7 +21,7 @@ static __device__ void hull_setup_body(const HullJob* __restrict__ jobs, int n_j
         if (threadIdx.x == 0) S->active = 0;
         return;
     }
-    const int hcap = retry_round ? J.n : hull_first_cap(J.n);
+    const int hcap = retry_round ? J.n : hull_first_cap(J.n, reduce_max_n);
     double mv = 0.0;
     if (J.tris && J.nt > 0 && J.n > 0) mv = block_mesh_signed_volume(J.pts, J.n, J.tris, J.nt, sh.dsh);
     if (threadIdx.x == 0) {

@@ -48,6 +48,7 @@ struct HullRes;
 struct HullState;
 size_t hull_wrap_buf_bytes(int n_wrap_ctas);
 #define HULL_TUNE_CLASSES 3
+#define HULL_REDUCE_MAX_N 32768     // default: clouds of 4,097-32,768 points start with quarter-size tables
 int hull_size_class(int max_pts);
 // Wrap CTAs for a batch of total_points points whose largest cloud has
 // max_pts (its size class picks the tuned points per CTA).
@@ -59,9 +60,10 @@ inline long long hull_wrap_points(int n_hulls, int max_pts)
 {
     return (long long)n_hulls * (max_pts > 256 ? max_pts : 256);
 }
+// reduce = false: every cloud starts with full-size tables (one round).
 void launch_hull_jobs(const HullJob* d_jobs, int n_jobs, HullState* d_states, HullRes* d_res, Arena* scratch,
                       Arena* out, int* d_ctl, int* d_wbuf, int n_wrap_ctas, unsigned long long* d_stats,
-                      cudaStream_t s, int max_pts);
+                      cudaStream_t s, int max_pts, bool reduce = true);
 void launch_jobs_from_offsets(const float* d_pts, const int* d_off, int n, float* d_v, int* d_t, int max_hv,
                               int max_ht, HullJob* d_jobs, cudaStream_t s);
 void launch_unpack_results(const HullRes* d_res, int n, int* d_nv, int* d_nt, float* d_vol, int* d_err, cudaStream_t s);

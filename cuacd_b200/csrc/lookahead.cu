@@ -478,7 +478,11 @@ struct Lookahead {
     int nwc = 1; size_t wbuf_bytes = 0;
 
     // Hulls of jobs [0, n) already in d_hjobs, results into res[0, n); waves
-    // keep the per-hull scratch within the scratch arena.
+    // keep the per-hull scratch within the scratch arena.  The search's
+    // fragments start with full-size hull tables: many are near-convex
+    // pieces of smooth meshes whose hulls outgrow quarter-size tables, and
+    // rebuilding those cost more (config-4 sample: 1.03 s against 0.87 s)
+    // than clearing full tables.
     int run_hulls(const std::vector<int>& sizes, FragRes* res)
     {
         const int n = (int)sizes.size();
@@ -486,7 +490,7 @@ struct Lookahead {
         while (f < n) {
             size_t acc = 0; int f1 = f;
             while (f1 < n) {
-                size_t e = al256(hull_scratch_bytes(sizes[f1] > 4 ? sizes[f1] : 4)) + 256;
+                size_t e = al256(hull_scratch_bytes(sizes[f1] > 4 ? sizes[f1] : 4, HULL_FIRST_CAP)) + 256;
                 if (f1 > f && acc + e > scr_cap) break;
                 acc += e; f1++;
             }
@@ -494,7 +498,7 @@ struct Lookahead {
             for (int k = f; k < f1; k++) { pts += std::max(sizes[k], 256); mx = std::max(mx, sizes[k]); }
             reset_scr();
             launch_hull_jobs(d_hjobs + f, f1 - f, d_hstates + f, res + f, d_scr, d_cur, d_hctl, d_wbuf,
-                             std::min(nwc, hull_wrap_ctas(pts, ctx->n_sm, mx)), nullptr, s, mx);
+                             std::min(nwc, hull_wrap_ctas(pts, ctx->n_sm, mx)), nullptr, s, mx, false);
             ctx->launches += 5;
             f = f1;
         }
