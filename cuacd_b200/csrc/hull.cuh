@@ -306,8 +306,17 @@ static __device__ __forceinline__ void warp_best(int& ci, float4& cq, float4 a, 
 // comparator.
 // Returns c (sorted id), -1 if all points are on the line, -2 if the warp
 // queues overflowed (the caller then uses the serial search).
+// ties_out (optional, edge mode): how many scanned points other than u, v
+// and c lie on the final plane (every point of the line through u and v
+// counts), same value on every lane; 0 means the face is the triangle
+// (v, u, c).  Exact: every point on the final plane is scanned (its box is
+// never strictly behind an earlier plane), and a point on it scanned under
+// an earlier plane would have become the candidate, so each is either the
+// candidate or counted against the plane it lies on -- a lane's count
+// survives a reduction only when its own candidate lies on the winning
+// plane (the two planes are then the same).
 static __device__ int warp_wrap(const HullCtx& H, int u, int v, const WarpLists W, int lane, int* nleaf_out,
-                                unsigned& n_pts, unsigned& n64, const int* dir = nullptr)
+                                unsigned& n_pts, unsigned& n64, const int* dir = nullptr, int* ties_out = nullptr)
 {
     // dir: wrap about the line through u with this direction (v unused)
     const unsigned lt = (1u << lane) - 1u;
@@ -322,13 +331,22 @@ static __device__ int warp_wrap(const HullCtx& H, int u, int v, const WarpLists 
         mx = dy * ez - dz * ey; my = dz * ex - dx * ez; mz = dx * ey - dy * ex;
         fx = (float)mx; fy = (float)my; fz = (float)mz;
     };
+    int tie = 0, online = 0;         // points on this lane's plane / on the line (other than u, v)
     auto take = [&](int qi) {
         float4 q = H.pts[qi];
         n_pts++;
-        if (on_line(dx, dy, dz, a, q)) return;
-        bool t = ci < 0;
-        if (!t) t = plane_sign(mx, my, mz, fx, fy, fz, a, q, n64) < 0;
-        if (t) { ci = qi; cq = q; setm(); }
+        if (on_line(dx, dy, dz, a, q)) { online += (qi != u && qi != v); return; }
+        if (ci < 0) { ci = qi; cq = q; setm(); tie = 0; return; }
+        const int sg = plane_sign(mx, my, mz, fx, fy, fz, a, q, n64);
+        if (sg < 0) { ci = qi; cq = q; setm(); tie = 0; }
+        else if (sg == 0 && qi != ci) tie++;
+    };
+    // warp reduction of the candidates; each lane's tie count follows it
+    auto reduce = [&]() {
+        const int c0 = ci; const float4 q0 = cq;
+        warp_best(ci, cq, a, dx, dy, dz, n64);
+        if (ci >= 0) setm();
+        if (ci != c0) tie = (c0 >= 0 && plane_sign(mx, my, mz, fx, fy, fz, a, q0, n64) == 0) ? tie + 1 : 0;
     };
     {
         const int lu = u / HULL_LEAF, lv = v / HULL_LEAF;
@@ -336,8 +354,7 @@ static __device__ int warp_wrap(const HullCtx& H, int u, int v, const WarpLists 
         const int i = leaf * HULL_LEAF + (lane & 15);
         if ((lane < 16 || lv != lu) && i < H.m) take(i);
     }
-    warp_best(ci, cq, a, dx, dy, dz, n64);
-    if (ci >= 0) setm();
+    reduce();
     // Depth-first sweep, 32 nodes per step from the top of a warp stack.
     // Each step's newly kept leaves are scanned at once, so the plane
     // tightens while the sweep is still near the seed and later boxes are
@@ -412,14 +429,17 @@ static __device__ int warp_wrap(const HullCtx& H, int u, int v, const WarpLists 
                 if (p < H.m) take(p);
             }
             // reduce only when some lane found a better point
-            if (__any_sync(FULL_MASK, ci != ci0)) {
-                warp_best(ci, cq, a, dx, dy, dz, n64);
-                if (ci >= 0) setm();
-            }
+            if (__any_sync(FULL_MASK, ci != ci0)) reduce();
             scanned = nl;
         }
     }
     *nleaf_out = nl;
+    if (ties_out) {
+        int t = tie + online;
+        #pragma unroll
+        for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(FULL_MASK, t, o);
+        *ties_out = t;
+    }
     return ci;
 }
 
@@ -1252,16 +1272,16 @@ static __device__ void hull_wrap_edge(HullState* S, int u, int v, HullWarp& W, c
 {
     const HullCtx H = hull_ctx(*S);
     const float4* P4 = H.pts;
-    int nl = 0;
+    int nl = 0, ties = 1;
     WarpLists L = Ls;
     bool locked = false;
-    int c = warp_wrap(H, u, v, L, lane, &nl, st_pts, st_64);
+    int c = warp_wrap(H, u, v, L, lane, &nl, st_pts, st_64, nullptr, &ties);
     if (c == -2) {                                   // shared lists too small: the hull's own
         locked = hull_lock(S, lane);
         if (!locked) return;
         if (lane == 0) atomicAdd(&S->stats[7], 1ull << 32);
         L.q = S->ocnt; L.leaf = S->ocnt + 2 * S->P; L.qcap = 2 * S->P; L.lcap = S->P;
-        c = warp_wrap(H, u, v, L, lane, &nl, st_pts, st_64);
+        c = warp_wrap(H, u, v, L, lane, &nl, st_pts, st_64, nullptr, &ties);
         if (c == -2) {                               // cannot happen: 2P + P hold the whole tree
             if (lane == 0) atomicOr(&S->err, KERR_BT_WARP_OOM);
             hull_unlock(S, lane);
@@ -1277,7 +1297,9 @@ static __device__ void hull_wrap_edge(HullState* S, int u, int v, HullWarp& W, c
         float4 pc = P4[c];
         double ex = pc.x - pu.x, ey = pc.y - pu.y, ez = pc.z - pu.z;
         nx = ey * dz - ez * dy; ny = ez * dx - ex * dz; nz = ex * dy - ey * dx;
-        ns = warp_coplanar(H, pu, nx, ny, nz, W, L, nl, lane, HULL_SMALL_S, st_cop, st_64);
+        // no other point on the plane: the triangle (v, u, c) without a
+        // coplanar pass
+        ns = ties == 0 ? 3 : warp_coplanar(H, pu, nx, ny, nz, W, L, nl, lane, HULL_SMALL_S, st_cop, st_64);
     }
     int k = -1;
     const int* poly = Pg;
