@@ -94,61 +94,104 @@ static __device__ __forceinline__ int cut_pt_in_tri(double px, double py, double
     return !(neg && pos);
 }
 
-// Ear clipping of one polygon by the whole CTA.  Every thread follows the
-// same serial walk (cur, remaining); the test of a convex candidate ear
-// against the polygon's remaining vertices is split over the CTA and
-// combined with __syncthreads_or, so the decisions -- and the triangles --
-// are those of the one-thread walk.  U/W hold the polygon's 2D coordinates
+// Ear clipping of one polygon by the whole CTA, with the decisions -- and
+// so the triangles -- of the one-thread walk (cur, remaining, iter): at cur
+// with prev p, clip (p, cur, next) when it is degenerate or convex with no
+// remaining vertex inside, advancing to next either way.  Every thread
+// follows the walk.  At a convex or degenerate cur the walk would, as long
+// as it keeps clipping, clip the fan p, c0 = cur, c1, c2, ... (each clip
+// makes p the prev of the next vertex), so the first K triangles of the fan
+// are tested in one pass of the CTA, triangle k against the vertices that
+// remain once c0 .. c(k-1) are clipped, and the walk clips up to the first
+// triangle that fails (a reflex triangle ends the fan before it).  One
+// barrier per pass instead of one per tested ear.  K adapts: it doubles
+// (up to CUT_EAR_SPEC) after a fan clipped whole and restarts at 2 after a
+// failed ear, so walks whose ears often fail test few triangles ahead.
+// Every thread writes the same fan (s_chain) and links and reads its own
+// writes; fan and inside masks are double-buffered by pass parity, and the
+// links of pass r + 1 are only written after its barrier, which every thread
+// reaches after its reads of pass r + 1.  U/W hold the polygon's 2D coordinates
 // (FP64), prv/nxt its links.  Returns the triangle count.
 #define CUT_EAR_SM 1024     // polygons up to this size keep U/W/prv/nxt in shared memory
+#define CUT_EAR_SPEC 32     // most fan triangles tested per pass
 static __device__ int cut_ear_clip_cta(const Cap2D& c, const int* poly, int n, double* U, double* W,
                                        int* prv, int* nxt, int* cap)
 {
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    __shared__ int s_chain[2][CUT_EAR_SPEC + 1];
+    __shared__ unsigned s_wm[2][CUT_NT / 32];
     for (int i = tid; i < n; i += CUT_NT) {
         prv[i] = (i + n - 1) % n; nxt[i] = (i + 1) % n;
         U[i] = cU(c, poly[i]); W[i] = cW(c, poly[i]);
     }
     __syncthreads();
-    int nc = 0;
-    int remaining = n, cur = 0, iter = 0;
-    while (remaining > 3 && iter < remaining) {
-        iter++;
-        const int p = prv[cur], q = nxt[cur];
-        const double up = U[p], wp = W[p], uc = U[cur], wc = W[cur], un = U[q], wn = W[q];
-        const double cr = (uc - up) * (wn - wp) - (wc - wp) * (un - up);
-        if (cr < -1e-9) { cur = q; continue; }
-        bool clip;
-        if (cr <= 1e-9) clip = true;
-        else {
-            int inside = 0;
-            for (int idx = tid; idx < n; idx += CUT_NT) {
-                if (idx == p || idx == cur || idx == q) continue;
-                if (nxt[prv[idx]] != idx) continue;
-                const double cu = U[idx], cw = W[idx];
-                if (fabs(cu - up) + fabs(cw - wp) > 1e-6 &&
-                    fabs(cu - uc) + fabs(cw - wc) > 1e-6 &&
-                    fabs(cu - un) + fabs(cw - wn) > 1e-6 &&
-                    cut_pt_in_tri(cu, cw, up, wp, uc, wc, un, wn)) inside = 1;
-            }
-            clip = __syncthreads_or(inside) == 0;
+    int nc = 0, remaining = n, cur = 0, iter = 0, kspec = 2;
+    for (int pass = 0;; pass++) {
+        const int b = pass & 1;
+        bool done = false;
+        for (;;) {                                   // reflex steps
+            if (!(remaining > 3 && iter < remaining)) { done = true; break; }
+            const int p = prv[cur], q = nxt[cur];
+            const double up = U[p], wp = W[p], uc = U[cur], wc = W[cur], un = U[q], wn = W[q];
+            const double cr = (uc - up) * (wn - wp) - (wc - wp) * (un - up);
+            if (cr < -1e-9) { iter++; cur = q; continue; }
+            break;
         }
-        if (clip) {
-            // Reflex steps and a degenerate ear meet no barrier, so a lagging
-            // thread may still be reading nxt[]/prv[] of an earlier step of
-            // the walk (nxt[p] among them): a degenerate ear waits before the
-            // links change, or that thread would follow another walk into
-            // another barrier (a tested ear already met __syncthreads_or).
-            // Every thread then writes the same two links itself, so its own
-            // next reads see them without a second barrier; no thread can
-            // write the next clip's links before all have met that clip's
-            // barrier.
-            if (cr <= 1e-9) __syncthreads();
-            if (tid == 0) { cap[3 * nc] = poly[p]; cap[3 * nc + 1] = poly[cur]; cap[3 * nc + 2] = poly[q]; }
-            nxt[p] = q; prv[q] = p;
-            nc++;
-            remaining--; cur = q; iter = 0;
-        } else cur = q;
+        if (done) break;
+        const int p = prv[cur];
+        const double up = U[p], wp = W[p];
+        const int kmax = min(kspec, remaining - 3);
+        int K = 0, cv = cur;
+        unsigned need = 0;                           // bit k: triangle k is convex (needs the inside test)
+        s_chain[b][0] = cur;
+        while (K < kmax) {
+            const int q = nxt[cv];
+            const double uc = U[cv], wc = W[cv], un = U[q], wn = W[q];
+            const double cr = (uc - up) * (wn - wp) - (wc - wp) * (un - up);
+            if (cr < -1e-9) break;                   // reflex: the fan ends before it
+            if (cr > 1e-9) need |= 1u << K;
+            s_chain[b][K + 1] = q;
+            K++; cv = q;
+        }
+        unsigned bits = 0;                           // bit k: a remaining vertex lies in fan triangle k
+        if (need) {
+            for (int idx = tid; idx < n; idx += CUT_NT) {
+                if (idx == p || nxt[prv[idx]] != idx) continue;
+                int pos = -1;
+                for (int j = 0; j <= K; j++) if (s_chain[b][j] == idx) { pos = j; break; }
+                // triangle k skips its own corners and the clipped c0 .. c(k-1)
+                const int kend = pos < 0 ? K : pos - 1;
+                const double cu = U[idx], cw = W[idx];
+                for (int k = 0; k < kend; k++) {
+                    if (!((need >> k) & 1u) || ((bits >> k) & 1u)) continue;
+                    const int ck = s_chain[b][k], cn = s_chain[b][k + 1];
+                    const double uc = U[ck], wc = W[ck], un = U[cn], wn = W[cn];
+                    if (fabs(cu - up) + fabs(cw - wp) > 1e-6 &&
+                        fabs(cu - uc) + fabs(cw - wc) > 1e-6 &&
+                        fabs(cu - un) + fabs(cw - wn) > 1e-6 &&
+                        cut_pt_in_tri(cu, cw, up, wp, uc, wc, un, wn)) bits |= 1u << k;
+                }
+            }
+        }
+        #pragma unroll
+        for (int o = 16; o > 0; o >>= 1) bits |= __shfl_xor_sync(FULL_MASK, bits, o);
+        if (lane == 0) s_wm[b][warp] = bits;
+        __syncthreads();
+        unsigned inside = 0;
+        for (int w = 0; w < CUT_NT / 32; w++) inside |= s_wm[b][w];
+        const unsigned fail = need & inside;
+        const int ks = fail ? __ffs(fail) - 1 : K;   // triangles clipped
+        // the clips in the walk's order; each made p the prev of the next vertex
+        if (tid == 0)
+            for (int k = 0; k < ks; k++) {
+                cap[3 * (nc + k)] = poly[p]; cap[3 * (nc + k) + 1] = poly[s_chain[b][k]];
+                cap[3 * (nc + k) + 2] = poly[s_chain[b][k + 1]];
+            }
+        for (int j = 1; j <= ks; j++) prv[s_chain[b][j]] = p;
+        if (ks > 0) nxt[p] = s_chain[b][ks];
+        nc += ks; remaining -= ks;
+        if (ks < K) { iter = (ks > 0 ? 0 : iter) + 1; cur = s_chain[b][ks + 1]; kspec = 2; }   // the failed ear
+        else        { iter = 0; cur = s_chain[b][K]; kspec = min(2 * kspec, CUT_EAR_SPEC); }
     }
     if (remaining == 3) {
         const int p = prv[cur], q = nxt[cur];
