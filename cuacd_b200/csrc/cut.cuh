@@ -233,10 +233,12 @@ static __device__ int cut_build_caps(const float* V, int n_all, const unsigned l
     // order: same result.
     const bool fast = nb <= CUT_EAR_SM;
     __shared__ int s_le[CUT_EAR_SM];
+    __shared__ int s_ea[CUT_EAR_SM], s_eb[CUT_EAR_SM];     // each edge's start and end vertex
     int* le = fast ? s_le : used;
     if (fast) {
         for (int i = tid; i < nb; i += CUT_NT) {
             const int a = (int)(be[i] >> 32), b = (int)(be[i] & 0xffffffffu);
+            s_ea[i] = a; s_eb[i] = b;
             s_U[i] = (a >= 0 && a < n_all) ? cU(C, a) : 0.0;
             s_W[i] = (a >= 0 && a < n_all) ? cW(C, a) : 0.0;
             s_nxt[i] = lower_bound_u64(be, nb, (unsigned long long)(unsigned)b << 32);
@@ -261,7 +263,7 @@ static __device__ int cut_build_caps(const float* V, int n_all, const unsigned l
         if (!fast) for (int i = 0; i < nb; i++) used[i] = 0;
         for (int st = 0; st < nb && !fail; st++) {
             if (fast ? s_prv[st] : used[st]) continue;
-            int first = (int)(be[st] >> 32), cur = (int)(be[st] & 0xffffffffu);
+            int first = fast ? s_ea[st] : (int)(be[st] >> 32), cur = fast ? s_eb[st] : (int)(be[st] & 0xffffffffu);
             if (first < 0 || first >= n_all || cur < 0 || cur >= n_all) { fail = 1; break; }
             int ce = st;
             if (fast) { s_prv[st] = 1; le[lvi] = st; } else used[st] = 1;
@@ -273,7 +275,7 @@ static __device__ int cut_build_caps(const float* V, int n_all, const unsigned l
                 lv[lvi] = cur;
                 int found = -1;
                 if (fast) {
-                    for (int k = s_nxt[ce]; k < nb && (int)(be[k] >> 32) == cur; k++) if (!s_prv[k]) { found = k; break; }
+                    for (int k = s_nxt[ce]; k < nb && s_ea[k] == cur; k++) if (!s_prv[k]) { found = k; break; }
                 } else {
                     int lo = lower_bound_u64(be, nb, (unsigned long long)(unsigned)cur << 32);
                     for (int k = lo; k < nb && (int)(be[k] >> 32) == cur; k++) if (!used[k]) { found = k; break; }
@@ -282,7 +284,7 @@ static __device__ int cut_build_caps(const float* V, int n_all, const unsigned l
                 if (fast) { s_prv[found] = 1; le[lvi] = found; } else used[found] = 1;
                 lvi++;
                 ce = found;
-                cur = (int)(be[found] & 0xffffffffu);
+                cur = fast ? s_eb[found] : (int)(be[found] & 0xffffffffu);
             }
             if (fail || cur != first) { fail = 1; break; }
             ls[n_loops] = start; lsz[n_loops] = lvi - start; n_loops++;
@@ -297,33 +299,56 @@ static __device__ int cut_build_caps(const float* V, int n_all, const unsigned l
     if (fail) return -1;
     __shared__ int parent[128], is_hole[128], hidx[128];
     __shared__ double hmax[128];
+    __shared__ double s_area[128];
+    __shared__ int s_ls[128], s_lsz[128], s_cross[2][128];
     int n_cap = 0;
+    // Nesting: a loop's parent is the smallest loop (by |area|) that a ray
+    // from its first vertex crosses an odd number of times.  Orientation and
+    // the areas (computed once per loop, after the orientation fix, in the
+    // walk's order) are thread 0's; the crossings of each loop's ray are
+    // counted by the CTA, edge by edge with the same test, so the parities
+    // -- and the parents -- are those of the serial count.
     if (tid == 0) {
         for (int i = 0; i < n_loops; i++)
             if (loop_area(ls[i], lsz[i]) < 0) loop_reverse(ls[i], lsz[i]);
-        for (int i = 0; i < n_loops; i++) { parent[i] = -1; is_hole[i] = 0; }
         for (int i = 0; i < n_loops; i++) {
-            if (lsz[i] < 3) continue;
-            double pu_ = LU(ls[i]), pv_ = LW(ls[i]);
-            double best_area = 1e300;
-            for (int j = 0; j < n_loops; j++) {
-                if (j == i || lsz[j] < 3) continue;
-                const int lp = ls[j];
-                int m = lsz[j], crossings = 0;
-                for (int k = 0; k < m; k++) {
-                    int kn = (k + 1) % m;
-                    double ay = LW(lp + k), by = LW(lp + kn);
-                    if ((ay <= pv_) == (by <= pv_)) continue;
-                    double ax = LU(lp + k), bx = LU(lp + kn);
-                    double t = (pv_ - ay) / (by - ay);
-                    if (ax + t * (bx - ax) > pu_) crossings++;
-                }
-                if (crossings & 1) {
-                    double a = fabs(loop_area(lp, m));
-                    if (a < best_area) { best_area = a; parent[i] = j; }
+            parent[i] = -1; is_hole[i] = 0; s_ls[i] = ls[i]; s_lsz[i] = lsz[i];
+            s_area[i] = lsz[i] >= 3 ? fabs(loop_area(ls[i], lsz[i])) : 0.0;
+        }
+    }
+    __syncthreads();
+    if (n_loops > 1) {
+        const int npos = s_ls[n_loops - 1] + s_lsz[n_loops - 1];
+        int round = 0;                               // counts buffered by round parity
+        for (int i = 0; i < n_loops; i++) {
+            if (s_lsz[i] < 3) continue;
+            int* cross = s_cross[round++ & 1];
+            for (int j = tid; j < n_loops; j += CUT_NT) cross[j] = 0;
+            __syncthreads();
+            const double pu_ = LU(s_ls[i]), pv_ = LW(s_ls[i]);
+            for (int pos = tid; pos < npos; pos += CUT_NT) {
+                int lo = 0, hi = n_loops - 1;            // the loop holding pos
+                while (lo < hi) { const int mid = (lo + hi + 1) >> 1; if (s_ls[mid] <= pos) lo = mid; else hi = mid - 1; }
+                const int j = lo, m = s_lsz[j];
+                if (j == i || m < 3) continue;
+                const int k = pos - s_ls[j], kn = (k + 1) % m;
+                const double ay = LW(s_ls[j] + k), by = LW(s_ls[j] + kn);
+                if ((ay <= pv_) == (by <= pv_)) continue;
+                const double ax = LU(s_ls[j] + k), bx = LU(s_ls[j] + kn);
+                const double t = (pv_ - ay) / (by - ay);
+                if (ax + t * (bx - ax) > pu_) atomicAdd(&cross[j], 1);
+            }
+            __syncthreads();
+            if (tid == 0) {
+                double best_area = 1e300;
+                for (int j = 0; j < n_loops; j++) {
+                    if (j == i || s_lsz[j] < 3) continue;
+                    if ((cross[j] & 1) && s_area[j] < best_area) { best_area = s_area[j]; parent[i] = j; }
                 }
             }
         }
+    }
+    if (tid == 0) {
         for (int i = 0; i < n_loops && !fail; i++) {
             int steps = 0;
             for (int p = parent[i]; p >= 0; p = parent[p]) if (++steps > n_loops) { fail = 1; break; }
