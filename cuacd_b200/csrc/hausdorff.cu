@@ -34,8 +34,6 @@ k_hd_prep(const HDSurf* __restrict__ surfs, int n_surf, Arena* arena, float reso
     hd_prep_cta(S, s_scr, resolution, min_samples, total_override, &preps[i], sh);
 }
 
-struct HDDir { int src, dst, pair, n_samples, chunk0; };
-
 // Plan the query directions: pair p has surfaces 2p (A) and 2p+1 (B);
 // direction 2p samples A against B, 2p+1 samples B against A.
 __global__ void k_hd_plan(const HDSurf* surfs, const HDPrep* preps, int n_pairs, HDDir* dirs, int* total_chunks,
@@ -60,143 +58,11 @@ __global__ void k_hd_plan(const HDSurf* surfs, const HDPrep* preps, int n_pairs,
     *counter = 0;
 }
 
-// Queries.  Each CTA takes chunks of HD_CHUNK samples from the device
-// counter; inside a chunk every lane is persistent: it takes the next sample
-// from the chunk as soon as its own search ends, and advances its search one
-// BVH node or leaf per step, so lanes do not wait for the warp's longest
-// search.  A search stops once its best distance is <= the pair's running
-// maximum (refreshed at every leaf); only finished searches above that
-// maximum raise it, so the final maximum is exact.
 __global__ void __launch_bounds__(HD_NT)
 k_hd_query(const HDSurf* __restrict__ surfs, const HDPrep* __restrict__ preps, const HDDir* __restrict__ dirs,
            int n_dirs, const int* total_chunks, int* counter, float* pair_max)
 {
-    __shared__ int s_chunk, s_next, s_a0;
-    __shared__ int s_pos[HD_CHUNK];              // sorted triangle position of each sample of the chunk
-    const int total = *total_chunks;
-    for (;;) {
-        if (threadIdx.x == 0) { s_chunk = atomicAdd(counter, 1); s_next = 0; }
-        __syncthreads();
-        const int c = s_chunk;
-        if (c >= total) break;
-        int lo = 0, hi = n_dirs;                 // last dir with chunk0 <= c
-        while (hi - lo > 1) { int m = (lo + hi) >> 1; if (dirs[m].chunk0 <= c) lo = m; else hi = m; }
-        while (lo + 1 < n_dirs && dirs[lo + 1].chunk0 <= c && dirs[lo].n_samples == 0) lo++;
-        const HDDir D = dirs[lo];
-        const HDSurf S = surfs[D.src];
-        const HDPrep& PS = preps[D.src];
-        const HDPrep PD = preps[D.dst];
-        const int s0 = (c - D.chunk0) * HD_CHUNK;
-        const int n_chunk = min(HD_CHUNK, D.n_samples - s0);
-        volatile float* vmax = pair_max + D.pair;
-        // map the chunk's samples to sorted triangle positions: the samples
-        // run in leaf order, so the chunk covers a contiguous position range
-        // starting at the last position whose first sample is <= s0
-        if (threadIdx.x == 0) {
-            int a = 0, b = S.nt;
-            while (b - a > 1) { int m = (a + b) >> 1; if ((int)(PS.keys[m] >> 32) <= s0) a = m; else b = m; }
-            s_a0 = a;
-        }
-        __syncthreads();
-        for (int i = s_a0 + threadIdx.x; i < S.nt; i += HD_NT) {
-            const int f = (int)(PS.keys[i] >> 32);
-            if (f >= s0 + n_chunk) break;            // first samples grow with i
-            const int g = i + 1 < S.nt ? (int)(PS.keys[i + 1] >> 32) : D.n_samples;
-            for (int x = max(f, s0); x < min(g, s0 + n_chunk); x++) s_pos[x - s0] = i;
-        }
-        __syncthreads();
-        bool has = false;
-        float3 q = make_float3(0.f, 0.f, 0.f);
-        float best = 0.f, stop = 0.f;
-        int node = 1, sp = 0;
-        int bl = -1, last_leaf = -1;                 // leaf of the current / previous best triangle
-        // min distance from q to the triangles of leaf l
-        auto leaf_d2 = [&](int l) {
-            float d = 3.4e38f;
-            const int base = l * HD_LEAF;
-            #pragma unroll
-            for (int jj = 0; jj < HD_LEAF; jj++) {
-                float4 A = __ldg(&PD.tri[3 * (base + jj)]), B = __ldg(&PD.tri[3 * (base + jj) + 1]);
-                float4 C = __ldg(&PD.tri[3 * (base + jj) + 2]);
-                if (A.x < 1e29f)
-                    d = fminf(d, hd_pt_tri_d2(q, make_float3(A.x, A.y, A.z), make_float3(B.x, B.y, B.z),
-                                              make_float3(C.x, C.y, C.z)));
-            }
-            return d;
-        };
-        int   stk_n[HD_STACK];
-        float stk_d[HD_STACK];
-        for (;;) {
-            bool got = false;
-            if (!has) {
-                const int j = atomicAdd(&s_next, 1);
-                if (j < n_chunk) {
-                    got = true;
-                    const int smp = s0 + j;
-                    const unsigned long long kk = PS.keys[s_pos[j]];
-                    const int t = (int)(kk & 0xffffffffull);
-                    const int k = smp - (int)(kk >> 32);
-                    q = hd_sample(S.v, S.t[3 * t], S.t[3 * t + 1], S.t[3 * t + 2], t, k);
-                    best = 3.4e38f; stop = *vmax; node = 1; sp = 0; has = true; bl = -1;
-                    // the previous sample's nearest leaf first: its distance
-                    // bounds this one's, and usually settles it at once
-                    if (last_leaf >= 0 && PD.P > 1) {
-                        best = leaf_d2(last_leaf); bl = last_leaf;
-                        if (best <= stop) has = false;
-                    }
-                }
-            }
-            // every lane votes once per iteration; the vote is empty only when
-            // every idle lane failed to take a sample: the chunk is done
-            if (!__any_sync(FULL_MASK, has || got)) break;
-            if (!has) continue;
-            if (PD.P == 1) {                             // one leaf: test it directly
-                for (int jj = 0; jj < HD_LEAF; jj++) {
-                    float4 A = PD.tri[3 * jj], B = PD.tri[3 * jj + 1], C = PD.tri[3 * jj + 2];
-                    if (A.x >= 1e29f) break;
-                    best = fminf(best, hd_pt_tri_d2(q, make_float3(A.x, A.y, A.z), make_float3(B.x, B.y, B.z),
-                                                    make_float3(C.x, C.y, C.z)));
-                }
-                if (best > stop) atomic_max_nonneg(pair_max + D.pair, best);
-                has = false;
-                continue;
-            }
-            bool pop = false;
-            if (node >= PD.P) {                          // leaf step
-                const float d = leaf_d2(node - PD.P);
-                if (d < best) { best = d; bl = node - PD.P; }
-                stop = fmaxf(stop, *vmax);
-                if (best <= stop) { has = false; last_leaf = bl; continue; }  // cannot raise the maximum
-                pop = true;
-            } else {                                     // internal step
-                float4 llo = __ldg(&PD.node[4 * node]), lhi = __ldg(&PD.node[4 * node + 1]);
-                float4 rlo = __ldg(&PD.node[4 * node + 2]), rhi = __ldg(&PD.node[4 * node + 3]);
-                float dl = hd_box_d2(q, llo, lhi), dr = hd_box_d2(q, rlo, rhi);
-                bool vl = dl < best && llo.x <= lhi.x, vr = dr < best && rlo.x <= rhi.x;
-                if (vl && vr) {
-                    int nn = dl <= dr ? 2 * node : 2 * node + 1;
-                    int ff = dl <= dr ? 2 * node + 1 : 2 * node;
-                    if (sp < HD_STACK) { stk_n[sp] = ff; stk_d[sp] = fmaxf(dl, dr); sp++; }
-                    node = nn;
-                } else if (vl) node = 2 * node;
-                else if (vr) node = 2 * node + 1;
-                else pop = true;
-            }
-            if (pop) {
-                bool found = false;
-                while (sp > 0) {
-                    sp--;
-                    if (stk_d[sp] < best) { node = stk_n[sp]; found = true; break; }
-                }
-                if (!found) {                            // search complete: best is the nearest distance
-                    if (best > stop) atomic_max_nonneg(pair_max + D.pair, best);
-                    has = false;
-                    last_leaf = bl;
-                }
-            }
-        }
-        __syncthreads();                             // chunk done before s_chunk / s_next change
-    }
+    hd_query_body(surfs, preps, dirs, n_dirs, total_chunks, counter, pair_max);
 }
 
 __global__ void k_hd_sqrt(const float* pair_max, int n, float* out, int stride_floats)

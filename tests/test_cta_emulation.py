@@ -166,3 +166,43 @@ def test_hull_overflow_paths_emulated(emu_hull_small_lists, tmp_path, oracle):
         assert err == 0
         np.testing.assert_array_equal(hv, c[vi])
         np.testing.assert_array_equal(ht, tri)
+
+
+@pytest.fixture(scope="module")
+def emu_hd(tmp_path_factory):
+    if shutil.which("g++") is None:
+        pytest.skip("g++ not available")
+    out = str(tmp_path_factory.mktemp("emuhd") / "emu_hd")
+    r = subprocess.run(["g++", "-std=c++20", "-O2", "-pthread", "-ffp-contract=off", "-I", EMU,
+                        os.path.join(EMU, "emu_hd.cpp"), "-o", out], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-2000:]
+    return out
+
+
+def test_hausdorff_query_emulated(emu_hd, tmp_path, oracle):
+    """The Hausdorff prep and query (cuacd_b200/csrc/hausdorff.cuh) run
+    on the CPU: every barrier and warp vote is reached by the whole CTA /
+    warp from one site (the query's warps vote inside loops whose lanes
+    search different BVH paths; a lane that skipped a vote would hang the
+    warp on the GPU), and the distance equals the oracle's within 1e-5.
+    Cases: a sphere against its hull, nested boxes, and a tetrahedron
+    (a one-leaf BVH) against an icosphere, both directions each."""
+    from cuacd_b200 import workloads as W
+    v, t = W.hausdorff_sphere(level=3)
+    hvi, htri, _ = oracle.hull(v)
+    tet = (np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [0, 0, 1]], np.float32),
+           np.array([[0, 2, 1], [0, 1, 3], [0, 3, 2], [1, 2, 3]], np.int32))
+    cases = [((v[hvi], htri), (v, t)), (box_mesh([-1] * 3, [1] * 3), box_mesh([-.5] * 3, [.5] * 3)),
+             (tet, W.icosphere(1))]
+    for k, (a, b) in enumerate(cases):
+        path = str(tmp_path / f"hd{k}.bin")
+        with open(path, "wb") as f:
+            np.array([len(a[0]), len(a[1]), len(b[0]), len(b[1]), 1000, 0], np.int32).tofile(f)
+            np.array([2000.0], np.float32).tofile(f)
+            for x in (a[0], a[1], b[0], b[1]):
+                np.ascontiguousarray(x, np.float32 if x.dtype.kind == "f" else np.int32).tofile(f)
+        r = subprocess.run([emu_hd, path], capture_output=True, text=True, timeout=600)
+        assert r.returncode == 0 and "[emu]" not in r.stderr, r.stderr[-2000:]
+        d = float(r.stdout.split()[0])
+        o = oracle.hausdorff(a[0], a[1], b[0], b[1], threads=8)
+        assert abs(d - o) < 1e-5, (k, d, o)
