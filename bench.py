@@ -772,6 +772,335 @@ def _stage_ms(lib, ctx, step, flush):
     return np.median(np.array(out), axis=0).tolist()
 
 
+# ---------------------------------------------------------------------------
+# Side-by-side legs against the reference's own GPU build (oracle/_ref, built
+# from the reference's sources by oracle/Makefile.ref): `python bench.py
+# --compare NAME --out OUT.json`.  Each loads the reference's CPython
+# extension the way its Python wrapper does, times its public calls and this
+# library's on the same seeded inputs, and writes one JSON file.  They are
+# measurements for the profiles, not part of the timed benchmark line.
+# ---------------------------------------------------------------------------
+
+SEARCH_KW = dict(max_iters=100, width=30, width2=5, threshold=0.05, depth=2, quick_depth=0, max_n_cutting=16)
+
+
+def _ref_module():
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    import make_ref_gpu as MR
+    return MR
+
+
+def compare_search(out_path, full=False):
+    """Whole lookahead searches: the reference (cuacd/__init__.py:367-454:
+    scipy hull of the input with outward winding, then
+    `_gpu.lookahead_decompose`) beside this library's exact and pruned
+    searches, on the six ridged spheres (32 concave edges) and the config-4
+    sample (or, with --full, all 512 meshes; 16 concave edges).  Per mesh:
+    triangles, parts, seconds, largest part rv cost; one untimed pass over
+    the six spheres first in every mode."""
+    MR = _ref_module()
+    W = workloads()
+    S = {"search": (search_meshes(), 32)}
+    if full:
+        S["config4_full"] = (W.batch_meshes(512, 500, 200_000, seed=3), 16)
+    else:
+        S["config4"] = (config4_sample(), 16)
+    kw = SEARCH_KW
+
+    def ref_search(g, v, t, n_edges):
+        import scipy.spatial
+        v = np.ascontiguousarray(v, np.float32)
+        t = np.ascontiguousarray(t, np.int32)
+        t0 = time.perf_counter()
+        h = scipy.spatial.ConvexHull(v)
+        hv = np.ascontiguousarray(h.points, np.float32)
+        ht = np.ascontiguousarray(h.simplices, np.int32)
+        cen = hv.mean(0)
+        nrm = np.cross(hv[ht[:, 1]] - hv[ht[:, 0]], hv[ht[:, 2]] - hv[ht[:, 0]])
+        inward = (nrm * (hv[ht[:, 0]] - cen)).sum(1) < 0
+        ht[inward] = ht[inward][:, [0, 2, 1]]
+        raw = g.lookahead_decompose(v.ctypes.data, len(v), t.ctypes.data, len(t), hv.ctypes.data, len(hv),
+                                    ht.ctypes.data, len(ht), kw["max_iters"], kw["width"], kw["width2"],
+                                    kw["threshold"], kw["depth"], kw["quick_depth"], kw["max_n_cutting"], 0, 0,
+                                    n_concave_edges=n_edges)
+        dt = time.perf_counter() - t0
+        parts = [(np.frombuffer(vb, np.float32).reshape(nv, 3), np.frombuffer(tb, np.int32).reshape(nt, 3),
+                  np.frombuffer(hvb, np.float32).reshape(hnv, 3), np.frombuffer(htb, np.int32).reshape(hnt, 3))
+                 for vb, tb, nv, nt, hvb, htb, hnv, hnt, _, _ in raw]
+        return parts, dt
+
+    def row(t, parts, dt):
+        return {"tris": int(len(t)), "parts": len(parts), "s": dt, "max_rv": part_cost_max(parts)}
+
+    rec = {"settings": {**kw, "n_concave_edges": {k: e for k, (_, e) in S.items()}}}
+    g = MR.load_ref()
+    for v, t in S["search"][0]:
+        ref_search(g, v, t, 32)
+    for name, (meshes, ne) in S.items():
+        rows = []
+        for v, t in meshes:
+            try:
+                parts, dt = ref_search(g, v, t, ne)
+                rows.append(row(t, parts, dt))
+            except Exception as e:                        # a failed search is recorded
+                rows.append({"tris": int(len(t)), "parts": 0, "s": 0.0, "max_rv": 0.0, "error": str(e)[:200]})
+        rec[f"reference_{name}"] = rows
+        print("reference", name, sum(r["s"] for r in rows), "s", sum(r["parts"] for r in rows), "parts", flush=True)
+    g.destroy()
+    import cuacd_b200
+    from cuacd_b200 import scorer as SC
+    with cuacd_b200.Context(0) as ctx, SC.Scorer.load(ctx, SC.RV_WEIGHTS_PATH) as rv:
+        for mname, extra in (("exact", {}), ("pruned", {"scorer": rv, "top_k": SEARCH_TOP_K, "beam": SEARCH_BEAM})):
+            for v, t in S["search"][0]:
+                ctx.lookahead_decompose(v, t, **kw, n_concave_edges=32, **extra)
+            for name, (meshes, ne) in S.items():
+                rows = []
+                for v, t in meshes:
+                    t0 = time.perf_counter()
+                    try:
+                        parts = ctx.lookahead_decompose(v, t, **kw, n_concave_edges=ne, **extra)
+                        rows.append(row(t, parts, time.perf_counter() - t0))
+                    except RuntimeError as e:
+                        rows.append({"tris": int(len(t)), "parts": 0, "s": 0.0, "max_rv": 0.0, "error": str(e)[:200]})
+                rec[f"{mname}_{name}"] = rows
+                print(mname, name, sum(r["s"] for r in rows), "s", sum(r["parts"] for r in rows), "parts", flush=True)
+    with open(out_path, "w") as f:
+        json.dump(rec, f)
+
+
+def compare_hull_sweep(out_path):
+    """Batched hull volumes over the shapes of the reference's arena sweep
+    (docs/arena_sweep.md: 10000x20, 1000x200, 100x2000, 10x20000 points;
+    sphere shell, cube interior, gaussian; seeded).  Reference: its
+    `Context.batch_hull_volume` steps (cuacd/__init__.py:185-233: pack,
+    `_gpu.hull_dandc` with caps n / 2n-4, FP32 volumes on the host), the
+    call alone and the whole method; this library: `batch_hull_volume`.
+    Wall clock, median of 5 after a warm-up; hull index sets compared."""
+    import statistics
+    MR = _ref_module()
+    shapes = [(10000, 20), (1000, 200), (100, 2000), (10, 20000)]
+    dists = ["sphere_shell", "cube_interior", "gaussian"]
+
+    def clouds(n, k, dist, seed):
+        rng = np.random.default_rng(seed)
+        if dist == "gaussian":
+            p = rng.normal(0, 0.5, (n, k, 3))
+        elif dist == "cube_interior":
+            p = rng.uniform(-1, 1, (n, k, 3))
+        else:
+            d = rng.normal(size=(n, k, 3))
+            p = d / np.linalg.norm(d, axis=2, keepdims=True) * rng.uniform(0.95, 1.0, (n, k, 1))
+        p = p.astype(np.float32)
+        return [p[i] for i in range(n)]
+
+    def ref_call(g, cl):
+        n = len(cl)
+        packed = np.ascontiguousarray(np.concatenate(cl), np.float32)
+        off = np.zeros(n + 1, np.int32)
+        off[1:] = np.cumsum([len(c) for c in cl])
+        mhv = max(len(c) for c in cl)
+        mht = max(max(2 * len(c) - 4 for c in cl), 4)
+        ov = np.empty(n * mhv * 3, np.float32)
+        ot = np.empty(n * mht * 3, np.int32)
+        onv, ont, err = (np.empty(n, np.int32) for _ in range(3))
+        t0 = time.perf_counter()
+        g.hull_dandc(packed.ctypes.data, len(packed), off.ctypes.data, n, mhv, mhv, mht, ov.ctypes.data,
+                     ot.ctypes.data, onv.ctypes.data, ont.ctypes.data, err.ctypes.data)
+        t_call = time.perf_counter() - t0
+        vols = np.empty(n, np.float32)
+        meshes = []
+        for i in range(n):
+            hv = ov[i * mhv * 3:(i * mhv + onv[i]) * 3].reshape(-1, 3)
+            ht = ot[i * mht * 3:(i * mht + ont[i]) * 3].reshape(-1, 3)
+            if len(ht):
+                a, b, c = hv[ht[:, 0]], hv[ht[:, 1]], hv[ht[:, 2]]
+                vols[i] = abs(np.einsum("ij,ij->i", a, np.cross(b, c)).sum() / 6.0)
+            else:
+                vols[i] = 0.0
+            meshes.append(hv)
+        return vols, err.copy(), t_call, meshes
+
+    cases = [(n, k, d, 100 + 10 * si + di) for si, (n, k) in enumerate(shapes) for di, d in enumerate(dists)]
+    data = {c: clouds(*c) for c in cases}
+    rows = {c: {"clouds": c[0], "points": c[1], "dist": c[2]} for c in cases}
+    g = MR.load_ref()
+    for c in cases:
+        cl = data[c]
+        ref_call(g, cl)
+        calls, whole = [], []
+        for _ in range(5):
+            t0 = time.perf_counter()
+            vols, err, t_call, meshes = ref_call(g, cl)
+            whole.append(time.perf_counter() - t0)
+            calls.append(t_call)
+        rows[c].update(ref_call_ms=1e3 * statistics.median(calls), ref_method_ms=1e3 * statistics.median(whole),
+                       ref_errors=int((err != 0).sum()))
+        rows[c]["_sets"] = [set(MR.index_set(x, m).tolist()) for x, m in zip(cl, meshes)]
+        rows[c]["_vol"] = vols
+        print("reference", c[:3], round(rows[c]["ref_call_ms"], 2), "ms", flush=True)
+    g.destroy()
+    import cuacd_b200
+    with cuacd_b200.Context(0) as ctx:
+        for c in cases:
+            cl = data[c]
+            ctx.batch_hull_volume(cl)
+            ts = []
+            for _ in range(5):
+                t0 = time.perf_counter()
+                vols, err = ctx.batch_hull_volume(cl)
+                ts.append(time.perf_counter() - t0)
+            r = rows[c]
+            r["ours_ms"] = 1e3 * statistics.median(ts)
+            r["ours_errors"] = int((err != 0).sum())
+            ours = [set(MR.index_set(x, m[0]).tolist()) for x, m in zip(cl, ctx.batch_hull_dandc_mesh(cl))]
+            r["sets_differing"] = int(sum(a != b for a, b in zip(ours, r.pop("_sets"))))
+            rv = r.pop("_vol")
+            r["max_rel_vol_diff"] = float(np.max(np.abs(vols - rv) / np.maximum(np.abs(rv), 1e-30)))
+            r["speedup_vs_ref_method"] = r["ref_method_ms"] / r["ours_ms"]
+            print("ours", c[:3], round(r["ours_ms"], 2), "ms, sets differing", r["sets_differing"], flush=True)
+    with open(out_path, "w") as f:
+        json.dump(list(rows.values()), f)
+
+
+def compare_hausdorff(out_path):
+    """The reference's Hausdorff benchmark (bench/hausdorff_bench.cu, built
+    into oracle/_ref/hausdorff_bench; GPU rows, `hausdorff_block`, one block
+    per pair: the bunny and the 49160 mesh against their hulls, batches 1 and
+    100, CUDA events, 2 warm-up and 5 timed launches) beside
+    `cuacd_hausdorff_batch_device` on the same meshes (extracted from the
+    benchmark's data header), batches and sampling, meshes resident, CUDA
+    events on the call's stream, 2 warm-up and 5 timed calls (mean)."""
+    import statistics
+    import torch
+    r = subprocess.run([os.path.join(REF_DIR, "hausdorff_bench")], capture_output=True, text=True, timeout=600)
+    if r.returncode != 0:
+        raise RuntimeError(r.stderr[-2000:])
+    lines = [l.split(",") for l in r.stdout.splitlines() if l.strip()]
+    ref = [x for x in (dict(zip(lines[0], l)) for l in lines[1:]) if x["algorithm"] == "hausdorff_block"]
+    import cuacd_b200
+    fn = cuacd_b200._fn("cuacd_hausdorff_batch_device")
+    data = np.load(os.path.join(REF_DIR, "hausdorff_bench_data.npz"))
+    sets = {"bunny": "BUNNY", "49160": "STL"}
+    P = ctypes.c_void_p
+    rows = []
+    with cuacd_b200.Context(0) as ctx:
+        for x in ref:
+            k, batch = sets[x["dataset"]], int(x["batch"])
+            mv, mt, hv, ht = (data[f"{k}_{n}"] for n in ("verts", "tris", "hull_verts", "hull_tris"))
+            dev = [torch.from_numpy(np.ascontiguousarray(np.tile(a, (batch, 1)), dt)).cuda()
+                   for a, dt in ((mv, np.float32), (mt, np.int32), (hv, np.float32), (ht, np.int32))]
+            offs = [np.arange(batch + 1, dtype=np.int32) * len(a) for a in (mv, mt, hv, ht)]
+            out = torch.zeros(batch, dtype=torch.float32, device="cuda")
+            stream = torch.cuda.Stream()
+
+            def call():
+                rc = fn(ctx.handle, batch, P(dev[0].data_ptr()), P(offs[0].ctypes.data), P(dev[1].data_ptr()),
+                        P(offs[1].ctypes.data), P(dev[2].data_ptr()), P(offs[2].ctypes.data), P(dev[3].data_ptr()),
+                        P(offs[3].ctypes.data), 2000.0, 1000, 0, P(out.data_ptr()), P(stream.cuda_stream))
+                if rc:
+                    raise RuntimeError(f"cuacd error {rc}")
+
+            for _ in range(2):
+                call()
+            ms = []
+            for _ in range(5):
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                call()
+                b.record(stream)
+                stream.synchronize()
+                ms.append(a.elapsed_time(b))
+            d = out.cpu().numpy()
+            m = statistics.mean(ms)
+            rows.append({"dataset": x["dataset"], "batch": batch, "ref_ms": float(x["mean_ms"]),
+                         "ref_std_ms": float(x["std_ms"]), "ref_dist": float(x["mean_dist"]), "ours_ms": m,
+                         "ours_std_ms": statistics.pstdev(ms), "ours_dist": float(d.mean()),
+                         "ours_dist_spread": float(d.max() - d.min()), "speedup": float(x["mean_ms"]) / m})
+            print(rows[-1], flush=True)
+    with open(out_path, "w") as f:
+        json.dump(rows, f)
+
+
+def compare_heap(out_path):
+    """Device allocation throughput: the reference's heap benchmark
+    (bench/malloc_test_bench.cu, built into oracle/_ref/malloc_test_bench;
+    its own heap and CUDA's device malloc/free) at 256 alloc-free iterations
+    per block instead of 1,024, so that this library's arena, which frees by
+    whole-arena reset, holds a run (1,024 blocks x 256 x 62 KB mean = 16 GB);
+    beside `cuacd_arena_bench` on the same workload (thread 0 of each block
+    drawing log-uniform sizes in [4 KiB, 256 KiB] into 16 slots), the arena
+    reset before each run.  CUDA events, 2 warm-up and 5 timed runs."""
+    iters, slots, smin, smax = 256, 16, 4096, 262144
+    r = subprocess.run([os.path.join(REF_DIR, "malloc_test_bench"), "--iters", str(iters), "--slots", str(slots),
+                        "--size-min", str(smin), "--size-max", str(smax), "--impl", "both"],
+                       capture_output=True, text=True, timeout=900)
+    if r.returncode != 0:
+        raise RuntimeError(r.stderr[-2000:])
+    lines = [l.split(",") for l in r.stdout.splitlines() if l.strip()]
+    ref = [dict(zip(lines[0], l)) for l in lines[1:]]
+    import cuacd_b200
+    fn = cuacd_b200._lib.cuacd_arena_bench
+    fn.restype = ctypes.c_int
+    fn.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_uint, ctypes.c_uint,
+                   ctypes.c_ulonglong, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_float),
+                   ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_int)]
+    ours = []
+    with cuacd_b200.Context(0) as ctx:
+        for grid in (1, 4, 16, 64, 256, 1024):
+            m, s, fl = ctypes.c_float(), ctypes.c_float(), ctypes.c_int()
+            rc = fn(ctx.handle, grid, iters, slots, smin, smax, 20 << 30, 2, 5, ctypes.byref(m), ctypes.byref(s),
+                    ctypes.byref(fl))
+            if rc:
+                raise RuntimeError(f"cuacd error {rc}")
+            ours.append({"grid": grid, "mean_ms": m.value, "std_ms": s.value, "failed_allocs": fl.value,
+                         "mops": grid * iters / (m.value * 1e-3) / 1e6})
+            print(ours[-1], flush=True)
+    with open(out_path, "w") as f:
+        json.dump({"iters": iters, "slots": slots, "size_min": smin, "size_max": smax, "reference": ref,
+                   "reference_log": r.stderr[-1000:], "ours": ours}, f)
+
+
+def compare_audit(out_path):
+    """Mesh audit: the reference's `_gpu.mesh_audit` (one 256-thread block
+    per mesh) beside `Context.check_mesh`, on the 40,960- and 327,680-
+    triangle spheres; wall clock of the public call, median of 5 after a
+    warm-up."""
+    import statistics
+    MR = _ref_module()
+    W = workloads()
+    big = [m for m in config4_sample() if len(m[1]) == 327680][0]
+    ms = [(n, np.ascontiguousarray(v, np.float32), np.ascontiguousarray(t, np.int32))
+          for n, v, t in (("40,960-tri sphere", *W.candidate_mesh()), ("327,680-tri sphere", *big))]
+
+    def timed(fn):
+        fn()
+        ts = []
+        for _ in range(5):
+            t0 = time.perf_counter()
+            r = fn()
+            ts.append(time.perf_counter() - t0)
+        return 1e3 * statistics.median(ts), r
+
+    rows = []
+    g = MR.load_ref()
+    for n, v, t in ms:
+        ref_ms, ref_f = timed(lambda: g.mesh_audit(v.ctypes.data, len(v), t.ctypes.data, len(t)))
+        rows.append({"mesh": n, "tris": int(len(t)), "ref_ms": ref_ms, "ref_flags": int(ref_f)})
+    g.destroy()
+    import cuacd_b200
+    with cuacd_b200.Context(0) as ctx:
+        for row, (n, v, t) in zip(rows, ms):
+            ours_ms, r = timed(lambda: ctx.check_mesh(v, t))
+            row.update({"ours_ms": ours_ms, "ours_flags": r["flags"], "speedup": row["ref_ms"] / ours_ms})
+            print(row, flush=True)
+    with open(out_path, "w") as f:
+        json.dump(rows, f)
+
+
+COMPARE = {"search": compare_search, "hull_sweep": compare_hull_sweep, "hausdorff": compare_hausdorff,
+           "heap": compare_heap, "audit": compare_audit}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -783,10 +1112,22 @@ def main():
     ap.add_argument("--no-reference-gpu", action="store_true",
                     help="reference arm: skip the reference's own GPU legs")
     ap.add_argument("--ref-gpu-child", action="store_true", help=argparse.SUPPRESS)
+    ap.add_argument("--compare", choices=sorted(COMPARE),
+                    help="side-by-side leg against the reference's own GPU build (writes --out)")
+    ap.add_argument("--out", help="JSON output of --compare")
+    ap.add_argument("--full", action="store_true", help="--compare search: all 512 config-4 meshes")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.ref_gpu_child:
         ref_gpu_child(args)
+        return
+    if args.compare:
+        if not args.out:
+            ap.error("--compare needs --out")
+        if args.compare == "search":
+            compare_search(args.out, full=args.full)
+        else:
+            COMPARE[args.compare](args.out)
         return
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
