@@ -199,6 +199,8 @@ k_cand_features(const float* __restrict__ v, int nv, const float4* __restrict__ 
 #define GM_BN 128
 #define GM_BK 64
 #define GM_NT 128
+#define GM_STAGES 2
+#define GM_DSMEM ((size_t)GM_STAGES * (GM_BM + GM_BN) * GM_BK * 2)   // 64 KB of slabs
 
 struct GemmArgs {
     const __nv_bfloat16* A; long long ar, ac;
@@ -272,14 +274,19 @@ static __host__ __device__ __forceinline__ int stage_mode(long long rs, long lon
 }
 
 // Stage rows [r0, r0 + 128) x K columns [k0, k0 + 64) of X (R x K, zero
-// outside) into a slab (all GM_NT threads).
+// outside) into a slab (all GM_NT threads).  A slab is 1,024 16-byte chunks
+// (8 elements along the contiguous dimension); the eight lanes of each
+// quarter warp write the eight chunks of one 128-byte core matrix (no bank
+// conflicts), and the four quarters of a warp read 64 contiguous bytes of
+// each of eight rows (mode 1) or of each of eight k (mode 2).
 static __device__ __forceinline__ void stage_slab(__nv_bfloat16* slab, const __nv_bfloat16* __restrict__ X, long long rs,
                                                   long long ks, int R, int K, int r0, int k0, int mode, int tid)
 {
     const __nv_bfloat16 zero = __float2bfloat16(0.f);
     if (mode == 1) {                                       // 8 consecutive k of one row per load
         for (int e = tid; e < GM_BM * (GM_BK / 8); e += GM_NT) {
-            const int r = e / (GM_BK / 8), c = 8 * (e % (GM_BK / 8));
+            // lane bits: r % 8, then k-group % 4; then k-group / 4, row block
+            const int r = 8 * (e >> 6) + (e & 7), c = 8 * (4 * ((e >> 5) & 1) + ((e >> 3) & 3));
             const int gr = r0 + r, gk = k0 + c;
             uint4 v;
             if (gr < R && gk + 7 < K) v = *reinterpret_cast<const uint4*>(X + gr * rs + gk);
@@ -292,7 +299,8 @@ static __device__ __forceinline__ void stage_slab(__nv_bfloat16* slab, const __n
         }
     } else if (mode == 2) {                                // 8 consecutive r of one k per load
         for (int e = tid; e < (GM_BM / 8) * GM_BK; e += GM_NT) {
-            const int r = 8 * (e % (GM_BM / 8)), k = e / (GM_BM / 8);
+            // lane bits: k % 8, then row block % 4; then k-group, row block / 4
+            const int k = 8 * ((e >> 5) & 7) + (e & 7), r = 8 * (4 * (e >> 8) + ((e >> 3) & 3));
             const int gr = r0 + r, gk = k0 + k;
             uint4 v;
             if (gk < K && gr + 7 < R) v = *reinterpret_cast<const uint4*>(X + gr + gk * ks);
@@ -312,17 +320,51 @@ static __device__ __forceinline__ void stage_slab(__nv_bfloat16* slab, const __n
     }
 }
 
+// One 16-byte global -> shared copy (cp.async, L2 only); src_bytes < 16
+// zero-fills the rest (0: all zero, src not read).
+static __device__ __forceinline__ void cp16(void* dst, const void* src, int src_bytes)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;"
+                 :: "r"(smem_addr(dst)), "l"(src), "r"(src_bytes) : "memory");
+}
+
+// stage_slab with asynchronous copies (modes 1 and 2: the same chunks in
+// the same places; mode 0 stores element by element).  The caller commits
+// the group and waits for it before the slab is read.
+static __device__ __forceinline__ void stage_slab_async(__nv_bfloat16* slab, const __nv_bfloat16* __restrict__ X,
+                                                        long long rs, long long ks, int R, int K, int r0, int k0,
+                                                        int mode, int tid)
+{
+    if (mode == 1) {
+        for (int e = tid; e < GM_BM * (GM_BK / 8); e += GM_NT) {
+            const int r = 8 * (e >> 6) + (e & 7), c = 8 * (4 * ((e >> 5) & 1) + ((e >> 3) & 3));
+            const int gr = r0 + r, gk = k0 + c;
+            const int n = (gr < R && gk < K) ? 2 * min(8, K - gk) : 0;
+            cp16(slab + slab_index(r, c), n ? (const void*)(X + gr * rs + gk) : (const void*)X, n);
+        }
+    } else if (mode == 2) {
+        for (int e = tid; e < (GM_BM / 8) * GM_BK; e += GM_NT) {
+            const int k = 8 * ((e >> 5) & 7) + (e & 7), r = 8 * (4 * (e >> 8) + ((e >> 3) & 3));
+            const int gr = r0 + r, gk = k0 + k;
+            const int n = (gk < K && gr < R) ? 2 * min(8, R - gr) : 0;
+            cp16(slab + slab_index_mn(r, k), n ? (const void*)(X + gr + gk * ks) : (const void*)X, n);
+        }
+    } else {
+        stage_slab(slab, X, rs, ks, R, K, r0, k0, 0, tid);
+    }
+}
+
 __global__ void __launch_bounds__(GM_NT)
 k_gemm_umma(GemmArgs g)
 {
-    __shared__ __align__(128) __nv_bfloat16 As[GM_BM * GM_BK];
-    __shared__ __align__(128) __nv_bfloat16 Bs[GM_BN * GM_BK];
-    __shared__ __align__(8) unsigned long long s_bar;
+    // GM_STAGES slab pairs (dynamic shared memory); after the last MMA the
+    // epilogue's transpose tiles
+    extern __shared__ __align__(1024) __nv_bfloat16 sm[];
+    __shared__ __align__(8) unsigned long long s_bar[GM_STAGES];
     __shared__ unsigned s_tmem;
     __shared__ int s_fail;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int m0 = blockIdx.y * GM_BM, n0 = blockIdx.x * GM_BN;
-    const unsigned bar = smem_addr(&s_bar);
     if (warp == 0) {                                  // 128 fp32 columns of tensor memory
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
                      :: "r"(smem_addr(&s_tmem)), "r"(GM_BN) : "memory");
@@ -330,7 +372,8 @@ k_gemm_umma(GemmArgs g)
     }
     if (tid == 0) {
         s_fail = 0;
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(bar), "r"(1) : "memory");
+        for (int b = 0; b < GM_STAGES; b++)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_addr(&s_bar[b])), "r"(1) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -340,18 +383,40 @@ k_gemm_umma(GemmArgs g)
     // A(i, k) = A[i*ar + k*ac]; B as an N x K operand: B(j, k) = B[j*bc + k*br]
     const int amode = stage_mode(g.ar, g.ac, g.K), bmode = stage_mode(g.bc, g.br, g.K);
     const unsigned idesc = umma_idesc_bf16(GM_BM, GM_BN, amode == 2, bmode == 2);
-    const unsigned a0 = smem_addr(As), b0 = smem_addr(Bs);
-    unsigned phase = 0;
-    bool issued = false;
-    for (int k0 = 0; k0 < g.K && !s_fail; k0 += GM_BK) {
-        // stage the slabs (zero outside the matrices) with 16-byte loads
-        // along whichever of the operand's dimensions is contiguous
-        stage_slab(As, g.A, g.ar, g.ac, g.M, g.K, m0, k0, amode, tid);
-        stage_slab(Bs, g.B, g.bc, g.br, g.N, g.K, n0, k0, bmode, tid);
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // generic stores -> tensor-core reads
+    const int nk = (g.K + GM_BK - 1) / GM_BK;
+    // slab pair kt goes to stage kt % 2: its copies are issued while the
+    // MMAs of slab kt - 1 run, once those of slab kt - 2 (the stage's last
+    // readers) have completed
+    auto stage = [&](int kt) {
+        __nv_bfloat16* As = sm + (size_t)(kt & 1) * (GM_BM + GM_BN) * GM_BK;
+        stage_slab_async(As, g.A, g.ar, g.ac, g.M, g.K, m0, kt * GM_BK, amode, tid);
+        stage_slab_async(As + GM_BM * GM_BK, g.B, g.bc, g.br, g.N, g.K, n0, kt * GM_BK, bmode, tid);
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    unsigned ph[GM_STAGES] = {0u, 0u};
+    bool pend[GM_STAGES] = {false, false};            // committed MMAs not yet waited for
+    // a wait that gives up waits once more (bounded) for the MMAs in flight
+    auto wait_stage = [&](int b) {
+        const unsigned bar = smem_addr(&s_bar[b]);
+        if (!mbar_wait(bar, ph[b]) && !mbar_wait(bar, ph[b]) && lane == 0) atomicOr(&s_fail, 1);
+        ph[b] ^= 1u; pend[b] = false;
+    };
+    if (nk > 0) stage(0);
+    for (int kt = 0; kt < nk && !s_fail; kt++) {
+        const int b = kt & 1;
+        if (kt + 1 < nk) {
+            if (pend[(kt + 1) & 1]) wait_stage((kt + 1) & 1);
+            stage(kt + 1);
+            asm volatile("cp.async.wait_group 1;" ::: "memory");
+        } else {
+            asm volatile("cp.async.wait_group 0;" ::: "memory");
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // copies -> tensor-core reads
         __syncthreads();
         if (tid == 0) {
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const unsigned a0 = smem_addr(sm + (size_t)b * (GM_BM + GM_BN) * GM_BK);
+            const unsigned b0 = a0 + GM_BM * GM_BK * 2;
             #pragma unroll
             for (int kk = 0; kk < GM_BK / 16; kk++) {
                 // K chunk pair (2kk, 2kk+1): leading offset = one chunk of
@@ -359,27 +424,32 @@ k_gemm_umma(GemmArgs g)
                 const unsigned off = (unsigned)(2 * kk * (GM_BM / 8) * 128);
                 const unsigned long long ad = umma_desc(a0 + off, (GM_BM / 8) * 128, 128);
                 const unsigned long long bd = umma_desc(b0 + off, (GM_BN / 8) * 128, 128);
-                const unsigned acc = (k0 > 0 || kk > 0) ? 1u : 0u;
+                const unsigned acc = (kt > 0 || kk > 0) ? 1u : 0u;
                 asm volatile("{\n .reg .pred p;\n setp.ne.u32 p, %4, 0;\n"
                              " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n"
                              :: "r"(tmem), "l"(ad), "l"(bd), "r"(idesc), "r"(acc) : "memory");
             }
             asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
-                         :: "r"(bar) : "memory");
+                         :: "r"(smem_addr(&s_bar[b])) : "memory");
         }
-        issued = true;
-        // a wait that gives up waits once more (bounded) for the MMAs in
-        // flight before the CTA stops and frees its tensor memory
-        if (!mbar_wait(bar, phase) && !mbar_wait(bar, phase) && lane == 0) atomicOr(&s_fail, 1);
-        phase ^= 1u;
-        __syncthreads();                               // the slabs are free again
+        pend[b] = true;
     }
+    // the last MMAs (and any copies still in flight) before the shared
+    // memory and the accumulator are read or released
+    for (int b = 0; b < GM_STAGES; b++) if (pend[b]) wait_stage(b);
+    asm volatile("cp.async.wait_all;" ::: "memory");
+    const bool issued = nk > 0;
+    __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     if (s_fail) {
         if (tid == 0 && g.err) atomicOr(g.err, KERR_TIMEOUT);
     } else if (issued) {
-        // epilogue: warp w owns accumulator lanes (rows) 32w .. 32w + 31
-        const int r = m0 + 32 * warp + lane;
+        // epilogue: warp w owns accumulator lanes (rows) 32w .. 32w + 31.
+        // Each 32 x 32 block goes through a padded shared tile so that the
+        // lanes then take consecutive columns of one row: coalesced loads of
+        // the mask and C, and coalesced stores.
+        float* const tile = reinterpret_cast<float*>(sm) + warp * (32 * 33);
+        const int c = n0 + lane;
         for (int c0 = 0; c0 < GM_BN; c0 += 32) {
             unsigned v[32];
             const unsigned taddr = tmem + ((unsigned)(32 * warp) << 16) + (unsigned)c0;
@@ -393,20 +463,24 @@ k_gemm_umma(GemmArgs g)
                            "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
                          : "r"(taddr));
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-            if (r >= g.M) continue;
             #pragma unroll
-            for (int q = 0; q < 32; q++) {
-                const int c = n0 + c0 + q;
-                if (c >= g.N) break;
-                float x = g.alpha * __uint_as_float(v[q]);
-                const size_t o = (size_t)r * g.ldc + c;
+            for (int q = 0; q < 32; q++) tile[lane * 33 + q] = __uint_as_float(v[q]);
+            __syncwarp();
+            const int cc = c + c0;
+            const float bias = (g.bias && cc < g.N) ? g.bias[cc] : 0.f;
+            for (int rr = 0; rr < 32; rr++) {
+                const int r = m0 + 32 * warp + rr;
+                if (r >= g.M || cc >= g.N) continue;
+                float x = g.alpha * tile[rr * 33 + lane];
+                const size_t o = (size_t)r * g.ldc + cc;
                 if (g.accumulate && g.Cf) x += g.Cf[o];
-                if (g.bias) x += g.bias[c];
-                if (g.mask && !(__bfloat162float(g.mask[(size_t)r * g.ldm + c]) > 0.f)) x = 0.f;
+                x += bias;
+                if (g.mask && !(__bfloat162float(g.mask[(size_t)r * g.ldm + cc]) > 0.f)) x = 0.f;
                 if (g.relu) x = fmaxf(x, 0.f);
                 if (g.Cf) g.Cf[o] = x;
                 if (g.Cb) g.Cb[o] = __float2bfloat16(x);
             }
+            __syncwarp();                                  // the tile is rewritten by the next block
         }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -417,9 +491,16 @@ k_gemm_umma(GemmArgs g)
 
 static void gemm(GemmArgs g, int* err, cudaStream_t s)
 {
+    static bool attr_set[64] = {false};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 0 && dev < 64 && !attr_set[dev]) {
+        cudaFuncSetAttribute(k_gemm_umma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GM_DSMEM);
+        attr_set[dev] = true;
+    }
     g.err = err;
     dim3 grid((g.N + GM_BN - 1) / GM_BN, (g.M + GM_BM - 1) / GM_BM);
-    if (g.M > 0 && g.N > 0) k_gemm_umma<<<grid, GM_NT, 0, s>>>(g);
+    if (g.M > 0 && g.N > 0) k_gemm_umma<<<grid, GM_NT, GM_DSMEM, s>>>(g);
 }
 
 __global__ void k_f32_to_bf16(const float* in, __nv_bfloat16* out, size_t n)
