@@ -12,13 +12,16 @@ value of depends on the batch and the device:
   time on a small one.
 
 They are tuned per size class of a batch's largest cloud (0: < 4,096
-points, 1: < 65,536, 2: larger) on a representative batch of that class:
-the config-1 clouds (256 x 1,000 uniform points), the fragments that the 30
-candidate planes cut from the config-3 sphere (5,000-20,000 points each),
-and two 163,842-point clouds (a level-7 icosphere, all of whose points are
-on its hull, and the largest displaced sphere of config 4).  Each shape is
-timed with CUDA events on device-resident inputs (median of `reps` calls
-after a warm-up call); the fastest is applied through
+points, 1: < 65,536, 2: larger) on representative batches of that class:
+the config-1 clouds (256 x 1,000 uniform points); the fragments that the 30
+candidate planes cut from the config-3 sphere (5,000-20,000 points each)
+and, alone, the vertices of a 81,920-triangle displaced sphere of config 4
+(40,962 points, the input hull a lookahead search starts from); and two
+163,842-point clouds (a level-7 icosphere, all of whose points are on its
+hull, and the largest displaced sphere of config 4).  Each shape is timed
+with CUDA events on device-resident inputs (median of `reps` calls after a
+warm-up call, summed over the class's batches); the fastest is applied
+through
 cuacd_hull_set_tuning and, with --write, stored per device name in
 tuning.json beside this file, which Context applies when it opens a device
 of that name.  The results are the same for every shape (the hull output
@@ -78,9 +81,10 @@ def apply_stored(ctx, path=TUNING_PATH):
 
 
 def workloads(ctx):
-    """Representative batch of each size class (see the module docstring)."""
+    """Representative batches of each size class (see the module
+    docstring): {class: [batch, ...]}, a batch being a list of clouds."""
     from . import workloads as W
-    out = {0: W.hull_clouds(256, 1000, 0)}
+    out = {0: [W.hull_clouds(256, 1000, 0)]}
     v, t = W.candidate_mesh()
     conc, axis, valid = ctx.candidate_planes(v, t, 16, 0.005, 3.49, 3, 0.0125)
     planes = np.concatenate([conc[:27], axis[valid]]).astype(np.float32)
@@ -89,11 +93,12 @@ def workloads(ctx):
         pv, pt, nv, nt = ctx.plane_cut(v, t, p)
         if len(pt) and len(nt):
             frags += [pv, nv]
-    out[1] = frags
+    sample = W.batch_meshes(512, 500, 200_000, seed=3, select={i for i in range(512) if i % 16 in (0, 5)})
+    lone = next(m[0] for m in sample if len(m[1]) == 81920)
+    out[1] = [frags, [lone]]
     iv, _ = W.icosphere(7)
-    big = max(W.batch_meshes(512, 500, 200_000, seed=3, select={i for i in range(0, 512, 16)}),
-              key=lambda m: len(m[0]))
-    out[2] = [iv.astype(np.float32), big[0]]
+    big = max(sample, key=lambda m: len(m[0]))
+    out[2] = [[iv.astype(np.float32), big[0]]]
     return out
 
 
@@ -149,19 +154,24 @@ def tune(ctx, reps=5, pts_per_cta=PTS_PER_CTA, seed_min_n=SEED_MIN_N, batches=No
     batches = batches if batches is not None else workloads(ctx)
     table, times = [], {}
     for cls in CLASSES:
-        b = _Batch(ctx, batches[cls])
+        group = batches[cls]
+        if len(group) and isinstance(group[0], np.ndarray):     # one batch given as its clouds
+            group = [group]
+        bs = [_Batch(ctx, g) for g in group]
         times[cls] = {}
         best = None
-        ref = None
+        refs = [None] * len(bs)
         for ppc in pts_per_cta:
             for seed in seed_min_n[cls]:
                 set_tuning(ctx, cls, ppc, seed)
-                ms = b.time_ms(reps)
-                res = b.result()
-                if ref is None:
-                    ref = res
-                elif not all(np.array_equal(x, y) for x, y in zip(ref, res)):
-                    raise RuntimeError(f"class {cls}: hull results changed with the launch shape {ppc}/{seed}")
+                ms = 0.0
+                for k, b in enumerate(bs):
+                    ms += b.time_ms(reps)
+                    res = b.result()
+                    if refs[k] is None:
+                        refs[k] = res
+                    elif not all(np.array_equal(x, y) for x, y in zip(refs[k], res)):
+                        raise RuntimeError(f"class {cls}: hull results changed with the launch shape {ppc}/{seed}")
                 times[cls][f"{ppc}/{seed}"] = ms
                 if best is None or ms < best[0]:
                     best = (ms, ppc, seed)

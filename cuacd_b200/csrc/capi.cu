@@ -131,12 +131,16 @@ extern "C" unsigned long long cuacd_launch_count(gpu_ctx_t ctx) { return ctx ? c
 // hulls
 // ---------------------------------------------------------------------------
 // Device bytes of one hull batch: jobs, states, results, control words,
-// per-warp wrap lists and per-cloud scratch.
+// per-warp wrap lists and per-cloud scratch.  The public batch calls build
+// every cloud with full-size tables in one round: callers' clouds are often
+// near-convex (an input mesh's vertices), whose hulls outgrow reduced first
+// tables, and the rebuild costs more than the clearing it saves (a lone
+// 10,242-point sphere: 11.3 -> 8.0 ms).
 static size_t hull_batch_need(int n_hulls, int max_pts, int nwc)
 {
     return al256(sizeof(HullJob) * (size_t)n_hulls) + al256(sizeof(HullState) * (size_t)n_hulls)
          + al256(sizeof(HullRes) * (size_t)n_hulls) + al256(64) + al256(hull_wrap_buf_bytes(nwc))
-         + al256(hull_scratch_bytes(max_pts)) * (size_t)n_hulls + 4096;
+         + al256(hull_scratch_bytes(max_pts, HULL_FIRST_CAP)) * (size_t)n_hulls + 4096;
 }
 
 static int launch_hull_batch(gpu_ctx* ctx, const float* d_pts, const int* d_off, int n_hulls,
@@ -150,12 +154,13 @@ static int launch_hull_batch(gpu_ctx* ctx, const float* d_pts, const int* d_off,
     HullRes* res = pool_take<HullRes>(ctx, n_hulls);
     int* ctl = pool_take<int>(ctx, 16);
     int* wbuf = (int*)pool_take<char>(ctx, hull_wrap_buf_bytes(nwc));
-    const size_t scr_bytes = al256(hull_scratch_bytes(max_pts)) * (size_t)n_hulls;
+    const size_t scr_bytes = al256(hull_scratch_bytes(max_pts, HULL_FIRST_CAP)) * (size_t)n_hulls;
     char* scratch = pool_take<char>(ctx, scr_bytes);
     if (!scratch) return ctx_fail(ctx, KERR_HEAP_OOM, "hull scratch does not fit the pool");
     launch_arena_reset(ctx->d_arena, scratch, scr_bytes, s);
     launch_jobs_from_offsets(d_pts, d_off, n_hulls, d_v, d_t, max_hv, max_ht, jobs, s);
-    launch_hull_jobs(jobs, n_hulls, states, res, ctx->d_arena, ctx->d_arena, ctl, wbuf, nwc, d_stats, s, max_pts);
+    launch_hull_jobs(jobs, n_hulls, states, res, ctx->d_arena, ctx->d_arena, ctl, wbuf, nwc, d_stats, s, max_pts,
+                     false);
     launch_unpack_results(res, n_hulls, d_nv, d_nt, d_vol, d_err, s);
     ctx->launches += 6;
     CK(cudaGetLastError());
