@@ -303,10 +303,12 @@ int cuacd_hull_stats(gpu_ctx_t ctx, const float* pts, int total_pts,
 int cuacd_hull_set_tuning(gpu_ctx_t ctx, int size_class, int pts_per_cta, int seed_min_n);
 int cuacd_hull_get_tuning(gpu_ctx_t ctx, int size_class, int* pts_per_cta, int* seed_min_n);
 
-/* Table sizing of the same pipeline, per size class: a cloud of 4,097 to
- * reduce_max_n points first builds in tables for a quarter of its points
- * (at least 4,096) and only a cloud whose hull outgrows them is built again
- * at full size; larger clouds start at full size (0: the default 32,768). */
+/* Table sizing of the candidate evaluator's fragment hulls, per size class
+ * (no counterpart in the reference): a fragment of 4,097 to reduce_max_n
+ * points first builds in tables for a quarter of its points (at least
+ * 4,096) and only one whose hull outgrows them is built again at full size;
+ * larger fragments start at full size (0: the default 32,768).  The public
+ * batch hull calls and the lookahead search always start at full size. */
 int cuacd_hull_set_table_limit(gpu_ctx_t ctx, int size_class, int reduce_max_n);
 int cuacd_hull_get_table_limit(gpu_ctx_t ctx, int size_class, int* reduce_max_n);
 
