@@ -168,6 +168,31 @@ def test_hull_overflow_paths_emulated(emu_hull_small_lists, tmp_path, oracle):
         np.testing.assert_array_equal(ht, tri)
 
 
+@pytest.fixture(scope="module", params=[8, 32])
+def emu_hull_leaf(request, tmp_path_factory):
+    """The pipeline built with BVH leaves of 8 or 32 points instead of 16."""
+    return _build_emu_hull(tmp_path_factory, [f"-DHULL_LEAF={request.param}"])
+
+
+def test_hull_leaf_sizes_emulated(emu_hull_leaf, tmp_path, oracle):
+    """Every kernel of the hull pipeline takes its leaf size from HULL_LEAF
+    (the seed scan included): with leaves of 8 and of 32 points the hulls
+    are still the oracle's, with no divergent barrier or warp misuse."""
+    v, t = W.candidate_mesh(32, 12, 0.35, seed=3)
+    frag = oracle.plane_cut(v, t, np.array([0.6, 0.0, 0.8, -0.2], np.float32))[0]
+    rng = np.random.default_rng(9)
+    d = rng.normal(size=(1500, 3))
+    shell = (d / np.linalg.norm(d, axis=1, keepdims=True)).astype(np.float32)
+    clouds = W.hull_clouds(2, 700, 1) + [frag, shell, np.load(os.path.join(GOLDEN, "hull_flat_leaves.npy"))]
+    got, reports = run_hulls(emu_hull_leaf, tmp_path, clouds)
+    assert not reports, reports[:5]
+    for c, (err, hv, ht) in zip(clouds, got):
+        vi, tri, vol = oracle.hull(c)
+        assert err == 0
+        np.testing.assert_array_equal(hv, c[vi])
+        np.testing.assert_array_equal(ht, tri)
+
+
 @pytest.fixture(scope="module")
 def emu_hd(tmp_path_factory):
     if shutil.which("g++") is None:
