@@ -31,7 +31,9 @@
 
 #define HD_NT     256
 #define HD_PREP_NT 1024           // threads of the per-surface prep CTA
-#define HD_LEAF   4
+#ifndef HD_LEAF
+#define HD_LEAF   4               // triangles per BVH leaf
+#endif
 #define HD_CHUNK  1024
 #define HD_STACK  48
 
