@@ -28,7 +28,9 @@
 #pragma once
 #include "common.cuh"
 
-#define HULL_NT       512
+#ifndef HULL_NT
+#define HULL_NT       512           // threads per hull CTA (set-up, wrap, output)
+#endif
 // Points per BVH leaf (8, 16 or 32).  32: a leaf is one point per lane of
 // the scanning warp and the tree one level shallower; on the config-3 step
 // the hull stage measured 5.06 ms (pruned) against 5.31 with 16 and 5.2
