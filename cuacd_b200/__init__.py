@@ -126,6 +126,7 @@ _opt("cuacd_candidate_features", _I, [_P, _P, _P, _I, _P, _I, _F, _P, _I, _P])
 _opt("cuacd_scorer_grad", _I, [_P, _P, _P, _P, _I, _P, _P])
 _opt("cuacd_scorer_train", _I, [_P, _P, _P, _P, _I, _I, _I, _F, _F, ctypes.c_uint, _P])
 _opt("cuacd_scorer_predict", _I, [_P, _P, _P, _I, _P])
+_opt("cuacd_scorer_gemm_counts", None, [ctypes.POINTER(ctypes.c_ulonglong), ctypes.POINTER(ctypes.c_ulonglong)])
 _opt("cuacd_eval_candidates_pruned_device", _I, [_P, _P, _P, _I, _P, _I, _F, _P, _I, _I, _F, _I, _I, _I, _F,
                                                  _P, _P, _P, _P, _P])
 _opt("cuacd_eval_candidates_pruned", _I, [_P, _P, _P, _I, _P, _I, _F, _P, _I, _I, _F, _I, _I, _I, _F,

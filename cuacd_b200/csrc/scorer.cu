@@ -20,6 +20,7 @@
 #include <random>
 #include <cmath>
 #include <cstring>
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include "context.cuh"
 #include "launch.h"
@@ -200,9 +201,11 @@ k_cand_features(const float* __restrict__ v, int nv, const float4* __restrict__ 
 #define GM_BK 64
 #define GM_NT 128
 #define GM_STAGES 2
-#define GM_DSMEM ((size_t)GM_STAGES * (GM_BM + GM_BN) * GM_BK * 2)   // 64 KB of slabs
+#define GM_DSMEM ((size_t)GM_STAGES * (GM_BM + GM_BN) * GM_BK * 2 + 1024)   // 64 KB of slabs + alignment
 
 struct GemmArgs {
+    CUtensorMap tma_a;          // A as a 2D tensor (K inner, M rows) when use_tma_a
+    int use_tma_a;
     const __nv_bfloat16* A; long long ar, ac;
     const __nv_bfloat16* B; long long br, bc;
     float* Cf; __nv_bfloat16* Cb; int ldc;
@@ -226,6 +229,18 @@ static __device__ __forceinline__ unsigned long long umma_desc(unsigned addr, un
 {
     return (unsigned long long)((addr >> 4) & 0x3FFF) | ((unsigned long long)((lbo >> 4) & 0x3FFF) << 16) |
            ((unsigned long long)((sbo >> 4) & 0x3FFF) << 32) | (1ull << 46);
+}
+
+// Descriptor of a K-major operand slab written by TMA with the 128-byte
+// swizzle: rows of 64 BF16 (128 bytes) whose 16-byte chunks are permuted by
+// the row's index mod 8; stride byte offset = 8 rows (1,024 bytes), leading
+// offset unused (1), layout type 2 (SWIZZLE_128B) at bits 61-63.  The slab
+// must start on a 1,024-byte boundary; the K = 16 steps inside it advance
+// the start address by 32 bytes.
+static __device__ __forceinline__ unsigned long long umma_desc_sw128(unsigned addr)
+{
+    return (unsigned long long)((addr >> 4) & 0x3FFF) | (1ull << 16) | ((unsigned long long)(1024 >> 4) << 32) |
+           (1ull << 46) | (2ull << 61);
 }
 
 // Instruction descriptor of kind::f16: FP32 accumulator, BF16 A and B, A /
@@ -355,12 +370,16 @@ static __device__ __forceinline__ void stage_slab_async(__nv_bfloat16* slab, con
 }
 
 __global__ void __launch_bounds__(GM_NT)
-k_gemm_umma(GemmArgs g)
+k_gemm_umma(const __grid_constant__ GemmArgs g)
 {
     // GM_STAGES slab pairs (dynamic shared memory); after the last MMA the
     // epilogue's transpose tiles
-    extern __shared__ __align__(1024) __nv_bfloat16 sm[];
+    extern __shared__ __align__(1024) __nv_bfloat16 sm_raw[];
+    // the stages start on a 1,024-byte boundary (the 128-byte swizzle of the
+    // TMA-written A slabs repeats every 1,024 bytes)
+    __nv_bfloat16* const sm = sm_raw + (((1024u - (smem_addr(sm_raw) & 1023u)) & 1023u) >> 1);
     __shared__ __align__(8) unsigned long long s_bar[GM_STAGES];
+    __shared__ __align__(8) unsigned long long s_full[GM_STAGES];     // TMA bytes of a stage's A slab landed
     __shared__ unsigned s_tmem;
     __shared__ int s_fail;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -372,8 +391,10 @@ k_gemm_umma(GemmArgs g)
     }
     if (tid == 0) {
         s_fail = 0;
-        for (int b = 0; b < GM_STAGES; b++)
+        for (int b = 0; b < GM_STAGES; b++) {
             asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_addr(&s_bar[b])), "r"(1) : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_addr(&s_full[b])), "r"(1) : "memory");
+        }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -387,19 +408,40 @@ k_gemm_umma(GemmArgs g)
     // slab pair kt goes to stage kt % 2: its copies are issued while the
     // MMAs of slab kt - 1 run, once those of slab kt - 2 (the stage's last
     // readers) have completed
+    unsigned phf[GM_STAGES] = {0u, 0u};
+    bool tpend[GM_STAGES] = {false, false};           // thread 0: a TMA copy not yet waited for
     auto stage = [&](int kt) {
         __nv_bfloat16* As = sm + (size_t)(kt & 1) * (GM_BM + GM_BN) * GM_BK;
-        stage_slab_async(As, g.A, g.ar, g.ac, g.M, g.K, m0, kt * GM_BK, amode, tid);
+        if (g.use_tma_a) {
+            // one thread: the 128 x 64 box at (k, row) = (kt * 64, m0),
+            // zero-filled outside the matrix, into the stage's A slab
+            if (tid == 0) {
+                const unsigned fb = smem_addr(&s_full[kt & 1]);
+                asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
+                             :: "r"(fb), "r"(GM_BM * GM_BK * 2) : "memory");
+                asm volatile("cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
+                             " [%0], [%1, {%2, %3}], [%4];"
+                             :: "r"(smem_addr(As)), "l"(reinterpret_cast<unsigned long long>(&g.tma_a)),
+                                "r"(kt * GM_BK), "r"(m0), "r"(fb) : "memory");
+                tpend[kt & 1] = true;
+            }
+        } else {
+            stage_slab_async(As, g.A, g.ar, g.ac, g.M, g.K, m0, kt * GM_BK, amode, tid);
+        }
         stage_slab_async(As + GM_BM * GM_BK, g.B, g.bc, g.br, g.N, g.K, n0, kt * GM_BK, bmode, tid);
         asm volatile("cp.async.commit_group;" ::: "memory");
     };
     unsigned ph[GM_STAGES] = {0u, 0u};
     bool pend[GM_STAGES] = {false, false};            // committed MMAs not yet waited for
-    // a wait that gives up waits once more (bounded) for the MMAs in flight
+    // Thread 0 waits for a stage's MMAs and a CTA barrier releases the
+    // others (so 127 threads do not poll the mbarrier); a wait that gives up
+    // waits once more (bounded) for the MMAs in flight.  pend[] is the same
+    // on every thread, so every thread meets the barrier.
     auto wait_stage = [&](int b) {
         const unsigned bar = smem_addr(&s_bar[b]);
-        if (!mbar_wait(bar, ph[b]) && !mbar_wait(bar, ph[b]) && lane == 0) atomicOr(&s_fail, 1);
+        if (tid == 0 && !mbar_wait(bar, ph[b]) && !mbar_wait(bar, ph[b])) atomicOr(&s_fail, 1);
         ph[b] ^= 1u; pend[b] = false;
+        __syncthreads();
     };
     if (nk > 0) stage(0);
     for (int kt = 0; kt < nk && !s_fail; kt++) {
@@ -414,6 +456,11 @@ k_gemm_umma(GemmArgs g)
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // copies -> tensor-core reads
         __syncthreads();
         if (tid == 0) {
+            // the TMA copy of this stage's A slab (bounded wait)
+            if (g.use_tma_a) {
+                if (!mbar_wait(smem_addr(&s_full[b]), phf[b])) atomicOr(&s_fail, 1);
+                phf[b] ^= 1u; tpend[b] = false;
+            }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             const unsigned a0 = smem_addr(sm + (size_t)b * (GM_BM + GM_BN) * GM_BK);
             const unsigned b0 = a0 + GM_BM * GM_BK * 2;
@@ -422,7 +469,8 @@ k_gemm_umma(GemmArgs g)
                 // K chunk pair (2kk, 2kk+1): leading offset = one chunk of
                 // 16 core matrices, stride offset = one core matrix
                 const unsigned off = (unsigned)(2 * kk * (GM_BM / 8) * 128);
-                const unsigned long long ad = umma_desc(a0 + off, (GM_BM / 8) * 128, 128);
+                const unsigned long long ad = g.use_tma_a ? umma_desc_sw128(a0 + 32u * kk)
+                                                          : umma_desc(a0 + off, (GM_BM / 8) * 128, 128);
                 const unsigned long long bd = umma_desc(b0 + off, (GM_BN / 8) * 128, 128);
                 const unsigned acc = (kt > 0 || kk > 0) ? 1u : 0u;
                 asm volatile("{\n .reg .pred p;\n setp.ne.u32 p, %4, 0;\n"
@@ -438,6 +486,10 @@ k_gemm_umma(GemmArgs g)
     // memory and the accumulator are read or released
     for (int b = 0; b < GM_STAGES; b++) if (pend[b]) wait_stage(b);
     asm volatile("cp.async.wait_all;" ::: "memory");
+    // a loop stopped early may leave a TMA copy in flight: it lands first
+    if (tid == 0)
+        for (int b = 0; b < GM_STAGES; b++)
+            if (tpend[b] && !mbar_wait(smem_addr(&s_full[b]), phf[b])) atomicOr(&s_fail, 1);
     const bool issued = nk > 0;
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -489,6 +541,48 @@ k_gemm_umma(GemmArgs g)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(GM_BN) : "memory");
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (the
+// library links the runtime statically and never the driver library).
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+static EncodeTiledFn encode_tiled()
+{
+    static EncodeTiledFn fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (EncodeTiledFn)p;
+    }
+    return fn;
+}
+
+// A K-major, contiguous A (A(i, k) = A[i*ar + k]) goes to the tensor core
+// through TMA: a 2D map (K inner, M rows, row pitch 2*ar bytes) with
+// 128 x 64 boxes and the 128-byte swizzle.  Other operands, or a map the
+// driver refuses, are staged with cp.async.
+static void gemm_tma_a(GemmArgs& g)
+{
+    g.use_tma_a = 0;
+    if (g.ac != 1 || g.ar % 8 != 0 || g.K % 8 != 0 || g.ar < g.K || ((size_t)g.A & 15)) return;
+    EncodeTiledFn fn = encode_tiled();
+    if (!fn) return;
+    const cuuint64_t dims[2] = {(cuuint64_t)g.K, (cuuint64_t)g.M};
+    const cuuint64_t strides[1] = {(cuuint64_t)g.ar * 2};
+    const cuuint32_t box[2] = {GM_BK, GM_BM};
+    const cuuint32_t estr[2] = {1, 1};
+    if (fn(&g.tma_a, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, (void*)g.A, dims, strides, box, estr,
+           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS)
+        g.use_tma_a = 1;
+}
+
+static unsigned long long g_gemm_tma = 0, g_gemm_staged = 0;   // launches by how A was staged
+
 static void gemm(GemmArgs g, int* err, cudaStream_t s)
 {
     static bool attr_set[64] = {false};
@@ -499,6 +593,8 @@ static void gemm(GemmArgs g, int* err, cudaStream_t s)
         attr_set[dev] = true;
     }
     g.err = err;
+    gemm_tma_a(g);
+    if (g.M > 0 && g.N > 0) { if (g.use_tma_a) g_gemm_tma++; else g_gemm_staged++; }
     dim3 grid((g.N + GM_BN - 1) / GM_BN, (g.M + GM_BM - 1) / GM_BM);
     if (g.M > 0 && g.N > 0) k_gemm_umma<<<grid, GM_NT, GM_DSMEM, s>>>(g);
 }
@@ -775,6 +871,12 @@ static int sc_upload_rows(gpu_ctx* ctx, cuacd_scorer* s, const float* X, const f
 // C ABI
 // ---------------------------------------------------------------------------
 extern "C" int cuacd_scorer_n_params(void) { return (int)N_PARAMS; }
+
+extern "C" void cuacd_scorer_gemm_counts(unsigned long long* tma, unsigned long long* staged)
+{
+    if (tma) *tma = g_gemm_tma;
+    if (staged) *staged = g_gemm_staged;
+}
 extern "C" int cuacd_scorer_n_features(void) { return SC_K; }
 
 extern "C" int cuacd_scorer_create(gpu_ctx_t ctx, unsigned seed, cuacd_scorer_t* out)

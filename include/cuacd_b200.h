@@ -376,6 +376,12 @@ int cuacd_scorer_train(gpu_ctx_t ctx, cuacd_scorer_t s, const float* X, const fl
 
 int cuacd_scorer_predict(gpu_ctx_t ctx, cuacd_scorer_t s, const float* X, int n, float* out);
 
+/* Diagnostic (no counterpart in the reference): scorer GEMM launches so far
+ * in this process, by how their A operand reached shared memory -- by TMA
+ * (a K-major contiguous A whose tensor map the driver accepted) or by the
+ * CTA's own copies (strided or broadcast operands). */
+void cuacd_scorer_gemm_counts(unsigned long long* tma, unsigned long long* staged);
+
 /* Surrogate-pruned evaluation (at most 1024 planes): predicted scores for
  * all planes, the exact evaluator for the top_k best predictions plus every
  * plane predicted within `margin` of the k-th.  Unevaluated planes get

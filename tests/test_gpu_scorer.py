@@ -212,3 +212,25 @@ def test_search_scorer_ranks_level0(ctx, S):
     random_hit = float(np.mean(np.minimum(48, sizes) / sizes))
     assert hit > random_hit + 0.3, (hit, random_hit)
     assert reg < 0.25 * rreg, (reg, rreg)
+
+
+def test_forward_stages_activations_by_tma(ctx, S, ref):
+    """A forward pass of 300 rows: every layer's A operand (the feature rows,
+    then the hidden activations) is a K-major contiguous matrix, so its
+    slabs reach shared memory by TMA (128-byte swizzle), and the output
+    still matches the FP64 forward of the same BF16 parameters."""
+    import ctypes
+    from cuacd_b200 import _fn
+    counts = lambda: [ctypes.c_ulonglong(0), ctypes.c_ulonglong(0)]
+    a0, s0 = counts()
+    _fn("cuacd_scorer_gemm_counts")(ctypes.byref(a0), ctypes.byref(s0))
+    X = np.random.default_rng(11).standard_normal((300, S.N_FEATURES)).astype(np.float32)
+    with S.Scorer(ctx, seed=3) as sc:
+        y = sc.predict(X)
+        mean, inv = sc.normalizer()
+        params = sc.params()
+    a1, s1 = counts()
+    _fn("cuacd_scorer_gemm_counts")(ctypes.byref(a1), ctypes.byref(s1))
+    assert a1.value - a0.value == 3 and s1.value == s0.value
+    ry = ref.forward(params, X, mean, inv)[0] / ref.TSCALE
+    assert np.abs(y - ry).max() <= 2e-2 * np.abs(ry).max() + 1e-3
