@@ -258,7 +258,87 @@ static __device__ int cut_build_caps(const float* V, int n_all, const unsigned l
     };
     auto loop_reverse = [&](int start, int m) { cut_reverse(lv + start, m); if (fast) cut_reverse(le + start, m); };
     int n_loops = 0, fail = 0;
-    if (tid == 0) {
+    // Parallel tracing.  When every boundary vertex starts exactly one edge
+    // and ends exactly one, "the first unused edge leaving the walk's vertex"
+    // is the successor permutation, and thread 0's walk (next loop at the
+    // smallest unused edge) yields its cycles, each from its smallest edge,
+    // in order of that edge.  The CTA finds each edge's cycle minimum and
+    // its distance from it by pointer jumping (log2 nb rounds each) and
+    // writes lv / le / ls / lsz as the walk would.  Any other boundary (a
+    // vertex with two outgoing edges, an open chain) takes the walk.
+    __shared__ int s_par, s_scanbuf[34];
+    bool traced = false;
+    if (fast && nb >= 64) {
+        int* succ = tmp;                              // tmp: 2 * poly_cap >= 8 nb + 128 ints
+        int* cnt = tmp + nb;
+        int* mA = tmp + 2 * nb; int* mB = tmp + 3 * nb;
+        int* jA = tmp + 4 * nb; int* jB = tmp + 5 * nb;
+        int* dA = tmp + 6 * nb; int* dB = tmp + 7 * nb;
+        for (int i = tid; i < nb; i += CUT_NT) cnt[i] = 0;
+        __syncthreads();
+        int bad = 0;
+        for (int i = tid; i < nb; i += CUT_NT) {
+            const int a = s_ea[i], b = s_eb[i];
+            int sc = s_nxt[i];
+            if (a < 0 || a >= n_all || b < 0 || b >= n_all) bad = 1;
+            if (sc >= nb || s_ea[sc] != b || (sc + 1 < nb && s_ea[sc + 1] == b)) { bad = 1; sc = i; }
+            succ[i] = sc;
+            atomicAdd(&cnt[sc], 1);
+        }
+        __syncthreads();
+        for (int i = tid; i < nb; i += CUT_NT) if (cnt[i] != 1) bad = 1;
+        if (!__syncthreads_or(bad)) {
+            int R = 0;
+            while ((1 << R) < nb) R++;
+            // cycle minimum: after R rounds each edge has seen 2^R >= nb edges of its cycle
+            for (int i = tid; i < nb; i += CUT_NT) { mA[i] = i; jA[i] = succ[i]; }
+            __syncthreads();
+            int *mc = mA, *mn = mB, *jc = jA, *jn = jB;
+            for (int r = 0; r < R; r++) {
+                for (int i = tid; i < nb; i += CUT_NT) { const int j = jc[i]; mn[i] = min(mc[i], mc[j]); jn[i] = jc[j]; }
+                __syncthreads();
+                int* t = mc; mc = mn; mn = t; t = jc; jc = jn; jn = t;
+            }
+            // steps to the cycle's last edge (the one whose successor is the minimum)
+            int *dc = dA, *dn = dB;
+            jc = jA; jn = jB;
+            for (int i = tid; i < nb; i += CUT_NT) {
+                const int last = succ[i] == mc[i];
+                jc[i] = last ? -1 : succ[i]; dc[i] = last ? 0 : 1;
+            }
+            __syncthreads();
+            for (int r = 0; r < R; r++) {
+                for (int i = tid; i < nb; i += CUT_NT) {
+                    const int j = jc[i];
+                    if (j >= 0) { dn[i] = dc[i] + dc[j]; jn[i] = jc[j]; } else { dn[i] = dc[i]; jn[i] = -1; }
+                }
+                __syncthreads();
+                int* t = dc; dc = dn; dn = t; t = jc; jc = jn; jn = t;
+            }
+            // loops in order of their smallest edge: starts and indices by two scans
+            int* start = jc;                          // free now
+            int* lid = jn;
+            for (int i = tid; i < nb; i += CUT_NT) {
+                const int is_min = mc[i] == i;
+                start[i] = is_min ? dc[i] + 1 : 0;
+                lid[i] = is_min;
+            }
+            __syncthreads();
+            cta_scan_inplace(start, nb, s_scanbuf);
+            const int nloops = cta_scan_inplace(lid, nb, s_scanbuf);
+            if (nloops <= 128) {
+                for (int i = tid; i < nb; i += CUT_NT) {
+                    const int m = mc[i];
+                    const int off = start[m] + (dc[m] - dc[i]);
+                    lv[off] = s_ea[i]; le[off] = i;
+                    if (m == i) { ls[lid[i]] = start[i]; lsz[lid[i]] = dc[i] + 1; }
+                }
+            }
+            if (tid == 0) { s_nl = nloops; s_fail = nloops > 128; }
+            traced = true;
+        }
+    }
+    if (tid == 0 && !traced) {
         int lvi = 0;
         if (!fast) for (int i = 0; i < nb; i++) used[i] = 0;
         for (int st = 0; st < nb && !fail; st++) {
