@@ -202,9 +202,34 @@ static __device__ int cut_ear_clip_cta(const Cap2D& c, const int* poly, int n, d
     return nc;
 }
 
+// CTA-wide minimum of (key, idx) pairs in lexicographic order, returned to
+// every thread (all CUT_NT threads call).
+static __device__ void cut_cta_lexmin(double& key, int& idx)
+{
+    __shared__ double s_k[CUT_NT / 32];
+    __shared__ int s_i[CUT_NT / 32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    #pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const double k2 = __shfl_xor_sync(FULL_MASK, key, o);
+        const int i2 = __shfl_xor_sync(FULL_MASK, idx, o);
+        if (k2 < key || (k2 == key && i2 < idx)) { key = k2; idx = i2; }
+    }
+    if (lane == 0) { s_k[w] = key; s_i[w] = idx; }
+    __syncthreads();
+    key = s_k[0]; idx = s_i[0];
+    for (int q = 1; q < CUT_NT / 32; q++)
+        if (s_k[q] < key || (s_k[q] == key && s_i[q] < idx)) { key = s_k[q]; idx = s_i[q]; }
+    __syncthreads();                                   // s_k / s_i free for the next call
+}
+
 // Caps from the directed boundary edges be[] (sorted by (a,b), packed a<<32|b).
-// Whole CTA: thread 0 traces the loops, nests them and bridges holes; the
-// ear clipping is CTA-wide.  gU/gW: 2*poly_cap doubles of global scratch for
+// Whole CTA: the loops are traced by pointer jumping when the boundary's
+// successor map is a permutation (else by thread 0's walk), nesting counts
+// ray crossings with the CTA, holes are bridged by CTA reductions and a
+// parallel splice, and the ear clipping is CTA-wide; thread 0 keeps the
+// short serial decisions (loop orientation, parent choice, hole order).
+// gU/gW: 2*poly_cap doubles of global scratch for
 // polygons longer than CUT_EAR_SM.  Returns n_cap >= 0 or -1 on failure.
 static __device__ int cut_build_caps(const float* V, int n_all, const unsigned long long* be, int nb,
                               float pa, float pb, float pc, int* used, int* lv, int* ls, int* lsz,
@@ -456,8 +481,9 @@ static __device__ int cut_build_caps(const float* V, int n_all, const unsigned l
             for (int i = tid; i < m; i += CUT_NT) poly[i] = lv[o + i];
             __syncthreads();
         }
+        // holes of this loop, by decreasing largest u (thread 0: a short list)
+        __shared__ int s_nin;
         if (tid == 0) {
-            pn = lsz[oi];
             int nin = 0;
             for (int i = 0; i < n_loops && nin < 128; i++) {
                 if (parent[i] != oi || lsz[i] < 3) continue;
@@ -473,37 +499,61 @@ static __device__ int cut_build_caps(const float* V, int n_all, const unsigned l
                     double tf = hmax[i]; hmax[i] = hmax[best]; hmax[best] = tf;
                 }
             }
-            for (int ii = 0; ii < nin && !fail; ii++) {
-                int hi = hidx[ii], hs = lsz[hi];
-                const int* hole = lv + ls[hi];
-                int m_idx = 0; double max_u = -1e300;
-                for (int j = 0; j < hs; j++) { double u = cU(C, hole[j]); if (u > max_u) { max_u = u; m_idx = j; } }
-                double mu_ = cU(C, hole[m_idx]), mv_ = cW(C, hole[m_idx]);
-                double best_t = 1e300; int best_edge = -1;
-                for (int j = 0; j < pn; j++) {
-                    int jn = (j + 1) % pn;
-                    double au = cU(C, poly[j]), av = cW(C, poly[j]);
-                    double bu = cU(C, poly[jn]), bv = cW(C, poly[jn]);
-                    double dv = bv - av; if (fabs(dv) < 1e-12) continue;
-                    double s_ = (mv_ - av) / dv;
-                    if (s_ < -1e-12 || s_ > 1.0 + 1e-12) continue;
-                    double tv = au + s_ * (bu - au) - mu_;
-                    if (tv > 1e-12 && tv < best_t) { best_t = tv; best_edge = j; }
-                }
-                if (best_edge < 0) { fail = 1; break; }
-                int jn = (best_edge + 1) % pn;
-                int p_pos = (cU(C, poly[best_edge]) >= cU(C, poly[jn])) ? best_edge : jn;
-                if (pn + hs + 2 > poly_cap) { fail = 1; break; }
-                int k = 0;
-                for (int j = 0; j <= p_pos; j++) tmp[k++] = poly[j];
-                for (int j = 0; j < hs; j++) tmp[k++] = hole[(m_idx + j) % hs];
-                tmp[k++] = hole[m_idx]; tmp[k++] = poly[p_pos];
-                for (int j = p_pos + 1; j < pn; j++) tmp[k++] = poly[j];
-                for (int j = 0; j < k; j++) poly[j] = tmp[j];
-                pn = k;
-            }
-            s_fail = fail; s_pn = pn;
+            s_nin = nin; s_pn = lsz[oi]; s_fail = 0;
         }
+        __syncthreads();
+        // Each hole is bridged to the loop by the CTA: its rightmost vertex
+        // (the first of largest u) and the loop edge its rightward ray meets
+        // first (the first of smallest t) are CTA reductions over the same
+        // per-vertex and per-edge expressions as a serial scan, with the
+        // serial scan's tie rule (smallest index); the spliced polygon is
+        // written in parallel.
+        const int nin = s_nin;
+        for (int ii = 0; ii < nin; ii++) {
+            const int pn0 = s_pn;
+            const int hi = hidx[ii], hs = lsz[hi];
+            const int* hole = lv + ls[hi];
+            double key = 1e300; int idx = 0x7fffffff;
+            for (int j = tid; j < hs; j += CUT_NT) {
+                const double k = -cU(C, hole[j]);
+                if (k < key || (k == key && j < idx)) { key = k; idx = j; }
+            }
+            cut_cta_lexmin(key, idx);
+            const int m_idx = idx;
+            const double mu_ = cU(C, hole[m_idx]), mv_ = cW(C, hole[m_idx]);
+            key = 1e300; idx = 0x7fffffff;
+            for (int j = tid; j < pn0; j += CUT_NT) {
+                const int jn = (j + 1) % pn0;
+                const double au = cU(C, poly[j]), av = cW(C, poly[j]);
+                const double bu = cU(C, poly[jn]), bv = cW(C, poly[jn]);
+                const double dv = bv - av;
+                if (fabs(dv) < 1e-12) continue;
+                const double s_ = (mv_ - av) / dv;
+                if (s_ < -1e-12 || s_ > 1.0 + 1e-12) continue;
+                const double tv = au + s_ * (bu - au) - mu_;
+                if (tv > 1e-12 && (tv < key || (tv == key && j < idx))) { key = tv; idx = j; }
+            }
+            cut_cta_lexmin(key, idx);
+            const int best_edge = idx;
+            if (best_edge == 0x7fffffff || pn0 + hs + 2 > poly_cap) { fail = 1; break; }   // uniform
+            const int jn = (best_edge + 1) % pn0;
+            const int p_pos = (cU(C, poly[best_edge]) >= cU(C, poly[jn])) ? best_edge : jn;
+            const int npn = pn0 + hs + 2;
+            for (int k = tid; k < npn; k += CUT_NT) {
+                int v;
+                if (k <= p_pos) v = poly[k];
+                else if (k <= p_pos + hs) v = hole[(m_idx + (k - p_pos - 1)) % hs];
+                else if (k == p_pos + hs + 1) v = hole[m_idx];
+                else if (k == p_pos + hs + 2) v = poly[p_pos];
+                else v = poly[k - hs - 2];
+                tmp[k] = v;
+            }
+            __syncthreads();
+            for (int k = tid; k < npn; k += CUT_NT) poly[k] = tmp[k];
+            if (tid == 0) s_pn = npn;
+            __syncthreads();
+        }
+        if (tid == 0 && fail) s_fail = 1;
         __syncthreads();
         fail = s_fail;
         pn = s_pn;

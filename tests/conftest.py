@@ -49,6 +49,43 @@ def l_shape():
     return np.vstack([v1, v2]), np.vstack([t1, t2 + len(v1)])
 
 
+def torus_mesh(R, r, nu=48, nv=16):
+    """Closed torus around the z axis (nu x nv grid), outward winding."""
+    u = np.arange(nu) * (2 * np.pi / nu)
+    w = np.arange(nv) * (2 * np.pi / nv)
+    U, V = np.meshgrid(u, w, indexing="ij")
+    verts = np.stack([(R + r * np.cos(V)) * np.cos(U), (R + r * np.cos(V)) * np.sin(U), r * np.sin(V)], -1)
+    idx = lambda i, j: (i % nu) * nv + (j % nv)
+    tris = []
+    for i in range(nu):
+        for j in range(nv):
+            a, b, c, d = idx(i, j), idx(i + 1, j), idx(i + 1, j + 1), idx(i, j + 1)
+            tris += [(a, b, c), (a, c, d)]
+    v = verts.reshape(-1, 3).astype(np.float32)
+    t = np.asarray(tris, np.int32)
+    e = v[t]
+    if np.einsum("ij,ij->i", e[:, 0], np.cross(e[:, 1], e[:, 2])).sum() < 0:
+        t = t[:, ::-1].copy()
+    return v, t
+
+
+def nested_tori():
+    """Three concentric tori (R = 1, 2, 3; r = 0.3): a cut across their ring
+    gives six nested circles, annuli inside annuli."""
+    parts = [torus_mesh(R, 0.3) for R in (1.0, 2.0, 3.0)]
+    v = np.concatenate([p[0] for p in parts])
+    offs = np.cumsum([0] + [len(p[0]) for p in parts[:-1]])
+    t = np.concatenate([p[1] + o for p, o in zip(parts, offs)]).astype(np.int32)
+    return v, t
+
+
+def box_with_cavity():
+    """Unit box holding an inverted inner box (a closed cavity)."""
+    a = box_mesh([0, 0, 0], [1, 1, 1])
+    b = box_mesh([0.3, 0.3, 0.3], [0.7, 0.7, 0.7])
+    return np.vstack([a[0], b[0]]).astype(np.float32), np.vstack([a[1], b[1][:, ::-1] + 8]).astype(np.int32)
+
+
 def is_watertight(t):
     """Every directed edge has exactly one reverse partner."""
     t = np.asarray(t)

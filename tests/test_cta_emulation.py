@@ -15,7 +15,7 @@ import subprocess
 import numpy as np
 import pytest
 
-from conftest import GOLDEN, ROOT, box_mesh
+from conftest import GOLDEN, ROOT, box_mesh, box_with_cavity, nested_tori
 from cuacd_b200 import workloads as W
 
 EMU = os.path.join(ROOT, "tests", "cta_emu")
@@ -75,6 +75,28 @@ def test_cube_and_sphere(emu_cut, tmp_path, oracle):
 def test_ear_clipping_race_case(emu_cut, tmp_path, oracle):
     g = np.load(os.path.join(GOLDEN, "cut_ear_race.npz"))
     v, t, planes = g["v"], g["t"], g["planes"]
+    rows, reports = run(emu_cut, tmp_path, v, t, planes)
+    assert not reports, reports[:5]
+    check(oracle, v, t, planes, rows)
+
+
+def test_nested_loops_and_holes_emulated(emu_cut, tmp_path, oracle):
+    """Caps with holes: loop nesting by ray crossings, and each hole bridged
+    to its loop by CTA reductions (rightmost hole vertex, first edge met) and
+    a parallel splice -- every barrier reached by the whole CTA, the
+    oracle's loop and cap-triangle counts."""
+    v, t = nested_tori()
+    planes = []
+    for plane in [(0, 0, 1, -0.013), (0.08, 0.05, 0.9955, -0.02), (1, 0, 0, -0.05)]:
+        n = np.asarray(plane[:3], np.float64)
+        planes.append([*(n / np.linalg.norm(n)), plane[3]])
+    planes = np.asarray(planes, np.float32)
+    rows, reports = run(emu_cut, tmp_path, v, t, planes)
+    assert not reports, reports[:5]
+    check(oracle, v, t, planes, rows)
+    assert max(r["loops"] for r in rows) >= 6
+    v, t = box_with_cavity()
+    planes = np.array([[0, 0, 1, -0.5], [0.6, 0.48, 0.64, -0.9]], np.float32)
     rows, reports = run(emu_cut, tmp_path, v, t, planes)
     assert not reports, reports[:5]
     check(oracle, v, t, planes, rows)

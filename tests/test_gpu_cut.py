@@ -3,7 +3,7 @@
 import numpy as np
 import pytest
 
-from conftest import box_mesh, l_shape, is_watertight
+from conftest import box_mesh, box_with_cavity, l_shape, is_watertight, nested_tori
 from cuacd_b200 import workloads as W
 
 pytestmark = pytest.mark.gpu
@@ -63,43 +63,18 @@ def test_batch_meshes_random_planes(ctx, oracle):
             _check(ctx, oracle, v, t, p)
 
 
-def _torus(R, r, nu=48, nv=16):
-    u = np.arange(nu) * (2 * np.pi / nu)
-    w = np.arange(nv) * (2 * np.pi / nv)
-    U, V = np.meshgrid(u, w, indexing="ij")
-    verts = np.stack([(R + r * np.cos(V)) * np.cos(U), (R + r * np.cos(V)) * np.sin(U), r * np.sin(V)], -1)
-    idx = lambda i, j: (i % nu) * nv + (j % nv)
-    tris = []
-    for i in range(nu):
-        for j in range(nv):
-            a, b, c, d = idx(i, j), idx(i + 1, j), idx(i + 1, j + 1), idx(i, j + 1)
-            tris += [(a, b, c), (a, c, d)]
-    v = verts.reshape(-1, 3).astype(np.float32)
-    t = np.asarray(tris, np.int32)
-    e = v[t]
-    if np.einsum("ij,ij->i", e[:, 0], np.cross(e[:, 1], e[:, 2])).sum() < 0:
-        t = t[:, ::-1].copy()
-    return v, t
-
-
 def test_nested_loops_and_holes(ctx, oracle):
     """Caps with holes and nesting (loop orientation, parent search, hole
     bridging): three concentric tori cut across their ring give six nested
     circles (annuli inside annuli); a box with an inverted inner box (a
     cavity) gives a square with a square hole."""
-    parts = [_torus(R, 0.3) for R in (1.0, 2.0, 3.0)]
-    v = np.concatenate([p[0] for p in parts])
-    offs = np.cumsum([0] + [len(p[0]) for p in parts[:-1]])
-    t = np.concatenate([p[1] + o for p, o in zip(parts, offs)]).astype(np.int32)
+    v, t = nested_tori()
     for plane in [(0, 0, 1, -0.013), (0, 0, 1, 0.1), (0.08, 0.05, 0.9955, -0.02), (1, 0, 0, -0.05)]:
         n = np.asarray(plane[:3], np.float64)
         p = (*(n / np.linalg.norm(n)).astype(np.float32), np.float32(plane[3]))
         (pv, pt, nv_, nt), info = _check(ctx, oracle, v, t, p)
         assert is_watertight(pt) and is_watertight(nt)
-    a = box_mesh([0, 0, 0], [1, 1, 1])
-    b = box_mesh([0.3, 0.3, 0.3], [0.7, 0.7, 0.7])
-    v = np.vstack([a[0], b[0]]).astype(np.float32)
-    t = np.vstack([a[1], b[1][:, ::-1] + 8]).astype(np.int32)
+    v, t = box_with_cavity()
     for plane in [(0, 0, 1, -0.5), (0, 1, 0, -0.45), (0.6, 0.48, 0.64, -0.9)]:
         (pv, pt, nv_, nt), info = _check(ctx, oracle, v, t, plane)
         assert is_watertight(pt) and is_watertight(nt)
