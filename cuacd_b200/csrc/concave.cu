@@ -144,7 +144,7 @@ static __device__ void concave_cta(const float* __restrict__ v, int nv, const in
     const int n_res = s_nres;
     __shared__ int s_cnt[1024];
     for (int s = tid; s < n_res; s += CC_NT) {
-        int v0 = res[4 * s], v1 = res[4 * s + 1], f0 = res[4 * s + 2], f1 = res[4 * s + 3];
+        int f0 = res[4 * s + 2], f1 = res[4 * s + 3];
         float n0[3], n1[3];
         int c = 0;
         if (cc_face_normal(v, t, f0, n0) && cc_face_normal(v, t, f1, n1)) {

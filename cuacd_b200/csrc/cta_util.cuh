@@ -8,13 +8,16 @@
 // pass 1 sums it, one CTA scan of the warp sums gives the segment offsets,
 // pass 2 scans the segment 32 values at a time with a running carry, so the
 // CTA meets three barriers whatever n is.
-static __device__ int cta_scan_inplace(int* data, int n, int* sh)
+// kRankFlags: the entries are flags (non-zero = set); a set entry becomes
+// the number of set entries before it, a clear one -1.
+template <bool kRankFlags>
+static __device__ int cta_scan_impl(int* data, int n, int* sh)
 {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
     const int seg = ((n + nw - 1) / nw + 31) & ~31;
     const int b = min(n, w * seg), e = min(n, b + seg);
     int sum = 0;
-    for (int i = b + lane; i < e; i += 32) sum += data[i];
+    for (int i = b + lane; i < e; i += 32) sum += kRankFlags ? (data[i] != 0) : data[i];
     #pragma unroll
     for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(FULL_MASK, sum, o);
     __syncthreads();                                   // sh may still be in use by the caller
@@ -35,19 +38,25 @@ static __device__ int cta_scan_inplace(int* data, int n, int* sh)
     const int total = sh[32];
     for (int base = b; base < e; base += 32) {         // warp-uniform trip count
         const int i = base + lane;
-        const int v = i < e ? data[i] : 0;
+        const int v = i < e ? (kRankFlags ? (data[i] != 0) : data[i]) : 0;
         int x = v;
         #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
             int y = __shfl_up_sync(FULL_MASK, x, o);
             if (lane >= o) x += y;
         }
-        if (i < e) data[i] = carry + x - v;
+        if (i < e) data[i] = (kRankFlags && !v) ? -1 : carry + x - v;
         carry += __shfl_sync(FULL_MASK, x, 31);
     }
     __syncthreads();
     return total;
 }
+
+static __device__ int cta_scan_inplace(int* data, int n, int* sh) { return cta_scan_impl<false>(data, n, sh); }
+
+// In-place ranks of set flags: data[i] != 0 becomes the number of set
+// entries before i, data[i] == 0 becomes -1.  Returns the number set.
+static __device__ int cta_rank_flags_inplace(int* data, int n, int* sh) { return cta_scan_impl<true>(data, n, sh); }
 
 // Bitonic sort of keys[0..n) ascending; the array must hold next_pow2(n)
 // entries (the tail is filled with ~0).  Whole CTA.

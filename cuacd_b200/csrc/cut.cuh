@@ -202,6 +202,23 @@ static __device__ int cut_ear_clip_cta(const Cap2D& c, const int* poly, int n, d
     return nc;
 }
 
+// i = tid, tid + CUT_NT, ... < n, each thread issuing the loads of
+// CUT_ILP iterations before their stores, so that a thread keeps several
+// independent global loads in flight.  For loops whose iterations are
+// independent: load(i) reads nothing that store(j) writes.
+#define CUT_ILP 4
+template <class Load, class Store>
+static __device__ __forceinline__ void cut_for_ilp(int n, Load load, Store store)
+{
+    for (int base = threadIdx.x; base < n; base += CUT_ILP * CUT_NT) {
+        decltype(load(0)) v[CUT_ILP];
+        #pragma unroll
+        for (int u = 0; u < CUT_ILP; u++) { const int i = base + u * CUT_NT; if (i < n) v[u] = load(i); }
+        #pragma unroll
+        for (int u = 0; u < CUT_ILP; u++) { const int i = base + u * CUT_NT; if (i < n) store(i, v[u]); }
+    }
+}
+
 // CTA-wide minimum of (key, idx) pairs in lexicographic order, returned to
 // every thread (all CUT_NT threads call).
 static __device__ void cut_cta_lexmin(double& key, int& idx)
@@ -291,7 +308,7 @@ static __device__ int cut_build_caps(const float* V, int n_all, const unsigned l
     // its distance from it by pointer jumping (log2 nb rounds each) and
     // writes lv / le / ls / lsz as the walk would.  Any other boundary (a
     // vertex with two outgoing edges, an open chain) takes the walk.
-    __shared__ int s_par, s_scanbuf[34];
+    __shared__ int s_scanbuf[34];
     bool traced = false;
     if (fast && nb >= 64) {
         int* succ = tmp;                              // tmp: 2 * poly_cap >= 8 nb + 128 ints
@@ -579,7 +596,7 @@ static __device__ void cut_cta(const float* __restrict__ verts, int nv, const in
                         float pa, float pb, float pc, float pd, Arena* arena, CutFixedOut fixed,
                         CutResult* res, CutShared& sh, Arena* out_arena = nullptr)
 {
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int tid = threadIdx.x, lane = tid & 31;
     Arena* const oarena = out_arena ? out_arena : arena;
     long long tph[5];
     tph[0] = clock64();
@@ -951,7 +968,7 @@ static __device__ void cut_cta(const float* __restrict__ verts, int nv, const in
     const int nb = sh.cnt[7];
     cta_sort_u64(be, nb);
     tph[3] = clock64();
-    // ---------------- caps (warp 0)
+    // ---------------- caps (whole CTA)
     const int poly_cap = nb * 4 + 64;
     CUT_ALLOC(15, int, 4 * nb + 3 * poly_cap + 3 * poly_cap);
     CUT_ALLOC(13, double, poly_cap > CUT_EAR_SM ? 2 * poly_cap : 1);   // ear-clip coordinates of long polygons
@@ -1015,8 +1032,8 @@ static __device__ void cut_cta(const float* __restrict__ verts, int nv, const in
             const int ns = side == 0 ? n_pos : n_neg;
             for (int v = tid; v < n_all; v += CUT_NT) remap[v] = 0;
             __syncthreads();
-            for (int i = tid; i < 3 * ns; i += CUT_NT) remap[st[i]] = 1;
-            for (int i = tid; i < 3 * n_cap; i += CUT_NT) remap[capt[i]] = 1;
+            cut_for_ilp(3 * ns, [&](int i) { return st[i]; }, [&](int, int v) { remap[v] = 1; });
+            cut_for_ilp(3 * n_cap, [&](int i) { return capt[i]; }, [&](int, int v) { remap[v] = 1; });
             __syncthreads();
             // remember used flags in the sign bit region: scan destroys them,
             // so mark unused as -1 after the scan by re-deriving from triangles
@@ -1043,9 +1060,11 @@ static __device__ void cut_cta(const float* __restrict__ verts, int nv, const in
             __syncthreads();
             if (s_err) goto fail_out;
             float* ov = (float*)sh.ptr[6 + 2 * side]; int* ot = (int*)sh.ptr[7 + 2 * side];
-            for (int v = tid; v < n_all; v += CUT_NT)
-                if (usedf[v]) { int j = remap[v]; ov[3 * j] = all[3 * v]; ov[3 * j + 1] = all[3 * v + 1]; ov[3 * j + 2] = all[3 * v + 2]; }
-            for (int i = tid; i < 3 * ns; i += CUT_NT) ot[i] = remap[st[i]];
+            cut_for_ilp(n_all, [&](int v) { return usedf[v] ? remap[v] : -1; },
+                        [&](int v, int j) {
+                            if (j >= 0) { ov[3 * j] = all[3 * v]; ov[3 * j + 1] = all[3 * v + 1]; ov[3 * j + 2] = all[3 * v + 2]; }
+                        });
+            cut_for_ilp(3 * ns, [&](int i) { return remap[st[i]]; }, [&](int i, int j) { ot[i] = j; });
             for (int t = tid; t < n_cap; t += CUT_NT) {
                 int v0 = capt[3 * t], v1 = capt[3 * t + 1], v2 = capt[3 * t + 2];
                 int o = 3 * (ns + t);

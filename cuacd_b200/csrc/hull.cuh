@@ -27,6 +27,7 @@
 // reference's (y,x,z,index) sort keeps the first (warp_sort.cuh:237-244).
 #pragma once
 #include "common.cuh"
+#include "cta_util.cuh"
 
 #ifndef HULL_NT
 #define HULL_NT       512           // threads per hull CTA (set-up, wrap, output)
@@ -764,7 +765,7 @@ struct HullWrapShared {
 };
 
 struct HullOutShared {
-    int scan[33];
+    int scan[34];
     double dsh[33];
 };
 
@@ -1011,8 +1012,7 @@ static __device__ void hull_setup_cta(const float* __restrict__ pts, int n, char
     // ---- cooperative (large) face: collect S by scanning all points, walk
     // the polygon with CTA reductions, publish the face.  u<0: first face.
     __shared__ int s_face_ok;
-    __shared__ int s_cur, s_prev, s_first;
-    __shared__ double s_N[3];
+    __shared__ int s_cur, s_first;
     auto coop_face = [&](int u, int v, double nx, double ny, double nz, int anchor) -> void {
         // anchor: a point on the plane
         if (tid == 0) { sh.n_S = 0; s_face_ok = 1; }
@@ -1057,9 +1057,9 @@ static __device__ void hull_setup_cta(const float* __restrict__ pts, int n, char
                     float4 q = P4[Sbuf[i]];
                     if (same_pos(q, P4[f]) && pidx(q) < pidx(P4[f])) f = Sbuf[i];
                 }
-                s_first = f; s_cur = f; s_prev = -1;
+                s_first = f; s_cur = f;
             }
-        } else if (tid == 0) { s_first = v; s_prev = v; s_cur = u; }
+        } else if (tid == 0) { s_first = v; s_cur = u; }
         __syncthreads();
         // corner list
         __shared__ int s_cstart, s_k;
@@ -1521,21 +1521,8 @@ static __device__ void hull_output_cta(const float* __restrict__ pts, const Hull
         for (int i = 0; i < F.y; i++) posn[pidx(P4[corners[F.x + i]])] = 1;
     }
     __syncthreads();
-    // exclusive scan over input indices -> output position
-    __shared__ int s_carry;
-    if (tid == 0) s_carry = 0;
-    __syncthreads();
-    for (int base = 0; base < n; base += HULL_NT) {
-        int i = base + tid;
-        int v = (i < n) ? posn[i] : 0;
-        int tot;
-        int ex = block_exclusive_scan(v, sh.scan, &tot);
-        if (i < n) posn[i] = v ? (s_carry + ex) : -1;
-        __syncthreads();
-        if (tid == 0) s_carry += tot;
-        __syncthreads();
-    }
-    const int nv_out = s_carry;
+    // input index -> output position (rank among the corners), -1 if none
+    const int nv_out = cta_rank_flags_inplace(posn, n, sh.scan);
     // triangles per owner (face's smallest corner)
     for (int f = tid; f < nfaces; f += HULL_NT) {
         int2 F = faces[f];
@@ -1544,19 +1531,7 @@ static __device__ void hull_output_cta(const float* __restrict__ pts, const Hull
         atomicAdd(&ocnt[posn[pidx(P4[corners[F.x + mi]])]], F.y - 2);
     }
     __syncthreads();
-    if (tid == 0) s_carry = 0;
-    __syncthreads();
-    for (int base = 0; base < nv_out; base += HULL_NT) {
-        int i = base + tid;
-        int v = (i < nv_out) ? ocnt[i] : 0;
-        int tot;
-        int ex = block_exclusive_scan(v, sh.scan, &tot);
-        if (i < nv_out) ocnt[i] = s_carry + ex;
-        __syncthreads();
-        if (tid == 0) s_carry += tot;
-        __syncthreads();
-    }
-    const int nt_out = s_carry;
+    const int nt_out = cta_scan_inplace(ocnt, nv_out, sh.scan);   // owner -> first triangle slot
     bool fits = nv_out <= max_hv && nt_out <= max_ht && !err0;
     if (fits) {
         for (int f = tid; f < nfaces; f += HULL_NT) {
