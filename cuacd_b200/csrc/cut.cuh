@@ -219,6 +219,50 @@ static __device__ __forceinline__ void cut_for_ilp(int n, Load load, Store store
     }
 }
 
+// Corner indices and vertex signs of the triangles t = base + u * CUT_NT,
+// u < CUT_ILP (those below nt): all index loads first, then all sign loads.
+static __device__ __forceinline__ void cut_load_tris(const int* __restrict__ tris, const signed char* sg, int nt,
+                                                     int base, int (&ix)[CUT_ILP][3], int (&sv)[CUT_ILP][3])
+{
+    #pragma unroll
+    for (int u = 0; u < CUT_ILP; u++) {
+        const int t = base + u * CUT_NT;
+        #pragma unroll
+        for (int k = 0; k < 3; k++) ix[u][k] = t < nt ? tris[3 * t + k] : 0;
+    }
+    #pragma unroll
+    for (int u = 0; u < CUT_ILP; u++)
+        #pragma unroll
+        for (int k = 0; k < 3; k++) sv[u][k] = base + u * CUT_NT < nt ? sg[ix[u][k]] : 0;
+}
+
+// Corners of the split triangles t = base + u * CUT_NT below n and whether
+// each lies on the cut (a new vertex, or an input vertex of sign 0).
+static __device__ __forceinline__ void cut_load_on_cut(const int* tri, const signed char* sg, int nv, int n,
+                                                       int base, int (&ix)[CUT_ILP][3], int (&on)[CUT_ILP][3])
+{
+    #pragma unroll
+    for (int u = 0; u < CUT_ILP; u++) {
+        const int t = base + u * CUT_NT;
+        #pragma unroll
+        for (int k = 0; k < 3; k++) ix[u][k] = t < n ? tri[3 * t + k] : 0;
+    }
+    #pragma unroll
+    for (int u = 0; u < CUT_ILP; u++)
+        #pragma unroll
+        for (int k = 0; k < 3; k++)
+            on[u][k] = base + u * CUT_NT < n && (ix[u][k] >= nv || sg[ix[u][k]] == 0);
+}
+
+// +1 / -1: every vertex on the positive / negative side or on the plane,
+// and one off it -- the triangle is its own piece on that side; 0: the
+// triangle crosses the plane or lies in it.
+static __device__ __forceinline__ int cut_tri_side(const int (&s)[3])
+{
+    const int hp = s[0] > 0 || s[1] > 0 || s[2] > 0, hn = s[0] < 0 || s[1] < 0 || s[2] < 0;
+    return hp && !hn ? 1 : (hn && !hp ? -1 : 0);
+}
+
 // CTA-wide minimum of (key, idx) pairs in lexicographic order, returned to
 // every thread (all CUT_NT threads call).
 static __device__ void cut_cta_lexmin(double& key, int& idx)
@@ -620,10 +664,15 @@ static __device__ void cut_cta(const float* __restrict__ verts, int nv, const in
         __syncthreads();
         // count crossing occurrences, and sides present
         int occ = 0, anyp = 0, anyn = 0;
-        for (int t = tid; t < nt; t += CUT_NT) {
-            int s0 = sg[tris[3 * t]], s1 = sg[tris[3 * t + 1]], s2 = sg[tris[3 * t + 2]];
-            int e0 = s0 >= 0, e1 = s1 >= 0, e2 = s2 >= 0;
-            occ += (e0 != e1) + (e1 != e2) + (e2 != e0);
+        for (int base = tid; base < nt; base += CUT_ILP * CUT_NT) {
+            int ix[CUT_ILP][3], sv[CUT_ILP][3];
+            cut_load_tris(tris, sg, nt, base, ix, sv);
+            #pragma unroll
+            for (int u = 0; u < CUT_ILP; u++) {
+                if (base + u * CUT_NT >= nt) continue;
+                const int e0 = sv[u][0] >= 0, e1 = sv[u][1] >= 0, e2 = sv[u][2] >= 0;
+                occ += (e0 != e1) + (e1 != e2) + (e2 != e0);
+            }
         }
         for (int v = tid; v < nv; v += CUT_NT) { anyp |= sg[v] > 0; anyn |= sg[v] < 0; }
         occ = warp_sum_i(occ);
@@ -755,19 +804,15 @@ static __device__ void cut_cta(const float* __restrict__ verts, int nv, const in
     if (tid == 0) sh.cnt[3] = 0;
     __syncthreads();
     // collection order does not matter: the keys are sorted next
-    for (int base = 0; base < nt; base += CUT_NT) {     // uniform trip count (warp shuffles)
-        int t = base + tid;
-        unsigned long long k[3]; int m = 0;
-        if (t < nt) {
-            for (int e = 0; e < 3; e++) {
-                int va = tris[3 * t + e], vb = tris[3 * t + (e + 1) % 3];
-                int ea = sg[va] >= 0, eb = sg[vb] >= 0;
-                if (ea != eb) {
-                    int lo = min(va, vb), hi = max(va, vb);
-                    k[m++] = ((unsigned long long)(unsigned)lo << 32) | (unsigned)hi;
-                }
-            }
-        }
+    for (int base = 0; base < nt; base += CUT_ILP * CUT_NT) {     // uniform trip count (warp shuffles)
+        int ix[CUT_ILP][3], sv[CUT_ILP][3];
+        cut_load_tris(tris, sg, nt, base + tid, ix, sv);
+        int m = 0;
+        #pragma unroll
+        for (int u = 0; u < CUT_ILP; u++)
+            #pragma unroll
+            for (int e = 0; e < 3; e++)
+                m += base + tid + u * CUT_NT < nt && (sv[u][e] >= 0) != (sv[u][(e + 1) % 3] >= 0);
         int x = m;                                      // warp inclusive scan of the counts
         #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
@@ -778,7 +823,16 @@ static __device__ void cut_cta(const float* __restrict__ verts, int nv, const in
         const int wt = __shfl_sync(FULL_MASK, x, 31);
         if (lane == 31 && wt) wb = atomicAdd(&sh.cnt[3], wt);
         wb = __shfl_sync(FULL_MASK, wb, 31);
-        for (int j = 0; j < m; j++) ce[wb + x - m + j] = k[j];
+        int j = wb + x - m;
+        #pragma unroll
+        for (int u = 0; u < CUT_ILP; u++)
+            #pragma unroll
+            for (int e = 0; e < 3; e++) {
+                if (base + tid + u * CUT_NT >= nt || (sv[u][e] >= 0) == (sv[u][(e + 1) % 3] >= 0)) continue;
+                const int va = ix[u][e], vb = ix[u][(e + 1) % 3];
+                const int lo = min(va, vb), hi = max(va, vb);
+                ce[j++] = ((unsigned long long)(unsigned)lo << 32) | (unsigned)hi;
+            }
     }
     __syncthreads();
     cta_sort_u64(ce, n_occ);
@@ -898,9 +952,28 @@ static __device__ void cut_cta(const float* __restrict__ verts, int nv, const in
         }
         return make_int2(np_, nn_);
     };
-    for (int t = tid; t < nt; t += CUT_NT) {
-        int2 c = split(t, 0, nullptr, nullptr, 0, 0);
-        poff[t] = c.x; noff[t] = c.y;
+    // A triangle with no vertex on the other side and one off the plane is
+    // its own single piece (split()'s first case); the batches below handle
+    // it inline and leave the rest (crossing or coplanar) to split().
+    for (int base = tid; base < nt; base += CUT_ILP * CUT_NT) {
+        int ix[CUT_ILP][3], sv[CUT_ILP][3];
+        cut_load_tris(tris, sg, nt, base, ix, sv);
+        unsigned rare = 0;
+        #pragma unroll
+        for (int u = 0; u < CUT_ILP; u++) {
+            const int t = base + u * CUT_NT;
+            if (t >= nt) continue;
+            const int side = cut_tri_side(sv[u]);
+            if (side == 0) { rare |= 1u << u; continue; }
+            poff[t] = side > 0; noff[t] = side < 0;
+        }
+        #pragma unroll 1
+        for (int u = 0; u < CUT_ILP; u++)
+            if (rare >> u & 1) {
+                const int t = base + u * CUT_NT;
+                const int2 c = split(t, 0, nullptr, nullptr, 0, 0);
+                poff[t] = c.x; noff[t] = c.y;
+            }
     }
     __syncthreads();
     const int n_pos = cta_scan_inplace(poff, nt, sh.scan);
@@ -911,7 +984,31 @@ static __device__ void cut_cta(const float* __restrict__ verts, int nv, const in
     if (s_err) goto fail_out;
     int* ptri = (int*)sh.ptr[11];
     int* ntri = (int*)sh.ptr[12];
-    for (int t = tid; t < nt; t += CUT_NT) split(t, 1, ptri, ntri, poff[t], noff[t]);
+    for (int base = tid; base < nt; base += CUT_ILP * CUT_NT) {
+        int ix[CUT_ILP][3], sv[CUT_ILP][3], po[CUT_ILP], no[CUT_ILP];
+        #pragma unroll
+        for (int u = 0; u < CUT_ILP; u++) {
+            const int t = base + u * CUT_NT;
+            if (t < nt) { po[u] = poff[t]; no[u] = noff[t]; }
+        }
+        cut_load_tris(tris, sg, nt, base, ix, sv);
+        unsigned rare = 0;
+        #pragma unroll
+        for (int u = 0; u < CUT_ILP; u++) {
+            const int t = base + u * CUT_NT;
+            if (t >= nt) continue;
+            const int side = cut_tri_side(sv[u]);
+            if (side == 0) { rare |= 1u << u; continue; }
+            int* dst = side > 0 ? ptri + 3 * po[u] : ntri + 3 * no[u];
+            dst[0] = ix[u][0]; dst[1] = ix[u][1]; dst[2] = ix[u][2];
+        }
+        #pragma unroll 1
+        for (int u = 0; u < CUT_ILP; u++)
+            if (rare >> u & 1) {
+                const int t = base + u * CUT_NT;
+                split(t, 1, ptri, ntri, poff[t], noff[t]);
+            }
+    }
     __syncthreads();
     tph[2] = clock64();
     // ---------------- boundary of the positive side among edges on the cut
@@ -919,12 +1016,15 @@ static __device__ void cut_cta(const float* __restrict__ verts, int nv, const in
     if (tid == 0) sh.cnt[5] = 0;
     __syncthreads();
     int nbc_local = 0;
-    for (int t = tid; t < n_pos; t += CUT_NT)
-        for (int e = 0; e < 3; e++) {
-            int a = ptri[3 * t + e], b = ptri[3 * t + (e + 1) % 3];
-            bool ona = a >= nv || sg[a] == 0, onb = b >= nv || sg[b] == 0;
-            nbc_local += (ona && onb);
-        }
+    for (int base = tid; base < n_pos; base += CUT_ILP * CUT_NT) {
+        int ix[CUT_ILP][3], on[CUT_ILP][3];
+        cut_load_on_cut(ptri, sg, nv, n_pos, base, ix, on);
+        #pragma unroll
+        for (int u = 0; u < CUT_ILP; u++)
+            #pragma unroll
+            for (int e = 0; e < 3; e++)
+                nbc_local += base + u * CUT_NT < n_pos && on[u][e] && on[u][(e + 1) % 3];
+    }
     nbc_local = warp_sum_i(nbc_local);
     if (lane == 0) atomicAdd(&sh.cnt[5], nbc_local);
     __syncthreads();
@@ -935,16 +1035,20 @@ static __device__ void cut_cta(const float* __restrict__ verts, int nv, const in
     unsigned long long* bk = (unsigned long long*)sh.ptr[13];
     if (tid == 0) sh.cnt[6] = 0;
     __syncthreads();
-    for (int t = tid; t < n_pos; t += CUT_NT)
-        for (int e = 0; e < 3; e++) {
-            int a = ptri[3 * t + e], b = ptri[3 * t + (e + 1) % 3];
-            bool ona = a >= nv || sg[a] == 0, onb = b >= nv || sg[b] == 0;
-            if (ona && onb) {
-                int lo = min(a, b), hi = max(a, b);
-                int s = atomicAdd(&sh.cnt[6], 1);
+    for (int base = tid; base < n_pos; base += CUT_ILP * CUT_NT) {
+        int ix[CUT_ILP][3], on[CUT_ILP][3];
+        cut_load_on_cut(ptri, sg, nv, n_pos, base, ix, on);
+        #pragma unroll
+        for (int u = 0; u < CUT_ILP; u++)
+            #pragma unroll
+            for (int e = 0; e < 3; e++) {
+                if (base + u * CUT_NT >= n_pos || !on[u][e] || !on[u][(e + 1) % 3]) continue;
+                const int a = ix[u][e], b = ix[u][(e + 1) % 3];
+                const int lo = min(a, b), hi = max(a, b);
+                const int s = atomicAdd(&sh.cnt[6], 1);
                 bk[s] = ((unsigned long long)(unsigned)lo << 33) | ((unsigned long long)(unsigned)hi << 1) | (a > b ? 1ull : 0ull);
             }
-        }
+    }
     __syncthreads();
     cta_sort_u64(bk, nbc);
     // unmatched directed edges -> be (a<<32|b), sorted
