@@ -168,7 +168,7 @@ def _decompose_worker(q_in, q_out, lock, opts, factory, current):
             if item is None:
                 break
             rel, v, t = item
-            current.value = rel.encode("utf-8", "replace")[:_CUR_BYTES - 1]
+            set_current(current, rel)
             t0 = time.perf_counter()
             parts = None
             for attempt in (0, 1):
@@ -206,21 +206,33 @@ def supervise(workers, poll=0.05):
     """Wait for every (name, process) to end.  The first that exits with a
     non-zero code ends the others (they may be blocked on a queue it will
     never serve); returns its (name, exit code), or None when all end
-    cleanly."""
+    cleanly.  Each poll takes one liveness snapshot, so a worker that fails
+    just as the last one ends is still seen."""
     while True:
-        for name, p in workers:
-            if not p.is_alive() and p.exitcode not in (0, None):
+        alive = [p.is_alive() for _, p in workers]
+        for (name, p), up in zip(workers, alive):
+            if not up and p.exitcode not in (0, None):
                 for _, q in workers:
                     if q.is_alive():
                         q.terminate()
                 for _, q in workers:
                     q.join()
                 return name, p.exitcode
-        if all(not p.is_alive() for _, p in workers):
+        if not any(alive):
             for _, p in workers:
                 p.join()
             return None
         time.sleep(poll)
+
+
+def set_current(buf, name):
+    """Record in the shared buffer the mesh the decomposer is on (truncated
+    to the buffer; a shorter name leaves no tail of the previous one)."""
+    buf.value = str(name).encode("utf-8", "replace")[:_CUR_BYTES - 1]
+
+
+def get_current(buf):
+    return bytes(buf.value).decode("utf-8", "replace")
 
 
 def run_pipeline(meshes, opts, factory):
@@ -240,7 +252,7 @@ def run_pipeline(meshes, opts, factory):
     name, code = failed
     where = ""
     if name == "decomposer":
-        mesh = bytes(current.value).decode("utf-8", "replace")
+        mesh = get_current(current)
         if mesh:
             where = f" while decomposing {mesh!r}"
     cause = ("a native crash (killed by a signal, no traceback)" if code < 0

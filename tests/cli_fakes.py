@@ -65,3 +65,35 @@ def flaky_factory(device, pool_bytes):
 
 def failing_factory(device, pool_bytes):
     return FakeContext(fail=True)
+
+
+# ---- supervisor tests ------------------------------------------------------
+class FakeProc:
+    """Process stand-in: alive for `ticks` liveness polls, then exited with
+    `code`."""
+
+    def __init__(self, code, ticks=0):
+        self.code, self.ticks, self.exitcode, self.terminated = code, ticks, None, False
+
+    def is_alive(self):
+        if self.ticks > 0:
+            self.ticks -= 1
+            return True
+        self.exitcode = self.code
+        return False
+
+    def terminate(self):
+        self.terminated = True
+        self.ticks = 0
+
+    def join(self, timeout=None):
+        pass
+
+
+def exit_after_one_item(q):
+    q.get()
+    os._exit(3)                        # no traceback, no end-of-stream marker
+
+
+def wait_for_item(q):
+    q.get()

@@ -288,3 +288,50 @@ def test_serial_and_bench_modes(tmp_path, capfd):
 def test_no_meshes(tmp_path, capfd):
     (tmp_path / "empty").mkdir()
     assert cli.main([str(tmp_path / "empty"), str(tmp_path / "o")], context_factory=cli_fakes.ok_factory) == 1
+
+
+def test_supervisor_clean_and_failed_workers():
+    assert cli.supervise([("loader", cli_fakes.FakeProc(0)), ("saver", cli_fakes.FakeProc(0))], poll=0) is None
+    survivor = cli_fakes.FakeProc(0, ticks=10)
+    assert cli.supervise([("decomposer", cli_fakes.FakeProc(-11)), ("loader", survivor)], poll=0) == \
+        ("decomposer", -11)
+    assert survivor.terminated
+
+
+def test_supervisor_sees_a_failure_on_the_last_poll():
+    # both end on the same poll; the non-zero one must not pass as a clean end
+    assert cli.supervise([("loader", cli_fakes.FakeProc(0)), ("saver", cli_fakes.FakeProc(3))], poll=0) == \
+        ("saver", 3)
+    # the failing one is still alive on the first poll and ends with the other
+    assert cli.supervise([("saver", cli_fakes.FakeProc(3, ticks=1)), ("loader", cli_fakes.FakeProc(0, ticks=1))],
+                         poll=0) == ("saver", 3)
+
+
+def test_supervisor_breaks_a_real_deadlock():
+    """A consumer that dies after one item leaves its peer blocked on a queue
+    forever; the supervisor ends the peer and reports the dead one."""
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q1, q2 = ctx.Queue(maxsize=2), ctx.Queue(maxsize=2)
+    dead = ctx.Process(target=cli_fakes.exit_after_one_item, args=(q1,))
+    blocked = ctx.Process(target=cli_fakes.wait_for_item, args=(q2,))
+    dead.start()
+    blocked.start()
+    q1.put(("mesh.obj", None, None))
+    try:
+        assert cli.supervise([("decomposer", dead), ("saver", blocked)]) == ("decomposer", 3)
+    finally:
+        dead.join(10)
+        blocked.join(10)
+    assert not blocked.is_alive()
+
+
+def test_current_mesh_buffer():
+    import multiprocessing as mp
+    buf = mp.get_context("spawn").Array("c", cli._CUR_BYTES)
+    cli.set_current(buf, "dir/a.obj")
+    assert cli.get_current(buf) == "dir/a.obj"
+    cli.set_current(buf, "b.obj")                      # no tail of the longer name
+    assert cli.get_current(buf) == "b.obj"
+    cli.set_current(buf, "x" * (cli._CUR_BYTES + 64))  # truncated, not dropped
+    assert cli.get_current(buf) == "x" * (cli._CUR_BYTES - 1)
