@@ -131,6 +131,12 @@ _opt("cuacd_eval_candidates_pruned_device", _I, [_P, _P, _P, _I, _P, _I, _F, _P,
                                                  _P, _P, _P, _P, _P])
 _opt("cuacd_eval_candidates_pruned", _I, [_P, _P, _P, _I, _P, _I, _F, _P, _I, _I, _F, _I, _I, _I, _F,
                                           _P, _P, _P, _P])
+_opt("gpu_preprocess", _I, [_P, _P, _I, _P, _I, _I, ctypes.POINTER(ctypes.POINTER(ctypes.c_float)),
+                            ctypes.POINTER(_I), ctypes.POINTER(ctypes.POINTER(ctypes.c_int)), ctypes.POINTER(_I)])
+_opt("cuacd_remesh_case_table", None, [_P])
+_libc_free = ctypes.CDLL(None).free          # gpu_preprocess's outputs come from malloc
+_libc_free.argtypes = [_P]
+_libc_free.restype = None
 
 
 def _fn(name):
@@ -224,7 +230,7 @@ class Context:
     def launch_count(self):
         return int(_lib.cuacd_launch_count(self._h))
 
-    # -- out of scope in this engine ---------------------------------------
+    # -- front end: audit and remesh ----------------------------------------
     def check_mesh(self, verts, tris):
         """Topology audit on the GPU (cuacd/__init__.py:124-152): a dict of
         booleans and the raw verdict bitmask -- watertight (no edge used by
@@ -247,7 +253,29 @@ class Context:
         }
 
     def preprocess(self, verts, tris, resolution=64):
-        raise NotImplementedError("preprocess (remeshing) is outside the candidate-evaluation path")
+        """Remesh into a watertight, manifold, consistently oriented mesh
+        (cuacd/__init__.py:158-180): the mesh is normalised into a padded
+        grid of resolution^3 nodes (a power of two >= 8, at most 1,024), the
+        distance to it within 3 cells is signed by a flood fill from the
+        grid's boundary, moved out by 0.9 cells and contoured by marching
+        cubes.  Returns (verts float32 (n, 3), tris int32 (m, 3))."""
+        r = int(resolution)
+        if r & (r - 1) or r < 8:
+            raise ValueError("resolution must be a power of two >= 8")
+        v = _as_f32(verts).reshape(-1, 3)
+        t = _as_i32(tris).reshape(-1, 3)
+        pv, pt = ctypes.POINTER(ctypes.c_float)(), ctypes.POINTER(ctypes.c_int)()
+        nv, nt = ctypes.c_int(0), ctypes.c_int(0)
+        rc = _fn("gpu_preprocess")(self._h, _ptr(v), len(v), _ptr(t), len(t), r, ctypes.byref(pv), ctypes.byref(nv),
+                                   ctypes.byref(pt), ctypes.byref(nt))
+        try:
+            self._check(rc)
+            out_v = np.ctypeslib.as_array(pv, (nv.value, 3)).copy() if nv.value else np.zeros((0, 3), np.float32)
+            out_t = np.ctypeslib.as_array(pt, (nt.value, 3)).copy() if nt.value else np.zeros((0, 3), np.int32)
+        finally:
+            _libc_free(ctypes.cast(pv, ctypes.c_void_p))
+            _libc_free(ctypes.cast(pt, ctypes.c_void_p))
+        return out_v, out_t
 
     # -- hulls --------------------------------------------------------------
     @staticmethod

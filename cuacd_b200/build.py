@@ -26,9 +26,10 @@ def sources():
     return sorted(f for f in os.listdir(CSRC) if f.endswith(".cu"))
 
 
-# Per-file flags: the FP32/FP64 expressions of the cut, the plane generator
-# and the audit's zero-area test must not be contracted.
-PER_FILE = {"cut.cu": ["-fmad=false"], "concave.cu": ["-fmad=false"], "audit.cu": ["-fmad=false"]}
+# Per-file flags: the FP32/FP64 expressions of the cut, the plane generator,
+# the audit's zero-area test and the remesh must not be contracted.
+PER_FILE = {"cut.cu": ["-fmad=false"], "concave.cu": ["-fmad=false"], "audit.cu": ["-fmad=false"],
+            "remesh.cu": ["-fmad=false"]}
 
 
 def _compile(src, extra):

@@ -19,11 +19,10 @@ the three steps in this process, one mesh at a time; --bench does the same
 with a fresh context per mesh, an untimed first run (which sets the pool's
 high-water mark) and a timed second run.
 
-The remesh front end of the reference (`--preprocess`, Context.preprocess)
-is not part of this library: with `--preprocess on` every mesh fails with
-that message, and with the default `auto` a mesh that the GPU audit flags
-(open, non-manifold or misoriented) is decomposed as it is, with a note on
-stderr.
+Before the search a mesh is remeshed (Context.preprocess at
+--preprocess-resolution) when --preprocess is `on`, or, with the default
+`auto`, when the GPU audit flags it (open, non-manifold or misoriented),
+as the reference does (cuacd/cli.py:50-55).
 """
 import argparse
 import multiprocessing
@@ -89,25 +88,21 @@ def build_parser():
                     help="skip the greedy merge-hulls pass")
     ap.add_argument("--serial", action="store_true", help="load, decompose and save in this process")
     ap.add_argument("--preprocess", choices=["auto", "on", "off"], default="auto",
-                    help="remesh front end: not part of this library (see the module docstring)")
-    ap.add_argument("--preprocess-resolution", type=int, default=64, help="accepted and unused")
+                    help="remesh to a watertight manifold first: auto (when the audit flags the mesh), on, off")
+    ap.add_argument("--preprocess-resolution", type=int, default=64,
+                    help="remesh grid resolution, a power of two (64)")
     ap.add_argument("--bench", action="store_true",
                     help="per mesh: fresh context, untimed run, timed run, pool high-water mark")
     return ap
 
 
-def decompose_mesh(ctx, verts, tris, opts, log=None):
+def decompose_mesh(ctx, verts, tris, opts):
     """Parts of one mesh in its own coordinates: [(verts, tris)] of the
     parts' convex hulls (or, with opts.parts, of the cut parts).  The mesh
     is centred on its bounding box and scaled by half its longest side
     before the search and mapped back after (cuacd/cli.py:50-84)."""
-    if opts.preprocess == "on":
-        raise RuntimeError("the remesh front end (--preprocess on) is not part of this library")
-    if opts.preprocess == "auto" and log is not None and len(tris):
-        audit = ctx.check_mesh(verts, tris)
-        if audit["needs_remesh"]:
-            log(f"mesh audit flags 0x{audit['flags']:x} (open, non-manifold or misoriented); "
-                "decomposed as it is, without a remesh")
+    if opts.preprocess == "on" or (opts.preprocess == "auto" and ctx.check_mesh(verts, tris)["needs_remesh"]):
+        verts, tris = ctx.preprocess(verts, tris, resolution=opts.preprocess_resolution)
     lo, hi = verts.min(axis=0), verts.max(axis=0)
     center = (lo + hi) / 2
     extent = float((hi - lo).max())
@@ -173,7 +168,7 @@ def _decompose_worker(q_in, q_out, lock, opts, factory, current):
             parts = None
             for attempt in (0, 1):
                 try:
-                    parts = decompose_mesh(ctx, v, t, opts, log=lambda m: _say(lock, f"{rel}: {m}", err=True))
+                    parts = decompose_mesh(ctx, v, t, opts)
                     break
                 except Exception as e:
                     if attempt:
@@ -274,12 +269,11 @@ def run_serial(meshes, opts, factory):
         except Exception as e:
             print(f"{rel}: context error: {e}", file=sys.stderr, flush=True)
             continue
-        log = lambda m, rel=rel: print(f"{rel}: {m}", file=sys.stderr, flush=True)
         try:
             if opts.bench:
-                decompose_mesh(ctx, v, t, opts, log)            # untimed: pool high-water mark
+                decompose_mesh(ctx, v, t, opts)                 # untimed: pool high-water mark
             t0 = time.perf_counter()
-            parts = decompose_mesh(ctx, v, t, opts, None if opts.bench else log)
+            parts = decompose_mesh(ctx, v, t, opts)
             dt = time.perf_counter() - t0
         except Exception as e:
             print(f"{rel}: decompose error: {e}", file=sys.stderr, flush=True)

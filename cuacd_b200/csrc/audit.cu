@@ -148,16 +148,3 @@ extern "C" int gpu_mesh_audit(gpu_ctx_t ctx, const float* verts, int n_verts, co
     *out_flags = f;
     return 0;
 }
-
-// The reference's PaMO remesh (csrc/preprocess.c) is not part of this library.
-extern "C" int gpu_preprocess(gpu_ctx_t ctx, const float* verts, int nv, const int* tris, int nt, int resolution,
-                              float** out_verts, int* out_nv, int** out_tris, int* out_nt)
-{
-    (void)verts; (void)nv; (void)tris; (void)nt; (void)resolution;
-    if (out_verts) *out_verts = nullptr;
-    if (out_nv) *out_nv = 0;
-    if (out_tris) *out_tris = nullptr;
-    if (out_nt) *out_nt = 0;
-    if (!ctx) return -1;
-    return ctx_fail(ctx, -1, "preprocess (the PaMO remesh front end) is not part of this library");
-}

@@ -118,13 +118,22 @@ int gpu_test_plane_cut(gpu_ctx_t ctx,
 int gpu_mesh_audit(gpu_ctx_t ctx, const float* verts, int n_verts, const int* tris, int n_tris,
                    unsigned int* out_flags);
 
-/* Stands in for gpu_preprocess (csrc/preprocess.h:17-24), the PaMO remesh
- * of the reference's front end, which this library does not build: it
- * writes NULL / 0 to the outputs and returns -1 with the reason in
- * gpu_last_error, so the reference's CPython module links unchanged and its
- * preprocess() raises RuntimeError. */
+/* Replaces gpu_preprocess (csrc/preprocess.h:17-24): remesh a triangle
+ * soup into a watertight, manifold, consistently oriented surface on a
+ * resolution^3 grid (a power of two in [8, 1024]) -- distance field within
+ * 3 cells of the triangles, signed by a flood fill from the grid boundary,
+ * moved out by 0.9 cells, contoured by marching cubes.  *out_verts /
+ * *out_tris are malloc'd (the caller frees them with free()); returns 0, 1
+ * for bad arguments (a null pointer, an empty mesh, an index outside
+ * [0, nv), a bad resolution, no extent), or a KERR_* / CUDA error. */
 int gpu_preprocess(gpu_ctx_t ctx, const float* verts, int nv, const int* tris, int nt,
                    int resolution, float** out_verts, int* out_nv, int** out_tris, int* out_nt);
+
+/* The remesh's marching-cubes case table (no counterpart in the reference,
+ * which contours with a dual method): per case, 17 ints -- the number of
+ * loops, four loop lengths, twelve cube edges (loops one after another, -1
+ * padded).  Host only; for checking the table. */
+void cuacd_remesh_case_table(int* out);
 
 /* Replaces gpu_test_postprocess_dc (csrc/postprocess.h:20-27): split a mesh
  * into its vertex-connected components.  Component c's vertices go to

@@ -1,0 +1,316 @@
+"""CPU restatement of the remesh front end (Context.preprocess), for tests
+only: the CUDA path in cuacd_b200/csrc/remesh.cu is checked against it
+value for value.  Test infrastructure; nothing in the library imports it.
+
+The pipeline follows the reference's stages and conventions
+(csrc/preprocess.c:1-13, 605-700): the mesh is normalised into a padded
+unit cube, p_norm = ((p - vmin) / extent + band) / margin with band = 3/R
+and margin = 1 + 2 band, and grid node g samples p_norm = (g + 0.5) / R;
+an unsigned distance field is computed within `band` (3 cells) of the
+triangles, signed by a flood fill from the grid's boundary that no grid
+edge crossed by a triangle lets through, shifted by 0.9/R (one node in
+0.9 cells of the surface already counts as inside, so the surface grows by
+0.9 cells), and contoured at 0; vertices map back by
+p = ((g + 0.5) / R * margin - band) * extent + vmin.  The reference reaches
+the same stages through a third-party rasteriser and a dual marching-cubes
+port; the contouring here is marching cubes with a case table generated
+from one rule (below), which makes every output closed, manifold and
+consistently oriented.  Parity with the reference is on the properties its
+own tests check (tests/test_preprocess.py), not on vertex positions.
+
+Everything is in grid units (u = p_norm * R - 0.5, nodes at integers) and
+float64 in a fixed operation order, which the CUDA path repeats (compiled
+without FMA contraction):
+  squared distance node-triangle: min of the three segment distances and,
+    when the node projects inside, the plane distance;
+  a node keeps float32(d2) when d2 <= 9 (band squared), the least over
+    triangles; other nodes are far;
+  a grid edge (node, node + e_k) is crossed when the line through the
+    node's other two coordinates meets the triangle (inclusive 2D test in
+    the projection) at a k-coordinate z with floor(z) = node_k;
+  field = (outside ? u : -u) - 0.9 with u = sqrt(d2) (1e9 when far),
+    rounded to float32; a node is inside when field < 0.
+"""
+import numpy as np
+
+BAND_CELLS = 3.0
+SHIFT_CELLS = 0.9
+T_CLAMP = 0.01
+FAR_D2 = np.float32(np.finfo(np.float32).max)
+
+# cube corners c: (x, y, z) = (c & 1, c >> 1 & 1, c >> 2 & 1); edges axis by
+# axis, each from the corner with that bit clear
+EDGES = [(c, c | (1 << a), a) for a in range(3) for c in range(8) if not c >> a & 1]
+
+
+def _edge_of(c0, c1):
+    lo, hi = min(c0, c1), max(c0, c1)
+    for e, (a, b, _) in enumerate(EDGES):
+        if (a, b) == (lo, hi):
+            return e
+    raise ValueError("not a cube edge")
+
+
+def _faces():
+    """Each face's corners in counter-clockwise order seen from outside."""
+    out = []
+    for a in range(3):
+        b, c = (a + 1) % 3, (a + 2) % 3
+        for s in (0, 1):
+            cyc = []
+            for (pb, pc) in ((0, 0), (1, 0), (1, 1), (0, 1)):
+                cyc.append((s << a) | (pb << b) | (pc << c))
+            out.append(cyc if s else cyc[::-1])
+    return out
+
+
+def mc_case_table():
+    """Marching-cubes loops of each of the 256 cases: a list of polygons,
+    each a list of cube edges in the order whose right-hand normal points
+    from inside to outside.
+
+    On each face, a segment runs from every edge where the cycle goes from
+    an inside corner to an outside one back to the edge that opened that
+    run of inside corners; on a face with two diagonal inside corners each
+    is cut off by its own segment (the inside is 6-connected), a rule that
+    depends only on the face, so neighbouring cells agree.  Every crossed
+    edge then starts one segment and ends one, and the segments close into
+    loops, each reversed and started at its first edge.  A loop of three
+    is one triangle; a longer one is fanned around a vertex at the mean of
+    its points (a fan from a corner could join two points of one face, as
+    the neighbouring cell may, and four triangles would share that
+    edge)."""
+    faces = _faces()
+    table = []
+    for case in range(256):
+        inside = [bool(case >> c & 1) for c in range(8)]
+        nxt = {}
+        for cyc in faces:
+            st = [inside[q] for q in cyc]
+            for i in range(4):
+                if st[i] and not st[(i + 1) % 4]:              # inside -> outside at edge i
+                    j = i
+                    while st[j]:                                # back to the run's first corner
+                        j = (j - 1) % 4
+                    nxt[_edge_of(cyc[i], cyc[(i + 1) % 4])] = _edge_of(cyc[j], cyc[(j + 1) % 4])
+        seen, out = set(), []
+        for e in range(12):
+            if e not in nxt or e in seen:
+                continue
+            loop = [e]
+            seen.add(e)
+            f = nxt[e]
+            while f != e:
+                loop.append(f)
+                seen.add(f)
+                f = nxt[f]
+            out.append([loop[0]] + loop[1:][::-1])
+        table.append(out)
+    return table
+
+
+def normalise(verts, R):
+    """(grid-unit vertices float64, vmin float32[3], extent float32,
+    band, margin)."""
+    v = np.asarray(verts, np.float32).reshape(-1, 3)
+    vmin, vmax = v.min(0), v.max(0)
+    extent = np.float32(max(vmax[d] - vmin[d] for d in range(3)))
+    band = 3.0 / R
+    margin = 1.0 + 2.0 * band
+    u = ((v.astype(np.float64) - vmin.astype(np.float64)) / np.float64(extent) + band) / margin * R - 0.5
+    return u, vmin, extent, band, margin
+
+
+def _dot(a, b):
+    return a[..., 0] * b[..., 0] + a[..., 1] * b[..., 1] + a[..., 2] * b[..., 2]
+
+
+def _cross(a, b):
+    return np.stack([a[..., 1] * b[..., 2] - a[..., 2] * b[..., 1],
+                     a[..., 2] * b[..., 0] - a[..., 0] * b[..., 2],
+                     a[..., 0] * b[..., 1] - a[..., 1] * b[..., 0]], -1)
+
+
+def _seg_d2(P, A, B):
+    AB = B - A
+    ll = _dot(AB, AB)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        t = np.where(ll > 0, _dot(P - A, AB) / np.where(ll > 0, ll, 1.0), 0.0)
+    t = np.minimum(np.maximum(t, 0.0), 1.0)
+    D = P - (A + t[..., None] * AB)
+    return _dot(D, D)
+
+
+def point_tri_d2(P, A, B, C):
+    """Squared distance of points P (n, 3) to triangle ABC (float64)."""
+    AB, BC, CA = B - A, C - B, A - C
+    n = _cross(AB, C - A)
+    nn = _dot(n, n)
+    d2 = np.minimum(np.minimum(_seg_d2(P, A, B), _seg_d2(P, B, C)), _seg_d2(P, C, A))
+    if nn > 0:
+        s0 = _dot(_cross(AB, P - A), n)
+        s1 = _dot(_cross(BC, P - B), n)
+        s2 = _dot(_cross(CA, P - C), n)
+        dp = _dot(P - A, n)
+        inside = (s0 >= 0) & (s1 >= 0) & (s2 >= 0)
+        d2 = np.where(inside, np.minimum(d2, dp * dp / nn), d2)
+    return d2
+
+
+def distance_grid(u, tris, R):
+    """float32 squared distance per node (x fastest), FAR_D2 beyond the band."""
+    g = np.full((R, R, R), FAR_D2, np.float32)            # [z, y, x]
+    for tri in np.asarray(tris).reshape(-1, 3):
+        A, B, C = u[tri[0]], u[tri[1]], u[tri[2]]
+        lo = np.maximum(np.ceil(np.minimum(np.minimum(A, B), C) - BAND_CELLS), 0).astype(int)
+        hi = np.minimum(np.floor(np.maximum(np.maximum(A, B), C) + BAND_CELLS), R - 1).astype(int)
+        if (hi < lo).any():
+            continue
+        zz, yy, xx = np.meshgrid(np.arange(lo[2], hi[2] + 1), np.arange(lo[1], hi[1] + 1),
+                                 np.arange(lo[0], hi[0] + 1), indexing="ij")
+        P = np.stack([xx, yy, zz], -1).astype(np.float64)
+        d2 = point_tri_d2(P, A, B, C)
+        cand = np.where(d2 <= BAND_CELLS * BAND_CELLS, d2, np.inf).astype(np.float32)
+        sub = g[lo[2]:hi[2] + 1, lo[1]:hi[1] + 1, lo[0]:hi[0] + 1]
+        np.minimum(sub, np.where(np.isinf(cand), FAR_D2, cand), out=sub)
+    return g
+
+
+def _orient(X, Y, Pi, Pj, i, j):
+    return (Y[i] - X[i]) * (Pj - X[j]) - (Y[j] - X[j]) * (Pi - X[i])
+
+
+def crossed_edges(u, tris, R):
+    """bool [3][z, y, x]: grid edge from the node along axis k is crossed."""
+    blk = np.zeros((3, R, R, R), bool)
+    for tri in np.asarray(tris).reshape(-1, 3):
+        A, B, C = u[tri[0]], u[tri[1]], u[tri[2]]
+        for k in range(3):
+            i, j = (k + 1) % 3, (k + 2) % 3
+            area = _orient(A, B, C[i], C[j], i, j)
+            if area == 0:
+                continue
+            a0 = max(int(np.ceil(min(A[i], B[i], C[i]))), 0)
+            a1 = min(int(np.floor(max(A[i], B[i], C[i]))), R - 1)
+            b0 = max(int(np.ceil(min(A[j], B[j], C[j]))), 0)
+            b1 = min(int(np.floor(max(A[j], B[j], C[j]))), R - 1)
+            if a1 < a0 or b1 < b0:
+                continue
+            aa, bb = np.meshgrid(np.arange(a0, a1 + 1, dtype=np.float64), np.arange(b0, b1 + 1, dtype=np.float64),
+                                 indexing="ij")
+            w0 = _orient(B, C, aa, bb, i, j)
+            w1 = _orient(C, A, aa, bb, i, j)
+            w2 = _orient(A, B, aa, bb, i, j)
+            ws = w0 + w1 + w2
+            hit = (((w0 >= 0) & (w1 >= 0) & (w2 >= 0)) | ((w0 <= 0) & (w1 <= 0) & (w2 <= 0))) & (ws != 0)
+            with np.errstate(divide="ignore", invalid="ignore"):
+                z = (w0 * A[k] + w1 * B[k] + w2 * C[k]) / np.where(ws != 0, ws, 1.0)
+            c = np.floor(z)
+            ok = hit & (c >= 0) & (c <= R - 2)
+            for a, b, cc in zip(aa[ok].astype(int), bb[ok].astype(int), c[ok].astype(int)):
+                idx = [0, 0, 0]
+                idx[k], idx[i], idx[j] = cc, a, b
+                blk[k, idx[2], idx[1], idx[0]] = True
+    return blk
+
+
+def outside_nodes(blk, R):
+    """Nodes reachable from the grid's boundary through uncrossed edges."""
+    out = np.zeros((R, R, R), bool)
+    out[0, :, :] = out[-1, :, :] = out[:, 0, :] = out[:, -1, :] = out[:, :, 0] = out[:, :, -1] = True
+    axis_of = {0: 2, 1: 1, 2: 0}                           # grid axis k -> array axis of [z, y, x]
+    while True:
+        before = out.sum()
+        for k in range(3):
+            ax = axis_of[k]
+            o = np.moveaxis(out, ax, 0)
+            b = np.moveaxis(blk[k], ax, 0)
+            for c in range(1, R):
+                o[c] |= o[c - 1] & ~b[c - 1]
+            for c in range(R - 2, -1, -1):
+                o[c] |= o[c + 1] & ~b[c]
+        if out.sum() == before:
+            return out
+
+
+def field(d2, outside):
+    far = d2 == FAR_D2
+    u = np.where(far, 1e9, np.sqrt(d2.astype(np.float64)))
+    return (np.where(outside, u, -u) - SHIFT_CELLS).astype(np.float32)
+
+
+def contour(sd, R, table=None):
+    """Marching cubes of sd < 0: (grid-unit vertices float64, tris int32).
+    Vertices: one per crossed grid edge in edge-id order (3 * node + axis),
+    then the centres of the loops longer than three, by cell (x fastest)
+    and loop.  Triangles: by cell, loop and fan order."""
+    loops = table or mc_case_table()
+    inside = sd < 0
+    # vertices on crossed grid edges, ordered by edge id 3 * node + axis
+    ids = np.full((R, R, R, 3), -1, np.int64)             # [z, y, x, axis]
+    verts = []
+    flat = []
+    for k, ax in ((0, 2), (1, 1), (2, 0)):
+        sl0 = [slice(None)] * 3
+        sl1 = [slice(None)] * 3
+        sl0[ax] = slice(0, R - 1)
+        sl1[ax] = slice(1, R)
+        diff = np.zeros((R, R, R), bool)
+        diff[tuple(sl0)] = inside[tuple(sl0)] != inside[tuple(sl1)]
+        for z, y, x in zip(*np.nonzero(diff)):
+            flat.append((((z * R + y) * R + x) * 3 + k, (x, y, z), k))
+    flat.sort()
+    for vid, (eid, (x, y, z), k) in enumerate(flat):
+        ids[z, y, x, k] = vid
+        n = [x, y, z]
+        n1 = list(n)
+        n1[k] += 1
+        s0 = np.float64(sd[z, y, x])
+        s1 = np.float64(sd[n1[2], n1[1], n1[0]])
+        t = s0 / (s0 - s1)
+        t = min(max(t, T_CLAMP), 1.0 - T_CLAMP)
+        p = [float(x), float(y), float(z)]
+        p[k] = p[k] + t
+        verts.append(p)
+    tris, centres = [], []
+    nedge = len(verts)
+    for z in range(R - 1):
+        for y in range(R - 1):
+            for x in range(R - 1):
+                case = 0
+                for c in range(8):
+                    if inside[z + (c >> 2 & 1), y + (c >> 1 & 1), x + (c & 1)]:
+                        case |= 1 << c
+                for poly in loops[case]:
+                    vid = []
+                    for e in poly:
+                        c0, _, k = EDGES[e]
+                        vid.append(ids[z + (c0 >> 2 & 1), y + (c0 >> 1 & 1), x + (c0 & 1), k])
+                    if len(vid) == 3:
+                        tris.append(vid)
+                        continue
+                    cx = cy = cz = 0.0
+                    for q in vid:
+                        cx += verts[q][0]; cy += verts[q][1]; cz += verts[q][2]
+                    m = float(len(vid))
+                    centre = nedge + len(centres)
+                    centres.append([cx / m, cy / m, cz / m])
+                    for i in range(len(vid)):
+                        tris.append([centre, vid[i], vid[(i + 1) % len(vid)]])
+    allv = np.asarray(verts + centres, np.float64).reshape(-1, 3)
+    return allv, np.asarray(tris, np.int32).reshape(-1, 3)
+
+
+def remesh(verts, tris, R):
+    """(verts float32, tris int32) of the remeshed surface."""
+    if R < 8 or R & (R - 1):
+        raise ValueError("resolution must be a power of two >= 8")
+    u, vmin, extent, band, margin = normalise(verts, R)
+    if not extent > 0:
+        raise ValueError("the mesh has no extent")
+    d2 = distance_grid(u, tris, R)
+    out = outside_nodes(crossed_edges(u, tris, R), R)
+    sd = field(d2, out)
+    gv, gt = contour(sd, R)
+    p = ((gv + 0.5) / R * margin - band) * np.float64(extent) + vmin.astype(np.float64)
+    return p.astype(np.float32), gt

@@ -23,13 +23,20 @@ def box_of(v):
 class FakeContext:
     """Every mesh gives two parts: (the mesh, its hull = the mesh) and
     (its bounding box, the box).  fail=True raises on every call; a mesh of
-    exactly `crash_nv` vertices kills the process."""
+    exactly `crash_nv` vertices kills the process.  The audit flags a mesh
+    with an odd triangle count; the remesh replaces a mesh by its bounding
+    box."""
 
     def __init__(self, fail=False, crash_nv=-1):
         self.fail, self.crash_nv, self.closed = fail, crash_nv, False
 
     def check_mesh(self, v, t):
-        return {"needs_remesh": False, "flags": 0}
+        odd = len(t) % 2 == 1
+        return {"needs_remesh": odd, "flags": 4 if odd else 0}
+
+    def preprocess(self, v, t, resolution=64):
+        assert resolution & (resolution - 1) == 0
+        return box_of(v), BOX_T
 
     def lookahead_decompose(self, v, t, **kw):
         if len(v) == self.crash_nv:

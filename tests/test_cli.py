@@ -265,13 +265,19 @@ def test_pipeline_reports_a_dead_decomposer(tmp_path, capfd):
     assert "native crash" in se
 
 
-def test_preprocess_on_is_refused_per_mesh(tmp_path, capfd):
-    src, _ = _tree(tmp_path)
-    out = tmp_path / "out"
-    rc = cli.main([str(src / "a.obj"), str(out), "--preprocess", "on", "--serial"],
-                  context_factory=cli_fakes.ok_factory)
-    so, se = capfd.readouterr()
-    assert rc == 0 and "remesh front end" in se and not (out / "a.glb").exists()
+def test_preprocess_modes(tmp_path, capfd):
+    """auto remeshes only what the audit flags (the fake flags an odd
+    triangle count and remeshes to the bounding box); on always; off never."""
+    src, meshes = _tree(tmp_path)
+    _write_obj(src / "odd.obj", meshes["a"][0], meshes["a"][1][:11])
+    for mode, remeshed in (("auto", {"odd"}), ("on", {"odd", "pyr"}), ("off", set())):
+        out = tmp_path / mode
+        assert cli.main([str(src), str(out), "-r", "--serial", "--preprocess", mode],
+                        context_factory=cli_fakes.ok_factory) == 0
+        for stem, rel in (("odd", "odd.glb"), ("pyr", "sub/pyr.glb")):       # 11 and 6 triangles as given
+            part0 = meshio.read_glb_parts((out / rel).read_bytes())[0]
+            assert (len(part0[2]) == 12) == (stem in remeshed), (mode, stem)
+    capfd.readouterr()
 
 
 def test_serial_and_bench_modes(tmp_path, capfd):

@@ -1,9 +1,8 @@
 """The drop-in boundary from the reference's side, on the CPU: the
 reference's CPython module (csrc/module.c, unmodified) compiles against
 include/ (cuacd_b200.h plus the reference header names that forward to it)
-and links against libcuacd_b200.so alone -- gpu_preprocess included, which
-this library exports as an explicit "not built" error -- and the module it
-makes imports with the reference's full method table."""
+and links against libcuacd_b200.so alone -- gpu_preprocess included -- and
+the module it makes imports with the reference's full method table."""
 import importlib.machinery
 import importlib.util
 import os

@@ -4,7 +4,9 @@ The GLB must hold exactly the hulls that Context.lookahead_decompose gives
 for the loaded mesh with the command's default options, after the
 command's normalisation (centre of the bounding box, half the longest
 side) is undone.  The input is two boxes meeting along an edge: loading
-merges their two shared corners, so they form one non-manifold component."""
+merges their two shared corners, so they form one non-manifold component,
+which the audit flags -- by default the command remeshes it first
+(Context.preprocess at resolution 64), with --preprocess off it does not."""
 import numpy as np
 import pytest
 
@@ -23,7 +25,7 @@ def _volume(v, t):
     return float(np.einsum("ij,ij->i", v[t[:, 0]], np.cross(v[t[:, 1]], v[t[:, 2]])).sum() / 6.0)
 
 
-@pytest.mark.parametrize("mode", [["--serial"], []])
+@pytest.mark.parametrize("mode", [["--serial"], [], ["--serial", "--preprocess", "off"]])
 def test_cli_matches_the_library(ctx, tmp_path, mode, capfd):
     v, t = l_shape()
     src = tmp_path / "in"
@@ -38,6 +40,10 @@ def test_cli_matches_the_library(ctx, tmp_path, mode, capfd):
 
     lv, lt = meshio.load_mesh(src / "ell.obj")
     assert len(lv) == 14                                   # 16 corners, 2 shared
+    audit = ctx.check_mesh(lv, lt)
+    assert audit["needs_remesh"]
+    if "off" not in mode:
+        lv, lt = ctx.preprocess(lv, lt, resolution=64)
     lo, hi = lv.min(axis=0), lv.max(axis=0)
     center = (lo + hi) / 2
     scale = float((hi - lo).max()) / 2

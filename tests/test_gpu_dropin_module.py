@@ -1,9 +1,10 @@
 """The reference's own CPython module (csrc/module.c, unmodified) built
 against this library's headers and linked to libcuacd_b200.so
 (oracle/Makefile.ref: oracle/_ref/_gpu_dropin.so), driven with the
-reference's argument formats (csrc/module.c:159-466): every call lands in
-this library and agrees with this library's own Python API; preprocess,
-which this library does not build, raises RuntimeError."""
+reference's argument formats (csrc/module.c:159-525): every call lands in
+this library and agrees with this library's own Python API, preprocess
+included (a bad resolution raises RuntimeError there, as the module maps
+any non-zero return)."""
 import importlib.machinery
 import importlib.util
 import os
@@ -97,5 +98,10 @@ def test_lookahead_and_preprocess(g, ctx):
         vb, tb, nv, nt = r[:4]
         assert (nv, nt) == (len(pv), len(pt))
         assert np.array_equal(np.frombuffer(vb, np.float32).reshape(nv, 3), pv)
+    vb, tb, pnv, pnt = g.preprocess(v.ctypes.data, len(v), t.ctypes.data, len(t), 64)
+    ov, ot = ctx.preprocess(v, t, resolution=64)
+    assert (pnv, pnt) == (len(ov), len(ot)) and pnt > 0
+    assert np.array_equal(np.frombuffer(vb, np.float32).reshape(pnv, 3), ov)
+    assert np.array_equal(np.frombuffer(tb, np.int32).reshape(pnt, 3), ot)
     with pytest.raises(RuntimeError):
-        g.preprocess(v.ctypes.data, len(v), t.ctypes.data, len(t), 64)
+        g.preprocess(v.ctypes.data, len(v), t.ctypes.data, len(t), 48)
