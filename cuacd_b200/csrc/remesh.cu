@@ -309,10 +309,11 @@ extern "C" int gpu_preprocess(gpu_ctx_t ctx, const float* verts, int nv, const i
     ctx->launches += 3;
     CK(cudaGetLastError());
 
-    // sign: sweeps until a round of the three axes changes nothing
+    // sign: sweeps until a round of the three axes changes nothing (a round
+    // that changes anything adds an outside node, so there are at most N)
     const int line_blocks = (int)(((long long)R * R + RM_NT - 1) / RM_NT);
-    for (int round = 0;; round++) {
-        if (round > 4 * R) return ctx_fail(ctx, KERR_MESH_INVALID, "preprocess: sign fill did not settle");
+    for (long long round = 0;; round++) {
+        if (round > N) return ctx_fail(ctx, KERR_MESH_INVALID, "preprocess: sign fill did not settle");
         CK(cudaMemsetAsync(misc, 0, sizeof(int), s));
         for (int k = 0; k < 3; k++) k_rm_sweep<<<line_blocks, RM_NT, 0, s>>>(outside, blk, R, k, misc);
         ctx->launches += 3;

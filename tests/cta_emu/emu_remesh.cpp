@@ -89,7 +89,7 @@ int main(int argc, char** argv)
             }
         }
     }
-    for (int round = 0;; round++) {                                                      // k_rm_sweep
+    for (long long round = 0;; round++) {                                                // k_rm_sweep
         bool changed = false;
         for (int k = 0; k < 3; k++) {
             const int i = (k + 1) % 3, j = (k + 2) % 3;
@@ -113,7 +113,7 @@ int main(int argc, char** argv)
                 }
             }
         }
-        if (!changed || round > 4 * R) break;
+        if (!changed || round > N) break;
     }
     std::vector<float> sd(N);                                                            // k_rm_field
     for (long long n = 0; n < N; n++) sd[n] = rm_field(d2[n], outside[n] != 0);
