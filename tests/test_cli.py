@@ -341,3 +341,34 @@ def test_current_mesh_buffer():
     assert cli.get_current(buf) == "b.obj"
     cli.set_current(buf, "x" * (cli._CUR_BYTES + 64))  # truncated, not dropped
     assert cli.get_current(buf) == "x" * (cli._CUR_BYTES - 1)
+
+
+def test_gltf_interleaved_accessor(tmp_path):
+    """POSITION interleaved with a 4-byte attribute (byteStride 16)."""
+    rows = np.zeros(8, np.dtype([("p", "<f4", (3,)), ("c", "u1", (4,))]))
+    rows["p"] = CUBE_V
+    idx = CUBE_T.astype("<u4").tobytes()
+    blob = rows.tobytes() + idx
+    js = {"asset": {"version": "2.0"}, "meshes": [{"primitives": [{"attributes": {"POSITION": 0}, "indices": 1}]}],
+          "accessors": [{"bufferView": 0, "componentType": 5126, "count": 8, "type": "VEC3"},
+                        {"bufferView": 1, "componentType": 5125, "count": CUBE_T.size, "type": "SCALAR"}],
+          "bufferViews": [{"buffer": 0, "byteOffset": 0, "byteLength": 128, "byteStride": 16},
+                          {"buffer": 0, "byteOffset": 128, "byteLength": len(idx)}],
+          "buffers": [{"byteLength": len(blob), "uri": "data:application/octet-stream;base64,"
+                       + base64.b64encode(blob).decode()}]}
+    (tmp_path / "i.gltf").write_text(json.dumps(js))
+    v, t = meshio.load_mesh(tmp_path / "i.gltf")             # no nodes: every mesh, untransformed
+    assert v.tolist() == CUBE_V.tolist() and t.tolist() == CUBE_T.tolist()
+
+
+def test_malformed_files_raise_value_error(tmp_path):
+    good = meshio.glb_bytes([(CUBE_V, CUBE_T)], ["c_0"])
+    cases = {"short.glb": good[:40], "bad.glb": b"glTF" + b"\0" * 16, "x.ply": b"ply\nformat ascii 1.0\n",
+             "y.ply": b"ply\nformat binary_little_endian 1.0\nelement vertex 8\nproperty float x\n"
+                      b"property float y\nproperty float z\nend_header\n" + b"\0" * 10,
+             "z.off": b"OF\n", "w.obj": b"v 0 0 0\nv 1 0 0\nv 0 1 0\nf 1 2 9\n", "q.stl": b"solid x\nvertex 0 0 0\n",
+             "n.xyz": b""}
+    for name, data in cases.items():
+        (tmp_path / name).write_bytes(data)
+        with pytest.raises(ValueError):
+            meshio.load_mesh(tmp_path / name)
