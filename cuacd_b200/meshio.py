@@ -61,10 +61,18 @@ def clean_mesh(verts, tris):
 
 
 def load_mesh(path):
-    """(verts, tris) of a mesh file, by its extension."""
+    """(verts, tris) of a mesh file, by its extension.  A file that does not
+    parse raises ValueError."""
     ext = os.path.splitext(str(path))[1].lower()
     with open(path, "rb") as f:
         data = f.read()
+    try:
+        return _load(data, ext, path)
+    except (IndexError, KeyError, struct.error, UnicodeDecodeError) as e:
+        raise ValueError(f"malformed {ext or 'mesh'} file: {type(e).__name__}: {e}") from None
+
+
+def _load(data, ext, path):
     if ext == ".obj":
         v, t = read_obj(data)
     elif ext == ".stl":

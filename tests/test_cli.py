@@ -367,7 +367,9 @@ def test_malformed_files_raise_value_error(tmp_path):
              "y.ply": b"ply\nformat binary_little_endian 1.0\nelement vertex 8\nproperty float x\n"
                       b"property float y\nproperty float z\nend_header\n" + b"\0" * 10,
              "z.off": b"OF\n", "w.obj": b"v 0 0 0\nv 1 0 0\nv 0 1 0\nf 1 2 9\n", "q.stl": b"solid x\nvertex 0 0 0\n",
-             "n.xyz": b""}
+             "n.xyz": b"", "h.off": b"OFF\n", "s.stl": b"solid x\nvertex 0 0\n",
+             "f.ply": b"ply\nformat ascii 1.0\nelement vertex 3\nproperty float x\nproperty float y\nproperty float z\n"
+                      b"element face 1\nproperty list uchar int corners\nend_header\n0 0 0\n1 0 0\n0 1 0\n3 0 1 2\n"}
     for name, data in cases.items():
         (tmp_path / name).write_bytes(data)
         with pytest.raises(ValueError):
