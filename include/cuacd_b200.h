@@ -129,11 +129,6 @@ int gpu_mesh_audit(gpu_ctx_t ctx, const float* verts, int n_verts, const int* tr
 int gpu_preprocess(gpu_ctx_t ctx, const float* verts, int nv, const int* tris, int nt,
                    int resolution, float** out_verts, int* out_nv, int** out_tris, int* out_nt);
 
-/* The remesh's marching-cubes case table (no counterpart in the reference,
- * which contours with a dual method): per case, 17 ints -- the number of
- * loops, four loop lengths, twelve cube edges (loops one after another, -1
- * padded).  Host only; for checking the table. */
-void cuacd_remesh_case_table(int* out);
 
 /* Replaces gpu_test_postprocess_dc (csrc/postprocess.h:20-27): split a mesh
  * into its vertex-connected components.  Component c's vertices go to
@@ -215,17 +210,6 @@ int cuacd_hausdorff(gpu_ctx_t ctx,
                     float resolution, int min_samples, int total,
                     float* out_hausdorff);
 
-/* Diagnostic: allocation throughput of the device arena that replaces the
- * reference's device heap (heap_alloc/heap_free, cuda/allocator.cuh:110-362),
- * on the workload of its heap benchmark (bench/malloc_test_bench.cu:76-125):
- * `grid` blocks, thread 0 of each makes `iters` allocations of log-uniform
- * sizes in [size_min, size_max] into `slots` per-block slots.  The arena
- * frees by whole-arena reset, once per run (arena_bytes of pool).  Reports
- * the mean and deviation of the kernel time over `measure` runs after
- * `warmup`, and the allocations of the last run that did not fit. */
-int cuacd_arena_bench(gpu_ctx_t ctx, int grid, int iters, int slots, unsigned size_min, unsigned size_max,
-                      unsigned long long arena_bytes, int warmup, int measure, float* out_mean_ms,
-                      float* out_std_ms, int* out_fail);
 
 /* Batched Hausdorff distance of n_pairs mesh pairs (A_i, B_i), each stage
  * launched once for the whole batch.  Replaces the reference's batch of
@@ -288,18 +272,6 @@ int cuacd_hull_batch_device(gpu_ctx_t ctx, const float* d_pts,
                             int* d_out_nv, int* d_out_nt, float* d_out_vol,
                             int* d_out_errors, void* stream);
 
-/* Diagnostic: exact hulls of a batch of clouds (host pointers) with the
- * hull kernels' work counters, 8 per cloud: BVH leaves kept by the wraps,
- * wraps, faces, points tested by the wraps, SM cycles spent in set-up (sort,
- * BVH, first face), device clock (ns) when the wrapping took the cloud's
- * first edge and when it finished, large faces (+ 2^32 per wrap on the
- * cloud's own node lists, + 2^48 per face built in its own buffers).  For a
- * cloud whose construction failed, slots 4-7 instead hold the first failure
- * as pairs of 32-bit values (low, high): (site, u), (v, c), (coplanar count,
- * corner count), and for a failed wrap the input indices of u and v. */
-int cuacd_hull_stats(gpu_ctx_t ctx, const float* pts, int total_pts,
-                     const int* offsets, int n_hulls, int* out_nv, int* out_nt,
-                     float* out_vol, unsigned long long* out_stats);
 
 /* Launch-shape tuning of the batched hull pipeline (no counterpart in the
  * reference, whose launch shapes are fixed: csrc/lookahead.c:572-573,
@@ -325,12 +297,6 @@ int cuacd_hull_get_table_limit(gpu_ctx_t ctx, int size_class, int* reduce_max_n)
  * streaming multiprocessor count (no counterpart in the reference). */
 int cuacd_device_info(gpu_ctx_t ctx, char* name, int cap, int* n_sm);
 
-/* Diagnostic (no counterpart in the reference): cut one mesh by n_planes
- * planes and report 8 ints per plane: crossing edges, boundary edges, cap
- * loops, cap triangles, and the SM cycles / 64 spent in the crossing,
- * split, boundary and cap+output phases of the cut kernel. */
-int cuacd_cut_stats(gpu_ctx_t ctx, const float* verts, int nv, const int* tris, int nt,
-                    const float* planes, int n_planes, int* out_stats);
 
 /* Number of kernel launches issued by this context so far (a counter the
  * benchmark reads around its timed region). */
@@ -385,11 +351,6 @@ int cuacd_scorer_train(gpu_ctx_t ctx, cuacd_scorer_t s, const float* X, const fl
 
 int cuacd_scorer_predict(gpu_ctx_t ctx, cuacd_scorer_t s, const float* X, int n, float* out);
 
-/* Diagnostic (no counterpart in the reference): scorer GEMM launches so far
- * in this process, by how their A operand reached shared memory -- by TMA
- * (a K-major contiguous A whose tensor map the driver accepted) or by the
- * CTA's own copies (strided or broadcast operands). */
-void cuacd_scorer_gemm_counts(unsigned long long* tma, unsigned long long* staged);
 
 /* Surrogate-pruned evaluation (at most 1024 planes): predicted scores for
  * all planes, the exact evaluator for the top_k best predictions plus every
@@ -522,6 +483,9 @@ int cuacd_lookahead_trace(gpu_ctx_t ctx, cuacd_scorer_t scorer, float* out_rows,
                           int max_iters, int width, int width2, float threshold, int depth,
                           int max_n_cutting, int n_concave_edges, float concave_eps,
                           float concave_threshold, int concave_iters, struct gpu_result* out);
+
+/* Diagnostics (work counters, phase timers, an allocator benchmark, the
+ * remesh's case table) are declared in cuacd_b200_diag.h. */
 
 #ifdef __cplusplus
 }

@@ -1,5 +1,6 @@
-"""The C-ABI library loads and exports every symbol include/cuacd_b200.h
-declares (CPU only; no compute call needs a GPU here)."""
+"""The C-ABI library loads and exports every symbol that include/cuacd_b200.h
+(the drop-in ABI) and include/cuacd_b200_diag.h (diagnostics) declare (CPU
+only; no compute call needs a GPU here)."""
 import ctypes
 import os
 import re
@@ -8,7 +9,7 @@ from conftest import ROOT
 
 
 def declared_functions():
-    src = open(os.path.join(ROOT, "include", "cuacd_b200.h")).read()
+    src = "".join(open(os.path.join(ROOT, "include", h)).read() for h in ("cuacd_b200.h", "cuacd_b200_diag.h"))
     src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
     names = re.findall(r"^\s*(?:[A-Za-z_][\w\s\*]*?)\b([a-z_][a-z0-9_]*)\s*\(", src, flags=re.M)
     return sorted(set(n for n in names if n not in ("if", "sizeof")))
