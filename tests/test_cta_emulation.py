@@ -102,6 +102,41 @@ def test_nested_loops_and_holes_emulated(emu_cut, tmp_path, oracle):
     check(oracle, v, t, planes, rows)
 
 
+def _cylinder(n, r=1.0, h=2.0):
+    a = np.arange(n) * 2 * np.pi / n
+    ring = np.stack([r * np.cos(a), r * np.sin(a), np.zeros(n)], 1)
+    v = np.vstack([ring, ring + [0, 0, h], [[0, 0, 0], [0, 0, h]]]).astype(np.float32)
+    t = []
+    for i in range(n):
+        j = (i + 1) % n
+        t += [(i, j, n + j), (i, n + j, n + i), (2 * n, j, i), (2 * n + 1, n + i, n + j)]
+    return v, np.asarray(t, np.int32)
+
+
+def test_long_cap_and_touching_loops_emulated(emu_cut, tmp_path, oracle):
+    """A 1,500-segment cylinder cut across: one 3,000-vertex cap, longer than
+    the shared-memory ear buffers (ear clipping from global memory; loops
+    traced by pointer jumping).  Two boxes that share an edge once their
+    equal corners are merged: a plane across the edge gives two loops that
+    touch (a vertex with two outgoing boundary edges: the serial walk), and
+    a plane through their shared face fails its cap (the mesh goes back
+    unsplit on the positive side)."""
+    from conftest import l_shape
+    from cuacd_b200 import meshio
+    v, t = _cylinder(1500)
+    planes = np.array([[0, 0, 1, -1.0]], np.float32)
+    rows, reports = run(emu_cut, tmp_path, v, t, planes)
+    assert not reports, reports[:5]
+    check(oracle, v, t, planes, rows)
+    assert rows[0]["cap"] == 2998
+    mv, mt = meshio.clean_mesh(*l_shape())
+    planes = np.array([[0, 0, 1, -0.25], [0, 1, 0, -0.5], [1, 0, 0, -1.0]], np.float32)
+    rows, reports = run(emu_cut, tmp_path, mv, mt, planes)
+    assert not reports, reports[:5]
+    check(oracle, mv, mt, planes, rows)
+    assert [oracle.plane_cut(mv, mt, p)[4]["cap_failed"] for p in planes] == [0, 1, 1]
+
+
 def _build_emu_hull(tmp_path_factory, defines=()):
     if shutil.which("g++") is None:
         pytest.skip("g++ not available")
