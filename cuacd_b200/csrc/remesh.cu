@@ -20,6 +20,7 @@
 // emulation test) and is checked value for value against the oracle.  This
 // file is built with -fmad=false: every FP64 expression rounds as written.
 #include <climits>
+#include <cmath>
 #include <cstdlib>
 #include <cstring>
 #include "context.cuh"
@@ -260,6 +261,9 @@ extern "C" int gpu_preprocess(gpu_ctx_t ctx, const float* verts, int nv, const i
     for (long long i = 0; i < 3ll * nt; i++)
         if (tris[i] < 0 || tris[i] >= nv)
             return ctx_fail(ctx, RM_EINVAL, "preprocess: triangle index %d outside [0, %d)", tris[i], nv);
+    for (long long i = 0; i < 3ll * nv; i++)
+        if (!std::isfinite(verts[i]))
+            return ctx_fail(ctx, RM_EINVAL, "preprocess: vertex coordinate %lld is not finite", i);
     RmParams P;
     float vmax[3];
     for (int k = 0; k < 3; k++) { P.vmin[k] = verts[k]; vmax[k] = verts[k]; }

@@ -77,3 +77,7 @@ def test_bad_arguments(ctx):
         ctx.preprocess(np.zeros((3, 3), np.float32), np.array([[0, 1, 2]]), resolution=16)   # no extent
     with pytest.raises(RuntimeError):
         ctx.preprocess(v, t, resolution=2048)
+    bad = v.copy()
+    bad[3, 1] = np.nan
+    with pytest.raises(RuntimeError):
+        ctx.preprocess(bad, t, resolution=16)                            # refused before any GPU work
