@@ -125,7 +125,8 @@ int gpu_mesh_audit(gpu_ctx_t ctx, const float* verts, int n_verts, const int* tr
  * moved out by 0.9 cells, contoured by marching cubes.  *out_verts /
  * *out_tris are malloc'd (the caller frees them with free()); returns 0, 1
  * for bad arguments (a null pointer, an empty mesh, an index outside
- * [0, nv), a bad resolution, no extent), or a KERR_* / CUDA error. */
+ * [0, nv), a non-finite coordinate, a bad resolution, no extent), or a
+ * KERR_* / CUDA error. */
 int gpu_preprocess(gpu_ctx_t ctx, const float* verts, int nv, const int* tris, int nt,
                    int resolution, float** out_verts, int* out_nv, int** out_tris, int* out_nt);
 

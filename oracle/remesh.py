@@ -16,7 +16,8 @@ the same stages through a third-party rasteriser and a dual marching-cubes
 port; the contouring here is marching cubes with a case table generated
 from one rule (below), which makes every output closed, manifold and
 consistently oriented.  Parity with the reference is on the properties its
-own tests check (tests/test_preprocess.py), not on vertex positions.
+own tests check (tests/test_preprocess.py); vertex positions: parity
+unpinned (the reference's dual contouring places them differently).
 
 Everything is in grid units (u = p_norm * R - 0.5, nodes at integers) and
 float64 in a fixed operation order, which the CUDA path repeats (compiled
