@@ -49,7 +49,7 @@ int cuacd_cut_stats(gpu_ctx_t ctx, const float* verts, int nv, const int* tris, 
 
 /* Diagnostic (no counterpart in the reference): scorer GEMM launches so far
  * in this process, by how their A operand reached shared memory -- by TMA
- * (a K-major contiguous A whose tensor map the driver accepted) or by the
+ * (a K-major contiguous A whose tensor map the CUDA driver accepted) or by the
  * CTA's own copies (strided or broadcast operands). */
 void cuacd_scorer_gemm_counts(unsigned long long* tma, unsigned long long* staged);
 
