@@ -275,7 +275,7 @@ def config4_leg(ctx, scorer):
     return out
 
 
-def remesh_leg(ctx, args):
+def remesh_leg(ctx, args, cpu_baseline=True):
     """Remesh front end (Context.preprocess): the 40,960-triangle ridged
     sphere of the headline workload at resolutions 64 and 128, through the
     public call (host arrays in and out), mean wall time over `steps` calls
@@ -294,6 +294,15 @@ def remesh_leg(ctx, args):
         out[f"R{R}"] = {"ms_per_call": dt * 1e3, "in_tris_per_s": len(t) / dt, "out_tris": int(len(rt)),
                         "out_verts": int(len(rv)), "gpu_launches_per_call": (ctx.launch_count() - l0) / args.steps,
                         "audit_flags": int(ctx.check_mesh(rv, rt)["flags"])}
+    if cpu_baseline and not args.no_cpu_baseline:
+        from oracle import remesh as RMO                    # the CPU restatement, timed as the baseline
+        t0 = time.perf_counter()
+        ov, ot = RMO.remesh(v, t, 64)
+        dt = time.perf_counter() - t0
+        gv, gt = ctx.preprocess(v, t, resolution=64)
+        out["cpu_baseline"] = {"value": dt * 1e3, "unit": "ms per call", "cores": 1, "kind": "port",
+                               "sample": "one call at R = 64 (numpy restatement)",
+                               "same_output": bool(np.array_equal(ov, gv) and np.array_equal(ot, gt))}
     return out
 
 
@@ -1346,7 +1355,7 @@ def main():
     line["config1"] = config1_leg(ctx, stream, flush, args)
     line["config2"] = config2_leg(ctx, stream, flush, args)
     try:
-        line["remesh"] = remesh_leg(ctx, args)
+        line["remesh"] = remesh_leg(ctx, args, cpu_baseline=rank == 0 and world_n == 1)
     except Exception as e:                                   # recorded, never fatal to the bench line
         line["remesh"] = {"error": str(e)[:300]}
     if not args.no_search:
