@@ -143,38 +143,45 @@ def _seg_d2(P, A, B):
 
 
 def point_tri_d2(P, A, B, C):
-    """Squared distance of points P (n, 3) to triangle ABC (float64)."""
+    """Squared distance of points P (..., 3) to triangles ABC (float64;
+    A, B, C broadcast against P, one triangle per leading index)."""
     AB, BC, CA = B - A, C - B, A - C
     n = _cross(AB, C - A)
     nn = _dot(n, n)
     d2 = np.minimum(np.minimum(_seg_d2(P, A, B), _seg_d2(P, B, C)), _seg_d2(P, C, A))
-    if nn > 0:
+    with np.errstate(divide="ignore", invalid="ignore"):
         s0 = _dot(_cross(AB, P - A), n)
         s1 = _dot(_cross(BC, P - B), n)
         s2 = _dot(_cross(CA, P - C), n)
         dp = _dot(P - A, n)
-        inside = (s0 >= 0) & (s1 >= 0) & (s2 >= 0)
-        d2 = np.where(inside, np.minimum(d2, dp * dp / nn), d2)
-    return d2
+        inside = (nn > 0) & (s0 >= 0) & (s1 >= 0) & (s2 >= 0)
+        return np.where(inside, np.minimum(d2, dp * dp / np.where(nn > 0, nn, 1.0)), d2)
 
 
-def distance_grid(u, tris, R):
-    """float32 squared distance per node (x fastest), FAR_D2 beyond the band."""
-    g = np.full((R, R, R), FAR_D2, np.float32)            # [z, y, x]
-    for tri in np.asarray(tris).reshape(-1, 3):
-        A, B, C = u[tri[0]], u[tri[1]], u[tri[2]]
-        lo = np.maximum(np.ceil(np.minimum(np.minimum(A, B), C) - BAND_CELLS), 0).astype(int)
-        hi = np.minimum(np.floor(np.maximum(np.maximum(A, B), C) + BAND_CELLS), R - 1).astype(int)
-        if (hi < lo).any():
-            continue
-        zz, yy, xx = np.meshgrid(np.arange(lo[2], hi[2] + 1), np.arange(lo[1], hi[1] + 1),
-                                 np.arange(lo[0], hi[0] + 1), indexing="ij")
-        P = np.stack([xx, yy, zz], -1).astype(np.float64)
-        d2 = point_tri_d2(P, A, B, C)
-        cand = np.where(d2 <= BAND_CELLS * BAND_CELLS, d2, np.inf).astype(np.float32)
-        sub = g[lo[2]:hi[2] + 1, lo[1]:hi[1] + 1, lo[0]:hi[0] + 1]
-        np.minimum(sub, np.where(np.isinf(cand), FAR_D2, cand), out=sub)
-    return g
+def distance_grid(u, tris, R, chunk=2048):
+    """float32 squared distance per node [z, y, x], FAR_D2 beyond the band.
+    Triangles whose node boxes have the same shape are evaluated together;
+    the least value per node does not depend on the order."""
+    g = np.full(R * R * R, FAR_D2, np.float32)
+    T = np.asarray(tris).reshape(-1, 3)
+    A, B, C = u[T[:, 0]], u[T[:, 1]], u[T[:, 2]]
+    lo = np.maximum(np.ceil(np.minimum(np.minimum(A, B), C) - BAND_CELLS), 0).astype(np.int64)
+    hi = np.minimum(np.floor(np.maximum(np.maximum(A, B), C) + BAND_CELLS), R - 1).astype(np.int64)
+    dims = hi - lo + 1
+    keep = np.flatnonzero((dims > 0).all(1))
+    shapes, group = np.unique(dims[keep], axis=0, return_inverse=True)
+    for gi, (nx, ny, nz) in enumerate(shapes):
+        members = keep[group.reshape(-1) == gi]
+        zz, yy, xx = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+        off = np.stack([xx, yy, zz], -1).reshape(-1, 3)                      # box nodes, x fastest
+        for c0 in range(0, len(members), chunk):
+            m = members[c0:c0 + chunk]
+            node = lo[m][:, None, :] + off[None, :, :]                       # (tris, nodes, 3)
+            d2 = point_tri_d2(node.astype(np.float64), A[m][:, None, :], B[m][:, None, :], C[m][:, None, :])
+            sel = d2 <= BAND_CELLS * BAND_CELLS
+            lin = (node[..., 2] * R + node[..., 1]) * R + node[..., 0]
+            np.minimum.at(g, lin[sel], d2[sel].astype(np.float32))
+    return g.reshape(R, R, R)
 
 
 def _orient(X, Y, Pi, Pj, i, j):
