@@ -188,38 +188,49 @@ def _orient(X, Y, Pi, Pj, i, j):
     return (Y[i] - X[i]) * (Pj - X[j]) - (Y[j] - X[j]) * (Pi - X[i])
 
 
-def crossed_edges(u, tris, R):
-    """bool [3][z, y, x]: grid edge from the node along axis k is crossed."""
-    blk = np.zeros((3, R, R, R), bool)
-    for tri in np.asarray(tris).reshape(-1, 3):
-        A, B, C = u[tri[0]], u[tri[1]], u[tri[2]]
-        for k in range(3):
-            i, j = (k + 1) % 3, (k + 2) % 3
-            area = _orient(A, B, C[i], C[j], i, j)
-            if area == 0:
-                continue
-            a0 = max(int(np.ceil(min(A[i], B[i], C[i]))), 0)
-            a1 = min(int(np.floor(max(A[i], B[i], C[i]))), R - 1)
-            b0 = max(int(np.ceil(min(A[j], B[j], C[j]))), 0)
-            b1 = min(int(np.floor(max(A[j], B[j], C[j]))), R - 1)
-            if a1 < a0 or b1 < b0:
-                continue
-            aa, bb = np.meshgrid(np.arange(a0, a1 + 1, dtype=np.float64), np.arange(b0, b1 + 1, dtype=np.float64),
-                                 indexing="ij")
-            w0 = _orient(B, C, aa, bb, i, j)
-            w1 = _orient(C, A, aa, bb, i, j)
-            w2 = _orient(A, B, aa, bb, i, j)
-            ws = w0 + w1 + w2
-            hit = (((w0 >= 0) & (w1 >= 0) & (w2 >= 0)) | ((w0 <= 0) & (w1 <= 0) & (w2 <= 0))) & (ws != 0)
-            with np.errstate(divide="ignore", invalid="ignore"):
-                z = (w0 * A[k] + w1 * B[k] + w2 * C[k]) / np.where(ws != 0, ws, 1.0)
-            c = np.floor(z)
-            ok = hit & (c >= 0) & (c <= R - 2)
-            for a, b, cc in zip(aa[ok].astype(int), bb[ok].astype(int), c[ok].astype(int)):
-                idx = [0, 0, 0]
-                idx[k], idx[i], idx[j] = cc, a, b
-                blk[k, idx[2], idx[1], idx[0]] = True
-    return blk
+def crossed_edges(u, tris, R, chunk=4096):
+    """bool [3][z, y, x]: grid edge from the node along axis k is crossed.
+    Per axis, triangles whose line boxes have the same shape are tested
+    together (the marks do not depend on the order)."""
+    blk = np.zeros((3, R * R * R), bool)
+    T = np.asarray(tris).reshape(-1, 3)
+    A, B, C = u[T[:, 0]], u[T[:, 1]], u[T[:, 2]]
+    for k in range(3):
+        i, j = (k + 1) % 3, (k + 2) % 3
+        area = (B[:, i] - A[:, i]) * (C[:, j] - A[:, j]) - (B[:, j] - A[:, j]) * (C[:, i] - A[:, i])
+        a0 = np.maximum(np.ceil(np.minimum(np.minimum(A[:, i], B[:, i]), C[:, i])), 0).astype(np.int64)
+        a1 = np.minimum(np.floor(np.maximum(np.maximum(A[:, i], B[:, i]), C[:, i])), R - 1).astype(np.int64)
+        b0 = np.maximum(np.ceil(np.minimum(np.minimum(A[:, j], B[:, j]), C[:, j])), 0).astype(np.int64)
+        b1 = np.minimum(np.floor(np.maximum(np.maximum(A[:, j], B[:, j]), C[:, j])), R - 1).astype(np.int64)
+        dims = np.stack([a1 - a0 + 1, b1 - b0 + 1], 1)
+        keep = np.flatnonzero((area != 0) & (dims > 0).all(1))
+        if len(keep) == 0:
+            continue
+        shapes, group = np.unique(dims[keep], axis=0, return_inverse=True)
+        for gi, (na, nb) in enumerate(shapes):
+            members = keep[group.reshape(-1) == gi]
+            aa0, bb0 = np.meshgrid(np.arange(na), np.arange(nb), indexing="ij")
+            aa0, bb0 = aa0.reshape(-1), bb0.reshape(-1)
+            for c0 in range(0, len(members), chunk):
+                m = members[c0:c0 + chunk]
+                Ai, Aj, Ak = A[m, i][:, None], A[m, j][:, None], A[m, k][:, None]
+                Bi, Bj, Bk = B[m, i][:, None], B[m, j][:, None], B[m, k][:, None]
+                Ci, Cj, Ck = C[m, i][:, None], C[m, j][:, None], C[m, k][:, None]
+                la = a0[m][:, None] + aa0[None, :]
+                lb = b0[m][:, None] + bb0[None, :]
+                pa, pb = la.astype(np.float64), lb.astype(np.float64)
+                w0 = (Ci - Bi) * (pb - Bj) - (Cj - Bj) * (pa - Bi)
+                w1 = (Ai - Ci) * (pb - Cj) - (Aj - Cj) * (pa - Ci)
+                w2 = (Bi - Ai) * (pb - Aj) - (Bj - Aj) * (pa - Ai)
+                ws = w0 + w1 + w2
+                hit = (((w0 >= 0) & (w1 >= 0) & (w2 >= 0)) | ((w0 <= 0) & (w1 <= 0) & (w2 <= 0))) & (ws != 0)
+                with np.errstate(divide="ignore", invalid="ignore"):
+                    z = np.floor((w0 * Ak + w1 * Bk + w2 * Ck) / np.where(ws != 0, ws, 1.0))
+                ok = hit & (z >= 0) & (z <= R - 2)
+                q = [None, None, None]
+                q[k], q[i], q[j] = z[ok].astype(np.int64), la[ok], lb[ok]
+                blk[k, (q[2] * R + q[1]) * R + q[0]] = True
+    return blk.reshape(3, R, R, R)
 
 
 def outside_nodes(blk, R):
