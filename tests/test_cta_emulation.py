@@ -137,6 +137,33 @@ def test_long_cap_and_touching_loops_emulated(emu_cut, tmp_path, oracle):
     assert [oracle.plane_cut(mv, mt, p)[4]["cap_failed"] for p in planes] == [0, 1, 1]
 
 
+def _l_prism():
+    """The L-shaped prism of the reference's boundary-traversal regression
+    (tests/test_boundary_loops.py:10-20 there): one closed manifold with a
+    reflex edge, its six-gon sides split into quads."""
+    xy = np.array([[0, 0], [2, 0], [2, 1], [1, 1], [1, 3], [0, 3]], np.float64)
+    v = np.concatenate([np.column_stack([xy, np.zeros(6)]), np.column_stack([xy, np.ones(6)])])
+    top = np.array([[0, 1, 3], [1, 2, 3], [0, 3, 5], [3, 4, 5]])
+    f = list(top[:, [0, 2, 1]]) + list(top + 6)
+    for i in range(6):
+        j = (i + 1) % 6
+        f += [[i, j, j + 6], [i, j + 6, i + 6]]
+    lo, hi = v.min(0), v.max(0)
+    v = (v - (lo + hi) / 2) / ((hi - lo).max() / 2)
+    return v.astype(np.float32), np.asarray(f, np.int32)
+
+
+def test_l_prism_cuts_emulated(emu_cut, tmp_path, oracle):
+    """Planes through the L-prism's notch, along its faces and oblique:
+    every barrier reached by the whole CTA, the oracle's counts."""
+    v, t = _l_prism()
+    planes = np.array([[1, 0, 0, 0.0], [0, 1, 0, 0.3333333], [0, 0, 1, 0.0], [1, 0, 0, 0.3333333],
+                       [0.6, 0.8, 0, -0.1], [0.48, 0.36, 0.8, 0.05], [0, 1, 0, -0.3333333]], np.float32)
+    rows, reports = run(emu_cut, tmp_path, v, t, planes)
+    assert not reports, reports[:5]
+    check(oracle, v, t, planes, rows)
+
+
 def _build_emu_hull(tmp_path_factory, defines=()):
     if shutil.which("g++") is None:
         pytest.skip("g++ not available")
